@@ -1,0 +1,466 @@
+#!/usr/bin/env python
+"""Render-path benchmark: panorama output Mpix/s of the B200 backend.
+
+Workload (one step): the full-size plain-method panorama - 24 RGGB frames of
+6000x4000 at 14 bits (black 512, gain U(0.7, 1.4), sigma_read 3 DN) in a 3x8
+grid with 30% overlap and focal length 4500 px, giving a 35400x9600 output in
+2048x2048 tiles with a 6-level seam blend.  A step demosaics the 24 CFA frames
+(device resident) and renders every tile: warp + gain + coverage, exact chamfer
+distance, ownership, seam DP and the multi-band compose.  Inputs (1.15 GB of
+CFA) and outputs (2 GB) are far larger than the 126 MB L2, so no flush is
+needed between steps.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Under torchrun each rank renders its own seeded panorama (independent
+objects, no data-path collective): weak scaling, value = all ranks' output
+pixels / max-over-ranks time.  Rank 0 prints one JSON line.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "Panorama output Mpix/s on 1 B200: learned vs plain blend at ≥45 dB PSNR"
+UNIT = "Mpix/s"
+PEAKS_FALLBACK = {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0}
+
+
+def log(*a):
+    print(*a, file=sys.stderr, flush=True)
+
+
+def measured_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return d, "measured"
+    return PEAKS_FALLBACK, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks/throttle sampling during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except Exception:
+            self.proc = None
+        time.sleep(0.3)
+        return self
+
+    def __exit__(self, *exc):
+        self.out = ""
+        if self.proc:
+            time.sleep(0.3)
+            self.proc.terminate()
+            try:
+                self.out, _ = self.proc.communicate(timeout=5)
+            except Exception:
+                self.proc.kill()
+        return False
+
+    def summary(self):
+        rows = []
+        for ln in (self.out or "").splitlines():
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                rows.append((float(parts[1]), float(parts[2]), float(parts[3]) if parts[3] not in ("[N/A]", "") else 0.0,
+                             parts[5:9]))
+            except ValueError:
+                continue
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        load = [r for r in rows if r[2] > 200.0] or rows
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in load for i, v in enumerate(r[3]) if v.lower().startswith("active")})
+        return {"sm_mhz": float(np.median([r[0] for r in load])), "sm_max_mhz": max(r[1] for r in rows),
+                "reasons": reasons, "samples": len(rows), "power_w_max": max(r[2] for r in rows)}
+
+
+# ---------------------------------------------------------------------------
+# our arm
+# ---------------------------------------------------------------------------
+def setup_ours(cfg, rank, device):
+    import torch
+
+    from image360_b200 import COORDS_REFERENCE, B200ComputeBackend, RenderPlan, synth
+    t0 = time.time()
+    cfg = synth.PanoConfig(**{**cfg.__dict__, "seed": cfg.seed + 1000 * rank})
+    pano = synth.make_panorama(cfg, device=device)
+    torch.cuda.synchronize()
+    log(f"[rank {rank}] synthetic panorama {pano.canvas_w}x{pano.canvas_h}, {len(pano.cfa)} frames, "
+        f"{len(pano.tiles)} tiles in {time.time() - t0:.1f}s")
+    be = B200ComputeBackend()
+    assert be.initialize() == 0, be.get_last_error()
+    black, cm, rc, filt = synth.demosaic_params(cfg)
+    cfa = [c.view(torch.int16).contiguous() for c in pano.cfa]
+    rgb = [torch.empty((cfg.frame_h, cfg.frame_w, 3), dtype=torch.int16, device=device) for _ in cfa]
+    outs = [torch.empty((t[3], t[2], 3), dtype=torch.int16, device=device) for t in pano.tiles]
+    gains = (1.0 / pano.gains).astype(np.float32)
+    frames = [(r.data_ptr(), cfg.frame_w, cfg.frame_h, H, float(g)) for r, H, g in zip(rgb, pano.to_canvas, gains)]
+    tiles = [(x, y, w, h, cs, o.data_ptr()) for (x, y, w, h, cs), o in zip(pano.tiles, outs)]
+    plan = RenderPlan(frames, tiles, cfg.bands, COORDS_REFERENCE)
+    return dict(cfg=cfg, pano=pano, be=be, cfa=cfa, rgb=rgb, outs=outs, plan=plan, demosaic=(black, cm, rc, filt))
+
+
+def make_step(S, stream_ptr):
+    be, plan = S["be"], S["plan"]
+    black, cm, rc, filt = S["demosaic"]
+    w, h = S["cfg"].frame_w, S["cfg"].frame_h
+    pairs = [(c.data_ptr(), r.data_ptr()) for c, r in zip(S["cfa"], S["rgb"])]
+
+    def step():
+        for c, r in pairs:
+            if be.launch_demosaic(c, w, h, black, cm, rc, filt, r, stream_ptr) != 0:
+                raise RuntimeError(be.get_last_error())
+        if plan.execute(stream_ptr) != 0:
+            raise RuntimeError(be.get_last_error())
+    return step
+
+
+def stage_bytes(stats, S):
+    """Algorithmic bytes per stage (formulas stated in DESIGN.md)."""
+    cfg = S["cfg"]
+    npx_in = len(S["cfa"]) * cfg.frame_w * cfg.frame_h
+    cov = stats["coveredItemPixels"]
+    out = stats["outputPixels"]
+    item_px = sum(t[2] * t[3] * len(t[4]) for t in S["pano"].tiles)
+    return {
+        "demosaic": npx_in * (2 + 6),
+        "warp_gain_coverage": cov * 6 * 2,
+        "chamfer_forward": item_px // 8 + item_px * 4,
+        "chamfer_backward": item_px * 8,
+        "blend_total": cov * 6 + out * 6,
+    }
+
+
+def run_ours(args, rank, world, local_rank):
+    import torch
+    import torch.distributed as dist
+
+    from image360_b200 import synth
+    device = f"cuda:{local_rank}"
+    torch.cuda.set_device(local_rank)
+    cfg = synth.C1 if args.scale == 1.0 else synth.scaled(synth.C1, args.scale, tile=synth.C1.tile)
+    S = setup_ours(cfg, rank, device)
+    stream = torch.cuda.Stream(device=device)
+    sp = stream.cuda_stream
+    step = make_step(S, sp)
+    plan = S["plan"]
+    with torch.cuda.stream(stream):
+        for _ in range(args.warmup):
+            step()
+        assert plan.wait(sp) == 0, S["be"].get_last_error()
+    torch.cuda.synchronize()
+    stats = plan.stats(sp)
+    stages = plan.profile(sp)
+    # demosaic stage timed alone with events on the launching stream
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
+    be, (black, cm, rc, filt) = S["be"], S["demosaic"]
+    with torch.cuda.stream(stream):
+        ev[0].record(stream)
+        for c, r in zip(S["cfa"], S["rgb"]):
+            be.launch_demosaic(c.data_ptr(), cfg.frame_w, cfg.frame_h, black, cm, rc, filt, r.data_ptr(), sp)
+        ev[1].record(stream)
+    torch.cuda.synchronize()
+    stages = {"demosaic": ev[0].elapsed_time(ev[1]), **stages}
+    # timed region
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local_rank) as clk:
+        with torch.cuda.stream(stream):
+            t0.record(stream)
+            for _ in range(args.steps):
+                step()
+            t1.record(stream)
+        torch.cuda.synchronize()
+    ms = t0.elapsed_time(t1)
+    assert plan.wait(sp) == 0, S["be"].get_last_error()
+    if world > 1:
+        tt = torch.tensor([ms], device=device, dtype=torch.float64)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        ms = float(tt.item())
+        dist.barrier()
+    out_px = stats["outputPixels"]
+    ms_step = ms / args.steps
+    value = world * out_px / 1e6 / (ms_step / 1e3)
+    e2e = run_e2e(args, S, stream, world, device) if not args.no_e2e else None
+    if rank != 0:
+        return None
+    peaks, peak_kind = measured_peaks()
+    sb = stage_bytes(stats, S)
+    blend_stages = ["chamfer_forward", "chamfer_backward", "ownership", "seam_dp", "pyramid_down", "blend_bands",
+                    "collapse", "level0_output"]
+    blend_ms = sum(stages[s] for s in blend_stages)
+    dom = max(stages, key=lambda k: stages[k])
+    dom_bytes = sb.get(dom)
+    roof = None
+    if dom_bytes is not None:
+        ach = dom_bytes / (stages[dom] / 1e3) / 1e9
+        roof = {"kernel": dom, "bound": "hbm", "achieved": round(ach, 1), "peak": peaks["hbm_gbs"], "unit": "GB/s",
+                "frac": round(ach / peaks["hbm_gbs"], 4), "traffic": None, "peak_source": peak_kind}
+    else:
+        roof = {"kernel": dom, "bound": "hbm", "achieved": None, "peak": peaks["hbm_gbs"], "unit": "GB/s",
+                "frac": None, "traffic": None, "peak_source": peak_kind}
+    per_stage = {}
+    for k, v in stages.items():
+        d = {"ms": round(v, 3)}
+        if k in sb:
+            d["GBps"] = round(sb[k] / (v / 1e3) / 1e9, 1)
+            d["frac"] = round(d["GBps"] / peaks["hbm_gbs"], 4)
+        per_stage[k] = d
+    per_stage["blend_total"] = {"ms": round(blend_ms, 3), "GBps": round(sb["blend_total"] / (blend_ms / 1e3) / 1e9, 1),
+                                "frac": round(sb["blend_total"] / (blend_ms / 1e3) / 1e9 / peaks["hbm_gbs"], 4)}
+    launches = (len(S["cfa"]) + stats["kernelsPerExecute"]) * args.steps
+    line = {
+        "metric": METRIC, "value": round(value, 2), "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": round(ms_step, 3), "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "u16 storage / fp32 arithmetic", "data": "synthetic (seeded scene, 14-bit RGGB)",
+        "config": {"workload": f"plain seam blend, 24 x {cfg.frame_w}x{cfg.frame_h} RGGB -> "
+                               f"{S['pano'].canvas_w}x{S['pano'].canvas_h} in {cfg.tile}^2 tiles, {cfg.bands} bands",
+                   "tiles": stats["numTiles"], "tile_contributors": stats["numItems"],
+                   "output_mpix": round(out_px / 1e6, 2), "coords": "reference (bit-exact vs CPU backend)",
+                   "l2": "inputs and outputs larger than L2 (no flush)", "blend": "plain (learned blend not built)",
+                   "parallelism": f"{world} independent panoramas"},
+        "roofline": roof, "stages": per_stage, "gpu_launches": launches,
+        "clocks": clk.summary(),
+        "e2e": e2e,
+    }
+    if not args.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_baseline(S, args)
+    return line
+
+
+def run_e2e(args, S, stream, world, device):
+    """Same step through the public API with HOST buffers: pinned CFA in,
+    H2D copies, demosaic + render, D2H of every output tile, all timed."""
+    import torch
+    sp = stream.cuda_stream
+    step = make_step(S, sp)
+    host_cfa = [c.cpu().pin_memory() for c in S["cfa"]]
+    host_out = [torch.empty(o.shape, dtype=o.dtype).pin_memory() for o in S["outs"]]
+    h2d = sum(c.numel() * 2 for c in host_cfa)
+    d2h = sum(o.numel() * 2 for o in host_out)
+
+    def e2e_step():
+        for hc, dc in zip(host_cfa, S["cfa"]):
+            dc.copy_(hc, non_blocking=True)
+        step()
+        for ho, do in zip(host_out, S["outs"]):
+            ho.copy_(do, non_blocking=True)
+
+    with torch.cuda.stream(stream):
+        for _ in range(max(1, args.warmup // 2)):
+            e2e_step()
+    torch.cuda.synchronize()
+    k = max(1, min(args.steps, 3))
+    t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with torch.cuda.stream(stream):
+        t0.record(stream)
+        for _ in range(k):
+            e2e_step()
+        t1.record(stream)
+    torch.cuda.synchronize()
+    ms = t0.elapsed_time(t1) / k
+    if world > 1:
+        import torch.distributed as dist
+        tt = torch.tensor([ms], device=device, dtype=torch.float64)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        ms = float(tt.item())
+    px = sum(o.shape[0] * o.shape[1] for o in S["outs"])
+    return {"value": round(world * px / 1e6 / (ms / 1e3), 2), "unit": UNIT, "h2d_bytes_per_step": h2d,
+            "d2h_bytes_per_step": d2h, "ms_per_step": round(ms, 3)}
+
+
+# ---------------------------------------------------------------------------
+# CPU side: the reference's own CPU code (oracle/_ref) or the C restatement
+# ---------------------------------------------------------------------------
+def _cpu_impl():
+    import oracle
+    oracle.build()
+    r = oracle.reference()
+    if r is not None:
+        return r, "reference"
+    return oracle.oracle(), "port"
+
+
+def cpu_demosaic_all(impl, kind, cfa_host, cfg, threads):
+    from image360_b200 import synth
+    black, cm, rc, filt = synth.demosaic_params(cfg)
+    if kind != "reference":
+        return [impl.demosaic(c, black, cm, rc, filt) for c in cfa_host]
+    import ctypes as ct
+    import oracle
+    outs = [np.zeros((cfg.frame_h, cfg.frame_w, 3), np.uint16) for _ in cfa_host]
+    impl.lib.ref_demosaic_frames(threads, impl.tier, len(cfa_host), oracle._ptr_array(cfa_host, ct.c_uint16),
+                                 cfg.frame_w, cfg.frame_h, ct.c_uint16(black), cm.ctypes.data_as(oracle._f32p),
+                                 rc.reshape(12).ctypes.data_as(oracle._f32p), ct.c_uint32(filt),
+                                 oracle._ptr_array(outs, ct.c_uint16))
+    return outs
+
+
+def cpu_sample(impl, kind, frames_host, pano, cfg, threads, n_tiles, n_frames_dem, cfa_host, gains):
+    """Times a bounded sample of the job on host cores; returns extrapolated
+    job seconds and a description."""
+    from image360_b200 import synth
+    black, cm, rc, filt = synth.demosaic_params(cfg)
+    rng = np.random.default_rng(7)
+    # demosaic sample: n frames on `threads` workers
+    idx = list(range(min(n_frames_dem, len(cfa_host))))
+    t0 = time.time()
+    if kind == "reference":
+        import ctypes as ct
+        import oracle
+        outs = [np.zeros((cfg.frame_h, cfg.frame_w, 3), np.uint16) for _ in idx]
+        cptr = oracle._ptr_array([cfa_host[i] for i in idx], ct.c_uint16)
+        optr = oracle._ptr_array(outs, ct.c_uint16)
+        impl.lib.ref_demosaic_frames(threads, impl.tier, len(idx), cptr, cfg.frame_w, cfg.frame_h, ct.c_uint16(black),
+                                     cm.ctypes.data_as(oracle._f32p), rc.reshape(12).ctypes.data_as(oracle._f32p),
+                                     ct.c_uint32(filt), optr)
+    else:
+        for i in idx:
+            impl.demosaic(cfa_host[i], black, cm, rc, filt)
+    t_dem = time.time() - t0
+    dem_job = t_dem * len(cfa_host) / len(idx) if kind == "reference" else t_dem * len(cfa_host) / len(idx) / 1.0
+    # render sample: tiles chosen with a fixed seed
+    order = rng.permutation(len(pano.tiles))[:n_tiles]
+    sample = [pano.tiles[i] for i in order]
+    inv = np.stack([synth.inverse_homography_f32(H) for H in pano.to_canvas])
+    if kind == "reference":
+        secs, _ = impl.render_tiles(threads, frames_host, inv, gains, sample, cfg.bands, want_out=False)
+    else:
+        secs, _ = impl.render_tiles(threads, frames_host, inv, gains, sample, cfg.bands, want_out=False)
+    work = lambda ts: sum(t[2] * t[3] * max(1, len(t[4])) for t in ts)
+    render_job = secs * work(pano.tiles) / work(sample)
+    return dem_job + render_job, t_dem + secs, (f"{len(idx)} frames demosaiced + {len(sample)} of {len(pano.tiles)} "
+                                               f"tiles rendered on {threads} threads, extrapolated by frames and "
+                                               f"by tile area x contributors")
+
+
+def cpu_baseline(S, args):
+    import torch
+    impl, kind = _cpu_impl()
+    threads = max(1, (os.cpu_count() or 2) - 1)
+    cfg, pano = S["cfg"], S["pano"]
+    frames_host = [r.cpu().numpy().view(np.uint16) for r in S["rgb"]]
+    cfa_host = [c.cpu().numpy().view(np.uint16) for c in S["cfa"]]
+    gains = (1.0 / pano.gains).astype(np.float32)
+    n_tiles = max(threads, args.cpu_tiles)
+    job_s, spent, desc = cpu_sample(impl, kind, frames_host, pano, cfg, threads, n_tiles, max(2, threads // 2),
+                                    cfa_host, gains)
+    out_px = sum(t[2] * t[3] for t in pano.tiles)
+    return {"value": round(out_px / 1e6 / job_s, 3), "unit": UNIT, "cores": threads, "kind": kind,
+            "sample": desc, "sample_seconds": round(spent, 1), "threads_model": "hardware_concurrency()-1 tasks"}
+
+
+def run_reference(args, rank, world):
+    """The reference's own CPU implementation of the path on this host's
+    cores, on the same workload, bounded per step; rank 0 only."""
+    if rank != 0:
+        return None
+    from image360_b200 import synth
+    impl, kind = _cpu_impl()
+    threads = os.cpu_count() or 1
+    cfg = synth.C1 if args.scale == 1.0 else synth.scaled(synth.C1, args.scale, tile=synth.C1.tile)
+    device = "cpu"
+    try:
+        import torch
+        if torch.cuda.is_available():
+            device = "cuda:0"  # synthetic input generation only; timed work is on the CPU
+    except Exception:
+        pass
+    pano = synth.make_panorama(cfg, device=device)
+    cfa_host = [c.cpu().numpy().view(np.uint16) for c in pano.cfa]
+    black, cm, rc, filt = synth.demosaic_params(cfg)
+    gains = (1.0 / pano.gains).astype(np.float32)
+    # every frame demosaiced once by the CPU code itself (untimed setup);
+    # the timed steps re-demosaic a sample of frames and render a sample of tiles
+    frames_host = cpu_demosaic_all(impl, kind, cfa_host, cfg, threads)
+    times = []
+    for s in range(args.warmup + args.steps):
+        job_s, spent, desc = cpu_sample(impl, kind, frames_host, pano, cfg, threads, max(threads, args.cpu_tiles),
+                                        max(2, threads // 2), cfa_host, gains)
+        if s >= args.warmup:
+            times.append(job_s)
+    out_px = sum(t[2] * t[3] for t in pano.tiles)
+    job = float(np.mean(times))
+    value = out_px / 1e6 / job
+    return {"metric": METRIC, "value": round(value, 3), "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": round(job * 1e3, 1), "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "u16 storage / fp32 arithmetic", "data": "synthetic (seeded scene, 14-bit RGGB)",
+            "impl": "reference",
+            "config": {"workload": f"plain seam blend, 24 x {cfg.frame_w}x{cfg.frame_h} RGGB -> "
+                                   f"{pano.canvas_w}x{pano.canvas_h} in {cfg.tile}^2 tiles, {cfg.bands} bands",
+                       "parallelism": f"{threads} host threads"},
+            "cpu_baseline": {"value": round(value, 3), "unit": UNIT, "cores": threads, "kind": kind, "sample": desc},
+            "e2e": {"value": round(value, 3), "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--scale", type=float, default=1.0, help="geometry scale of the workload (1.0 = full size)")
+    ap.add_argument("--cpu-tiles", type=int, default=8, help="tiles in the CPU-baseline sample")
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3 and args.impl == "ours":
+        log("note: warmup raised to 3")
+        args.warmup = 3
+    rank = int(os.environ.get("RANK", 0))
+    world = int(os.environ.get("WORLD_SIZE", 1))
+    local_rank = int(os.environ.get("LOCAL_RANK", 0))
+    if world > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as dist
+        os.environ.setdefault("MASTER_ADDR", "127.0.0.1")
+        if args.impl == "ours":
+            torch.cuda.set_device(local_rank)
+        dist.init_process_group("nccl" if args.impl == "ours" else "gloo", timeout=datetime.timedelta(seconds=600))
+    try:
+        if args.impl == "reference":
+            line = run_reference(args, rank, world)
+        else:
+            line = run_ours(args, rank, world, local_rank)
+        if rank == 0 and line is not None:
+            print(json.dumps(line), flush=True)
+    finally:
+        if world > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,289 @@
+"""image360_b200: B200 (sm_100a) render backend for the Image360 stitching engine.
+
+Python mirror of the backend's C-ABI (``include/image360_b200.h``) for tests,
+benchmarks and Python callers.  The compute runs in the in-tree shared library
+``image360_b200/lib/libimage360_b200.so`` (hand-written sm_100a kernels); this
+module only marshals arguments.  There is no CPU fallback: if the library is
+missing, loading fails loudly.
+
+Method names and argument meaning follow ``WindowsApp::Compute::IComputeBackend``
+(WindowsApp.Compute/HeaderFiles/IComputeBackend.h:21-49) and
+``Kernels::SeamBlend::BlendChunkContributors`` (SeamBlendKernels.h:91); every
+call returns a ``ComputeResult`` code (ComputeTypes.h:32-50).
+"""
+from __future__ import annotations
+
+import ctypes as ct
+import enum
+import os
+import re
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "lib", "libimage360_b200.so")
+HEADER = os.path.join(HERE, "..", "include", "image360_b200.h")
+
+__all__ = ["ComputeResult", "B200ComputeBackend", "RenderPlan", "load_library", "exported_symbols",
+           "header_symbols", "COORDS_REFERENCE", "COORDS_FP64_ORIGIN"]
+
+COORDS_REFERENCE = 0
+COORDS_FP64_ORIGIN = 1
+
+
+class ComputeResult(enum.IntEnum):
+    """WindowsApp::Compute::ComputeResult (ComputeTypes.h:32-50)."""
+    SUCCESS = 0
+    NO_GPU = 1
+    INVALID_PARAM = 2
+    OUT_OF_MEMORY = 3
+    KERNEL_LAUNCH_FAILED = 4
+    CUDA_ERROR = 5
+    NOT_SUPPORTED = 6
+
+
+class GpuInfo(ct.Structure):
+    _fields_ = [("deviceId", ct.c_int), ("name", ct.c_char * 256), ("totalMemory", ct.c_size_t),
+                ("freeMemory", ct.c_size_t), ("computeMajor", ct.c_int), ("computeMinor", ct.c_int),
+                ("maxThreadsPerBlock", ct.c_int), ("multiProcessorCount", ct.c_int), ("hasTensorCores", ct.c_int)]
+
+
+class Frame(ct.Structure):
+    _fields_ = [("rgb", ct.c_void_p), ("width", ct.c_int), ("height", ct.c_int), ("toCanvas", ct.c_double * 9),
+                ("gain", ct.c_float)]
+
+
+class RenderStats(ct.Structure):
+    _fields_ = [("numTiles", ct.c_int), ("numItems", ct.c_int), ("kernelsPerExecute", ct.c_int),
+                ("outputPixels", ct.c_longlong), ("coveredItemPixels", ct.c_longlong), ("scratchBytes", ct.c_longlong)]
+
+
+class Tile(ct.Structure):
+    _fields_ = [("x", ct.c_int), ("y", ct.c_int), ("width", ct.c_int), ("height", ct.c_int), ("first", ct.c_int),
+                ("count", ct.c_int), ("dOut", ct.c_void_p)]
+
+
+_u16p = ct.POINTER(ct.c_uint16)
+_f32p = ct.POINTER(ct.c_float)
+_lib = None
+
+
+def header_symbols(path: str = HEADER) -> list[str]:
+    """Names of the functions declared in the C-ABI header."""
+    text = open(path).read()
+    return sorted(set(re.findall(r"I360B_API\s+[\w\s\*]*?\b(i360b_\w+)\s*\(", text)))
+
+
+def load_library(path: str = LIB_PATH):
+    """Loads the in-tree library (build it with image360_b200.build)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(path):
+        raise RuntimeError(f"image360_b200 native library not built: {path} (run python -m image360_b200.build)")
+    L = ct.CDLL(path)
+    vp, i, f = ct.c_void_p, ct.c_int, ct.c_float
+    L.i360b_get_last_error.restype = ct.c_char_p
+    L.i360b_render_plan_scratch_bytes.restype = ct.c_size_t
+    L.i360b_render_plan_scratch_bytes.argtypes = [vp]
+    L.i360b_render_plan_create.argtypes = [ct.POINTER(Frame), i, ct.POINTER(Tile), i, ct.POINTER(ct.c_int), i, i,
+                                           ct.POINTER(vp)]
+    L.i360b_render_plan_execute.argtypes = [vp, vp]
+    L.i360b_render_plan_wait.argtypes = [vp, vp]
+    L.i360b_render_plan_destroy.argtypes = [vp]
+    L.i360b_render_plan_stats.argtypes = [vp, vp, ct.POINTER(RenderStats)]
+    L.i360b_render_plan_profile.argtypes = [vp, vp, ct.POINTER(ct.c_float), i]
+    L.i360b_render_stage_name.restype = ct.c_char_p
+    L.i360b_launch_demosaic.argtypes = [vp, i, i, ct.c_uint16, _f32p, _f32p, ct.c_uint32, vp, vp]
+    L.i360b_launch_warp.argtypes = [vp, i, i, vp, i, i, _f32p, i, i, f, vp]
+    L.i360b_launch_median.argtypes = [ct.POINTER(vp), i, vp, i, i, f, vp]
+    L.i360b_launch_gain.argtypes = [vp, i, f, vp]
+    L.i360b_launch_blend.argtypes = [ct.POINTER(vp), i, i, i, i, vp, vp]
+    _lib = L
+    return L
+
+
+def exported_symbols(path: str = LIB_PATH) -> list[str]:
+    """Dynamic symbols the library exports (via nm; no CUDA call)."""
+    import subprocess
+    out = subprocess.run(["nm", "-D", "--defined-only", path], capture_output=True, text=True, check=True).stdout
+    return sorted({ln.split()[-1] for ln in out.splitlines() if " T " in ln})
+
+
+def _p16(a: np.ndarray):
+    return a.ctypes.data_as(_u16p)
+
+
+def _pf(a: np.ndarray):
+    return a.ctypes.data_as(_f32p)
+
+
+class B200ComputeBackend:
+    """Host-buffer operations of IComputeBackend, executed on the B200.
+
+    Mirrors the reference's backend object: ``initialize()`` first, then each
+    operation returns a ComputeResult; ``get_last_error()`` gives the message.
+    Output arrays are written in place, exactly as the reference's caller-owned
+    output buffers are.
+    """
+
+    def __init__(self):
+        self.lib = load_library()
+
+    # lifecycle (IComputeBackend.h:21-25)
+    def initialize(self) -> ComputeResult:
+        return ComputeResult(self.lib.i360b_initialize())
+
+    def shutdown(self) -> None:
+        self.lib.i360b_shutdown()
+
+    def is_initialized(self) -> bool:
+        return bool(self.lib.i360b_is_initialized())
+
+    def get_gpu_info(self) -> dict:
+        info = GpuInfo()
+        self.lib.i360b_get_gpu_info(ct.byref(info))
+        return {k: (getattr(info, k).decode() if k == "name" else getattr(info, k)) for k, _ in GpuInfo._fields_}
+
+    def get_last_error(self) -> str:
+        return self.lib.i360b_get_last_error().decode()
+
+    # IComputeBackend.h:29-32
+    def warp_perspective(self, src: np.ndarray, dst: np.ndarray, homography, offset_x: int = 0,
+                         offset_y: int = 0) -> ComputeResult:
+        src = np.ascontiguousarray(src, np.uint16)
+        H = np.ascontiguousarray(homography, np.float32).reshape(9)
+        assert dst.dtype == np.uint16 and dst.flags.c_contiguous
+        return ComputeResult(self.lib.i360b_warp_perspective(_p16(src), src.shape[1], src.shape[0], _p16(dst),
+                                                             dst.shape[1], dst.shape[0], _pf(H), int(offset_x),
+                                                             int(offset_y)))
+
+    # IComputeBackend.h:35-38
+    def median_stack(self, inputs, output: np.ndarray, width: int, height: int,
+                     sigma_threshold: float = 2.0) -> ComputeResult:
+        ins = [np.ascontiguousarray(a, np.uint16) for a in inputs]
+        arr = (_u16p * max(1, len(ins)))(*[_p16(a) for a in ins])
+        return ComputeResult(self.lib.i360b_median_stack(arr, len(ins), _p16(output), int(width), int(height),
+                                                         ct.c_float(sigma_threshold)))
+
+    # IComputeBackend.h:41-42
+    def apply_gain(self, data: np.ndarray, gain: float) -> ComputeResult:
+        assert data.dtype == np.uint16 and data.flags.c_contiguous
+        return ComputeResult(self.lib.i360b_apply_gain(_p16(data), data.size, ct.c_float(gain)))
+
+    # IComputeBackend.h:46-49
+    def demosaic_bayer(self, cfa: np.ndarray, black_level: int, cam_mul, rgb_cam, filters: int,
+                       rgb_out: np.ndarray) -> ComputeResult:
+        cfa = np.ascontiguousarray(cfa, np.uint16)
+        cm = np.ascontiguousarray(cam_mul, np.float32).reshape(4)
+        rc = np.ascontiguousarray(rgb_cam, np.float32).reshape(12)
+        return ComputeResult(self.lib.i360b_demosaic_bayer(_p16(cfa), cfa.shape[1], cfa.shape[0],
+                                                           ct.c_uint16(black_level), _pf(cm), _pf(rc),
+                                                           ct.c_uint32(filters), _p16(rgb_out)))
+
+    # SeamBlendKernels.h:91 (+ band count)
+    def blend_chunk_contributors(self, warped, width: int, height: int, out: np.ndarray,
+                                 num_bands: int = 5) -> ComputeResult:
+        bufs = [np.ascontiguousarray(b, np.uint16) for b in warped]
+        arr = (_u16p * max(1, len(bufs)))(*[_p16(b) for b in bufs])
+        return ComputeResult(self.lib.i360b_blend_chunk_contributors(arr, len(bufs), int(width), int(height),
+                                                                     int(num_bands), _p16(out)))
+
+    # device-resident launchers: pointers are integers (e.g. torch data_ptr()).
+    def launch_demosaic(self, d_cfa: int, width: int, height: int, black_level: int, cam_mul, rgb_cam, filters: int,
+                        d_out: int, stream: int = 0) -> ComputeResult:
+        cm = np.ascontiguousarray(cam_mul, np.float32).reshape(4)
+        rc = np.ascontiguousarray(rgb_cam, np.float32).reshape(12)
+        return ComputeResult(self.lib.i360b_launch_demosaic(d_cfa, width, height, black_level, _pf(cm), _pf(rc),
+                                                            filters, d_out, stream or None))
+
+    def launch_warp(self, d_src: int, src_w: int, src_h: int, d_dst: int, dst_w: int, dst_h: int, homography,
+                    offset_x: int = 0, offset_y: int = 0, gain: float = 1.0, stream: int = 0) -> ComputeResult:
+        H = np.ascontiguousarray(homography, np.float32).reshape(9)
+        return ComputeResult(self.lib.i360b_launch_warp(d_src, src_w, src_h, d_dst, dst_w, dst_h, _pf(H), offset_x,
+                                                        offset_y, gain, stream or None))
+
+    def launch_median(self, d_inputs, width: int, height: int, d_out: int, sigma: float = 2.0,
+                      stream: int = 0) -> ComputeResult:
+        arr = (ct.c_void_p * max(1, len(d_inputs)))(*d_inputs)
+        return ComputeResult(self.lib.i360b_launch_median(arr, len(d_inputs), d_out, width, height, sigma,
+                                                          stream or None))
+
+    def launch_gain(self, d_data: int, n: int, gain: float, stream: int = 0) -> ComputeResult:
+        return ComputeResult(self.lib.i360b_launch_gain(d_data, n, gain, stream or None))
+
+    def launch_blend(self, d_warped, width: int, height: int, d_out: int, num_bands: int = 5,
+                     stream: int = 0) -> ComputeResult:
+        arr = (ct.c_void_p * max(1, len(d_warped)))(*d_warped)
+        return ComputeResult(self.lib.i360b_launch_blend(arr, len(d_warped), width, height, num_bands, d_out,
+                                                         stream or None))
+
+
+class RenderPlan:
+    """Batched render of a panorama's output tiles (one persistent plan,
+    replayed as a CUDA graph).
+
+    frames: list of (device_ptr, width, height, to_canvas 3x3 (float64), gain).
+    tiles:  list of (x, y, width, height, [frame indices], device_out_ptr).
+    """
+
+    def __init__(self, frames, tiles, num_bands: int, coord_mode: int = COORDS_REFERENCE):
+        self.lib = load_library()
+        fr = (Frame * len(frames))()
+        for i, (ptr, w, h, H, g) in enumerate(frames):
+            fr[i].rgb = ptr
+            fr[i].width = w
+            fr[i].height = h
+            for q, v in enumerate(np.asarray(H, np.float64).reshape(9)):
+                fr[i].toCanvas[q] = float(v)
+            fr[i].gain = g
+        contrib = []
+        tl = (Tile * len(tiles))()
+        for i, (x, y, w, h, cs, out) in enumerate(tiles):
+            tl[i].x, tl[i].y, tl[i].width, tl[i].height = x, y, w, h
+            tl[i].first = len(contrib)
+            tl[i].count = len(cs)
+            tl[i].dOut = out
+            contrib.extend(int(c) for c in cs)
+        carr = (ct.c_int * max(1, len(contrib)))(*contrib)
+        self._h = ct.c_void_p()
+        rc = self.lib.i360b_render_plan_create(fr, len(frames), tl, len(tiles), carr, num_bands, coord_mode,
+                                               ct.byref(self._h))
+        if rc != 0:
+            raise RuntimeError(f"render plan: {ComputeResult(rc).name}: {self.lib.i360b_get_last_error().decode()}")
+
+    @property
+    def scratch_bytes(self) -> int:
+        return self.lib.i360b_render_plan_scratch_bytes(self._h)
+
+    def stats(self, stream: int = 0) -> dict:
+        st = RenderStats()
+        rc = self.lib.i360b_render_plan_stats(self._h, stream or None, ct.byref(st))
+        if rc != 0:
+            raise RuntimeError(self.lib.i360b_get_last_error().decode())
+        return {k: getattr(st, k) for k, _ in RenderStats._fields_}
+
+    def profile(self, stream: int = 0) -> dict:
+        """One un-captured run with CUDA events between stages: {stage: ms}."""
+        ms = (ct.c_float * 16)()
+        rc = self.lib.i360b_render_plan_profile(self._h, stream or None, ms, 16)
+        if rc != 0:
+            raise RuntimeError(self.lib.i360b_get_last_error().decode())
+        return {self.lib.i360b_render_stage_name(i).decode(): float(ms[i]) for i in range(9)}
+
+    def execute(self, stream: int = 0) -> ComputeResult:
+        return ComputeResult(self.lib.i360b_render_plan_execute(self._h, stream or None))
+
+    def wait(self, stream: int = 0) -> ComputeResult:
+        return ComputeResult(self.lib.i360b_render_plan_wait(self._h, stream or None))
+
+    def close(self) -> None:
+        if self._h:
+            self.lib.i360b_render_plan_destroy(self._h)
+            self._h = ct.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

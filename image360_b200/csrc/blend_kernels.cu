@@ -1,0 +1,873 @@
+// Seam-blend kernels for a batch of tiles.  Every kernel reproduces the FP32
+// arithmetic of WindowsApp.Core/SourceFiles/SeamBlend.cpp in the same order,
+// so the GPU owner map and output are bit-identical to the CPU backend's.
+#include "blend_kernels.cuh"
+
+#include <cuda/atomic>
+#include <cfloat>
+
+namespace i360b
+{
+namespace
+{
+constexpr unsigned kFull = 0xffffffffu;
+constexpr long long kSpinCycles = 2000000000ll;  // ~1 s at B200 clocks: bounded waits
+
+__device__ __forceinline__ float f_inf() { return __int_as_float(0x7f800000); }
+
+__device__ __forceinline__ bool cov_bit(const uint32_t* cov, int covWords, int x, int y)
+{
+    return (__ldg(cov + (size_t)y * covWords + (x >> 5)) >> (x & 31)) & 1u;
+}
+
+// ---------------------------------------------------------------------------
+// Coverage (SeamBlend.cpp:564-567): covered = any channel != 0, as bits, plus
+// the inclusive bounding box of covered pixels (SeamBlend.cpp:263-280).
+// A warp owns 32 consecutive pixels of one row, so its ballot is one word.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ void emit_coverage(const ItemDev& it, const TileDev& T, int x, int y, bool covered)
+{
+    unsigned m = __ballot_sync(kFull, covered);
+    int lane = threadIdx.x & 31;
+    if (y < T.h && lane == 0) it.cov[(size_t)y * T.covWords + (x >> 5)] = m;
+    if (m)
+    {
+        int mnx = __reduce_min_sync(kFull, covered ? x : 0x7fffffff);
+        int mxx = __reduce_max_sync(kFull, covered ? x : -1);
+        if (lane == 0)
+        {
+            atomicMin(it.bbox + 0, mnx);
+            atomicMin(it.bbox + 1, y);
+            atomicMax(it.bbox + 2, mxx);
+            atomicMax(it.bbox + 3, y);
+        }
+    }
+}
+
+__global__ void __launch_bounds__(256) k_coverage(BlendArgs a, const Unit* __restrict__ units)
+{
+    Unit u = units[blockIdx.x];
+    const ItemDev& it = a.items[u.id];
+    const TileDev& T = a.tiles[it.tile];
+    int x = u.bx * 32 + (threadIdx.x & 31);
+    int y = u.by * 8 + (threadIdx.x >> 5);
+    bool covered = false;
+    if (x < T.w && y < T.h)
+    {
+        const unsigned short* p = it.img + ((size_t)y * T.w + x) * 3;
+        covered = (p[0] | p[1] | p[2]) != 0;
+    }
+    emit_coverage(it, T, x, y, covered);
+}
+
+// ---------------------------------------------------------------------------
+// Tile warp: WarpPerspective + ApplyGain for one contributor into its tile
+// buffer (RenderExecutor.cpp:104-114), with coverage emitted in the same pass.
+// Arithmetic identical to k_warp in pixel_ops.cu.
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(256) k_warp_tiles(BlendArgs a, const Unit* __restrict__ units)
+{
+    Unit u = units[blockIdx.x];
+    const ItemDev& it = a.items[u.id];
+    const TileDev& T = a.tiles[it.tile];
+    int x = u.bx * 32 + (threadIdx.x & 31);
+    int y = u.by * 8 + (threadIdx.x >> 5);
+    bool covered = false;
+    if (x < T.w && y < T.h)
+    {
+        float dX = (float)(x + it.offX), dY = (float)(y + it.offY);
+        const float* H = it.H;
+        float sx = fadd(fadd(fmul(H[0], dX), fmul(H[1], dY)), H[2]);
+        float sy = fadd(fadd(fmul(H[3], dX), fmul(H[4], dY)), H[5]);
+        float sw1 = fadd(fadd(fmul(H[6], dX), fmul(H[7], dY)), H[8]);
+        unsigned short o[3] = {0, 0, 0};
+        if (!(fabsf(sw1) < 1e-10f))
+        {
+            sx = fdiv(sx, sw1);
+            sy = fdiv(sy, sw1);
+            if (sx >= 0.0f && sx < (float)(it.srcW - 1) && sy >= 0.0f && sy < (float)(it.srcH - 1))
+            {
+                int x0 = (int)floorf(sx), y0 = (int)floorf(sy);
+                float fx = fsub(sx, (float)x0), fy = fsub(sy, (float)y0);
+                float gx = fsub(1.0f, fx), gy = fsub(1.0f, fy);
+                float w00 = fmul(gx, gy), w10 = fmul(fx, gy), w01 = fmul(gx, fy), w11 = fmul(fx, fy);
+                const unsigned short* r0 = it.src + ((size_t)y0 * it.srcW + x0) * 3;
+                const unsigned short* r1 = r0 + (size_t)it.srcW * 3;
+                bool applyGain = !gain_is_identity(it.gain);
+#pragma unroll
+                for (int c = 0; c < 3; ++c)
+                {
+                    float v = fadd(fadd(fadd(fmul(w00, (float)__ldg(r0 + c)), fmul(w10, (float)__ldg(r0 + 3 + c))),
+                                        fmul(w01, (float)__ldg(r1 + c))),
+                                   fmul(w11, (float)__ldg(r1 + 3 + c)));
+                    unsigned short q = clamp_trunc_u16(v);
+                    if (applyGain) q = clamp_trunc_u16(fmul((float)q, it.gain));
+                    o[c] = q;
+                }
+            }
+        }
+        unsigned short* d = const_cast<unsigned short*>(it.img) + ((size_t)y * T.w + x) * 3;
+        d[0] = o[0];
+        d[1] = o[1];
+        d[2] = o[2];
+        covered = (o[0] | o[1] | o[2]) != 0;
+    }
+    emit_coverage(it, T, x, y, covered);
+}
+
+// ---------------------------------------------------------------------------
+// Chamfer distance (SeamBlend.cpp:206-242), exact.
+//
+// The raster recurrence d[p] = min(init, left+1, up+1, upleft+sqrt2,
+// upright+sqrt2) is a DAG with a unique solution, so any schedule that applies
+// the same rounded operations reproduces the CPU bit for bit.  Each row is
+//     a[x] = min(init[x], prev[x]+1, prev[x-1]+sqrt2, prev[x+1]+sqrt2)
+//     d[x] = min(a[x], d[x-1] + 1)               (fl(+1) each step)
+// The second line is a scan whose operator "v -> min(L, g^S(v))", with
+// g(v) = fl(v + 1), composes as (L1,S1);(L2,S2) = (min(L2, g^S2(L1)), S1+S2),
+// because fl(.+1) is monotone.  g^n(v) is evaluated exactly by add_ones().
+//
+// Rows are pipelined over the CTA's warps (row y on warp y % NW) in chunks of
+// 256 columns, each warp waiting (bounded) until the row above has published
+// the columns it needs.  Chunk boundaries are skewed by one column per row so
+// a row lags the one above by a single chunk.  The backward pass is the same
+// code on mirrored coordinates with the forward result as init.
+// ---------------------------------------------------------------------------
+constexpr int kDtE = 8;
+constexpr int kDtCW = 32 * kDtE;
+
+__host__ __device__ __forceinline__ int dt_ring_stride(int W) { return W + (W >> 3) + 8; }
+__device__ __forceinline__ int ring_idx(int x) { return x + (x >> 3); }  // 1 pad per 8: conflict-free lanes
+
+// fl-sequential v + 1 + 1 + ... (n times), v >= 0.  Inside one binade
+// [2^e, 2^(e+1)) with e <= 23 adding 1 is exact, so only the step that crosses
+// into the next binade rounds; each crossing is one rounded add.
+__device__ __forceinline__ float add_ones(float v, int n)
+{
+    while (n > 0)
+    {
+        if (!(v < 16777216.0f)) return v;  // +inf (or beyond the distances that occur)
+        int m;
+        if (v < 1.0f) m = 1;
+        else
+        {
+            float B = __int_as_float((__float_as_int(v) & 0x7f800000) + 0x00800000);
+            m = (int)ceilf(fsub(B, v));  // exact: Sterbenz
+        }
+        int k = m < n ? m : n;
+        v = fadd(v, (float)k);
+        n -= k;
+    }
+    return v;
+}
+
+template <bool BACK>
+__global__ void __launch_bounds__(512) k_dt(BlendArgs a, const int* __restrict__ itemList, int nw)
+{
+    extern __shared__ float smem[];
+    const ItemDev& it = a.items[itemList[blockIdx.x]];
+    const TileDev& T = a.tiles[it.tile];
+    const int W = T.w, H = T.h, covWords = T.covWords;
+    const int RS = dt_ring_stride(W);
+    float* ring = smem;
+    int* prog = reinterpret_cast<int*>(smem + (size_t)nw * RS);
+    if (threadIdx.x < nw) prog[threadIdx.x] = -1;
+    __syncthreads();
+    const float kInf = (float)(W + H);
+    const float kDiag = 1.41421356f;
+    const float INF = f_inf();
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const uint32_t* cov = it.cov;
+    const float* d1 = it.d1;
+    float* out = BACK ? it.d : it.d1;
+
+    for (int vy = warp; vy < H; vy += nw)
+    {
+        const int ry = BACK ? H - 1 - vy : vy;
+        const int slot = vy % nw, pslot = (vy + nw - 1) % nw;
+        const int skew = vy % kDtCW;
+        float carry = INF;
+        for (int x0 = -skew; x0 < W; x0 += kDtCW)
+        {
+            const int x1 = min(x0 + kDtCW, W);
+            if (vy > 0)
+            {
+                const int target = (vy - 1) * (W + 1) + min(x1 + 1, W);
+                int ok = 1;
+                if (lane == 0)
+                {
+                    cuda::atomic_ref<int, cuda::thread_scope_block> pr(prog[pslot]);
+                    long long t0 = clock64();
+                    int spins = 0;
+                    while (pr.load(cuda::memory_order_acquire) < target)
+                    {
+                        if ((++spins & 1023) == 0)
+                        {
+                            if (*(volatile int*)a.error || clock64() - t0 > kSpinCycles)
+                            {
+                                atomicExch(a.error, 1);
+                                ok = 0;
+                                break;
+                            }
+                        }
+                    }
+                }
+                ok = __shfl_sync(kFull, ok, 0);
+                if (!ok) return;
+            }
+            const int xb = x0 + lane * kDtE;
+            float pv[kDtE + 2];
+#pragma unroll
+            for (int k = 0; k < kDtE + 2; ++k)
+            {
+                int x = xb - 1 + k;
+                pv[k] = (vy > 0 && x >= 0 && x < W) ? ring[pslot * RS + ring_idx(x)] : INF;
+            }
+            float l[kDtE];
+            float prev = INF;
+#pragma unroll
+            for (int k = 0; k < kDtE; ++k)
+            {
+                int x = xb + k;
+                float av = INF;
+                if (x >= 0 && x < W)
+                {
+                    int rx = BACK ? W - 1 - x : x;
+                    if (BACK) av = __ldg(d1 + (size_t)ry * W + rx);
+                    else av = cov_bit(cov, covWords, rx, ry) ? kInf : 0.0f;
+                    if (vy > 0)
+                    {
+                        av = fminf(av, fadd(pv[k + 1], 1.0f));
+                        if (x > 0) av = fminf(av, fadd(pv[k], kDiag));
+                        if (x < W - 1) av = fminf(av, fadd(pv[k + 2], kDiag));
+                    }
+                }
+                l[k] = fminf(av, fadd(prev, 1.0f));
+                prev = l[k];
+            }
+            // Inclusive scan over lanes of (L, S=kDtE) segments.
+            float Lc = l[kDtE - 1];
+#pragma unroll
+            for (int dd = 1; dd < 32; dd <<= 1)
+            {
+                float Lp = __shfl_up_sync(kFull, Lc, dd);
+                if (lane >= dd) Lc = fminf(Lc, add_ones(Lp, kDtE * dd));
+            }
+            float excl = __shfl_up_sync(kFull, Lc, 1);
+            if (lane == 0) excl = INF;
+            float v = fminf(excl, add_ones(carry, lane * kDtE));
+#pragma unroll
+            for (int k = 0; k < kDtE; ++k)
+            {
+                v = fminf(l[k], fadd(v, 1.0f));
+                int x = xb + k;
+                if (x >= 0 && x < W)
+                {
+                    ring[slot * RS + ring_idx(x)] = v;
+                    int rx = BACK ? W - 1 - x : x;
+                    out[(size_t)ry * W + rx] = v;
+                }
+            }
+            carry = __shfl_sync(kFull, v, 31);
+            __syncwarp();
+            if (lane == 0)
+            {
+                cuda::atomic_ref<int, cuda::thread_scope_block> pr(prog[slot]);
+                pr.store(vy * (W + 1) + x1, cuda::memory_order_release);
+            }
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Ownership (SeamBlend.cpp:244-261): argmax over contributors of d > 0,
+// strict '>' so ties keep the lowest index; -1 where nothing covers.
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(256) k_owner(BlendArgs a, const Unit* __restrict__ units)
+{
+    Unit u = units[blockIdx.x];
+    const TileDev& T = a.tiles[u.id];
+    long long n = (long long)T.w * T.h;
+    long long p = (long long)u.bx * 1024 + threadIdx.x;
+#pragma unroll
+    for (int j = 0; j < 4; ++j, p += 256)
+    {
+        if (p >= n) break;
+        int best = -1;
+        float bestD = 0.0f;
+        for (int k = 0; k < T.numItems; ++k)
+        {
+            float v = __ldg(a.items[T.firstItem + k].d + p);
+            if (v > bestD)
+            {
+                bestD = v;
+                best = k;
+            }
+        }
+        T.owner[p] = (signed char)best;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Seam refinement (SeamBlend.cpp:293-445) for every overlapping pair of a
+// tile, in the reference's (i, j) order, one CTA per tile.  Lines are scanned
+// warp-parallel; the dynamic program over contested lines is sequential (it
+// is in the reference too) and runs in one warp with the per-line state in
+// shared memory.
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(256) k_seam(BlendArgs a, const int* __restrict__ tileList, int smemLines)
+{
+    extern __shared__ unsigned char sm_seam[];
+    __shared__ float dpBuf[2][64];
+    __shared__ int sLast, sBestK;
+    const TileDev& T = a.tiles[tileList[blockIdx.x]];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, tid = threadIdx.x;
+    const int K = T.numItems;
+    const int w = T.w;
+    const bool inSmem = T.maxLines <= smemLines;
+    int* sLo = inSmem ? reinterpret_cast<int*>(sm_seam) : T.lo;
+    int* sHi = inSmem ? sLo + smemLines : T.hi;
+    int* sPrev = inSmem ? sHi + smemLines : T.prevLine;
+    unsigned char* sBack = inSmem ? reinterpret_cast<unsigned char*>(sPrev + smemLines) : T.back;
+
+    for (int i = 0; i < K; ++i)
+    {
+        const ItemDev& I = a.items[T.firstItem + i];
+        int bI[4] = {I.bbox[0], I.bbox[1], I.bbox[2], I.bbox[3]};
+        if (bI[2] < 0) continue;
+        for (int j = i + 1; j < K; ++j)
+        {
+            const ItemDev& J = a.items[T.firstItem + j];
+            int bJ[4] = {J.bbox[0], J.bbox[1], J.bbox[2], J.bbox[3]};
+            if (bJ[2] < 0) continue;
+            int ox0 = max(bI[0], bJ[0]), oy0 = max(bI[1], bJ[1]);
+            int ox1 = min(bI[2], bJ[2]), oy1 = min(bI[3], bJ[3]);
+            if (!(ox0 <= ox1 && oy0 <= oy1)) continue;
+            const int bw = ox1 - ox0 + 1, bh = oy1 - oy0 + 1;
+            const bool rowScan = bw >= bh;
+            float cI = rowScan ? fmul((float)(bI[0] + bI[2]), 0.5f) : fmul((float)(bI[1] + bI[3]), 0.5f);
+            float cJ = rowScan ? fmul((float)(bJ[0] + bJ[2]), 0.5f) : fmul((float)(bJ[1] + bJ[3]), 0.5f);
+            const bool iLow = cI <= cJ;
+            const int numLines = rowScan ? bh : bw;
+            const int lineLen = rowScan ? bw : bh;
+            const signed char ci = (signed char)i, cj = (signed char)j;
+            auto pix = [&](int line, int t) -> size_t {
+                return rowScan ? (size_t)(oy0 + line) * w + (ox0 + t) : (size_t)(oy0 + t) * w + (ox0 + line);
+            };
+            auto pxy = [&](int line, int t, int& x, int& y) {
+                x = rowScan ? ox0 + t : ox0 + line;
+                y = rowScan ? oy0 + line : oy0 + t;
+            };
+
+            // Phase 1: crossover and contested band per line.
+            for (int line = warp; line < numLines; line += 8)
+            {
+                int first = -1000, cross = -1;
+                for (int t0 = 0; t0 < lineLen && cross < 0; t0 += 32)
+                {
+                    int t = t0 + lane;
+                    int o = -2;
+                    bool isIJ = false;
+                    if (t < lineLen)
+                    {
+                        o = T.owner[pix(line, t)];
+                        isIJ = (o == ci || o == cj);
+                    }
+                    unsigned m = __ballot_sync(kFull, isIJ);
+                    if (!m) continue;
+                    if (first == -1000)
+                    {
+                        int fl = __ffs(m) - 1;
+                        first = __shfl_sync(kFull, o, fl);
+                        unsigned md = __ballot_sync(kFull, isIJ && o != first);
+                        md &= (fl == 31) ? 0u : ~((2u << fl) - 1u);
+                        if (md) cross = t0 + __ffs(md) - 1;
+                    }
+                    else
+                    {
+                        unsigned md = __ballot_sync(kFull, isIJ && o != first);
+                        if (md) cross = t0 + __ffs(md) - 1;
+                    }
+                }
+                int lo = 1, hi = 0;
+                if (cross >= 0)
+                {
+                    int bLo = max(0, cross - kSeamRadius);
+                    int bHi = min(lineLen - 1, cross + kSeamRadius);
+                    bool both0 = false, both1 = false;
+                    int t = bLo + lane;
+                    if (t <= bHi)
+                    {
+                        int x, y;
+                        pxy(line, t, x, y);
+                        both0 = cov_bit(I.cov, T.covWords, x, y) && cov_bit(J.cov, T.covWords, x, y);
+                    }
+                    t = bLo + 32 + lane;
+                    if (t <= bHi)
+                    {
+                        int x, y;
+                        pxy(line, t, x, y);
+                        both1 = cov_bit(I.cov, T.covWords, x, y) && cov_bit(J.cov, T.covWords, x, y);
+                    }
+                    unsigned m0 = __ballot_sync(kFull, both0), m1 = __ballot_sync(kFull, both1);
+                    if (m0 | m1)
+                    {
+                        lo = bLo + (m0 ? __ffs(m0) - 1 : 32 + __ffs(m1) - 1);
+                        hi = bLo + (m1 ? 32 + 31 - __clz(m1) : 31 - __clz(m0));
+                    }
+                }
+                if (lane == 0)
+                {
+                    sLo[line] = lo;
+                    sHi[line] = hi;
+                }
+            }
+            __syncthreads();
+
+            // Phase 2: per-pixel colour cost of every contested candidate.
+            for (int idx = tid; idx < numLines * kSeamBand; idx += 256)
+            {
+                int line = idx / kSeamBand, k = idx - line * kSeamBand;
+                if (k == 0) T.chosen[line] = -1;
+                int lo = sLo[line], hi = sHi[line];
+                if (k > hi - lo) continue;
+                size_t p = pix(line, lo + k);
+                const unsigned short* pa = I.img + p * 3;
+                const unsigned short* pb = J.img + p * 3;
+                float c = 0.0f;
+#pragma unroll
+                for (int ch = 0; ch < 3; ++ch) c = fadd(c, fabsf(fsub((float)pa[ch], (float)pb[ch])));
+                T.cost[(size_t)line * kSeamBand + k] = c;
+            }
+            __syncthreads();
+
+            // Phase 3: dynamic program over contested lines (one warp).
+            if (warp == 0)
+            {
+                int last = -1, cur = 0, lastW = 0;
+                for (int line = 0; line < numLines; ++line)
+                {
+                    int lo = sLo[line], hi = sHi[line];
+                    if (hi < lo)
+                    {
+                        if (lane == 0) sPrev[line] = -1;
+                        continue;
+                    }
+                    int lw = hi - lo + 1;
+                    int plo = last >= 0 ? sLo[last] : 0;
+                    int pw = lastW;
+                    for (int k = lane; k < lw; k += 32)
+                    {
+                        float c = T.cost[(size_t)line * kSeamBand + k];
+                        int t = lo + k;
+                        float val;
+                        int bp = -1;
+                        if (last < 0) val = c;
+                        else
+                        {
+                            float best = FLT_MAX;
+                            for (int pk = 0; pk < pw; ++pk)
+                            {
+                                float c2 = fadd(dpBuf[cur ^ 1][pk], fmul(kSeamSmooth, fabsf((float)(t - (plo + pk)))));
+                                if (c2 < best)
+                                {
+                                    best = c2;
+                                    bp = pk;
+                                }
+                            }
+                            val = fadd(c, best);
+                        }
+                        dpBuf[cur][k] = val;
+                        sBack[(size_t)line * kSeamBand + k] = (unsigned char)(bp < 0 ? 255 : bp);
+                    }
+                    if (lane == 0) sPrev[line] = last;
+                    last = line;
+                    lastW = lw;
+                    cur ^= 1;
+                    __syncwarp();
+                }
+                if (lane == 0)
+                {
+                    sLast = last;
+                    int bestK = 0;
+                    if (last >= 0)
+                    {
+                        float best = FLT_MAX;
+                        for (int k = 0; k < lastW; ++k)
+                            if (dpBuf[cur ^ 1][k] < best)
+                            {
+                                best = dpBuf[cur ^ 1][k];
+                                bestK = k;
+                            }
+                    }
+                    sBestK = bestK;
+                }
+            }
+            __syncthreads();
+
+            // Phase 4: backtrack.
+            if (tid == 0 && sLast >= 0)
+            {
+                int line = sLast, k = sBestK;
+                while (line >= 0 && k >= 0)
+                {
+                    T.chosen[line] = sLo[line] + k;
+                    int pl = sPrev[line];
+                    int pk = sBack[(size_t)line * kSeamBand + k];
+                    line = pl;
+                    k = pk == 255 ? -1 : pk;
+                }
+            }
+            __syncthreads();
+
+            // Phase 5: reassign I/J pixels inside each contested band.
+            if (sLast >= 0)
+            {
+                for (int idx = tid; idx < numLines * kSeamBand; idx += 256)
+                {
+                    int line = idx / kSeamBand, k = idx - line * kSeamBand;
+                    int ch = T.chosen[line];
+                    if (ch < 0) continue;
+                    int lo = sLo[line], hi = sHi[line];
+                    if (k > hi - lo) continue;
+                    int t = lo + k;
+                    size_t p = pix(line, t);
+                    signed char o = T.owner[p];
+                    if (o != ci && o != cj) continue;
+                    bool onLow = t < ch;
+                    T.owner[p] = (onLow == iLow) ? ci : cj;
+                }
+            }
+            __syncthreads();
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Pyramid (SeamBlend.cpp:15-201, 447-546).
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ float blur5(float a, float b, float c, float d, float e)
+{
+    // k0*a + k1*b + k2*c + k1*d + k0*e, left to right (SeamBlend.cpp:31-36).
+    const float k0 = 1.0f / 16.0f, k1 = 4.0f / 16.0f, k2 = 6.0f / 16.0f;
+    return fadd(fadd(fadd(fadd(fmul(k0, a), fmul(k1, b)), fmul(k2, c)), fmul(k1, d)), fmul(k0, e));
+}
+
+struct UpCoef
+{
+    int x0, x1, y0, y1;
+    float wx, wy;
+};
+
+// Align-corners bilinear resize coefficients (SeamBlend.cpp:85-115).
+__device__ __forceinline__ UpCoef up_coef(int sw, int sh, int dw, int dh, int x, int y)
+{
+    float sx = (sw > 1) ? fdiv((float)(sw - 1), (float)max(1, dw - 1)) : 0.0f;
+    float sy = (sh > 1) ? fdiv((float)(sh - 1), (float)max(1, dh - 1)) : 0.0f;
+    UpCoef c;
+    float fy = fmul(sy, (float)y);
+    c.y0 = min(__float2int_rz(fy), sh - 1);
+    c.y1 = min(c.y0 + 1, sh - 1);
+    c.wy = fsub(fy, (float)c.y0);
+    float fx = fmul(sx, (float)x);
+    c.x0 = min(__float2int_rz(fx), sw - 1);
+    c.x1 = min(c.x0 + 1, sw - 1);
+    c.wx = fsub(fx, (float)c.x0);
+    return c;
+}
+
+__device__ __forceinline__ float up_mix(float v00, float v10, float v01, float v11, float wx, float wy)
+{
+    float ix = fsub(1.0f, wx), iy = fsub(1.0f, wy);
+    return fadd(fmul(iy, fadd(fmul(ix, v00), fmul(wx, v10))), fmul(wy, fadd(fmul(ix, v01), fmul(wx, v11))));
+}
+
+// Hole-filled Gaussian value G = num * (den > 1e-6 ? 1/den : 0)
+// (SeamBlend.cpp:175-180).
+__device__ __forceinline__ float3 gauss_of(float4 nd)
+{
+    float inv = (nd.w > 1e-6f) ? fdiv(1.0f, nd.w) : 0.0f;
+    return make_float3(fmul(nd.x, inv), fmul(nd.y, inv), fmul(nd.z, inv));
+}
+
+// Blur + decimate one level (SeamBlend.cpp:60-79) for num(3), den and weight
+// together.  A CTA makes a 32x8 block of level l+1 from a 68x20 footprint of
+// level l staged in shared memory with replicated borders.
+constexpr int kDnTW = 32, kDnTH = 8;
+constexpr int kDnSW = 2 * kDnTW + 4, kDnSH = 2 * kDnTH + 4;
+
+template <bool L0>
+__global__ void __launch_bounds__(256) k_down(BlendArgs a, const Unit* __restrict__ units, int level)
+{
+    __shared__ float s[5][kDnSH][kDnSW];
+    __shared__ float t[5][kDnSH][kDnTW];
+    Unit u = units[blockIdx.x];
+    const ItemDev& it = a.items[u.id];
+    const TileDev& T = a.tiles[it.tile];
+    const int sw = T.lw[level], sh = T.lh[level];
+    const int dw = T.lw[level + 1], dh = T.lh[level + 1];
+    const int X0 = u.bx * kDnTW, Y0 = u.by * kDnTH;
+    const int tid = threadIdx.x;
+    const float4* ndS = L0 ? nullptr : it.nd + T.loff[level];
+    const float* wgS = L0 ? nullptr : it.wg + T.loff[level];
+    for (int idx = tid; idx < kDnSW * kDnSH; idx += 256)
+    {
+        int r = idx / kDnSW, c = idx - r * kDnSW;
+        int gx = min(max(2 * X0 - 2 + c, 0), sw - 1);
+        int gy = min(max(2 * Y0 - 2 + r, 0), sh - 1);
+        size_t p = (size_t)gy * sw + gx;
+        if (L0)
+        {
+            const unsigned short* px = it.img + p * 3;
+            unsigned short r0 = px[0], r1 = px[1], r2 = px[2];
+            float m = (r0 | r1 | r2) ? 1.0f : 0.0f;
+            s[0][r][c] = fmul((float)r0, m);
+            s[1][r][c] = fmul((float)r1, m);
+            s[2][r][c] = fmul((float)r2, m);
+            s[3][r][c] = m;
+            s[4][r][c] = (T.owner[p] == it.k) ? 1.0f : 0.0f;
+        }
+        else
+        {
+            float4 v = ndS[p];
+            s[0][r][c] = v.x;
+            s[1][r][c] = v.y;
+            s[2][r][c] = v.z;
+            s[3][r][c] = v.w;
+            s[4][r][c] = wgS[p];
+        }
+    }
+    __syncthreads();
+    // Horizontal taps at the even columns that survive decimation.
+    for (int idx = tid; idx < 5 * kDnSH * kDnTW; idx += 256)
+    {
+        int ch = idx / (kDnSH * kDnTW);
+        int rem = idx - ch * kDnSH * kDnTW;
+        int r = rem / kDnTW, i = rem - r * kDnTW;
+        const float* row = s[ch][r];
+        t[ch][r][i] = blur5(row[2 * i], row[2 * i + 1], row[2 * i + 2], row[2 * i + 3], row[2 * i + 4]);
+    }
+    __syncthreads();
+    int i = tid & 31, j = tid >> 5;
+    int X = X0 + i, Y = Y0 + j;
+    if (X >= dw || Y >= dh) return;
+    float o[5];
+#pragma unroll
+    for (int ch = 0; ch < 5; ++ch)
+        o[ch] = blur5(t[ch][2 * j][i], t[ch][2 * j + 1][i], t[ch][2 * j + 2][i], t[ch][2 * j + 3][i], t[ch][2 * j + 4][i]);
+    size_t q = T.loff[level + 1] + (size_t)Y * dw + X;
+    it.nd[q] = make_float4(o[0], o[1], o[2], o[3]);
+    it.wg[q] = o[4];
+}
+
+// Blended band of one level: sum over the tile's contributors, in index
+// order, of weight * Laplacian (SeamBlend.cpp:501-509), where
+// Laplacian = G_l - Up(G_l+1) or G_top (SeamBlend.cpp:184-201).
+// Contributors that own no pixel have an all-zero weight pyramid and add
+// exactly +-0, so summing every contributor equals the reference's sum.
+__global__ void __launch_bounds__(256) k_blend_level(BlendArgs a, const Unit* __restrict__ units, int level)
+{
+    Unit u = units[blockIdx.x];
+    const TileDev& T = a.tiles[u.id];
+    int x = u.bx * 32 + (threadIdx.x & 31), y = u.by * 8 + (threadIdx.x >> 5);
+    const int lw = T.lw[level], lh = T.lh[level];
+    if (x >= lw || y >= lh) return;
+    const bool top = level == T.bands - 1;
+    UpCoef c;
+    if (!top) c = up_coef(T.lw[level + 1], T.lh[level + 1], lw, lh, x, y);
+    const size_t p = T.loff[level] + (size_t)y * lw + x;
+    float acc0 = 0.0f, acc1 = 0.0f, acc2 = 0.0f;
+    for (int k = 0; k < T.numItems; ++k)
+    {
+        const ItemDev& it = a.items[T.firstItem + k];
+        float wv = __ldg(it.wg + p);
+        float3 g = gauss_of(it.nd[p]);
+        if (!top)
+        {
+            const float4* up = it.nd + T.loff[level + 1];
+            const int uw = T.lw[level + 1];
+            float3 a00 = gauss_of(up[(size_t)c.y0 * uw + c.x0]);
+            float3 a10 = gauss_of(up[(size_t)c.y0 * uw + c.x1]);
+            float3 a01 = gauss_of(up[(size_t)c.y1 * uw + c.x0]);
+            float3 a11 = gauss_of(up[(size_t)c.y1 * uw + c.x1]);
+            g.x = fsub(g.x, up_mix(a00.x, a10.x, a01.x, a11.x, c.wx, c.wy));
+            g.y = fsub(g.y, up_mix(a00.y, a10.y, a01.y, a11.y, c.wx, c.wy));
+            g.z = fsub(g.z, up_mix(a00.z, a10.z, a01.z, a11.z, c.wx, c.wy));
+        }
+        acc0 = fadd(acc0, fmul(wv, g.x));
+        acc1 = fadd(acc1, fmul(wv, g.y));
+        acc2 = fadd(acc2, fmul(wv, g.z));
+    }
+    float* b = T.blend + p * 3;
+    b[0] = acc0;
+    b[1] = acc1;
+    b[2] = acc2;
+}
+
+// Collapse one level in place: recon_l = blended_l + Up(recon_l+1)
+// (SeamBlend.cpp:514-525).
+__global__ void __launch_bounds__(256) k_collapse(BlendArgs a, const Unit* __restrict__ units, int level)
+{
+    Unit u = units[blockIdx.x];
+    const TileDev& T = a.tiles[u.id];
+    int x = u.bx * 32 + (threadIdx.x & 31), y = u.by * 8 + (threadIdx.x >> 5);
+    const int lw = T.lw[level], lh = T.lh[level];
+    if (x >= lw || y >= lh) return;
+    const int uw = T.lw[level + 1];
+    UpCoef c = up_coef(uw, T.lh[level + 1], lw, lh, x, y);
+    const float* r = T.blend + T.loff[level + 1] * 3;
+    float* b = T.blend + (T.loff[level] + (size_t)y * lw + x) * 3;
+#pragma unroll
+    for (int ch = 0; ch < 3; ++ch)
+    {
+        float v = up_mix(r[((size_t)c.y0 * uw + c.x0) * 3 + ch], r[((size_t)c.y0 * uw + c.x1) * 3 + ch],
+                         r[((size_t)c.y1 * uw + c.x0) * 3 + ch], r[((size_t)c.y1 * uw + c.x1) * 3 + ch], c.wx, c.wy);
+        b[ch] = fadd(b[ch], v);
+    }
+}
+
+// Level 0 and output (SeamBlend.cpp:514-545).  The level-0 weight of a pixel
+// is 1 for its owner and 0 for every other contributor, so the blended level-0
+// band is exactly the owner's Laplacian img - Up(G1); the output is
+// clamp(that + Up(recon_1)) + 0.5 truncated, and 0 where nobody owns.
+__global__ void __launch_bounds__(256) k_final0(BlendArgs a, const Unit* __restrict__ units)
+{
+    Unit u = units[blockIdx.x];
+    const TileDev& T = a.tiles[u.id];
+    int x = u.bx * 32 + (threadIdx.x & 31), y = u.by * 8 + (threadIdx.x >> 5);
+    if (x >= T.w || y >= T.h) return;
+    size_t p = (size_t)y * T.w + x;
+    unsigned short* o = T.out + p * 3;
+    int own = T.owner[p];
+    if (own < 0)
+    {
+        o[0] = o[1] = o[2] = 0;
+        return;
+    }
+    const ItemDev& it = a.items[T.firstItem + own];
+    const unsigned short* px = it.img + p * 3;
+    float r[3] = {(float)px[0], (float)px[1], (float)px[2]};
+    if (T.bands > 1)
+    {
+        const int uw = T.lw[1], uh = T.lh[1];
+        UpCoef c = up_coef(uw, uh, T.w, T.h, x, y);
+        const float4* g1 = it.nd + T.loff[1];
+        float3 a00 = gauss_of(g1[(size_t)c.y0 * uw + c.x0]);
+        float3 a10 = gauss_of(g1[(size_t)c.y0 * uw + c.x1]);
+        float3 a01 = gauss_of(g1[(size_t)c.y1 * uw + c.x0]);
+        float3 a11 = gauss_of(g1[(size_t)c.y1 * uw + c.x1]);
+        float lap[3] = {fsub(r[0], up_mix(a00.x, a10.x, a01.x, a11.x, c.wx, c.wy)),
+                        fsub(r[1], up_mix(a00.y, a10.y, a01.y, a11.y, c.wx, c.wy)),
+                        fsub(r[2], up_mix(a00.z, a10.z, a01.z, a11.z, c.wx, c.wy))};
+        const float* rc = T.blend + T.loff[1] * 3;
+#pragma unroll
+        for (int ch = 0; ch < 3; ++ch)
+        {
+            float up = up_mix(rc[((size_t)c.y0 * uw + c.x0) * 3 + ch], rc[((size_t)c.y0 * uw + c.x1) * 3 + ch],
+                              rc[((size_t)c.y1 * uw + c.x0) * 3 + ch], rc[((size_t)c.y1 * uw + c.x1) * 3 + ch], c.wx,
+                              c.wy);
+            r[ch] = fadd(lap[ch], up);
+        }
+    }
+#pragma unroll
+    for (int ch = 0; ch < 3; ++ch)
+    {
+        float v = r[ch];
+        v = v < 65535.0f ? v : 65535.0f;
+        v = 0.0f < v ? v : 0.0f;
+        o[ch] = (unsigned short)__float2uint_rz(fadd(v, 0.5f));
+    }
+}
+}  // namespace
+
+int dt_rows_in_flight(int maxW)
+{
+    size_t row = (size_t)dt_ring_stride(maxW) * sizeof(float);
+    int nw = (int)((200 * 1024) / row);
+    if (nw > 16) nw = 16;
+    return nw;
+}
+
+int launch_coverage(const BlendArgs& a, const Unit* units, int n, cudaStream_t s)
+{
+    if (n <= 0) return I360B_SUCCESS;
+    k_coverage<<<n, 256, 0, s>>>(a, units);
+    return check_launch("coverage kernel");
+}
+
+int launch_warp_tiles(const BlendArgs& a, const Unit* units, int n, cudaStream_t s)
+{
+    if (n <= 0) return I360B_SUCCESS;
+    k_warp_tiles<<<n, 256, 0, s>>>(a, units);
+    return check_launch("tile warp kernel");
+}
+
+int launch_dt(const BlendArgs& a, const int* itemList, int n, bool backward, int maxW, cudaStream_t s)
+{
+    if (n <= 0) return I360B_SUCCESS;
+    int nw = dt_rows_in_flight(maxW);
+    if (nw < 2) return fail(I360B_NOT_SUPPORTED, "Chunk width %d exceeds the distance-transform row buffer.", maxW);
+    size_t smem = (size_t)nw * dt_ring_stride(maxW) * sizeof(float) + 64 * sizeof(int);
+    if (backward)
+    {
+        cudaFuncSetAttribute(k_dt<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        k_dt<true><<<n, nw * 32, smem, s>>>(a, itemList, nw);
+    }
+    else
+    {
+        cudaFuncSetAttribute(k_dt<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        k_dt<false><<<n, nw * 32, smem, s>>>(a, itemList, nw);
+    }
+    return check_launch("distance transform kernel");
+}
+
+int launch_owner(const BlendArgs& a, const Unit* units, int n, cudaStream_t s)
+{
+    if (n <= 0) return I360B_SUCCESS;
+    k_owner<<<n, 256, 0, s>>>(a, units);
+    return check_launch("ownership kernel");
+}
+
+int launch_seam(const BlendArgs& a, const int* tileList, int n, int maxLines, cudaStream_t s);
+
+int launch_seam(const BlendArgs& a, const int* tileList, int n, cudaStream_t s)
+{
+    // Per-line state (lo, hi, prev: 3 ints; back pointers: kSeamBand bytes)
+    // is kept in shared memory for lines up to this count.
+    const int smemLines = 3072;
+    size_t smem = (size_t)smemLines * (3 * sizeof(int) + kSeamBand);
+    if (n <= 0) return I360B_SUCCESS;
+    cudaFuncSetAttribute(k_seam, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    k_seam<<<n, 256, smem, s>>>(a, tileList, smemLines);
+    return check_launch("seam kernel");
+}
+
+int launch_down(const BlendArgs& a, const Unit* units, int n, int level, cudaStream_t s)
+{
+    if (n <= 0) return I360B_SUCCESS;
+    if (level == 0) k_down<true><<<n, 256, 0, s>>>(a, units, level);
+    else k_down<false><<<n, 256, 0, s>>>(a, units, level);
+    return check_launch("pyramid down kernel");
+}
+
+int launch_blend_level(const BlendArgs& a, const Unit* units, int n, int level, cudaStream_t s)
+{
+    if (n <= 0) return I360B_SUCCESS;
+    k_blend_level<<<n, 256, 0, s>>>(a, units, level);
+    return check_launch("blend level kernel");
+}
+
+int launch_collapse(const BlendArgs& a, const Unit* units, int n, int level, cudaStream_t s)
+{
+    if (n <= 0) return I360B_SUCCESS;
+    k_collapse<<<n, 256, 0, s>>>(a, units, level);
+    return check_launch("collapse kernel");
+}
+
+int launch_final0(const BlendArgs& a, const Unit* units, int n, cudaStream_t s)
+{
+    if (n <= 0) return I360B_SUCCESS;
+    k_final0<<<n, 256, 0, s>>>(a, units);
+    return check_launch("final level kernel");
+}
+}  // namespace i360b

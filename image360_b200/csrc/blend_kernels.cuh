@@ -1,0 +1,83 @@
+// Device data layout and kernels of the seam blend
+// (Kernels::SeamBlend::BlendChunkContributors, SeamBlend.cpp:549-587) for a
+// batch of output tiles ("chunks"), each with its own contributors ("items").
+#pragma once
+
+#include "common.cuh"
+
+namespace i360b
+{
+constexpr int kMaxBands = 8;
+constexpr int kSeamRadius = 24;                 // SeamBlend.cpp:319
+constexpr int kSeamBand = 2 * kSeamRadius + 1;  // candidates per line
+constexpr float kSeamSmooth = 2.0f;             // SeamBlend.cpp:309
+
+// One (tile, contributor) pair.  All buffers live in the plan's arena.
+struct ItemDev
+{
+    const unsigned short* img;  // warped RGB48, tile-sized, (0,0,0) = no data
+    uint32_t* cov;              // coverage bits, covWords per row
+    float* d1;                  // chamfer forward pass
+    float* d;                   // chamfer distance (final)
+    int* bbox;                  // x0, y0, x1, y1 of covered pixels (x0 > x1 = empty)
+    float4* nd;                 // pyramid levels 1.. : (num.rgb, den)
+    float* wg;                  // pyramid levels 1.. : weight
+    float H[9];                 // destination(tile) -> source(frame) matrix
+    const unsigned short* src;  // source frame (render path)
+    int srcW, srcH;
+    int offX, offY;             // added to tile-local x, y before H
+    float gain;
+    int tile;
+    int k;                      // contributor index inside its tile
+};
+
+struct TileDev
+{
+    int w, h;
+    int bands;       // clamped band count (SeamBlend.cpp:457-459)
+    int firstItem;   // items [firstItem, firstItem + numItems)
+    int numItems;
+    int covWords;    // 32-bit words per coverage row
+    signed char* owner;
+    float* blend;    // levels 1.. : 3 floats per pixel (blended band, then reconstruction)
+    unsigned short* out;
+    int lw[kMaxBands], lh[kMaxBands];
+    long long loff[kMaxBands];  // pixel offset of level l (l >= 1) in the per-level arrays
+    // seam scratch
+    int* lo;
+    int* hi;
+    int* prevLine;
+    int* chosen;
+    float* cost;
+    unsigned char* back;
+    int maxLines;
+};
+
+// A CTA's assignment inside a batched launch: object id and block coords.
+struct Unit
+{
+    int id;
+    int bx;
+    int by;
+    int level;
+};
+
+struct BlendArgs
+{
+    ItemDev* items;
+    TileDev* tiles;
+    int* error;  // set non-zero by a kernel that gave up (bounded waits)
+};
+
+// Kernel launchers (blend_kernels.cu).
+int launch_coverage(const BlendArgs& a, const Unit* units, int n, cudaStream_t s);
+int launch_warp_tiles(const BlendArgs& a, const Unit* units, int n, cudaStream_t s);
+int launch_dt(const BlendArgs& a, const int* itemList, int n, bool backward, int maxW, cudaStream_t s);
+int launch_owner(const BlendArgs& a, const Unit* units, int n, cudaStream_t s);
+int launch_seam(const BlendArgs& a, const int* tileList, int n, cudaStream_t s);
+int launch_down(const BlendArgs& a, const Unit* units, int n, int level, cudaStream_t s);
+int launch_blend_level(const BlendArgs& a, const Unit* units, int n, int level, cudaStream_t s);
+int launch_collapse(const BlendArgs& a, const Unit* units, int n, int level, cudaStream_t s);
+int launch_final0(const BlendArgs& a, const Unit* units, int n, cudaStream_t s);
+int dt_rows_in_flight(int maxW);
+}  // namespace i360b

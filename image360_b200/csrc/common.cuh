@@ -1,0 +1,94 @@
+// Shared device helpers and host-side runtime plumbing for the B200 render
+// backend.  sm_100a only.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <cstdint>
+#include <cstddef>
+
+#include "../../include/image360_b200.h"
+
+namespace i360b
+{
+// ---------------------------------------------------------------------------
+// Exact FP32 arithmetic.  The reference's CPU kernels are compiled without FMA
+// contraction (scalar tier and SeamBlend carry no -mfma), so every product and
+// sum is rounded separately and in source order.  These wrappers keep nvcc from
+// fusing multiply-adds, which would change the last bit and break parity.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ float fadd(float a, float b) { return __fadd_rn(a, b); }
+__device__ __forceinline__ float fsub(float a, float b) { return __fsub_rn(a, b); }
+__device__ __forceinline__ float fmul(float a, float b) { return __fmul_rn(a, b); }
+__device__ __forceinline__ float fdiv(float a, float b) { return __fdiv_rn(a, b); }
+
+// (unsigned short)min(max(v, 0), 65535): clamp then truncate toward zero, the
+// quantisation at every stage boundary of the reference (e.g.
+// WarpPerspectiveKernels.h:41, BayerDemosaicKernels.h:58,73, GainColorOps.cpp:23).
+__device__ __forceinline__ unsigned short clamp_trunc_u16(float v)
+{
+    v = v > 0.0f ? v : 0.0f;  // NaN -> 0
+    v = v < 65535.0f ? v : 65535.0f;
+    return static_cast<unsigned short>(__float2uint_rz(v));
+}
+
+// ApplyGain's skip rule (GainColorOps.cpp:22 and RenderExecutor.cpp:111).
+__host__ __device__ __forceinline__ bool gain_is_identity(float gain)
+{
+    float d = gain - 1.0f;
+    d = d < 0.0f ? -d : d;
+    return d < 1e-6f;
+}
+
+constexpr int kMaxContributors = 32;  // RenderExecutor.cpp:15, CpuComputeBackend.cpp:143
+
+// ---------------------------------------------------------------------------
+// Host runtime (context.cu)
+// ---------------------------------------------------------------------------
+
+// Thread-local last error; returns `code` so call sites can `return fail(...)`.
+int fail(int code, const char* fmt, ...);
+void clear_error();
+// Maps a CUDA error to a result code and records the message.
+int cuda_fail(cudaError_t e, const char* what);
+// Checks for a launch error of the kernel just enqueued.
+int check_launch(const char* what);
+
+bool initialized();
+int device();
+int sm_count();
+// The calling thread's stream for the synchronous host-buffer API.
+cudaStream_t thread_stream();
+// Stream-ordered allocation from the device's pool (kept for the process life).
+int dev_alloc(void** p, size_t bytes, cudaStream_t s, const char* what);
+void dev_free(void* p, cudaStream_t s);
+
+// Requires an initialised context (lazy-initialises on first use).
+int ensure_ready();
+
+#define I360B_TRY(expr)             \
+    do                              \
+    {                               \
+        int _rc = (expr);           \
+        if (_rc != I360B_SUCCESS)   \
+            return _rc;             \
+    } while (0)
+
+#define I360B_CUDA(expr, what)                        \
+    do                                                \
+    {                                                 \
+        cudaError_t _e = (expr);                      \
+        if (_e != cudaSuccess)                        \
+            return ::i360b::cuda_fail(_e, what);      \
+    } while (0)
+
+// Kernel launchers shared between translation units (all stream-ordered).
+int launch_demosaic(const unsigned short* cfa, int w, int h, unsigned short black, const float* camMul,
+                    const float* rgbCam, uint32_t filters, unsigned short* out, cudaStream_t s);
+int launch_warp(const unsigned short* src, int sw, int sh, unsigned short* dst, int dw, int dh, const float* H,
+                int offX, int offY, float gain, cudaStream_t s);
+int launch_median(const unsigned short* const* inputs, int n, unsigned short* out, int w, int h, float sigma,
+                  cudaStream_t s);
+int launch_gain(unsigned short* data, long long n, float gain, cudaStream_t s);
+int launch_blend_chunk(const unsigned short* const* warped, int k, int w, int h, int bands, unsigned short* out,
+                       cudaStream_t s);
+}  // namespace i360b

@@ -1,0 +1,644 @@
+// Batched seam-blend render of many uneven output tiles.
+//
+// A plan turns a tile list into flat per-kernel work lists ("units": one CTA
+// each) over all tiles at once, carves every intermediate out of one device
+// arena, and enqueues the fixed kernel sequence
+//     warp(+gain, coverage) -> chamfer fwd -> chamfer bwd -> ownership ->
+//     seam DP -> pyramid down x(L-1) -> blended bands -> collapse -> level 0
+// which is captured once into a CUDA graph and replayed.  The same machinery
+// serves the single-chunk blend API (one tile, pre-warped contributors).
+#include "blend_kernels.cuh"
+#include "render_plan.hpp"
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <vector>
+
+namespace i360b
+{
+namespace
+{
+__global__ void k_init_bbox(ItemDev* items, int n)
+{
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    int* b = items[i].bbox;
+    b[0] = 0x7fffffff;
+    b[1] = 0x7fffffff;
+    b[2] = -1;
+    b[3] = -1;
+}
+
+// Frame homography -> per-item destination->source matrix.
+//  REFERENCE: round the frame->canvas matrix to float, invert it with the FP32
+//  adjugate of HomographyMath.cpp:94-116, keep the tile origin as the integer
+//  offset RenderExecutor passes (RenderExecutor.cpp:101-108).
+//  FP64_ORIGIN: invert in FP64 and fold the tile origin into the matrix in
+//  FP64 (H * T(x0, y0)), rounding to float once; offsets become 0.
+__global__ void k_setup_items(ItemDev* items, const double* toCanvas, const int* itemFrame, const int* tileXY,
+                              int n, int mode, int* singular)
+{
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const double* m = toCanvas + 9 * itemFrame[i];
+    ItemDev& it = items[i];
+    int tx = tileXY[2 * i], ty = tileXY[2 * i + 1];
+    if (mode == I360B_COORDS_REFERENCE)
+    {
+        float a = (float)m[0], b = (float)m[1], c = (float)m[2], d = (float)m[3], e = (float)m[4], f = (float)m[5],
+              g = (float)m[6], i2 = (float)m[7], j = (float)m[8];
+        float det = fadd(fsub(fmul(a, fsub(fmul(e, j), fmul(f, i2))), fmul(b, fsub(fmul(d, j), fmul(f, g)))),
+                         fmul(c, fsub(fmul(d, i2), fmul(e, g))));
+        if (fabsf(det) < 1e-12f)
+        {
+            singular[i] = 1;
+            return;
+        }
+        float inv = fdiv(1.0f, det);
+        it.H[0] = fmul(fsub(fmul(e, j), fmul(f, i2)), inv);
+        it.H[1] = fmul(fsub(fmul(c, i2), fmul(b, j)), inv);
+        it.H[2] = fmul(fsub(fmul(b, f), fmul(c, e)), inv);
+        it.H[3] = fmul(fsub(fmul(f, g), fmul(d, j)), inv);
+        it.H[4] = fmul(fsub(fmul(a, j), fmul(c, g)), inv);
+        it.H[5] = fmul(fsub(fmul(c, d), fmul(a, f)), inv);
+        it.H[6] = fmul(fsub(fmul(d, i2), fmul(e, g)), inv);
+        it.H[7] = fmul(fsub(fmul(b, g), fmul(a, i2)), inv);
+        it.H[8] = fmul(fsub(fmul(a, e), fmul(b, d)), inv);
+        it.offX = tx;
+        it.offY = ty;
+        singular[i] = 0;
+    }
+    else
+    {
+        double a = m[0], b = m[1], c = m[2], d = m[3], e = m[4], f = m[5], g = m[6], i2 = m[7], j = m[8];
+        double det = a * (e * j - f * i2) - b * (d * j - f * g) + c * (d * i2 - e * g);
+        if (fabs(det) < 1e-12)
+        {
+            singular[i] = 1;
+            return;
+        }
+        double inv = 1.0 / det;
+        double Hi[9] = {(e * j - f * i2) * inv, (c * i2 - b * j) * inv, (b * f - c * e) * inv,
+                        (f * g - d * j) * inv,  (a * j - c * g) * inv,  (c * d - a * f) * inv,
+                        (d * i2 - e * g) * inv, (b * g - a * i2) * inv, (a * e - b * d) * inv};
+        for (int r = 0; r < 3; ++r)
+        {
+            it.H[r * 3 + 0] = (float)Hi[r * 3 + 0];
+            it.H[r * 3 + 1] = (float)Hi[r * 3 + 1];
+            it.H[r * 3 + 2] = (float)(Hi[r * 3 + 0] * tx + Hi[r * 3 + 1] * ty + Hi[r * 3 + 2]);
+        }
+        it.offX = 0;
+        it.offY = 0;
+        singular[i] = 0;
+    }
+}
+
+size_t align256(size_t v) { return (v + 255) & ~size_t(255); }
+
+__global__ void k_count_cov(const ItemDev* items, const TileDev* tiles, int n, unsigned long long* out)
+{
+    int i = blockIdx.x;
+    if (i >= n) return;
+    const ItemDev& it = items[i];
+    const TileDev& T = tiles[it.tile];
+    long long words = (long long)T.h * T.covWords;
+    unsigned long long c = 0;
+    for (long long q = threadIdx.x; q < words; q += blockDim.x) c += __popc(it.cov[q]);
+    atomicAdd(out, c);
+}
+}  // namespace
+
+int Plan::build(const std::vector<TileSpec>& specs, int numBands, bool renderPath)
+{
+    render = renderPath;
+    nTiles = (int)specs.size();
+    if (numBands < 1) return fail(I360B_INVALID_PARAM, "numBands must be >= 1.");
+    bandsReq = std::min(numBands, kMaxBands);
+    if (numBands > kMaxBands)
+        bandsReq = kMaxBands;  // a band count above what any tile can hold is clamped per tile anyway
+    // ---- host layout ------------------------------------------------------
+    tiles.assign(nTiles, TileDev{});
+    items.clear();
+    size_t bytes = 0;
+    struct Off
+    {
+        size_t warped, cov, d1, d, bbox, nd, wg;
+    };
+    std::vector<Off> itemOff;
+    struct TOff
+    {
+        size_t owner, blend, lo, hi, prev, chosen, cost, back;
+    };
+    std::vector<TOff> tileOff(nTiles);
+    maxW = 1;
+    for (int t = 0; t < nTiles; ++t)
+    {
+        const TileSpec& S = specs[t];
+        TileDev& T = tiles[t];
+        T.w = S.w;
+        T.h = S.h;
+        // SeamBlend.cpp:457-459.
+        int maxBands = 1;
+        {
+            int w = S.w, h = S.h;
+            while (w > 1 && h > 1 && maxBands < numBands)
+            {
+                w = (w + 1) / 2;
+                h = (h + 1) / 2;
+                ++maxBands;
+            }
+        }
+        T.bands = std::min(numBands, std::max(1, maxBands));
+        if (T.bands > kMaxBands) return fail(I360B_INVALID_PARAM, "numBands above %d is not supported.", kMaxBands);
+        T.firstItem = (int)items.size();
+        T.numItems = (int)S.items.size();
+        T.covWords = (S.w + 31) / 32;
+        T.out = S.out;
+        T.maxLines = std::max(S.w, S.h);
+        T.lw[0] = S.w;
+        T.lh[0] = S.h;
+        long long acc = 0;
+        T.loff[0] = 0;
+        for (int l = 1; l < kMaxBands; ++l)
+        {
+            T.lw[l] = (T.lw[l - 1] + 1) / 2;
+            T.lh[l] = (T.lh[l - 1] + 1) / 2;
+            T.loff[l] = acc;
+            if (l < T.bands) acc += (long long)T.lw[l] * T.lh[l];
+        }
+        size_t pyrPx = (size_t)acc;
+        maxW = std::max(maxW, S.w);
+        size_t px = (size_t)S.w * S.h;
+        TOff& to = tileOff[t];
+        to.owner = bytes; bytes += align256(px);
+        to.blend = bytes; bytes += align256(std::max<size_t>(pyrPx, 1) * 12);
+        size_t ml = (size_t)T.maxLines;
+        to.lo = bytes; bytes += align256(ml * 4);
+        to.hi = bytes; bytes += align256(ml * 4);
+        to.prev = bytes; bytes += align256(ml * 4);
+        to.chosen = bytes; bytes += align256(ml * 4);
+        to.cost = bytes; bytes += align256(ml * kSeamBand * 4);
+        to.back = bytes; bytes += align256(ml * kSeamBand);
+        for (int k = 0; k < T.numItems; ++k)
+        {
+            const ItemSpec& I = S.items[k];
+            ItemDev it{};
+            it.tile = t;
+            it.k = k;
+            it.img = I.img;
+            it.src = I.src;
+            it.srcW = I.srcW;
+            it.srcH = I.srcH;
+            it.gain = I.gain;
+            for (int q = 0; q < 9; ++q) it.H[q] = I.H[q];
+            it.offX = I.offX;
+            it.offY = I.offY;
+            Off o{};
+            if (renderPath) { o.warped = bytes; bytes += align256(px * 6); }
+            o.cov = bytes; bytes += align256((size_t)S.h * T.covWords * 4);
+            o.d1 = bytes; bytes += align256(px * 4);
+            o.d = bytes; bytes += align256(px * 4);
+            o.bbox = bytes; bytes += 256;
+            o.nd = bytes; bytes += align256(std::max<size_t>(pyrPx, 1) * 16);
+            o.wg = bytes; bytes += align256(std::max<size_t>(pyrPx, 1) * 4);
+            items.push_back(it);
+            itemOff.push_back(o);
+        }
+    }
+    nItems = (int)items.size();
+    // ---- work lists -------------------------------------------------------
+    std::vector<Unit> units;
+    auto addBlocks = [&](int id, int w, int h) {
+        for (int by = 0; by < (h + 7) / 8; ++by)
+            for (int bx = 0; bx < (w + 31) / 32; ++bx) units.push_back(Unit{id, bx, by, 0});
+    };
+    lists.clear();
+    auto beginList = [&]() { return (int)units.size(); };
+    auto endList = [&](int start) { lists.push_back(Range{start, (int)units.size() - start}); };
+    int s;
+    s = beginList();  // 0: coverage / warp
+    for (int i = 0; i < nItems; ++i) addBlocks(i, tiles[items[i].tile].w, tiles[items[i].tile].h);
+    endList(s);
+    s = beginList();  // 1: ownership
+    for (int t = 0; t < nTiles; ++t)
+    {
+        long long n = (long long)tiles[t].w * tiles[t].h;
+        for (long long b = 0; b < (n + 1023) / 1024; ++b) units.push_back(Unit{t, (int)b, 0, 0});
+    }
+    endList(s);
+    s = beginList();  // 2: level 0 output
+    for (int t = 0; t < nTiles; ++t) addBlocks(t, tiles[t].w, tiles[t].h);
+    endList(s);
+    for (int l = 0; l < kMaxBands - 1; ++l)  // 3 + l: down from level l
+    {
+        s = beginList();
+        for (int i = 0; i < nItems; ++i)
+        {
+            const TileDev& T = tiles[items[i].tile];
+            if (T.bands > l + 1) addBlocks(i, T.lw[l + 1], T.lh[l + 1]);
+        }
+        endList(s);
+    }
+    for (int l = 0; l < kMaxBands; ++l)  // 3 + (kMaxBands-1) + l: blend band at level l (l >= 1)
+    {
+        s = beginList();
+        if (l >= 1)
+            for (int t = 0; t < nTiles; ++t)
+                if (tiles[t].bands > l) addBlocks(t, tiles[t].lw[l], tiles[t].lh[l]);
+        endList(s);
+    }
+    for (int l = 0; l < kMaxBands; ++l)  // 3 + 2*kMaxBands - 1 + l: collapse at level l (1 <= l <= bands-2)
+    {
+        s = beginList();
+        if (l >= 1)
+            for (int t = 0; t < nTiles; ++t)
+                if (tiles[t].bands > l + 1) addBlocks(t, tiles[t].lw[l], tiles[t].lh[l]);
+        endList(s);
+    }
+    std::vector<int> ints;
+    for (int i = 0; i < nItems; ++i) ints.push_back(i);
+    int seamStart = (int)ints.size();
+    for (int t = 0; t < nTiles; ++t)
+        if (tiles[t].numItems >= 2) ints.push_back(t);
+    nSeam = (int)ints.size() - seamStart;
+    // ---- device allocation -----------------------------------------------
+    size_t unitBytes = align256(std::max<size_t>(units.size(), 1) * sizeof(Unit));
+    size_t intBytes = align256(std::max<size_t>(ints.size(), 1) * sizeof(int));
+    size_t itemBytes = align256(std::max(nItems, 1) * sizeof(ItemDev));
+    size_t tileBytes = align256(std::max(nTiles, 1) * sizeof(TileDev));
+    size_t metaOff = bytes;
+    bytes += unitBytes + intBytes + itemBytes + tileBytes + 256;
+    arenaBytes = bytes;
+    cudaError_t e = cudaMalloc(&arena, bytes);
+    if (e != cudaSuccess)
+    {
+        cudaGetLastError();
+        arena = nullptr;
+        return fail(e == cudaErrorMemoryAllocation ? I360B_OUT_OF_MEMORY : I360B_CUDA_ERROR,
+                    "render plan: device allocation of %zu bytes failed (%s)", bytes, cudaGetErrorString(e));
+    }
+    char* base = static_cast<char*>(arena);
+    for (int t = 0; t < nTiles; ++t)
+    {
+        TileDev& T = tiles[t];
+        const TOff& to = tileOff[t];
+        T.owner = reinterpret_cast<signed char*>(base + to.owner);
+        T.blend = reinterpret_cast<float*>(base + to.blend);
+        T.lo = reinterpret_cast<int*>(base + to.lo);
+        T.hi = reinterpret_cast<int*>(base + to.hi);
+        T.prevLine = reinterpret_cast<int*>(base + to.prev);
+        T.chosen = reinterpret_cast<int*>(base + to.chosen);
+        T.cost = reinterpret_cast<float*>(base + to.cost);
+        T.back = reinterpret_cast<unsigned char*>(base + to.back);
+    }
+    for (int i = 0; i < nItems; ++i)
+    {
+        ItemDev& it = items[i];
+        const Off& o = itemOff[i];
+        if (renderPath) it.img = reinterpret_cast<unsigned short*>(base + o.warped);
+        it.cov = reinterpret_cast<uint32_t*>(base + o.cov);
+        it.d1 = reinterpret_cast<float*>(base + o.d1);
+        it.d = reinterpret_cast<float*>(base + o.d);
+        it.bbox = reinterpret_cast<int*>(base + o.bbox);
+        it.nd = reinterpret_cast<float4*>(base + o.nd);
+        it.wg = reinterpret_cast<float*>(base + o.wg);
+    }
+    dUnits = reinterpret_cast<Unit*>(base + metaOff);
+    dInts = reinterpret_cast<int*>(base + metaOff + unitBytes);
+    dItems = reinterpret_cast<ItemDev*>(base + metaOff + unitBytes + intBytes);
+    dTiles = reinterpret_cast<TileDev*>(base + metaOff + unitBytes + intBytes + itemBytes);
+    dError = reinterpret_cast<int*>(base + metaOff + unitBytes + intBytes + itemBytes + tileBytes);
+    I360B_CUDA(cudaMemcpy(dUnits, units.data(), units.size() * sizeof(Unit), cudaMemcpyHostToDevice), "plan upload");
+    I360B_CUDA(cudaMemcpy(dInts, ints.data(), ints.size() * sizeof(int), cudaMemcpyHostToDevice), "plan upload");
+    if (nItems) I360B_CUDA(cudaMemcpy(dItems, items.data(), nItems * sizeof(ItemDev), cudaMemcpyHostToDevice), "plan upload");
+    if (nTiles) I360B_CUDA(cudaMemcpy(dTiles, tiles.data(), nTiles * sizeof(TileDev), cudaMemcpyHostToDevice), "plan upload");
+    I360B_CUDA(cudaMemset(dError, 0, sizeof(int)), "plan upload");
+    seamList = dInts + seamStart;
+    return I360B_SUCCESS;
+}
+
+Plan::~Plan()
+{
+    if (graphExec) cudaGraphExecDestroy(graphExec);
+    if (graph) cudaGraphDestroy(graph);
+    if (hostErr) cudaFreeHost(hostErr);
+    if (arena) cudaFree(arena);
+}
+
+const char* const kStageNames[kStages] = {"warp_gain_coverage", "chamfer_forward", "chamfer_backward",
+                                          "ownership", "seam_dp", "pyramid_down", "blend_bands", "collapse",
+                                          "level0_output"};
+
+int Plan::kernels_per_execute() const
+{
+    int n = (nItems > 0 ? 1 : 0) + (lists[0].count > 0 ? 1 : 0) + (nItems > 0 ? 2 : 0) + (lists[1].count > 0 ? 1 : 0) +
+            (nSeam > 0 ? 1 : 0) + (lists[2].count > 0 ? 1 : 0);
+    for (size_t i = 3; i < lists.size(); ++i) n += lists[i].count > 0 ? 1 : 0;
+    return n;
+}
+
+int Plan::enqueue(cudaStream_t s, cudaEvent_t* ev)
+{
+    BlendArgs a{dItems, dTiles, dError};
+    auto L = [&](int idx) { return lists[idx]; };
+    auto mark = [&](int i) {
+        if (ev) cudaEventRecord(ev[i], s);
+    };
+    mark(0);
+    if (nItems > 0) k_init_bbox<<<(nItems + 127) / 128, 128, 0, s>>>(dItems, nItems);
+    I360B_TRY(check_launch("bbox init kernel"));
+    I360B_CUDA(cudaMemsetAsync(dError, 0, sizeof(int), s), "error flag reset");
+    Range r = L(0);
+    if (render) I360B_TRY(launch_warp_tiles(a, dUnits + r.start, r.count, s));
+    else I360B_TRY(launch_coverage(a, dUnits + r.start, r.count, s));
+    mark(1);
+    I360B_TRY(launch_dt(a, dInts, nItems, false, maxW, s));
+    mark(2);
+    I360B_TRY(launch_dt(a, dInts, nItems, true, maxW, s));
+    mark(3);
+    r = L(1);
+    I360B_TRY(launch_owner(a, dUnits + r.start, r.count, s));
+    mark(4);
+    I360B_TRY(launch_seam(a, seamList, nSeam, s));
+    mark(5);
+    for (int l = 0; l < kMaxBands - 1; ++l)
+    {
+        r = L(3 + l);
+        I360B_TRY(launch_down(a, dUnits + r.start, r.count, l, s));
+    }
+    mark(6);
+    for (int l = kMaxBands - 1; l >= 1; --l)
+    {
+        r = L(3 + (kMaxBands - 1) + l);
+        I360B_TRY(launch_blend_level(a, dUnits + r.start, r.count, l, s));
+    }
+    mark(7);
+    for (int l = kMaxBands - 1; l >= 1; --l)
+    {
+        r = L(3 + 2 * kMaxBands - 1 + l);
+        I360B_TRY(launch_collapse(a, dUnits + r.start, r.count, l, s));
+    }
+    mark(8);
+    r = L(2);
+    I360B_TRY(launch_final0(a, dUnits + r.start, r.count, s));
+    mark(9);
+    return I360B_SUCCESS;
+}
+
+int Plan::execute(cudaStream_t s, bool useGraph)
+{
+    if (!useGraph) return enqueue(s);
+    if (!graphExec)
+    {
+        cudaStream_t cap = nullptr;
+        I360B_CUDA(cudaStreamCreateWithFlags(&cap, cudaStreamNonBlocking), "graph capture stream");
+        I360B_CUDA(cudaStreamBeginCapture(cap, cudaStreamCaptureModeThreadLocal), "graph capture");
+        int rc = enqueue(cap);
+        cudaError_t e = cudaStreamEndCapture(cap, &graph);
+        cudaStreamDestroy(cap);
+        if (rc != I360B_SUCCESS) return rc;
+        if (e != cudaSuccess) return cuda_fail(e, "graph capture");
+        I360B_CUDA(cudaGraphInstantiate(&graphExec, graph, 0), "graph instantiate");
+    }
+    I360B_CUDA(cudaGraphLaunch(graphExec, s), "graph launch");
+    return I360B_SUCCESS;
+}
+
+int Plan::check(cudaStream_t s)
+{
+    if (!hostErr) I360B_CUDA(cudaMallocHost(&hostErr, sizeof(int)), "pinned flag");
+    I360B_CUDA(cudaMemcpyAsync(hostErr, dError, sizeof(int), cudaMemcpyDeviceToHost, s), "error flag readback");
+    I360B_CUDA(cudaStreamSynchronize(s), "render synchronize");
+    if (*hostErr) return fail(I360B_KERNEL_LAUNCH_FAILED, "A render kernel gave up waiting (bounded spin); output invalid.");
+    return I360B_SUCCESS;
+}
+
+// Device-side setup of render-path items: matrices, singular contributors.
+int setup_render_items(const std::vector<double>& toCanvas, const std::vector<int>& itemFrame,
+                       const std::vector<int>& tileXY, int mode, std::vector<float>& Hout, std::vector<int>& offOut,
+                       std::vector<int>& singular)
+{
+    int n = (int)itemFrame.size();
+    Hout.assign((size_t)n * 9, 0.0f);
+    offOut.assign((size_t)n * 2, 0);
+    singular.assign(n, 0);
+    if (n == 0) return I360B_SUCCESS;
+    cudaStream_t s = thread_stream();
+    void *dM = nullptr, *dF = nullptr, *dXY = nullptr, *dS = nullptr, *dIt = nullptr;
+    int rc = I360B_SUCCESS;
+    std::vector<ItemDev> tmp(n);
+    if ((rc = dev_alloc(&dM, toCanvas.size() * 8, s, "setup")) || (rc = dev_alloc(&dF, n * 4, s, "setup")) ||
+        (rc = dev_alloc(&dXY, n * 8, s, "setup")) || (rc = dev_alloc(&dS, n * 4, s, "setup")) ||
+        (rc = dev_alloc(&dIt, n * sizeof(ItemDev), s, "setup")))
+        goto done;
+    cudaMemcpyAsync(dM, toCanvas.data(), toCanvas.size() * 8, cudaMemcpyHostToDevice, s);
+    cudaMemcpyAsync(dF, itemFrame.data(), n * 4, cudaMemcpyHostToDevice, s);
+    cudaMemcpyAsync(dXY, tileXY.data(), n * 8, cudaMemcpyHostToDevice, s);
+    k_setup_items<<<(n + 127) / 128, 128, 0, s>>>(static_cast<ItemDev*>(dIt), static_cast<double*>(dM),
+                                                 static_cast<int*>(dF), static_cast<int*>(dXY), n, mode,
+                                                 static_cast<int*>(dS));
+    if ((rc = check_launch("homography setup kernel"))) goto done;
+    cudaMemcpyAsync(tmp.data(), dIt, n * sizeof(ItemDev), cudaMemcpyDeviceToHost, s);
+    cudaMemcpyAsync(singular.data(), dS, n * 4, cudaMemcpyDeviceToHost, s);
+    {
+        cudaError_t e = cudaStreamSynchronize(s);
+        if (e != cudaSuccess) { rc = cuda_fail(e, "homography setup"); goto done; }
+    }
+    for (int i = 0; i < n; ++i)
+    {
+        for (int q = 0; q < 9; ++q) Hout[(size_t)i * 9 + q] = tmp[i].H[q];
+        offOut[2 * i] = tmp[i].offX;
+        offOut[2 * i + 1] = tmp[i].offY;
+    }
+done:
+    dev_free(dM, s);
+    dev_free(dF, s);
+    dev_free(dXY, s);
+    dev_free(dS, s);
+    dev_free(dIt, s);
+    return rc;
+}
+
+int launch_blend_chunk(const unsigned short* const* warped, int k, int w, int h, int bands, unsigned short* out,
+                       cudaStream_t s)
+{
+    std::vector<TileSpec> specs(1);
+    specs[0].w = w;
+    specs[0].h = h;
+    specs[0].out = out;
+    for (int i = 0; i < k; ++i)
+    {
+        ItemSpec it{};
+        it.img = warped[i];
+        specs[0].items.push_back(it);
+    }
+    Plan p;
+    I360B_TRY(p.build(specs, bands, false));
+    I360B_TRY(p.execute(s, false));
+    return p.check(s);
+}
+}  // namespace i360b
+
+// ---------------------------------------------------------------------------
+// C-ABI: render plans.
+// ---------------------------------------------------------------------------
+struct i360b_render_plan
+{
+    i360b::Plan plan;
+};
+
+using namespace i360b;
+
+extern "C" int i360b_render_plan_create(const i360b_frame* frames, int numFrames, const i360b_tile* tiles,
+                                        int numTiles, const int* contributors, int numBands, int coordMode,
+                                        i360b_render_plan** outPlan)
+{
+    clear_error();
+    if (!outPlan) return fail(I360B_INVALID_PARAM, "Null pointer argument.");
+    *outPlan = nullptr;
+    if (!frames || !tiles || numFrames <= 0 || numTiles <= 0) return fail(I360B_INVALID_PARAM, "Null or empty frame/tile list.");
+    if (numBands < 1) return fail(I360B_INVALID_PARAM, "numBands must be >= 1.");
+    if (coordMode != I360B_COORDS_REFERENCE && coordMode != I360B_COORDS_FP64_ORIGIN)
+        return fail(I360B_INVALID_PARAM, "Unknown coordinate mode %d.", coordMode);
+    I360B_TRY(ensure_ready());
+    for (int f = 0; f < numFrames; ++f)
+        if (!frames[f].rgb || frames[f].width <= 0 || frames[f].height <= 0)
+            return fail(I360B_INVALID_PARAM, "Frame %d has a null buffer or invalid dimensions.", f);
+    std::vector<double> M((size_t)numFrames * 9);
+    for (int f = 0; f < numFrames; ++f)
+        for (int q = 0; q < 9; ++q) M[(size_t)f * 9 + q] = frames[f].toCanvas[q];
+    std::vector<int> itemFrame, tileXY;
+    for (int t = 0; t < numTiles; ++t)
+    {
+        const i360b_tile& T = tiles[t];
+        if (T.width <= 0 || T.height <= 0 || !T.dOut || T.count < 0 || T.first < 0)
+            return fail(I360B_INVALID_PARAM, "Tile %d has invalid geometry or a null output.", t);
+        if (T.count > 0 && !contributors) return fail(I360B_INVALID_PARAM, "Null contributor list.");
+        if (T.count > kMaxContributors) return fail(I360B_INVALID_PARAM, "Tile %d has %d contributors (max %d).", t, T.count, kMaxContributors);
+        for (int k = 0; k < T.count; ++k)
+        {
+            int f = contributors[T.first + k];
+            if (f < 0 || f >= numFrames) return fail(I360B_INVALID_PARAM, "Tile %d names frame %d.", t, f);
+            itemFrame.push_back(f);
+            tileXY.push_back(T.x);
+            tileXY.push_back(T.y);
+        }
+    }
+    std::vector<float> H;
+    std::vector<int> off, singular;
+    I360B_TRY(setup_render_items(M, itemFrame, tileXY, coordMode, H, off, singular));
+    std::vector<TileSpec> specs(numTiles);
+    int idx = 0;
+    for (int t = 0; t < numTiles; ++t)
+    {
+        const i360b_tile& T = tiles[t];
+        specs[t].w = T.width;
+        specs[t].h = T.height;
+        specs[t].out = T.dOut;
+        for (int k = 0; k < T.count; ++k, ++idx)
+        {
+            // RenderExecutor.cpp:102 skips a contributor whose homography does
+            // not invert; it then takes no part in the blend.
+            if (singular[idx]) continue;
+            const i360b_frame& F = frames[contributors[T.first + k]];
+            ItemSpec it{};
+            it.src = F.rgb;
+            it.srcW = F.width;
+            it.srcH = F.height;
+            it.gain = F.gain;
+            for (int q = 0; q < 9; ++q) it.H[q] = H[(size_t)idx * 9 + q];
+            it.offX = off[2 * idx];
+            it.offY = off[2 * idx + 1];
+            specs[t].items.push_back(it);
+        }
+    }
+    auto* p = new (std::nothrow) i360b_render_plan;
+    if (!p) return fail(I360B_OUT_OF_MEMORY, "Host allocation failed.");
+    int rc = p->plan.build(specs, numBands, true);
+    if (rc != I360B_SUCCESS)
+    {
+        delete p;
+        return rc;
+    }
+    *outPlan = p;
+    return I360B_SUCCESS;
+}
+
+extern "C" int i360b_render_plan_execute(i360b_render_plan* plan, void* stream)
+{
+    clear_error();
+    if (!plan) return fail(I360B_INVALID_PARAM, "Null plan.");
+    I360B_TRY(ensure_ready());
+    return plan->plan.execute(static_cast<cudaStream_t>(stream), true);
+}
+
+extern "C" int i360b_render_plan_wait(i360b_render_plan* plan, void* stream)
+{
+    clear_error();
+    if (!plan) return fail(I360B_INVALID_PARAM, "Null plan.");
+    I360B_TRY(ensure_ready());
+    return plan->plan.check(static_cast<cudaStream_t>(stream));
+}
+
+extern "C" size_t i360b_render_plan_scratch_bytes(const i360b_render_plan* plan)
+{
+    return plan ? plan->plan.arenaBytes : 0;
+}
+
+extern "C" void i360b_render_plan_destroy(i360b_render_plan* plan)
+{
+    if (!plan) return;
+    cudaDeviceSynchronize();
+    delete plan;
+}
+
+
+extern "C" int i360b_render_plan_stats(i360b_render_plan* plan, void* stream, i360b_render_stats* out)
+{
+    clear_error();
+    if (!plan || !out) return fail(I360B_INVALID_PARAM, "Null pointer argument.");
+    I360B_TRY(ensure_ready());
+    Plan& P = plan->plan;
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    std::memset(out, 0, sizeof(*out));
+    out->numTiles = P.nTiles;
+    out->numItems = P.nItems;
+    out->kernelsPerExecute = P.kernels_per_execute();
+    long long px = 0;
+    for (const TileDev& T : P.tiles) px += (long long)T.w * T.h;
+    out->outputPixels = px;
+    out->scratchBytes = (long long)P.arenaBytes;
+    void* d = nullptr;
+    I360B_TRY(dev_alloc(&d, sizeof(unsigned long long), s, "stats"));
+    cudaMemsetAsync(d, 0, sizeof(unsigned long long), s);
+    if (P.nItems > 0)
+        k_count_cov<<<P.nItems, 256, 0, s>>>(P.dItems, P.dTiles, P.nItems, static_cast<unsigned long long*>(d));
+    unsigned long long c = 0;
+    cudaMemcpyAsync(&c, d, sizeof(c), cudaMemcpyDeviceToHost, s);
+    dev_free(d, s);
+    I360B_CUDA(cudaStreamSynchronize(s), "stats");
+    out->coveredItemPixels = (long long)c;
+    return I360B_SUCCESS;
+}
+
+extern "C" int i360b_render_plan_profile(i360b_render_plan* plan, void* stream, float* stageMs, int maxStages)
+{
+    clear_error();
+    if (!plan || !stageMs) return fail(I360B_INVALID_PARAM, "Null pointer argument.");
+    I360B_TRY(ensure_ready());
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    cudaEvent_t ev[kStages + 1];
+    for (int i = 0; i <= kStages; ++i) I360B_CUDA(cudaEventCreate(&ev[i]), "profile events");
+    int rc = plan->plan.enqueue(s, ev);
+    if (rc == I360B_SUCCESS) rc = plan->plan.check(s);
+    for (int i = 0; i < kStages && i < maxStages && rc == I360B_SUCCESS; ++i)
+        cudaEventElapsedTime(&stageMs[i], ev[i], ev[i + 1]);
+    for (int i = 0; i <= kStages; ++i) cudaEventDestroy(ev[i]);
+    return rc;
+}
+
+extern "C" const char* i360b_render_stage_name(int stage)
+{
+    return (stage >= 0 && stage < kStages) ? kStageNames[stage] : "";
+}

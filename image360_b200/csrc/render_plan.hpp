@@ -1,0 +1,71 @@
+// Host-side description of a batched seam-blend render (see render.cu).
+#pragma once
+
+#include "blend_kernels.cuh"
+
+#include <vector>
+
+namespace i360b
+{
+// One contributor of one tile.  Either `img` (a pre-warped tile-sized RGB48
+// device buffer) or the source frame + matrix for the fused warp.
+struct ItemSpec
+{
+    const unsigned short* img = nullptr;
+    const unsigned short* src = nullptr;
+    int srcW = 0, srcH = 0;
+    float H[9] = {1, 0, 0, 0, 1, 0, 0, 0, 1};
+    int offX = 0, offY = 0;
+    float gain = 1.0f;
+};
+
+struct TileSpec
+{
+    int w = 0, h = 0;
+    unsigned short* out = nullptr;
+    std::vector<ItemSpec> items;
+};
+
+constexpr int kStages = 9;
+extern const char* const kStageNames[kStages];
+
+struct Range
+{
+    int start;
+    int count;
+};
+
+struct Plan
+{
+    bool render = false;
+    int nTiles = 0, nItems = 0, nSeam = 0, bandsReq = 0, maxW = 1;
+    std::vector<ItemDev> items;
+    std::vector<TileDev> tiles;
+    std::vector<Range> lists;
+    void* arena = nullptr;
+    size_t arenaBytes = 0;
+    Unit* dUnits = nullptr;
+    int* dInts = nullptr;
+    int* seamList = nullptr;
+    ItemDev* dItems = nullptr;
+    TileDev* dTiles = nullptr;
+    int* dError = nullptr;
+    int* hostErr = nullptr;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t graphExec = nullptr;
+
+    Plan() = default;
+    Plan(const Plan&) = delete;
+    Plan& operator=(const Plan&) = delete;
+    ~Plan();
+
+    int build(const std::vector<TileSpec>& specs, int numBands, bool renderPath);
+    // Enqueues the kernel sequence; with `ev` non-null records ev[i] before
+    // stage i and ev[kStages] at the end (stage order of kStageNames).
+    int enqueue(cudaStream_t s, cudaEvent_t* ev = nullptr);
+    int kernels_per_execute() const;
+    int execute(cudaStream_t s, bool useGraph);
+    // Waits for the stream and reports a kernel that gave up (bounded waits).
+    int check(cudaStream_t s);
+};
+}  // namespace i360b

@@ -1,0 +1,223 @@
+/*
+ * image360_b200 - B200 (sm_100a) render backend for the Image360 stitching
+ * engine: the C-ABI boundary.
+ *
+ * Every entry point takes plain pointers and sizes and returns an int that is
+ * numerically identical to WindowsApp::Compute::ComputeResult
+ * (WindowsApp.Compute/HeaderFiles/ComputeTypes.h:32-50).  No exception ever
+ * crosses this boundary.  The last error message is kept per calling thread
+ * (the reference keeps one char[512] per backend object,
+ * WindowsApp.Core/HeaderFiles/CpuComputeBackend.h:88; calls arrive from several
+ * TaskScheduler threads at once, TaskScheduler.cpp:67, so a per-thread message
+ * is what makes GetLastError() meaningful here).
+ *
+ * Two kinds of entry point:
+ *   - i360b_<op>: the IComputeBackend operations.  Host buffers in, host
+ *     buffers out, synchronous: results are in host memory on return.  Each
+ *     calling thread gets its own CUDA stream.  Device memory comes from a
+ *     stream-ordered pool that is kept for the life of the process.
+ *   - i360b_launch_<op> / i360b_render_*: device-resident, stream-ordered
+ *     launchers for callers that keep frames in HBM.  `stream` is a
+ *     cudaStream_t passed as void* (NULL = the legacy default stream).
+ *
+ * Pixel format: RGB48 = interleaved unsigned short x3, row-major; (0,0,0)
+ * means "no data" (WindowsApp.Core/SourceFiles/SeamBlend.cpp:565).
+ */
+#ifndef IMAGE360_B200_H
+#define IMAGE360_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#if defined(__GNUC__)
+#define I360B_API __attribute__((visibility("default")))
+#else
+#define I360B_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ComputeResult values (ComputeTypes.h:32-50). */
+enum
+{
+    I360B_SUCCESS = 0,
+    I360B_NO_GPU = 1,
+    I360B_INVALID_PARAM = 2,
+    I360B_OUT_OF_MEMORY = 3,
+    I360B_KERNEL_LAUNCH_FAILED = 4,
+    I360B_CUDA_ERROR = 5,
+    I360B_NOT_SUPPORTED = 6
+};
+
+/* Mirrors WindowsApp::Compute::GpuInfo (ComputeTypes.h:18-29), with the bool
+ * stored as int for a stable C layout. */
+typedef struct i360b_gpu_info
+{
+    int deviceId;
+    char name[256];
+    size_t totalMemory;
+    size_t freeMemory;
+    int computeMajor;
+    int computeMinor;
+    int maxThreadsPerBlock;
+    int multiProcessorCount;
+    int hasTensorCores;
+} i360b_gpu_info;
+
+/* ---- lifecycle: IComputeBackend::Initialize/Shutdown/IsInitialized/
+ *      GetGpuInfo/GetLastError (IComputeBackend.h:21-25) ---------------- */
+
+/* Picks the visible device with the most memory (as CudaPipeline::Initialize
+ * does, CudaPipeline.cpp:137-152) and requires compute capability 10.x.
+ * Returns I360B_NO_GPU when there is none. */
+I360B_API int i360b_initialize(void);
+I360B_API void i360b_shutdown(void);
+I360B_API int i360b_is_initialized(void);
+I360B_API int i360b_get_gpu_info(i360b_gpu_info* out);
+/* Last error message of the calling thread ("" when none). */
+I360B_API const char* i360b_get_last_error(void);
+/* Records "<op> is not supported by the B200 backend" as the calling thread's
+ * last error and returns I360B_NOT_SUPPORTED: the result of the eight
+ * IComputeBackend operations outside the render path (IComputeBackend.h:53-168). */
+I360B_API int i360b_not_supported(const char* op);
+
+/* ---- IComputeBackend host-buffer operations ---------------------------- */
+
+/* IComputeBackend::WarpPerspective (IComputeBackend.h:29-32).  Backward
+ * bilinear warp; `homography` is 9 floats, row-major, mapping DESTINATION
+ * pixel (x+offsetX, y+offsetY) to SOURCE (WarpPerspectiveKernels.h:46-53).
+ * Out-of-bounds or singular pixels are written as (0,0,0). */
+I360B_API int i360b_warp_perspective(const unsigned short* srcData, int srcW, int srcH, unsigned short* dstData,
+                           int dstW, int dstH, const float* homography, int offsetX, int offsetY);
+
+/* IComputeBackend::MedianStack (IComputeBackend.h:35-38).  numInputs must be
+ * 1..32 (CpuComputeBackend.cpp:143).  Each input is width*height*3 values. */
+I360B_API int i360b_median_stack(const unsigned short* const* inputs, int numInputs, unsigned short* output, int width,
+                       int height, float sigmaThreshold);
+
+/* IComputeBackend::ApplyGain (IComputeBackend.h:41-42).  numPixels counts
+ * unsigned shorts (RenderExecutor passes width*height*3). */
+I360B_API int i360b_apply_gain(unsigned short* data, int numPixels, float gain);
+
+/* IComputeBackend::DemosaicBayer (IComputeBackend.h:46-49).  rgbCam is the
+ * 3x4 matrix as 12 floats, row-major. */
+I360B_API int i360b_demosaic_bayer(const unsigned short* cfaData, int width, int height, unsigned short blackLevel,
+                         const float camMul[4], const float rgbCam[12], uint32_t filters, unsigned short* rgbOut);
+
+/* ---- blend extension (no IComputeBackend counterpart) ------------------ */
+
+/* Kernels::SeamBlend::BlendChunkContributors (SeamBlendKernels.h:91,
+ * SeamBlend.cpp:549-587) with the band count exposed as
+ * Detail::MultiBandCompose does (SeamBlendKernels.h:75-79); 5 reproduces the
+ * reference's kDefaultNumBands.  numContributors may be 0 (all-zero output). */
+I360B_API int i360b_blend_chunk_contributors(const unsigned short* const* warpedBuffers, int numContributors, int width,
+                                   int height, int numBands, unsigned short* outResult);
+
+/* ---- device-resident launchers ----------------------------------------- */
+
+/* DemosaicBayer on device buffers. */
+I360B_API int i360b_launch_demosaic(const unsigned short* dCfa, int width, int height, unsigned short blackLevel,
+                          const float camMul[4], const float rgbCam[12], uint32_t filters, unsigned short* dRgbOut,
+                          void* stream);
+
+/* WarpPerspective on device buffers, followed by ApplyGain(gain) in the same
+ * pass (RenderExecutor.cpp:105-114 does the two back to back; gain is skipped
+ * when |gain-1| <= 1e-6 exactly as there). */
+I360B_API int i360b_launch_warp(const unsigned short* dSrc, int srcW, int srcH, unsigned short* dDst, int dstW, int dstH,
+                      const float* homography, int offsetX, int offsetY, float gain, void* stream);
+
+/* MedianStack on device buffers; dInputs is a HOST array of numInputs device
+ * pointers. */
+I360B_API int i360b_launch_median(const unsigned short* const* dInputs, int numInputs, unsigned short* dOutput, int width,
+                        int height, float sigmaThreshold, void* stream);
+
+/* ApplyGain on a device buffer. */
+I360B_API int i360b_launch_gain(unsigned short* dData, int numValues, float gain, void* stream);
+
+/* Seam blend of one chunk whose K warped buffers are already on the device
+ * (dWarped is a HOST array of K device pointers). */
+I360B_API int i360b_launch_blend(const unsigned short* const* dWarped, int numContributors, int width, int height,
+                       int numBands, unsigned short* dOut, void* stream);
+
+/* ---- batched render of a panorama's output tiles ----------------------- */
+
+/* One source frame: a demosaiced RGB48 image in device memory and its
+ * homography from frame pixels to canvas pixels (Homography, Types.h:138-141,
+ * in double).  gain is applied after the warp (RenderExecutor.cpp:111-114). */
+typedef struct i360b_frame
+{
+    const unsigned short* rgb;
+    int width;
+    int height;
+    double toCanvas[9];
+    float gain;
+} i360b_frame;
+
+/* One output tile (a RenderExecutor chunk, Types.h:143-152): canvas
+ * rectangle, its contributors contributors[first .. first+count), and the
+ * device RGB48 buffer (width*height*3) it is written to. */
+typedef struct i360b_tile
+{
+    int x;
+    int y;
+    int width;
+    int height;
+    int first;
+    int count;
+    unsigned short* dOut;
+} i360b_tile;
+
+/* Coordinate modes of the tile warp. */
+enum
+{
+    /* Inverse homography in FP32 by the adjugate (HomographyMath.cpp:94-116)
+     * and destination coordinates (x + tile.x, y + tile.y) in FP32, exactly as
+     * RenderExecutor feeds WarpPerspective: bit-identical to the CPU backend. */
+    I360B_COORDS_REFERENCE = 0,
+    /* Inverse homography in FP64 on the GPU and each tile's origin mapped in
+     * FP64; FP32 only for offsets inside the tile. */
+    I360B_COORDS_FP64_ORIGIN = 1
+};
+
+typedef struct i360b_render_plan i360b_render_plan;
+
+/* Builds a reusable plan (work lists, device scratch) for rendering `numTiles`
+ * uneven tiles from `numFrames` frames with `numBands` pyramid levels.  The
+ * frame and tile arrays are copied; device pointers inside them must stay
+ * valid while the plan is used. */
+I360B_API int i360b_render_plan_create(const i360b_frame* frames, int numFrames, const i360b_tile* tiles, int numTiles,
+                             const int* contributors, int numBands, int coordMode, i360b_render_plan** outPlan);
+/* Enqueues the whole render on `stream` (captured once as a CUDA graph and
+ * replayed on later calls).  Asynchronous: returns once enqueued. */
+I360B_API int i360b_render_plan_execute(i360b_render_plan* plan, void* stream);
+/* Waits for `stream` and reports a render kernel that gave up one of its
+ * bounded waits (I360B_KERNEL_LAUNCH_FAILED; the output is then invalid). */
+I360B_API int i360b_render_plan_wait(i360b_render_plan* plan, void* stream);
+/* Plan statistics.  coveredItemPixels (sum over tile contributors of their
+ * covered pixels after the last execute) needs a completed execute. */
+typedef struct i360b_render_stats
+{
+    int numTiles;
+    int numItems;          /* (tile, contributor) pairs */
+    int kernelsPerExecute; /* kernel launches one execute enqueues */
+    long long outputPixels;
+    long long coveredItemPixels;
+    long long scratchBytes;
+} i360b_render_stats;
+I360B_API int i360b_render_plan_stats(i360b_render_plan* plan, void* stream, i360b_render_stats* out);
+/* Runs the plan once without the graph, timing each stage with CUDA events on
+ * `stream`; stageMs receives up to maxStages values (9 stages, names from
+ * i360b_render_stage_name).  Synchronous. */
+I360B_API int i360b_render_plan_profile(i360b_render_plan* plan, void* stream, float* stageMs, int maxStages);
+I360B_API const char* i360b_render_stage_name(int stage);
+/* Device bytes of scratch the plan holds. */
+I360B_API size_t i360b_render_plan_scratch_bytes(const i360b_render_plan* plan);
+I360B_API void i360b_render_plan_destroy(i360b_render_plan* plan);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif

@@ -1,0 +1,330 @@
+"""Test infrastructure only: ctypes bindings for the CPU oracle.
+
+``C`` wraps ``liboracle.so`` (the plain-C restatement in ``i360_oracle.c``) and
+``R`` wraps ``_ref/libi360ref.so`` (the reference's own CPU kernels compiled from
+its sources, present only where the reference tree was available at build time).
+Only ``tests/``, ``__graft_entry__.smoke()`` and ``bench.py``'s CPU-baseline leg
+import this package; the product path never does.
+
+All image arguments are numpy ``uint16`` arrays, RGB48 as ``(h, w, 3)``.
+"""
+from __future__ import annotations
+
+import ctypes as ct
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ORACLE_SO = os.path.join(HERE, "liboracle.so")
+REF_SO = os.path.join(HERE, "_ref", "libi360ref.so")
+
+_u16p = ct.POINTER(ct.c_uint16)
+_f32p = ct.POINTER(ct.c_float)
+_f64p = ct.POINTER(ct.c_double)
+_i32p = ct.POINTER(ct.c_int32)
+_u8p = ct.POINTER(ct.c_uint8)
+
+
+def build(with_ref: bool = True) -> None:
+    """Compile liboracle.so (and _ref when the reference sources exist)."""
+    target = "all" if with_ref else "oracle"
+    subprocess.run(["make", "-s", "-C", HERE, target], check=True)
+
+
+def _p(a, t):
+    return a.ctypes.data_as(t)
+
+
+def _ptr_array(arrs, ctype):
+    arr = (ct.POINTER(ctype) * max(1, len(arrs)))()
+    for i, a in enumerate(arrs):
+        arr[i] = a.ctypes.data_as(ct.POINTER(ctype))
+    return arr
+
+
+class _Oracle:
+    """numpy-facing wrapper of the C restatement (liboracle.so)."""
+
+    def __init__(self, path: str = ORACLE_SO):
+        if not os.path.exists(path):
+            build(with_ref=False)
+        self.lib = ct.CDLL(path)
+        L = self.lib
+        L.or_render_tiles.restype = ct.c_double
+        L.or_invert_h.restype = ct.c_int
+        L.or_bbox.restype = ct.c_int
+        L.or_clamp_bands.restype = ct.c_int
+
+    def demosaic(self, cfa, black, cam_mul, rgb_cam, filters=0x94949494, f64=False):
+        cfa = np.ascontiguousarray(cfa, np.uint16)
+        h, w = cfa.shape
+        out = np.zeros((h, w, 3), np.uint16)
+        fn = self.lib.or_demosaic_f64 if f64 else self.lib.or_demosaic
+        fn(_p(cfa, _u16p), w, h, ct.c_uint16(black), _p(np.asarray(cam_mul, np.float32), _f32p),
+           _p(np.ascontiguousarray(rgb_cam, np.float32).reshape(12), _f32p), ct.c_uint32(filters),
+           _p(out, _u16p))
+        return out
+
+    def warp(self, src, dst_w, dst_h, inv_h, off_x=0, off_y=0, f64=False):
+        dst_w, dst_h = int(dst_w), int(dst_h)
+        src = np.ascontiguousarray(src, np.uint16)
+        sh, sw = src.shape[:2]
+        out = np.zeros((dst_h, dst_w, 3), np.uint16)
+        if f64:
+            H = np.ascontiguousarray(inv_h, np.float64).reshape(9)
+            self.lib.or_warp_f64(_p(src, _u16p), sw, sh, _p(out, _u16p), dst_w, dst_h, _p(H, _f64p),
+                                 int(off_x), int(off_y))
+        else:
+            H = np.ascontiguousarray(inv_h, np.float32).reshape(9)
+            self.lib.or_warp(_p(src, _u16p), sw, sh, _p(out, _u16p), dst_w, dst_h, _p(H, _f32p),
+                             int(off_x), int(off_y))
+        return out
+
+    def median(self, inputs, sigma=2.0):
+        ins = [np.ascontiguousarray(a, np.uint16) for a in inputs]
+        h, w = ins[0].shape[:2]
+        out = np.zeros((h, w, 3), np.uint16)
+        self.lib.or_median(_ptr_array(ins, ct.c_uint16), len(ins), _p(out, _u16p), w, h, ct.c_float(sigma))
+        return out
+
+    def gain(self, data, gain):
+        d = np.array(data, np.uint16, copy=True)
+        self.lib.or_gain(_p(d, _u16p), d.size, ct.c_float(gain))
+        return d
+
+    def invert_h(self, H):
+        H = np.ascontiguousarray(H, np.float32).reshape(9)
+        out = np.zeros(9, np.float32)
+        ok = self.lib.or_invert_h(_p(H, _f32p), _p(out, _f32p))
+        return (out if ok else None)
+
+    def coverage(self, img):
+        img = np.ascontiguousarray(img, np.uint16)
+        h, w = img.shape[:2]
+        cov = np.zeros((h, w), np.uint8)
+        self.lib.or_coverage(_p(img, _u16p), w, h, _p(cov, _u8p))
+        return cov
+
+    def coverage_distance(self, cov):
+        cov = np.ascontiguousarray(cov, np.uint8)
+        h, w = cov.shape
+        d = np.zeros((h, w), np.float32)
+        self.lib.or_coverage_distance(_p(cov, _u8p), w, h, _p(d, _f32p))
+        return d
+
+    def ownership(self, dists):
+        ds = [np.ascontiguousarray(d, np.float32) for d in dists]
+        h, w = ds[0].shape
+        o = np.zeros((h, w), np.int32)
+        self.lib.or_ownership(_ptr_array(ds, ct.c_float), len(ds), w, h, _p(o, _i32p))
+        return o
+
+    def bbox(self, cov):
+        cov = np.ascontiguousarray(cov, np.uint8)
+        h, w = cov.shape
+        b = np.zeros(4, np.int32)
+        ok = self.lib.or_bbox(_p(cov, _u8p), w, h, _p(b, _i32p))
+        return b, bool(ok)
+
+    def compose(self, bufs, dists, owner, bands, f64=False):
+        bs = [np.ascontiguousarray(b, np.uint16) for b in bufs]
+        h, w = owner.shape
+        owner = np.ascontiguousarray(owner, np.int32)
+        out = np.zeros((h, w, 3), np.uint16)
+        if f64:
+            self.lib.or_compose_f64(_ptr_array(bs, ct.c_uint16), _p(owner, _i32p), len(bs), w, h, bands,
+                                    _p(out, _u16p))
+        else:
+            ds = [np.ascontiguousarray(d, np.float32) for d in dists]
+            self.lib.or_compose(_ptr_array(bs, ct.c_uint16), _ptr_array(ds, ct.c_float), _p(owner, _i32p),
+                                len(bs), w, h, bands, _p(out, _u16p))
+        return out
+
+    def blend(self, bufs, bands=5, return_owner=False):
+        bs = [np.ascontiguousarray(b, np.uint16) for b in bufs]
+        h, w = bs[0].shape[:2]
+        out = np.zeros((h, w, 3), np.uint16)
+        owner = np.zeros((h, w), np.int32)
+        self.lib.or_blend_chunk_ex(_ptr_array(bs, ct.c_uint16), len(bs), w, h, bands, _p(out, _u16p),
+                                   _p(owner, _i32p))
+        return (out, owner) if return_owner else out
+
+    def clamp_bands(self, w, h, bands):
+        return self.lib.or_clamp_bands(w, h, bands)
+
+    def render_tiles(self, threads, frames, inv_h, gains, tiles, bands, want_out=True):
+        """tiles: list of (x, y, w, h, [frame indices]). Returns (seconds, outputs)."""
+        return _render_tiles(self.lib.or_render_tiles, None, threads, frames, inv_h, gains, tiles, bands,
+                             want_out)
+
+
+def _render_tiles(fn, tier, threads, frames, inv_h, gains, tiles, bands, want_out):
+    fr = [np.ascontiguousarray(f, np.uint16) for f in frames]
+    fw = np.array([f.shape[1] for f in fr], np.int32)
+    fh = np.array([f.shape[0] for f in fr], np.int32)
+    H = np.ascontiguousarray(inv_h, np.float32).reshape(-1)
+    g = np.ascontiguousarray(gains, np.float32)
+    rect = np.array([t[:4] for t in tiles], np.int32).reshape(-1)
+    off = np.zeros(len(tiles) + 1, np.int32)
+    for i, t in enumerate(tiles):
+        off[i + 1] = off[i] + len(t[4])
+    con = np.array([c for t in tiles for c in t[4]] or [0], np.int32)
+    outs = [np.zeros((t[3], t[2], 3), np.uint16) for t in tiles] if want_out else []
+    optrs = (_u16p * max(1, len(tiles)))()
+    for i, o in enumerate(outs):
+        optrs[i] = o.ctypes.data_as(_u16p)
+    args = [threads]
+    if tier is not None:
+        args.append(tier)
+    args += [_ptr_array(fr, ct.c_uint16), _p(fw, _i32p), _p(fh, _i32p), _p(H, _f32p), _p(g, _f32p),
+             len(tiles), _p(rect, _i32p), _p(off, _i32p), _p(con, _i32p), bands,
+             optrs if want_out else None]
+    secs = fn(*args)
+    return secs, outs
+
+
+class _Reference:
+    """numpy-facing wrapper of the reference's own CPU code (_ref/libi360ref.so)."""
+
+    def __init__(self, path: str = REF_SO):
+        self.lib = ct.CDLL(path)
+        L = self.lib
+        L.ref_render_tiles.restype = ct.c_double
+        L.ref_demosaic_frames.restype = ct.c_double
+        L.ref_backend_new.restype = ct.c_void_p
+        L.ref_backend_last_error.restype = ct.c_char_p
+        L.ref_backend_last_error.argtypes = [ct.c_void_p]
+        for n in ("ref_backend_free", "ref_backend_init"):
+            getattr(L, n).argtypes = [ct.c_void_p]
+        self.tier = L.ref_simd_tier()
+
+    def demosaic(self, cfa, black, cam_mul, rgb_cam, filters=0x94949494, tier=0):
+        cfa = np.ascontiguousarray(cfa, np.uint16)
+        h, w = cfa.shape
+        out = np.zeros((h, w, 3), np.uint16)
+        self.lib.ref_demosaic(tier, _p(cfa, _u16p), w, h, ct.c_uint16(black),
+                              _p(np.asarray(cam_mul, np.float32), _f32p),
+                              _p(np.ascontiguousarray(rgb_cam, np.float32).reshape(12), _f32p),
+                              ct.c_uint32(filters), _p(out, _u16p))
+        return out
+
+    def warp(self, src, dst_w, dst_h, inv_h, off_x=0, off_y=0, tier=0):
+        dst_w, dst_h = int(dst_w), int(dst_h)
+        src = np.ascontiguousarray(src, np.uint16)
+        sh, sw = src.shape[:2]
+        out = np.zeros((dst_h, dst_w, 3), np.uint16)
+        H = np.ascontiguousarray(inv_h, np.float32).reshape(9)
+        self.lib.ref_warp(tier, _p(src, _u16p), sw, sh, _p(out, _u16p), dst_w, dst_h, _p(H, _f32p),
+                          int(off_x), int(off_y))
+        return out
+
+    def median(self, inputs, sigma=2.0, tier=0):
+        ins = [np.ascontiguousarray(a, np.uint16) for a in inputs]
+        h, w = ins[0].shape[:2]
+        out = np.zeros((h, w, 3), np.uint16)
+        self.lib.ref_median(tier, _ptr_array(ins, ct.c_uint16), len(ins), _p(out, _u16p), w, h,
+                            ct.c_float(sigma))
+        return out
+
+    def gain(self, data, gain):
+        d = np.array(data, np.uint16, copy=True)
+        self.lib.ref_gain(_p(d, _u16p), d.size, ct.c_float(gain))
+        return d
+
+    def invert_h(self, H):
+        H = np.ascontiguousarray(H, np.float32).reshape(9)
+        out = np.zeros(9, np.float32)
+        ok = self.lib.ref_invert_h(_p(H, _f32p), _p(out, _f32p))
+        return (out if ok else None)
+
+    def coverage_distance(self, cov):
+        cov = np.ascontiguousarray(cov, np.uint8)
+        h, w = cov.shape
+        d = np.zeros((h, w), np.float32)
+        self.lib.ref_coverage_distance(_p(cov, _u8p), w, h, _p(d, _f32p))
+        return d
+
+    def ownership(self, dists):
+        ds = [np.ascontiguousarray(d, np.float32) for d in dists]
+        h, w = ds[0].shape
+        o = np.zeros((h, w), np.int32)
+        self.lib.ref_ownership(_ptr_array(ds, ct.c_float), len(ds), w, h, _p(o, _i32p))
+        return o
+
+    def bbox(self, cov):
+        cov = np.ascontiguousarray(cov, np.uint8)
+        h, w = cov.shape
+        b = np.zeros(4, np.int32)
+        ok = self.lib.ref_bbox(_p(cov, _u8p), w, h, _p(b, _i32p))
+        return b, bool(ok)
+
+    def compose(self, bufs, dists, owner, bands):
+        bs = [np.ascontiguousarray(b, np.uint16) for b in bufs]
+        ds = [np.ascontiguousarray(d, np.float32) for d in dists]
+        h, w = owner.shape
+        owner = np.ascontiguousarray(owner, np.int32)
+        out = np.zeros((h, w, 3), np.uint16)
+        self.lib.ref_compose(_ptr_array(bs, ct.c_uint16), _ptr_array(ds, ct.c_float), _p(owner, _i32p),
+                             len(bs), w, h, bands, _p(out, _u16p))
+        return out
+
+    def blend(self, bufs, bands=None):
+        bs = [np.ascontiguousarray(b, np.uint16) for b in bufs]
+        h, w = bs[0].shape[:2]
+        out = np.zeros((h, w, 3), np.uint16)
+        if bands is None:
+            self.lib.ref_blend_chunk(_ptr_array(bs, ct.c_uint16), len(bs), w, h, _p(out, _u16p))
+        else:
+            self.lib.ref_blend_chunk_bands(_ptr_array(bs, ct.c_uint16), len(bs), w, h, bands, _p(out, _u16p))
+        return out
+
+    def render_tiles(self, threads, frames, inv_h, gains, tiles, bands, want_out=True, tier=None):
+        return _render_tiles(self.lib.ref_render_tiles, self.tier if tier is None else tier, threads, frames,
+                             inv_h, gains, tiles, bands, want_out)
+
+    def backend(self):
+        return _RefBackend(self.lib)
+
+
+class _RefBackend:
+    """CpuComputeBackend facade (argument checks and result codes)."""
+
+    def __init__(self, lib):
+        self.lib = lib
+        self.h = ct.c_void_p(lib.ref_backend_new())
+
+    def __del__(self):
+        try:
+            self.lib.ref_backend_free(self.h)
+        except Exception:
+            pass
+
+    def initialize(self):
+        return self.lib.ref_backend_init(self.h)
+
+    def last_error(self):
+        return self.lib.ref_backend_last_error(self.h).decode()
+
+    def call(self, name, *args):
+        return getattr(self.lib, "ref_backend_" + name)(self.h, *args)
+
+
+_C = None
+_R = None
+
+
+def oracle() -> _Oracle:
+    global _C
+    if _C is None:
+        _C = _Oracle()
+    return _C
+
+
+def reference():
+    """The reference's own CPU code, or None when _ref was not built here."""
+    global _R
+    if _R is None and os.path.exists(REF_SO):
+        _R = _Reference()
+    return _R

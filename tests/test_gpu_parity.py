@@ -1,0 +1,150 @@
+"""GPU parity of every render-path kernel against the CPU oracle.
+
+The oracle (oracle/i360_oracle.c) restates the reference's scalar CPU backend
+and is itself pinned to the reference (test_oracle_ref.py, golden fixtures).
+Bars: demosaic, warp, median, gain and blend bit-exact (the reference's own
+cross-tier tolerance for demosaic/median is exact; for warp it is <= 1, and the
+seam blend's 1-LSB bar is met with 0).
+"""
+import numpy as np
+import pytest
+
+from image360_b200 import ComputeResult, synth
+
+pytestmark = pytest.mark.gpu
+
+RGB_CAM = np.array([[1.9, -0.7, -0.2, 0.0], [-0.3, 1.5, -0.2, 0.0], [0.0, -0.4, 1.6, 0.0]], np.float32)
+CAM_MUL = np.array([1.8, 1.0, 1.5, 1.0], np.float32)
+
+
+def test_initialize_and_info(backend):
+    info = backend.get_gpu_info()
+    assert info["computeMajor"] == 10
+    assert info["multiProcessorCount"] > 0
+
+
+@pytest.mark.parametrize("w,h", [(24, 20), (1, 1), (2, 3), (37, 29), (640, 480), (1001, 77)])
+@pytest.mark.parametrize("filters", [synth.RGGB, 0x16161616, 0x61616161, 0x49494949])
+def test_demosaic_exact(backend, oracle_c, w, h, filters):
+    rng = np.random.default_rng(w * 1000 + h)
+    cfa = rng.integers(0, 16384, (h, w), dtype=np.uint16)
+    out = np.zeros((h, w, 3), np.uint16)
+    assert backend.demosaic_bayer(cfa, 64, CAM_MUL, RGB_CAM, filters, out) == ComputeResult.SUCCESS
+    ref = oracle_c.demosaic(cfa, 64, CAM_MUL, RGB_CAM, filters)
+    assert np.array_equal(out, ref)
+
+
+def test_demosaic_engine_smoke_vector(backend, oracle_c):
+    # tests/engine_smoke/main.cpp:259-279
+    w, h = 24, 20
+    y, x = np.mgrid[0:h, 0:w]
+    cfa = (200 + (x * 31 + y * 19) % 3000).astype(np.uint16)
+    out = np.zeros((h, w, 3), np.uint16)
+    assert backend.demosaic_bayer(cfa, 64, CAM_MUL, RGB_CAM, synth.RGGB, out) == ComputeResult.SUCCESS
+    assert np.array_equal(out, oracle_c.demosaic(cfa, 64, CAM_MUL, RGB_CAM, synth.RGGB))
+
+
+def _warp_cases():
+    rng = np.random.default_rng(5)
+    cases = []
+    for i in range(12):
+        sw, sh = (int(v) for v in rng.integers(2, 300, 2))
+        dw, dh = (int(v) for v in rng.integers(1, 300, 2))
+        a = rng.uniform(-0.3, 0.3)
+        H = [np.cos(a), -np.sin(a), rng.uniform(-20, 20), np.sin(a), np.cos(a), rng.uniform(-20, 20),
+             rng.uniform(-1e-3, 1e-3), rng.uniform(-1e-3, 1e-3), 1.0]
+        cases.append((sw, sh, dw, dh, H, int(rng.integers(-30, 30)), int(rng.integers(-30, 30))))
+    cases.append((40, 30, 40, 30, [np.cos(0.06), -np.sin(0.06), 1.7, np.sin(0.06), np.cos(0.06), 0.9, 0, 0, 1], 0, 0))
+    cases.append((16, 16, 16, 16, [1, 0, 0, 0, 1, 0, 0, 0, 1], 0, 0))
+    cases.append((16, 16, 16, 16, [1, 0, 0, 0, 1, 0, 0, 0, 0], 0, 0))        # singular: all zeros
+    cases.append((16, 16, 8, 8, [1, 0, 1e9, 0, 1, 0, 0, 0, 1], 0, 0))       # far outside
+    return cases
+
+
+@pytest.mark.parametrize("case", _warp_cases())
+def test_warp_exact(backend, oracle_c, case):
+    sw, sh, dw, dh, H, ox, oy = case
+    rng = np.random.default_rng(sw * 7 + dh)
+    src = rng.integers(0, 65536, (sh, sw, 3), dtype=np.uint16)
+    H = np.array(H, np.float32)
+    out = np.zeros((dh, dw, 3), np.uint16)
+    assert backend.warp_perspective(src, out, H, ox, oy) == ComputeResult.SUCCESS
+    assert np.array_equal(out, oracle_c.warp(src, dw, dh, H, ox, oy))
+
+
+@pytest.mark.parametrize("n", [1, 2, 3, 4, 5, 8, 9, 16, 17, 21, 31, 32])
+def test_median_exact(backend, oracle_c, n):
+    rng = np.random.default_rng(n)
+    w, h = 53, 17
+    ins = [rng.integers(0, 16384, (h, w, 3), dtype=np.uint16) for _ in range(n)]
+    for i in range(min(3, n)):
+        ins[i][5, 5, :] = 60000
+    ins[0][0, 0, 0] = 65535
+    out = np.zeros((h, w, 3), np.uint16)
+    assert backend.median_stack(ins, out, w, h, 2.0) == ComputeResult.SUCCESS
+    assert np.array_equal(out, oracle_c.median(ins, 2.0))
+
+
+def test_median_engine_smoke_shape(backend, oracle_c):
+    # 17x13x3, 21 inputs, three 60000 outliers at index 100 (engine_smoke/main.cpp:178-193)
+    rng = np.random.default_rng(777)
+    ins = [rng.integers(0, 4001, (13, 17, 3), dtype=np.uint16) for _ in range(21)]
+    for i in range(3):
+        ins[i].reshape(-1)[100] = 60000
+    out = np.zeros((13, 17, 3), np.uint16)
+    assert backend.median_stack(ins, out, 17, 13) == ComputeResult.SUCCESS
+    assert np.array_equal(out, oracle_c.median(ins))
+
+
+@pytest.mark.parametrize("gain", [2.0, 0.5, 1.0, 1.0000001, 1.37, 0.8123])
+def test_gain_exact(backend, oracle_c, gain):
+    rng = np.random.default_rng(3)
+    d = rng.integers(0, 65536, 1003, dtype=np.uint16)
+    ref = oracle_c.gain(d, gain)
+    got = d.copy()
+    assert backend.apply_gain(got, gain) == ComputeResult.SUCCESS
+    assert np.array_equal(got, ref)
+
+
+def test_gain_known_answer(backend):
+    d = np.array([100, 200, 300, 400], np.uint16)   # engine_smoke/main.cpp:111-114
+    assert backend.apply_gain(d, 2.0) == ComputeResult.SUCCESS
+    assert d.tolist() == [200, 400, 600, 800]
+
+
+def _rand_buf(rng, w, h):
+    img = np.zeros((h, w, 3), np.uint16)
+    x0, x1 = sorted(rng.integers(0, w, 2))
+    y0, y1 = sorted(rng.integers(0, h, 2))
+    yy, xx = np.mgrid[0:h, 0:w]
+    m = (xx >= x0) & (xx <= x1 + 3) & (yy >= y0) & (yy <= y1 + 3) & (xx + yy > rng.integers(0, w // 2 + 1))
+    v = rng.integers(100, 30000, (h, w, 3)).astype(np.uint16)
+    img[m] = v[m]
+    return img
+
+
+@pytest.mark.parametrize("seed", range(8))
+def test_blend_random_exact(backend, oracle_c, seed):
+    rng = np.random.default_rng(100 + seed)
+    w, h = (int(v) for v in rng.integers(3, 300, 2))
+    k = int(rng.integers(1, 6))
+    bufs = [_rand_buf(rng, w, h) for _ in range(k)]
+    for bands in (1, 3, 5, 6):
+        out = np.zeros((h, w, 3), np.uint16)
+        assert backend.blend_chunk_contributors(bufs, w, h, out, bands) == ComputeResult.SUCCESS, backend.get_last_error()
+        ref = oracle_c.blend(bufs, bands)
+        assert np.array_equal(out, ref), (seed, bands, int(np.abs(out.astype(int) - ref).max()))
+
+
+def test_blend_empty_and_single(backend, oracle_c):
+    w, h = 50, 30
+    out = np.ones((h, w, 3), np.uint16)
+    assert backend.blend_chunk_contributors([], w, h, out, 5) == ComputeResult.SUCCESS
+    assert not out.any()
+    full = np.random.default_rng(1).integers(1, 60000, (h, w, 3)).astype(np.uint16)
+    out = np.zeros((h, w, 3), np.uint16)
+    assert backend.blend_chunk_contributors([full], w, h, out, 5) == ComputeResult.SUCCESS
+    assert np.array_equal(out, oracle_c.blend([full], 5))
+    zero = np.zeros((h, w, 3), np.uint16)
+    assert backend.blend_chunk_contributors([zero, full, zero], w, h, out, 5) == ComputeResult.SUCCESS
+    assert np.array_equal(out, oracle_c.blend([zero, full, zero], 5))

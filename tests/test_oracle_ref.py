@@ -1,0 +1,93 @@
+"""Pins the C oracle against the reference's own CPU code run live
+(oracle/_ref, compiled from the reference sources; skipped where it was not
+built).  Random shapes, edge sizes and every stage of the seam blend."""
+import numpy as np
+import pytest
+
+CAM = [1.8, 1.0, 1.5, 1.0]
+RGB = np.array([[1.9, -0.7, -0.2, 0.0], [-0.3, 1.5, -0.2, 0.0], [0.0, -0.4, 1.6, 0.0]], np.float32)
+
+
+@pytest.mark.parametrize("w,h", [(24, 20), (1, 1), (2, 3), (37, 29), (3, 1)])
+@pytest.mark.parametrize("filters", [0x94949494, 0x16161616, 0x61616161, 0x49494949])
+def test_demosaic(oracle_c, reference, w, h, filters):
+    rng = np.random.default_rng(w * 31 + h)
+    cfa = rng.integers(0, 65536, (h, w), dtype=np.uint16)
+    a = oracle_c.demosaic(cfa, 64, CAM, RGB, filters)
+    assert np.array_equal(a, reference.demosaic(cfa, 64, CAM, RGB, filters, tier=0))
+    assert np.abs(a.astype(int) - reference.demosaic(cfa, 64, CAM, RGB, filters, tier=reference.tier)).max() <= 1
+
+
+@pytest.mark.parametrize("seed", range(10))
+def test_warp(oracle_c, reference, seed):
+    rng = np.random.default_rng(seed)
+    sw, sh = (int(v) for v in rng.integers(2, 60, 2))
+    dw, dh = (int(v) for v in rng.integers(1, 70, 2))
+    src = rng.integers(0, 65536, (sh, sw, 3), dtype=np.uint16)
+    a = rng.uniform(-0.3, 0.3)
+    H = np.array([np.cos(a), -np.sin(a), rng.uniform(-5, 5), np.sin(a), np.cos(a), rng.uniform(-5, 5),
+                  rng.uniform(-1e-3, 1e-3), rng.uniform(-1e-3, 1e-3), 1], np.float32)
+    ox, oy = (int(v) for v in rng.integers(-10, 10, 2))
+    out = oracle_c.warp(src, dw, dh, H, ox, oy)
+    assert np.array_equal(out, reference.warp(src, dw, dh, H, ox, oy, tier=0))
+    assert np.abs(out.astype(int) - reference.warp(src, dw, dh, H, ox, oy, tier=reference.tier)).max() <= 1
+
+
+@pytest.mark.parametrize("n", [1, 3, 4, 7, 16, 21, 32, 40])
+def test_median(oracle_c, reference, n):
+    rng = np.random.default_rng(n)
+    ins = [rng.integers(0, 4000, (7, 9, 3), dtype=np.uint16) for _ in range(n)]
+    ins[0][1, 1, 1] = 60000
+    assert np.array_equal(oracle_c.median(ins), reference.median(ins, tier=0))
+
+
+def test_gain_and_inverse(oracle_c, reference):
+    rng = np.random.default_rng(2)
+    d = rng.integers(0, 65536, 999, dtype=np.uint16)
+    for g in [0.5, 1.0, 1.0000001, 1.37, 2.0, 3.9]:
+        assert np.array_equal(oracle_c.gain(d, g), reference.gain(d, g))
+    for _ in range(200):
+        H = rng.normal(size=9).astype(np.float32)
+        a, b = oracle_c.invert_h(H), reference.invert_h(H)
+        assert (a is None and b is None) or np.array_equal(a, b)
+    assert oracle_c.invert_h(np.zeros(9, np.float32)) is None
+
+
+def _rand_buf(rng, w, h):
+    img = np.zeros((h, w, 3), np.uint16)
+    x0, x1 = sorted(rng.integers(0, w, 2))
+    y0, y1 = sorted(rng.integers(0, h, 2))
+    yy, xx = np.mgrid[0:h, 0:w]
+    m = (xx >= x0) & (xx <= x1 + 3) & (yy >= y0) & (yy <= y1 + 3) & (xx + yy > rng.integers(0, w // 2 + 1))
+    v = rng.integers(100, 30000, (h, w, 3)).astype(np.uint16)
+    img[m] = v[m]
+    return img
+
+
+@pytest.mark.parametrize("seed", range(12))
+def test_seam_blend_stages(oracle_c, reference, seed):
+    rng = np.random.default_rng(1000 + seed)
+    w, h = (int(v) for v in rng.integers(3, 90, 2))
+    k = int(rng.integers(1, 5))
+    bufs = [_rand_buf(rng, w, h) for _ in range(k)]
+    covs = [oracle_c.coverage(b) for b in bufs]
+    dists = []
+    for c in covs:
+        d = oracle_c.coverage_distance(c)
+        assert np.array_equal(d, reference.coverage_distance(c))
+        b1, v1 = oracle_c.bbox(c)
+        b2, v2 = reference.bbox(c)
+        assert v1 == v2 and np.array_equal(b1, b2)
+        dists.append(d)
+    owner = oracle_c.ownership(dists)
+    assert np.array_equal(owner, reference.ownership(dists))
+    for bands in (1, 2, 5, 6, 9):
+        assert np.array_equal(oracle_c.compose(bufs, dists, owner, bands), reference.compose(bufs, dists, owner, bands))
+        assert np.array_equal(oracle_c.blend(bufs, bands), reference.blend(bufs, bands))
+    assert np.array_equal(oracle_c.blend(bufs, 5), reference.blend(bufs))
+
+
+def test_blend_empty(oracle_c, reference):
+    z = np.zeros((10, 12, 3), np.uint16)
+    assert not oracle_c.blend([z, z], 5).any()
+    assert not reference.blend([z, z]).any()
