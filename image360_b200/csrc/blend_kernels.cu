@@ -23,96 +23,176 @@ __device__ __forceinline__ bool cov_bit(const uint32_t* cov, int covWords, int x
 // ---------------------------------------------------------------------------
 // Coverage (SeamBlend.cpp:564-567): covered = any channel != 0, as bits, plus
 // the inclusive bounding box of covered pixels (SeamBlend.cpp:263-280).
-// A warp owns 32 consecutive pixels of one row, so its ballot is one word.
+// A CTA owns a band of kBandRows full-width rows of one contributor; each warp
+// walks its rows 32 pixels at a time, so one ballot is one coverage word.
 // ---------------------------------------------------------------------------
-__device__ __forceinline__ void emit_coverage(const ItemDev& it, const TileDev& T, int x, int y, bool covered)
+struct BoxAcc
 {
-    unsigned m = __ballot_sync(kFull, covered);
-    int lane = threadIdx.x & 31;
-    if (y < T.h && lane == 0) it.cov[(size_t)y * T.covWords + (x >> 5)] = m;
-    if (m)
+    int x0 = 0x7fffffff, y0 = 0x7fffffff, x1 = -1, y1 = -1, n = 0;
+    __device__ __forceinline__ void add(bool c, int x, int y)
     {
-        int mnx = __reduce_min_sync(kFull, covered ? x : 0x7fffffff);
-        int mxx = __reduce_max_sync(kFull, covered ? x : -1);
-        if (lane == 0)
+        if (c)
         {
-            atomicMin(it.bbox + 0, mnx);
-            atomicMin(it.bbox + 1, y);
-            atomicMax(it.bbox + 2, mxx);
-            atomicMax(it.bbox + 3, y);
+            ++n;
+            x0 = min(x0, x);
+            x1 = max(x1, x);
+            y0 = min(y0, y);
+            y1 = max(y1, y);
         }
     }
-}
+    // Block-wide reduction and one atomic update of the contributor's box.
+    __device__ __forceinline__ void flush(int* bbox)
+    {
+        __shared__ int sb[5][8];
+        int v0 = __reduce_min_sync(kFull, x0), v1 = __reduce_min_sync(kFull, y0);
+        int v2 = __reduce_max_sync(kFull, x1), v3 = __reduce_max_sync(kFull, y1);
+        int v4 = __reduce_add_sync(kFull, n);
+        int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+        if (lane == 0)
+        {
+            sb[0][warp] = v0;
+            sb[1][warp] = v1;
+            sb[2][warp] = v2;
+            sb[3][warp] = v3;
+            sb[4][warp] = v4;
+        }
+        __syncthreads();
+        if (threadIdx.x == 0)
+        {
+            int nw = blockDim.x >> 5;
+            for (int w = 1; w < nw; ++w)
+            {
+                v0 = min(v0, sb[0][w]);
+                v1 = min(v1, sb[1][w]);
+                v2 = max(v2, sb[2][w]);
+                v3 = max(v3, sb[3][w]);
+                v4 += sb[4][w];
+            }
+            if (v2 >= 0)
+            {
+                atomicMin(bbox + 0, v0);
+                atomicMin(bbox + 1, v1);
+                atomicMax(bbox + 2, v2);
+                atomicMax(bbox + 3, v3);
+                atomicAdd(bbox + 4, v4);
+            }
+        }
+    }
+};
 
 __global__ void __launch_bounds__(256) k_coverage(BlendArgs a, const Unit* __restrict__ units)
 {
-    Unit u = units[blockIdx.x];
+    const Unit u = units[blockIdx.x];
     const ItemDev& it = a.items[u.id];
     const TileDev& T = a.tiles[it.tile];
-    int x = u.bx * 32 + (threadIdx.x & 31);
-    int y = u.by * 8 + (threadIdx.x >> 5);
-    bool covered = false;
-    if (x < T.w && y < T.h)
+    const int W = T.w, H = T.h, lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    BoxAcc box;
+    for (int r = 0; r < kBandRows / 8; ++r)
     {
-        const unsigned short* p = it.img + ((size_t)y * T.w + x) * 3;
-        covered = (p[0] | p[1] | p[2]) != 0;
+        const int y = u.by * kBandRows + warp * (kBandRows / 8) + r;
+        if (y >= H) break;
+        for (int x0 = 0; x0 < W; x0 += 32)
+        {
+            const int x = x0 + lane;
+            bool covered = false;
+            if (x < W)
+            {
+                const unsigned short* p = it.img + ((size_t)y * W + x) * 3;
+                covered = (p[0] | p[1] | p[2]) != 0;
+            }
+            unsigned m = __ballot_sync(kFull, covered);
+            if (lane == 0) it.cov[(size_t)y * T.covWords + (x0 >> 5)] = m;
+            box.add(covered, x, y);
+        }
     }
-    emit_coverage(it, T, x, y, covered);
+    box.flush(it.bbox);
 }
 
 // ---------------------------------------------------------------------------
-// Tile warp: WarpPerspective + ApplyGain for one contributor into its tile
-// buffer (RenderExecutor.cpp:104-114), with coverage emitted in the same pass.
-// Arithmetic identical to k_warp in pixel_ops.cu.
+// Tile warp: WarpPerspective + ApplyGain of one contributor into its tile
+// buffer (RenderExecutor.cpp:104-114), coverage and box emitted in the same
+// pass.  Arithmetic identical to k_warp in pixel_ops.cu.
 // ---------------------------------------------------------------------------
+__device__ __forceinline__ void warp_px(const ItemDev& it, float dX, float dY, unsigned short o[3])
+{
+    const float* H = it.H;
+    float sx = fadd(fadd(fmul(H[0], dX), fmul(H[1], dY)), H[2]);
+    float sy = fadd(fadd(fmul(H[3], dX), fmul(H[4], dY)), H[5]);
+    float sw1 = fadd(fadd(fmul(H[6], dX), fmul(H[7], dY)), H[8]);
+    o[0] = o[1] = o[2] = 0;
+    if (fabsf(sw1) < 1e-10f) return;
+    sx = fdiv(sx, sw1);
+    sy = fdiv(sy, sw1);
+    if (!(sx >= 0.0f && sx < (float)(it.srcW - 1) && sy >= 0.0f && sy < (float)(it.srcH - 1))) return;
+    int x0 = (int)floorf(sx), y0 = (int)floorf(sy);
+    float fx = fsub(sx, (float)x0), fy = fsub(sy, (float)y0);
+    float gx = fsub(1.0f, fx), gy = fsub(1.0f, fy);
+    float w00 = fmul(gx, gy), w10 = fmul(fx, gy), w01 = fmul(gx, fy), w11 = fmul(fx, fy);
+    const unsigned short* r0 = it.src + ((size_t)y0 * it.srcW + x0) * 3;
+    const unsigned short* r1 = r0 + (size_t)it.srcW * 3;
+    unsigned short a0 = __ldg(r0), a1 = __ldg(r0 + 1), a2 = __ldg(r0 + 2), a3 = __ldg(r0 + 3), a4 = __ldg(r0 + 4),
+                   a5 = __ldg(r0 + 5);
+    unsigned short b0 = __ldg(r1), b1 = __ldg(r1 + 1), b2 = __ldg(r1 + 2), b3 = __ldg(r1 + 3), b4 = __ldg(r1 + 4),
+                   b5 = __ldg(r1 + 5);
+    const unsigned short t00[3] = {a0, a1, a2}, t10[3] = {a3, a4, a5}, t01[3] = {b0, b1, b2}, t11[3] = {b3, b4, b5};
+    const bool applyGain = !gain_is_identity(it.gain);
+#pragma unroll
+    for (int c = 0; c < 3; ++c)
+    {
+        float v = fadd(fadd(fadd(fmul(w00, (float)t00[c]), fmul(w10, (float)t10[c])), fmul(w01, (float)t01[c])),
+                       fmul(w11, (float)t11[c]));
+        unsigned short q = clamp_trunc_u16(v);
+        if (applyGain) q = clamp_trunc_u16(fmul((float)q, it.gain));
+        o[c] = q;
+    }
+}
+
 __global__ void __launch_bounds__(256) k_warp_tiles(BlendArgs a, const Unit* __restrict__ units)
 {
-    Unit u = units[blockIdx.x];
+    const Unit u = units[blockIdx.x];
     const ItemDev& it = a.items[u.id];
     const TileDev& T = a.tiles[it.tile];
-    int x = u.bx * 32 + (threadIdx.x & 31);
-    int y = u.by * 8 + (threadIdx.x >> 5);
-    bool covered = false;
-    if (x < T.w && y < T.h)
+    const int W = T.w, H = T.h, lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    unsigned short* img = const_cast<unsigned short*>(it.img);
+    BoxAcc box;
+    for (int r = 0; r < kBandRows / 8; ++r)
     {
-        float dX = (float)(x + it.offX), dY = (float)(y + it.offY);
-        const float* H = it.H;
-        float sx = fadd(fadd(fmul(H[0], dX), fmul(H[1], dY)), H[2]);
-        float sy = fadd(fadd(fmul(H[3], dX), fmul(H[4], dY)), H[5]);
-        float sw1 = fadd(fadd(fmul(H[6], dX), fmul(H[7], dY)), H[8]);
-        unsigned short o[3] = {0, 0, 0};
-        if (!(fabsf(sw1) < 1e-10f))
+        const int y = u.by * kBandRows + warp * (kBandRows / 8) + r;
+        if (y >= H) break;
+        const float dY = (float)(y + it.offY);
+        for (int x0 = 0; x0 < W; x0 += 64)
         {
-            sx = fdiv(sx, sw1);
-            sy = fdiv(sy, sw1);
-            if (sx >= 0.0f && sx < (float)(it.srcW - 1) && sy >= 0.0f && sy < (float)(it.srcH - 1))
+            // Two independent pixels per lane keep more gathers in flight.
+            const int xa = x0 + lane, xb = x0 + 32 + lane;
+            unsigned short oa[3] = {0, 0, 0}, ob[3] = {0, 0, 0};
+            if (xa < W) warp_px(it, (float)(xa + it.offX), dY, oa);
+            if (xb < W) warp_px(it, (float)(xb + it.offX), dY, ob);
+            bool ca = (oa[0] | oa[1] | oa[2]) != 0, cb = (ob[0] | ob[1] | ob[2]) != 0;
+            if (xa < W)
             {
-                int x0 = (int)floorf(sx), y0 = (int)floorf(sy);
-                float fx = fsub(sx, (float)x0), fy = fsub(sy, (float)y0);
-                float gx = fsub(1.0f, fx), gy = fsub(1.0f, fy);
-                float w00 = fmul(gx, gy), w10 = fmul(fx, gy), w01 = fmul(gx, fy), w11 = fmul(fx, fy);
-                const unsigned short* r0 = it.src + ((size_t)y0 * it.srcW + x0) * 3;
-                const unsigned short* r1 = r0 + (size_t)it.srcW * 3;
-                bool applyGain = !gain_is_identity(it.gain);
-#pragma unroll
-                for (int c = 0; c < 3; ++c)
-                {
-                    float v = fadd(fadd(fadd(fmul(w00, (float)__ldg(r0 + c)), fmul(w10, (float)__ldg(r0 + 3 + c))),
-                                        fmul(w01, (float)__ldg(r1 + c))),
-                                   fmul(w11, (float)__ldg(r1 + 3 + c)));
-                    unsigned short q = clamp_trunc_u16(v);
-                    if (applyGain) q = clamp_trunc_u16(fmul((float)q, it.gain));
-                    o[c] = q;
-                }
+                unsigned short* d = img + ((size_t)y * W + xa) * 3;
+                d[0] = oa[0];
+                d[1] = oa[1];
+                d[2] = oa[2];
             }
+            if (xb < W)
+            {
+                unsigned short* d = img + ((size_t)y * W + xb) * 3;
+                d[0] = ob[0];
+                d[1] = ob[1];
+                d[2] = ob[2];
+            }
+            unsigned ma = __ballot_sync(kFull, ca), mb = __ballot_sync(kFull, cb);
+            if (lane == 0)
+            {
+                it.cov[(size_t)y * T.covWords + (x0 >> 5)] = ma;
+                if (x0 + 32 < W) it.cov[(size_t)y * T.covWords + (x0 >> 5) + 1] = mb;
+            }
+            box.add(ca, xa, y);
+            box.add(cb, xb, y);
         }
-        unsigned short* d = const_cast<unsigned short*>(it.img) + ((size_t)y * T.w + x) * 3;
-        d[0] = o[0];
-        d[1] = o[1];
-        d[2] = o[2];
-        covered = (o[0] | o[1] | o[2]) != 0;
     }
-    emit_coverage(it, T, x, y, covered);
+    box.flush(it.bbox);
 }
 
 // ---------------------------------------------------------------------------
@@ -144,6 +224,14 @@ __device__ __forceinline__ int ring_idx(int x) { return x + (x >> 3); }  // 1 pa
 // into the next binade rounds; each crossing is one rounded add.
 __device__ __forceinline__ float add_ones(float v, int n)
 {
+    if (n <= 0) return v;
+    if (v >= 1.0f && v < 16777216.0f)
+    {
+        // Common case: v + n stays below the next power of two, so the n
+        // steps are exact and equal one add.
+        float B = __int_as_float((__float_as_int(v) & 0x7f800000) + 0x00800000);
+        if (fsub(B, v) > (float)n) return fadd(v, (float)n);
+    }
     while (n > 0)
     {
         if (!(v < 16777216.0f)) return v;  // +inf (or beyond the distances that occur)
@@ -168,6 +256,13 @@ __global__ void __launch_bounds__(512) k_dt(BlendArgs a, const int* __restrict__
     const ItemDev& it = a.items[itemList[blockIdx.x]];
     const TileDev& T = a.tiles[it.tile];
     const int W = T.w, H = T.h, covWords = T.covWords;
+    // A contributor that covers none or all of its tile has d == 0 or
+    // d == kInf everywhere (no seed / nothing to seed); the ownership kernel
+    // substitutes those values, so the transform is skipped.
+    {
+        const int cnt = it.bbox[4];
+        if (cnt == 0 || (long long)cnt == (long long)W * H) return;
+    }
     const int RS = dt_ring_stride(W);
     float* ring = smem;
     int* prog = reinterpret_cast<int*>(smem + (size_t)nw * RS);
@@ -190,6 +285,37 @@ __global__ void __launch_bounds__(512) k_dt(BlendArgs a, const int* __restrict__
         for (int x0 = -skew; x0 < W; x0 += kDtCW)
         {
             const int x1 = min(x0 + kDtCW, W);
+            const int xb = x0 + lane * kDtE;
+            // Initial values do not depend on the row above: load them before
+            // waiting so the global latency overlaps the wait.
+            float iv[kDtE];
+            if (BACK)
+            {
+#pragma unroll
+                for (int k = 0; k < kDtE; ++k)
+                {
+                    int x = xb + k;
+                    iv[k] = (x >= 0 && x < W) ? __ldg(d1 + (size_t)ry * W + (W - 1 - x)) : INF;
+                }
+            }
+            else
+            {
+                int xs = max(xb, 0), xe = min(xb + kDtE - 1, W - 1);
+                uint32_t w0 = 0, w1 = 0;
+                if (xs <= xe)
+                {
+                    w0 = __ldg(cov + (size_t)ry * covWords + (xs >> 5));
+                    w1 = __ldg(cov + (size_t)ry * covWords + (xe >> 5));
+                }
+#pragma unroll
+                for (int k = 0; k < kDtE; ++k)
+                {
+                    int x = xb + k;
+                    bool c = false;
+                    if (x >= 0 && x < W) c = (((x >> 5) == (xs >> 5) ? w0 : w1) >> (x & 31)) & 1u;
+                    iv[k] = (x >= 0 && x < W) ? (c ? kInf : 0.0f) : INF;
+                }
+            }
             if (vy > 0)
             {
                 const int target = (vy - 1) * (W + 1) + min(x1 + 1, W);
@@ -201,7 +327,10 @@ __global__ void __launch_bounds__(512) k_dt(BlendArgs a, const int* __restrict__
                     int spins = 0;
                     while (pr.load(cuda::memory_order_acquire) < target)
                     {
-                        if ((++spins & 1023) == 0)
+                        // Back off so waiting warps leave the issue slots to
+                        // the warps computing the rows they wait for.
+                        __nanosleep(64);
+                        if ((++spins & 255) == 0)
                         {
                             if (*(volatile int*)a.error || clock64() - t0 > kSpinCycles)
                             {
@@ -215,7 +344,6 @@ __global__ void __launch_bounds__(512) k_dt(BlendArgs a, const int* __restrict__
                 ok = __shfl_sync(kFull, ok, 0);
                 if (!ok) return;
             }
-            const int xb = x0 + lane * kDtE;
             float pv[kDtE + 2];
 #pragma unroll
             for (int k = 0; k < kDtE + 2; ++k)
@@ -229,18 +357,12 @@ __global__ void __launch_bounds__(512) k_dt(BlendArgs a, const int* __restrict__
             for (int k = 0; k < kDtE; ++k)
             {
                 int x = xb + k;
-                float av = INF;
-                if (x >= 0 && x < W)
+                float av = iv[k];
+                if (vy > 0 && x >= 0 && x < W)
                 {
-                    int rx = BACK ? W - 1 - x : x;
-                    if (BACK) av = __ldg(d1 + (size_t)ry * W + rx);
-                    else av = cov_bit(cov, covWords, rx, ry) ? kInf : 0.0f;
-                    if (vy > 0)
-                    {
-                        av = fminf(av, fadd(pv[k + 1], 1.0f));
-                        if (x > 0) av = fminf(av, fadd(pv[k], kDiag));
-                        if (x < W - 1) av = fminf(av, fadd(pv[k + 2], kDiag));
-                    }
+                    av = fminf(av, fadd(pv[k + 1], 1.0f));
+                    if (x > 0) av = fminf(av, fadd(pv[k], kDiag));
+                    if (x < W - 1) av = fminf(av, fadd(pv[k + 2], kDiag));
                 }
                 l[k] = fminf(av, fadd(prev, 1.0f));
                 prev = l[k];
@@ -285,19 +407,22 @@ __global__ void __launch_bounds__(512) k_dt(BlendArgs a, const int* __restrict__
 // ---------------------------------------------------------------------------
 __global__ void __launch_bounds__(256) k_owner(BlendArgs a, const Unit* __restrict__ units)
 {
-    Unit u = units[blockIdx.x];
+    const Unit u = units[blockIdx.x];
     const TileDev& T = a.tiles[u.id];
-    long long n = (long long)T.w * T.h;
-    long long p = (long long)u.bx * 1024 + threadIdx.x;
-#pragma unroll
-    for (int j = 0; j < 4; ++j, p += 256)
+    const long long base = (long long)u.by * kBandRows * T.w;
+    const long long n = min((long long)kBandRows * T.w, (long long)T.w * T.h - base);
+    for (long long q = threadIdx.x; q < n; q += blockDim.x)
     {
-        if (p >= n) break;
+        const long long p = base + q;
         int best = -1;
         float bestD = 0.0f;
+        const long long full = (long long)T.w * T.h;
+        const float kInf = (float)(T.w + T.h);
         for (int k = 0; k < T.numItems; ++k)
         {
-            float v = __ldg(a.items[T.firstItem + k].d + p);
+            const ItemDev& it = a.items[T.firstItem + k];
+            const int cnt = it.bbox[4];
+            float v = cnt == 0 ? 0.0f : ((long long)cnt == full ? kInf : __ldg(it.d + p));
             if (v > bestD)
             {
                 bestD = v;
@@ -359,75 +484,128 @@ __global__ void __launch_bounds__(256) k_seam(BlendArgs a, const int* __restrict
                 y = rowScan ? oy0 + line : oy0 + t;
             };
 
-            // Phase 1: crossover and contested band per line.
-            for (int line = warp; line < numLines; line += 8)
+            // Phase 1: crossover and contested band per line
+            // (SeamBlend.cpp:325-360).  Row scans: a warp walks one line with
+            // ballots.  Column scans: each lane walks one column, so a warp's
+            // owner loads are 32 consecutive bytes of one row.
+            auto band_of = [&](int line, int cross, int& lo, int& hi) {
+                lo = 1;
+                hi = 0;
+                if (cross < 0) return;
+                int bLo = max(0, cross - kSeamRadius), bHi = min(lineLen - 1, cross + kSeamRadius);
+                for (int t = bLo; t <= bHi; ++t)
+                {
+                    int x, y;
+                    pxy(line, t, x, y);
+                    if (cov_bit(I.cov, T.covWords, x, y) && cov_bit(J.cov, T.covWords, x, y))
+                    {
+                        if (hi < lo) lo = t;
+                        hi = t;
+                    }
+                }
+            };
+            if (rowScan)
             {
-                int first = -1000, cross = -1;
-                for (int t0 = 0; t0 < lineLen && cross < 0; t0 += 32)
+                for (int line = warp; line < numLines; line += 8)
                 {
-                    int t = t0 + lane;
-                    int o = -2;
-                    bool isIJ = false;
-                    if (t < lineLen)
+                    int first = -1000, cross = -1;
+                    for (int t0 = 0; t0 < lineLen && cross < 0; t0 += 32)
                     {
-                        o = T.owner[pix(line, t)];
-                        isIJ = (o == ci || o == cj);
+                        int t = t0 + lane;
+                        int o = -2;
+                        bool isIJ = false;
+                        if (t < lineLen)
+                        {
+                            o = T.owner[pix(line, t)];
+                            isIJ = (o == ci || o == cj);
+                        }
+                        unsigned m = __ballot_sync(kFull, isIJ);
+                        if (!m) continue;
+                        if (first == -1000)
+                        {
+                            int fl = __ffs(m) - 1;
+                            first = __shfl_sync(kFull, o, fl);
+                            unsigned md = __ballot_sync(kFull, isIJ && o != first);
+                            md &= (fl == 31) ? 0u : ~((2u << fl) - 1u);
+                            if (md) cross = t0 + __ffs(md) - 1;
+                        }
+                        else
+                        {
+                            unsigned md = __ballot_sync(kFull, isIJ && o != first);
+                            if (md) cross = t0 + __ffs(md) - 1;
+                        }
                     }
-                    unsigned m = __ballot_sync(kFull, isIJ);
-                    if (!m) continue;
-                    if (first == -1000)
+                    // band: lanes test the <= 49 candidates, two rounds
+                    int lo = 1, hi = 0;
+                    if (cross >= 0)
                     {
-                        int fl = __ffs(m) - 1;
-                        first = __shfl_sync(kFull, o, fl);
-                        unsigned md = __ballot_sync(kFull, isIJ && o != first);
-                        md &= (fl == 31) ? 0u : ~((2u << fl) - 1u);
-                        if (md) cross = t0 + __ffs(md) - 1;
+                        int bLo = max(0, cross - kSeamRadius);
+                        int bHi = min(lineLen - 1, cross + kSeamRadius);
+                        bool both0 = false, both1 = false;
+                        int t = bLo + lane;
+                        if (t <= bHi)
+                        {
+                            int x, y;
+                            pxy(line, t, x, y);
+                            both0 = cov_bit(I.cov, T.covWords, x, y) && cov_bit(J.cov, T.covWords, x, y);
+                        }
+                        t = bLo + 32 + lane;
+                        if (t <= bHi)
+                        {
+                            int x, y;
+                            pxy(line, t, x, y);
+                            both1 = cov_bit(I.cov, T.covWords, x, y) && cov_bit(J.cov, T.covWords, x, y);
+                        }
+                        unsigned m0 = __ballot_sync(kFull, both0), m1 = __ballot_sync(kFull, both1);
+                        if (m0 | m1)
+                        {
+                            lo = bLo + (m0 ? __ffs(m0) - 1 : 32 + __ffs(m1) - 1);
+                            hi = bLo + (m1 ? 32 + 31 - __clz(m1) : 31 - __clz(m0));
+                        }
                     }
-                    else
+                    if (lane == 0)
                     {
-                        unsigned md = __ballot_sync(kFull, isIJ && o != first);
-                        if (md) cross = t0 + __ffs(md) - 1;
+                        sLo[line] = lo;
+                        sHi[line] = hi;
                     }
                 }
-                int lo = 1, hi = 0;
-                if (cross >= 0)
+            }
+            else
+            {
+                for (int line = tid; line < numLines; line += 256)
                 {
-                    int bLo = max(0, cross - kSeamRadius);
-                    int bHi = min(lineLen - 1, cross + kSeamRadius);
-                    bool both0 = false, both1 = false;
-                    int t = bLo + lane;
-                    if (t <= bHi)
+                    int first = -1000, cross = -1;
+                    for (int t = 0; t < lineLen; ++t)
                     {
-                        int x, y;
-                        pxy(line, t, x, y);
-                        both0 = cov_bit(I.cov, T.covWords, x, y) && cov_bit(J.cov, T.covWords, x, y);
+                        int o = T.owner[pix(line, t)];
+                        if (o != ci && o != cj) continue;
+                        if (first == -1000)
+                        {
+                            first = o;
+                            continue;
+                        }
+                        if (o != first)
+                        {
+                            cross = t;
+                            break;
+                        }
                     }
-                    t = bLo + 32 + lane;
-                    if (t <= bHi)
-                    {
-                        int x, y;
-                        pxy(line, t, x, y);
-                        both1 = cov_bit(I.cov, T.covWords, x, y) && cov_bit(J.cov, T.covWords, x, y);
-                    }
-                    unsigned m0 = __ballot_sync(kFull, both0), m1 = __ballot_sync(kFull, both1);
-                    if (m0 | m1)
-                    {
-                        lo = bLo + (m0 ? __ffs(m0) - 1 : 32 + __ffs(m1) - 1);
-                        hi = bLo + (m1 ? 32 + 31 - __clz(m1) : 31 - __clz(m0));
-                    }
-                }
-                if (lane == 0)
-                {
+                    int lo, hi;
+                    band_of(line, cross, lo, hi);
                     sLo[line] = lo;
                     sHi[line] = hi;
                 }
             }
             __syncthreads();
 
-            // Phase 2: per-pixel colour cost of every contested candidate.
+            // Phase 2: per-pixel colour cost of every contested candidate
+            // (SeamBlend.cpp:382-383), indexed so consecutive threads touch
+            // neighbouring pixels for either scan direction.
             for (int idx = tid; idx < numLines * kSeamBand; idx += 256)
             {
-                int line = idx / kSeamBand, k = idx - line * kSeamBand;
+                int line, k;
+                if (rowScan) { line = idx / kSeamBand; k = idx - line * kSeamBand; }
+                else { k = idx / numLines; line = idx - k * numLines; }
                 if (k == 0) T.chosen[line] = -1;
                 int lo = sLo[line], hi = sHi[line];
                 if (k > hi - lo) continue;
@@ -441,41 +619,85 @@ __global__ void __launch_bounds__(256) k_seam(BlendArgs a, const int* __restrict
             }
             __syncthreads();
 
-            // Phase 3: dynamic program over contested lines (one warp).
+            // Phase 3: dynamic program over contested lines (SeamBlend.cpp:362-407),
+            // one warp.  The next contested line's costs are loaded before the
+            // current line's minimisation; each candidate's argmin over the
+            // previous line runs as four interleaved chains merged with the
+            // lowest-index tie rule of the strict '<' scan.
             if (warp == 0)
             {
-                int last = -1, cur = 0, lastW = 0;
-                for (int line = 0; line < numLines; ++line)
-                {
-                    int lo = sLo[line], hi = sHi[line];
-                    if (hi < lo)
+                auto next_contested = [&](int from) {
+                    int l = from;
+                    while (l < numLines && sHi[l] < sLo[l])
                     {
-                        if (lane == 0) sPrev[line] = -1;
-                        continue;
+                        if (lane == 0) sPrev[l] = -1;
+                        ++l;
                     }
-                    int lw = hi - lo + 1;
-                    int plo = last >= 0 ? sLo[last] : 0;
-                    int pw = lastW;
-                    for (int k = lane; k < lw; k += 32)
+                    return l;
+                };
+                int last = -1, cur = 0, lastW = 0;
+                int line = next_contested(0);
+                float c0 = 0.0f, c1 = 0.0f;
+                if (line < numLines)
+                {
+                    if (lane < sHi[line] - sLo[line] + 1) c0 = T.cost[(size_t)line * kSeamBand + lane];
+                    if (lane + 32 < sHi[line] - sLo[line] + 1) c1 = T.cost[(size_t)line * kSeamBand + lane + 32];
+                }
+                while (line < numLines)
+                {
+                    const int lo = sLo[line], lw = sHi[line] - lo + 1;
+                    const int nxt = next_contested(line + 1);
+                    float n0 = 0.0f, n1 = 0.0f;
+                    if (nxt < numLines)
                     {
-                        float c = T.cost[(size_t)line * kSeamBand + k];
-                        int t = lo + k;
+                        int nw2 = sHi[nxt] - sLo[nxt] + 1;
+                        if (lane < nw2) n0 = T.cost[(size_t)nxt * kSeamBand + lane];
+                        if (lane + 32 < nw2) n1 = T.cost[(size_t)nxt * kSeamBand + lane + 32];
+                    }
+                    const int plo = last >= 0 ? sLo[last] : 0;
+#pragma unroll
+                    for (int half = 0; half < 2; ++half)
+                    {
+                        const int k = lane + 32 * half;
+                        if (k >= lw) continue;
+                        const float c = half ? c1 : c0;
+                        const int t = lo + k;
                         float val;
                         int bp = -1;
                         if (last < 0) val = c;
                         else
                         {
-                            float best = FLT_MAX;
-                            for (int pk = 0; pk < pw; ++pk)
+                            float best[4] = {FLT_MAX, FLT_MAX, FLT_MAX, FLT_MAX};
+                            int bi[4] = {-1, -1, -1, -1};
+                            for (int pk = 0; pk < lastW; pk += 4)
                             {
-                                float c2 = fadd(dpBuf[cur ^ 1][pk], fmul(kSeamSmooth, fabsf((float)(t - (plo + pk)))));
-                                if (c2 < best)
+#pragma unroll
+                                for (int q = 0; q < 4; ++q)
                                 {
-                                    best = c2;
-                                    bp = pk;
+                                    int kk = pk + q;
+                                    if (kk < lastW)
+                                    {
+                                        float c2 = fadd(dpBuf[cur ^ 1][kk],
+                                                        fmul(kSeamSmooth, fabsf((float)(t - (plo + kk)))));
+                                        if (c2 < best[q])
+                                        {
+                                            best[q] = c2;
+                                            bi[q] = kk;
+                                        }
+                                    }
                                 }
                             }
-                            val = fadd(c, best);
+                            // Merge: smaller value wins, equal values keep the lower index.
+                            float b = best[0];
+                            bp = bi[0];
+#pragma unroll
+                            for (int q = 1; q < 4; ++q)
+                                if (bi[q] >= 0 && (best[q] < b || (best[q] == b && (bp < 0 || bi[q] < bp))))
+                                {
+                                    b = best[q];
+                                    bp = bi[q];
+                                }
+                            val = fadd(c, b);
                         }
                         dpBuf[cur][k] = val;
                         sBack[(size_t)line * kSeamBand + k] = (unsigned char)(bp < 0 ? 255 : bp);
@@ -484,6 +706,9 @@ __global__ void __launch_bounds__(256) k_seam(BlendArgs a, const int* __restrict
                     last = line;
                     lastW = lw;
                     cur ^= 1;
+                    c0 = n0;
+                    c1 = n1;
+                    line = nxt;
                     __syncwarp();
                 }
                 if (lane == 0)
@@ -525,7 +750,9 @@ __global__ void __launch_bounds__(256) k_seam(BlendArgs a, const int* __restrict
             {
                 for (int idx = tid; idx < numLines * kSeamBand; idx += 256)
                 {
-                    int line = idx / kSeamBand, k = idx - line * kSeamBand;
+                    int line, k;
+                    if (rowScan) { line = idx / kSeamBand; k = idx - line * kSeamBand; }
+                    else { k = idx / numLines; line = idx - k * numLines; }
                     int ch = T.chosen[line];
                     if (ch < 0) continue;
                     int lo = sLo[line], hi = sHi[line];
@@ -593,14 +820,15 @@ __device__ __forceinline__ float3 gauss_of(float4 nd)
 // Blur + decimate one level (SeamBlend.cpp:60-79) for num(3), den and weight
 // together.  A CTA makes a 32x8 block of level l+1 from a 68x20 footprint of
 // level l staged in shared memory with replicated borders.
-constexpr int kDnTW = 32, kDnTH = 8;
+constexpr int kDnTW = 32, kDnTH = 16;
 constexpr int kDnSW = 2 * kDnTW + 4, kDnSH = 2 * kDnTH + 4;
 
 template <bool L0>
 __global__ void __launch_bounds__(256) k_down(BlendArgs a, const Unit* __restrict__ units, int level)
 {
-    __shared__ float s[5][kDnSH][kDnSW];
-    __shared__ float t[5][kDnSH][kDnTW];
+    extern __shared__ float dn_smem[];
+    auto s = reinterpret_cast<float (*)[kDnSH][kDnSW]>(dn_smem);
+    auto t = reinterpret_cast<float (*)[kDnSH][kDnTW]>(dn_smem + 5 * kDnSH * kDnSW);
     Unit u = units[blockIdx.x];
     const ItemDev& it = a.items[u.id];
     const TileDev& T = a.tiles[it.tile];
@@ -648,16 +876,20 @@ __global__ void __launch_bounds__(256) k_down(BlendArgs a, const Unit* __restric
         t[ch][r][i] = blur5(row[2 * i], row[2 * i + 1], row[2 * i + 2], row[2 * i + 3], row[2 * i + 4]);
     }
     __syncthreads();
-    int i = tid & 31, j = tid >> 5;
-    int X = X0 + i, Y = Y0 + j;
-    if (X >= dw || Y >= dh) return;
-    float o[5];
+    const int i = tid & 31;
+    for (int j = tid >> 5; j < kDnTH; j += 8)
+    {
+        int X = X0 + i, Y = Y0 + j;
+        if (X >= dw || Y >= dh) continue;
+        float o[5];
 #pragma unroll
-    for (int ch = 0; ch < 5; ++ch)
-        o[ch] = blur5(t[ch][2 * j][i], t[ch][2 * j + 1][i], t[ch][2 * j + 2][i], t[ch][2 * j + 3][i], t[ch][2 * j + 4][i]);
-    size_t q = T.loff[level + 1] + (size_t)Y * dw + X;
-    it.nd[q] = make_float4(o[0], o[1], o[2], o[3]);
-    it.wg[q] = o[4];
+        for (int ch = 0; ch < 5; ++ch)
+            o[ch] = blur5(t[ch][2 * j][i], t[ch][2 * j + 1][i], t[ch][2 * j + 2][i], t[ch][2 * j + 3][i],
+                          t[ch][2 * j + 4][i]);
+        size_t q = T.loff[level + 1] + (size_t)Y * dw + X;
+        it.nd[q] = make_float4(o[0], o[1], o[2], o[3]);
+        it.wg[q] = o[4];
+    }
 }
 
 // Blended band of one level: sum over the tile's contributors, in index
@@ -667,62 +899,73 @@ __global__ void __launch_bounds__(256) k_down(BlendArgs a, const Unit* __restric
 // exactly +-0, so summing every contributor equals the reference's sum.
 __global__ void __launch_bounds__(256) k_blend_level(BlendArgs a, const Unit* __restrict__ units, int level)
 {
-    Unit u = units[blockIdx.x];
+    const Unit u = units[blockIdx.x];
     const TileDev& T = a.tiles[u.id];
-    int x = u.bx * 32 + (threadIdx.x & 31), y = u.by * 8 + (threadIdx.x >> 5);
     const int lw = T.lw[level], lh = T.lh[level];
-    if (x >= lw || y >= lh) return;
     const bool top = level == T.bands - 1;
-    UpCoef c;
-    if (!top) c = up_coef(T.lw[level + 1], T.lh[level + 1], lw, lh, x, y);
-    const size_t p = T.loff[level] + (size_t)y * lw + x;
-    float acc0 = 0.0f, acc1 = 0.0f, acc2 = 0.0f;
-    for (int k = 0; k < T.numItems; ++k)
+    const int uw = T.lw[level + 1], uh = T.lh[level + 1];
+    const long long base = (long long)u.by * kBandRows * lw;
+    const long long n = min((long long)kBandRows * lw, (long long)lw * lh - base);
+    for (long long q = threadIdx.x; q < n; q += blockDim.x)
     {
-        const ItemDev& it = a.items[T.firstItem + k];
-        float wv = __ldg(it.wg + p);
-        float3 g = gauss_of(it.nd[p]);
-        if (!top)
+        const long long pl = base + q;
+        const int y = (int)(pl / lw), x = (int)(pl - (long long)y * lw);
+        UpCoef c;
+        if (!top) c = up_coef(uw, uh, lw, lh, x, y);
+        const size_t p = T.loff[level] + pl;
+        float acc0 = 0.0f, acc1 = 0.0f, acc2 = 0.0f;
+        for (int k = 0; k < T.numItems; ++k)
         {
-            const float4* up = it.nd + T.loff[level + 1];
-            const int uw = T.lw[level + 1];
-            float3 a00 = gauss_of(up[(size_t)c.y0 * uw + c.x0]);
-            float3 a10 = gauss_of(up[(size_t)c.y0 * uw + c.x1]);
-            float3 a01 = gauss_of(up[(size_t)c.y1 * uw + c.x0]);
-            float3 a11 = gauss_of(up[(size_t)c.y1 * uw + c.x1]);
-            g.x = fsub(g.x, up_mix(a00.x, a10.x, a01.x, a11.x, c.wx, c.wy));
-            g.y = fsub(g.y, up_mix(a00.y, a10.y, a01.y, a11.y, c.wx, c.wy));
-            g.z = fsub(g.z, up_mix(a00.z, a10.z, a01.z, a11.z, c.wx, c.wy));
+            const ItemDev& it = a.items[T.firstItem + k];
+            float wv = __ldg(it.wg + p);
+            float3 g = gauss_of(it.nd[p]);
+            if (!top)
+            {
+                const float4* up = it.nd + T.loff[level + 1];
+                float3 a00 = gauss_of(up[(size_t)c.y0 * uw + c.x0]);
+                float3 a10 = gauss_of(up[(size_t)c.y0 * uw + c.x1]);
+                float3 a01 = gauss_of(up[(size_t)c.y1 * uw + c.x0]);
+                float3 a11 = gauss_of(up[(size_t)c.y1 * uw + c.x1]);
+                g.x = fsub(g.x, up_mix(a00.x, a10.x, a01.x, a11.x, c.wx, c.wy));
+                g.y = fsub(g.y, up_mix(a00.y, a10.y, a01.y, a11.y, c.wx, c.wy));
+                g.z = fsub(g.z, up_mix(a00.z, a10.z, a01.z, a11.z, c.wx, c.wy));
+            }
+            acc0 = fadd(acc0, fmul(wv, g.x));
+            acc1 = fadd(acc1, fmul(wv, g.y));
+            acc2 = fadd(acc2, fmul(wv, g.z));
         }
-        acc0 = fadd(acc0, fmul(wv, g.x));
-        acc1 = fadd(acc1, fmul(wv, g.y));
-        acc2 = fadd(acc2, fmul(wv, g.z));
+        float* b = T.blend + p * 3;
+        b[0] = acc0;
+        b[1] = acc1;
+        b[2] = acc2;
     }
-    float* b = T.blend + p * 3;
-    b[0] = acc0;
-    b[1] = acc1;
-    b[2] = acc2;
 }
 
 // Collapse one level in place: recon_l = blended_l + Up(recon_l+1)
 // (SeamBlend.cpp:514-525).
 __global__ void __launch_bounds__(256) k_collapse(BlendArgs a, const Unit* __restrict__ units, int level)
 {
-    Unit u = units[blockIdx.x];
+    const Unit u = units[blockIdx.x];
     const TileDev& T = a.tiles[u.id];
-    int x = u.bx * 32 + (threadIdx.x & 31), y = u.by * 8 + (threadIdx.x >> 5);
     const int lw = T.lw[level], lh = T.lh[level];
-    if (x >= lw || y >= lh) return;
-    const int uw = T.lw[level + 1];
-    UpCoef c = up_coef(uw, T.lh[level + 1], lw, lh, x, y);
+    const int uw = T.lw[level + 1], uh = T.lh[level + 1];
     const float* r = T.blend + T.loff[level + 1] * 3;
-    float* b = T.blend + (T.loff[level] + (size_t)y * lw + x) * 3;
-#pragma unroll
-    for (int ch = 0; ch < 3; ++ch)
+    const long long base = (long long)u.by * kBandRows * lw;
+    const long long n = min((long long)kBandRows * lw, (long long)lw * lh - base);
+    for (long long q = threadIdx.x; q < n; q += blockDim.x)
     {
-        float v = up_mix(r[((size_t)c.y0 * uw + c.x0) * 3 + ch], r[((size_t)c.y0 * uw + c.x1) * 3 + ch],
-                         r[((size_t)c.y1 * uw + c.x0) * 3 + ch], r[((size_t)c.y1 * uw + c.x1) * 3 + ch], c.wx, c.wy);
-        b[ch] = fadd(b[ch], v);
+        const long long pl = base + q;
+        const int y = (int)(pl / lw), x = (int)(pl - (long long)y * lw);
+        UpCoef c = up_coef(uw, uh, lw, lh, x, y);
+        float* b = T.blend + (T.loff[level] + pl) * 3;
+#pragma unroll
+        for (int ch = 0; ch < 3; ++ch)
+        {
+            float v = up_mix(r[((size_t)c.y0 * uw + c.x0) * 3 + ch], r[((size_t)c.y0 * uw + c.x1) * 3 + ch],
+                             r[((size_t)c.y1 * uw + c.x0) * 3 + ch], r[((size_t)c.y1 * uw + c.x1) * 3 + ch], c.wx,
+                             c.wy);
+            b[ch] = fadd(b[ch], v);
+        }
     }
 }
 
@@ -732,50 +975,55 @@ __global__ void __launch_bounds__(256) k_collapse(BlendArgs a, const Unit* __res
 // clamp(that + Up(recon_1)) + 0.5 truncated, and 0 where nobody owns.
 __global__ void __launch_bounds__(256) k_final0(BlendArgs a, const Unit* __restrict__ units)
 {
-    Unit u = units[blockIdx.x];
+    const Unit u = units[blockIdx.x];
     const TileDev& T = a.tiles[u.id];
-    int x = u.bx * 32 + (threadIdx.x & 31), y = u.by * 8 + (threadIdx.x >> 5);
-    if (x >= T.w || y >= T.h) return;
-    size_t p = (size_t)y * T.w + x;
-    unsigned short* o = T.out + p * 3;
-    int own = T.owner[p];
-    if (own < 0)
+    const int W = T.w, H = T.h;
+    const int uw = T.lw[1], uh = T.lh[1];
+    const long long base = (long long)u.by * kBandRows * W;
+    const long long n = min((long long)kBandRows * W, (long long)W * H - base);
+    for (long long q = threadIdx.x; q < n; q += blockDim.x)
     {
-        o[0] = o[1] = o[2] = 0;
-        return;
-    }
-    const ItemDev& it = a.items[T.firstItem + own];
-    const unsigned short* px = it.img + p * 3;
-    float r[3] = {(float)px[0], (float)px[1], (float)px[2]};
-    if (T.bands > 1)
-    {
-        const int uw = T.lw[1], uh = T.lh[1];
-        UpCoef c = up_coef(uw, uh, T.w, T.h, x, y);
-        const float4* g1 = it.nd + T.loff[1];
-        float3 a00 = gauss_of(g1[(size_t)c.y0 * uw + c.x0]);
-        float3 a10 = gauss_of(g1[(size_t)c.y0 * uw + c.x1]);
-        float3 a01 = gauss_of(g1[(size_t)c.y1 * uw + c.x0]);
-        float3 a11 = gauss_of(g1[(size_t)c.y1 * uw + c.x1]);
-        float lap[3] = {fsub(r[0], up_mix(a00.x, a10.x, a01.x, a11.x, c.wx, c.wy)),
-                        fsub(r[1], up_mix(a00.y, a10.y, a01.y, a11.y, c.wx, c.wy)),
-                        fsub(r[2], up_mix(a00.z, a10.z, a01.z, a11.z, c.wx, c.wy))};
-        const float* rc = T.blend + T.loff[1] * 3;
+        const long long p = base + q;
+        const int y = (int)(p / W), x = (int)(p - (long long)y * W);
+        unsigned short* o = T.out + p * 3;
+        const int own = T.owner[p];
+        if (own < 0)
+        {
+            o[0] = o[1] = o[2] = 0;
+            continue;
+        }
+        const ItemDev& it = a.items[T.firstItem + own];
+        const unsigned short* px = it.img + p * 3;
+        float r[3] = {(float)px[0], (float)px[1], (float)px[2]};
+        if (T.bands > 1)
+        {
+            UpCoef c = up_coef(uw, uh, W, H, x, y);
+            const float4* g1 = it.nd + T.loff[1];
+            float3 a00 = gauss_of(g1[(size_t)c.y0 * uw + c.x0]);
+            float3 a10 = gauss_of(g1[(size_t)c.y0 * uw + c.x1]);
+            float3 a01 = gauss_of(g1[(size_t)c.y1 * uw + c.x0]);
+            float3 a11 = gauss_of(g1[(size_t)c.y1 * uw + c.x1]);
+            float lap[3] = {fsub(r[0], up_mix(a00.x, a10.x, a01.x, a11.x, c.wx, c.wy)),
+                            fsub(r[1], up_mix(a00.y, a10.y, a01.y, a11.y, c.wx, c.wy)),
+                            fsub(r[2], up_mix(a00.z, a10.z, a01.z, a11.z, c.wx, c.wy))};
+            const float* rc = T.blend + T.loff[1] * 3;
+#pragma unroll
+            for (int ch = 0; ch < 3; ++ch)
+            {
+                float up = up_mix(rc[((size_t)c.y0 * uw + c.x0) * 3 + ch], rc[((size_t)c.y0 * uw + c.x1) * 3 + ch],
+                                  rc[((size_t)c.y1 * uw + c.x0) * 3 + ch], rc[((size_t)c.y1 * uw + c.x1) * 3 + ch],
+                                  c.wx, c.wy);
+                r[ch] = fadd(lap[ch], up);
+            }
+        }
 #pragma unroll
         for (int ch = 0; ch < 3; ++ch)
         {
-            float up = up_mix(rc[((size_t)c.y0 * uw + c.x0) * 3 + ch], rc[((size_t)c.y0 * uw + c.x1) * 3 + ch],
-                              rc[((size_t)c.y1 * uw + c.x0) * 3 + ch], rc[((size_t)c.y1 * uw + c.x1) * 3 + ch], c.wx,
-                              c.wy);
-            r[ch] = fadd(lap[ch], up);
+            float v = r[ch];
+            v = v < 65535.0f ? v : 65535.0f;
+            v = 0.0f < v ? v : 0.0f;
+            o[ch] = (unsigned short)__float2uint_rz(fadd(v, 0.5f));
         }
-    }
-#pragma unroll
-    for (int ch = 0; ch < 3; ++ch)
-    {
-        float v = r[ch];
-        v = v < 65535.0f ? v : 65535.0f;
-        v = 0.0f < v ? v : 0.0f;
-        o[ch] = (unsigned short)__float2uint_rz(fadd(v, 0.5f));
     }
 }
 }  // namespace
@@ -845,8 +1093,17 @@ int launch_seam(const BlendArgs& a, const int* tileList, int n, cudaStream_t s)
 int launch_down(const BlendArgs& a, const Unit* units, int n, int level, cudaStream_t s)
 {
     if (n <= 0) return I360B_SUCCESS;
-    if (level == 0) k_down<true><<<n, 256, 0, s>>>(a, units, level);
-    else k_down<false><<<n, 256, 0, s>>>(a, units, level);
+    const int smem = (5 * kDnSH * kDnSW + 5 * kDnSH * kDnTW) * (int)sizeof(float);
+    if (level == 0)
+    {
+        cudaFuncSetAttribute(k_down<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+        k_down<true><<<n, 256, smem, s>>>(a, units, level);
+    }
+    else
+    {
+        cudaFuncSetAttribute(k_down<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+        k_down<false><<<n, 256, smem, s>>>(a, units, level);
+    }
     return check_launch("pyramid down kernel");
 }
 

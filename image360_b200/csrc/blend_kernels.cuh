@@ -8,6 +8,7 @@
 namespace i360b
 {
 constexpr int kMaxBands = 8;
+constexpr int kBandRows = 16;  // rows per CTA of the per-pixel band kernels
 constexpr int kSeamRadius = 24;                 // SeamBlend.cpp:319
 constexpr int kSeamBand = 2 * kSeamRadius + 1;  // candidates per line
 constexpr float kSeamSmooth = 2.0f;             // SeamBlend.cpp:309
@@ -19,7 +20,7 @@ struct ItemDev
     uint32_t* cov;              // coverage bits, covWords per row
     float* d1;                  // chamfer forward pass
     float* d;                   // chamfer distance (final)
-    int* bbox;                  // x0, y0, x1, y1 of covered pixels (x0 > x1 = empty)
+    int* bbox;                  // x0, y0, x1, y1 of covered pixels (x0 > x1 = empty), then the covered count
     float4* nd;                 // pyramid levels 1.. : (num.rgb, den)
     float* wg;                  // pyramid levels 1.. : weight
     float H[9];                 // destination(tile) -> source(frame) matrix

@@ -28,6 +28,7 @@ __global__ void k_init_bbox(ItemDev* items, int n)
     b[1] = 0x7fffffff;
     b[2] = -1;
     b[3] = -1;
+    b[4] = 0;
 }
 
 // Frame homography -> per-item destination->source matrix.
@@ -209,8 +210,13 @@ int Plan::build(const std::vector<TileSpec>& specs, int numBands, bool renderPat
     nItems = (int)items.size();
     // ---- work lists -------------------------------------------------------
     std::vector<Unit> units;
+    // Band units: kBandRows full-width rows each (per-pixel kernels).
+    auto addBands = [&](int id, int h) {
+        for (int by = 0; by < (h + kBandRows - 1) / kBandRows; ++by) units.push_back(Unit{id, 0, by, 0});
+    };
+    // Block units of the pyramid down kernel: 32 x 16 outputs each.
     auto addBlocks = [&](int id, int w, int h) {
-        for (int by = 0; by < (h + 7) / 8; ++by)
+        for (int by = 0; by < (h + 15) / 16; ++by)
             for (int bx = 0; bx < (w + 31) / 32; ++bx) units.push_back(Unit{id, bx, by, 0});
     };
     lists.clear();
@@ -218,17 +224,13 @@ int Plan::build(const std::vector<TileSpec>& specs, int numBands, bool renderPat
     auto endList = [&](int start) { lists.push_back(Range{start, (int)units.size() - start}); };
     int s;
     s = beginList();  // 0: coverage / warp
-    for (int i = 0; i < nItems; ++i) addBlocks(i, tiles[items[i].tile].w, tiles[items[i].tile].h);
+    for (int i = 0; i < nItems; ++i) addBands(i, tiles[items[i].tile].h);
     endList(s);
     s = beginList();  // 1: ownership
-    for (int t = 0; t < nTiles; ++t)
-    {
-        long long n = (long long)tiles[t].w * tiles[t].h;
-        for (long long b = 0; b < (n + 1023) / 1024; ++b) units.push_back(Unit{t, (int)b, 0, 0});
-    }
+    for (int t = 0; t < nTiles; ++t) addBands(t, tiles[t].h);
     endList(s);
     s = beginList();  // 2: level 0 output
-    for (int t = 0; t < nTiles; ++t) addBlocks(t, tiles[t].w, tiles[t].h);
+    for (int t = 0; t < nTiles; ++t) addBands(t, tiles[t].h);
     endList(s);
     for (int l = 0; l < kMaxBands - 1; ++l)  // 3 + l: down from level l
     {
@@ -245,7 +247,7 @@ int Plan::build(const std::vector<TileSpec>& specs, int numBands, bool renderPat
         s = beginList();
         if (l >= 1)
             for (int t = 0; t < nTiles; ++t)
-                if (tiles[t].bands > l) addBlocks(t, tiles[t].lw[l], tiles[t].lh[l]);
+                if (tiles[t].bands > l) addBands(t, tiles[t].lh[l]);
         endList(s);
     }
     for (int l = 0; l < kMaxBands; ++l)  // 3 + 2*kMaxBands - 1 + l: collapse at level l (1 <= l <= bands-2)
@@ -253,7 +255,7 @@ int Plan::build(const std::vector<TileSpec>& specs, int numBands, bool renderPat
         s = beginList();
         if (l >= 1)
             for (int t = 0; t < nTiles; ++t)
-                if (tiles[t].bands > l + 1) addBlocks(t, tiles[t].lw[l], tiles[t].lh[l]);
+                if (tiles[t].bands > l + 1) addBands(t, tiles[t].lh[l]);
         endList(s);
     }
     std::vector<int> ints;
