@@ -200,57 +200,25 @@ __global__ void __launch_bounds__(256) k_warp_tiles(BlendArgs a, const Unit* __r
 //
 // The raster recurrence d[p] = min(init, left+1, up+1, upleft+sqrt2,
 // upright+sqrt2) is a DAG with a unique solution, so any schedule that applies
-// the same rounded operations reproduces the CPU bit for bit.  Each row is
-//     a[x] = min(init[x], prev[x]+1, prev[x-1]+sqrt2, prev[x+1]+sqrt2)
-//     d[x] = min(a[x], d[x-1] + 1)               (fl(+1) each step)
-// The second line is a scan whose operator "v -> min(L, g^S(v))", with
-// g(v) = fl(v + 1), composes as (L1,S1);(L2,S2) = (min(L2, g^S2(L1)), S1+S2),
-// because fl(.+1) is monotone.  g^n(v) is evaluated exactly by add_ones().
+// the same rounded operations (min is exact and order-free) reproduces the CPU
+// result bit for bit.
 //
-// Rows are pipelined over the CTA's warps (row y on warp y % NW) in chunks of
-// 256 columns, each warp waiting (bounded) until the row above has published
-// the columns it needs.  Chunk boundaries are skewed by one column per row so
-// a row lags the one above by a single chunk.  The backward pass is the same
-// code on mirrored coordinates with the forward result as init.
+// Systolic wavefront: lane r of a warp owns row 32g + r and walks it one
+// column per step, kLag columns behind the lane above, so at every step the
+// three values it needs from the row above (x-1, x, x+1) have already been
+// produced; the newest one arrives by one __shfl_up_sync, the two older ones
+// are kept from earlier steps.  Lane 0 takes its row above from a shared-memory
+// ring written by lane 31 of the previous row group, with a bounded wait on
+// that group's published progress.  The backward pass is the same code on
+// mirrored coordinates with the forward result as init.
 // ---------------------------------------------------------------------------
-constexpr int kDtE = 8;
-constexpr int kDtCW = 32 * kDtE;
+constexpr int kLag = 4;      // columns a row lags the row above
+constexpr int kDtRing = 8;   // row-group hand-off slots
 
-__host__ __device__ __forceinline__ int dt_ring_stride(int W) { return W + (W >> 3) + 8; }
-__device__ __forceinline__ int ring_idx(int x) { return x + (x >> 3); }  // 1 pad per 8: conflict-free lanes
-
-// fl-sequential v + 1 + 1 + ... (n times), v >= 0.  Inside one binade
-// [2^e, 2^(e+1)) with e <= 23 adding 1 is exact, so only the step that crosses
-// into the next binade rounds; each crossing is one rounded add.
-__device__ __forceinline__ float add_ones(float v, int n)
-{
-    if (n <= 0) return v;
-    if (v >= 1.0f && v < 16777216.0f)
-    {
-        // Common case: v + n stays below the next power of two, so the n
-        // steps are exact and equal one add.
-        float B = __int_as_float((__float_as_int(v) & 0x7f800000) + 0x00800000);
-        if (fsub(B, v) > (float)n) return fadd(v, (float)n);
-    }
-    while (n > 0)
-    {
-        if (!(v < 16777216.0f)) return v;  // +inf (or beyond the distances that occur)
-        int m;
-        if (v < 1.0f) m = 1;
-        else
-        {
-            float B = __int_as_float((__float_as_int(v) & 0x7f800000) + 0x00800000);
-            m = (int)ceilf(fsub(B, v));  // exact: Sterbenz
-        }
-        int k = m < n ? m : n;
-        v = fadd(v, (float)k);
-        n -= k;
-    }
-    return v;
-}
+__host__ __device__ __forceinline__ int dt_ring_stride(int W) { return W + 4; }
 
 template <bool BACK>
-__global__ void __launch_bounds__(512) k_dt(BlendArgs a, const int* __restrict__ itemList, int nw)
+__global__ void __launch_bounds__(1024, 1) k_dt(BlendArgs a, const int* __restrict__ itemList, int nslots)
 {
     extern __shared__ float smem[];
     const ItemDev& it = a.items[itemList[blockIdx.x]];
@@ -265,8 +233,8 @@ __global__ void __launch_bounds__(512) k_dt(BlendArgs a, const int* __restrict__
     }
     const int RS = dt_ring_stride(W);
     float* ring = smem;
-    int* prog = reinterpret_cast<int*>(smem + (size_t)nw * RS);
-    if (threadIdx.x < nw) prog[threadIdx.x] = -1;
+    int* prog = reinterpret_cast<int*>(smem + (size_t)nslots * RS);
+    if (threadIdx.x < nslots) prog[threadIdx.x] = -1;
     __syncthreads();
     const float kInf = (float)(W + H);
     const float kDiag = 1.41421356f;
@@ -275,127 +243,91 @@ __global__ void __launch_bounds__(512) k_dt(BlendArgs a, const int* __restrict__
     const uint32_t* cov = it.cov;
     const float* d1 = it.d1;
     float* out = BACK ? it.d : it.d1;
+    const int nG = (H + 31) >> 5;
+    const int nwarps = blockDim.x >> 5;
 
-    for (int vy = warp; vy < H; vy += nw)
+    for (int g = warp; g < nG; g += nwarps)
     {
+        const int vy = g * 32 + lane;
+        const bool rowOk = vy < H;
         const int ry = BACK ? H - 1 - vy : vy;
-        const int slot = vy % nw, pslot = (vy + nw - 1) % nw;
-        const int skew = vy % kDtCW;
-        float carry = INF;
-        for (int x0 = -skew; x0 < W; x0 += kDtCW)
+        const int slot = g % nslots, pslot = (g + nslots - 1) % nslots;
+        float left = INF;               // own row, column x-1
+        float upm1 = INF, up0 = INF;    // row above, columns x-1 and x
+        float hist[kLag];               // own outputs of the last kLag steps (hist[0] newest)
+#pragma unroll
+        for (int q = 0; q < kLag; ++q) hist[q] = INF;
+        int seen = -1;                  // lane 0: progress of the group above already observed
+        const int nSteps = W + 31 * kLag;
+        for (int t0 = 0; t0 < nSteps; t0 += kLag)
         {
-            const int x1 = min(x0 + kDtCW, W);
-            const int xb = x0 + lane * kDtE;
-            // Initial values do not depend on the row above: load them before
-            // waiting so the global latency overlaps the wait.
-            float iv[kDtE];
-            if (BACK)
+            // Lane 0 needs the row above up to column x+1 for every x of this block.
+            if (g > 0 && lane == 0)
             {
-#pragma unroll
-                for (int k = 0; k < kDtE; ++k)
-                {
-                    int x = xb + k;
-                    iv[k] = (x >= 0 && x < W) ? __ldg(d1 + (size_t)ry * W + (W - 1 - x)) : INF;
-                }
-            }
-            else
-            {
-                int xs = max(xb, 0), xe = min(xb + kDtE - 1, W - 1);
-                uint32_t w0 = 0, w1 = 0;
-                if (xs <= xe)
-                {
-                    w0 = __ldg(cov + (size_t)ry * covWords + (xs >> 5));
-                    w1 = __ldg(cov + (size_t)ry * covWords + (xe >> 5));
-                }
-#pragma unroll
-                for (int k = 0; k < kDtE; ++k)
-                {
-                    int x = xb + k;
-                    bool c = false;
-                    if (x >= 0 && x < W) c = (((x >> 5) == (xs >> 5) ? w0 : w1) >> (x & 31)) & 1u;
-                    iv[k] = (x >= 0 && x < W) ? (c ? kInf : 0.0f) : INF;
-                }
-            }
-            if (vy > 0)
-            {
-                const int target = (vy - 1) * (W + 1) + min(x1 + 1, W);
-                int ok = 1;
-                if (lane == 0)
+                const int need = min(t0 + kLag + 1, W);
+                const int target = (g - 1) * (W + 1) + need;
+                if (seen < target)
                 {
                     cuda::atomic_ref<int, cuda::thread_scope_block> pr(prog[pslot]);
-                    long long t0 = clock64();
+                    long long tstart = clock64();
                     int spins = 0;
-                    while (pr.load(cuda::memory_order_acquire) < target)
+                    while ((seen = pr.load(cuda::memory_order_acquire)) < target)
                     {
-                        // Back off so waiting warps leave the issue slots to
-                        // the warps computing the rows they wait for.
-                        __nanosleep(64);
-                        if ((++spins & 255) == 0)
+                        // The producer is normally one block ahead: poll first,
+                        // back off only if the wait is long.
+                        if (++spins > 256) __nanosleep(64);
+                        if ((spins & 255) == 0 && (*(volatile int*)a.error || clock64() - tstart > kSpinCycles))
                         {
-                            if (*(volatile int*)a.error || clock64() - t0 > kSpinCycles)
-                            {
-                                atomicExch(a.error, 1);
-                                ok = 0;
-                                break;
-                            }
+                            atomicExch(a.error, 1);
+                            break;
                         }
                     }
                 }
-                ok = __shfl_sync(kFull, ok, 0);
-                if (!ok) return;
             }
-            float pv[kDtE + 2];
+            if (__shfl_sync(kFull, (g > 0 && lane == 0) ? (seen < (g - 1) * (W + 1) + min(t0 + kLag + 1, W) ? 1 : 0) : 0, 0))
+                return;  // gave up waiting (error flag set)
 #pragma unroll
-            for (int k = 0; k < kDtE + 2; ++k)
+            for (int q = 0; q < kLag; ++q)
             {
-                int x = xb - 1 + k;
-                pv[k] = (vy > 0 && x >= 0 && x < W) ? ring[pslot * RS + ring_idx(x)] : INF;
-            }
-            float l[kDtE];
-            float prev = INF;
-#pragma unroll
-            for (int k = 0; k < kDtE; ++k)
-            {
-                int x = xb + k;
-                float av = iv[k];
-                if (vy > 0 && x >= 0 && x < W)
+                const int x = t0 + q - kLag * lane;
+                // Publish to the lane below my output of kLag-1 steps ago: its up[x+1].
+                float recv = __shfl_up_sync(kFull, hist[kLag - 2], 1);
+                if (lane == 0) recv = (g > 0 && x + 1 >= 0 && x + 1 < W) ? ring[pslot * RS + x + 1] : INF;
+                const float upp1 = recv;
+                float d = INF;
+                if (rowOk && x >= 0 && x < W)
                 {
-                    av = fminf(av, fadd(pv[k + 1], 1.0f));
-                    if (x > 0) av = fminf(av, fadd(pv[k], kDiag));
-                    if (x < W - 1) av = fminf(av, fadd(pv[k + 2], kDiag));
+                    const int rx = BACK ? W - 1 - x : x;
+                    float av;
+                    if (BACK) av = __ldg(d1 + (size_t)ry * W + rx);
+                    else av = ((__ldg(cov + (size_t)ry * covWords + (rx >> 5)) >> (rx & 31)) & 1u) ? kInf : 0.0f;
+                    if (x > 0) av = fminf(av, fadd(left, 1.0f));
+                    if (vy > 0)
+                    {
+                        av = fminf(av, fadd(up0, 1.0f));
+                        if (x > 0) av = fminf(av, fadd(upm1, kDiag));
+                        if (x < W - 1) av = fminf(av, fadd(upp1, kDiag));
+                    }
+                    d = av;
+                    out[(size_t)ry * W + rx] = d;
+                    if (lane == 31) ring[slot * RS + x] = d;
                 }
-                l[k] = fminf(av, fadd(prev, 1.0f));
-                prev = l[k];
-            }
-            // Inclusive scan over lanes of (L, S=kDtE) segments.
-            float Lc = l[kDtE - 1];
+                left = d;
+                upm1 = up0;
+                up0 = upp1;
 #pragma unroll
-            for (int dd = 1; dd < 32; dd <<= 1)
-            {
-                float Lp = __shfl_up_sync(kFull, Lc, dd);
-                if (lane >= dd) Lc = fminf(Lc, add_ones(Lp, kDtE * dd));
+                for (int k = kLag - 1; k > 0; --k) hist[k] = hist[k - 1];
+                hist[0] = d;
             }
-            float excl = __shfl_up_sync(kFull, Lc, 1);
-            if (lane == 0) excl = INF;
-            float v = fminf(excl, add_ones(carry, lane * kDtE));
-#pragma unroll
-            for (int k = 0; k < kDtE; ++k)
+            // Lane 31 publishes how many columns of its row are final.
+            if (lane == 31)
             {
-                v = fminf(l[k], fadd(v, 1.0f));
-                int x = xb + k;
-                if (x >= 0 && x < W)
+                const int x = t0 + kLag - 1 - kLag * 31;
+                if (x >= 0)
                 {
-                    ring[slot * RS + ring_idx(x)] = v;
-                    int rx = BACK ? W - 1 - x : x;
-                    out[(size_t)ry * W + rx] = v;
+                    cuda::atomic_ref<int, cuda::thread_scope_block> pr(prog[slot]);
+                    pr.store(g * (W + 1) + min(x + 1, W), cuda::memory_order_release);
                 }
-            }
-            carry = __shfl_sync(kFull, v, 31);
-            __syncwarp();
-            if (lane == 0)
-            {
-                cuda::atomic_ref<int, cuda::thread_scope_block> pr(prog[slot]);
-                pr.store(vy * (W + 1) + x1, cuda::memory_order_release);
             }
         }
     }
@@ -435,18 +367,40 @@ __global__ void __launch_bounds__(256) k_owner(BlendArgs a, const Unit* __restri
 
 // ---------------------------------------------------------------------------
 // Seam refinement (SeamBlend.cpp:293-445) for every overlapping pair of a
-// tile, in the reference's (i, j) order, one CTA per tile.  Lines are scanned
-// warp-parallel; the dynamic program over contested lines is sequential (it
-// is in the reference too) and runs in one warp with the per-line state in
-// shared memory.
+// tile, in the reference's (i, j) order, one 1024-thread CTA per tile.
+// Lines are scanned in parallel (row lines: a warp per line with 16-byte owner
+// loads; column lines: a lane per line, 16 loads in flight); the dynamic
+// program over contested lines is sequential, as in the reference, and runs
+// on two warps (one candidate per lane) with the per-line state in shared
+// memory.
 // ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(256) k_seam(BlendArgs a, const int* __restrict__ tileList, int smemLines)
+constexpr int kSeamThreads = 1024;
+constexpr int kDpThreads = 64;
+
+// First byte of a 16-byte chunk (positions t = tb + b) that satisfies the
+// predicate, or INT_MAX.
+template <typename Pred>
+__device__ __forceinline__ int first_in_chunk(uint4 v, int tb, int lineLen, Pred pred)
+{
+    const unsigned w[4] = {v.x, v.y, v.z, v.w};
+#pragma unroll
+    for (int b = 0; b < 16; ++b)
+    {
+        const int t = tb + b;
+        const int o = (int)(signed char)((w[b >> 2] >> ((b & 3) * 8)) & 0xffu);
+        if (t >= 0 && t < lineLen && pred(o)) return t;
+    }
+    return 0x7fffffff;
+}
+
+__global__ void __launch_bounds__(kSeamThreads, 1) k_seam(BlendArgs a, const int* __restrict__ tileList, int smemLines)
 {
     extern __shared__ unsigned char sm_seam[];
     __shared__ float dpBuf[2][64];
     __shared__ int sLast, sBestK;
     const TileDev& T = a.tiles[tileList[blockIdx.x]];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, tid = threadIdx.x;
+    constexpr int nwarps = kSeamThreads / 32;
     const int K = T.numItems;
     const int w = T.w;
     const bool inSmem = T.maxLines <= smemLines;
@@ -458,105 +412,94 @@ __global__ void __launch_bounds__(256) k_seam(BlendArgs a, const int* __restrict
     for (int i = 0; i < K; ++i)
     {
         const ItemDev& I = a.items[T.firstItem + i];
-        int bI[4] = {I.bbox[0], I.bbox[1], I.bbox[2], I.bbox[3]};
+        const int bI[4] = {I.bbox[0], I.bbox[1], I.bbox[2], I.bbox[3]};
         if (bI[2] < 0) continue;
         for (int j = i + 1; j < K; ++j)
         {
             const ItemDev& J = a.items[T.firstItem + j];
-            int bJ[4] = {J.bbox[0], J.bbox[1], J.bbox[2], J.bbox[3]};
+            const int bJ[4] = {J.bbox[0], J.bbox[1], J.bbox[2], J.bbox[3]};
             if (bJ[2] < 0) continue;
-            int ox0 = max(bI[0], bJ[0]), oy0 = max(bI[1], bJ[1]);
-            int ox1 = min(bI[2], bJ[2]), oy1 = min(bI[3], bJ[3]);
+            const int ox0 = max(bI[0], bJ[0]), oy0 = max(bI[1], bJ[1]);
+            const int ox1 = min(bI[2], bJ[2]), oy1 = min(bI[3], bJ[3]);
             if (!(ox0 <= ox1 && oy0 <= oy1)) continue;
             const int bw = ox1 - ox0 + 1, bh = oy1 - oy0 + 1;
             const bool rowScan = bw >= bh;
-            float cI = rowScan ? fmul((float)(bI[0] + bI[2]), 0.5f) : fmul((float)(bI[1] + bI[3]), 0.5f);
-            float cJ = rowScan ? fmul((float)(bJ[0] + bJ[2]), 0.5f) : fmul((float)(bJ[1] + bJ[3]), 0.5f);
+            const float cI = rowScan ? fmul((float)(bI[0] + bI[2]), 0.5f) : fmul((float)(bI[1] + bI[3]), 0.5f);
+            const float cJ = rowScan ? fmul((float)(bJ[0] + bJ[2]), 0.5f) : fmul((float)(bJ[1] + bJ[3]), 0.5f);
             const bool iLow = cI <= cJ;
             const int numLines = rowScan ? bh : bw;
             const int lineLen = rowScan ? bw : bh;
-            const signed char ci = (signed char)i, cj = (signed char)j;
+            const int ci = i, cj = j;
             auto pix = [&](int line, int t) -> size_t {
                 return rowScan ? (size_t)(oy0 + line) * w + (ox0 + t) : (size_t)(oy0 + t) * w + (ox0 + line);
             };
-            auto pxy = [&](int line, int t, int& x, int& y) {
-                x = rowScan ? ox0 + t : ox0 + line;
-                y = rowScan ? oy0 + line : oy0 + t;
+            auto both_cov = [&](int line, int t) -> bool {
+                const int x = rowScan ? ox0 + t : ox0 + line;
+                const int y = rowScan ? oy0 + line : oy0 + t;
+                return cov_bit(I.cov, T.covWords, x, y) && cov_bit(J.cov, T.covWords, x, y);
             };
-
-            // Phase 1: crossover and contested band per line
-            // (SeamBlend.cpp:325-360).  Row scans: a warp walks one line with
-            // ballots.  Column scans: each lane walks one column, so a warp's
-            // owner loads are 32 consecutive bytes of one row.
+            // Contested band of a line (SeamBlend.cpp:347-359).
             auto band_of = [&](int line, int cross, int& lo, int& hi) {
                 lo = 1;
                 hi = 0;
                 if (cross < 0) return;
-                int bLo = max(0, cross - kSeamRadius), bHi = min(lineLen - 1, cross + kSeamRadius);
+                const int bLo = max(0, cross - kSeamRadius), bHi = min(lineLen - 1, cross + kSeamRadius);
                 for (int t = bLo; t <= bHi; ++t)
-                {
-                    int x, y;
-                    pxy(line, t, x, y);
-                    if (cov_bit(I.cov, T.covWords, x, y) && cov_bit(J.cov, T.covWords, x, y))
+                    if (both_cov(line, t))
                     {
                         if (hi < lo) lo = t;
                         hi = t;
                     }
-                }
             };
+
+            // Phase 1: crossover of each line (SeamBlend.cpp:334-345) and its band.
             if (rowScan)
             {
-                for (int line = warp; line < numLines; line += 8)
+                for (int line = warp; line < numLines; line += nwarps)
                 {
-                    int first = -1000, cross = -1;
-                    for (int t0 = 0; t0 < lineLen && cross < 0; t0 += 32)
+                    const signed char* rowp = T.owner + pix(line, 0);
+                    const uintptr_t base = reinterpret_cast<uintptr_t>(rowp) & ~uintptr_t(15);
+                    const int off = (int)(reinterpret_cast<uintptr_t>(rowp) - base);
+                    const int nChunks = (off + lineLen + 15) >> 4;
+                    const uint4* src = reinterpret_cast<const uint4*>(base);
+                    // pass A: first position owned by I or J, and that owner
+                    int p1 = 0x7fffffff, v1 = -1;
+                    for (int c0 = 0; c0 < nChunks && p1 == 0x7fffffff; c0 += 32)
                     {
-                        int t = t0 + lane;
-                        int o = -2;
-                        bool isIJ = false;
-                        if (t < lineLen)
-                        {
-                            o = T.owner[pix(line, t)];
-                            isIJ = (o == ci || o == cj);
-                        }
-                        unsigned m = __ballot_sync(kFull, isIJ);
-                        if (!m) continue;
-                        if (first == -1000)
-                        {
-                            int fl = __ffs(m) - 1;
-                            first = __shfl_sync(kFull, o, fl);
-                            unsigned md = __ballot_sync(kFull, isIJ && o != first);
-                            md &= (fl == 31) ? 0u : ~((2u << fl) - 1u);
-                            if (md) cross = t0 + __ffs(md) - 1;
-                        }
-                        else
-                        {
-                            unsigned md = __ballot_sync(kFull, isIJ && o != first);
-                            if (md) cross = t0 + __ffs(md) - 1;
-                        }
+                        const int c = c0 + lane;
+                        int f = 0x7fffffff;
+                        if (c < nChunks)
+                            f = first_in_chunk(src[c], c * 16 - off, lineLen, [&](int o) { return o == ci || o == cj; });
+                        p1 = __reduce_min_sync(kFull, f);
                     }
-                    // band: lanes test the <= 49 candidates, two rounds
+                    int cross = -1;
+                    if (p1 != 0x7fffffff)
+                    {
+                        v1 = (int)T.owner[pix(line, p1)];
+                        const int cStart = (p1 + off) >> 4;
+                        int f2 = 0x7fffffff;
+                        for (int c0 = cStart; c0 < nChunks && f2 == 0x7fffffff; c0 += 32)
+                        {
+                            const int c = c0 + lane;
+                            int f = 0x7fffffff;
+                            if (c < nChunks)
+                                f = first_in_chunk(src[c], c * 16 - off, lineLen, [&](int o) {
+                                    return (o == ci || o == cj) && o != v1;
+                                });
+                            if (f <= p1) f = 0x7fffffff;  // only positions after the first I/J pixel
+                            f2 = __reduce_min_sync(kFull, f);
+                        }
+                        if (f2 != 0x7fffffff) cross = f2;
+                    }
                     int lo = 1, hi = 0;
                     if (cross >= 0)
                     {
-                        int bLo = max(0, cross - kSeamRadius);
-                        int bHi = min(lineLen - 1, cross + kSeamRadius);
-                        bool both0 = false, both1 = false;
-                        int t = bLo + lane;
-                        if (t <= bHi)
-                        {
-                            int x, y;
-                            pxy(line, t, x, y);
-                            both0 = cov_bit(I.cov, T.covWords, x, y) && cov_bit(J.cov, T.covWords, x, y);
-                        }
-                        t = bLo + 32 + lane;
-                        if (t <= bHi)
-                        {
-                            int x, y;
-                            pxy(line, t, x, y);
-                            both1 = cov_bit(I.cov, T.covWords, x, y) && cov_bit(J.cov, T.covWords, x, y);
-                        }
-                        unsigned m0 = __ballot_sync(kFull, both0), m1 = __ballot_sync(kFull, both1);
+                        const int bLo = max(0, cross - kSeamRadius);
+                        const int bHi = min(lineLen - 1, cross + kSeamRadius);
+                        const int ta = bLo + lane, tb = bLo + 32 + lane;
+                        const bool b0 = ta <= bHi && both_cov(line, ta);
+                        const bool b1 = tb <= bHi && both_cov(line, tb);
+                        const unsigned m0 = __ballot_sync(kFull, b0), m1 = __ballot_sync(kFull, b1);
                         if (m0 | m1)
                         {
                             lo = bLo + (m0 ? __ffs(m0) - 1 : 32 + __ffs(m1) - 1);
@@ -572,22 +515,22 @@ __global__ void __launch_bounds__(256) k_seam(BlendArgs a, const int* __restrict
             }
             else
             {
-                for (int line = tid; line < numLines; line += 256)
+                for (int line = tid; line < numLines; line += kSeamThreads)
                 {
                     int first = -1000, cross = -1;
-                    for (int t = 0; t < lineLen; ++t)
+                    for (int t0 = 0; t0 < lineLen && cross < 0; t0 += 16)
                     {
-                        int o = T.owner[pix(line, t)];
-                        if (o != ci && o != cj) continue;
-                        if (first == -1000)
+                        // 16 independent loads in flight, then a sequential walk.
+                        int ov[16];
+#pragma unroll
+                        for (int q = 0; q < 16; ++q) ov[q] = (t0 + q < lineLen) ? (int)T.owner[pix(line, t0 + q)] : -2;
+#pragma unroll
+                        for (int q = 0; q < 16; ++q)
                         {
-                            first = o;
-                            continue;
-                        }
-                        if (o != first)
-                        {
-                            cross = t;
-                            break;
+                            const int o = ov[q];
+                            if (cross >= 0 || (o != ci && o != cj)) continue;
+                            if (first == -1000) first = o;
+                            else if (o != first) cross = t0 + q;
                         }
                     }
                     int lo, hi;
@@ -598,18 +541,19 @@ __global__ void __launch_bounds__(256) k_seam(BlendArgs a, const int* __restrict
             }
             __syncthreads();
 
-            // Phase 2: per-pixel colour cost of every contested candidate
-            // (SeamBlend.cpp:382-383), indexed so consecutive threads touch
-            // neighbouring pixels for either scan direction.
-            for (int idx = tid; idx < numLines * kSeamBand; idx += 256)
+            // Phase 2: colour cost of every contested candidate
+            // (SeamBlend.cpp:381-383); consecutive threads take neighbouring
+            // pixels for either scan direction.
+#pragma unroll 4
+            for (int idx = tid; idx < numLines * kSeamBand; idx += kSeamThreads)
             {
                 int line, k;
                 if (rowScan) { line = idx / kSeamBand; k = idx - line * kSeamBand; }
                 else { k = idx / numLines; line = idx - k * numLines; }
                 if (k == 0) T.chosen[line] = -1;
-                int lo = sLo[line], hi = sHi[line];
+                const int lo = sLo[line], hi = sHi[line];
                 if (k > hi - lo) continue;
-                size_t p = pix(line, lo + k);
+                const size_t p = pix(line, lo + k);
                 const unsigned short* pa = I.img + p * 3;
                 const unsigned short* pb = J.img + p * 3;
                 float c = 0.0f;
@@ -619,54 +563,34 @@ __global__ void __launch_bounds__(256) k_seam(BlendArgs a, const int* __restrict
             }
             __syncthreads();
 
-            // Phase 3: dynamic program over contested lines (SeamBlend.cpp:362-407),
-            // one warp.  The next contested line's costs are loaded before the
-            // current line's minimisation; each candidate's argmin over the
-            // previous line runs as four interleaved chains merged with the
-            // lowest-index tie rule of the strict '<' scan.
-            if (warp == 0)
+            // Phase 3: dynamic program over contested lines (SeamBlend.cpp:362-407)
+            // on the first kDpThreads threads, one candidate k per thread.  Each
+            // candidate's argmin over the previous line runs as four interleaved
+            // chains merged with the lowest-index rule of the strict '<' scan.
+            if (tid < kDpThreads)
             {
-                auto next_contested = [&](int from) {
-                    int l = from;
-                    while (l < numLines && sHi[l] < sLo[l])
-                    {
-                        if (lane == 0) sPrev[l] = -1;
-                        ++l;
-                    }
-                    return l;
-                };
+                const int k = tid;
                 int last = -1, cur = 0, lastW = 0;
-                int line = next_contested(0);
-                float c0 = 0.0f, c1 = 0.0f;
-                if (line < numLines)
-                {
-                    if (lane < sHi[line] - sLo[line] + 1) c0 = T.cost[(size_t)line * kSeamBand + lane];
-                    if (lane + 32 < sHi[line] - sLo[line] + 1) c1 = T.cost[(size_t)line * kSeamBand + lane + 32];
-                }
+                int line = 0;
+                while (line < numLines && sHi[line] < sLo[line]) ++line;
+                float c = 0.0f;
+                if (line < numLines && k <= sHi[line] - sLo[line]) c = T.cost[(size_t)line * kSeamBand + k];
                 while (line < numLines)
                 {
                     const int lo = sLo[line], lw = sHi[line] - lo + 1;
-                    const int nxt = next_contested(line + 1);
-                    float n0 = 0.0f, n1 = 0.0f;
-                    if (nxt < numLines)
+                    int nxt = line + 1;
+                    while (nxt < numLines && sHi[nxt] < sLo[nxt]) ++nxt;
+                    float cn = 0.0f;
+                    if (nxt < numLines && k <= sHi[nxt] - sLo[nxt]) cn = T.cost[(size_t)nxt * kSeamBand + k];
+                    if (k < lw)
                     {
-                        int nw2 = sHi[nxt] - sLo[nxt] + 1;
-                        if (lane < nw2) n0 = T.cost[(size_t)nxt * kSeamBand + lane];
-                        if (lane + 32 < nw2) n1 = T.cost[(size_t)nxt * kSeamBand + lane + 32];
-                    }
-                    const int plo = last >= 0 ? sLo[last] : 0;
-#pragma unroll
-                    for (int half = 0; half < 2; ++half)
-                    {
-                        const int k = lane + 32 * half;
-                        if (k >= lw) continue;
-                        const float c = half ? c1 : c0;
                         const int t = lo + k;
                         float val;
                         int bp = -1;
                         if (last < 0) val = c;
                         else
                         {
+                            const int plo = sLo[last];
                             float best[4] = {FLT_MAX, FLT_MAX, FLT_MAX, FLT_MAX};
                             int bi[4] = {-1, -1, -1, -1};
                             for (int pk = 0; pk < lastW; pk += 4)
@@ -674,11 +598,10 @@ __global__ void __launch_bounds__(256) k_seam(BlendArgs a, const int* __restrict
 #pragma unroll
                                 for (int q = 0; q < 4; ++q)
                                 {
-                                    int kk = pk + q;
+                                    const int kk = pk + q;
                                     if (kk < lastW)
                                     {
-                                        float c2 = fadd(dpBuf[cur ^ 1][kk],
-                                                        fmul(kSeamSmooth, fabsf((float)(t - (plo + kk)))));
+                                        float c2 = fadd(dpBuf[cur ^ 1][kk], fmul(kSeamSmooth, fabsf((float)(t - (plo + kk)))));
                                         if (c2 < best[q])
                                         {
                                             best[q] = c2;
@@ -687,7 +610,6 @@ __global__ void __launch_bounds__(256) k_seam(BlendArgs a, const int* __restrict
                                     }
                                 }
                             }
-                            // Merge: smaller value wins, equal values keep the lower index.
                             float b = best[0];
                             bp = bi[0];
 #pragma unroll
@@ -702,27 +624,28 @@ __global__ void __launch_bounds__(256) k_seam(BlendArgs a, const int* __restrict
                         dpBuf[cur][k] = val;
                         sBack[(size_t)line * kSeamBand + k] = (unsigned char)(bp < 0 ? 255 : bp);
                     }
-                    if (lane == 0) sPrev[line] = last;
+                    // Lines skipped between `line` and `nxt` have no predecessor entry.
+                    for (int l2 = line + 1 + k; l2 < nxt; l2 += kDpThreads) sPrev[l2] = -1;
+                    if (k == 0) sPrev[line] = last;
                     last = line;
                     lastW = lw;
                     cur ^= 1;
-                    c0 = n0;
-                    c1 = n1;
+                    c = cn;
                     line = nxt;
-                    __syncwarp();
+                    asm volatile("bar.sync 1, %0;" ::"r"(kDpThreads) : "memory");
                 }
-                if (lane == 0)
+                if (k == 0)
                 {
                     sLast = last;
                     int bestK = 0;
                     if (last >= 0)
                     {
                         float best = FLT_MAX;
-                        for (int k = 0; k < lastW; ++k)
-                            if (dpBuf[cur ^ 1][k] < best)
+                        for (int q = 0; q < lastW; ++q)
+                            if (dpBuf[cur ^ 1][q] < best)
                             {
-                                best = dpBuf[cur ^ 1][k];
-                                bestK = k;
+                                best = dpBuf[cur ^ 1][q];
+                                bestK = q;
                             }
                     }
                     sBestK = bestK;
@@ -730,39 +653,40 @@ __global__ void __launch_bounds__(256) k_seam(BlendArgs a, const int* __restrict
             }
             __syncthreads();
 
-            // Phase 4: backtrack.
+            // Phase 4: backtrack (SeamBlend.cpp:411-428).
             if (tid == 0 && sLast >= 0)
             {
                 int line = sLast, k = sBestK;
                 while (line >= 0 && k >= 0)
                 {
                     T.chosen[line] = sLo[line] + k;
-                    int pl = sPrev[line];
-                    int pk = sBack[(size_t)line * kSeamBand + k];
+                    const int pl = sPrev[line];
+                    const int pk = sBack[(size_t)line * kSeamBand + k];
                     line = pl;
                     k = pk == 255 ? -1 : pk;
                 }
             }
             __syncthreads();
 
-            // Phase 5: reassign I/J pixels inside each contested band.
+            // Phase 5: reassign I/J pixels inside each contested band
+            // (SeamBlend.cpp:430-444).
             if (sLast >= 0)
             {
-                for (int idx = tid; idx < numLines * kSeamBand; idx += 256)
+                for (int idx = tid; idx < numLines * kSeamBand; idx += kSeamThreads)
                 {
                     int line, k;
                     if (rowScan) { line = idx / kSeamBand; k = idx - line * kSeamBand; }
                     else { k = idx / numLines; line = idx - k * numLines; }
-                    int ch = T.chosen[line];
+                    const int ch = T.chosen[line];
                     if (ch < 0) continue;
-                    int lo = sLo[line], hi = sHi[line];
+                    const int lo = sLo[line], hi = sHi[line];
                     if (k > hi - lo) continue;
-                    int t = lo + k;
-                    size_t p = pix(line, t);
-                    signed char o = T.owner[p];
+                    const int t = lo + k;
+                    const size_t p = pix(line, t);
+                    const signed char o = T.owner[p];
                     if (o != ci && o != cj) continue;
-                    bool onLow = t < ch;
-                    T.owner[p] = (onLow == iLow) ? ci : cj;
+                    const bool onLow = t < ch;
+                    T.owner[p] = (signed char)((onLow == iLow) ? ci : cj);
                 }
             }
             __syncthreads();
@@ -1031,9 +955,8 @@ __global__ void __launch_bounds__(256) k_final0(BlendArgs a, const Unit* __restr
 int dt_rows_in_flight(int maxW)
 {
     size_t row = (size_t)dt_ring_stride(maxW) * sizeof(float);
-    int nw = (int)((200 * 1024) / row);
-    if (nw > 16) nw = 16;
-    return nw;
+    int n = (int)((210 * 1024) / row);
+    return n > kDtRing ? kDtRing : n;
 }
 
 int launch_coverage(const BlendArgs& a, const Unit* units, int n, cudaStream_t s)
@@ -1053,18 +976,18 @@ int launch_warp_tiles(const BlendArgs& a, const Unit* units, int n, cudaStream_t
 int launch_dt(const BlendArgs& a, const int* itemList, int n, bool backward, int maxW, cudaStream_t s)
 {
     if (n <= 0) return I360B_SUCCESS;
-    int nw = dt_rows_in_flight(maxW);
-    if (nw < 2) return fail(I360B_NOT_SUPPORTED, "Chunk width %d exceeds the distance-transform row buffer.", maxW);
-    size_t smem = (size_t)nw * dt_ring_stride(maxW) * sizeof(float) + 64 * sizeof(int);
+    int slots = dt_rows_in_flight(maxW);
+    if (slots < 2) return fail(I360B_NOT_SUPPORTED, "Chunk width %d exceeds the distance-transform row ring.", maxW);
+    size_t smem = (size_t)slots * dt_ring_stride(maxW) * sizeof(float) + 64 * sizeof(int);
     if (backward)
     {
         cudaFuncSetAttribute(k_dt<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        k_dt<true><<<n, nw * 32, smem, s>>>(a, itemList, nw);
+        k_dt<true><<<n, 1024, smem, s>>>(a, itemList, slots);
     }
     else
     {
         cudaFuncSetAttribute(k_dt<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        k_dt<false><<<n, nw * 32, smem, s>>>(a, itemList, nw);
+        k_dt<false><<<n, 1024, smem, s>>>(a, itemList, slots);
     }
     return check_launch("distance transform kernel");
 }
@@ -1086,7 +1009,7 @@ int launch_seam(const BlendArgs& a, const int* tileList, int n, cudaStream_t s)
     size_t smem = (size_t)smemLines * (3 * sizeof(int) + kSeamBand);
     if (n <= 0) return I360B_SUCCESS;
     cudaFuncSetAttribute(k_seam, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    k_seam<<<n, 256, smem, s>>>(a, tileList, smemLines);
+    k_seam<<<n, kSeamThreads, smem, s>>>(a, tileList, smemLines);
     return check_launch("seam kernel");
 }
 
