@@ -250,6 +250,7 @@ def run_ours(args, rank, world, local_rank):
                    "l2": "inputs and outputs larger than L2 (no flush)", "blend": "plain (learned blend not built)",
                    "parallelism": f"{world} independent panoramas"},
         "roofline": roof, "stages": per_stage, "gpu_launches": launches,
+        "seam_phase_cycles": stats["seamPhaseCycles"],
         "clocks": clk.summary(),
         "e2e": e2e,
     }

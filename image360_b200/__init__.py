@@ -55,7 +55,8 @@ class Frame(ct.Structure):
 
 class RenderStats(ct.Structure):
     _fields_ = [("numTiles", ct.c_int), ("numItems", ct.c_int), ("kernelsPerExecute", ct.c_int),
-                ("outputPixels", ct.c_longlong), ("coveredItemPixels", ct.c_longlong), ("scratchBytes", ct.c_longlong)]
+                ("outputPixels", ct.c_longlong), ("coveredItemPixels", ct.c_longlong), ("scratchBytes", ct.c_longlong),
+                ("seamPhaseCycles", ct.c_longlong * 5)]
 
 
 class Tile(ct.Structure):
@@ -261,7 +262,9 @@ class RenderPlan:
         rc = self.lib.i360b_render_plan_stats(self._h, stream or None, ct.byref(st))
         if rc != 0:
             raise RuntimeError(self.lib.i360b_get_last_error().decode())
-        return {k: getattr(st, k) for k, _ in RenderStats._fields_}
+        d = {k: getattr(st, k) for k, _ in RenderStats._fields_}
+        d["seamPhaseCycles"] = list(d["seamPhaseCycles"])
+        return d
 
     def profile(self, stream: int = 0) -> dict:
         """One un-captured run with CUDA events between stages: {stage: ms}."""

@@ -213,12 +213,12 @@ __global__ void __launch_bounds__(256) k_warp_tiles(BlendArgs a, const Unit* __r
 // mirrored coordinates with the forward result as init.
 // ---------------------------------------------------------------------------
 constexpr int kLag = 4;      // columns a row lags the row above
-constexpr int kDtRing = 8;   // row-group hand-off slots
+constexpr int kDtRing = 4;   // row-group hand-off slots
 
-__host__ __device__ __forceinline__ int dt_ring_stride(int W) { return W + 4; }
+__host__ __device__ __forceinline__ int dt_ring_stride(int W) { return (W + 7) & ~3; }
 
 template <bool BACK>
-__global__ void __launch_bounds__(1024, 1) k_dt(BlendArgs a, const int* __restrict__ itemList, int nslots)
+__global__ void __launch_bounds__(512, 2) k_dt(BlendArgs a, const int* __restrict__ itemList, int nslots)
 {
     extern __shared__ float smem[];
     const ItemDev& it = a.items[itemList[blockIdx.x]];
@@ -240,32 +240,35 @@ __global__ void __launch_bounds__(1024, 1) k_dt(BlendArgs a, const int* __restri
     const float kDiag = 1.41421356f;
     const float INF = f_inf();
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const uint32_t* cov = it.cov;
-    const float* d1 = it.d1;
-    float* out = BACK ? it.d : it.d1;
     const int nG = (H + 31) >> 5;
     const int nwarps = blockDim.x >> 5;
+    const bool vec = (W & 3) == 0;  // 16-byte row alignment of d1/d and the ring
 
     for (int g = warp; g < nG; g += nwarps)
     {
         const int vy = g * 32 + lane;
         const bool rowOk = vy < H;
-        const int ry = BACK ? H - 1 - vy : vy;
+        const bool fullGroup = g > 0 && g * 32 + 31 < H;
+        const int ry = BACK ? H - 1 - vy : (rowOk ? vy : 0);
+        const int rys = rowOk ? (BACK ? ry : vy) : 0;
+        float* outRow = (BACK ? it.d : it.d1) + (size_t)rys * W;
+        const float* d1Row = it.d1 + (size_t)rys * W;
+        const uint32_t* covRow = it.cov + (size_t)rys * covWords;
         const int slot = g % nslots, pslot = (g + nslots - 1) % nslots;
+        float* ringOut = ring + slot * RS;
+        const float* ringIn = ring + pslot * RS;
         float left = INF;               // own row, column x-1
         float upm1 = INF, up0 = INF;    // row above, columns x-1 and x
-        float hist[kLag];               // own outputs of the last kLag steps (hist[0] newest)
-#pragma unroll
-        for (int q = 0; q < kLag; ++q) hist[q] = INF;
+        float h0 = INF, h1 = INF, h2 = INF;  // own outputs 1, 2, 3 steps ago
         int seen = -1;                  // lane 0: progress of the group above already observed
         const int nSteps = W + 31 * kLag;
         for (int t0 = 0; t0 < nSteps; t0 += kLag)
         {
             // Lane 0 needs the row above up to column x+1 for every x of this block.
+            int bad = 0;
             if (g > 0 && lane == 0)
             {
-                const int need = min(t0 + kLag + 1, W);
-                const int target = (g - 1) * (W + 1) + need;
+                const int target = (g - 1) * (W + 1) + min(t0 + kLag + 1, W);
                 if (seen < target)
                 {
                     cuda::atomic_ref<int, cuda::thread_scope_block> pr(prog[pslot]);
@@ -279,55 +282,172 @@ __global__ void __launch_bounds__(1024, 1) k_dt(BlendArgs a, const int* __restri
                         if ((spins & 255) == 0 && (*(volatile int*)a.error || clock64() - tstart > kSpinCycles))
                         {
                             atomicExch(a.error, 1);
+                            bad = 1;
                             break;
                         }
                     }
                 }
             }
-            if (__shfl_sync(kFull, (g > 0 && lane == 0) ? (seen < (g - 1) * (W + 1) + min(t0 + kLag + 1, W) ? 1 : 0) : 0, 0))
-                return;  // gave up waiting (error flag set)
+            if (__shfl_sync(kFull, bad, 0)) return;  // gave up waiting (error flag set)
+            const int xb = t0 - kLag * lane;       // my first column of this block (multiple of 4)
+            // Interior block of a full group below row 0: every lane's four
+            // columns lie in [1, W-2], so no edge condition applies and the
+            // step is branch-free.
+            if (fullGroup && t0 - kLag * 31 >= 1 && t0 + kLag < W)
+            {
+                float iv[kLag];
+                if (BACK)
+                {
+                    if (vec)
+                    {
+                        const float4 q = __ldg(reinterpret_cast<const float4*>(d1Row + (W - kLag - xb)));
+                        iv[0] = q.w; iv[1] = q.z; iv[2] = q.y; iv[3] = q.x;
+                    }
+                    else
+                    {
+#pragma unroll
+                        for (int q = 0; q < kLag; ++q) iv[q] = __ldg(d1Row + (W - 1 - xb - q));
+                    }
+                }
+                else
+                {
+                    const uint32_t wd = __ldg(covRow + (xb >> 5)) >> (xb & 31);
+#pragma unroll
+                    for (int q = 0; q < kLag; ++q) iv[q] = ((wd >> q) & 1u) ? kInf : 0.0f;
+                }
+                float dv[kLag];
+#pragma unroll
+                for (int q = 0; q < kLag; ++q)
+                {
+                    const float recv = __shfl_up_sync(kFull, h2, 1);
+                    const float rv = lane == 0 ? ringIn[xb + q + 1] : 0.0f;
+                    const float upp1 = lane == 0 ? rv : recv;
+                    float av = fminf(iv[q], fadd(up0, 1.0f));
+                    av = fminf(av, fadd(upm1, kDiag));
+                    av = fminf(av, fadd(upp1, kDiag));
+                    av = fminf(av, fadd(left, 1.0f));
+                    dv[q] = av;
+                    left = av;
+                    upm1 = up0;
+                    up0 = upp1;
+                    h2 = h1;
+                    h1 = h0;
+                    h0 = av;
+                }
+                if (vec)
+                {
+                    if (BACK)
+                        *reinterpret_cast<float4*>(outRow + (W - kLag - xb)) = make_float4(dv[3], dv[2], dv[1], dv[0]);
+                    else *reinterpret_cast<float4*>(outRow + xb) = make_float4(dv[0], dv[1], dv[2], dv[3]);
+                }
+                else
+                {
+#pragma unroll
+                    for (int q = 0; q < kLag; ++q) outRow[BACK ? W - 1 - xb - q : xb + q] = dv[q];
+                }
+                if (lane == 31)
+                {
+                    *reinterpret_cast<float4*>(ringOut + xb) = make_float4(dv[0], dv[1], dv[2], dv[3]);
+                    cuda::atomic_ref<int, cuda::thread_scope_block> pr(prog[slot]);
+                    pr.store(g * (W + 1) + xb + kLag, cuda::memory_order_release);
+                }
+                continue;
+            }
+            const bool inside = rowOk && xb >= 0 && xb + kLag <= W;
+            // Initial values of the block: one coverage word or 16 bytes of d1.
+            float iv[kLag];
+            if (inside)
+            {
+                if (BACK)
+                {
+                    const int r0 = W - kLag - xb;  // real columns r0 .. r0+3 are x = xb+3 .. xb
+                    if (vec)
+                    {
+                        const float4 q = __ldg(reinterpret_cast<const float4*>(d1Row + r0));
+                        iv[0] = q.w; iv[1] = q.z; iv[2] = q.y; iv[3] = q.x;
+                    }
+                    else
+                    {
+#pragma unroll
+                        for (int q = 0; q < kLag; ++q) iv[q] = __ldg(d1Row + (W - 1 - xb - q));
+                    }
+                }
+                else
+                {
+                    const uint32_t wd = __ldg(covRow + (xb >> 5)) >> (xb & 31);
+#pragma unroll
+                    for (int q = 0; q < kLag; ++q) iv[q] = ((wd >> q) & 1u) ? kInf : 0.0f;
+                }
+            }
+            else
+            {
+#pragma unroll
+                for (int q = 0; q < kLag; ++q)
+                {
+                    const int x = xb + q;
+                    iv[q] = INF;
+                    if (rowOk && x >= 0 && x < W)
+                    {
+                        const int rx = BACK ? W - 1 - x : x;
+                        iv[q] = BACK ? __ldg(d1Row + rx) : (((__ldg(covRow + (rx >> 5)) >> (rx & 31)) & 1u) ? kInf : 0.0f);
+                    }
+                }
+            }
+            float dv[kLag];
 #pragma unroll
             for (int q = 0; q < kLag; ++q)
             {
-                const int x = t0 + q - kLag * lane;
+                const int x = xb + q;
                 // Publish to the lane below my output of kLag-1 steps ago: its up[x+1].
-                float recv = __shfl_up_sync(kFull, hist[kLag - 2], 1);
-                if (lane == 0) recv = (g > 0 && x + 1 >= 0 && x + 1 < W) ? ring[pslot * RS + x + 1] : INF;
+                float recv = __shfl_up_sync(kFull, h2, 1);
+                if (lane == 0) recv = (g > 0 && x + 1 >= 0 && x + 1 < W) ? ringIn[x + 1] : INF;
                 const float upp1 = recv;
-                float d = INF;
-                if (rowOk && x >= 0 && x < W)
+                float av = iv[q];
+                if (vy > 0)
                 {
-                    const int rx = BACK ? W - 1 - x : x;
-                    float av;
-                    if (BACK) av = __ldg(d1 + (size_t)ry * W + rx);
-                    else av = ((__ldg(cov + (size_t)ry * covWords + (rx >> 5)) >> (rx & 31)) & 1u) ? kInf : 0.0f;
-                    if (x > 0) av = fminf(av, fadd(left, 1.0f));
-                    if (vy > 0)
-                    {
-                        av = fminf(av, fadd(up0, 1.0f));
-                        if (x > 0) av = fminf(av, fadd(upm1, kDiag));
-                        if (x < W - 1) av = fminf(av, fadd(upp1, kDiag));
-                    }
-                    d = av;
-                    out[(size_t)ry * W + rx] = d;
-                    if (lane == 31) ring[slot * RS + x] = d;
+                    av = fminf(av, fadd(up0, 1.0f));
+                    if (x > 0) av = fminf(av, fadd(upm1, kDiag));
+                    if (x < W - 1) av = fminf(av, fadd(upp1, kDiag));
                 }
+                if (x > 0) av = fminf(av, fadd(left, 1.0f));
+                const bool ok = rowOk && x >= 0 && x < W;
+                const float d = ok ? av : INF;
+                dv[q] = d;
                 left = d;
                 upm1 = up0;
                 up0 = upp1;
+                h2 = h1;
+                h1 = h0;
+                h0 = d;
+            }
+            // Block results: one 16-byte store to the row (and to the ring for
+            // the last row of the group).
+            if (inside && vec)
+            {
+                if (BACK)
+                    *reinterpret_cast<float4*>(outRow + (W - kLag - xb)) = make_float4(dv[3], dv[2], dv[1], dv[0]);
+                else *reinterpret_cast<float4*>(outRow + xb) = make_float4(dv[0], dv[1], dv[2], dv[3]);
+                if (lane == 31) *reinterpret_cast<float4*>(ringOut + xb) = make_float4(dv[0], dv[1], dv[2], dv[3]);
+            }
+            else
+            {
 #pragma unroll
-                for (int k = kLag - 1; k > 0; --k) hist[k] = hist[k - 1];
-                hist[0] = d;
+                for (int q = 0; q < kLag; ++q)
+                {
+                    const int x = xb + q;
+                    if (rowOk && x >= 0 && x < W)
+                    {
+                        outRow[BACK ? W - 1 - x : x] = dv[q];
+                        if (lane == 31) ringOut[x] = dv[q];
+                    }
+                }
             }
             // Lane 31 publishes how many columns of its row are final.
-            if (lane == 31)
+            if (lane == 31 && xb + kLag - 1 >= 0)
             {
-                const int x = t0 + kLag - 1 - kLag * 31;
-                if (x >= 0)
-                {
-                    cuda::atomic_ref<int, cuda::thread_scope_block> pr(prog[slot]);
-                    pr.store(g * (W + 1) + min(x + 1, W), cuda::memory_order_release);
-                }
+                __syncwarp(0x80000000u);
+                cuda::atomic_ref<int, cuda::thread_scope_block> pr(prog[slot]);
+                pr.store(g * (W + 1) + min(xb + kLag, W), cuda::memory_order_release);
             }
         }
     }
@@ -375,7 +495,7 @@ __global__ void __launch_bounds__(256) k_owner(BlendArgs a, const Unit* __restri
 // memory.
 // ---------------------------------------------------------------------------
 constexpr int kSeamThreads = 1024;
-constexpr int kDpThreads = 64;
+constexpr int kDpThreads = 128;
 
 // First byte of a 16-byte chunk (positions t = tb + b) that satisfies the
 // predicate, or INT_MAX.
@@ -452,6 +572,7 @@ __global__ void __launch_bounds__(kSeamThreads, 1) k_seam(BlendArgs a, const int
                     }
             };
 
+            long long tp = clock64();
             // Phase 1: crossover of each line (SeamBlend.cpp:334-345) and its band.
             if (rowScan)
             {
@@ -541,6 +662,7 @@ __global__ void __launch_bounds__(kSeamThreads, 1) k_seam(BlendArgs a, const int
             }
             __syncthreads();
 
+            if (tid == 0) { long long now = clock64(); atomicAdd(a.seamCycles + 0, (unsigned long long)(now - tp)); tp = now; }
             // Phase 2: colour cost of every contested candidate
             // (SeamBlend.cpp:381-383); consecutive threads take neighbouring
             // pixels for either scan direction.
@@ -563,13 +685,16 @@ __global__ void __launch_bounds__(kSeamThreads, 1) k_seam(BlendArgs a, const int
             }
             __syncthreads();
 
+            if (tid == 0) { long long now = clock64(); atomicAdd(a.seamCycles + 1, (unsigned long long)(now - tp)); tp = now; }
             // Phase 3: dynamic program over contested lines (SeamBlend.cpp:362-407)
-            // on the first kDpThreads threads, one candidate k per thread.  Each
-            // candidate's argmin over the previous line runs as four interleaved
-            // chains merged with the lowest-index rule of the strict '<' scan.
+            // on the first kDpThreads threads: thread pairs share a candidate k,
+            // each scanning half of the previous line's entries in four
+            // interleaved chains; the halves merge with the lowest-index rule
+            // of the reference's strict '<' scan.  Penalties 2|t - pt| are
+            // exact small integers, formed in float without conversions.
             if (tid < kDpThreads)
             {
-                const int k = tid;
+                const int k = tid >> 1, half = tid & 1;
                 int last = -1, cur = 0, lastW = 0;
                 int line = 0;
                 while (line < numLines && sHi[line] < sLo[line]) ++line;
@@ -582,51 +707,72 @@ __global__ void __launch_bounds__(kSeamThreads, 1) k_seam(BlendArgs a, const int
                     while (nxt < numLines && sHi[nxt] < sLo[nxt]) ++nxt;
                     float cn = 0.0f;
                     if (nxt < numLines && k <= sHi[nxt] - sLo[nxt]) cn = T.cost[(size_t)nxt * kSeamBand + k];
-                    if (k < lw)
+                    float val = c;
+                    int bp = -1;
+                    float b = FLT_MAX;
+                    if (last >= 0 && k < lw)
                     {
-                        const int t = lo + k;
-                        float val;
-                        int bp = -1;
-                        if (last < 0) val = c;
-                        else
+                        const int plo = sLo[last];
+                        const int hsplit = (lastW + 1) >> 1;
+                        const int pb = half ? hsplit : 0, pe = half ? lastW : hsplit;
+                        const float d0 = (float)(lo + k - plo - pb);  // t - pt at pk = pb
+                        float best[4] = {FLT_MAX, FLT_MAX, FLT_MAX, FLT_MAX};
+                        int bi[4] = {-1, -1, -1, -1};
+                        for (int pk = pb; pk < pe; pk += 4)
                         {
-                            const int plo = sLo[last];
-                            float best[4] = {FLT_MAX, FLT_MAX, FLT_MAX, FLT_MAX};
-                            int bi[4] = {-1, -1, -1, -1};
-                            for (int pk = 0; pk < lastW; pk += 4)
-                            {
 #pragma unroll
-                                for (int q = 0; q < 4; ++q)
+                            for (int q = 0; q < 4; ++q)
+                            {
+                                const int kk = pk + q;
+                                if (kk < pe)
                                 {
-                                    const int kk = pk + q;
-                                    if (kk < lastW)
+                                    const float dd = fsub(d0, (float)(kk - pb));
+                                    const float pen = fadd(fabsf(dd), fabsf(dd));
+                                    const float c2 = fadd(dpBuf[cur ^ 1][kk], pen);
+                                    if (c2 < best[q])
                                     {
-                                        float c2 = fadd(dpBuf[cur ^ 1][kk], fmul(kSeamSmooth, fabsf((float)(t - (plo + kk)))));
-                                        if (c2 < best[q])
-                                        {
-                                            best[q] = c2;
-                                            bi[q] = kk;
-                                        }
+                                        best[q] = c2;
+                                        bi[q] = kk;
                                     }
                                 }
                             }
-                            float b = best[0];
-                            bp = bi[0];
-#pragma unroll
-                            for (int q = 1; q < 4; ++q)
-                                if (bi[q] >= 0 && (best[q] < b || (best[q] == b && (bp < 0 || bi[q] < bp))))
-                                {
-                                    b = best[q];
-                                    bp = bi[q];
-                                }
-                            val = fadd(c, b);
                         }
+                        b = best[0];
+                        bp = bi[0];
+#pragma unroll
+                        for (int q = 1; q < 4; ++q)
+                            if (bi[q] >= 0 && (best[q] < b || (best[q] == b && (bp < 0 || bi[q] < bp))))
+                            {
+                                b = best[q];
+                                bp = bi[q];
+                            }
+                    }
+                    // Merge with the partner half (the lower half holds lower indices).
+                    {
+                        const float ob = __shfl_xor_sync(0xffffffffu, b, 1);
+                        const int obp = __shfl_xor_sync(0xffffffffu, bp, 1);
+                        const float b0 = half ? ob : b, b1 = half ? b : ob;
+                        const int i0 = half ? obp : bp, i1 = half ? bp : obp;
+                        if (i0 >= 0 && (i1 < 0 || !(b1 < b0)))
+                        {
+                            b = b0;
+                            bp = i0;
+                        }
+                        else
+                        {
+                            b = b1;
+                            bp = i1;
+                        }
+                    }
+                    if (last >= 0 && k < lw) val = fadd(c, b);
+                    if (half == 0 && k < lw)
+                    {
                         dpBuf[cur][k] = val;
                         sBack[(size_t)line * kSeamBand + k] = (unsigned char)(bp < 0 ? 255 : bp);
                     }
                     // Lines skipped between `line` and `nxt` have no predecessor entry.
-                    for (int l2 = line + 1 + k; l2 < nxt; l2 += kDpThreads) sPrev[l2] = -1;
-                    if (k == 0) sPrev[line] = last;
+                    for (int l2 = line + 1 + tid; l2 < nxt; l2 += kDpThreads) sPrev[l2] = -1;
+                    if (tid == 0) sPrev[line] = last;
                     last = line;
                     lastW = lw;
                     cur ^= 1;
@@ -634,7 +780,7 @@ __global__ void __launch_bounds__(kSeamThreads, 1) k_seam(BlendArgs a, const int
                     line = nxt;
                     asm volatile("bar.sync 1, %0;" ::"r"(kDpThreads) : "memory");
                 }
-                if (k == 0)
+                if (tid == 0)
                 {
                     sLast = last;
                     int bestK = 0;
@@ -652,7 +798,7 @@ __global__ void __launch_bounds__(kSeamThreads, 1) k_seam(BlendArgs a, const int
                 }
             }
             __syncthreads();
-
+            if (tid == 0) { long long now = clock64(); atomicAdd(a.seamCycles + 2, (unsigned long long)(now - tp)); tp = now; }
             // Phase 4: backtrack (SeamBlend.cpp:411-428).
             if (tid == 0 && sLast >= 0)
             {
@@ -668,6 +814,7 @@ __global__ void __launch_bounds__(kSeamThreads, 1) k_seam(BlendArgs a, const int
             }
             __syncthreads();
 
+            if (tid == 0) { long long now = clock64(); atomicAdd(a.seamCycles + 3, (unsigned long long)(now - tp)); tp = now; }
             // Phase 5: reassign I/J pixels inside each contested band
             // (SeamBlend.cpp:430-444).
             if (sLast >= 0)
@@ -690,6 +837,7 @@ __global__ void __launch_bounds__(kSeamThreads, 1) k_seam(BlendArgs a, const int
                 }
             }
             __syncthreads();
+            if (tid == 0) atomicAdd(a.seamCycles + 4, (unsigned long long)(clock64() - tp));
         }
     }
 }
@@ -955,7 +1103,8 @@ __global__ void __launch_bounds__(256) k_final0(BlendArgs a, const Unit* __restr
 int dt_rows_in_flight(int maxW)
 {
     size_t row = (size_t)dt_ring_stride(maxW) * sizeof(float);
-    int n = (int)((210 * 1024) / row);
+    int n = (int)((100 * 1024) / row);  // two CTAs per SM
+    if (n < 2) n = (int)((210 * 1024) / row);
     return n > kDtRing ? kDtRing : n;
 }
 
@@ -982,12 +1131,12 @@ int launch_dt(const BlendArgs& a, const int* itemList, int n, bool backward, int
     if (backward)
     {
         cudaFuncSetAttribute(k_dt<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        k_dt<true><<<n, 1024, smem, s>>>(a, itemList, slots);
+        k_dt<true><<<n, 512, smem, s>>>(a, itemList, slots);
     }
     else
     {
         cudaFuncSetAttribute(k_dt<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        k_dt<false><<<n, 1024, smem, s>>>(a, itemList, slots);
+        k_dt<false><<<n, 512, smem, s>>>(a, itemList, slots);
     }
     return check_launch("distance transform kernel");
 }

@@ -67,7 +67,8 @@ struct BlendArgs
 {
     ItemDev* items;
     TileDev* tiles;
-    int* error;  // set non-zero by a kernel that gave up (bounded waits)
+    int* error;                        // set non-zero by a kernel that gave up (bounded waits)
+    unsigned long long* seamCycles;    // per-phase SM cycles of the seam kernel (5 counters)
 };
 
 // Kernel launchers (blend_kernels.cu).

@@ -270,7 +270,7 @@ int Plan::build(const std::vector<TileSpec>& specs, int numBands, bool renderPat
     size_t itemBytes = align256(std::max(nItems, 1) * sizeof(ItemDev));
     size_t tileBytes = align256(std::max(nTiles, 1) * sizeof(TileDev));
     size_t metaOff = bytes;
-    bytes += unitBytes + intBytes + itemBytes + tileBytes + 256;
+    bytes += unitBytes + intBytes + itemBytes + tileBytes + 256 + 256;
     arenaBytes = bytes;
     cudaError_t e = cudaMalloc(&arena, bytes);
     if (e != cudaSuccess)
@@ -311,11 +311,13 @@ int Plan::build(const std::vector<TileSpec>& specs, int numBands, bool renderPat
     dItems = reinterpret_cast<ItemDev*>(base + metaOff + unitBytes + intBytes);
     dTiles = reinterpret_cast<TileDev*>(base + metaOff + unitBytes + intBytes + itemBytes);
     dError = reinterpret_cast<int*>(base + metaOff + unitBytes + intBytes + itemBytes + tileBytes);
+    dSeamCycles = reinterpret_cast<unsigned long long*>(base + metaOff + unitBytes + intBytes + itemBytes + tileBytes + 256);
     I360B_CUDA(cudaMemcpy(dUnits, units.data(), units.size() * sizeof(Unit), cudaMemcpyHostToDevice), "plan upload");
     I360B_CUDA(cudaMemcpy(dInts, ints.data(), ints.size() * sizeof(int), cudaMemcpyHostToDevice), "plan upload");
     if (nItems) I360B_CUDA(cudaMemcpy(dItems, items.data(), nItems * sizeof(ItemDev), cudaMemcpyHostToDevice), "plan upload");
     if (nTiles) I360B_CUDA(cudaMemcpy(dTiles, tiles.data(), nTiles * sizeof(TileDev), cudaMemcpyHostToDevice), "plan upload");
     I360B_CUDA(cudaMemset(dError, 0, sizeof(int)), "plan upload");
+    I360B_CUDA(cudaMemset(dSeamCycles, 0, 5 * sizeof(unsigned long long)), "plan upload");
     seamList = dInts + seamStart;
     return I360B_SUCCESS;
 }
@@ -342,7 +344,7 @@ int Plan::kernels_per_execute() const
 
 int Plan::enqueue(cudaStream_t s, cudaEvent_t* ev)
 {
-    BlendArgs a{dItems, dTiles, dError};
+    BlendArgs a{dItems, dTiles, dError, dSeamCycles};
     auto L = [&](int idx) { return lists[idx]; };
     auto mark = [&](int i) {
         if (ev) cudaEventRecord(ev[i], s);
@@ -621,6 +623,9 @@ extern "C" int i360b_render_plan_stats(i360b_render_plan* plan, void* stream, i3
     dev_free(d, s);
     I360B_CUDA(cudaStreamSynchronize(s), "stats");
     out->coveredItemPixels = (long long)c;
+    unsigned long long cyc[5];
+    I360B_CUDA(cudaMemcpy(cyc, P.dSeamCycles, sizeof(cyc), cudaMemcpyDeviceToHost), "stats");
+    for (int i = 0; i < 5; ++i) out->seamPhaseCycles[i] = (long long)cyc[i];
     return I360B_SUCCESS;
 }
 

@@ -50,6 +50,7 @@ struct Plan
     ItemDev* dItems = nullptr;
     TileDev* dTiles = nullptr;
     int* dError = nullptr;
+    unsigned long long* dSeamCycles = nullptr;
     int* hostErr = nullptr;
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t graphExec = nullptr;

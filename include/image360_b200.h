@@ -205,6 +205,10 @@ typedef struct i360b_render_stats
     long long outputPixels;
     long long coveredItemPixels;
     long long scratchBytes;
+    /* SM cycles spent in the seam kernel's five phases (crossover scan, colour
+     * cost, dynamic program, backtrack, reassignment), summed over tiles and
+     * executions since the plan was created. */
+    long long seamPhaseCycles[5];
 } i360b_render_stats;
 I360B_API int i360b_render_plan_stats(i360b_render_plan* plan, void* stream, i360b_render_stats* out);
 /* Runs the plan once without the graph, timing each stage with CUDA events on
