@@ -160,13 +160,14 @@ __global__ void __launch_bounds__(256) k_warp_tiles(BlendArgs a, const Unit* __r
         const int y = u.by * kBandRows + warp * (kBandRows / 8) + r;
         if (y >= H) break;
         const float dY = (float)(y + it.offY);
+        const bool rowIn = y >= it.vy0 && y <= it.vy1;
         for (int x0 = 0; x0 < W; x0 += 64)
         {
             // Two independent pixels per lane keep more gathers in flight.
             const int xa = x0 + lane, xb = x0 + 32 + lane;
             unsigned short oa[3] = {0, 0, 0}, ob[3] = {0, 0, 0};
-            if (xa < W) warp_px(it, (float)(xa + it.offX), dY, oa);
-            if (xb < W) warp_px(it, (float)(xb + it.offX), dY, ob);
+            if (rowIn && xa < W && xa >= it.vx0 && xa <= it.vx1) warp_px(it, (float)(xa + it.offX), dY, oa);
+            if (rowIn && xb < W && xb >= it.vx0 && xb <= it.vx1) warp_px(it, (float)(xb + it.offX), dY, ob);
             bool ca = (oa[0] | oa[1] | oa[2]) != 0, cb = (ob[0] | ob[1] | ob[2]) != 0;
             if (xa < W)
             {
@@ -453,28 +454,59 @@ __global__ void __launch_bounds__(512, 2) k_dt(BlendArgs a, const int* __restric
     }
 }
 
+
+// A tile's contributor descriptors staged in shared memory: the per-pixel
+// loops below then index shared memory instead of chasing items[k] in global
+// memory for every pixel.
+constexpr int kMaxTileItems = 128;  // above the 127-contributor limit of the blend entry points
+
+struct ItemCache
+{
+    const unsigned short* img[kMaxTileItems];
+    const float* d[kMaxTileItems];
+    const float4* nd[kMaxTileItems];
+    const float* wg[kMaxTileItems];
+    int cnt[kMaxTileItems];
+};
+
+__device__ __forceinline__ void load_item_cache(ItemCache& c, const BlendArgs& a, const TileDev& T)
+{
+    for (int k = threadIdx.x; k < T.numItems && k < kMaxTileItems; k += blockDim.x)
+    {
+        const ItemDev& it = a.items[T.firstItem + k];
+        c.img[k] = it.img;
+        c.d[k] = it.d;
+        c.nd[k] = it.nd;
+        c.wg[k] = it.wg;
+        c.cnt[k] = it.bbox[4];
+    }
+    __syncthreads();
+}
+
 // ---------------------------------------------------------------------------
 // Ownership (SeamBlend.cpp:244-261): argmax over contributors of d > 0,
 // strict '>' so ties keep the lowest index; -1 where nothing covers.
 // ---------------------------------------------------------------------------
 __global__ void __launch_bounds__(256) k_owner(BlendArgs a, const Unit* __restrict__ units)
 {
+    __shared__ ItemCache C;
     const Unit u = units[blockIdx.x];
     const TileDev& T = a.tiles[u.id];
+    load_item_cache(C, a, T);
+    const int K = T.numItems;
+    const long long full = (long long)T.w * T.h;
+    const float kInf = (float)(T.w + T.h);
     const long long base = (long long)u.by * kBandRows * T.w;
-    const long long n = min((long long)kBandRows * T.w, (long long)T.w * T.h - base);
+    const long long n = min((long long)kBandRows * T.w, full - base);
     for (long long q = threadIdx.x; q < n; q += blockDim.x)
     {
         const long long p = base + q;
         int best = -1;
         float bestD = 0.0f;
-        const long long full = (long long)T.w * T.h;
-        const float kInf = (float)(T.w + T.h);
-        for (int k = 0; k < T.numItems; ++k)
+        for (int k = 0; k < K; ++k)
         {
-            const ItemDev& it = a.items[T.firstItem + k];
-            const int cnt = it.bbox[4];
-            float v = cnt == 0 ? 0.0f : ((long long)cnt == full ? kInf : __ldg(it.d + p));
+            const int cnt = C.cnt[k];
+            const float v = cnt == 0 ? 0.0f : ((long long)cnt == full ? kInf : __ldg(C.d[k] + p));
             if (v > bestD)
             {
                 bestD = v;
@@ -858,11 +890,10 @@ struct UpCoef
     float wx, wy;
 };
 
-// Align-corners bilinear resize coefficients (SeamBlend.cpp:85-115).
-__device__ __forceinline__ UpCoef up_coef(int sw, int sh, int dw, int dh, int x, int y)
+// Align-corners bilinear resize coefficients (SeamBlend.cpp:85-115); the
+// scales sx, sy = (src-1)/(dst-1) are computed once per tile and level.
+__device__ __forceinline__ UpCoef up_coef_s(float sx, float sy, int sw, int sh, int x, int y)
 {
-    float sx = (sw > 1) ? fdiv((float)(sw - 1), (float)max(1, dw - 1)) : 0.0f;
-    float sy = (sh > 1) ? fdiv((float)(sh - 1), (float)max(1, dh - 1)) : 0.0f;
     UpCoef c;
     float fy = fmul(sy, (float)y);
     c.y0 = min(__float2int_rz(fy), sh - 1);
@@ -885,7 +916,8 @@ __device__ __forceinline__ float up_mix(float v00, float v10, float v01, float v
 // (SeamBlend.cpp:175-180).
 __device__ __forceinline__ float3 gauss_of(float4 nd)
 {
-    float inv = (nd.w > 1e-6f) ? fdiv(1.0f, nd.w) : 0.0f;
+    // 1.0f / den, correctly rounded (the reference's division).
+    float inv = (nd.w > 1e-6f) ? __frcp_rn(nd.w) : 0.0f;
     return make_float3(fmul(nd.x, inv), fmul(nd.y, inv), fmul(nd.z, inv));
 }
 
@@ -898,10 +930,15 @@ constexpr int kDnSW = 2 * kDnTW + 4, kDnSH = 2 * kDnTH + 4;
 template <bool L0>
 __global__ void __launch_bounds__(256) k_down(BlendArgs a, const Unit* __restrict__ units, int level)
 {
+    // Footprint staged deinterleaved (even / odd columns in separate planes)
+    // so the horizontal taps of consecutive output columns are consecutive
+    // shared-memory words: no bank conflicts.
+    constexpr int HW = kDnSW / 2;
     extern __shared__ float dn_smem[];
-    auto s = reinterpret_cast<float (*)[kDnSH][kDnSW]>(dn_smem);
-    auto t = reinterpret_cast<float (*)[kDnSH][kDnTW]>(dn_smem + 5 * kDnSH * kDnSW);
-    Unit u = units[blockIdx.x];
+    auto E = reinterpret_cast<float (*)[kDnSH][HW]>(dn_smem);
+    auto O = reinterpret_cast<float (*)[kDnSH][HW]>(dn_smem + 5 * kDnSH * HW);
+    auto t = reinterpret_cast<float (*)[kDnSH][kDnTW]>(dn_smem + 10 * kDnSH * HW);
+    const Unit u = units[blockIdx.x];
     const ItemDev& it = a.items[u.id];
     const TileDev& T = a.tiles[it.tile];
     const int sw = T.lw[level], sh = T.lh[level];
@@ -910,57 +947,148 @@ __global__ void __launch_bounds__(256) k_down(BlendArgs a, const Unit* __restric
     const int tid = threadIdx.x;
     const float4* ndS = L0 ? nullptr : it.nd + T.loff[level];
     const float* wgS = L0 ? nullptr : it.wg + T.loff[level];
-    for (int idx = tid; idx < kDnSW * kDnSH; idx += 256)
+    for (int idx = tid; idx < HW * kDnSH; idx += 256)
     {
-        int r = idx / kDnSW, c = idx - r * kDnSW;
-        int gx = min(max(2 * X0 - 2 + c, 0), sw - 1);
-        int gy = min(max(2 * Y0 - 2 + r, 0), sh - 1);
-        size_t p = (size_t)gy * sw + gx;
-        if (L0)
+        const int r = idx / HW, cp = idx - r * HW;
+        const int gy = min(max(2 * Y0 - 2 + r, 0), sh - 1);
+#pragma unroll
+        for (int e = 0; e < 2; ++e)
         {
-            const unsigned short* px = it.img + p * 3;
-            unsigned short r0 = px[0], r1 = px[1], r2 = px[2];
-            float m = (r0 | r1 | r2) ? 1.0f : 0.0f;
-            s[0][r][c] = fmul((float)r0, m);
-            s[1][r][c] = fmul((float)r1, m);
-            s[2][r][c] = fmul((float)r2, m);
-            s[3][r][c] = m;
-            s[4][r][c] = (T.owner[p] == it.k) ? 1.0f : 0.0f;
-        }
-        else
-        {
-            float4 v = ndS[p];
-            s[0][r][c] = v.x;
-            s[1][r][c] = v.y;
-            s[2][r][c] = v.z;
-            s[3][r][c] = v.w;
-            s[4][r][c] = wgS[p];
+            const int gx = min(max(2 * X0 - 2 + 2 * cp + e, 0), sw - 1);
+            const size_t p = (size_t)gy * sw + gx;
+            float v[5];
+            if (L0)
+            {
+                const unsigned short* px = it.img + p * 3;
+                const unsigned short r0 = px[0], r1 = px[1], r2 = px[2];
+                const float m = (r0 | r1 | r2) ? 1.0f : 0.0f;
+                v[0] = fmul((float)r0, m);
+                v[1] = fmul((float)r1, m);
+                v[2] = fmul((float)r2, m);
+                v[3] = m;
+                v[4] = (T.owner[p] == it.k) ? 1.0f : 0.0f;
+            }
+            else
+            {
+                const float4 q = ndS[p];
+                v[0] = q.x;
+                v[1] = q.y;
+                v[2] = q.z;
+                v[3] = q.w;
+                v[4] = wgS[p];
+            }
+#pragma unroll
+            for (int ch = 0; ch < 5; ++ch)
+            {
+                if (e == 0) E[ch][r][cp] = v[ch];
+                else O[ch][r][cp] = v[ch];
+            }
         }
     }
     __syncthreads();
-    // Horizontal taps at the even columns that survive decimation.
+    // Horizontal taps at the even columns that survive decimation:
+    // output i is centred on footprint column 2i + 2.
     for (int idx = tid; idx < 5 * kDnSH * kDnTW; idx += 256)
     {
-        int ch = idx / (kDnSH * kDnTW);
-        int rem = idx - ch * kDnSH * kDnTW;
-        int r = rem / kDnTW, i = rem - r * kDnTW;
-        const float* row = s[ch][r];
-        t[ch][r][i] = blur5(row[2 * i], row[2 * i + 1], row[2 * i + 2], row[2 * i + 3], row[2 * i + 4]);
+        const int ch = idx / (kDnSH * kDnTW);
+        const int rem = idx - ch * kDnSH * kDnTW;
+        const int r = rem / kDnTW, i = rem - r * kDnTW;
+        t[ch][r][i] = blur5(E[ch][r][i], O[ch][r][i], E[ch][r][i + 1], O[ch][r][i + 1], E[ch][r][i + 2]);
     }
     __syncthreads();
     const int i = tid & 31;
     for (int j = tid >> 5; j < kDnTH; j += 8)
     {
-        int X = X0 + i, Y = Y0 + j;
+        const int X = X0 + i, Y = Y0 + j;
         if (X >= dw || Y >= dh) continue;
         float o[5];
 #pragma unroll
         for (int ch = 0; ch < 5; ++ch)
             o[ch] = blur5(t[ch][2 * j][i], t[ch][2 * j + 1][i], t[ch][2 * j + 2][i], t[ch][2 * j + 3][i],
                           t[ch][2 * j + 4][i]);
-        size_t q = T.loff[level + 1] + (size_t)Y * dw + X;
+        const size_t q = T.loff[level + 1] + (size_t)Y * dw + X;
         it.nd[q] = make_float4(o[0], o[1], o[2], o[3]);
         it.wg[q] = o[4];
+    }
+}
+
+// Level 0 -> 1 in integer arithmetic.  At level 0 every blur input is an
+// integer: pixel values (<= 65535, zero where uncovered), the 0/1 coverage
+// and the 0/1 ownership mask.  With the [1,4,6,4,1]/16 kernel each product
+// of the reference's FP32 sequence is exact, every horizontal partial sum is
+// a multiple of 1/16 below 2^16 and every vertical one a multiple of 1/256
+// below 2^16 (at most 24 significant bits), so no step rounds: the level-1
+// value IS (sum_ij c_i c_j v_ij) / 256.  Computing that sum in integers is
+// bit-identical to the FP32 chain of SeamBlend.cpp:15-79.  Coverage and
+// ownership sums (<= 256 each) share one int as den << 16 | weight.
+__global__ void __launch_bounds__(256) k_down0(BlendArgs a, const Unit* __restrict__ units)
+{
+    constexpr int HW = kDnSW / 2;
+    extern __shared__ int dn_ismem[];
+    auto E = reinterpret_cast<int (*)[kDnSH][HW]>(dn_ismem);
+    auto O = reinterpret_cast<int (*)[kDnSH][HW]>(dn_ismem + 4 * kDnSH * HW);
+    auto t = reinterpret_cast<int (*)[kDnSH][kDnTW]>(dn_ismem + 8 * kDnSH * HW);
+    const Unit u = units[blockIdx.x];
+    const ItemDev& it = a.items[u.id];
+    const TileDev& T = a.tiles[it.tile];
+    const int sw = T.lw[0], sh = T.lh[0];
+    const int dw = T.lw[1], dh = T.lh[1];
+    const int X0 = u.bx * kDnTW, Y0 = u.by * kDnTH;
+    const int tid = threadIdx.x;
+    const signed char k = (signed char)it.k;
+    for (int idx = tid; idx < HW * kDnSH; idx += 256)
+    {
+        const int r = idx / HW, cp = idx - r * HW;
+        const int gy = min(max(2 * Y0 - 2 + r, 0), sh - 1);
+#pragma unroll
+        for (int e = 0; e < 2; ++e)
+        {
+            const int gx = min(max(2 * X0 - 2 + 2 * cp + e, 0), sw - 1);
+            const size_t p = (size_t)gy * sw + gx;
+            const unsigned short* px = it.img + p * 3;
+            const int r0 = __ldg(px), r1 = __ldg(px + 1), r2 = __ldg(px + 2);
+            const int m = (r0 | r1 | r2) ? 1 : 0;
+            const int dwv = (m << 16) | (T.owner[p] == k ? 1 : 0);
+            if (e == 0)
+            {
+                E[0][r][cp] = r0;
+                E[1][r][cp] = r1;
+                E[2][r][cp] = r2;
+                E[3][r][cp] = dwv;
+            }
+            else
+            {
+                O[0][r][cp] = r0;
+                O[1][r][cp] = r1;
+                O[2][r][cp] = r2;
+                O[3][r][cp] = dwv;
+            }
+        }
+    }
+    __syncthreads();
+    for (int idx = tid; idx < 4 * kDnSH * kDnTW; idx += 256)
+    {
+        const int ch = idx / (kDnSH * kDnTW);
+        const int rem = idx - ch * kDnSH * kDnTW;
+        const int r = rem / kDnTW, i = rem - r * kDnTW;
+        t[ch][r][i] = E[ch][r][i] + 4 * O[ch][r][i] + 6 * E[ch][r][i + 1] + 4 * O[ch][r][i + 1] + E[ch][r][i + 2];
+    }
+    __syncthreads();
+    const int i = tid & 31;
+    for (int j = tid >> 5; j < kDnTH; j += 8)
+    {
+        const int X = X0 + i, Y = Y0 + j;
+        if (X >= dw || Y >= dh) continue;
+        int S[4];
+#pragma unroll
+        for (int ch = 0; ch < 4; ++ch)
+            S[ch] = t[ch][2 * j][i] + 4 * t[ch][2 * j + 1][i] + 6 * t[ch][2 * j + 2][i] + 4 * t[ch][2 * j + 3][i] +
+                    t[ch][2 * j + 4][i];
+        const float s256 = 1.0f / 256.0f;
+        const size_t q = T.loff[1] + (size_t)Y * dw + X;
+        it.nd[q] = make_float4(fmul((float)S[0], s256), fmul((float)S[1], s256), fmul((float)S[2], s256),
+                               fmul((float)(S[3] >> 16), s256));
+        it.wg[q] = fmul((float)(S[3] & 0xffff), s256);
     }
 }
 
@@ -971,8 +1099,11 @@ __global__ void __launch_bounds__(256) k_down(BlendArgs a, const Unit* __restric
 // exactly +-0, so summing every contributor equals the reference's sum.
 __global__ void __launch_bounds__(256) k_blend_level(BlendArgs a, const Unit* __restrict__ units, int level)
 {
+    __shared__ ItemCache C;
     const Unit u = units[blockIdx.x];
     const TileDev& T = a.tiles[u.id];
+    load_item_cache(C, a, T);
+    const int K = T.numItems;
     const int lw = T.lw[level], lh = T.lh[level];
     const bool top = level == T.bands - 1;
     const int uw = T.lw[level + 1], uh = T.lh[level + 1];
@@ -983,17 +1114,16 @@ __global__ void __launch_bounds__(256) k_blend_level(BlendArgs a, const Unit* __
         const long long pl = base + q;
         const int y = (int)(pl / lw), x = (int)(pl - (long long)y * lw);
         UpCoef c;
-        if (!top) c = up_coef(uw, uh, lw, lh, x, y);
+        if (!top) c = up_coef_s(T.usx[level], T.usy[level], uw, uh, x, y);
         const size_t p = T.loff[level] + pl;
         float acc0 = 0.0f, acc1 = 0.0f, acc2 = 0.0f;
-        for (int k = 0; k < T.numItems; ++k)
+        for (int k = 0; k < K; ++k)
         {
-            const ItemDev& it = a.items[T.firstItem + k];
-            float wv = __ldg(it.wg + p);
-            float3 g = gauss_of(it.nd[p]);
+            float wv = __ldg(C.wg[k] + p);
+            float3 g = gauss_of(C.nd[k][p]);
             if (!top)
             {
-                const float4* up = it.nd + T.loff[level + 1];
+                const float4* up = C.nd[k] + T.loff[level + 1];
                 float3 a00 = gauss_of(up[(size_t)c.y0 * uw + c.x0]);
                 float3 a10 = gauss_of(up[(size_t)c.y0 * uw + c.x1]);
                 float3 a01 = gauss_of(up[(size_t)c.y1 * uw + c.x0]);
@@ -1028,7 +1158,7 @@ __global__ void __launch_bounds__(256) k_collapse(BlendArgs a, const Unit* __res
     {
         const long long pl = base + q;
         const int y = (int)(pl / lw), x = (int)(pl - (long long)y * lw);
-        UpCoef c = up_coef(uw, uh, lw, lh, x, y);
+        UpCoef c = up_coef_s(T.usx[level], T.usy[level], uw, uh, x, y);
         float* b = T.blend + (T.loff[level] + pl) * 3;
 #pragma unroll
         for (int ch = 0; ch < 3; ++ch)
@@ -1047,54 +1177,69 @@ __global__ void __launch_bounds__(256) k_collapse(BlendArgs a, const Unit* __res
 // clamp(that + Up(recon_1)) + 0.5 truncated, and 0 where nobody owns.
 __global__ void __launch_bounds__(256) k_final0(BlendArgs a, const Unit* __restrict__ units)
 {
+    __shared__ ItemCache C;
     const Unit u = units[blockIdx.x];
     const TileDev& T = a.tiles[u.id];
+    load_item_cache(C, a, T);
     const int W = T.w, H = T.h;
     const int uw = T.lw[1], uh = T.lh[1];
+    const float* rc = T.blend + T.loff[1] * 3;
     const long long base = (long long)u.by * kBandRows * W;
     const long long n = min((long long)kBandRows * W, (long long)W * H - base);
-    for (long long q = threadIdx.x; q < n; q += blockDim.x)
+    constexpr int B = 4;  // pixels per thread in flight
+    for (long long q0 = threadIdx.x; q0 < n; q0 += (long long)blockDim.x * B)
     {
-        const long long p = base + q;
-        const int y = (int)(p / W), x = (int)(p - (long long)y * W);
-        unsigned short* o = T.out + p * 3;
-        const int own = T.owner[p];
-        if (own < 0)
+        int own[B];
+        long long pp[B];
+#pragma unroll
+        for (int b = 0; b < B; ++b)
         {
-            o[0] = o[1] = o[2] = 0;
-            continue;
+            pp[b] = base + q0 + (long long)b * blockDim.x;
+            own[b] = (q0 + (long long)b * blockDim.x < n) ? (int)T.owner[pp[b]] : -2;
         }
-        const ItemDev& it = a.items[T.firstItem + own];
-        const unsigned short* px = it.img + p * 3;
-        float r[3] = {(float)px[0], (float)px[1], (float)px[2]};
-        if (T.bands > 1)
+#pragma unroll
+        for (int b = 0; b < B; ++b)
         {
-            UpCoef c = up_coef(uw, uh, W, H, x, y);
-            const float4* g1 = it.nd + T.loff[1];
-            float3 a00 = gauss_of(g1[(size_t)c.y0 * uw + c.x0]);
-            float3 a10 = gauss_of(g1[(size_t)c.y0 * uw + c.x1]);
-            float3 a01 = gauss_of(g1[(size_t)c.y1 * uw + c.x0]);
-            float3 a11 = gauss_of(g1[(size_t)c.y1 * uw + c.x1]);
-            float lap[3] = {fsub(r[0], up_mix(a00.x, a10.x, a01.x, a11.x, c.wx, c.wy)),
-                            fsub(r[1], up_mix(a00.y, a10.y, a01.y, a11.y, c.wx, c.wy)),
-                            fsub(r[2], up_mix(a00.z, a10.z, a01.z, a11.z, c.wx, c.wy))};
-            const float* rc = T.blend + T.loff[1] * 3;
+            if (own[b] == -2) continue;
+            const long long p = pp[b];
+            unsigned short* o = T.out + p * 3;
+            if (own[b] < 0)
+            {
+                o[0] = o[1] = o[2] = 0;
+                continue;
+            }
+            const int y = (int)(p / W), x = (int)(p - (long long)y * W);
+            const unsigned short* px = C.img[own[b]] + p * 3;
+            float r[3] = {(float)__ldg(px), (float)__ldg(px + 1), (float)__ldg(px + 2)};
+            if (T.bands > 1)
+            {
+                const UpCoef c = up_coef_s(T.usx[0], T.usy[0], uw, uh, x, y);
+                const float4* g1 = C.nd[own[b]] + T.loff[1];
+                const float3 a00 = gauss_of(__ldg(g1 + (size_t)c.y0 * uw + c.x0));
+                const float3 a10 = gauss_of(__ldg(g1 + (size_t)c.y0 * uw + c.x1));
+                const float3 a01 = gauss_of(__ldg(g1 + (size_t)c.y1 * uw + c.x0));
+                const float3 a11 = gauss_of(__ldg(g1 + (size_t)c.y1 * uw + c.x1));
+                const float lap[3] = {fsub(r[0], up_mix(a00.x, a10.x, a01.x, a11.x, c.wx, c.wy)),
+                                      fsub(r[1], up_mix(a00.y, a10.y, a01.y, a11.y, c.wx, c.wy)),
+                                      fsub(r[2], up_mix(a00.z, a10.z, a01.z, a11.z, c.wx, c.wy))};
+#pragma unroll
+                for (int ch = 0; ch < 3; ++ch)
+                {
+                    const float up = up_mix(__ldg(rc + ((size_t)c.y0 * uw + c.x0) * 3 + ch),
+                                            __ldg(rc + ((size_t)c.y0 * uw + c.x1) * 3 + ch),
+                                            __ldg(rc + ((size_t)c.y1 * uw + c.x0) * 3 + ch),
+                                            __ldg(rc + ((size_t)c.y1 * uw + c.x1) * 3 + ch), c.wx, c.wy);
+                    r[ch] = fadd(lap[ch], up);
+                }
+            }
 #pragma unroll
             for (int ch = 0; ch < 3; ++ch)
             {
-                float up = up_mix(rc[((size_t)c.y0 * uw + c.x0) * 3 + ch], rc[((size_t)c.y0 * uw + c.x1) * 3 + ch],
-                                  rc[((size_t)c.y1 * uw + c.x0) * 3 + ch], rc[((size_t)c.y1 * uw + c.x1) * 3 + ch],
-                                  c.wx, c.wy);
-                r[ch] = fadd(lap[ch], up);
+                float v = r[ch];
+                v = v < 65535.0f ? v : 65535.0f;
+                v = 0.0f < v ? v : 0.0f;
+                o[ch] = (unsigned short)__float2uint_rz(fadd(v, 0.5f));
             }
-        }
-#pragma unroll
-        for (int ch = 0; ch < 3; ++ch)
-        {
-            float v = r[ch];
-            v = v < 65535.0f ? v : 65535.0f;
-            v = 0.0f < v ? v : 0.0f;
-            o[ch] = (unsigned short)__float2uint_rz(fadd(v, 0.5f));
         }
     }
 }
@@ -1165,11 +1310,12 @@ int launch_seam(const BlendArgs& a, const int* tileList, int n, cudaStream_t s)
 int launch_down(const BlendArgs& a, const Unit* units, int n, int level, cudaStream_t s)
 {
     if (n <= 0) return I360B_SUCCESS;
-    const int smem = (5 * kDnSH * kDnSW + 5 * kDnSH * kDnTW) * (int)sizeof(float);
+    const int smem = (10 * kDnSH * (kDnSW / 2) + 5 * kDnSH * kDnTW) * (int)sizeof(float);
     if (level == 0)
     {
-        cudaFuncSetAttribute(k_down<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-        k_down<true><<<n, 256, smem, s>>>(a, units, level);
+        const int ismem = (8 * kDnSH * (kDnSW / 2) + 4 * kDnSH * kDnTW) * (int)sizeof(int);
+        cudaFuncSetAttribute(k_down0, cudaFuncAttributeMaxDynamicSharedMemorySize, ismem);
+        k_down0<<<n, 256, ismem, s>>>(a, units);
     }
     else
     {

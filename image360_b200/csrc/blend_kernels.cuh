@@ -30,6 +30,7 @@ struct ItemDev
     float gain;
     int tile;
     int k;                      // contributor index inside its tile
+    int vx0, vy0, vx1, vy1;     // tile-local box outside which the warp is surely (0,0,0)
 };
 
 struct TileDev
@@ -44,6 +45,7 @@ struct TileDev
     unsigned short* out;
     int lw[kMaxBands], lh[kMaxBands];
     long long loff[kMaxBands];  // pixel offset of level l (l >= 1) in the per-level arrays
+    float usx[kMaxBands], usy[kMaxBands];  // align-corners scales of Up(level l+1 -> l), FP32 as SeamBlend.cpp:89-90
     // seam scratch
     int* lo;
     int* hi;

@@ -23,6 +23,11 @@ struct DemosaicParams
     float rgbCam[12];
     uint32_t filters;
     unsigned short black;
+    // Standard Bayer layout (2x2-periodic, one R, one B, G on a diagonal):
+    // colour of site (y & 1, x & 1), else std2x2 = 0 and only the generic
+    // path runs.
+    int std2x2;
+    int color2x2[4];
 };
 
 __device__ __forceinline__ int bayer_color(int row, int col, uint32_t filters)
@@ -31,10 +36,44 @@ __device__ __forceinline__ int bayer_color(int row, int col, uint32_t filters)
     return (int)((filters >> ((((row << 1) & 14) | (col & 1)) << 1)) & 3u);
 }
 
+// 3x3 same-colour average of DemosaicPixel (BayerDemosaicKernels.h:25-60) for
+// any filter word and any position (borders average fewer neighbours).
+__device__ __forceinline__ void demosaic_generic(const float (*s)[kDmTW + 2], int lx, int ly, int x, int y,
+                                                 int w, int h, uint32_t filters, float rgb[3])
+{
+    float acc[3] = {0.0f, 0.0f, 0.0f};
+    int cnt[3] = {0, 0, 0};
+#pragma unroll
+    for (int dy = -1; dy <= 1; ++dy)
+#pragma unroll
+        for (int dx = -1; dx <= 1; ++dx)
+        {
+            int nx = x + dx, ny = y + dy;
+            if (nx < 0 || ny < 0 || nx >= w || ny >= h) continue;
+            int ch = bayer_color(ny, nx, filters);
+            int slot = ch == 3 ? 1 : ch;
+            float v = s[ly + 1 + dy][lx + 1 + dx];
+            // Integer-valued sums below 2^24: exact in any order.
+            if (slot == 0) { acc[0] += v; cnt[0]++; }
+            else if (slot == 1) { acc[1] += v; cnt[1]++; }
+            else { acc[2] += v; cnt[2]++; }
+        }
+    int mine = bayer_color(y, x, filters);
+    int my = mine == 3 ? 1 : mine;
+#pragma unroll
+    for (int c = 0; c < 3; ++c)
+    {
+        float v = acc[c];
+        if (c == my) v = s[ly + 1][lx + 1];
+        else if (cnt[c] != 0) v = fdiv(v, (float)cnt[c]);
+        rgb[c] = v;
+    }
+}
+
 __global__ void __launch_bounds__(256) k_demosaic(const unsigned short* __restrict__ cfa, int w, int h,
                                                   DemosaicParams P, unsigned short* __restrict__ out)
 {
-    __shared__ unsigned short s[kDmTH + 2][kDmTW + 2];
+    __shared__ float s[kDmTH + 2][kDmTW + 2];
     const int tx0 = blockIdx.x * kDmTW, ty0 = blockIdx.y * kDmTH;
     const int tid = threadIdx.y * 32 + threadIdx.x;
     for (int i = tid; i < (kDmTH + 2) * (kDmTW + 2); i += 256)
@@ -48,57 +87,99 @@ __global__ void __launch_bounds__(256) k_demosaic(const unsigned short* __restri
             raw = raw > P.black ? (unsigned short)(raw - P.black) : (unsigned short)0;
             v = clamp_trunc_u16(fmul((float)raw, P.camMul[bayer_color(gy, gx, P.filters)]));
         }
-        s[r][c] = v;
+        s[r][c] = (float)v;
     }
     __syncthreads();
+    const bool evenW = (w & 1) == 0;
+    // The quad's 4x4 neighbourhood, read once.
+    float nb[4][4];
+#pragma unroll
+    for (int r = 0; r < 4; ++r)
+#pragma unroll
+        for (int c = 0; c < 4; ++c) nb[r][c] = s[threadIdx.y * 2 + r][threadIdx.x * 2 + c];
 #pragma unroll
     for (int oy = 0; oy < 2; ++oy)
+    {
+        unsigned short px[2][3];
+        const int ly = threadIdx.y * 2 + oy, y = ty0 + ly;
 #pragma unroll
         for (int ox = 0; ox < 2; ++ox)
         {
-            int lx = threadIdx.x * 2 + ox, ly = threadIdx.y * 2 + oy;
-            int x = tx0 + lx, y = ty0 + ly;
-            if (x >= w || y >= h) continue;
-            float rgb[3] = {0.0f, 0.0f, 0.0f};
-            int cnt[3] = {0, 0, 0};
-#pragma unroll
-            for (int dy = -1; dy <= 1; ++dy)
-#pragma unroll
-                for (int dx = -1; dx <= 1; ++dx)
-                {
-                    int nx = x + dx, ny = y + dy;
-                    if (nx < 0 || ny < 0 || nx >= w || ny >= h) continue;
-                    int ch = bayer_color(ny, nx, P.filters);
-                    int slot = ch == 3 ? 1 : ch;
-                    float v = (float)s[ly + 1 + dy][lx + 1 + dx];
-                    // Integer-valued sums below 2^24: exact in any order.
-                    if (slot == 0) { rgb[0] += v; cnt[0]++; }
-                    else if (slot == 1) { rgb[1] += v; cnt[1]++; }
-                    else { rgb[2] += v; cnt[2]++; }
-                }
-            int mine = bayer_color(y, x, P.filters);
-            int my = mine == 3 ? 1 : mine;
-            float own = (float)s[ly + 1][lx + 1];
-            unsigned short px[3];
-#pragma unroll
-            for (int c = 0; c < 3; ++c)
+            const int lx = threadIdx.x * 2 + ox, x = tx0 + lx;
+            float R = 0.0f, G = 0.0f, B = 0.0f;
+            if (P.std2x2 && x >= 1 && y >= 1 && x < w - 1 && y < h - 1)
             {
-                float v = rgb[c];
-                if (c == my) v = own;
-                else if (cnt[c] != 0) v = fdiv(v, (float)cnt[c]);
-                px[c] = clamp_trunc_u16(v);
+                // Interior of a standard Bayer layout: the same-colour
+                // neighbours are the cross (4), the diagonals (4), or a
+                // horizontal / vertical pair (2 each); dividing by 4 or 2 is
+                // exact, so these are the reference's averages bit for bit.
+                // quad-local neighbourhood: centre at nb[oy + 1][ox + 1]
+                const float c = nb[oy + 1][ox + 1];
+                const float n = nb[oy][ox + 1], so = nb[oy + 2][ox + 1];
+                const float we = nb[oy + 1][ox], ea = nb[oy + 1][ox + 2];
+                const int cls = P.color2x2[((y & 1) << 1) | (x & 1)];
+                if (cls != 1)
+                {
+                    const float cross = ((n + we) + ea) + so;
+                    const float diag = ((nb[oy][ox] + nb[oy][ox + 2]) + nb[oy + 2][ox]) + nb[oy + 2][ox + 2];
+                    G = fmul(cross, 0.25f);
+                    const float other = fmul(diag, 0.25f);
+                    R = cls == 0 ? c : other;
+                    B = cls == 0 ? other : c;
+                }
+                else
+                {
+                    const int hc = P.color2x2[((y & 1) << 1) | ((x + 1) & 1)];  // colour of the left/right pair
+                    const float hp = fmul(we + ea, 0.5f), vp = fmul(n + so, 0.5f);
+                    G = c;
+                    R = hc == 0 ? hp : vp;
+                    B = hc == 0 ? vp : hp;
+                }
             }
-            float r = (float)px[0], g = (float)px[1], b = (float)px[2];
-            unsigned short* o = out + ((size_t)y * w + x) * 3;
+            else if (x < w && y < h)
+            {
+                float rgb[3];
+                demosaic_generic(s, lx, ly, x, y, w, h, P.filters, rgb);
+                R = rgb[0];
+                G = rgb[1];
+                B = rgb[2];
+            }
+            // Truncate to uint16 (DemosaicPixel), then the 3x4 colour matrix
+            // (ApplyColorMatrixPixel, BayerDemosaicKernels.h:64-75).
+            const float r = (float)clamp_trunc_u16(R), g = (float)clamp_trunc_u16(G), b = (float)clamp_trunc_u16(B);
 #pragma unroll
             for (int row = 0; row < 3; ++row)
             {
                 float val = fadd(fadd(fadd(fmul(P.rgbCam[row * 4 + 0], r), fmul(P.rgbCam[row * 4 + 1], g)),
                                       fmul(P.rgbCam[row * 4 + 2], b)),
                                  P.rgbCam[row * 4 + 3]);
-                o[row] = clamp_trunc_u16(val);
+                px[ox][row] = clamp_trunc_u16(val);
             }
         }
+        const int x0 = tx0 + threadIdx.x * 2;
+        if (y >= h || x0 >= w) continue;
+        unsigned short* o = out + ((size_t)y * w + x0) * 3;
+        if (evenW && x0 + 1 < w)
+        {
+            // x0 even and w even: 12 bytes at a 4-byte-aligned address.
+            uint32_t* o32 = reinterpret_cast<uint32_t*>(o);
+            o32[0] = (uint32_t)px[0][0] | ((uint32_t)px[0][1] << 16);
+            o32[1] = (uint32_t)px[0][2] | ((uint32_t)px[1][0] << 16);
+            o32[2] = (uint32_t)px[1][1] | ((uint32_t)px[1][2] << 16);
+        }
+        else
+        {
+            o[0] = px[0][0];
+            o[1] = px[0][1];
+            o[2] = px[0][2];
+            if (x0 + 1 < w)
+            {
+                o[3] = px[1][0];
+                o[4] = px[1][1];
+                o[5] = px[1][2];
+            }
+        }
+    }
 }
 
 // ---------------------------------------------------------------------------
@@ -279,6 +360,23 @@ int launch_demosaic(const unsigned short* cfa, int w, int h, unsigned short blac
     for (int i = 0; i < 12; ++i) P.rgbCam[i] = rgbCam[i];
     P.filters = filters;
     P.black = black;
+    // Standard Bayer layout test on the filter word (rows repeat with period
+    // 2; one R, one B, G/G2 on a diagonal).
+    {
+        auto col = [&](int r, int c) { return (int)((filters >> ((((r << 1) & 14) | (c & 1)) << 1)) & 3u); };
+        bool periodic = true;
+        for (int r = 2; r < 8; ++r)
+            for (int c = 0; c < 2; ++c) periodic = periodic && col(r, c) == col(r & 1, c);
+        int c00 = col(0, 0), c01 = col(0, 1), c10 = col(1, 0), c11 = col(1, 1);
+        auto isG = [](int v) { return v == 1 || v == 3; };
+        bool diagG = (isG(c00) && isG(c11) && ((c01 == 0 && c10 == 2) || (c01 == 2 && c10 == 0))) ||
+                     (isG(c01) && isG(c10) && ((c00 == 0 && c11 == 2) || (c00 == 2 && c11 == 0)));
+        P.std2x2 = (periodic && diagG) ? 1 : 0;
+        P.color2x2[0] = isG(c00) ? 1 : c00;
+        P.color2x2[1] = isG(c01) ? 1 : c01;
+        P.color2x2[2] = isG(c10) ? 1 : c10;
+        P.color2x2[3] = isG(c11) ? 1 : c11;
+    }
     dim3 grid((w + kDmTW - 1) / kDmTW, (h + kDmTH - 1) / kDmTH);
     k_demosaic<<<grid, dim3(32, 8), 0, s>>>(cfa, w, h, P, out);
     return check_launch("demosaic kernel");

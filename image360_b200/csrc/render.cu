@@ -168,6 +168,15 @@ int Plan::build(const std::vector<TileSpec>& specs, int numBands, bool renderPat
             T.loff[l] = acc;
             if (l < T.bands) acc += (long long)T.lw[l] * T.lh[l];
         }
+        for (int l = 0; l + 1 < kMaxBands; ++l)
+        {
+            // SeamBlend.cpp:89-90: (w-1)/max(1, outW-1), 0 when w <= 1 (host
+            // float division is IEEE round-to-nearest, as on the device).
+            const int sw = T.lw[l + 1], sh = T.lh[l + 1], dw = T.lw[l], dh = T.lh[l];
+            T.usx[l] = (sw > 1) ? (float)(sw - 1) / (float)std::max(1, dw - 1) : 0.0f;
+            T.usy[l] = (sh > 1) ? (float)(sh - 1) / (float)std::max(1, dh - 1) : 0.0f;
+        }
+        T.usx[kMaxBands - 1] = T.usy[kMaxBands - 1] = 0.0f;
         size_t pyrPx = (size_t)acc;
         maxW = std::max(maxW, S.w);
         size_t px = (size_t)S.w * S.h;
@@ -195,6 +204,10 @@ int Plan::build(const std::vector<TileSpec>& specs, int numBands, bool renderPat
             for (int q = 0; q < 9; ++q) it.H[q] = I.H[q];
             it.offX = I.offX;
             it.offY = I.offY;
+            it.vx0 = I.vx0;
+            it.vy0 = I.vy0;
+            it.vx1 = I.vx1;
+            it.vy1 = I.vy1;
             Off o{};
             if (renderPath) { o.warped = bytes; bytes += align256(px * 6); }
             o.cov = bytes; bytes += align256((size_t)S.h * T.covWords * 4);
@@ -554,6 +567,34 @@ extern "C" int i360b_render_plan_create(const i360b_frame* frames, int numFrames
             for (int q = 0; q < 9; ++q) it.H[q] = H[(size_t)idx * 9 + q];
             it.offX = off[2 * idx];
             it.offY = off[2 * idx + 1];
+            // Canvas footprint of the frame (corners through the FP64
+            // homography) in tile coordinates, widened by 2 px: outside it
+            // every destination pixel maps outside the source, so the tile
+            // warp writes (0,0,0) there without evaluating the mapping.  Only
+            // used when the frame->canvas map keeps w > 0 at the corners.
+            {
+                const double* m = F.toCanvas;
+                double mnx = 1e300, mny = 1e300, mxx = -1e300, mxy = -1e300;
+                bool ok = true;
+                const double cx[4] = {0.0, (double)F.width, 0.0, (double)F.width};
+                const double cy[4] = {0.0, 0.0, (double)F.height, (double)F.height};
+                for (int q = 0; q < 4; ++q)
+                {
+                    double wq = m[6] * cx[q] + m[7] * cy[q] + m[8];
+                    if (!(wq > 1e-9)) { ok = false; break; }
+                    double px = (m[0] * cx[q] + m[1] * cy[q] + m[2]) / wq;
+                    double py = (m[3] * cx[q] + m[4] * cy[q] + m[5]) / wq;
+                    mnx = std::min(mnx, px); mxx = std::max(mxx, px);
+                    mny = std::min(mny, py); mxy = std::max(mxy, py);
+                }
+                if (ok)
+                {
+                    it.vx0 = (int)std::max(-1.0, std::floor(mnx - 2.0 - T.x));
+                    it.vy0 = (int)std::max(-1.0, std::floor(mny - 2.0 - T.y));
+                    it.vx1 = (int)std::min((double)T.width, std::ceil(mxx + 2.0 - T.x));
+                    it.vy1 = (int)std::min((double)T.height, std::ceil(mxy + 2.0 - T.y));
+                }
+            }
             specs[t].items.push_back(it);
         }
     }

@@ -17,6 +17,8 @@ struct ItemSpec
     float H[9] = {1, 0, 0, 0, 1, 0, 0, 0, 1};
     int offX = 0, offY = 0;
     float gain = 1.0f;
+    // Tile-local box outside which the warp is surely empty (default: all).
+    int vx0 = 0, vy0 = 0, vx1 = 0x3fffffff, vy1 = 0x3fffffff;
 };
 
 struct TileSpec

@@ -24,7 +24,7 @@ def test_initialize_and_info(backend):
 
 
 @pytest.mark.parametrize("w,h", [(24, 20), (1, 1), (2, 3), (37, 29), (640, 480), (1001, 77)])
-@pytest.mark.parametrize("filters", [synth.RGGB, 0x16161616, 0x61616161, 0x49494949])
+@pytest.mark.parametrize("filters", [synth.RGGB, 0x16161616, 0x61616161, 0x49494949, 0x1E1E1E1E, 0xB4B4B4B4, 0x94616194])
 def test_demosaic_exact(backend, oracle_c, w, h, filters):
     rng = np.random.default_rng(w * 1000 + h)
     cfa = rng.integers(0, 16384, (h, w), dtype=np.uint16)
@@ -148,3 +148,26 @@ def test_blend_empty_and_single(backend, oracle_c):
     zero = np.zeros((h, w, 3), np.uint16)
     assert backend.blend_chunk_contributors([zero, full, zero], w, h, out, 5) == ComputeResult.SUCCESS
     assert np.array_equal(out, oracle_c.blend([zero, full, zero], 5))
+
+
+def test_blend_many_contributors(backend, oracle_c):
+    # More contributors than a render tile allows (32): the single-chunk blend
+    # accepts up to 127, as the reference's SeamBlend has no cap.
+    rng = np.random.default_rng(77)
+    w, h = 61, 47
+    bufs = [_rand_buf(rng, w, h) for _ in range(40)]
+    out = np.zeros((h, w, 3), np.uint16)
+    assert backend.blend_chunk_contributors(bufs, w, h, out, 4) == ComputeResult.SUCCESS, backend.get_last_error()
+    assert np.array_equal(out, oracle_c.blend(bufs, 4))
+
+
+def test_invalid_params(backend):
+    o = np.zeros((4, 4, 3), np.uint16)
+    assert backend.median_stack([o] * 33, o, 4, 4) == ComputeResult.INVALID_PARAM
+    assert backend.get_last_error() == "numInputs must be 1-32."
+    assert backend.median_stack([], o, 4, 4) == ComputeResult.INVALID_PARAM
+    assert backend.warp_perspective(o, np.zeros((0, 4, 3), np.uint16), np.eye(3)) == ComputeResult.INVALID_PARAM
+    assert backend.get_last_error() == "Invalid dimensions."
+    assert backend.apply_gain(np.zeros(0, np.uint16), 2.0) == ComputeResult.INVALID_PARAM
+    assert backend.blend_chunk_contributors([o] * 128, 4, 4, o) == ComputeResult.INVALID_PARAM
+    assert backend.blend_chunk_contributors([o], 4, 4, o, 0) == ComputeResult.INVALID_PARAM

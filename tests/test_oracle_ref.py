@@ -9,7 +9,7 @@ RGB = np.array([[1.9, -0.7, -0.2, 0.0], [-0.3, 1.5, -0.2, 0.0], [0.0, -0.4, 1.6,
 
 
 @pytest.mark.parametrize("w,h", [(24, 20), (1, 1), (2, 3), (37, 29), (3, 1)])
-@pytest.mark.parametrize("filters", [0x94949494, 0x16161616, 0x61616161, 0x49494949])
+@pytest.mark.parametrize("filters", [0x94949494, 0x16161616, 0x61616161, 0x49494949, 0x1E1E1E1E, 0xB4B4B4B4, 0x94616194])
 def test_demosaic(oracle_c, reference, w, h, filters):
     rng = np.random.default_rng(w * 31 + h)
     cfa = rng.integers(0, 65536, (h, w), dtype=np.uint16)
