@@ -559,7 +559,11 @@ __global__ void __launch_bounds__(kSeamThreads, 1) k_seam(BlendArgs a, const int
     int* sLo = inSmem ? reinterpret_cast<int*>(sm_seam) : T.lo;
     int* sHi = inSmem ? sLo + smemLines : T.hi;
     int* sPrev = inSmem ? sHi + smemLines : T.prevLine;
-    unsigned char* sBack = inSmem ? reinterpret_cast<unsigned char*>(sPrev + smemLines) : T.back;
+    // Contested lines in increasing order (the DP's iteration list).
+    int* sList = inSmem ? sPrev + smemLines : T.list;
+    unsigned char* sBack = inSmem ? reinterpret_cast<unsigned char*>(sList + smemLines) : T.back;
+    __shared__ int sWarpCnt[kSeamThreads / 32 + 1];
+    __shared__ int sNumContested;
 
     for (int i = 0; i < K; ++i)
     {
@@ -718,27 +722,78 @@ __global__ void __launch_bounds__(kSeamThreads, 1) k_seam(BlendArgs a, const int
             __syncthreads();
 
             if (tid == 0) { long long now = clock64(); atomicAdd(a.seamCycles + 1, (unsigned long long)(now - tp)); tp = now; }
-            // Phase 3: dynamic program over contested lines (SeamBlend.cpp:362-407)
-            // on the first kDpThreads threads: thread pairs share a candidate k,
-            // each scanning half of the previous line's entries in four
-            // interleaved chains; the halves merge with the lowest-index rule
-            // of the reference's strict '<' scan.  Penalties 2|t - pt| are
-            // exact small integers, formed in float without conversions.
+            // Phase 3a: compact the contested lines (hi >= lo) in order.
+            {
+                const int per = (numLines + kSeamThreads - 1) / kSeamThreads;  // lines per thread, contiguous
+                const int l0 = tid * per, l1 = min(l0 + per, numLines);
+                int c = 0;
+                for (int l = l0; l < l1; ++l) c += sHi[l] >= sLo[l] ? 1 : 0;
+                int incl = c;
+#pragma unroll
+                for (int d = 1; d < 32; d <<= 1)
+                {
+                    int v = __shfl_up_sync(kFull, incl, d);
+                    if (lane >= d) incl += v;
+                }
+                if (lane == 31) sWarpCnt[warp] = incl;
+                __syncthreads();
+                if (tid == 0)
+                {
+                    int acc = 0;
+                    for (int w2 = 0; w2 < nwarps; ++w2)
+                    {
+                        int v = sWarpCnt[w2];
+                        sWarpCnt[w2] = acc;
+                        acc += v;
+                    }
+                    sNumContested = acc;
+                }
+                __syncthreads();
+                int pos = sWarpCnt[warp] + incl - c;
+                for (int l = l0; l < l1; ++l)
+                {
+                    sPrev[l] = -1;
+                    if (sHi[l] >= sLo[l]) sList[pos++] = l;
+                }
+                __syncthreads();
+            }
+            // Phase 3b: dynamic program over contested lines
+            // (SeamBlend.cpp:362-407) on the first kDpThreads threads: thread
+            // pairs share a candidate k, each scanning half of the previous
+            // line's entries in four interleaved chains; the halves merge with
+            // the lowest-index rule of the reference's strict '<' scan.
+            // Penalties 2|t - pt| are exact small integers formed in float.
+            // Candidate costs are fetched kPre lines ahead.
             if (tid < kDpThreads)
             {
+                constexpr int kPre = 4;
                 const int k = tid >> 1, half = tid & 1;
-                int last = -1, cur = 0, lastW = 0;
-                int line = 0;
-                while (line < numLines && sHi[line] < sLo[line]) ++line;
-                float c = 0.0f;
-                if (line < numLines && k <= sHi[line] - sLo[line]) c = T.cost[(size_t)line * kSeamBand + k];
-                while (line < numLines)
+                const int nC = sNumContested;
+                float cq[kPre];
+#pragma unroll
+                for (int q = 0; q < kPre; ++q)
                 {
+                    cq[q] = 0.0f;
+                    if (q < nC)
+                    {
+                        const int l = sList[q];
+                        if (k <= sHi[l] - sLo[l]) cq[q] = T.cost[(size_t)l * kSeamBand + k];
+                    }
+                }
+                int last = -1, cur = 0, lastW = 0;
+                for (int ci2 = 0; ci2 < nC; ++ci2)
+                {
+                    const int line = sList[ci2];
                     const int lo = sLo[line], lw = sHi[line] - lo + 1;
-                    int nxt = line + 1;
-                    while (nxt < numLines && sHi[nxt] < sLo[nxt]) ++nxt;
-                    float cn = 0.0f;
-                    if (nxt < numLines && k <= sHi[nxt] - sLo[nxt]) cn = T.cost[(size_t)nxt * kSeamBand + k];
+                    const float c = cq[0];
+#pragma unroll
+                    for (int q = 0; q + 1 < kPre; ++q) cq[q] = cq[q + 1];
+                    cq[kPre - 1] = 0.0f;
+                    if (ci2 + kPre < nC)
+                    {
+                        const int l = sList[ci2 + kPre];
+                        if (k <= sHi[l] - sLo[l]) cq[kPre - 1] = T.cost[(size_t)l * kSeamBand + k];
+                    }
                     float val = c;
                     int bp = -1;
                     float b = FLT_MAX;
@@ -802,14 +857,10 @@ __global__ void __launch_bounds__(kSeamThreads, 1) k_seam(BlendArgs a, const int
                         dpBuf[cur][k] = val;
                         sBack[(size_t)line * kSeamBand + k] = (unsigned char)(bp < 0 ? 255 : bp);
                     }
-                    // Lines skipped between `line` and `nxt` have no predecessor entry.
-                    for (int l2 = line + 1 + tid; l2 < nxt; l2 += kDpThreads) sPrev[l2] = -1;
                     if (tid == 0) sPrev[line] = last;
                     last = line;
                     lastW = lw;
                     cur ^= 1;
-                    c = cn;
-                    line = nxt;
                     asm volatile("bar.sync 1, %0;" ::"r"(kDpThreads) : "memory");
                 }
                 if (tid == 0)
@@ -1300,7 +1351,7 @@ int launch_seam(const BlendArgs& a, const int* tileList, int n, cudaStream_t s)
     // Per-line state (lo, hi, prev: 3 ints; back pointers: kSeamBand bytes)
     // is kept in shared memory for lines up to this count.
     const int smemLines = 3072;
-    size_t smem = (size_t)smemLines * (3 * sizeof(int) + kSeamBand);
+    size_t smem = (size_t)smemLines * (4 * sizeof(int) + kSeamBand);
     if (n <= 0) return I360B_SUCCESS;
     cudaFuncSetAttribute(k_seam, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     k_seam<<<n, kSeamThreads, smem, s>>>(a, tileList, smemLines);

@@ -51,6 +51,7 @@ struct TileDev
     int* hi;
     int* prevLine;
     int* chosen;
+    int* list;
     float* cost;
     unsigned char* back;
     int maxLines;

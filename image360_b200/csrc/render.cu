@@ -129,7 +129,7 @@ int Plan::build(const std::vector<TileSpec>& specs, int numBands, bool renderPat
     std::vector<Off> itemOff;
     struct TOff
     {
-        size_t owner, blend, lo, hi, prev, chosen, cost, back;
+        size_t owner, blend, lo, hi, prev, chosen, list, cost, back;
     };
     std::vector<TOff> tileOff(nTiles);
     maxW = 1;
@@ -188,6 +188,7 @@ int Plan::build(const std::vector<TileSpec>& specs, int numBands, bool renderPat
         to.hi = bytes; bytes += align256(ml * 4);
         to.prev = bytes; bytes += align256(ml * 4);
         to.chosen = bytes; bytes += align256(ml * 4);
+        to.list = bytes; bytes += align256(ml * 4);
         to.cost = bytes; bytes += align256(ml * kSeamBand * 4);
         to.back = bytes; bytes += align256(ml * kSeamBand);
         for (int k = 0; k < T.numItems; ++k)
@@ -304,6 +305,7 @@ int Plan::build(const std::vector<TileSpec>& specs, int numBands, bool renderPat
         T.hi = reinterpret_cast<int*>(base + to.hi);
         T.prevLine = reinterpret_cast<int*>(base + to.prev);
         T.chosen = reinterpret_cast<int*>(base + to.chosen);
+        T.list = reinterpret_cast<int*>(base + to.list);
         T.cost = reinterpret_cast<float*>(base + to.cost);
         T.back = reinterpret_cast<unsigned char*>(base + to.back);
     }

@@ -171,3 +171,22 @@ def test_invalid_params(backend):
     assert backend.apply_gain(np.zeros(0, np.uint16), 2.0) == ComputeResult.INVALID_PARAM
     assert backend.blend_chunk_contributors([o] * 128, 4, 4, o) == ComputeResult.INVALID_PARAM
     assert backend.blend_chunk_contributors([o], 4, 4, o, 0) == ComputeResult.INVALID_PARAM
+
+
+def test_blend_wide_chunk(backend, oracle_c):
+    # Lines longer than the seam kernel keeps in shared memory (3072).
+    rng = np.random.default_rng(5)
+    w, h = 3300, 40
+    a = np.zeros((h, w, 3), np.uint16)
+    b = np.zeros((h, w, 3), np.uint16)
+    a[:, :2000] = rng.integers(100, 30000, (h, 2000, 3))
+    b[:, 1200:] = rng.integers(100, 30000, (h, w - 1200, 3))
+    b[5:30, 1500:1600] = 60000
+    out = np.zeros((h, w, 3), np.uint16)
+    assert backend.blend_chunk_contributors([a, b], w, h, out, 5) == ComputeResult.SUCCESS, backend.get_last_error()
+    assert np.array_equal(out, oracle_c.blend([a, b], 5))
+    # column scan: tall chunk
+    at, bt = np.ascontiguousarray(a.transpose(1, 0, 2)), np.ascontiguousarray(b.transpose(1, 0, 2))
+    out = np.zeros((w, h, 3), np.uint16)
+    assert backend.blend_chunk_contributors([at, bt], h, w, out, 5) == ComputeResult.SUCCESS, backend.get_last_error()
+    assert np.array_equal(out, oracle_c.blend([at, bt], 5))
