@@ -100,6 +100,7 @@ def load_library(path: str = LIB_PATH):
     L.i360b_launch_median.argtypes = [ct.POINTER(vp), i, vp, i, i, f, vp]
     L.i360b_launch_gain.argtypes = [vp, i, f, vp]
     L.i360b_launch_blend.argtypes = [ct.POINTER(vp), i, i, i, i, vp, vp]
+    L.i360b_launch_blend_noalloc.argtypes = [ct.POINTER(vp), i, i, i, i, vp, vp]
     _lib = L
     return L
 
@@ -218,6 +219,16 @@ class B200ComputeBackend:
         arr = (ct.c_void_p * max(1, len(d_warped)))(*d_warped)
         return ComputeResult(self.lib.i360b_launch_blend(arr, len(d_warped), width, height, num_bands, d_out,
                                                          stream or None))
+
+
+def launch_blend_noalloc(d_warped, width: int, height: int, d_out: int, num_bands: int = 5,
+                         stream: int = 0) -> ComputeResult:
+    """i360b_launch_blend_noalloc: the device blend with no device allocation
+    (for callers that cannot allocate once running; see the C header)."""
+    L = load_library()
+    arr = (ct.c_void_p * max(1, len(d_warped)))(*d_warped)
+    return ComputeResult(L.i360b_launch_blend_noalloc(arr, len(d_warped), width, height, num_bands, d_out,
+                                                      stream or None))
 
 
 class RenderPlan:

@@ -91,4 +91,8 @@ int launch_median(const unsigned short* const* inputs, int n, unsigned short* ou
 int launch_gain(unsigned short* data, long long n, float gain, cudaStream_t s);
 int launch_blend_chunk(const unsigned short* const* warped, int k, int w, int h, int bands, unsigned short* out,
                        cudaStream_t s);
+// The same blend with all device scratch carved from a caller-provided buffer
+// (no allocation); synchronous on `s`.
+int launch_blend_chunk_in(void* arena, size_t arenaBytes, const unsigned short* const* warped, int k, int w, int h,
+                          int bands, unsigned short* out, cudaStream_t s);
 }  // namespace i360b

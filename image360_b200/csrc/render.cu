@@ -110,7 +110,8 @@ __global__ void k_count_cov(const ItemDev* items, const TileDev* tiles, int n, u
 }
 }  // namespace
 
-int Plan::build(const std::vector<TileSpec>& specs, int numBands, bool renderPath)
+int Plan::build(const std::vector<TileSpec>& specs, int numBands, bool renderPath, void* extArena, size_t extBytes,
+                cudaStream_t stream)
 {
     render = renderPath;
     nTiles = (int)specs.size();
@@ -286,13 +287,25 @@ int Plan::build(const std::vector<TileSpec>& specs, int numBands, bool renderPat
     size_t metaOff = bytes;
     bytes += unitBytes + intBytes + itemBytes + tileBytes + 256 + 256;
     arenaBytes = bytes;
-    cudaError_t e = cudaMalloc(&arena, bytes);
-    if (e != cudaSuccess)
+    if (extArena)
     {
-        cudaGetLastError();
-        arena = nullptr;
-        return fail(e == cudaErrorMemoryAllocation ? I360B_OUT_OF_MEMORY : I360B_CUDA_ERROR,
-                    "render plan: device allocation of %zu bytes failed (%s)", bytes, cudaGetErrorString(e));
+        if (bytes > extBytes)
+            return fail(I360B_INVALID_PARAM,
+                        "chunk needs %zu bytes of device scratch; the allocation-free entry point holds %zu", bytes,
+                        extBytes);
+        arena = extArena;
+        ownsArena = false;
+    }
+    else
+    {
+        cudaError_t e = cudaMalloc(&arena, bytes);
+        if (e != cudaSuccess)
+        {
+            cudaGetLastError();
+            arena = nullptr;
+            return fail(e == cudaErrorMemoryAllocation ? I360B_OUT_OF_MEMORY : I360B_CUDA_ERROR,
+                        "render plan: device allocation of %zu bytes failed (%s)", bytes, cudaGetErrorString(e));
+        }
     }
     char* base = static_cast<char*>(arena);
     for (int t = 0; t < nTiles; ++t)
@@ -327,12 +340,33 @@ int Plan::build(const std::vector<TileSpec>& specs, int numBands, bool renderPat
     dTiles = reinterpret_cast<TileDev*>(base + metaOff + unitBytes + intBytes + itemBytes);
     dError = reinterpret_cast<int*>(base + metaOff + unitBytes + intBytes + itemBytes + tileBytes);
     dSeamCycles = reinterpret_cast<unsigned long long*>(base + metaOff + unitBytes + intBytes + itemBytes + tileBytes + 256);
-    I360B_CUDA(cudaMemcpy(dUnits, units.data(), units.size() * sizeof(Unit), cudaMemcpyHostToDevice), "plan upload");
-    I360B_CUDA(cudaMemcpy(dInts, ints.data(), ints.size() * sizeof(int), cudaMemcpyHostToDevice), "plan upload");
-    if (nItems) I360B_CUDA(cudaMemcpy(dItems, items.data(), nItems * sizeof(ItemDev), cudaMemcpyHostToDevice), "plan upload");
-    if (nTiles) I360B_CUDA(cudaMemcpy(dTiles, tiles.data(), nTiles * sizeof(TileDev), cudaMemcpyHostToDevice), "plan upload");
-    I360B_CUDA(cudaMemset(dError, 0, sizeof(int)), "plan upload");
-    I360B_CUDA(cudaMemset(dSeamCycles, 0, 5 * sizeof(unsigned long long)), "plan upload");
+    if (extArena)
+    {
+        // Caller-provided scratch: upload the tables on the caller's stream
+        // (the scratch may still be in use by earlier work on that stream).
+        I360B_CUDA(cudaMemcpyAsync(dUnits, units.data(), units.size() * sizeof(Unit), cudaMemcpyHostToDevice, stream),
+                   "plan upload");
+        I360B_CUDA(cudaMemcpyAsync(dInts, ints.data(), ints.size() * sizeof(int), cudaMemcpyHostToDevice, stream),
+                   "plan upload");
+        if (nItems)
+            I360B_CUDA(cudaMemcpyAsync(dItems, items.data(), nItems * sizeof(ItemDev), cudaMemcpyHostToDevice, stream),
+                       "plan upload");
+        if (nTiles)
+            I360B_CUDA(cudaMemcpyAsync(dTiles, tiles.data(), nTiles * sizeof(TileDev), cudaMemcpyHostToDevice, stream),
+                       "plan upload");
+        I360B_CUDA(cudaMemsetAsync(dError, 0, sizeof(int), stream), "plan upload");
+        I360B_CUDA(cudaMemsetAsync(dSeamCycles, 0, 5 * sizeof(unsigned long long), stream), "plan upload");
+        I360B_CUDA(cudaStreamSynchronize(stream), "plan upload");
+    }
+    else
+    {
+        I360B_CUDA(cudaMemcpy(dUnits, units.data(), units.size() * sizeof(Unit), cudaMemcpyHostToDevice), "plan upload");
+        I360B_CUDA(cudaMemcpy(dInts, ints.data(), ints.size() * sizeof(int), cudaMemcpyHostToDevice), "plan upload");
+        if (nItems) I360B_CUDA(cudaMemcpy(dItems, items.data(), nItems * sizeof(ItemDev), cudaMemcpyHostToDevice), "plan upload");
+        if (nTiles) I360B_CUDA(cudaMemcpy(dTiles, tiles.data(), nTiles * sizeof(TileDev), cudaMemcpyHostToDevice), "plan upload");
+        I360B_CUDA(cudaMemset(dError, 0, sizeof(int)), "plan upload");
+        I360B_CUDA(cudaMemset(dSeamCycles, 0, 5 * sizeof(unsigned long long)), "plan upload");
+    }
     seamList = dInts + seamStart;
     return I360B_SUCCESS;
 }
@@ -342,7 +376,7 @@ Plan::~Plan()
     if (graphExec) cudaGraphExecDestroy(graphExec);
     if (graph) cudaGraphDestroy(graph);
     if (hostErr) cudaFreeHost(hostErr);
-    if (arena) cudaFree(arena);
+    if (arena && ownsArena) cudaFree(arena);
 }
 
 const char* const kStageNames[kStages] = {"warp_gain_coverage", "chamfer_forward", "chamfer_backward",
@@ -496,6 +530,30 @@ int launch_blend_chunk(const unsigned short* const* warped, int k, int w, int h,
     I360B_TRY(p.build(specs, bands, false));
     I360B_TRY(p.execute(s, false));
     return p.check(s);
+}
+
+int launch_blend_chunk_in(void* arena, size_t arenaBytes, const unsigned short* const* warped, int k, int w, int h,
+                          int bands, unsigned short* out, cudaStream_t s)
+{
+    std::vector<TileSpec> specs(1);
+    specs[0].w = w;
+    specs[0].h = h;
+    specs[0].out = out;
+    for (int i = 0; i < k; ++i)
+    {
+        ItemSpec it{};
+        it.img = warped[i];
+        specs[0].items.push_back(it);
+    }
+    Plan p;
+    I360B_TRY(p.build(specs, bands, false, arena, arenaBytes, s));
+    I360B_TRY(p.enqueue(s));
+    // Status of the bounded waits, read without a pinned staging buffer.
+    int flag = 0;
+    I360B_CUDA(cudaMemcpyAsync(&flag, p.dError, sizeof(int), cudaMemcpyDeviceToHost, s), "error flag readback");
+    I360B_CUDA(cudaStreamSynchronize(s), "blend synchronize");
+    if (flag) return fail(I360B_KERNEL_LAUNCH_FAILED, "A blend kernel gave up waiting (bounded spin); output invalid.");
+    return I360B_SUCCESS;
 }
 }  // namespace i360b
 

@@ -62,7 +62,12 @@ struct Plan
     Plan& operator=(const Plan&) = delete;
     ~Plan();
 
-    int build(const std::vector<TileSpec>& specs, int numBands, bool renderPath);
+    // With extArena non-null the plan lives in that caller-provided device
+    // buffer of extBytes bytes (no allocation; INVALID_PARAM if too small)
+    // and its tables are uploaded on stream `s`.
+    int build(const std::vector<TileSpec>& specs, int numBands, bool renderPath, void* extArena = nullptr,
+              size_t extBytes = 0, cudaStream_t s = nullptr);
+    bool ownsArena = true;
     // Enqueues the kernel sequence; with `ev` non-null records ev[i] before
     // stage i and ev[kStages] at the end (stage order of kStageNames).
     int enqueue(cudaStream_t s, cudaEvent_t* ev = nullptr);

@@ -141,6 +141,22 @@ I360B_API int i360b_launch_gain(unsigned short* dData, int numValues, float gain
 I360B_API int i360b_launch_blend(const unsigned short* const* dWarped, int numContributors, int width, int height,
                        int numBands, unsigned short* dOut, void* stream);
 
+/* Allocation-free variant of i360b_launch_blend.  No counterpart in the
+ * reference: it exists for callers that must not allocate device memory once
+ * running - hosts that reserve the GPU's memory up front for their own pool
+ * (where a cudaMalloc fails or breaks their budget) and latency-critical
+ * render loops (where cudaMalloc/cudaFree would synchronise the device).  All
+ * of the blend's scratch comes from one static 12 MiB device array compiled
+ * into the library (held on every GPU that loads it until exit); a chunk
+ * needing more - roughly width*height*(15*numContributors + 5) bytes, e.g.
+ * 256x256 with 8 contributors fits - returns I360B_INVALID_PARAM.  The caller
+ * passes device inputs and output as for i360b_launch_blend.  Synchronous: it
+ * waits for `stream` before returning.  Every call reuses the same array, so
+ * calls whose GPU work overlaps race; serialise them.  The first call on each
+ * device looks up the array's device address. */
+I360B_API int i360b_launch_blend_noalloc(const unsigned short* const* dWarped, int numContributors, int width,
+                                         int height, int numBands, unsigned short* dOut, void* stream);
+
 /* ---- batched render of a panorama's output tiles ----------------------- */
 
 /* One source frame: a demosaiced RGB48 image in device memory and its
