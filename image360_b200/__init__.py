@@ -283,7 +283,7 @@ class RenderPlan:
         rc = self.lib.i360b_render_plan_profile(self._h, stream or None, ms, 16)
         if rc != 0:
             raise RuntimeError(self.lib.i360b_get_last_error().decode())
-        return {self.lib.i360b_render_stage_name(i).decode(): float(ms[i]) for i in range(9)}
+        return {self.lib.i360b_render_stage_name(i).decode(): float(ms[i]) for i in range(10)}
 
     def execute(self, stream: int = 0) -> ComputeResult:
         return ComputeResult(self.lib.i360b_render_plan_execute(self._h, stream or None))

@@ -380,7 +380,8 @@ Plan::~Plan()
 }
 
 const char* const kStageNames[kStages] = {"warp_gain_coverage", "chamfer_forward", "chamfer_backward",
-                                          "ownership", "seam_dp", "pyramid_down", "blend_bands", "collapse",
+                                          "ownership",          "seam_dp",         "pyramid_down0",
+                                          "pyramid_down",       "blend_bands",     "collapse",
                                           "level0_output"};
 
 int Plan::kernels_per_execute() const
@@ -419,23 +420,24 @@ int Plan::enqueue(cudaStream_t s, cudaEvent_t* ev)
     {
         r = L(3 + l);
         I360B_TRY(launch_down(a, dUnits + r.start, r.count, l, s));
+        if (l == 0) mark(6);
     }
-    mark(6);
+    mark(7);
     for (int l = kMaxBands - 1; l >= 1; --l)
     {
         r = L(3 + (kMaxBands - 1) + l);
         I360B_TRY(launch_blend_level(a, dUnits + r.start, r.count, l, s));
     }
-    mark(7);
+    mark(8);
     for (int l = kMaxBands - 1; l >= 1; --l)
     {
         r = L(3 + 2 * kMaxBands - 1 + l);
         I360B_TRY(launch_collapse(a, dUnits + r.start, r.count, l, s));
     }
-    mark(8);
+    mark(9);
     r = L(2);
     I360B_TRY(launch_final0(a, dUnits + r.start, r.count, s));
-    mark(9);
+    mark(10);
     return I360B_SUCCESS;
 }
 

@@ -28,7 +28,7 @@ struct TileSpec
     std::vector<ItemSpec> items;
 };
 
-constexpr int kStages = 9;
+constexpr int kStages = 10;
 extern const char* const kStageNames[kStages];
 
 struct Range

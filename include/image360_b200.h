@@ -228,7 +228,7 @@ typedef struct i360b_render_stats
 } i360b_render_stats;
 I360B_API int i360b_render_plan_stats(i360b_render_plan* plan, void* stream, i360b_render_stats* out);
 /* Runs the plan once without the graph, timing each stage with CUDA events on
- * `stream`; stageMs receives up to maxStages values (9 stages, names from
+ * `stream`; stageMs receives up to maxStages values (10 stages, names from
  * i360b_render_stage_name).  Synchronous. */
 I360B_API int i360b_render_plan_profile(i360b_render_plan* plan, void* stream, float* stageMs, int maxStages);
 I360B_API const char* i360b_render_stage_name(int stage);
