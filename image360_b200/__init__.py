@@ -69,9 +69,11 @@ _f32p = ct.POINTER(ct.c_float)
 _lib = None
 
 
-def header_symbols(path: str = HEADER) -> list[str]:
-    """Names of the functions declared in the C-ABI header."""
-    text = open(path).read()
+def header_symbols(path: str | None = None) -> list[str]:
+    """Names of the functions declared in the C-ABI headers (include/*.h)."""
+    incdir = os.path.dirname(HEADER)
+    paths = [path] if path else [os.path.join(incdir, f) for f in sorted(os.listdir(incdir)) if f.endswith(".h")]
+    text = "".join(open(p).read() for p in paths)
     return sorted(set(re.findall(r"I360B_API\s+[\w\s\*]*?\b(i360b_\w+)\s*\(", text)))
 
 

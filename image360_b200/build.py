@@ -20,7 +20,7 @@ OBJDIR = os.path.join(HERE, "_build")
 # rounds every product and sum separately).
 PARITY_SOURCES = ["context.cu", "pixel_ops.cu", "blend_kernels.cu", "render.cu", "capi.cu", "noalloc.cu"]
 # Everything else (tensor-core learned blend) may contract.
-FAST_SOURCES: list[str] = []
+FAST_SOURCES: list[str] = ["learned.cu"]
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 COMMON = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-Xcompiler", "-fvisibility=hidden",
@@ -43,7 +43,8 @@ def build(verbose: bool = False, jobs: int = 8) -> str:
     os.makedirs(LIBDIR, exist_ok=True)
     os.makedirs(OBJDIR, exist_ok=True)
     headers = [os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith((".cuh", ".hpp", ".h"))]
-    headers.append(os.path.join(HERE, "..", "include", "image360_b200.h"))
+    incdir = os.path.join(HERE, "..", "include")
+    headers += [os.path.join(incdir, f) for f in os.listdir(incdir) if f.endswith(".h")]
     procs = []
     objs = []
     for src, extra in [(s, ["-fmad=false"]) for s in PARITY_SOURCES] + [(s, []) for s in FAST_SOURCES]:

@@ -1,0 +1,1510 @@
+// Learned seam blend: tcgen05 (5th-generation tensor core) implicit-GEMM 3x3
+// convolutions, forward and backward, the U-Net-lite built from them, its
+// loss and Adam, all on the GPU.  No reference counterpart (the reference
+// blends overlaps with SeamBlend.cpp:549-587 only); the network's shape is in
+// include/image360_b200_blendnet.h.
+//
+// Convolution as GEMM, per CTA tile of R image rows x 128 pixels:
+//   D[pixel][cout] += A[pixel][(tap, cin)] * B[cout][(tap, cin)]
+// with M = 128 pixels of one row, N = cout, K = 9 * cin in steps of 16.
+// The input halo ((R+2) rows x 130 pixels x cin) sits in shared memory as
+// 8-channel chunks, each a [pixel][8 channels] array of 16-byte rows; any
+// 8 consecutive pixels of it are one 8x16-byte "core matrix" of the K-major
+// no-swizzle layout, so the A operand of tap (dy, dx) is the same buffer with
+// the descriptor's start address moved by (dy * 130 + dx) * 16 bytes - no
+// im2col copy.  Weights are K-major [k/8][cout][8].  fp32 accumulators live in
+// TMEM, two slots so the epilogue of one tile overlaps the MMAs of the next,
+// and halos are double-buffered with cp.async so the next load overlaps both.
+//
+// Weight gradient: D[(tap, cin)][cout] += X[pixel + tap][cin] * G[pixel][cout]
+// summed over pixels (K), with both operands MN-major (the 8 channels of a
+// pixel are the contiguous 16 bytes); each CTA owns a 128-row chunk of
+// (tap, cin) and a slice of the pixels, and writes an fp32 partial that a
+// small kernel reduces.
+#include "common.cuh"
+#include "tc_common.cuh"
+#include "../../include/image360_b200_blendnet.h"
+
+#include <cuda_bf16.h>
+
+#include <cmath>
+#include <cstring>
+#include <mutex>
+#include <random>
+#include <vector>
+
+namespace i360b
+{
+namespace
+{
+using bf16 = __nv_bfloat16;
+
+constexpr int kTileX = 128;                // pixels per MMA row block (M)
+constexpr int kHaloW = kTileX + 2;         // halo row length
+constexpr long long kWaitSpins = 1ll << 26;  // bounded mbarrier waits
+constexpr int kSlots = 4;
+constexpr float kInScale = 1.0f / 32768.0f;
+
+enum
+{
+    LD_PLAIN = 0,
+    LD_CONCAT = 1
+};
+enum
+{
+    EP_RELU = I360B_CONV_BIAS_RELU,
+    EP_LOGITS = I360B_CONV_LOGITS,
+    EP_MASK = I360B_CONV_MASK,
+    EP_RAW = I360B_CONV_RAW,
+    EP_COMPOSITE = 4
+};
+
+struct ConvArgs
+{
+    const bf16* x;  // [n][h][w][cin], or the skip [n][h][w][cs] for LD_CONCAT
+    const bf16* u;  // LD_CONCAT: [n][h/2][w/2][cin - cs]
+    int cs;
+    int n, h, w;
+    const bf16* wt;     // [npad][9 * cin], k = tap * cin + c
+    const float* bias;  // [npad]
+    void* out;
+    const bf16* act;  // EP_MASK: [n][h][w][npad]
+    const i360b_blend_job* jobs;  // EP_COMPOSITE: one per image
+    int* error;
+};
+
+template <int CIN, int NPAD, int R>
+struct ConvShape
+{
+    static constexpr int kC8 = CIN / 8;
+    static constexpr uint32_t kChunk = (R + 2) * kHaloW * 16;  // bytes of one 8-channel halo chunk
+    static constexpr uint32_t kHalo = kC8 * kChunk;
+    static constexpr uint32_t kW = 9u * CIN * NPAD * 2;
+    static constexpr uint32_t kSmem = kW + 2 * kHalo + 64;
+    static constexpr uint32_t kSlotCols = R * NPAD;
+    static constexpr uint32_t kTmem = tc::tmem_cols(2 * kSlotCols);
+    static constexpr int kKSteps = 9 * CIN / 16;
+    static_assert(CIN % 16 == 0 && NPAD % 16 == 0 && NPAD >= 16 && NPAD <= 256, "MMA shape");
+    static_assert(2 * kSlotCols <= 512, "TMEM capacity");
+    static_assert(kChunk / 16 < (1u << 14), "descriptor LBO range");
+    static_assert(kSmem <= 227u * 1024u, "shared memory");
+};
+
+__device__ __forceinline__ uint4 pack8_bf16(const float* v)
+{
+    uint4 r;
+    __nv_bfloat162 p0 = __floats2bfloat162_rn(v[0], v[1]);
+    __nv_bfloat162 p1 = __floats2bfloat162_rn(v[2], v[3]);
+    __nv_bfloat162 p2 = __floats2bfloat162_rn(v[4], v[5]);
+    __nv_bfloat162 p3 = __floats2bfloat162_rn(v[6], v[7]);
+    r.x = *reinterpret_cast<uint32_t*>(&p0);
+    r.y = *reinterpret_cast<uint32_t*>(&p1);
+    r.z = *reinterpret_cast<uint32_t*>(&p2);
+    r.w = *reinterpret_cast<uint32_t*>(&p3);
+    return r;
+}
+
+__device__ __forceinline__ void unpack8_bf16(uint4 q, float* v)
+{
+    const uint32_t w[4] = {q.x, q.y, q.z, q.w};
+#pragma unroll
+    for (int i = 0; i < 4; ++i)
+    {
+        __nv_bfloat162 p = *reinterpret_cast<const __nv_bfloat162*>(&w[i]);
+        float2 f = __bfloat1622float2(p);
+        v[2 * i] = f.x;
+        v[2 * i + 1] = f.y;
+    }
+}
+
+// Source of one 16-byte (8-channel) chunk of the convolution input at (img,
+// yy, xx); yy, xx inside the image.
+template <int CIN, int LD>
+__device__ __forceinline__ const bf16* input_chunk(const bf16* x, const bf16* u, int cs, int h, int w, int img, int yy,
+                                                   int xx, int c8)
+{
+    if (LD == LD_PLAIN) return x + ((((size_t)img * h + yy) * w + xx) * CIN + c8 * 8);
+    const int sc8 = cs >> 3;
+    if (c8 < sc8) return x + ((((size_t)img * h + yy) * w + xx) * cs + c8 * 8);
+    return u + ((((size_t)img * (h >> 1) + (yy >> 1)) * (w >> 1) + (xx >> 1)) * (CIN - cs) + (c8 - sc8) * 8);
+}
+
+// Softmax-weighted composite of a pixel's covered layers (the network head).
+__device__ __forceinline__ void composite_pixel(const i360b_blend_job& J, int y, int x, const float* l, float* outDN,
+                                                float* wts, float (*v)[3], bool* cov, int& nCov)
+{
+    float m = -INFINITY;
+    nCov = 0;
+#pragma unroll
+    for (int i = 0; i < kSlots; ++i)
+    {
+        cov[i] = false;
+        v[i][0] = v[i][1] = v[i][2] = 0.0f;
+        if (J.slot[i])
+        {
+            const unsigned short* p = J.slot[i] + (long long)y * J.rowStride + (long long)x * J.pixStride;
+            const unsigned short r = p[0], g = p[1], b = p[2];
+            cov[i] = (r | g | b) != 0;
+            v[i][0] = r;
+            v[i][1] = g;
+            v[i][2] = b;
+        }
+        if (cov[i])
+        {
+            m = fmaxf(m, l[i]);
+            ++nCov;
+        }
+    }
+    float sum = 0.0f;
+#pragma unroll
+    for (int i = 0; i < kSlots; ++i)
+    {
+        wts[i] = cov[i] ? __expf(l[i] - m) : 0.0f;
+        sum += wts[i];
+    }
+    const float inv = nCov ? 1.0f / sum : 0.0f;
+    outDN[0] = outDN[1] = outDN[2] = 0.0f;
+#pragma unroll
+    for (int i = 0; i < kSlots; ++i)
+    {
+        wts[i] *= inv;
+        outDN[0] += wts[i] * v[i][0];
+        outDN[1] += wts[i] * v[i][1];
+        outDN[2] += wts[i] * v[i][2];
+    }
+}
+
+// ---------------------------------------------------------------------------
+// 3x3 convolution (forward, or backward-data with flipped transposed weights).
+// Persistent: CTA b handles tiles b, b + gridDim.x, ...; 128 threads; thread 0
+// issues the MMAs, all four warps load and run the epilogue (warp w owns TMEM
+// lanes 32w..32w+31 = pixels 32w..32w+31 of the tile).
+// ---------------------------------------------------------------------------
+template <int CIN, int NPAD, int R, int LD, int EP>
+__global__ void __launch_bounds__(128, 1) k_conv3x3(ConvArgs a)
+{
+    using S = ConvShape<CIN, NPAD, R>;
+    extern __shared__ __align__(128) unsigned char smem[];
+    unsigned char* wsm = smem;
+    unsigned char* halo0 = smem + S::kW;
+    uint64_t* mbar = reinterpret_cast<uint64_t*>(smem + S::kW + 2 * S::kHalo);
+    uint32_t* tmemSlot = reinterpret_cast<uint32_t*>(mbar + 2);
+
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int tilesX = a.w / kTileX, tilesY = (a.h + R - 1) / R;
+    const long long nTiles = (long long)a.n * tilesY * tilesX;
+    if ((long long)blockIdx.x >= nTiles) return;
+    const int myTiles = (int)((nTiles - 1 - blockIdx.x) / gridDim.x) + 1;
+
+    auto coord = [&](long long t, int& img, int& y0, int& x0) {
+        x0 = (int)(t % tilesX) * kTileX;
+        const long long r = t / tilesX;
+        y0 = (int)(r % tilesY) * R;
+        img = (int)(r / tilesY);
+    };
+    auto loadHalo = [&](long long t, unsigned char* buf) {
+        int img, y0, x0;
+        coord(t, img, y0, x0);
+        constexpr int kN = S::kC8 * (R + 2) * kHaloW;
+        for (int q = tid; q < kN; q += 128)
+        {
+            const int c8 = q % S::kC8;
+            const int rest = q / S::kC8;
+            const int hx = rest % kHaloW, hr = rest / kHaloW;
+            const int yy = y0 - 1 + hr, xx = x0 - 1 + hx;
+            const bool ok = yy >= 0 && yy < a.h && xx >= 0 && xx < a.w;
+            const bf16* src = ok ? input_chunk<CIN, LD>(a.x, a.u, a.cs, a.h, a.w, img, yy, xx, c8) : a.x;
+            tc::cp_async16(buf + c8 * S::kChunk + (hr * kHaloW + hx) * 16, src, ok ? 16 : 0);
+        }
+    };
+
+    if (warp == 0) tc::tmem_alloc(tmemSlot, S::kTmem);
+    if (tid == 0)
+    {
+        tc::mbar_init(&mbar[0], 1);
+        tc::mbar_init(&mbar[1], 1);
+        tc::fence_mbar_init();
+    }
+    {
+        constexpr int kK8 = 9 * S::kC8;
+        for (int q = tid; q < NPAD * kK8; q += 128)
+        {
+            const int n = q / kK8, k8 = q % kK8;
+            tc::cp_async16(wsm + k8 * (NPAD * 16) + n * 16, a.wt + (size_t)n * 9 * CIN + k8 * 8, 16);
+        }
+    }
+    loadHalo(blockIdx.x, halo0);
+    tc::cp_async_commit();
+    tc::fence_before_sync();
+    __syncthreads();
+    tc::fence_after_sync();
+    const uint32_t tmem = *tmemSlot;
+
+    auto issue = [&](int slot) {
+        tc::fence_after_sync();
+        const uint32_t hb = tc::smem_u32(halo0 + slot * S::kHalo), wb = tc::smem_u32(wsm);
+        constexpr uint32_t idesc = tc::idesc_bf16_f32(128, NPAD);
+        for (int r = 0; r < R; ++r)
+        {
+            const uint32_t d = tmem + slot * S::kSlotCols + r * NPAD;
+#pragma unroll 4
+            for (int ks = 0; ks < S::kKSteps; ++ks)
+            {
+                const int k0 = ks * 16, tap = k0 / CIN, c8 = (k0 % CIN) >> 3;
+                const int dy = tap / 3, dx = tap % 3;
+                const uint32_t aAddr = hb + c8 * S::kChunk + ((r + dy) * kHaloW + dx) * 16;
+                const uint32_t bAddr = wb + (2 * ks) * (NPAD * 16);
+                tc::mma_bf16(d, tc::smem_desc(aAddr, S::kChunk, 128), tc::smem_desc(bAddr, NPAD * 16, 128), idesc,
+                             ks > 0 ? 1u : 0u);
+            }
+        }
+        tc::mma_commit(&mbar[slot]);
+    };
+
+    auto epilogue = [&](long long t, int slot) {
+        int img, y0, x0;
+        coord(t, img, y0, x0);
+        const int px = x0 + warp * 32 + lane;
+        const uint32_t base = tmem + ((uint32_t)(warp * 32) << 16) + slot * S::kSlotCols;
+        for (int r = 0; r < R; ++r)
+        {
+            const int y = y0 + r;
+            const bool valid = y < a.h;  // uniform across the warp
+            const size_t pix = ((size_t)img * a.h + y) * a.w + px;
+            if (EP == EP_LOGITS || EP == EP_COMPOSITE)
+            {
+                float v[16];
+                tc::tmem_ld16(base + r * NPAD, v);
+                if (!valid) continue;
+                float l[4];
+#pragma unroll
+                for (int j = 0; j < 4; ++j) l[j] = v[j] + a.bias[j];
+                if (EP == EP_LOGITS)
+                {
+                    reinterpret_cast<float4*>(a.out)[pix] = make_float4(l[0], l[1], l[2], l[3]);
+                }
+                else
+                {
+                    const i360b_blend_job& J = a.jobs[img];
+                    if (px < J.width && y < J.height)
+                    {
+                        float o[3], wts[4], vv[4][3];
+                        bool cov[4];
+                        int nCov;
+                        composite_pixel(J, y, px, l, o, wts, vv, cov, nCov);
+                        unsigned short* q = J.out + (long long)y * J.outRowStride + (long long)px * 3;
+#pragma unroll
+                        for (int c = 0; c < 3; ++c)
+                            q[c] = (unsigned short)__float2uint_rn(fminf(fmaxf(o[c], 0.0f), 65535.0f));
+                    }
+                }
+            }
+            else
+            {
+#pragma unroll 1
+                for (int cb = 0; cb < NPAD / 16; ++cb)
+                {
+                    float v[16];
+                    tc::tmem_ld16(base + r * NPAD + cb * 16, v);
+                    if (!valid) continue;
+                    if (EP == EP_RELU)
+                    {
+#pragma unroll
+                        for (int j = 0; j < 16; ++j) v[j] = fmaxf(v[j] + a.bias[cb * 16 + j], 0.0f);
+                    }
+                    if (EP == EP_MASK)
+                    {
+                        const uint4* ap = reinterpret_cast<const uint4*>(a.act + pix * NPAD + cb * 16);
+                        float m[16];
+                        unpack8_bf16(ap[0], m);
+                        unpack8_bf16(ap[1], m + 8);
+#pragma unroll
+                        for (int j = 0; j < 16; ++j) v[j] = m[j] > 0.0f ? v[j] : 0.0f;
+                    }
+                    uint4* op = reinterpret_cast<uint4*>(static_cast<bf16*>(a.out) + pix * NPAD + cb * 16);
+                    op[0] = pack8_bf16(v);
+                    op[1] = pack8_bf16(v + 8);
+                }
+            }
+        }
+        tc::fence_before_sync();
+    };
+
+    bool ok = true;
+    for (int i = 0; i < myTiles; ++i)
+    {
+        const int s = i & 1;
+        const long long t = blockIdx.x + (long long)i * gridDim.x;
+        if (i + 1 < myTiles)
+        {
+            if (i >= 1 && !tc::mbar_wait(&mbar[s ^ 1], ((i - 1) >> 1) & 1, kWaitSpins)) ok = false;
+            if (ok) loadHalo(t + gridDim.x, halo0 + (s ^ 1) * S::kHalo);
+            tc::cp_async_commit();
+            tc::cp_async_wait<1>();
+        }
+        else
+        {
+            tc::cp_async_wait<0>();
+        }
+        tc::fence_proxy_async();
+        if (__syncthreads_or(!ok))
+        {
+            ok = false;
+            break;
+        }
+        if (tid == 0) issue(s);
+        if (i >= 1)
+        {
+            bool done = tc::mbar_wait(&mbar[s ^ 1], ((i - 1) >> 1) & 1, kWaitSpins);
+            done = __all_sync(0xffffffffu, done);
+            if (!done) ok = false;
+            else
+            {
+                tc::fence_after_sync();
+                epilogue(t - gridDim.x, s ^ 1);
+            }
+        }
+    }
+    if (ok)
+    {
+        const int last = myTiles - 1;
+        bool done = tc::mbar_wait(&mbar[last & 1], (last >> 1) & 1, kWaitSpins);
+        done = __all_sync(0xffffffffu, done);
+        if (!done) ok = false;
+        else
+        {
+            tc::fence_after_sync();
+            epilogue(blockIdx.x + (long long)last * gridDim.x, last & 1);
+        }
+    }
+    if (!ok && lane == 0) atomicOr(a.error, 1);
+    tc::cp_async_wait<0>();
+    tc::fence_before_sync();
+    __syncthreads();
+    if (warp == 0)
+    {
+        tc::fence_after_sync();
+        tc::tmem_dealloc(tmem, S::kTmem);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Weight gradient.  grid = (slices, chunks); CTA (s, c) accumulates rows
+// c*128 .. c*128+127 of (tap, cin) over pixel tiles s, s + slices, ... (one
+// tile = 128 pixels of one row) and writes partial[s][row][cout].
+// ---------------------------------------------------------------------------
+struct WgradArgs
+{
+    const bf16* x;
+    const bf16* u;
+    int cs;
+    const bf16* g;  // [n][h][w][COUT]
+    int n, h, w;
+    float* partial;  // [gridDim.x][gridDim.y * 128][COUT]
+    int* error;
+};
+
+template <int CIN, int COUT>
+struct WgradShape
+{
+    static constexpr int kC8 = CIN / 8;
+    static constexpr int kRows8 = 9 * kC8;
+    static constexpr int kChunks = (kRows8 + 15) / 16;
+    static constexpr uint32_t kA = 16 * 2048;
+    static constexpr uint32_t kB = (COUT / 8) * 2048;
+    static constexpr uint32_t kStage = kA + kB;
+    static constexpr uint32_t kSmem = 2 * kStage + 64;
+    static constexpr uint32_t kTmem = tc::tmem_cols(COUT);
+    static_assert(COUT % 16 == 0 && COUT >= 16 && COUT <= 256, "MMA shape");
+};
+
+template <int CIN, int COUT, int LD>
+__global__ void __launch_bounds__(128, 1) k_conv3x3_wgrad(WgradArgs a)
+{
+    using S = WgradShape<CIN, COUT>;
+    extern __shared__ __align__(128) unsigned char smem[];
+    uint64_t* mbar = reinterpret_cast<uint64_t*>(smem + 2 * S::kStage);
+    uint32_t* tmemSlot = reinterpret_cast<uint32_t*>(mbar + 2);
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int chunk = blockIdx.y;
+    const int tilesX = a.w / kTileX;
+    const long long nTiles = (long long)a.n * a.h * tilesX;
+    const int myTiles = (long long)blockIdx.x < nTiles ? (int)((nTiles - 1 - blockIdx.x) / gridDim.x) + 1 : 0;
+    float* part = a.partial + ((size_t)blockIdx.x * (gridDim.y * 128) + (size_t)chunk * 128) * COUT;
+    if (myTiles == 0)
+    {
+        for (int q = tid; q < 128 * COUT; q += 128) part[q] = 0.0f;
+        return;
+    }
+
+    auto load = [&](long long t, unsigned char* buf) {
+        const int x0 = (int)(t % tilesX) * kTileX;
+        const long long r = t / tilesX;
+        const int y = (int)(r % a.h), img = (int)(r / a.h);
+        for (int q = tid; q < 16 * kTileX; q += 128)
+        {
+            const int lg = q & 15, px = q >> 4;
+            const int r8 = chunk * 16 + lg;
+            const int tap = r8 / S::kC8, c8 = r8 % S::kC8;
+            const int yy = y + tap / 3 - 1, xx = x0 + px + tap % 3 - 1;
+            const bool ok = r8 < S::kRows8 && yy >= 0 && yy < a.h && xx >= 0 && xx < a.w;
+            const bf16* src = ok ? input_chunk<CIN, LD>(a.x, a.u, a.cs, a.h, a.w, img, yy, xx, c8) : a.x;
+            tc::cp_async16(buf + lg * 2048 + px * 16, src, ok ? 16 : 0);
+        }
+        constexpr int kG8 = COUT / 8;
+        for (int q = tid; q < kG8 * kTileX; q += 128)
+        {
+            const int c8 = q % kG8, px = q / kG8;
+            const bf16* src = a.g + ((((size_t)img * a.h + y) * a.w + x0 + px) * COUT + c8 * 8);
+            tc::cp_async16(buf + S::kA + c8 * 2048 + px * 16, src, 16);
+        }
+    };
+
+    if (warp == 0) tc::tmem_alloc(tmemSlot, S::kTmem);
+    if (tid == 0)
+    {
+        tc::mbar_init(&mbar[0], 1);
+        tc::mbar_init(&mbar[1], 1);
+        tc::fence_mbar_init();
+    }
+    load(blockIdx.x, smem);
+    tc::cp_async_commit();
+    tc::fence_before_sync();
+    __syncthreads();
+    tc::fence_after_sync();
+    const uint32_t tmem = *tmemSlot;
+    constexpr uint32_t idesc = tc::idesc_bf16_f32(128, COUT) | (1u << 15) | (1u << 16);  // A, B MN-major
+
+    bool ok = true;
+    for (int i = 0; i < myTiles; ++i)
+    {
+        const int s = i & 1;
+        const long long t = blockIdx.x + (long long)i * gridDim.x;
+        if (i + 1 < myTiles)
+        {
+            if (i >= 1 && !tc::mbar_wait(&mbar[s ^ 1], ((i - 1) >> 1) & 1, kWaitSpins)) ok = false;
+            if (ok) load(t + gridDim.x, smem + (s ^ 1) * S::kStage);
+            tc::cp_async_commit();
+            tc::cp_async_wait<1>();
+        }
+        else
+        {
+            tc::cp_async_wait<0>();
+        }
+        tc::fence_proxy_async();
+        if (__syncthreads_or(!ok))
+        {
+            ok = false;
+            break;
+        }
+        if (tid == 0)
+        {
+            tc::fence_after_sync();
+            const uint32_t a0 = tc::smem_u32(smem + s * S::kStage), b0 = a0 + S::kA;
+#pragma unroll
+            for (int j = 0; j < kTileX / 16; ++j)
+                tc::mma_bf16(tmem, tc::smem_desc(a0 + j * 256, 128, 2048), tc::smem_desc(b0 + j * 256, 128, 2048),
+                             idesc, (i > 0 || j > 0) ? 1u : 0u);
+            tc::mma_commit(&mbar[s]);
+        }
+    }
+    if (ok)
+    {
+        const int last = myTiles - 1;
+        bool done = tc::mbar_wait(&mbar[last & 1], (last >> 1) & 1, kWaitSpins);
+        done = __all_sync(0xffffffffu, done);
+        if (!done) ok = false;
+        else
+        {
+            tc::fence_after_sync();
+            float* row = part + (size_t)(warp * 32 + lane) * COUT;
+#pragma unroll 1
+            for (int cb = 0; cb < COUT / 16; ++cb)
+            {
+                float v[16];
+                tc::tmem_ld16(tmem + ((uint32_t)(warp * 32) << 16) + cb * 16, v);
+                float4* o = reinterpret_cast<float4*>(row + cb * 16);
+                o[0] = make_float4(v[0], v[1], v[2], v[3]);
+                o[1] = make_float4(v[4], v[5], v[6], v[7]);
+                o[2] = make_float4(v[8], v[9], v[10], v[11]);
+                o[3] = make_float4(v[12], v[13], v[14], v[15]);
+            }
+            tc::fence_before_sync();
+        }
+    }
+    if (!ok && lane == 0) atomicOr(a.error, 1);
+    tc::cp_async_wait<0>();
+    tc::fence_before_sync();
+    __syncthreads();
+    if (warp == 0)
+    {
+        tc::fence_after_sync();
+        tc::tmem_dealloc(tmem, S::kTmem);
+    }
+}
+
+// dW[co][k] = sum over slices of partial[slice][k][co] (k = tap * cin + ci).
+__global__ void k_wgrad_reduce(const float* __restrict__ partial, int slices, int rowsTotal, int coutStride, int cin,
+                               int cout, float* __restrict__ dw)
+{
+    const int K = 9 * cin;
+    const int idx = blockIdx.x * blockDim.x + threadIdx.x;
+    if (idx >= K * cout) return;
+    const int co = idx / K, k = idx % K;
+    float s = 0.0f;
+    for (int g = 0; g < slices; ++g) s += partial[((size_t)g * rowsTotal + k) * coutStride + co];
+    dw[(size_t)co * K + k] = s;
+}
+
+// ---------------------------------------------------------------------------
+// Glue: input packing, pooling, loss, gradient routing, bias gradients, Adam.
+// ---------------------------------------------------------------------------
+__global__ void k_pack_input(const i360b_blend_job* __restrict__ jobs, int n, int h, int w, bf16* __restrict__ x0)
+{
+    const long long total = (long long)n * h * w;
+    for (long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x; idx < total;
+         idx += (long long)gridDim.x * blockDim.x)
+    {
+        const int img = (int)(idx / ((long long)h * w));
+        const int rem = (int)(idx % ((long long)h * w));
+        const int y = rem / w, x = rem % w;
+        const i360b_blend_job& J = jobs[img];
+        float ch[16];
+#pragma unroll
+        for (int i = 0; i < 16; ++i) ch[i] = 0.0f;
+        if (x < J.width && y < J.height)
+        {
+#pragma unroll
+            for (int i = 0; i < kSlots; ++i)
+            {
+                if (!J.slot[i]) continue;
+                const unsigned short* p = J.slot[i] + (long long)y * J.rowStride + (long long)x * J.pixStride;
+                const unsigned short r = p[0], g = p[1], b = p[2];
+                if ((r | g | b) == 0) continue;
+                ch[4 * i] = r * kInScale;
+                ch[4 * i + 1] = g * kInScale;
+                ch[4 * i + 2] = b * kInScale;
+                ch[4 * i + 3] = 1.0f;
+            }
+        }
+        uint4* o = reinterpret_cast<uint4*>(x0 + idx * 16);
+        o[0] = pack8_bf16(ch);
+        o[1] = pack8_bf16(ch + 8);
+    }
+}
+
+// 2x2 average pool of [n][h][w][C] (C = 8 * c8n) into [n][h/2][w/2][C].
+__global__ void k_pool2(const bf16* __restrict__ in, int n, int h, int w, int c8n, bf16* __restrict__ out)
+{
+    const int hh = h >> 1, wh = w >> 1;
+    const long long total = (long long)n * hh * wh * c8n;
+    for (long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x; idx < total;
+         idx += (long long)gridDim.x * blockDim.x)
+    {
+        const int c8 = (int)(idx % c8n);
+        long long r = idx / c8n;
+        const int xh = (int)(r % wh);
+        r /= wh;
+        const int yh = (int)(r % hh), img = (int)(r / hh);
+        float acc[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+        for (int dy = 0; dy < 2; ++dy)
+            for (int dx = 0; dx < 2; ++dx)
+            {
+                float v[8];
+                const size_t p = ((size_t)img * h + 2 * yh + dy) * w + 2 * xh + dx;
+                unpack8_bf16(reinterpret_cast<const uint4*>(in + p * c8n * 8)[c8], v);
+#pragma unroll
+                for (int j = 0; j < 8; ++j) acc[j] += v[j];
+            }
+#pragma unroll
+        for (int j = 0; j < 8; ++j) acc[j] *= 0.25f;
+        reinterpret_cast<uint4*>(out + idx * 8)[0] = pack8_bf16(acc);
+    }
+}
+
+// Gradient of the upsampled half of the concatenation: g5 = (sum over the 2x2
+// children of du[..., skip: skip+C]) * (a5 > 0), at half resolution.
+__global__ void k_upsample_grad(const bf16* __restrict__ du, int duC, int skip, const bf16* __restrict__ act, int n,
+                                int h, int w, int c8n, bf16* __restrict__ g)
+{
+    const int hh = h >> 1, wh = w >> 1;
+    const long long total = (long long)n * hh * wh * c8n;
+    for (long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x; idx < total;
+         idx += (long long)gridDim.x * blockDim.x)
+    {
+        const int c8 = (int)(idx % c8n);
+        long long r = idx / c8n;
+        const int xh = (int)(r % wh);
+        r /= wh;
+        const int yh = (int)(r % hh), img = (int)(r / hh);
+        float acc[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+        for (int dy = 0; dy < 2; ++dy)
+            for (int dx = 0; dx < 2; ++dx)
+            {
+                float v[8];
+                const size_t p = ((size_t)img * h + 2 * yh + dy) * w + 2 * xh + dx;
+                unpack8_bf16(*reinterpret_cast<const uint4*>(du + p * duC + skip + c8 * 8), v);
+#pragma unroll
+                for (int j = 0; j < 8; ++j) acc[j] += v[j];
+            }
+        float m[8];
+        unpack8_bf16(reinterpret_cast<const uint4*>(act)[idx], m);
+#pragma unroll
+        for (int j = 0; j < 8; ++j) acc[j] = m[j] > 0.0f ? acc[j] : 0.0f;
+        reinterpret_cast<uint4*>(g)[idx] = pack8_bf16(acc);
+    }
+}
+
+// Gradient of the skip activation: g2 = (du[..., 0:C] + dpool / 4 upsampled)
+// * (a2 > 0), at full resolution (C = 8 * c8n channels).
+__global__ void k_skip_grad(const bf16* __restrict__ du, int duC, const bf16* __restrict__ dpool,
+                            const bf16* __restrict__ act, int n, int h, int w, int c8n, bf16* __restrict__ g)
+{
+    const long long total = (long long)n * h * w * c8n;
+    for (long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x; idx < total;
+         idx += (long long)gridDim.x * blockDim.x)
+    {
+        const int c8 = (int)(idx % c8n);
+        long long r = idx / c8n;
+        const int x = (int)(r % w);
+        r /= w;
+        const int y = (int)(r % h), img = (int)(r / h);
+        float a[8], b[8], m[8];
+        unpack8_bf16(*reinterpret_cast<const uint4*>(du + (size_t)(idx / c8n) * duC + c8 * 8), a);
+        const size_t ph = ((size_t)img * (h >> 1) + (y >> 1)) * (w >> 1) + (x >> 1);
+        unpack8_bf16(reinterpret_cast<const uint4*>(dpool + ph * c8n * 8)[c8], b);
+        unpack8_bf16(reinterpret_cast<const uint4*>(act)[idx], m);
+#pragma unroll
+        for (int j = 0; j < 8; ++j) a[j] = m[j] > 0.0f ? a[j] + 0.25f * b[j] : 0.0f;
+        reinterpret_cast<uint4*>(g)[idx] = pack8_bf16(a);
+    }
+}
+
+// Loss of the blend head and its gradient with respect to the 4 logits
+// (written as 16-channel bf16, channels 4..15 zero, the layout the last
+// layer's backward consumes).
+__global__ void k_loss(const i360b_blend_job* __restrict__ jobs, int n, int h, int w, const float4* __restrict__ logits,
+                       float invCount, bf16* __restrict__ g8, double* __restrict__ lossAcc)
+{
+    __shared__ float red[32];
+    const long long total = (long long)n * h * w;
+    float lsum = 0.0f;
+    for (long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x; idx < total;
+         idx += (long long)gridDim.x * blockDim.x)
+    {
+        const int img = (int)(idx / ((long long)h * w));
+        const int rem = (int)(idx % ((long long)h * w));
+        const int y = rem / w, x = rem % w;
+        const i360b_blend_job& J = jobs[img];
+        float dl[16];
+#pragma unroll
+        for (int j = 0; j < 16; ++j) dl[j] = 0.0f;
+        if (x < J.width && y < J.height)
+        {
+            const float4 lv = logits[idx];
+            const float l[4] = {lv.x, lv.y, lv.z, lv.w};
+            float o[3], wts[4], v[4][3];
+            bool cov[4];
+            int nCov;
+            composite_pixel(J, y, x, l, o, wts, v, cov, nCov);
+            const unsigned short* tp = J.target + (long long)y * J.targetRowStride + (long long)x * 3;
+            float d[3];
+#pragma unroll
+            for (int c = 0; c < 3; ++c)
+            {
+                const float e = (o[c] - (float)tp[c]) * kInScale;
+                lsum += e * e;
+                d[c] = 2.0f * e * invCount;
+            }
+#pragma unroll
+            for (int i = 0; i < kSlots; ++i)
+            {
+                if (!cov[i]) continue;
+                float s = 0.0f;
+#pragma unroll
+                for (int c = 0; c < 3; ++c) s += d[c] * (v[i][c] - o[c]) * kInScale;
+                dl[i] = wts[i] * s;
+            }
+        }
+        uint4* q = reinterpret_cast<uint4*>(g8 + idx * 16);
+        q[0] = pack8_bf16(dl);
+        q[1] = pack8_bf16(dl + 8);
+    }
+    for (int o = 16; o > 0; o >>= 1) lsum += __shfl_xor_sync(0xffffffffu, lsum, o);
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = lsum;
+    __syncthreads();
+    if (threadIdx.x < 32)
+    {
+        float v = threadIdx.x < (blockDim.x >> 5) ? red[threadIdx.x] : 0.0f;
+        for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+        if (threadIdx.x == 0) atomicAdd(lossAcc, (double)v * invCount);
+    }
+}
+
+// db[c] += sum over pixels of g[p][c], c < cout (g has C = 8 * c8n channels).
+__global__ void k_bias_grad(const bf16* __restrict__ g, long long pixels, int c8n, int cout, float* __restrict__ db)
+{
+    __shared__ float red[256 * 8];
+    const int lanes = blockDim.x / c8n;
+    const int c8 = threadIdx.x % c8n, lane = threadIdx.x / c8n;
+    float acc[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    if (lane < lanes)
+        for (long long p = (long long)blockIdx.x * lanes + lane; p < pixels; p += (long long)gridDim.x * lanes)
+        {
+            float v[8];
+            unpack8_bf16(reinterpret_cast<const uint4*>(g + p * c8n * 8)[c8], v);
+#pragma unroll
+            for (int j = 0; j < 8; ++j) acc[j] += v[j];
+        }
+#pragma unroll
+    for (int j = 0; j < 8; ++j) red[threadIdx.x * 8 + j] = lane < lanes ? acc[j] : 0.0f;
+    __syncthreads();
+    const int C = c8n * 8;
+    if ((int)threadIdx.x < C && (int)threadIdx.x < cout)
+    {
+        const int cc8 = threadIdx.x >> 3, j = threadIdx.x & 7;
+        float s = 0.0f;
+        for (int l = 0; l < lanes; ++l) s += red[(l * c8n + cc8) * 8 + j];
+        atomicAdd(&db[threadIdx.x], s);
+    }
+}
+
+__global__ void k_adam(float* __restrict__ p, const float* __restrict__ g, float* __restrict__ m, float* __restrict__ v,
+                       int count, float lr, float c1, float c2)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= count) return;
+    const float gi = g[i];
+    const float mi = 0.9f * m[i] + 0.1f * gi;
+    const float vi = 0.999f * v[i] + 0.001f * gi * gi;
+    m[i] = mi;
+    v[i] = vi;
+    p[i] -= lr * (mi * c1) / (sqrtf(vi * c2) + 1e-8f);
+}
+
+// Network layer table.
+struct LayerDef
+{
+    int cin, cout;
+};
+constexpr LayerDef kNet[8] = {{16, 32}, {32, 32}, {32, 64}, {64, 64}, {64, 64}, {96, 32}, {32, 32}, {32, 4}};
+constexpr int kNumLayers = 8;
+
+__host__ __device__ constexpr int pad16(int c) { return (c + 15) / 16 * 16; }
+
+struct PackArgs
+{
+    const float* params;
+    int cin[kNumLayers], cout[kNumLayers];
+    long long wOff[kNumLayers], bOff[kNumLayers];
+    bf16* fwd[kNumLayers];    // [pad16(cout)][9 * cin]
+    bf16* dgrad[kNumLayers];  // [cin][9 * pad16(cout)] flipped, transposed
+    float* bias[kNumLayers];  // [pad16(cout)]
+};
+
+// Packs the fp32 master parameters into the bf16 operands of the forward and
+// backward-data convolutions (blockIdx.y = layer).
+__global__ void k_pack_weights(PackArgs a)
+{
+    const int l = blockIdx.y;
+    const int cin = a.cin[l], cout = a.cout[l], np = pad16(cout);
+    const int K = 9 * cin, Kd = 9 * np;
+    const float* W = a.params + a.wOff[l];
+    const int nf = np * K, nd = cin * Kd;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nf + nd + np; i += gridDim.x * blockDim.x)
+    {
+        if (i < nf)
+        {
+            const int n = i / K, k = i % K;
+            a.fwd[l][i] = __float2bfloat16_rn(n < cout ? W[(size_t)n * K + k] : 0.0f);
+        }
+        else if (i < nf + nd)
+        {
+            const int j = i - nf, ci = j / Kd, kd = j % Kd, tap = kd / np, co = kd % np;
+            a.dgrad[l][j] = __float2bfloat16_rn(co < cout ? W[(size_t)co * K + (8 - tap) * cin + ci] : 0.0f);
+        }
+        else
+        {
+            const int c = i - nf - nd;
+            a.bias[l][c] = c < cout ? a.params[a.bOff[l] + c] : 0.0f;
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Launchers
+// ---------------------------------------------------------------------------
+int grid_for(long long work, int perSm)
+{
+    const long long cap = (long long)sm_count() * perSm;
+    return (int)std::max<long long>(1, std::min<long long>(work, cap));
+}
+
+int elementwise_grid(long long n, int block = 256)
+{
+    return (int)std::max<long long>(1, std::min<long long>((n + block - 1) / block, (long long)sm_count() * 16));
+}
+
+template <int CIN, int NPAD, int R, int LD, int EP>
+int run_conv(const ConvArgs& a, cudaStream_t s)
+{
+    using S = ConvShape<CIN, NPAD, R>;
+    static std::once_flag once;
+    static int perSm = 1;
+    static cudaError_t attrErr = cudaSuccess;
+    std::call_once(once, [] {
+        attrErr = cudaFuncSetAttribute(k_conv3x3<CIN, NPAD, R, LD, EP>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)S::kSmem);
+        int occ = 1;
+        if (attrErr == cudaSuccess)
+            attrErr = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_conv3x3<CIN, NPAD, R, LD, EP>, 128, S::kSmem);
+        perSm = std::max(1, std::min<int>(occ, 512 / (int)S::kTmem));
+    });
+    if (attrErr != cudaSuccess) return cuda_fail(attrErr, "conv3x3 attributes");
+    const long long tiles = (long long)a.n * ((a.h + R - 1) / R) * (a.w / kTileX);
+    if (tiles == 0) return I360B_SUCCESS;
+    k_conv3x3<CIN, NPAD, R, LD, EP><<<grid_for(tiles, perSm), 128, S::kSmem, s>>>(a);
+    return check_launch("conv3x3 kernel");
+}
+
+// The (cin, npad) shapes the network uses, forward and backward.
+int dispatch_conv(int cin, int npad, int loader, int ep, const ConvArgs& a, cudaStream_t s)
+{
+#define I360B_CONV(CI, NP, R, LD, EP_)                                        \
+    if (cin == CI && npad == NP && loader == LD && ep == EP_) return run_conv<CI, NP, R, LD, EP_>(a, s);
+    // forward
+    I360B_CONV(16, 32, 4, LD_PLAIN, EP_RELU)
+    I360B_CONV(32, 32, 2, LD_PLAIN, EP_RELU)
+    I360B_CONV(32, 64, 2, LD_PLAIN, EP_RELU)
+    I360B_CONV(64, 64, 2, LD_PLAIN, EP_RELU)
+    I360B_CONV(96, 32, 1, LD_CONCAT, EP_RELU)
+    I360B_CONV(32, 16, 4, LD_PLAIN, EP_LOGITS)
+    I360B_CONV(32, 16, 4, LD_PLAIN, EP_COMPOSITE)
+    // backward data
+    I360B_CONV(16, 32, 4, LD_PLAIN, EP_MASK)
+    I360B_CONV(32, 32, 2, LD_PLAIN, EP_MASK)
+    I360B_CONV(32, 96, 2, LD_PLAIN, EP_RAW)
+    I360B_CONV(64, 64, 2, LD_PLAIN, EP_MASK)
+    I360B_CONV(64, 32, 2, LD_PLAIN, EP_RAW)
+#undef I360B_CONV
+    return fail(I360B_NOT_SUPPORTED, "conv3x3: no kernel for cin=%d cout=%d loader=%d epilogue=%d", cin, npad, loader,
+                ep);
+}
+
+template <int CIN, int COUT, int LD>
+int run_wgrad(const WgradArgs& base, float* dw, int cout, void* scratch, size_t scratchBytes, cudaStream_t s)
+{
+    using S = WgradShape<CIN, COUT>;
+    static std::once_flag once;
+    static int perSm = 1;
+    static cudaError_t attrErr = cudaSuccess;
+    std::call_once(once, [] {
+        attrErr = cudaFuncSetAttribute(k_conv3x3_wgrad<CIN, COUT, LD>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)S::kSmem);
+        int occ = 1;
+        if (attrErr == cudaSuccess)
+            attrErr = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_conv3x3_wgrad<CIN, COUT, LD>, 128, S::kSmem);
+        perSm = std::max(1, std::min<int>(std::min(occ, 2), 512 / (int)S::kTmem));
+    });
+    if (attrErr != cudaSuccess) return cuda_fail(attrErr, "wgrad attributes");
+    const long long tiles = (long long)base.n * base.h * (base.w / kTileX);
+    const int slices = (int)std::max<long long>(
+        1, std::min<long long>(tiles, (long long)sm_count() * perSm / S::kChunks));
+    const size_t need = (size_t)slices * S::kChunks * 128 * COUT * sizeof(float);
+    if (need > scratchBytes) return fail(I360B_OUT_OF_MEMORY, "wgrad scratch too small (%zu > %zu)", need, scratchBytes);
+    WgradArgs a = base;
+    a.partial = static_cast<float*>(scratch);
+    k_conv3x3_wgrad<CIN, COUT, LD><<<dim3(slices, S::kChunks), 128, S::kSmem, s>>>(a);
+    I360B_TRY(check_launch("wgrad kernel"));
+    const int total = 9 * CIN * cout;
+    k_wgrad_reduce<<<(total + 255) / 256, 256, 0, s>>>(a.partial, slices, S::kChunks * 128, COUT, CIN, cout, dw);
+    return check_launch("wgrad reduce kernel");
+}
+
+size_t wgrad_scratch_bytes()
+{
+    // Upper bound over the supported shapes: slices <= 2 * SMs / chunks.
+    size_t mx = 0;
+    const int sms = sm_count();
+    auto f = [&](int cin, int cout) {
+        const int chunks = (9 * cin / 8 + 15) / 16;
+        const size_t slices = std::max(1, 2 * sms / chunks);
+        mx = std::max(mx, slices * chunks * 128 * cout * sizeof(float));
+    };
+    f(16, 32), f(32, 32), f(32, 64), f(64, 64), f(96, 32), f(32, 16);
+    return mx;
+}
+
+int dispatch_wgrad(int cin, int cout, int loader, const WgradArgs& a, float* dw, int coutReal, void* scratch,
+                   size_t bytes, cudaStream_t s)
+{
+#define I360B_WG(CI, CO, LD) \
+    if (cin == CI && cout == CO && loader == LD) return run_wgrad<CI, CO, LD>(a, dw, coutReal, scratch, bytes, s);
+    I360B_WG(16, 32, LD_PLAIN)
+    I360B_WG(32, 32, LD_PLAIN)
+    I360B_WG(32, 64, LD_PLAIN)
+    I360B_WG(64, 64, LD_PLAIN)
+    I360B_WG(96, 32, LD_CONCAT)
+    I360B_WG(32, 16, LD_PLAIN)
+#undef I360B_WG
+    return fail(I360B_NOT_SUPPORTED, "conv3x3 wgrad: no kernel for cin=%d cout=%d loader=%d", cin, cout, loader);
+}
+
+int check_window(int n, int w, int h)
+{
+    if (n <= 0 || w <= 0 || h <= 0) return fail(I360B_INVALID_PARAM, "Invalid dimensions.");
+    if (w % 256 != 0 || h % 2 != 0)
+        return fail(I360B_INVALID_PARAM, "blend network windows need width %% 256 == 0 and even height (got %dx%d)", w,
+                    h);
+    return I360B_SUCCESS;
+}
+}  // namespace
+
+// ---------------------------------------------------------------------------
+// The network object
+// ---------------------------------------------------------------------------
+struct BlendNet
+{
+    int device = 0;
+    long long wOff[kNumLayers], bOff[kNumLayers];
+    int nParams = 0;
+    float* params = nullptr;
+    float* grads = nullptr;
+    float* adamM = nullptr;
+    float* adamV = nullptr;
+    bf16* packed = nullptr;  // forward and backward-data weights of all layers
+    float* biasPacked = nullptr;
+    bf16* fwdW[kNumLayers];
+    bf16* dgW[kNumLayers];
+    float* bias[kNumLayers];
+    int step = 0;
+    // Per-batch buffers (grown on demand).
+    size_t capPix = 0;
+    char* act = nullptr;
+    bf16 *x0 = nullptr, *a1 = nullptr, *a2 = nullptr, *p2 = nullptr, *a3 = nullptr, *a4 = nullptr, *a5 = nullptr,
+         *a6 = nullptr, *a7 = nullptr;
+    float* logits = nullptr;
+    bf16 *g8 = nullptr, *gA = nullptr, *gB = nullptr, *du = nullptr, *gh1 = nullptr, *gh2 = nullptr, *dp = nullptr;
+    void* wgScratch = nullptr;
+    size_t wgBytes = 0;
+    double* dLoss = nullptr;
+    int* dError = nullptr;
+    i360b_blend_job* dJobs = nullptr;
+    i360b_blend_job* hJobs = nullptr;  // pinned staging
+    int jobCap = 0;
+    cudaEvent_t jobsUploaded = nullptr;
+    std::mutex mu;
+
+    ~BlendNet()
+    {
+        cudaFree(params);
+        cudaFree(grads);
+        cudaFree(adamM);
+        cudaFree(adamV);
+        cudaFree(packed);
+        cudaFree(biasPacked);
+        cudaFree(act);
+        cudaFree(wgScratch);
+        cudaFree(dLoss);
+        cudaFree(dError);
+        cudaFree(dJobs);
+        if (hJobs) cudaFreeHost(hJobs);
+        if (jobsUploaded) cudaEventDestroy(jobsUploaded);
+    }
+
+    int init(unsigned long long seed)
+    {
+        long long off = 0;
+        for (int l = 0; l < kNumLayers; ++l)
+        {
+            wOff[l] = off;
+            off += 9LL * kNet[l].cin * kNet[l].cout;
+            bOff[l] = off;
+            off += kNet[l].cout;
+        }
+        nParams = (int)off;
+        const size_t pb = (size_t)nParams * sizeof(float);
+        I360B_CUDA(cudaMalloc(&params, pb), "blendnet params");
+        I360B_CUDA(cudaMalloc(&grads, pb), "blendnet grads");
+        I360B_CUDA(cudaMalloc(&adamM, pb), "blendnet adam");
+        I360B_CUDA(cudaMalloc(&adamV, pb), "blendnet adam");
+        I360B_CUDA(cudaMemset(adamM, 0, pb), "blendnet adam");
+        I360B_CUDA(cudaMemset(adamV, 0, pb), "blendnet adam");
+        size_t pk = 0, bk = 0;
+        for (int l = 0; l < kNumLayers; ++l)
+        {
+            pk += (size_t)pad16(kNet[l].cout) * 9 * kNet[l].cin + (size_t)kNet[l].cin * 9 * pad16(kNet[l].cout);
+            bk += pad16(kNet[l].cout);
+        }
+        I360B_CUDA(cudaMalloc(&packed, pk * sizeof(bf16)), "blendnet packed weights");
+        I360B_CUDA(cudaMalloc(&biasPacked, bk * sizeof(float)), "blendnet packed bias");
+        size_t o = 0, ob = 0;
+        for (int l = 0; l < kNumLayers; ++l)
+        {
+            fwdW[l] = packed + o;
+            o += (size_t)pad16(kNet[l].cout) * 9 * kNet[l].cin;
+            dgW[l] = packed + o;
+            o += (size_t)kNet[l].cin * 9 * pad16(kNet[l].cout);
+            bias[l] = biasPacked + ob;
+            ob += pad16(kNet[l].cout);
+        }
+        wgBytes = wgrad_scratch_bytes();
+        I360B_CUDA(cudaMalloc(&wgScratch, wgBytes), "blendnet wgrad scratch");
+        I360B_CUDA(cudaMalloc(&dLoss, sizeof(double)), "blendnet loss");
+        I360B_CUDA(cudaMalloc(&dError, sizeof(int)), "blendnet error flag");
+        I360B_CUDA(cudaMemset(dError, 0, sizeof(int)), "blendnet error flag");
+        I360B_CUDA(cudaEventCreateWithFlags(&jobsUploaded, cudaEventDisableTiming), "blendnet event");
+        // He-normal weights, zero biases, zero last layer (the untrained head
+        // is then the coverage-weighted mean of the layers).
+        std::vector<float> h(nParams, 0.0f);
+        std::mt19937_64 rng(seed);
+        std::normal_distribution<float> nd(0.0f, 1.0f);
+        for (int l = 0; l < kNumLayers - 1; ++l)
+        {
+            const float sd = std::sqrt(2.0f / (9.0f * kNet[l].cin));
+            for (long long i = 0; i < 9LL * kNet[l].cin * kNet[l].cout; ++i) h[wOff[l] + i] = nd(rng) * sd;
+        }
+        return upload(h.data());
+    }
+
+    int upload(const float* host)
+    {
+        I360B_CUDA(cudaMemcpy(params, host, (size_t)nParams * sizeof(float), cudaMemcpyHostToDevice), "param upload");
+        return pack(nullptr);
+    }
+
+    int pack(cudaStream_t s)
+    {
+        PackArgs a;
+        a.params = params;
+        for (int l = 0; l < kNumLayers; ++l)
+        {
+            a.cin[l] = kNet[l].cin;
+            a.cout[l] = kNet[l].cout;
+            a.wOff[l] = wOff[l];
+            a.bOff[l] = bOff[l];
+            a.fwd[l] = fwdW[l];
+            a.dgrad[l] = dgW[l];
+            a.bias[l] = bias[l];
+        }
+        k_pack_weights<<<dim3(64, kNumLayers), 256, 0, s>>>(a);
+        return check_launch("weight pack kernel");
+    }
+
+    int reserve(int n, int w, int h)
+    {
+        const size_t pix = (size_t)n * w * h;
+        if (pix <= capPix) return I360B_SUCCESS;
+        cudaDeviceSynchronize();
+        cudaFree(act);
+        act = nullptr;
+        capPix = 0;
+        const size_t half = pix / 4;
+        // bf16 element counts of every buffer, then the fp32 logits.
+        const size_t counts[] = {pix * 16,  pix * 32, pix * 32, half * 32, half * 64, half * 64, half * 64,
+                                 pix * 32,  pix * 32, pix * 16, pix * 32,  pix * 32,  pix * 96,  half * 64,
+                                 half * 64, half * 32};
+        size_t total = 0;
+        for (size_t c : counts) total += (c * sizeof(bf16) + 255) / 256 * 256;
+        total += pix * 4 * sizeof(float);
+        cudaError_t e = cudaMalloc(&act, total);
+        if (e != cudaSuccess)
+        {
+            cudaGetLastError();
+            act = nullptr;
+            return fail(I360B_OUT_OF_MEMORY, "blend network: %zu bytes of activations for %d windows of %dx%d", total,
+                        n, w, h);
+        }
+        bf16** slots[] = {&x0, &a1, &a2, &p2, &a3, &a4, &a5, &a6, &a7, &g8, &gA, &gB, &du, &gh1, &gh2, &dp};
+        size_t o = 0;
+        for (size_t i = 0; i < sizeof(counts) / sizeof(counts[0]); ++i)
+        {
+            *slots[i] = reinterpret_cast<bf16*>(act + o);
+            o += (counts[i] * sizeof(bf16) + 255) / 256 * 256;
+        }
+        logits = reinterpret_cast<float*>(act + o);
+        capPix = pix;
+        return I360B_SUCCESS;
+    }
+
+    int upload_jobs(const i360b_blend_job* jobs, int n, cudaStream_t s)
+    {
+        if (!jobs) return fail(I360B_INVALID_PARAM, "Null pointer argument.");
+        if (n > jobCap)
+        {
+            cudaDeviceSynchronize();
+            cudaFree(dJobs);
+            if (hJobs) cudaFreeHost(hJobs);
+            dJobs = nullptr;
+            hJobs = nullptr;
+            jobCap = 0;
+            I360B_CUDA(cudaMalloc(&dJobs, (size_t)n * sizeof(i360b_blend_job)), "blend jobs");
+            I360B_CUDA(cudaMallocHost(&hJobs, (size_t)n * sizeof(i360b_blend_job)), "blend jobs");
+            jobCap = n;
+        }
+        else
+        {
+            I360B_CUDA(cudaEventSynchronize(jobsUploaded), "blend jobs");
+        }
+        std::memcpy(hJobs, jobs, (size_t)n * sizeof(i360b_blend_job));
+        I360B_CUDA(cudaMemcpyAsync(dJobs, hJobs, (size_t)n * sizeof(i360b_blend_job), cudaMemcpyHostToDevice, s),
+                   "blend jobs");
+        I360B_CUDA(cudaEventRecord(jobsUploaded, s), "blend jobs");
+        return I360B_SUCCESS;
+    }
+
+    ConvArgs conv(const bf16* x, int n, int w, int h, int l, void* out, int ep) const
+    {
+        ConvArgs a{};
+        a.x = x;
+        a.n = n;
+        a.h = h;
+        a.w = w;
+        a.wt = fwdW[l];
+        a.bias = bias[l];
+        a.out = out;
+        a.jobs = dJobs;
+        a.error = dError;
+        (void)ep;
+        return a;
+    }
+
+    // Forward pass; the last layer writes logits (train) or the composite.
+    int forward(int n, int w, int h, bool composite, cudaStream_t s)
+    {
+        const int hw = w / 2, hh = h / 2;
+        k_pack_input<<<elementwise_grid((long long)n * w * h), 256, 0, s>>>(dJobs, n, h, w, x0);
+        I360B_TRY(check_launch("input pack kernel"));
+        I360B_TRY(dispatch_conv(16, 32, LD_PLAIN, EP_RELU, conv(x0, n, w, h, 0, a1, EP_RELU), s));
+        I360B_TRY(dispatch_conv(32, 32, LD_PLAIN, EP_RELU, conv(a1, n, w, h, 1, a2, EP_RELU), s));
+        k_pool2<<<elementwise_grid((long long)n * hw * hh * 4), 256, 0, s>>>(a2, n, h, w, 4, p2);
+        I360B_TRY(check_launch("pool kernel"));
+        I360B_TRY(dispatch_conv(32, 64, LD_PLAIN, EP_RELU, conv(p2, n, hw, hh, 2, a3, EP_RELU), s));
+        I360B_TRY(dispatch_conv(64, 64, LD_PLAIN, EP_RELU, conv(a3, n, hw, hh, 3, a4, EP_RELU), s));
+        I360B_TRY(dispatch_conv(64, 64, LD_PLAIN, EP_RELU, conv(a4, n, hw, hh, 4, a5, EP_RELU), s));
+        ConvArgs c6 = conv(a2, n, w, h, 5, a6, EP_RELU);
+        c6.u = a5;
+        c6.cs = 32;
+        I360B_TRY(dispatch_conv(96, 32, LD_CONCAT, EP_RELU, c6, s));
+        I360B_TRY(dispatch_conv(32, 32, LD_PLAIN, EP_RELU, conv(a6, n, w, h, 6, a7, EP_RELU), s));
+        if (composite) return dispatch_conv(32, 16, LD_PLAIN, EP_COMPOSITE, conv(a7, n, w, h, 7, nullptr, 0), s);
+        return dispatch_conv(32, 16, LD_PLAIN, EP_LOGITS, conv(a7, n, w, h, 7, logits, 0), s);
+    }
+
+    // Backward data through layer l (flipped, transposed weights).
+    int dgrad(int l, const bf16* g, int n, int w, int h, const bf16* actMask, void* out, int ep, cudaStream_t s)
+    {
+        ConvArgs a{};
+        a.x = g;
+        a.n = n;
+        a.h = h;
+        a.w = w;
+        a.wt = dgW[l];
+        a.out = out;
+        a.act = actMask;
+        a.error = dError;
+        return dispatch_conv(pad16(kNet[l].cout), kNet[l].cin, LD_PLAIN, ep, a, s);
+    }
+
+    int wgrad(int l, const bf16* x, const bf16* u, int cs, const bf16* g, int n, int w, int h, cudaStream_t s)
+    {
+        WgradArgs a{};
+        a.x = x;
+        a.u = u;
+        a.cs = cs;
+        a.g = g;
+        a.n = n;
+        a.h = h;
+        a.w = w;
+        a.error = dError;
+        I360B_TRY(dispatch_wgrad(kNet[l].cin, pad16(kNet[l].cout), cs ? LD_CONCAT : LD_PLAIN, a, grads + wOff[l],
+                                 kNet[l].cout, wgScratch, wgBytes, s));
+        const long long pixels = (long long)n * w * h;
+        const int c8n = pad16(kNet[l].cout) / 8;
+        k_bias_grad<<<std::min<long long>(sm_count() * 4, (pixels + 255) / 256), 256, 0, s>>>(g, pixels, c8n,
+                                                                                              kNet[l].cout,
+                                                                                              grads + bOff[l]);
+        return check_launch("bias gradient kernel");
+    }
+
+    // Loss, then every parameter gradient into `grads`.
+    int backward(int n, int w, int h, cudaStream_t s)
+    {
+        const int hw = w / 2, hh = h / 2;
+        const long long pix = (long long)n * w * h;
+        I360B_CUDA(cudaMemsetAsync(dLoss, 0, sizeof(double), s), "loss reset");
+        I360B_CUDA(cudaMemsetAsync(grads, 0, (size_t)nParams * sizeof(float), s), "grad reset");
+        k_loss<<<elementwise_grid(pix), 256, 0, s>>>(dJobs, n, h, w, reinterpret_cast<const float4*>(logits),
+                                                   (float)(1.0 / (3.0 * (double)pix)), g8, dLoss);
+        I360B_TRY(check_launch("loss kernel"));
+        // layer 8 (32 -> 4): input a7
+        I360B_TRY(wgrad(7, a7, nullptr, 0, g8, n, w, h, s));
+        I360B_TRY(dgrad(7, g8, n, w, h, a7, gA, EP_MASK, s));  // gA = g7
+        // layer 7 (32 -> 32): input a6
+        I360B_TRY(wgrad(6, a6, nullptr, 0, gA, n, w, h, s));
+        I360B_TRY(dgrad(6, gA, n, w, h, a6, gB, EP_MASK, s));  // gB = g6
+        // layer 6 (96 -> 32): input concat(a2, up(a5))
+        I360B_TRY(wgrad(5, a2, a5, 32, gB, n, w, h, s));
+        I360B_TRY(dgrad(5, gB, n, w, h, nullptr, du, EP_RAW, s));
+        k_upsample_grad<<<elementwise_grid((long long)n * hw * hh * 8), 256, 0, s>>>(du, 96, 32, a5, n, h, w, 8, gh1);
+        I360B_TRY(check_launch("upsample gradient kernel"));  // gh1 = g5
+        // layer 5 (64 -> 64): input a4
+        I360B_TRY(wgrad(4, a4, nullptr, 0, gh1, n, hw, hh, s));
+        I360B_TRY(dgrad(4, gh1, n, hw, hh, a4, gh2, EP_MASK, s));  // gh2 = g4
+        // layer 4 (64 -> 64): input a3
+        I360B_TRY(wgrad(3, a3, nullptr, 0, gh2, n, hw, hh, s));
+        I360B_TRY(dgrad(3, gh2, n, hw, hh, a3, gh1, EP_MASK, s));  // gh1 = g3
+        // layer 3 (32 -> 64): input p2
+        I360B_TRY(wgrad(2, p2, nullptr, 0, gh1, n, hw, hh, s));
+        I360B_TRY(dgrad(2, gh1, n, hw, hh, nullptr, dp, EP_RAW, s));  // dp = d(pool)
+        k_skip_grad<<<elementwise_grid(pix * 4), 256, 0, s>>>(du, 96, dp, a2, n, h, w, 4, gA);
+        I360B_TRY(check_launch("skip gradient kernel"));  // gA = g2
+        // layer 2 (32 -> 32): input a1
+        I360B_TRY(wgrad(1, a1, nullptr, 0, gA, n, w, h, s));
+        I360B_TRY(dgrad(1, gA, n, w, h, a1, gB, EP_MASK, s));  // gB = g1
+        // layer 1 (16 -> 32): input x0
+        return wgrad(0, x0, nullptr, 0, gB, n, w, h, s);
+    }
+
+    int adam(float lr, cudaStream_t s)
+    {
+        ++step;
+        const float c1 = (float)(1.0 / (1.0 - std::pow(0.9, step)));
+        const float c2 = (float)(1.0 / (1.0 - std::pow(0.999, step)));
+        k_adam<<<(nParams + 255) / 256, 256, 0, s>>>(params, grads, adamM, adamV, nParams, lr, c1, c2);
+        I360B_TRY(check_launch("adam kernel"));
+        return pack(s);
+    }
+
+    int check_error(cudaStream_t s)
+    {
+        int e = 0;
+        I360B_CUDA(cudaMemcpyAsync(&e, dError, sizeof(int), cudaMemcpyDeviceToHost, s), "error flag");
+        I360B_CUDA(cudaStreamSynchronize(s), "blend network");
+        if (e)
+        {
+            cudaMemsetAsync(dError, 0, sizeof(int), s);
+            return fail(I360B_KERNEL_LAUNCH_FAILED, "a tensor-core convolution gave up waiting for its MMAs");
+        }
+        return I360B_SUCCESS;
+    }
+};
+}  // namespace i360b
+
+struct i360b_blendnet
+{
+    i360b::BlendNet net;
+};
+
+using namespace i360b;
+
+namespace
+{
+int net_prologue(i360b_blendnet* net)
+{
+    clear_error();
+    if (!initialized()) return fail(I360B_CUDA_ERROR, "Not initialized.");
+    I360B_TRY(ensure_ready());
+    if (!net) return fail(I360B_INVALID_PARAM, "Null pointer argument.");
+    return I360B_SUCCESS;
+}
+}  // namespace
+
+extern "C" int i360b_blendnet_param_count(void)
+{
+    int n = 0;
+    for (int l = 0; l < kNumLayers; ++l) n += 9 * kNet[l].cin * kNet[l].cout + kNet[l].cout;
+    return n;
+}
+
+extern "C" int i360b_blendnet_create(unsigned long long seed, i360b_blendnet** outNet)
+{
+    clear_error();
+    if (!initialized()) return fail(I360B_CUDA_ERROR, "Not initialized.");
+    I360B_TRY(ensure_ready());
+    if (!outNet) return fail(I360B_INVALID_PARAM, "Null pointer argument.");
+    *outNet = nullptr;
+    auto* p = new (std::nothrow) i360b_blendnet;
+    if (!p) return fail(I360B_OUT_OF_MEMORY, "blend network: host allocation failed");
+    int rc = p->net.init(seed);
+    if (rc != I360B_SUCCESS)
+    {
+        delete p;
+        return rc;
+    }
+    I360B_CUDA(cudaDeviceSynchronize(), "blend network init");
+    *outNet = p;
+    return I360B_SUCCESS;
+}
+
+extern "C" void i360b_blendnet_destroy(i360b_blendnet* net)
+{
+    if (!net) return;
+    cudaDeviceSynchronize();
+    delete net;
+}
+
+extern "C" int i360b_blendnet_get_params(i360b_blendnet* net, float* hostParams, int count)
+{
+    I360B_TRY(net_prologue(net));
+    if (!hostParams || count != net->net.nParams) return fail(I360B_INVALID_PARAM, "parameter count mismatch");
+    I360B_CUDA(cudaDeviceSynchronize(), "blend network");
+    I360B_CUDA(cudaMemcpy(hostParams, net->net.params, (size_t)count * sizeof(float), cudaMemcpyDeviceToHost),
+               "param download");
+    return I360B_SUCCESS;
+}
+
+extern "C" int i360b_blendnet_set_params(i360b_blendnet* net, const float* hostParams, int count)
+{
+    I360B_TRY(net_prologue(net));
+    if (!hostParams || count != net->net.nParams) return fail(I360B_INVALID_PARAM, "parameter count mismatch");
+    I360B_CUDA(cudaDeviceSynchronize(), "blend network");
+    I360B_TRY(net->net.upload(hostParams));
+    I360B_CUDA(cudaDeviceSynchronize(), "blend network");
+    return I360B_SUCCESS;
+}
+
+extern "C" int i360b_blendnet_logits(i360b_blendnet* net, const i360b_blend_job* jobs, int n, int w, int h,
+                                     float* dLogits)
+{
+    I360B_TRY(net_prologue(net));
+    I360B_TRY(check_window(n, w, h));
+    if (!dLogits) return fail(I360B_INVALID_PARAM, "Null pointer argument.");
+    BlendNet& N = net->net;
+    std::lock_guard<std::mutex> lk(N.mu);
+    cudaStream_t s = thread_stream();
+    I360B_TRY(N.reserve(n, w, h));
+    I360B_TRY(N.upload_jobs(jobs, n, s));
+    I360B_TRY(N.forward(n, w, h, false, s));
+    I360B_CUDA(cudaMemcpyAsync(dLogits, N.logits, (size_t)n * w * h * 4 * sizeof(float), cudaMemcpyDeviceToDevice, s),
+               "logits copy");
+    return N.check_error(s);
+}
+
+extern "C" int i360b_blendnet_gradients(i360b_blendnet* net, const i360b_blend_job* jobs, int n, int w, int h,
+                                        float* hostGrad, double* hostLoss)
+{
+    I360B_TRY(net_prologue(net));
+    I360B_TRY(check_window(n, w, h));
+    BlendNet& N = net->net;
+    std::lock_guard<std::mutex> lk(N.mu);
+    cudaStream_t s = thread_stream();
+    I360B_TRY(N.reserve(n, w, h));
+    I360B_TRY(N.upload_jobs(jobs, n, s));
+    I360B_TRY(N.forward(n, w, h, false, s));
+    I360B_TRY(N.backward(n, w, h, s));
+    I360B_TRY(N.check_error(s));
+    if (hostGrad)
+        I360B_CUDA(cudaMemcpy(hostGrad, N.grads, (size_t)N.nParams * sizeof(float), cudaMemcpyDeviceToHost),
+                   "grad download");
+    if (hostLoss) I360B_CUDA(cudaMemcpy(hostLoss, N.dLoss, sizeof(double), cudaMemcpyDeviceToHost), "loss download");
+    return I360B_SUCCESS;
+}
+
+extern "C" int i360b_blendnet_train_step(i360b_blendnet* net, const i360b_blend_job* jobs, int n, int w, int h,
+                                         float lr, double* hostLoss, void* stream)
+{
+    I360B_TRY(net_prologue(net));
+    I360B_TRY(check_window(n, w, h));
+    BlendNet& N = net->net;
+    std::lock_guard<std::mutex> lk(N.mu);
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    I360B_TRY(N.reserve(n, w, h));
+    I360B_TRY(N.upload_jobs(jobs, n, s));
+    I360B_TRY(N.forward(n, w, h, false, s));
+    I360B_TRY(N.backward(n, w, h, s));
+    I360B_TRY(N.adam(lr, s));
+    if (hostLoss)
+    {
+        I360B_CUDA(cudaMemcpyAsync(hostLoss, N.dLoss, sizeof(double), cudaMemcpyDeviceToHost, s), "loss download");
+        return N.check_error(s);
+    }
+    return I360B_SUCCESS;
+}
+
+extern "C" int i360b_blendnet_infer(i360b_blendnet* net, const i360b_blend_job* jobs, int n, int w, int h,
+                                    void* stream)
+{
+    I360B_TRY(net_prologue(net));
+    I360B_TRY(check_window(n, w, h));
+    BlendNet& N = net->net;
+    std::lock_guard<std::mutex> lk(N.mu);
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    I360B_TRY(N.reserve(n, w, h));
+    I360B_TRY(N.upload_jobs(jobs, n, s));
+    return N.forward(n, w, h, true, s);
+}
+
+extern "C" int i360b_conv3x3_forward(const void* dX, const void* dU, int skipChannels, int n, int h, int w, int cin,
+                                     int cout, const void* dWeights, const float* dBias, int epilogue,
+                                     const void* dAct, void* dOut, void* stream)
+{
+    clear_error();
+    if (!initialized()) return fail(I360B_CUDA_ERROR, "Not initialized.");
+    I360B_TRY(ensure_ready());
+    if (!dX || !dWeights || !dOut || (skipChannels > 0 && !dU)) return fail(I360B_INVALID_PARAM, "Null pointer argument.");
+    if (n <= 0 || h <= 0 || w <= 0 || w % kTileX != 0) return fail(I360B_INVALID_PARAM, "Invalid dimensions.");
+    if ((epilogue == EP_RELU || epilogue == EP_LOGITS) && !dBias) return fail(I360B_INVALID_PARAM, "Null pointer argument.");
+    if (epilogue == EP_MASK && !dAct) return fail(I360B_INVALID_PARAM, "Null pointer argument.");
+    if (epilogue < EP_RELU || epilogue > EP_RAW) return fail(I360B_INVALID_PARAM, "unknown epilogue %d", epilogue);
+    if (skipChannels > 0 && (h % 2 || w % 256 || skipChannels % 8 || skipChannels >= cin))
+        return fail(I360B_INVALID_PARAM, "Invalid dimensions.");
+    static int* dErr = nullptr;
+    if (!dErr) I360B_CUDA(cudaMalloc(&dErr, sizeof(int)), "error flag");
+    ConvArgs a{};
+    a.x = static_cast<const bf16*>(dX);
+    a.u = static_cast<const bf16*>(dU);
+    a.cs = skipChannels;
+    a.n = n;
+    a.h = h;
+    a.w = w;
+    a.wt = static_cast<const bf16*>(dWeights);
+    a.bias = dBias;
+    a.out = dOut;
+    a.act = static_cast<const bf16*>(dAct);
+    a.error = dErr;
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    I360B_CUDA(cudaMemsetAsync(dErr, 0, sizeof(int), s), "error flag");
+    I360B_TRY(dispatch_conv(cin, cout, skipChannels > 0 ? LD_CONCAT : LD_PLAIN, epilogue, a, s));
+    int e = 0;
+    I360B_CUDA(cudaMemcpyAsync(&e, dErr, sizeof(int), cudaMemcpyDeviceToHost, s), "error flag");
+    I360B_CUDA(cudaStreamSynchronize(s), "conv3x3");
+    if (e) return fail(I360B_KERNEL_LAUNCH_FAILED, "conv3x3 gave up waiting for its MMAs");
+    return I360B_SUCCESS;
+}
+
+extern "C" int i360b_conv3x3_wgrad(const void* dX, const void* dU, int skipChannels, const void* dGrad, int n, int h,
+                                   int w, int cin, int cout, float* dGradW, void* stream)
+{
+    clear_error();
+    if (!initialized()) return fail(I360B_CUDA_ERROR, "Not initialized.");
+    I360B_TRY(ensure_ready());
+    if (!dX || !dGrad || !dGradW || (skipChannels > 0 && !dU)) return fail(I360B_INVALID_PARAM, "Null pointer argument.");
+    if (n <= 0 || h <= 0 || w <= 0 || w % kTileX != 0) return fail(I360B_INVALID_PARAM, "Invalid dimensions.");
+    if (skipChannels > 0 && (h % 2 || w % 256 || skipChannels % 8 || skipChannels >= cin))
+        return fail(I360B_INVALID_PARAM, "Invalid dimensions.");
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    static int* dErr = nullptr;
+    if (!dErr) I360B_CUDA(cudaMalloc(&dErr, sizeof(int)), "error flag");
+    const size_t bytes = wgrad_scratch_bytes();
+    void* scratch = nullptr;
+    I360B_TRY(dev_alloc(&scratch, bytes, s, "wgrad scratch"));
+    WgradArgs a{};
+    a.x = static_cast<const bf16*>(dX);
+    a.u = static_cast<const bf16*>(dU);
+    a.cs = skipChannels;
+    a.g = static_cast<const bf16*>(dGrad);
+    a.n = n;
+    a.h = h;
+    a.w = w;
+    a.error = dErr;
+    I360B_CUDA(cudaMemsetAsync(dErr, 0, sizeof(int), s), "error flag");
+    int rc = dispatch_wgrad(cin, cout, skipChannels > 0 ? LD_CONCAT : LD_PLAIN, a, dGradW, cout, scratch, bytes, s);
+    int e = 0;
+    cudaMemcpyAsync(&e, dErr, sizeof(int), cudaMemcpyDeviceToHost, s);
+    cudaStreamSynchronize(s);
+    dev_free(scratch, s);
+    if (rc != I360B_SUCCESS) return rc;
+    if (e) return fail(I360B_KERNEL_LAUNCH_FAILED, "conv3x3 wgrad gave up waiting for its MMAs");
+    return I360B_SUCCESS;
+}

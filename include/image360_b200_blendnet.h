@@ -1,0 +1,115 @@
+/*
+ * image360_b200 - learned seam blend: the C-ABI of the blend network and its
+ * tensor-core convolution primitives.
+ *
+ * No counterpart in the reference, which blends overlaps only with the
+ * multi-band Laplacian seam blend (WindowsApp.Core/SourceFiles/SeamBlend.cpp:549-587).
+ * The network stands in for that blend on overlap windows:
+ *
+ *   input   16 channels per pixel: up to 4 warped RGB48 layers, each as R, G, B
+ *           (value / 32768) and a coverage mask (1 where the layer is not
+ *           (0,0,0), SeamBlend.cpp:565), in bf16;
+ *   net     a 2-scale U-Net-lite of eight 3x3 convolutions with zero padding:
+ *           16->32, 32->32 (full resolution, kept as the skip), 2x2 average
+ *           pool, 32->64, 64->64, 64->64 (half resolution), nearest 2x
+ *           upsample concatenated after the skip (96 channels), 96->32, 32->32,
+ *           32->4; ReLU after all but the last; bf16 weights and activations,
+ *           fp32 accumulation (tcgen05 tensor cores) and fp32 bias;
+ *   head    the 4 outputs are per-layer blend logits; a softmax over the
+ *           layers that cover the pixel weights the layers' original 16-bit
+ *           values into the RGB48 output (no layer covers -> 0).
+ *
+ * With all logits equal (the untrained network: the last layer starts at
+ * zero) the head is the coverage-weighted mean of the layers.  Training
+ * minimises the mean squared error against the plain seam blend of the same
+ * window (Adam).  Window width must be a multiple of 256, height even.
+ *
+ * All pointers named d* are device pointers; `stream` is a cudaStream_t.
+ */
+#ifndef IMAGE360_B200_BLENDNET_H
+#define IMAGE360_B200_BLENDNET_H
+
+#include "image360_b200.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* One window of a batch.  Slot i of pixel (x, y) of the window is
+ * slot[i][y * rowStride + x * pixStride + c] for c = R, G, B (element
+ * offsets); a null slot is an absent layer.  Pixels with x >= width or
+ * y >= height lie outside the image (input zero, nothing written). */
+typedef struct i360b_blend_job
+{
+    const unsigned short* slot[4];
+    long long pixStride;
+    long long rowStride;
+    int width;
+    int height;
+    /* Training: target RGB48 of the window (same stride convention). */
+    const unsigned short* target;
+    long long targetRowStride;
+    /* Inference: RGB48 output (3 elements per pixel). */
+    unsigned short* out;
+    long long outRowStride;
+} i360b_blend_job;
+
+typedef struct i360b_blendnet i360b_blendnet;
+
+/* Number of fp32 parameters (weights [cout][ky][kx][cin] then bias, layer by
+ * layer). */
+I360B_API int i360b_blendnet_param_count(void);
+/* A network with He-normal weights from `seed`, zero biases and a zero last
+ * layer, on the current device. */
+I360B_API int i360b_blendnet_create(unsigned long long seed, i360b_blendnet** outNet);
+I360B_API void i360b_blendnet_destroy(i360b_blendnet* net);
+I360B_API int i360b_blendnet_get_params(i360b_blendnet* net, float* hostParams, int count);
+I360B_API int i360b_blendnet_set_params(i360b_blendnet* net, const float* hostParams, int count);
+/* Forward pass of `n` windows of w x h; writes the 4 logits per pixel as fp32
+ * [n][h][w][4] to dLogits.  Synchronous. */
+I360B_API int i360b_blendnet_logits(i360b_blendnet* net, const i360b_blend_job* jobs, int n, int w, int h,
+                                    float* dLogits);
+/* Loss (mean squared error over n*h*w*3 values, in units of 1/32768) and its
+ * gradient with respect to every parameter (hostGrad: param_count floats).
+ * Synchronous. */
+I360B_API int i360b_blendnet_gradients(i360b_blendnet* net, const i360b_blend_job* jobs, int n, int w, int h,
+                                       float* hostGrad, double* hostLoss);
+/* One Adam step (beta 0.9/0.999, eps 1e-8) at learning rate lr on the batch.
+ * hostLoss, when non-null, receives the batch loss before the step (the call
+ * then waits for the stream). */
+I360B_API int i360b_blendnet_train_step(i360b_blendnet* net, const i360b_blend_job* jobs, int n, int w, int h,
+                                        float lr, double* hostLoss, void* stream);
+/* Inference: blends each window into its job's output.  Asynchronous. */
+I360B_API int i360b_blendnet_infer(i360b_blendnet* net, const i360b_blend_job* jobs, int n, int w, int h,
+                                   void* stream);
+
+/* ---- convolution primitives (NHWC bf16, width a multiple of 128) --------- */
+
+/* Epilogues of i360b_conv3x3_forward. */
+enum
+{
+    I360B_CONV_BIAS_RELU = 0, /* out = bf16(max(acc + bias, 0)) */
+    I360B_CONV_LOGITS = 1,    /* out = fp32 (acc + bias) for channels 0..3 */
+    I360B_CONV_MASK = 2,      /* out = bf16(dAct > 0 ? acc : 0) (ReLU backward) */
+    I360B_CONV_RAW = 3        /* out = bf16(acc) */
+};
+
+/* 3x3 convolution, stride 1, zero padding 1.  dX is [n][h][w][cin]; with
+ * skipChannels > 0 the input is instead the concatenation of dX
+ * ([n][h][w][skipChannels]) and the nearest 2x upsample of dU
+ * ([n][h/2][w/2][cin - skipChannels]).  dWeights is bf16 [cout][3][3][cin],
+ * dBias fp32 [cout].  Supported (cin, cout): the layer shapes of the blend
+ * network and of its backward pass. */
+I360B_API int i360b_conv3x3_forward(const void* dX, const void* dU, int skipChannels, int n, int h, int w, int cin,
+                                    int cout, const void* dWeights, const float* dBias, int epilogue,
+                                    const void* dAct, void* dOut, void* stream);
+/* Weight gradient of that convolution: dGradW[cout][3][3][cin] (fp32,
+ * overwritten) = sum over pixels of dGrad[p][co] * input[p + tap][ci]. */
+I360B_API int i360b_conv3x3_wgrad(const void* dX, const void* dU, int skipChannels, const void* dGrad, int n, int h,
+                                  int w, int cin, int cout, float* dGradW, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* IMAGE360_B200_BLENDNET_H */
