@@ -212,6 +212,14 @@ __global__ void __launch_bounds__(256) k_warp_tiles(BlendArgs a, const Unit* __r
 // ring written by lane 31 of the previous row group, with a bounded wait on
 // that group's published progress.  The backward pass is the same code on
 // mirrored coordinates with the forward result as init.
+//
+// Progress is published per row group (prog[g] = columns of row group g's
+// last row that are final), never per ring slot: group g + nslots reuses
+// group g's slot while group g + 1 may still be waiting for columns of group
+// g, so a per-slot counter would let g + nslots's progress release that wait
+// early.  The slot data itself is safe to reuse: group g + nslots writes
+// column x only after group g + 1 has read well past x (each group trails
+// the one above by more than kLag * 31 columns, and nslots >= 2).
 // ---------------------------------------------------------------------------
 constexpr int kLag = 4;      // columns a row lags the row above
 constexpr int kDtRing = 4;   // row-group hand-off slots
@@ -235,7 +243,7 @@ __global__ void __launch_bounds__(512, 2) k_dt(BlendArgs a, const int* __restric
     const int RS = dt_ring_stride(W);
     float* ring = smem;
     int* prog = reinterpret_cast<int*>(smem + (size_t)nslots * RS);
-    if (threadIdx.x < nslots) prog[threadIdx.x] = -1;
+    for (int i = threadIdx.x; i < (H + 31) >> 5; i += blockDim.x) prog[i] = -1;
     __syncthreads();
     const float kInf = (float)(W + H);
     const float kDiag = 1.41421356f;
@@ -255,7 +263,7 @@ __global__ void __launch_bounds__(512, 2) k_dt(BlendArgs a, const int* __restric
         float* outRow = (BACK ? it.d : it.d1) + (size_t)rys * W;
         const float* d1Row = it.d1 + (size_t)rys * W;
         const uint32_t* covRow = it.cov + (size_t)rys * covWords;
-        const int slot = g % nslots, pslot = (g + nslots - 1) % nslots;
+        const int slot = g % nslots, pslot = (g + nslots - 1) % nslots;  // ring slots of g and g - 1
         float* ringOut = ring + slot * RS;
         const float* ringIn = ring + pslot * RS;
         float left = INF;               // own row, column x-1
@@ -269,10 +277,10 @@ __global__ void __launch_bounds__(512, 2) k_dt(BlendArgs a, const int* __restric
             int bad = 0;
             if (g > 0 && lane == 0)
             {
-                const int target = (g - 1) * (W + 1) + min(t0 + kLag + 1, W);
+                const int target = min(t0 + kLag + 1, W);
                 if (seen < target)
                 {
-                    cuda::atomic_ref<int, cuda::thread_scope_block> pr(prog[pslot]);
+                    cuda::atomic_ref<int, cuda::thread_scope_block> pr(prog[g - 1]);
                     long long tstart = clock64();
                     int spins = 0;
                     while ((seen = pr.load(cuda::memory_order_acquire)) < target)
@@ -349,8 +357,8 @@ __global__ void __launch_bounds__(512, 2) k_dt(BlendArgs a, const int* __restric
                 if (lane == 31)
                 {
                     *reinterpret_cast<float4*>(ringOut + xb) = make_float4(dv[0], dv[1], dv[2], dv[3]);
-                    cuda::atomic_ref<int, cuda::thread_scope_block> pr(prog[slot]);
-                    pr.store(g * (W + 1) + xb + kLag, cuda::memory_order_release);
+                    cuda::atomic_ref<int, cuda::thread_scope_block> pr(prog[g]);
+                    pr.store(xb + kLag, cuda::memory_order_release);
                 }
                 continue;
             }
@@ -402,6 +410,10 @@ __global__ void __launch_bounds__(512, 2) k_dt(BlendArgs a, const int* __restric
                 // Publish to the lane below my output of kLag-1 steps ago: its up[x+1].
                 float recv = __shfl_up_sync(kFull, h2, 1);
                 if (lane == 0) recv = (g > 0 && x + 1 >= 0 && x + 1 < W) ? ringIn[x + 1] : INF;
+                // Lanes 1..31 receive up[0] at their step x = -1; lane 0 starts
+                // at x = 0 and takes it from the ring (final: the first wait
+                // covered columns 0..kLag).
+                if (lane == 0 && x == 0 && g > 0) up0 = ringIn[0];
                 const float upp1 = recv;
                 float av = iv[q];
                 if (vy > 0)
@@ -447,8 +459,8 @@ __global__ void __launch_bounds__(512, 2) k_dt(BlendArgs a, const int* __restric
             if (lane == 31 && xb + kLag - 1 >= 0)
             {
                 __syncwarp(0x80000000u);
-                cuda::atomic_ref<int, cuda::thread_scope_block> pr(prog[slot]);
-                pr.store(g * (W + 1) + min(xb + kLag, W), cuda::memory_order_release);
+                cuda::atomic_ref<int, cuda::thread_scope_block> pr(prog[g]);
+                pr.store(min(xb + kLag, W), cuda::memory_order_release);
             }
         }
     }
@@ -1296,11 +1308,16 @@ __global__ void __launch_bounds__(256) k_final0(BlendArgs a, const Unit* __restr
 }
 }  // namespace
 
-int dt_rows_in_flight(int maxW)
+// Shared-memory bytes of the per-row-group progress counters.
+size_t dt_prog_bytes(int maxH) { return (size_t)(((maxH + 31) >> 5) + 1) * sizeof(int); }
+
+int dt_rows_in_flight(int maxW, int maxH)
 {
-    size_t row = (size_t)dt_ring_stride(maxW) * sizeof(float);
-    int n = (int)((100 * 1024) / row);  // two CTAs per SM
-    if (n < 2) n = (int)((210 * 1024) / row);
+    const size_t row = (size_t)dt_ring_stride(maxW) * sizeof(float);
+    const size_t prog = dt_prog_bytes(maxH);
+    auto fit = [&](size_t budget) { return budget > prog ? (int)((budget - prog) / row) : 0; };
+    int n = fit(100 * 1024);  // two CTAs per SM
+    if (n < 2) n = fit(210 * 1024);
     return n > kDtRing ? kDtRing : n;
 }
 
@@ -1318,12 +1335,13 @@ int launch_warp_tiles(const BlendArgs& a, const Unit* units, int n, cudaStream_t
     return check_launch("tile warp kernel");
 }
 
-int launch_dt(const BlendArgs& a, const int* itemList, int n, bool backward, int maxW, cudaStream_t s)
+int launch_dt(const BlendArgs& a, const int* itemList, int n, bool backward, int maxW, int maxH, cudaStream_t s)
 {
     if (n <= 0) return I360B_SUCCESS;
-    int slots = dt_rows_in_flight(maxW);
-    if (slots < 2) return fail(I360B_NOT_SUPPORTED, "Chunk width %d exceeds the distance-transform row ring.", maxW);
-    size_t smem = (size_t)slots * dt_ring_stride(maxW) * sizeof(float) + 64 * sizeof(int);
+    int slots = dt_rows_in_flight(maxW, maxH);
+    if (slots < 2)
+        return fail(I360B_NOT_SUPPORTED, "Chunk %dx%d exceeds the distance-transform row ring.", maxW, maxH);
+    size_t smem = (size_t)slots * dt_ring_stride(maxW) * sizeof(float) + dt_prog_bytes(maxH);
     if (backward)
     {
         cudaFuncSetAttribute(k_dt<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);

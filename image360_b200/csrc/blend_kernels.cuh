@@ -77,12 +77,12 @@ struct BlendArgs
 // Kernel launchers (blend_kernels.cu).
 int launch_coverage(const BlendArgs& a, const Unit* units, int n, cudaStream_t s);
 int launch_warp_tiles(const BlendArgs& a, const Unit* units, int n, cudaStream_t s);
-int launch_dt(const BlendArgs& a, const int* itemList, int n, bool backward, int maxW, cudaStream_t s);
+int launch_dt(const BlendArgs& a, const int* itemList, int n, bool backward, int maxW, int maxH, cudaStream_t s);
 int launch_owner(const BlendArgs& a, const Unit* units, int n, cudaStream_t s);
 int launch_seam(const BlendArgs& a, const int* tileList, int n, cudaStream_t s);
 int launch_down(const BlendArgs& a, const Unit* units, int n, int level, cudaStream_t s);
 int launch_blend_level(const BlendArgs& a, const Unit* units, int n, int level, cudaStream_t s);
 int launch_collapse(const BlendArgs& a, const Unit* units, int n, int level, cudaStream_t s);
 int launch_final0(const BlendArgs& a, const Unit* units, int n, cudaStream_t s);
-int dt_rows_in_flight(int maxW);
+int dt_rows_in_flight(int maxW, int maxH);
 }  // namespace i360b

@@ -134,6 +134,7 @@ int Plan::build(const std::vector<TileSpec>& specs, int numBands, bool renderPat
     };
     std::vector<TOff> tileOff(nTiles);
     maxW = 1;
+    maxH = 1;
     for (int t = 0; t < nTiles; ++t)
     {
         const TileSpec& S = specs[t];
@@ -180,6 +181,7 @@ int Plan::build(const std::vector<TileSpec>& specs, int numBands, bool renderPat
         T.usx[kMaxBands - 1] = T.usy[kMaxBands - 1] = 0.0f;
         size_t pyrPx = (size_t)acc;
         maxW = std::max(maxW, S.w);
+        maxH = std::max(maxH, S.h);
         size_t px = (size_t)S.w * S.h;
         TOff& to = tileOff[t];
         to.owner = bytes; bytes += align256(px);
@@ -392,6 +394,17 @@ int Plan::kernels_per_execute() const
     return n;
 }
 
+int Plan::enqueue_warp(cudaStream_t s)
+{
+    BlendArgs a{dItems, dTiles, dError, dSeamCycles};
+    if (nItems > 0) k_init_bbox<<<(nItems + 127) / 128, 128, 0, s>>>(dItems, nItems);
+    I360B_TRY(check_launch("bbox init kernel"));
+    I360B_CUDA(cudaMemsetAsync(dError, 0, sizeof(int), s), "error flag reset");
+    const Range r = lists[0];
+    if (render) return launch_warp_tiles(a, dUnits + r.start, r.count, s);
+    return launch_coverage(a, dUnits + r.start, r.count, s);
+}
+
 int Plan::enqueue(cudaStream_t s, cudaEvent_t* ev)
 {
     BlendArgs a{dItems, dTiles, dError, dSeamCycles};
@@ -400,16 +413,12 @@ int Plan::enqueue(cudaStream_t s, cudaEvent_t* ev)
         if (ev) cudaEventRecord(ev[i], s);
     };
     mark(0);
-    if (nItems > 0) k_init_bbox<<<(nItems + 127) / 128, 128, 0, s>>>(dItems, nItems);
-    I360B_TRY(check_launch("bbox init kernel"));
-    I360B_CUDA(cudaMemsetAsync(dError, 0, sizeof(int), s), "error flag reset");
-    Range r = L(0);
-    if (render) I360B_TRY(launch_warp_tiles(a, dUnits + r.start, r.count, s));
-    else I360B_TRY(launch_coverage(a, dUnits + r.start, r.count, s));
+    I360B_TRY(enqueue_warp(s));
+    Range r;
     mark(1);
-    I360B_TRY(launch_dt(a, dInts, nItems, false, maxW, s));
+    I360B_TRY(launch_dt(a, dInts, nItems, false, maxW, maxH, s));
     mark(2);
-    I360B_TRY(launch_dt(a, dInts, nItems, true, maxW, s));
+    I360B_TRY(launch_dt(a, dInts, nItems, true, maxW, maxH, s));
     mark(3);
     r = L(1);
     I360B_TRY(launch_owner(a, dUnits + r.start, r.count, s));
@@ -562,11 +571,6 @@ int launch_blend_chunk_in(void* arena, size_t arenaBytes, const unsigned short* 
 // ---------------------------------------------------------------------------
 // C-ABI: render plans.
 // ---------------------------------------------------------------------------
-struct i360b_render_plan
-{
-    i360b::Plan plan;
-};
-
 using namespace i360b;
 
 extern "C" int i360b_render_plan_create(const i360b_frame* frames, int numFrames, const i360b_tile* tiles,
@@ -697,6 +701,7 @@ extern "C" void i360b_render_plan_destroy(i360b_render_plan* plan)
 {
     if (!plan) return;
     cudaDeviceSynchronize();
+    release_learned_scratch(&plan->plan);
     delete plan;
 }
 

@@ -37,10 +37,20 @@ struct Range
     int count;
 };
 
+// A 256x256 window of an output tile for the learned blend (partial at the
+// tile's right and bottom edges): which contributors reach it.
+struct SubTile
+{
+    int tile, ox, oy, w, h;
+    int kind;     // 0 no contributor, 1 one (copied), 2 two to four (network)
+    int overflow; // more than 4 reached it; the 4 with the largest overlap kept
+    int item[4];  // global item indices, -1 unused
+};
+
 struct Plan
 {
     bool render = false;
-    int nTiles = 0, nItems = 0, nSeam = 0, bandsReq = 0, maxW = 1;
+    int nTiles = 0, nItems = 0, nSeam = 0, bandsReq = 0, maxW = 1, maxH = 1;
     std::vector<ItemDev> items;
     std::vector<TileDev> tiles;
     std::vector<Range> lists;
@@ -54,6 +64,7 @@ struct Plan
     int* dError = nullptr;
     unsigned long long* dSeamCycles = nullptr;
     int* hostErr = nullptr;
+    std::vector<SubTile> subTiles;  // built on first learned render
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t graphExec = nullptr;
 
@@ -71,9 +82,24 @@ struct Plan
     // Enqueues the kernel sequence; with `ev` non-null records ev[i] before
     // stage i and ev[kStages] at the end (stage order of kStageNames).
     int enqueue(cudaStream_t s, cudaEvent_t* ev = nullptr);
+    // Only the first stage: bounding-box reset and the warp (render path) or
+    // coverage pass, leaving every contributor's tile-space image in the arena.
+    int enqueue_warp(cudaStream_t s);
     int kernels_per_execute() const;
     int execute(cudaStream_t s, bool useGraph);
     // Waits for the stream and reports a kernel that gave up (bounded waits).
     int check(cudaStream_t s);
 };
 }  // namespace i360b
+
+namespace i360b
+{
+// Frees the learned-render scratch kept for a plan (learned.cu).
+void release_learned_scratch(const Plan* p);
+}  // namespace i360b
+
+// The opaque handle of the C-ABI (include/image360_b200.h).
+struct i360b_render_plan
+{
+    i360b::Plan plan;
+};
