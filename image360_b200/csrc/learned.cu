@@ -22,11 +22,13 @@
 // (tap, cin) and a slice of the pixels, and writes an fp32 partial that a
 // small kernel reduces.
 #include "common.cuh"
+#include "render_plan.hpp"
 #include "tc_common.cuh"
 #include "../../include/image360_b200_blendnet.h"
 
 #include <cuda_bf16.h>
 
+#include <algorithm>
 #include <cmath>
 #include <cstring>
 #include <mutex>
@@ -980,6 +982,7 @@ struct BlendNet
     int step = 0;
     // Per-batch buffers (grown on demand).
     size_t capPix = 0;
+    bool capTraining = false;
     char* act = nullptr;
     bf16 *x0 = nullptr, *a1 = nullptr, *a2 = nullptr, *p2 = nullptr, *a3 = nullptr, *a4 = nullptr, *a5 = nullptr,
          *a6 = nullptr, *a7 = nullptr;
@@ -993,7 +996,22 @@ struct BlendNet
     i360b_blend_job* hJobs = nullptr;  // pinned staging
     int jobCap = 0;
     cudaEvent_t jobsUploaded = nullptr;
+    // Recorded at the end of every call on the caller's stream; the next call
+    // (possibly on another stream) waits for it, because all calls share the
+    // activation buffers and the job table.
+    cudaEvent_t lastUse = nullptr;
     std::mutex mu;
+
+    int begin(cudaStream_t s)
+    {
+        I360B_CUDA(cudaStreamWaitEvent(s, lastUse, 0), "blend network ordering");
+        return I360B_SUCCESS;
+    }
+    int end(cudaStream_t s, int rc)
+    {
+        cudaEventRecord(lastUse, s);
+        return rc;
+    }
 
     ~BlendNet()
     {
@@ -1010,6 +1028,7 @@ struct BlendNet
         cudaFree(dJobs);
         if (hJobs) cudaFreeHost(hJobs);
         if (jobsUploaded) cudaEventDestroy(jobsUploaded);
+        if (lastUse) cudaEventDestroy(lastUse);
     }
 
     int init(unsigned long long seed)
@@ -1054,6 +1073,8 @@ struct BlendNet
         I360B_CUDA(cudaMalloc(&dError, sizeof(int)), "blendnet error flag");
         I360B_CUDA(cudaMemset(dError, 0, sizeof(int)), "blendnet error flag");
         I360B_CUDA(cudaEventCreateWithFlags(&jobsUploaded, cudaEventDisableTiming), "blendnet event");
+        I360B_CUDA(cudaEventCreateWithFlags(&lastUse, cudaEventDisableTiming), "blendnet event");
+        I360B_CUDA(cudaEventRecord(lastUse, nullptr), "blendnet event");
         // He-normal weights, zero biases, zero last layer (the untrained head
         // is then the coverage-weighted mean of the layers).
         std::vector<float> h(nParams, 0.0f);
@@ -1091,19 +1112,23 @@ struct BlendNet
         return check_launch("weight pack kernel");
     }
 
-    int reserve(int n, int w, int h)
+    // Activation buffers for n windows of w x h; the backward buffers only
+    // when training.
+    int reserve(int n, int w, int h, bool training)
     {
         const size_t pix = (size_t)n * w * h;
-        if (pix <= capPix) return I360B_SUCCESS;
+        if (pix <= capPix && (!training || capTraining)) return I360B_SUCCESS;
         cudaDeviceSynchronize();
         cudaFree(act);
         act = nullptr;
         capPix = 0;
         const size_t half = pix / 4;
+        const size_t tr = training ? 1 : 0;
         // bf16 element counts of every buffer, then the fp32 logits.
-        const size_t counts[] = {pix * 16,  pix * 32, pix * 32, half * 32, half * 64, half * 64, half * 64,
-                                 pix * 32,  pix * 32, pix * 16, pix * 32,  pix * 32,  pix * 96,  half * 64,
-                                 half * 64, half * 32};
+        const size_t counts[] = {pix * 16,       pix * 32,       pix * 32,       half * 32,      half * 64,
+                                 half * 64,      half * 64,      pix * 32,       pix * 32,       tr * pix * 16,
+                                 tr * pix * 32,  tr * pix * 32,  tr * pix * 96,  tr * half * 64, tr * half * 64,
+                                 tr * half * 32};
         size_t total = 0;
         for (size_t c : counts) total += (c * sizeof(bf16) + 255) / 256 * 256;
         total += pix * 4 * sizeof(float);
@@ -1124,6 +1149,7 @@ struct BlendNet
         }
         logits = reinterpret_cast<float*>(act + o);
         capPix = pix;
+        capTraining = training;
         return I360B_SUCCESS;
     }
 
@@ -1153,7 +1179,7 @@ struct BlendNet
         return I360B_SUCCESS;
     }
 
-    ConvArgs conv(const bf16* x, int n, int w, int h, int l, void* out, int ep) const
+    ConvArgs conv(const bf16* x, int n, int w, int h, int l, void* out, const i360b_blend_job* jobs) const
     {
         ConvArgs a{};
         a.x = x;
@@ -1163,32 +1189,32 @@ struct BlendNet
         a.wt = fwdW[l];
         a.bias = bias[l];
         a.out = out;
-        a.jobs = dJobs;
+        a.jobs = jobs;
         a.error = dError;
-        (void)ep;
         return a;
     }
 
-    // Forward pass; the last layer writes logits (train) or the composite.
-    int forward(int n, int w, int h, bool composite, cudaStream_t s)
+    // Forward pass over the windows jobs[0..n); the last layer writes logits
+    // (training) or the blended output (composite).
+    int forward(const i360b_blend_job* jobs, int n, int w, int h, bool composite, cudaStream_t s)
     {
         const int hw = w / 2, hh = h / 2;
-        k_pack_input<<<elementwise_grid((long long)n * w * h), 256, 0, s>>>(dJobs, n, h, w, x0);
+        k_pack_input<<<elementwise_grid((long long)n * w * h), 256, 0, s>>>(jobs, n, h, w, x0);
         I360B_TRY(check_launch("input pack kernel"));
-        I360B_TRY(dispatch_conv(16, 32, LD_PLAIN, EP_RELU, conv(x0, n, w, h, 0, a1, EP_RELU), s));
-        I360B_TRY(dispatch_conv(32, 32, LD_PLAIN, EP_RELU, conv(a1, n, w, h, 1, a2, EP_RELU), s));
+        I360B_TRY(dispatch_conv(16, 32, LD_PLAIN, EP_RELU, conv(x0, n, w, h, 0, a1, jobs), s));
+        I360B_TRY(dispatch_conv(32, 32, LD_PLAIN, EP_RELU, conv(a1, n, w, h, 1, a2, jobs), s));
         k_pool2<<<elementwise_grid((long long)n * hw * hh * 4), 256, 0, s>>>(a2, n, h, w, 4, p2);
         I360B_TRY(check_launch("pool kernel"));
-        I360B_TRY(dispatch_conv(32, 64, LD_PLAIN, EP_RELU, conv(p2, n, hw, hh, 2, a3, EP_RELU), s));
-        I360B_TRY(dispatch_conv(64, 64, LD_PLAIN, EP_RELU, conv(a3, n, hw, hh, 3, a4, EP_RELU), s));
-        I360B_TRY(dispatch_conv(64, 64, LD_PLAIN, EP_RELU, conv(a4, n, hw, hh, 4, a5, EP_RELU), s));
-        ConvArgs c6 = conv(a2, n, w, h, 5, a6, EP_RELU);
+        I360B_TRY(dispatch_conv(32, 64, LD_PLAIN, EP_RELU, conv(p2, n, hw, hh, 2, a3, jobs), s));
+        I360B_TRY(dispatch_conv(64, 64, LD_PLAIN, EP_RELU, conv(a3, n, hw, hh, 3, a4, jobs), s));
+        I360B_TRY(dispatch_conv(64, 64, LD_PLAIN, EP_RELU, conv(a4, n, hw, hh, 4, a5, jobs), s));
+        ConvArgs c6 = conv(a2, n, w, h, 5, a6, jobs);
         c6.u = a5;
         c6.cs = 32;
         I360B_TRY(dispatch_conv(96, 32, LD_CONCAT, EP_RELU, c6, s));
-        I360B_TRY(dispatch_conv(32, 32, LD_PLAIN, EP_RELU, conv(a6, n, w, h, 6, a7, EP_RELU), s));
-        if (composite) return dispatch_conv(32, 16, LD_PLAIN, EP_COMPOSITE, conv(a7, n, w, h, 7, nullptr, 0), s);
-        return dispatch_conv(32, 16, LD_PLAIN, EP_LOGITS, conv(a7, n, w, h, 7, logits, 0), s);
+        I360B_TRY(dispatch_conv(32, 32, LD_PLAIN, EP_RELU, conv(a6, n, w, h, 6, a7, jobs), s));
+        if (composite) return dispatch_conv(32, 16, LD_PLAIN, EP_COMPOSITE, conv(a7, n, w, h, 7, nullptr, jobs), s);
+        return dispatch_conv(32, 16, LD_PLAIN, EP_LOGITS, conv(a7, n, w, h, 7, logits, jobs), s);
     }
 
     // Backward data through layer l (flipped, transposed weights).
@@ -1373,12 +1399,17 @@ extern "C" int i360b_blendnet_logits(i360b_blendnet* net, const i360b_blend_job*
     BlendNet& N = net->net;
     std::lock_guard<std::mutex> lk(N.mu);
     cudaStream_t s = thread_stream();
-    I360B_TRY(N.reserve(n, w, h));
-    I360B_TRY(N.upload_jobs(jobs, n, s));
-    I360B_TRY(N.forward(n, w, h, false, s));
-    I360B_CUDA(cudaMemcpyAsync(dLogits, N.logits, (size_t)n * w * h * 4 * sizeof(float), cudaMemcpyDeviceToDevice, s),
-               "logits copy");
-    return N.check_error(s);
+    I360B_TRY(N.begin(s));
+    int rc = [&]() -> int {
+        I360B_TRY(N.reserve(n, w, h, false));
+        I360B_TRY(N.upload_jobs(jobs, n, s));
+        I360B_TRY(N.forward(N.dJobs, n, w, h, false, s));
+        I360B_CUDA(cudaMemcpyAsync(dLogits, N.logits, (size_t)n * w * h * 4 * sizeof(float), cudaMemcpyDeviceToDevice,
+                                   s),
+                   "logits copy");
+        return N.check_error(s);
+    }();
+    return N.end(s, rc);
 }
 
 extern "C" int i360b_blendnet_gradients(i360b_blendnet* net, const i360b_blend_job* jobs, int n, int w, int h,
@@ -1389,16 +1420,21 @@ extern "C" int i360b_blendnet_gradients(i360b_blendnet* net, const i360b_blend_j
     BlendNet& N = net->net;
     std::lock_guard<std::mutex> lk(N.mu);
     cudaStream_t s = thread_stream();
-    I360B_TRY(N.reserve(n, w, h));
-    I360B_TRY(N.upload_jobs(jobs, n, s));
-    I360B_TRY(N.forward(n, w, h, false, s));
-    I360B_TRY(N.backward(n, w, h, s));
-    I360B_TRY(N.check_error(s));
-    if (hostGrad)
-        I360B_CUDA(cudaMemcpy(hostGrad, N.grads, (size_t)N.nParams * sizeof(float), cudaMemcpyDeviceToHost),
-                   "grad download");
-    if (hostLoss) I360B_CUDA(cudaMemcpy(hostLoss, N.dLoss, sizeof(double), cudaMemcpyDeviceToHost), "loss download");
-    return I360B_SUCCESS;
+    I360B_TRY(N.begin(s));
+    int rc = [&]() -> int {
+        I360B_TRY(N.reserve(n, w, h, true));
+        I360B_TRY(N.upload_jobs(jobs, n, s));
+        I360B_TRY(N.forward(N.dJobs, n, w, h, false, s));
+        I360B_TRY(N.backward(n, w, h, s));
+        I360B_TRY(N.check_error(s));
+        if (hostGrad)
+            I360B_CUDA(cudaMemcpy(hostGrad, N.grads, (size_t)N.nParams * sizeof(float), cudaMemcpyDeviceToHost),
+                       "grad download");
+        if (hostLoss)
+            I360B_CUDA(cudaMemcpy(hostLoss, N.dLoss, sizeof(double), cudaMemcpyDeviceToHost), "loss download");
+        return I360B_SUCCESS;
+    }();
+    return N.end(s, rc);
 }
 
 extern "C" int i360b_blendnet_train_step(i360b_blendnet* net, const i360b_blend_job* jobs, int n, int w, int h,
@@ -1409,17 +1445,21 @@ extern "C" int i360b_blendnet_train_step(i360b_blendnet* net, const i360b_blend_
     BlendNet& N = net->net;
     std::lock_guard<std::mutex> lk(N.mu);
     cudaStream_t s = static_cast<cudaStream_t>(stream);
-    I360B_TRY(N.reserve(n, w, h));
-    I360B_TRY(N.upload_jobs(jobs, n, s));
-    I360B_TRY(N.forward(n, w, h, false, s));
-    I360B_TRY(N.backward(n, w, h, s));
-    I360B_TRY(N.adam(lr, s));
-    if (hostLoss)
-    {
-        I360B_CUDA(cudaMemcpyAsync(hostLoss, N.dLoss, sizeof(double), cudaMemcpyDeviceToHost, s), "loss download");
-        return N.check_error(s);
-    }
-    return I360B_SUCCESS;
+    I360B_TRY(N.begin(s));
+    int rc = [&]() -> int {
+        I360B_TRY(N.reserve(n, w, h, true));
+        I360B_TRY(N.upload_jobs(jobs, n, s));
+        I360B_TRY(N.forward(N.dJobs, n, w, h, false, s));
+        I360B_TRY(N.backward(n, w, h, s));
+        I360B_TRY(N.adam(lr, s));
+        if (hostLoss)
+        {
+            I360B_CUDA(cudaMemcpyAsync(hostLoss, N.dLoss, sizeof(double), cudaMemcpyDeviceToHost, s), "loss download");
+            return N.check_error(s);
+        }
+        return I360B_SUCCESS;
+    }();
+    return N.end(s, rc);
 }
 
 extern "C" int i360b_blendnet_infer(i360b_blendnet* net, const i360b_blend_job* jobs, int n, int w, int h,
@@ -1430,9 +1470,13 @@ extern "C" int i360b_blendnet_infer(i360b_blendnet* net, const i360b_blend_job* 
     BlendNet& N = net->net;
     std::lock_guard<std::mutex> lk(N.mu);
     cudaStream_t s = static_cast<cudaStream_t>(stream);
-    I360B_TRY(N.reserve(n, w, h));
-    I360B_TRY(N.upload_jobs(jobs, n, s));
-    return N.forward(n, w, h, true, s);
+    I360B_TRY(N.begin(s));
+    int rc = [&]() -> int {
+        I360B_TRY(N.reserve(n, w, h, false));
+        I360B_TRY(N.upload_jobs(jobs, n, s));
+        return N.forward(N.dJobs, n, w, h, true, s);
+    }();
+    return N.end(s, rc);
 }
 
 extern "C" int i360b_conv3x3_forward(const void* dX, const void* dU, int skipChannels, int n, int h, int w, int cin,
@@ -1506,5 +1550,424 @@ extern "C" int i360b_conv3x3_wgrad(const void* dX, const void* dU, int skipChann
     dev_free(scratch, s);
     if (rc != I360B_SUCCESS) return rc;
     if (e) return fail(I360B_KERNEL_LAUNCH_FAILED, "conv3x3 wgrad gave up waiting for its MMAs");
+    return I360B_SUCCESS;
+}
+
+// ---------------------------------------------------------------------------
+// Learned render of a plan's output tiles
+// ---------------------------------------------------------------------------
+namespace i360b
+{
+namespace
+{
+constexpr int kSub = 256;  // learned-blend window side
+
+// Copy (src non-null) or clear a w x h RGB48 rectangle; strides in elements.
+struct Region
+{
+    const unsigned short* src;
+    unsigned short* dst;
+    int w, h;
+    long long srcRow, dstRow;
+};
+
+__global__ void k_regions(const Region* __restrict__ regs, int n)
+{
+    for (int r = blockIdx.y; r < n; r += gridDim.y)
+    {
+        const Region R = regs[r];
+        const int vals = R.w * 3;
+        for (int y = blockIdx.x; y < R.h; y += gridDim.x)
+        {
+            unsigned short* d = R.dst + y * R.dstRow;
+            if (R.src)
+            {
+                const unsigned short* src = R.src + y * R.srcRow;
+                for (int i = threadIdx.x; i < vals; i += blockDim.x) d[i] = src[i];
+            }
+            else
+                for (int i = threadIdx.x; i < vals; i += blockDim.x) d[i] = 0;
+        }
+    }
+}
+
+// Per region: sum of squared differences and largest absolute difference
+// between two RGB48 rectangles (src = learned, dst = plain).
+__global__ void k_judge(const Region* __restrict__ regs, int n, double* __restrict__ sse, int* __restrict__ maxErr)
+{
+    __shared__ double rs[8];
+    __shared__ int rm[8];
+    for (int r = blockIdx.x; r < n; r += gridDim.x)
+    {
+        const Region R = regs[r];
+        const int vals = R.w * 3;
+        double acc = 0.0;
+        int mx = 0;
+        for (int y = 0; y < R.h; ++y)
+        {
+            const unsigned short* a = R.src + y * R.srcRow;
+            const unsigned short* b = R.dst + y * R.dstRow;
+            for (int i = threadIdx.x; i < vals; i += blockDim.x)
+            {
+                const int d = (int)a[i] - (int)b[i];
+                acc += (double)d * d;
+                mx = max(mx, abs(d));
+            }
+        }
+        for (int o = 16; o > 0; o >>= 1)
+        {
+            acc += __shfl_xor_sync(0xffffffffu, acc, o);
+            mx = max(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+        }
+        if ((threadIdx.x & 31) == 0)
+        {
+            rs[threadIdx.x >> 5] = acc;
+            rm[threadIdx.x >> 5] = mx;
+        }
+        __syncthreads();
+        if (threadIdx.x == 0)
+        {
+            double t = 0.0;
+            int m = 0;
+            for (int w = 0; w < (int)(blockDim.x >> 5); ++w)
+            {
+                t += rs[w];
+                m = max(m, rm[w]);
+            }
+            sse[r] = t;
+            maxErr[r] = m;
+        }
+        __syncthreads();
+    }
+}
+
+int launch_regions(const std::vector<Region>& regs, Region* dRegs, cudaStream_t s)
+{
+    if (regs.empty()) return I360B_SUCCESS;
+    I360B_CUDA(cudaMemcpyAsync(dRegs, regs.data(), regs.size() * sizeof(Region), cudaMemcpyHostToDevice, s),
+               "region upload");
+    k_regions<<<dim3(16, (unsigned)std::min<size_t>(regs.size(), 65535)), 256, 0, s>>>(dRegs, (int)regs.size());
+    return check_launch("region copy kernel");
+}
+
+// Footprint box of an item intersects a rectangle (inclusive box ends).
+bool box_hits(const ItemDev& it, int x0, int y0, int w, int h)
+{
+    return it.vx0 < x0 + w && it.vx1 >= x0 && it.vy0 < y0 + h && it.vy1 >= y0;
+}
+
+long long box_overlap(const ItemDev& it, int x0, int y0, int w, int h)
+{
+    const long long ix = std::max(0, std::min(it.vx1 + 1, x0 + w) - std::max(it.vx0, x0));
+    const long long iy = std::max(0, std::min(it.vy1 + 1, y0 + h) - std::max(it.vy0, y0));
+    return ix * iy;
+}
+
+void build_subtiles(Plan& P)
+{
+    if (!P.subTiles.empty()) return;
+    for (int t = 0; t < P.nTiles; ++t)
+    {
+        const TileDev& T = P.tiles[t];
+        for (int oy = 0; oy < T.h; oy += kSub)
+            for (int ox = 0; ox < T.w; ox += kSub)
+            {
+                SubTile st{};
+                st.tile = t;
+                st.ox = ox;
+                st.oy = oy;
+                st.w = std::min(kSub, T.w - ox);
+                st.h = std::min(kSub, T.h - oy);
+                std::vector<std::pair<long long, int>> hits;
+                for (int k = 0; k < T.numItems; ++k)
+                {
+                    const ItemDev& it = P.items[T.firstItem + k];
+                    if (box_hits(it, ox, oy, st.w, st.h)) hits.push_back({box_overlap(it, ox, oy, st.w, st.h), k});
+                }
+                if (hits.size() > 4)
+                {
+                    st.overflow = 1;
+                    std::stable_sort(hits.begin(), hits.end(),
+                                     [](const auto& a, const auto& b) { return a.first > b.first; });
+                    hits.resize(4);
+                    std::sort(hits.begin(), hits.end(), [](const auto& a, const auto& b) { return a.second < b.second; });
+                }
+                for (int i = 0; i < 4; ++i) st.item[i] = i < (int)hits.size() ? T.firstItem + hits[i].second : -1;
+                st.kind = hits.empty() ? 0 : hits.size() == 1 ? 1 : 2;
+                P.subTiles.push_back(st);
+            }
+    }
+}
+
+// Device scratch of the learned render, per (plan, thread of use).
+struct LearnedScratch
+{
+    i360b_blend_job* dJobs = nullptr;
+    size_t jobCap = 0;
+    Region* dRegs = nullptr;
+    size_t regCap = 0;
+    double* dSse = nullptr;
+    int* dMax = nullptr;
+    size_t judgeCap = 0;
+    ~LearnedScratch()
+    {
+        cudaFree(dJobs);
+        cudaFree(dRegs);
+        cudaFree(dSse);
+        cudaFree(dMax);
+    }
+    int jobs(size_t n)
+    {
+        if (n <= jobCap) return I360B_SUCCESS;
+        cudaFree(dJobs);
+        dJobs = nullptr;
+        jobCap = 0;
+        I360B_CUDA(cudaMalloc(&dJobs, std::max<size_t>(n, 1) * sizeof(i360b_blend_job)), "learned jobs");
+        jobCap = n;
+        return I360B_SUCCESS;
+    }
+    int regs(size_t n)
+    {
+        if (n <= regCap) return I360B_SUCCESS;
+        cudaFree(dRegs);
+        dRegs = nullptr;
+        regCap = 0;
+        I360B_CUDA(cudaMalloc(&dRegs, std::max<size_t>(n, 1) * sizeof(Region)), "learned regions");
+        regCap = n;
+        return I360B_SUCCESS;
+    }
+    int judge(size_t n)
+    {
+        if (n <= judgeCap) return I360B_SUCCESS;
+        cudaFree(dSse);
+        cudaFree(dMax);
+        dSse = nullptr;
+        dMax = nullptr;
+        judgeCap = 0;
+        I360B_CUDA(cudaMalloc(&dSse, std::max<size_t>(n, 1) * sizeof(double)), "judge");
+        I360B_CUDA(cudaMalloc(&dMax, std::max<size_t>(n, 1) * sizeof(int)), "judge");
+        judgeCap = n;
+        return I360B_SUCCESS;
+    }
+};
+
+std::mutex g_scratchMu;
+std::vector<std::pair<const Plan*, LearnedScratch*>> g_scratch;
+
+LearnedScratch& scratch_for(const Plan* p)
+{
+    std::lock_guard<std::mutex> lk(g_scratchMu);
+    for (auto& e : g_scratch)
+        if (e.first == p) return *e.second;
+    g_scratch.push_back({p, new LearnedScratch});
+    return *g_scratch.back().second;
+}
+}  // namespace
+
+void release_learned_scratch(const Plan* p)
+{
+    std::lock_guard<std::mutex> lk(g_scratchMu);
+    for (size_t i = 0; i < g_scratch.size(); ++i)
+        if (g_scratch[i].first == p)
+        {
+            delete g_scratch[i].second;
+            g_scratch.erase(g_scratch.begin() + i);
+            return;
+        }
+}
+
+int learned_render(Plan& P, BlendNet& N, unsigned short* const* tileOut, int maxBatch, cudaStream_t s, float* stageMs)
+{
+    if (!P.render) return fail(I360B_INVALID_PARAM, "learned render needs a render plan");
+    build_subtiles(P);
+    LearnedScratch& S = scratch_for(&P);
+    auto outOf = [&](int t) { return tileOut ? tileOut[t] : P.tiles[t].out; };
+    std::vector<i360b_blend_job> jobs;
+    std::vector<Region> regs;
+    for (const SubTile& st : P.subTiles)
+    {
+        const TileDev& T = P.tiles[st.tile];
+        unsigned short* out = outOf(st.tile);
+        if (!out) return fail(I360B_INVALID_PARAM, "Tile %d has a null learned output.", st.tile);
+        const size_t off = ((size_t)st.oy * T.w + st.ox) * 3;
+        if (st.kind == 2)
+        {
+            i360b_blend_job j{};
+            for (int i = 0; i < 4; ++i) j.slot[i] = st.item[i] >= 0 ? P.items[st.item[i]].img + off : nullptr;
+            j.pixStride = 3;
+            j.rowStride = 3LL * T.w;
+            j.width = st.w;
+            j.height = st.h;
+            j.out = out + off;
+            j.outRowStride = 3LL * T.w;
+            jobs.push_back(j);
+        }
+        else
+        {
+            regs.push_back(Region{st.kind == 1 ? P.items[st.item[0]].img + off : nullptr, out + off, st.w, st.h,
+                                  3LL * T.w, 3LL * T.w});
+        }
+    }
+    I360B_TRY(S.jobs(jobs.size()));
+    I360B_TRY(S.regs(regs.size()));
+    cudaEvent_t ev[4] = {};
+    if (stageMs)
+        for (auto& e : ev) I360B_CUDA(cudaEventCreate(&e), "stage events");
+    auto mark = [&](int i) {
+        if (stageMs) cudaEventRecord(ev[i], s);
+    };
+    mark(0);
+    I360B_TRY(P.enqueue_warp(s));
+    mark(1);
+    I360B_TRY(launch_regions(regs, S.dRegs, s));
+    mark(2);
+    if (!jobs.empty())
+    {
+        I360B_CUDA(cudaMemcpyAsync(S.dJobs, jobs.data(), jobs.size() * sizeof(i360b_blend_job), cudaMemcpyHostToDevice,
+                                   s),
+                   "learned jobs upload");
+        const int batch = std::max(1, std::min<int>(maxBatch, (int)jobs.size()));
+        I360B_TRY(N.reserve(batch, kSub, kSub, false));
+        for (size_t b = 0; b < jobs.size(); b += batch)
+        {
+            const int n = (int)std::min<size_t>(batch, jobs.size() - b);
+            I360B_TRY(N.forward(S.dJobs + b, n, kSub, kSub, true, s));
+        }
+    }
+    mark(3);
+    if (stageMs)
+    {
+        I360B_CUDA(cudaEventSynchronize(ev[3]), "stage events");
+        for (int i = 0; i < 3; ++i) cudaEventElapsedTime(&stageMs[i], ev[i], ev[i + 1]);
+        for (auto& e : ev) cudaEventDestroy(e);
+    }
+    // Host vectors must outlive the asynchronous uploads.
+    I360B_CUDA(cudaStreamSynchronize(s), "learned render");
+    return I360B_SUCCESS;
+}
+
+int learned_judge(Plan& P, unsigned short* const* tileOut, double minPsnr, double peak, i360b_learned_stats* st,
+                  float* psnrOut, int maxOut, cudaStream_t s)
+{
+    build_subtiles(P);
+    LearnedScratch& S = scratch_for(&P);
+    const size_t n = P.subTiles.size();
+    std::vector<Region> regs(n);
+    for (size_t i = 0; i < n; ++i)
+    {
+        const SubTile& t = P.subTiles[i];
+        const TileDev& T = P.tiles[t.tile];
+        const size_t off = ((size_t)t.oy * T.w + t.ox) * 3;
+        if (!tileOut[t.tile]) return fail(I360B_INVALID_PARAM, "Tile %d has a null learned output.", t.tile);
+        regs[i] = Region{tileOut[t.tile] + off, P.tiles[t.tile].out + off, t.w, t.h, 3LL * T.w, 3LL * T.w};
+    }
+    I360B_TRY(S.regs(n));
+    I360B_TRY(S.judge(n));
+    if (n)
+    {
+        I360B_CUDA(cudaMemcpyAsync(S.dRegs, regs.data(), n * sizeof(Region), cudaMemcpyHostToDevice, s), "judge");
+        k_judge<<<(unsigned)std::min<size_t>(n, 65535), 256, 0, s>>>(S.dRegs, (int)n, S.dSse, S.dMax);
+        I360B_TRY(check_launch("judge kernel"));
+    }
+    std::vector<double> sse(n);
+    std::vector<int> mx(n);
+    if (n)
+    {
+        I360B_CUDA(cudaMemcpyAsync(sse.data(), S.dSse, n * sizeof(double), cudaMemcpyDeviceToHost, s), "judge");
+        I360B_CUDA(cudaMemcpyAsync(mx.data(), S.dMax, n * sizeof(int), cudaMemcpyDeviceToHost, s), "judge");
+    }
+    I360B_CUDA(cudaStreamSynchronize(s), "judge");
+    i360b_learned_stats r{};
+    r.subTiles = (int)n;
+    r.minPsnr = INFINITY;
+    double psum = 0.0;
+    int pcount = 0;
+    std::vector<Region> fallback;
+    for (size_t i = 0; i < n; ++i)
+    {
+        const SubTile& t = P.subTiles[i];
+        r.netSubTiles += t.kind == 2;
+        r.copySubTiles += t.kind == 1;
+        r.emptySubTiles += t.kind == 0;
+        r.overflowSubTiles += t.overflow;
+        const double cnt = 3.0 * t.w * t.h;
+        const double mse = sse[i] / cnt;
+        const double psnr = mse > 0.0 ? 10.0 * std::log10(peak * peak / mse) : INFINITY;
+        if (psnrOut && (int)i < maxOut) psnrOut[i] = (float)psnr;
+        r.maxAbsError = std::max(r.maxAbsError, mx[i]);
+        r.minPsnr = std::min(r.minPsnr, psnr);
+        if (std::isfinite(psnr))
+        {
+            psum += psnr;
+            ++pcount;
+        }
+        if (psnr < minPsnr)
+        {
+            ++r.fallbackSubTiles;
+            // plain -> learned output
+            fallback.push_back(
+                Region{regs[i].dst, const_cast<unsigned short*>(regs[i].src), t.w, t.h, regs[i].dstRow, regs[i].srcRow});
+        }
+    }
+    r.judgedSubTiles = (int)n;
+    r.meanPsnr = pcount ? psum / pcount : INFINITY;
+    I360B_TRY(S.regs(std::max(n, fallback.size())));
+    I360B_TRY(launch_regions(fallback, S.dRegs, s));
+    I360B_CUDA(cudaStreamSynchronize(s), "judge fallback");
+    if (st) *st = r;
+    return I360B_SUCCESS;
+}
+}  // namespace i360b
+
+extern "C" int i360b_render_plan_learned(i360b_render_plan* plan, i360b_blendnet* net,
+                                         unsigned short* const* dTileOut, int maxBatch, void* stream, float* stageMs)
+{
+    I360B_TRY(net_prologue(net));
+    if (!plan) return fail(I360B_INVALID_PARAM, "Null plan.");
+    if (maxBatch < 1) return fail(I360B_INVALID_PARAM, "maxBatch must be >= 1.");
+    BlendNet& N = net->net;
+    std::lock_guard<std::mutex> lk(N.mu);
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    I360B_TRY(N.begin(s));
+    int rc = learned_render(plan->plan, N, dTileOut, maxBatch, s, stageMs);
+    if (rc == I360B_SUCCESS) rc = N.check_error(s);
+    return N.end(s, rc);
+}
+
+extern "C" int i360b_render_plan_judge(i360b_render_plan* plan, unsigned short* const* dTileOut, double minPsnrDb,
+                                       double peak, i360b_learned_stats* stats, float* hostSubTilePsnr,
+                                       int maxSubTiles, void* stream)
+{
+    clear_error();
+    if (!initialized()) return fail(I360B_CUDA_ERROR, "Not initialized.");
+    I360B_TRY(ensure_ready());
+    if (!plan || !dTileOut) return fail(I360B_INVALID_PARAM, "Null pointer argument.");
+    if (!(peak > 0.0)) return fail(I360B_INVALID_PARAM, "peak must be > 0.");
+    return learned_judge(plan->plan, dTileOut, minPsnrDb, peak, stats, hostSubTilePsnr, maxSubTiles,
+                         static_cast<cudaStream_t>(stream));
+}
+
+extern "C" int i360b_render_plan_tile_items(i360b_render_plan* plan, int tile, int maxItems,
+                                            const unsigned short** dImages, int* boxes, int* numItems)
+{
+    clear_error();
+    if (!plan || !numItems) return fail(I360B_INVALID_PARAM, "Null pointer argument.");
+    const Plan& P = plan->plan;
+    if (tile < 0 || tile >= P.nTiles) return fail(I360B_INVALID_PARAM, "Tile %d out of range.", tile);
+    if (!P.render) return fail(I360B_INVALID_PARAM, "not a render plan");
+    const TileDev& T = P.tiles[tile];
+    *numItems = T.numItems;
+    for (int k = 0; k < T.numItems && k < maxItems; ++k)
+    {
+        const ItemDev& it = P.items[T.firstItem + k];
+        if (dImages) dImages[k] = it.img;
+        if (boxes)
+        {
+            boxes[4 * k] = it.vx0;
+            boxes[4 * k + 1] = it.vy0;
+            boxes[4 * k + 2] = it.vx1;
+            boxes[4 * k + 3] = it.vy1;
+        }
+    }
     return I360B_SUCCESS;
 }

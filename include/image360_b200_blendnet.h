@@ -83,6 +83,50 @@ I360B_API int i360b_blendnet_train_step(i360b_blendnet* net, const i360b_blend_j
 I360B_API int i360b_blendnet_infer(i360b_blendnet* net, const i360b_blend_job* jobs, int n, int w, int h,
                                    void* stream);
 
+/* ---- learned render of a panorama --------------------------------------- */
+
+/* Every output tile of a render plan is cut into 256x256 windows (partial at
+ * the tile's right and bottom edges).  A window that no contributor's
+ * footprint reaches is cleared, one that a single contributor reaches gets
+ * that contributor's warped pixels, and one that 2 to 4 reach is blended by
+ * the network (with more than 4, the 4 with the largest footprint overlap). */
+typedef struct i360b_learned_stats
+{
+    int subTiles;         /* windows of all output tiles */
+    int netSubTiles;      /* blended by the network */
+    int copySubTiles;     /* one contributor: copied */
+    int emptySubTiles;    /* no contributor: zero */
+    int overflowSubTiles; /* more than 4 contributors reached the window */
+    int judgedSubTiles;   /* compared with the plain seam blend */
+    int fallbackSubTiles; /* below the PSNR threshold: replaced by the plain blend */
+    int maxAbsError;      /* largest |learned - plain| before fallback */
+    double minPsnr;       /* lowest window PSNR before fallback (inf: identical) */
+    double meanPsnr;      /* mean over windows with a finite PSNR */
+} i360b_learned_stats;
+
+/* Warps every contributor (the plan's first stage) and renders each tile with
+ * the learned blend into dTileOut[t] (width*height*3 RGB48 per tile; NULL =
+ * the plan's own outputs), at most maxBatch network windows per pass.
+ * stageMs, when non-null, receives 3 times in ms (warp, copies, network).
+ * Returns once the render has completed on `stream`. */
+I360B_API int i360b_render_plan_learned(i360b_render_plan* plan, i360b_blendnet* net,
+                                        unsigned short* const* dTileOut, int maxBatch, void* stream, float* stageMs);
+/* The per-window judge and fallback: compares every window of dTileOut with
+ * the plan's own outputs, which must hold the plain seam blend of a completed
+ * i360b_render_plan_execute; PSNR = 10 log10(peak^2 / MSE) over the window's
+ * RGB values.  Windows below minPsnrDb are overwritten with the plain blend.
+ * hostSubTilePsnr (optional) receives up to maxSubTiles PSNRs in window order
+ * (tile by tile, rows of windows).  Synchronous. */
+I360B_API int i360b_render_plan_judge(i360b_render_plan* plan, unsigned short* const* dTileOut, double minPsnrDb,
+                                      double peak, i360b_learned_stats* stats, float* hostSubTilePsnr,
+                                      int maxSubTiles, void* stream);
+/* The warped contributor images of tile `tile` after an execute (device RGB48,
+ * tile-sized) and their footprint boxes {x0, y0, x1, y1} in tile pixels
+ * (outside the box the image is zero).  numItems receives the count; up to
+ * maxItems entries are written. */
+I360B_API int i360b_render_plan_tile_items(i360b_render_plan* plan, int tile, int maxItems,
+                                           const unsigned short** dImages, int* boxes, int* numItems);
+
 /* ---- convolution primitives (NHWC bf16, width a multiple of 128) --------- */
 
 /* Epilogues of i360b_conv3x3_forward. */

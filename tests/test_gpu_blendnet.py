@@ -179,7 +179,7 @@ def test_inference_matches_oracle_head(backend):
     params = _random_params(9)
     net = bn.BlendNet(seed=2)
     net.set_params(params)
-    _, _, out, jobs = _device_batch(layers)
+    dl, _, out, jobs = _device_batch(layers)  # dl backs the jobs: keep it alive
     net.infer(jobs, n, w, h)
     logits = torch.zeros((n, h, w, 4), dtype=torch.float32, device="cuda")
     net.logits(jobs, n, w, h, logits)
@@ -205,7 +205,7 @@ def test_untrained_network_blends_the_coverage_mean(backend):
     n, h, w = 2, 8, 256
     layers = _layers(31, n, h, w)
     net = bn.BlendNet(seed=3)
-    _, _, out, jobs = _device_batch(layers)
+    dl, _, out, jobs = _device_batch(layers)  # dl backs the jobs: keep it alive
     net.infer(jobs, n, w, h)
     torch.cuda.synchronize()
     cov = (layers != 0).any(-1)
@@ -234,7 +234,7 @@ def test_invalid_windows_are_rejected(backend):
     from image360_b200 import blendnet as bn
     net = bn.BlendNet(seed=5)
     layers = _layers(1, 1, 8, 256)
-    _, _, _, jobs = _device_batch(layers)
+    dl, _, _, jobs = _device_batch(layers)  # dl backs the jobs: keep it alive
     with pytest.raises(RuntimeError, match="INVALID_PARAM"):
         net.infer(jobs, 1, 200, 8)
     with pytest.raises(RuntimeError, match="INVALID_PARAM"):
