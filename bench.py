@@ -199,6 +199,9 @@ def run_ours(args, rank, world, local_rank):
     device = f"cuda:{local_rank}"
     torch.cuda.set_device(local_rank)
     cfg = synth.C1 if args.scale == 1.0 else synth.scaled(synth.C1, args.scale, tile=synth.C1.tile)
+    net = untrained = train_info = None
+    if not args.no_learned:
+        net, untrained, train_info = prepare_network(args, cfg, rank)
     S = setup_ours(cfg, rank, device)
     stream = torch.cuda.Stream(device=device)
     sp = stream.cuda_stream
@@ -290,9 +293,169 @@ def run_ours(args, rank, world, local_rank):
         "clocks": clk.summary(),
         "e2e": e2e,
     }
+    if net is not None:
+        lr = run_learned(args, S, stream, net, untrained, train_info)
+        lr["speedup_vs_plain"] = round(lr["value"] / value * world, 3)
+        lr["speedup_vs_plain_with_fallback"] = round(lr["with_fallback"]["value"] / value * world, 3)
+        line["learned"] = lr
+        line["config"]["blend"] = ("plain seam blend (value); learned blend measured in 'learned' "
+                                   "(same frames, 256x256 overlap windows, judged per window at 45 dB)")
     if not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(S, args)
     return line
+
+
+def prepare_network(args, cfg, rank):
+    """Trains the blend network on the GPU (own kernels) on seeded panoramas
+    of the benchmark's configuration other than the benchmarked one, or loads
+    weights given with --weights; also makes the untrained network."""
+    import torch
+
+    from image360_b200 import blendnet as bn, learned
+    t0 = time.time()
+    if args.weights:
+        net = bn.BlendNet(seed=1)
+        net.set_params(np.fromfile(args.weights, np.float32))
+        info = {"weights": os.path.basename(args.weights)}
+    else:
+        base = synth_cfg_for_training(cfg, rank)
+        net = learned.train_on_scenes(base, args.train_scenes, args.train_steps, args.train_batch, 1e-3, seed=1 + rank,
+                                      log=log)
+        info = {"scenes": args.train_scenes, "steps": args.train_steps, "batch": args.train_batch, "lr": 1e-3,
+                "windows": args.train_steps * args.train_batch, "optimizer": "adam",
+                "target": "plain 6-level seam blend of the same window", "seconds": round(time.time() - t0, 1)}
+    torch.cuda.synchronize()
+    torch.cuda.empty_cache()
+    return net, bn.BlendNet(seed=2), info
+
+
+def synth_cfg_for_training(cfg, rank):
+    from image360_b200 import synth
+    return synth.PanoConfig(**{**cfg.__dict__, "seed": cfg.seed + 1000 * rank})
+
+
+def network_flops_per_px() -> float:
+    """Algorithmic FLOPs of the blend network per window pixel (2 * 9 * cin *
+    cout per layer, half-resolution layers at a quarter of the pixels)."""
+    from image360_b200 import blendnet as bn
+    area = [1, 1, 0.25, 0.25, 0.25, 1, 1, 1]
+    return sum(2.0 * 9 * ci * co * a for (ci, co), a in zip(bn.LAYERS, area))
+
+
+def run_learned(args, S, stream, net, untrained, train_info):
+    """The learned form of the same step (demosaic + warp + per-window network
+    or copy), its per-window judge against the plain blend just rendered, the
+    cost of the fallback, and the same judge for the untrained network (the
+    coverage-weighted mean, i.e. the method without learning)."""
+    import torch
+
+    from image360_b200 import RenderPlan, COORDS_REFERENCE, learned
+    sp = stream.cuda_stream
+    cfg, be, plan = S["cfg"], S["be"], S["plan"]
+    black, cm, rc, filt = S["demosaic"]
+    render = learned.PanoramaRender.__new__(learned.PanoramaRender)  # view over the bench's own scene
+    render.cfg, render.pano, render.be, render.plan = cfg, S["pano"], be, plan
+    render.cfa, render.rgb, render.outs, render.demosaic_args, render._items = S["cfa"], S["rgb"], S["outs"], \
+        S["demosaic"], None
+    louts = [torch.empty_like(o) for o in S["outs"]]
+
+    def step():
+        for c, r in zip(S["cfa"], S["rgb"]):
+            be.launch_demosaic(c.data_ptr(), cfg.frame_w, cfg.frame_h, black, cm, rc, filt, r.data_ptr(), sp)
+        render.learned(net, louts, args.learned_batch, stream=sp)
+
+    with torch.cuda.stream(stream):
+        for _ in range(args.warmup):
+            step()
+    torch.cuda.synchronize()
+    t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with torch.cuda.stream(stream):
+        t0.record(stream)
+        for _ in range(args.steps):
+            step()
+        t1.record(stream)
+    torch.cuda.synchronize()
+    ms_step = t0.elapsed_time(t1) / args.steps
+    stages = render.learned(net, louts, args.learned_batch, stream=sp)
+    # the plan's own outputs hold the plain blend of the same frames
+    with torch.cuda.stream(stream):
+        assert plan.execute(sp) == 0 and plan.wait(sp) == 0
+    torch.cuda.synchronize()
+    peak = learned.white_level(cfg)
+    st, ps = render.judge(louts, 45.0, peak, stream=sp)
+    fin = ps[np.isfinite(ps)]
+    win = render.windows()
+    kind = win[:, 3]
+    # fallback cost: the plain blend of every tile holding a failing window
+    fb_tiles = sorted({int(t) for t, ok in zip(win[:, 0], ps >= 45.0) if not ok})
+    fb_ms = 0.0
+    if fb_tiles:
+        sub_outs = [torch.empty_like(S["outs"][t]) for t in fb_tiles]
+        frames = [(r.data_ptr(), cfg.frame_w, cfg.frame_h, H, float(g))
+                  for r, H, g in zip(S["rgb"], S["pano"].to_canvas, (1.0 / S["pano"].gains).astype(np.float32))]
+        tiles = [(*S["pano"].tiles[t][:5], o.data_ptr()) for t, o in zip(fb_tiles, sub_outs)]
+        sub = RenderPlan(frames, tiles, cfg.bands, COORDS_REFERENCE)
+        with torch.cuda.stream(stream):
+            for _ in range(2):
+                sub.execute(sp)
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record(stream)
+            for _ in range(args.steps):
+                sub.execute(sp)
+            b.record(stream)
+        torch.cuda.synchronize()
+        assert sub.wait(sp) == 0
+        fb_ms = a.elapsed_time(b) / args.steps
+        sub.close()
+    # the method without learning: the untrained network's head
+    untr = None
+    if untrained is not None:
+        uouts = [torch.empty_like(o) for o in S["outs"]]
+        render.learned(untrained, uouts, args.learned_batch, stream=sp)
+        ust, ups = render.judge(uouts, 45.0, peak, stream=sp)
+        untr = {"fallback_windows": ust["fallbackSubTiles"], **_by_kind(ups, kind, "network_windows")}
+        del uouts
+    out_px = sum(t[2] * t[3] for t in S["pano"].tiles)
+    net_px = st["netSubTiles"] * learned.WINDOW * learned.WINDOW
+    flops = net_px * network_flops_per_px()
+    tfl = flops / (stages["network"] / 1e3) / 1e12
+    peaks, peak_kind = measured_peaks()
+    res = {
+        "value": round(out_px / 1e6 / (ms_step / 1e3), 2), "unit": UNIT, "ms_per_step": round(ms_step, 3),
+        "with_fallback": {"value": round(out_px / 1e6 / ((ms_step + fb_ms) / 1e3), 2),
+                          "ms_per_step": round(ms_step + fb_ms, 3), "fallback_ms": round(fb_ms, 3),
+                          "fallback_tiles": len(fb_tiles)},
+        "stages_ms": {k: round(v, 3) for k, v in stages.items()},
+        "network": {"windows": st["netSubTiles"], "window": learned.WINDOW, "gflop": round(flops / 1e9, 1),
+                    "tflops": round(tfl, 1), "bound": "tensor",
+                    "peak": peaks.get("bf16_tflops_sustained", peaks["bf16_tflops"]), "unit": "TFLOP/s",
+                    "frac": round(tfl / peaks.get("bf16_tflops_sustained", peaks["bf16_tflops"]), 4),
+                    "peak_source": peak_kind + " (bf16_tflops_sustained: the network runs inside a long step)"},
+        "windows": {k: st[k] for k in ("subTiles", "netSubTiles", "copySubTiles", "emptySubTiles", "overflowSubTiles")},
+        "judge": {"threshold_db": 45.0, "peak_dn": peak, "fallback_windows": st["fallbackSubTiles"],
+                  "min_psnr_db": round(st["minPsnr"], 2), "mean_psnr_db": round(st["meanPsnr"], 2),
+                  "p1_psnr_db": round(float(np.percentile(fin, 1)), 2), "p5_psnr_db": round(float(np.percentile(fin, 5)), 2),
+                  "median_psnr_db": round(float(np.median(fin)), 2), "max_abs_error": st["maxAbsError"],
+                  "windows_at_or_above_45db": round(float(np.mean(ps >= 45.0)), 4),
+                  "network_windows": _by_kind(ps, kind, None)["network_windows"],
+                  "copy_windows": _by_kind(ps, kind, None, 1)["copy_windows"]},
+        "untrained_head": untr, "train": train_info,
+    }
+    del louts
+    return res
+
+
+def _by_kind(ps, kind, key, k=2):
+    """PSNR summary of the windows of one kind (2 network, 1 copy)."""
+    name = {2: "network_windows", 1: "copy_windows"}[k]
+    sel = ps[kind == k]
+    fin = sel[np.isfinite(sel)]
+    d = {"count": int(sel.size), "below_45db": int(np.sum(sel < 45.0)),
+         "mean_psnr_db": round(float(fin.mean()), 2) if fin.size else None,
+         "p1_psnr_db": round(float(np.percentile(fin, 1)), 2) if fin.size else None,
+         "p5_psnr_db": round(float(np.percentile(fin, 5)), 2) if fin.size else None,
+         "median_psnr_db": round(float(np.median(fin)), 2) if fin.size else None}
+    return {name: d} if key is None else {key: d}
 
 
 def run_e2e(args, S, stream, world, device):
@@ -470,6 +633,12 @@ def main():
     ap.add_argument("--cpu-tiles", type=int, default=45, help="tiles in the CPU-baseline sample")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-learned", action="store_true", help="skip the learned blend")
+    ap.add_argument("--train-steps", type=int, default=782, help="Adam steps (782 x 64 = 50k windows)")
+    ap.add_argument("--train-batch", type=int, default=64)
+    ap.add_argument("--train-scenes", type=int, default=4)
+    ap.add_argument("--learned-batch", type=int, default=256, help="network windows per pass")
+    ap.add_argument("--weights", default="", help="trained parameters (fp32) instead of training")
     args = ap.parse_args()
     if args.warmup < 3 and args.impl == "ours":
         log("note: warmup raised to 3")

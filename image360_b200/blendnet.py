@@ -40,6 +40,8 @@ def _bind():
     L.i360b_blendnet_gradients.argtypes = [vp, jp, i, i, i, ct.POINTER(ct.c_float), ct.POINTER(ct.c_double)]
     L.i360b_blendnet_train_step.argtypes = [vp, jp, i, i, i, f, ct.POINTER(ct.c_double), vp]
     L.i360b_blendnet_infer.argtypes = [vp, jp, i, i, i, vp]
+    L.i360b_blendnet_profile.argtypes = [vp, jp, i, i, i, ct.POINTER(ct.c_float), i]
+    L.i360b_blendnet_kernel_name.restype = ct.c_char_p
     L.i360b_conv3x3_forward.argtypes = [vp, vp, i, i, i, i, i, i, vp, vp, i, vp, vp, vp]
     L.i360b_conv3x3_wgrad.argtypes = [vp, vp, i, vp, i, i, i, i, i, vp, vp]
     L._blendnet_bound = True
@@ -114,6 +116,8 @@ class BlendNet:
     def __init__(self, seed: int = 0):
         L = _bind()
         self._L = L
+        if not L.i360b_is_initialized():
+            _check(L.i360b_initialize())
         h = ct.c_void_p()
         _check(L.i360b_blendnet_create(ct.c_ulonglong(seed), ct.byref(h)))
         self._h = h
@@ -160,6 +164,12 @@ class BlendNet:
 
     def infer(self, jobs, n: int, w: int, h: int, stream=None):
         _check(self._L.i360b_blendnet_infer(self._h, jobs, n, w, h, _ptr(stream)))
+
+    def profile(self, jobs, n: int, w: int, h: int) -> dict:
+        """One inference pass timed per kernel: {kernel name: ms}."""
+        ms = (ct.c_float * 16)()
+        _check(self._L.i360b_blendnet_profile(self._h, jobs, n, w, h, ms, 16))
+        return {self._L.i360b_blendnet_kernel_name(i).decode(): float(ms[i]) for i in range(10)}
 
 
 def conv3x3_forward(x, weights, bias, cout: int, epilogue: int, out, u=None, skip: int = 0, act=None, stream=None):

@@ -1195,26 +1195,44 @@ struct BlendNet
     }
 
     // Forward pass over the windows jobs[0..n); the last layer writes logits
-    // (training) or the blended output (composite).
-    int forward(const i360b_blend_job* jobs, int n, int w, int h, bool composite, cudaStream_t s)
+    // (training) or the blended output (composite).  With `ev` non-null,
+    // records ev[i] before kernel i and ev[kForwardKernels] after the last.
+    static constexpr int kForwardKernels = 10;
+    int forward(const i360b_blend_job* jobs, int n, int w, int h, bool composite, cudaStream_t s,
+                cudaEvent_t* ev = nullptr)
     {
         const int hw = w / 2, hh = h / 2;
+        auto mark = [&](int i) {
+            if (ev) cudaEventRecord(ev[i], s);
+        };
+        mark(0);
         k_pack_input<<<elementwise_grid((long long)n * w * h), 256, 0, s>>>(jobs, n, h, w, x0);
         I360B_TRY(check_launch("input pack kernel"));
+        mark(1);
         I360B_TRY(dispatch_conv(16, 32, LD_PLAIN, EP_RELU, conv(x0, n, w, h, 0, a1, jobs), s));
+        mark(2);
         I360B_TRY(dispatch_conv(32, 32, LD_PLAIN, EP_RELU, conv(a1, n, w, h, 1, a2, jobs), s));
+        mark(3);
         k_pool2<<<elementwise_grid((long long)n * hw * hh * 4), 256, 0, s>>>(a2, n, h, w, 4, p2);
         I360B_TRY(check_launch("pool kernel"));
+        mark(4);
         I360B_TRY(dispatch_conv(32, 64, LD_PLAIN, EP_RELU, conv(p2, n, hw, hh, 2, a3, jobs), s));
+        mark(5);
         I360B_TRY(dispatch_conv(64, 64, LD_PLAIN, EP_RELU, conv(a3, n, hw, hh, 3, a4, jobs), s));
+        mark(6);
         I360B_TRY(dispatch_conv(64, 64, LD_PLAIN, EP_RELU, conv(a4, n, hw, hh, 4, a5, jobs), s));
+        mark(7);
         ConvArgs c6 = conv(a2, n, w, h, 5, a6, jobs);
         c6.u = a5;
         c6.cs = 32;
         I360B_TRY(dispatch_conv(96, 32, LD_CONCAT, EP_RELU, c6, s));
+        mark(8);
         I360B_TRY(dispatch_conv(32, 32, LD_PLAIN, EP_RELU, conv(a6, n, w, h, 6, a7, jobs), s));
-        if (composite) return dispatch_conv(32, 16, LD_PLAIN, EP_COMPOSITE, conv(a7, n, w, h, 7, nullptr, jobs), s);
-        return dispatch_conv(32, 16, LD_PLAIN, EP_LOGITS, conv(a7, n, w, h, 7, logits, jobs), s);
+        mark(9);
+        if (composite) I360B_TRY(dispatch_conv(32, 16, LD_PLAIN, EP_COMPOSITE, conv(a7, n, w, h, 7, nullptr, jobs), s));
+        else I360B_TRY(dispatch_conv(32, 16, LD_PLAIN, EP_LOGITS, conv(a7, n, w, h, 7, logits, jobs), s));
+        mark(10);
+        return I360B_SUCCESS;
     }
 
     // Backward data through layer l (flipped, transposed weights).
@@ -1477,6 +1495,39 @@ extern "C" int i360b_blendnet_infer(i360b_blendnet* net, const i360b_blend_job* 
         return N.forward(N.dJobs, n, w, h, true, s);
     }();
     return N.end(s, rc);
+}
+
+extern "C" int i360b_blendnet_profile(i360b_blendnet* net, const i360b_blend_job* jobs, int n, int w, int h,
+                                      float* kernelMs, int maxKernels)
+{
+    I360B_TRY(net_prologue(net));
+    I360B_TRY(check_window(n, w, h));
+    if (!kernelMs) return fail(I360B_INVALID_PARAM, "Null pointer argument.");
+    BlendNet& N = net->net;
+    std::lock_guard<std::mutex> lk(N.mu);
+    cudaStream_t s = thread_stream();
+    I360B_TRY(N.begin(s));
+    cudaEvent_t ev[BlendNet::kForwardKernels + 1] = {};
+    int rc = [&]() -> int {
+        for (auto& e : ev) I360B_CUDA(cudaEventCreate(&e), "profile events");
+        I360B_TRY(N.reserve(n, w, h, false));
+        I360B_TRY(N.upload_jobs(jobs, n, s));
+        I360B_TRY(N.forward(N.dJobs, n, w, h, true, s, ev));
+        I360B_CUDA(cudaEventSynchronize(ev[BlendNet::kForwardKernels]), "profile");
+        for (int i = 0; i < BlendNet::kForwardKernels && i < maxKernels; ++i)
+            cudaEventElapsedTime(&kernelMs[i], ev[i], ev[i + 1]);
+        return N.check_error(s);
+    }();
+    for (auto& e : ev)
+        if (e) cudaEventDestroy(e);
+    return N.end(s, rc);
+}
+
+extern "C" const char* i360b_blendnet_kernel_name(int i)
+{
+    static const char* const names[] = {"pack_input", "conv1_16_32",  "conv2_32_32", "pool",        "conv3_32_64",
+                                        "conv4_64_64", "conv5_64_64", "conv6_96_32", "conv7_32_32", "conv8_32_4_blend"};
+    return i >= 0 && i < 10 ? names[i] : nullptr;
 }
 
 extern "C" int i360b_conv3x3_forward(const void* dX, const void* dU, int skipChannels, int n, int h, int w, int cin,
@@ -1945,6 +1996,29 @@ extern "C" int i360b_render_plan_judge(i360b_render_plan* plan, unsigned short* 
     if (!(peak > 0.0)) return fail(I360B_INVALID_PARAM, "peak must be > 0.");
     return learned_judge(plan->plan, dTileOut, minPsnrDb, peak, stats, hostSubTilePsnr, maxSubTiles,
                          static_cast<cudaStream_t>(stream));
+}
+
+extern "C" int i360b_render_plan_windows(i360b_render_plan* plan, int maxWindows, int* info, int* numWindows)
+{
+    clear_error();
+    if (!plan || !numWindows) return fail(I360B_INVALID_PARAM, "Null pointer argument.");
+    Plan& P = plan->plan;
+    if (!P.render) return fail(I360B_INVALID_PARAM, "not a render plan");
+    build_subtiles(P);
+    *numWindows = (int)P.subTiles.size();
+    if (info)
+        for (int i = 0; i < (int)P.subTiles.size() && i < maxWindows; ++i)
+        {
+            const SubTile& t = P.subTiles[i];
+            int* o = info + 6 * i;
+            o[0] = t.tile;
+            o[1] = t.ox;
+            o[2] = t.oy;
+            o[3] = t.kind;
+            o[4] = t.overflow;
+            o[5] = (t.item[0] >= 0) + (t.item[1] >= 0) + (t.item[2] >= 0) + (t.item[3] >= 0);
+        }
+    return I360B_SUCCESS;
 }
 
 extern "C" int i360b_render_plan_tile_items(i360b_render_plan* plan, int tile, int maxItems,

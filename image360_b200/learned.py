@@ -41,6 +41,7 @@ def _bind():
     L.i360b_render_plan_judge.argtypes = [vp, ct.POINTER(vp), ct.c_double, ct.c_double, ct.POINTER(LearnedStats),
                                           ct.POINTER(ct.c_float), i, vp]
     L.i360b_render_plan_tile_items.argtypes = [vp, i, i, ct.POINTER(vp), ct.POINTER(ct.c_int), ct.POINTER(ct.c_int)]
+    L.i360b_render_plan_windows.argtypes = [vp, i, ct.POINTER(ct.c_int), ct.POINTER(ct.c_int)]
     L._learned_bound = True
     return L
 
@@ -131,6 +132,16 @@ class PanoramaRender:
         d = {k: getattr(st, k) for k, _ in LearnedStats._fields_}
         return d, np.frombuffer(ps, np.float32).copy()
 
+    def windows(self) -> np.ndarray:
+        """[n, 6] int array {tile, x, y, kind (0 clear, 1 copy, 2 network),
+        overflow, contributors} in judge order."""
+        L = _bind()
+        n = ct.c_int()
+        _check(L.i360b_render_plan_windows(self.plan._h, 0, None, ct.byref(n)))
+        buf = (ct.c_int * (6 * max(n.value, 1)))()
+        _check(L.i360b_render_plan_windows(self.plan._h, n.value, buf, ct.byref(n)))
+        return np.frombuffer(buf, np.int32)[:6 * n.value].reshape(-1, 6).copy()
+
     def close(self):
         self.plan.close()
 
@@ -202,6 +213,32 @@ def training_config(base: synth.PanoConfig, seed: int) -> synth.PanoConfig:
     return synth.PanoConfig(**{**base.__dict__, "seed": seed})
 
 
+def train_on_scenes(base: synth.PanoConfig, scenes: int, steps: int, batch: int = 64, lr: float = 1e-3,
+                    seed: int = 1, log=None) -> bn.BlendNet:
+    """Trains a new network on ``scenes`` seeded panoramas of configuration
+    ``base`` (seeds 7000 + 31 k, disjoint from the benchmark's), one scene
+    resident at a time, ``steps`` Adam steps in total."""
+    import torch
+    net = bn.BlendNet(seed=seed)
+    done = 0
+    for k in range(scenes):
+        t0 = time.time()
+        r = PanoramaRender(training_config(base, 7000 + 31 * k))
+        r.render_plain()
+        n = (steps - done) // (scenes - k)
+        if log:
+            log(f"scene {k}: {r.pano.canvas_w}x{r.pano.canvas_h}, {len(r.tiles)} tiles, rendered in "
+                f"{time.time() - t0:.1f}s; {n} steps")
+        losses = train(net, [r], n, batch, lr, seed=seed + k, log=log)
+        done += n
+        r.close()
+        del r
+        torch.cuda.empty_cache()
+        if log and losses:
+            log(f"scene {k}: last-50 loss {np.mean(losses[-50:]):.3e}")
+    return net
+
+
 def main():
     import torch
     ap = argparse.ArgumentParser(description=__doc__.split("\n")[0])
@@ -216,23 +253,11 @@ def main():
     args = ap.parse_args()
     log = lambda *a: print(*a, flush=True)
     base = synth.C1 if args.scale == 1.0 else synth.scaled(synth.C1, args.scale)
-    renders = []
-    for k in range(args.scenes):
-        t0 = time.time()
-        r = PanoramaRender(training_config(base, 7000 + 31 * k))
-        r.render_plain()
-        renders.append(r)
-        log(f"scene {k}: {r.pano.canvas_w}x{r.pano.canvas_h}, {len(r.tiles)} tiles, rendered in "
-            f"{time.time() - t0:.1f}s")
-    net = bn.BlendNet(seed=args.seed)
-    losses = train(net, renders, args.steps, args.batch, args.lr, seed=args.seed, log=log)
-    log(f"trained {args.steps} steps x {args.batch} windows; last-50 loss {np.mean(losses[-50:]):.3e}")
+    net = train_on_scenes(base, args.scenes, args.steps, args.batch, args.lr, args.seed, log)
     if args.out:
         net.get_params().tofile(args.out)
         log(f"weights -> {args.out}")
     if args.eval:
-        for r in renders:
-            r.close()
         torch.cuda.empty_cache()
         ev = PanoramaRender(base)
         ev.render_plain()

@@ -83,6 +83,13 @@ I360B_API int i360b_blendnet_train_step(i360b_blendnet* net, const i360b_blend_j
 I360B_API int i360b_blendnet_infer(i360b_blendnet* net, const i360b_blend_job* jobs, int n, int w, int h,
                                    void* stream);
 
+/* One inference pass timed kernel by kernel with CUDA events: kernelMs
+ * receives up to maxKernels times (10 kernels, names from
+ * i360b_blendnet_kernel_name).  Synchronous. */
+I360B_API int i360b_blendnet_profile(i360b_blendnet* net, const i360b_blend_job* jobs, int n, int w, int h,
+                                     float* kernelMs, int maxKernels);
+I360B_API const char* i360b_blendnet_kernel_name(int kernel);
+
 /* ---- learned render of a panorama --------------------------------------- */
 
 /* Every output tile of a render plan is cut into 256x256 windows (partial at
@@ -120,6 +127,11 @@ I360B_API int i360b_render_plan_learned(i360b_render_plan* plan, i360b_blendnet*
 I360B_API int i360b_render_plan_judge(i360b_render_plan* plan, unsigned short* const* dTileOut, double minPsnrDb,
                                       double peak, i360b_learned_stats* stats, float* hostSubTilePsnr,
                                       int maxSubTiles, void* stream);
+/* The plan's windows in judge order: 6 ints per window {tile, x, y, kind
+ * (0 clear, 1 copy, 2 network), overflow (more than 4 contributors reached
+ * it), contributors kept}; numWindows receives the count, up to maxWindows
+ * entries are written. */
+I360B_API int i360b_render_plan_windows(i360b_render_plan* plan, int maxWindows, int* info, int* numWindows);
 /* The warped contributor images of tile `tile` after an execute (device RGB48,
  * tile-sized) and their footprint boxes {x0, y0, x1, y1} in tile pixels
  * (outside the box the image is zero).  numItems receives the count; up to
