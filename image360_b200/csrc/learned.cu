@@ -26,6 +26,8 @@
 #include "tc_common.cuh"
 #include "../../include/image360_b200_blendnet.h"
 
+#include <cuda.h>
+#include <cudaTypedefs.h>
 #include <cuda_bf16.h>
 
 #include <algorithm>
@@ -41,8 +43,7 @@ namespace
 {
 using bf16 = __nv_bfloat16;
 
-constexpr int kTileX = 128;                // pixels per MMA row block (M)
-constexpr int kHaloW = kTileX + 2;         // halo row length
+constexpr int kTileX = 128;                // pixels per weight-gradient tile (one row)
 constexpr long long kWaitSpins = 1ll << 26;  // bounded mbarrier waits
 constexpr int kSlots = 4;
 constexpr float kInScale = 1.0f / 32768.0f;
@@ -75,20 +76,31 @@ struct ConvArgs
     int* error;
 };
 
-template <int CIN, int NPAD, int R>
+// Tile geometry of the 3x3 convolution: TW x TH output pixels per tile, split
+// into M blocks of 8 columns x 16 rows; the input halo of (TW+2) x (TH+2)
+// pixels is kept per 8-channel chunk with row pitch kP = TW+2 pixels.
+template <int CIN, int NPAD, int TW, int TH, int STAGES, int LD>
 struct ConvShape
 {
     static constexpr int kC8 = CIN / 8;
-    static constexpr uint32_t kChunk = (R + 2) * kHaloW * 16;  // bytes of one 8-channel halo chunk
-    static constexpr uint32_t kHalo = kC8 * kChunk;
+    static constexpr int kP = TW + 2;
+    static constexpr int kHaloPx = (TW + 2) * (TH + 2);
+    static constexpr uint32_t kBox = kHaloPx * 16;                  // bytes of one chunk box
+    static constexpr uint32_t kChunk = (kBox + 127) / 128 * 128;    // TMA destinations 128-byte aligned
+    static constexpr uint32_t kStage = kC8 * kChunk;
     static constexpr uint32_t kW = 9u * CIN * NPAD * 2;
-    static constexpr uint32_t kSmem = kW + 2 * kHalo + 64;
-    static constexpr uint32_t kSlotCols = R * NPAD;
+    static constexpr int kBX = TW / 8, kBY = TH / 16, kMB = kBX * kBY;
+    static constexpr uint32_t kSlotCols = kMB * NPAD;
     static constexpr uint32_t kTmem = tc::tmem_cols(2 * kSlotCols);
     static constexpr int kKSteps = 9 * CIN / 16;
+    static constexpr int kThreads = LD == LD_CONCAT ? 320 : 192;
+    static constexpr uint32_t kBars = (2 * STAGES + 4) * 8 + 16;
+    static constexpr uint32_t kSmem = 128 + kW + STAGES * kStage + kBars;
     static_assert(CIN % 16 == 0 && NPAD % 16 == 0 && NPAD >= 16 && NPAD <= 256, "MMA shape");
+    static_assert(TW % 8 == 0 && TH % 16 == 0 && TW + 2 <= 256 && TH + 2 <= 256, "tile shape");
     static_assert(2 * kSlotCols <= 512, "TMEM capacity");
-    static_assert(kChunk / 16 < (1u << 14), "descriptor LBO range");
+    static_assert(kW % 128 == 0, "ring alignment");
+    static_assert(kChunk / 16 < (1u << 14) && kP < (1 << 14), "descriptor offset range");
     static_assert(kSmem <= 227u * 1024u, "shared memory");
 };
 
@@ -177,210 +189,270 @@ __device__ __forceinline__ void composite_pixel(const i360b_blend_job& J, int y,
 }
 
 // ---------------------------------------------------------------------------
-// 3x3 convolution (forward, or backward-data with flipped transposed weights).
-// Persistent: CTA b handles tiles b, b + gridDim.x, ...; 128 threads; thread 0
-// issues the MMAs, all four warps load and run the epilogue (warp w owns TMEM
-// lanes 32w..32w+31 = pixels 32w..32w+31 of the tile).
+// 3x3 convolution (forward, or backward-data with flipped transposed weights),
+// persistent and warp-specialised; CTA b handles tiles b, b + gridDim.x, ...
+//
+// The A operand of tap (dy, dx) for M block (bx, by) is the halo chunk with
+// the descriptor start moved by ((16 by + dy) kP + 8 bx + dx) * 16 bytes: the
+// 8 pixels of a block row are one core matrix (8 rows of 16 bytes) and the 16
+// block rows are core-matrix groups kP * 16 bytes apart (SBO); the two
+// 8-channel halves of a K step are one chunk apart (LBO).
+//
+// Roles:
+//   warp 4 lane 0  TMA producer: one 4-D box (8 channels x (TW+2) x (TH+2))
+//                  per chunk into a STAGES-deep ring, zero fill outside the
+//                  image;
+//   warps 6-9      (concatenated input only) cp.async producers of the
+//                  nearest-upsampled half-resolution channels;
+//   warp 5 lane 0  MMA issuer: MB x 9 CIN/16 tcgen05.mma per tile into one of
+//                  two TMEM accumulators; commits free the ring stage and
+//                  publish the accumulator;
+//   warps 0-3      epilogue: TMEM lanes 32w..32w+31 (rows 4w..4w+3 of each M
+//                  block) -> bias/ReLU, mask, raw or blend head -> global.
+// Every wait is bounded; a timeout sets the error flag and the CTA winds
+// down after its loads have landed.
 // ---------------------------------------------------------------------------
-template <int CIN, int NPAD, int R, int LD, int EP>
-__global__ void __launch_bounds__(128, 1) k_conv3x3(ConvArgs a)
+template <int CIN, int NPAD, int TW, int TH, int STAGES, int LD, int EP>
+__global__ void __launch_bounds__(ConvShape<CIN, NPAD, TW, TH, STAGES, LD>::kThreads, 1)
+    k_conv3x3(const __grid_constant__ CUtensorMap tmap, ConvArgs a)
 {
-    using S = ConvShape<CIN, NPAD, R>;
-    extern __shared__ __align__(128) unsigned char smem[];
+    using S = ConvShape<CIN, NPAD, TW, TH, STAGES, LD>;
+    extern __shared__ unsigned char smemRaw[];
+    unsigned char* smem =
+        reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(smemRaw) + 127) & ~uintptr_t(127));
     unsigned char* wsm = smem;
-    unsigned char* halo0 = smem + S::kW;
-    uint64_t* mbar = reinterpret_cast<uint64_t*>(smem + S::kW + 2 * S::kHalo);
-    uint32_t* tmemSlot = reinterpret_cast<uint32_t*>(mbar + 2);
+    unsigned char* ring = smem + S::kW;
+    uint64_t* full = reinterpret_cast<uint64_t*>(ring + STAGES * S::kStage);
+    uint64_t* empty = full + STAGES;
+    uint64_t* accFull = empty + STAGES;
+    uint64_t* accEmpty = accFull + 2;
+    uint32_t* tmemSlot = reinterpret_cast<uint32_t*>(accEmpty + 2);
 
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-    const int tilesX = a.w / kTileX, tilesY = (a.h + R - 1) / R;
-    const long long nTiles = (long long)a.n * tilesY * tilesX;
+    const int tilesX = (a.w + TW - 1) / TW, tilesY = (a.h + TH - 1) / TH;
+    const long long nTiles = (long long)a.n * tilesX * tilesY;
     if ((long long)blockIdx.x >= nTiles) return;
     const int myTiles = (int)((nTiles - 1 - blockIdx.x) / gridDim.x) + 1;
-
-    auto coord = [&](long long t, int& img, int& y0, int& x0) {
-        x0 = (int)(t % tilesX) * kTileX;
+    auto coord = [&](int i, int& img, int& y0, int& x0) {
+        const long long t = blockIdx.x + (long long)i * gridDim.x;
+        x0 = (int)(t % tilesX) * TW;
         const long long r = t / tilesX;
-        y0 = (int)(r % tilesY) * R;
+        y0 = (int)(r % tilesY) * TH;
         img = (int)(r / tilesY);
     };
-    auto loadHalo = [&](long long t, unsigned char* buf) {
-        int img, y0, x0;
-        coord(t, img, y0, x0);
-        constexpr int kN = S::kC8 * (R + 2) * kHaloW;
-        for (int q = tid; q < kN; q += 128)
-        {
-            const int c8 = q % S::kC8;
-            const int rest = q / S::kC8;
-            const int hx = rest % kHaloW, hr = rest / kHaloW;
-            const int yy = y0 - 1 + hr, xx = x0 - 1 + hx;
-            const bool ok = yy >= 0 && yy < a.h && xx >= 0 && xx < a.w;
-            const bf16* src = ok ? input_chunk<CIN, LD>(a.x, a.u, a.cs, a.h, a.w, img, yy, xx, c8) : a.x;
-            tc::cp_async16(buf + c8 * S::kChunk + (hr * kHaloW + hx) * 16, src, ok ? 16 : 0);
-        }
-    };
+    const int tmaChunks = LD == LD_CONCAT ? (a.cs >> 3) : S::kC8;
 
     if (warp == 0) tc::tmem_alloc(tmemSlot, S::kTmem);
     if (tid == 0)
     {
-        tc::mbar_init(&mbar[0], 1);
-        tc::mbar_init(&mbar[1], 1);
+        for (int s = 0; s < STAGES; ++s)
+        {
+            tc::mbar_init(&full[s], LD == LD_CONCAT ? 1 + 128 : 1);
+            tc::mbar_init(&empty[s], 1);
+        }
+        for (int k = 0; k < 2; ++k)
+        {
+            tc::mbar_init(&accFull[k], 1);
+            tc::mbar_init(&accEmpty[k], 4);
+        }
         tc::fence_mbar_init();
     }
     {
         constexpr int kK8 = 9 * S::kC8;
-        for (int q = tid; q < NPAD * kK8; q += 128)
+        for (int q = tid; q < NPAD * kK8; q += blockDim.x)
         {
             const int n = q / kK8, k8 = q % kK8;
             tc::cp_async16(wsm + k8 * (NPAD * 16) + n * 16, a.wt + (size_t)n * 9 * CIN + k8 * 8, 16);
         }
+        tc::cp_async_commit();
+        tc::cp_async_wait<0>();
+        tc::fence_proxy_async();
     }
-    loadHalo(blockIdx.x, halo0);
-    tc::cp_async_commit();
     tc::fence_before_sync();
     __syncthreads();
     tc::fence_after_sync();
     const uint32_t tmem = *tmemSlot;
+    bool ok = true;
 
-    auto issue = [&](int slot) {
-        tc::fence_after_sync();
-        const uint32_t hb = tc::smem_u32(halo0 + slot * S::kHalo), wb = tc::smem_u32(wsm);
-        constexpr uint32_t idesc = tc::idesc_bf16_f32(128, NPAD);
-        for (int r = 0; r < R; ++r)
+    if (warp == 4)
+    {
+        if (lane == 0)
         {
-            const uint32_t d = tmem + slot * S::kSlotCols + r * NPAD;
-#pragma unroll 4
-            for (int ks = 0; ks < S::kKSteps; ++ks)
+            int issued = 0;
+            for (int i = 0; i < myTiles; ++i)
             {
-                const int k0 = ks * 16, tap = k0 / CIN, c8 = (k0 % CIN) >> 3;
-                const int dy = tap / 3, dx = tap % 3;
-                const uint32_t aAddr = hb + c8 * S::kChunk + ((r + dy) * kHaloW + dx) * 16;
-                const uint32_t bAddr = wb + (2 * ks) * (NPAD * 16);
-                tc::mma_bf16(d, tc::smem_desc(aAddr, S::kChunk, 128), tc::smem_desc(bAddr, NPAD * 16, 128), idesc,
-                             ks > 0 ? 1u : 0u);
+                const int s = i % STAGES;
+                if (!tc::mbar_wait(&empty[s], ((i / STAGES) & 1) ^ 1, kWaitSpins))
+                {
+                    ok = false;
+                    break;
+                }
+                int img, y0, x0;
+                coord(i, img, y0, x0);
+                unsigned char* st = ring + s * S::kStage;
+                tc::mbar_arrive_expect_tx(&full[s], (uint32_t)tmaChunks * S::kBox);
+                for (int c = 0; c < tmaChunks; ++c)
+                    tc::tma_load_4d(st + c * S::kChunk, &tmap, c * 8, x0 - 1, y0 - 1, img, &full[s]);
+                issued = i + 1;
+            }
+            // The last loads must land before the CTA may exit.
+            for (int j = max(0, issued - STAGES); j < issued; ++j)
+                if (!tc::mbar_wait(&full[j % STAGES], (j / STAGES) & 1, kWaitSpins)) ok = false;
+        }
+    }
+    else if (LD == LD_CONCAT && warp >= 6)
+    {
+        const int ptid = tid - 192;
+        const int sc8 = a.cs >> 3, nu8 = S::kC8 - sc8, uc = CIN - a.cs;
+        const int hh = a.h >> 1, hw = a.w >> 1;
+        for (int i = 0; i < myTiles; ++i)
+        {
+            const int s = i % STAGES;
+            if (!tc::mbar_wait(&empty[s], ((i / STAGES) & 1) ^ 1, kWaitSpins))
+            {
+                ok = false;
+                break;
+            }
+            int img, y0, x0;
+            coord(i, img, y0, x0);
+            unsigned char* st = ring + s * S::kStage;
+            const int nq = nu8 * S::kHaloPx;
+            for (int q = ptid; q < nq; q += 128)
+            {
+                const int cu = q % nu8, px = q / nu8;
+                const int hx = px % S::kP, hy = px / S::kP;
+                const int yy = y0 - 1 + hy, xx = x0 - 1 + hx;
+                const bool in = yy >= 0 && yy < a.h && xx >= 0 && xx < a.w;
+                const bf16* src =
+                    in ? a.u + ((((size_t)img * hh + (yy >> 1)) * hw + (xx >> 1)) * uc + cu * 8) : a.u;
+                tc::cp_async16(st + (sc8 + cu) * S::kChunk + px * 16, src, in ? 16 : 0);
+            }
+            tc::cp_async_arrive_noinc(&full[s]);
+        }
+        tc::cp_async_wait<0>();
+    }
+    else if (warp == 5)
+    {
+        if (lane == 0)
+        {
+            constexpr uint32_t idesc = tc::idesc_bf16_f32(128, NPAD);
+            const uint32_t wb = tc::smem_u32(wsm);
+            for (int i = 0; i < myTiles; ++i)
+            {
+                const int s = i % STAGES, acc = i & 1;
+                if (!tc::mbar_wait(&full[s], (i / STAGES) & 1, kWaitSpins) ||
+                    !tc::mbar_wait(&accEmpty[acc], ((i >> 1) & 1) ^ 1, kWaitSpins))
+                {
+                    ok = false;
+                    break;
+                }
+                if (LD == LD_CONCAT) tc::fence_proxy_async();  // cp.async data -> tensor core
+                tc::fence_after_sync();
+                const uint32_t hb = tc::smem_u32(ring + s * S::kStage);
+                for (int b = 0; b < S::kMB; ++b)
+                {
+                    const int bx = b % S::kBX, by = b / S::kBX;
+                    const uint32_t d = tmem + acc * S::kSlotCols + b * NPAD;
+#pragma unroll 4
+                    for (int ks = 0; ks < S::kKSteps; ++ks)
+                    {
+                        const int k0 = ks * 16, tap = k0 / CIN, c8 = (k0 % CIN) >> 3;
+                        const int dy = tap / 3, dx = tap % 3;
+                        const uint32_t aAddr = hb + c8 * S::kChunk + ((by * 16 + dy) * S::kP + bx * 8 + dx) * 16;
+                        tc::mma_bf16(d, tc::smem_desc(aAddr, S::kChunk, S::kP * 16),
+                                     tc::smem_desc(wb + 2 * ks * (NPAD * 16), NPAD * 16, 128), idesc, ks > 0 ? 1u : 0u);
+                    }
+                }
+                tc::mma_commit(&empty[s]);
+                tc::mma_commit(&accFull[acc]);
             }
         }
-        tc::mma_commit(&mbar[slot]);
-    };
-
-    auto epilogue = [&](long long t, int slot) {
-        int img, y0, x0;
-        coord(t, img, y0, x0);
-        const int px = x0 + warp * 32 + lane;
-        const uint32_t base = tmem + ((uint32_t)(warp * 32) << 16) + slot * S::kSlotCols;
-        for (int r = 0; r < R; ++r)
+    }
+    else if (warp < 4)
+    {
+        for (int i = 0; i < myTiles; ++i)
         {
-            const int y = y0 + r;
-            const bool valid = y < a.h;  // uniform across the warp
-            const size_t pix = ((size_t)img * a.h + y) * a.w + px;
-            if (EP == EP_LOGITS || EP == EP_COMPOSITE)
+            const int acc = i & 1;
+            bool done = tc::mbar_wait(&accFull[acc], (i >> 1) & 1, kWaitSpins);
+            done = __all_sync(0xffffffffu, done);
+            if (!done)
             {
-                float v[16];
-                tc::tmem_ld16(base + r * NPAD, v);
-                if (!valid) continue;
-                float l[4];
-#pragma unroll
-                for (int j = 0; j < 4; ++j) l[j] = v[j] + a.bias[j];
-                if (EP == EP_LOGITS)
+                ok = false;
+                break;
+            }
+            tc::fence_after_sync();
+            int img, y0, x0;
+            coord(i, img, y0, x0);
+            const uint32_t base = tmem + ((uint32_t)(warp * 32) << 16) + acc * S::kSlotCols;
+            for (int b = 0; b < S::kMB; ++b)
+            {
+                const int bx = b % S::kBX, by = b / S::kBX;
+                const int y = y0 + by * 16 + warp * 4 + (lane >> 3);
+                const int x = x0 + bx * 8 + (lane & 7);
+                const bool valid = y < a.h && x < a.w;
+                const size_t pix = ((size_t)img * a.h + y) * a.w + x;
+                if (EP == EP_LOGITS || EP == EP_COMPOSITE)
                 {
-                    reinterpret_cast<float4*>(a.out)[pix] = make_float4(l[0], l[1], l[2], l[3]);
+                    float v[16];
+                    tc::tmem_ld16(base + b * NPAD, v);
+                    if (!valid) continue;
+                    float l[4];
+#pragma unroll
+                    for (int j = 0; j < 4; ++j) l[j] = v[j] + a.bias[j];
+                    if (EP == EP_LOGITS)
+                    {
+                        reinterpret_cast<float4*>(a.out)[pix] = make_float4(l[0], l[1], l[2], l[3]);
+                    }
+                    else
+                    {
+                        const i360b_blend_job& J = a.jobs[img];
+                        if (x < J.width && y < J.height)
+                        {
+                            float o[3], wts[4], vv[4][3];
+                            bool cov[4];
+                            int nCov;
+                            composite_pixel(J, y, x, l, o, wts, vv, cov, nCov);
+                            unsigned short* q = J.out + (long long)y * J.outRowStride + (long long)x * 3;
+#pragma unroll
+                            for (int c = 0; c < 3; ++c)
+                                q[c] = (unsigned short)__float2uint_rn(fminf(fmaxf(o[c], 0.0f), 65535.0f));
+                        }
+                    }
                 }
                 else
                 {
-                    const i360b_blend_job& J = a.jobs[img];
-                    if (px < J.width && y < J.height)
-                    {
-                        float o[3], wts[4], vv[4][3];
-                        bool cov[4];
-                        int nCov;
-                        composite_pixel(J, y, px, l, o, wts, vv, cov, nCov);
-                        unsigned short* q = J.out + (long long)y * J.outRowStride + (long long)px * 3;
-#pragma unroll
-                        for (int c = 0; c < 3; ++c)
-                            q[c] = (unsigned short)__float2uint_rn(fminf(fmaxf(o[c], 0.0f), 65535.0f));
-                    }
-                }
-            }
-            else
-            {
 #pragma unroll 1
-                for (int cb = 0; cb < NPAD / 16; ++cb)
-                {
-                    float v[16];
-                    tc::tmem_ld16(base + r * NPAD + cb * 16, v);
-                    if (!valid) continue;
-                    if (EP == EP_RELU)
+                    for (int cb = 0; cb < NPAD / 16; ++cb)
                     {
+                        float v[16];
+                        tc::tmem_ld16(base + b * NPAD + cb * 16, v);
+                        if (!valid) continue;
+                        if (EP == EP_RELU)
+                        {
 #pragma unroll
-                        for (int j = 0; j < 16; ++j) v[j] = fmaxf(v[j] + a.bias[cb * 16 + j], 0.0f);
-                    }
-                    if (EP == EP_MASK)
-                    {
-                        const uint4* ap = reinterpret_cast<const uint4*>(a.act + pix * NPAD + cb * 16);
-                        float m[16];
-                        unpack8_bf16(ap[0], m);
-                        unpack8_bf16(ap[1], m + 8);
+                            for (int j = 0; j < 16; ++j) v[j] = fmaxf(v[j] + a.bias[cb * 16 + j], 0.0f);
+                        }
+                        if (EP == EP_MASK)
+                        {
+                            const uint4* ap = reinterpret_cast<const uint4*>(a.act + pix * NPAD + cb * 16);
+                            float m[16];
+                            unpack8_bf16(ap[0], m);
+                            unpack8_bf16(ap[1], m + 8);
 #pragma unroll
-                        for (int j = 0; j < 16; ++j) v[j] = m[j] > 0.0f ? v[j] : 0.0f;
+                            for (int j = 0; j < 16; ++j) v[j] = m[j] > 0.0f ? v[j] : 0.0f;
+                        }
+                        uint4* op = reinterpret_cast<uint4*>(static_cast<bf16*>(a.out) + pix * NPAD + cb * 16);
+                        op[0] = pack8_bf16(v);
+                        op[1] = pack8_bf16(v + 8);
                     }
-                    uint4* op = reinterpret_cast<uint4*>(static_cast<bf16*>(a.out) + pix * NPAD + cb * 16);
-                    op[0] = pack8_bf16(v);
-                    op[1] = pack8_bf16(v + 8);
                 }
             }
-        }
-        tc::fence_before_sync();
-    };
-
-    bool ok = true;
-    for (int i = 0; i < myTiles; ++i)
-    {
-        const int s = i & 1;
-        const long long t = blockIdx.x + (long long)i * gridDim.x;
-        if (i + 1 < myTiles)
-        {
-            if (i >= 1 && !tc::mbar_wait(&mbar[s ^ 1], ((i - 1) >> 1) & 1, kWaitSpins)) ok = false;
-            if (ok) loadHalo(t + gridDim.x, halo0 + (s ^ 1) * S::kHalo);
-            tc::cp_async_commit();
-            tc::cp_async_wait<1>();
-        }
-        else
-        {
-            tc::cp_async_wait<0>();
-        }
-        tc::fence_proxy_async();
-        if (__syncthreads_or(!ok))
-        {
-            ok = false;
-            break;
-        }
-        if (tid == 0) issue(s);
-        if (i >= 1)
-        {
-            bool done = tc::mbar_wait(&mbar[s ^ 1], ((i - 1) >> 1) & 1, kWaitSpins);
-            done = __all_sync(0xffffffffu, done);
-            if (!done) ok = false;
-            else
-            {
-                tc::fence_after_sync();
-                epilogue(t - gridDim.x, s ^ 1);
-            }
+            tc::fence_before_sync();
+            __syncwarp();
+            if (lane == 0) tc::mbar_arrive(&accEmpty[acc]);
         }
     }
-    if (ok)
-    {
-        const int last = myTiles - 1;
-        bool done = tc::mbar_wait(&mbar[last & 1], (last >> 1) & 1, kWaitSpins);
-        done = __all_sync(0xffffffffu, done);
-        if (!done) ok = false;
-        else
-        {
-            tc::fence_after_sync();
-            epilogue(blockIdx.x + (long long)last * gridDim.x, last & 1);
-        }
-    }
-    if (!ok && lane == 0) atomicOr(a.error, 1);
-    tc::cp_async_wait<0>();
+    if (!ok) atomicOr(a.error, 1);
     tc::fence_before_sync();
     __syncthreads();
     if (warp == 0)
@@ -847,47 +919,79 @@ int elementwise_grid(long long n, int block = 256)
     return (int)std::max<long long>(1, std::min<long long>((n + block - 1) / block, (long long)sm_count() * 16));
 }
 
-template <int CIN, int NPAD, int R, int LD, int EP>
+// Tensor map of an NHWC bf16 tensor as (C, W, H, N) with a box of 8
+// channels x boxW x boxH x 1 (zero fill outside).  The encoder comes from the
+// driver through the runtime (no link against the driver library).
+int make_input_map(CUtensorMap* m, const bf16* base, int c, int n, int h, int w, int boxW, int boxH)
+{
+    static PFN_cuTensorMapEncodeTiled_v12000 encode = nullptr;
+    static std::once_flag once;
+    static cudaError_t err = cudaSuccess;
+    std::call_once(once, [] {
+        cudaDriverEntryPointQueryResult q;
+        err = cudaGetDriverEntryPointByVersion("cuTensorMapEncodeTiled", reinterpret_cast<void**>(&encode), 12000,
+                                               cudaEnableDefault, &q);
+        if (err == cudaSuccess && q != cudaDriverEntryPointSuccess) err = cudaErrorSymbolNotFound;
+    });
+    if (err != cudaSuccess || !encode) return cuda_fail(err, "cuTensorMapEncodeTiled entry point");
+    if ((reinterpret_cast<uintptr_t>(base) & 15) || c % 8)
+        return fail(I360B_INVALID_PARAM, "conv3x3 input must be 16-byte aligned with channels a multiple of 8");
+    const cuuint64_t dims[4] = {(cuuint64_t)c, (cuuint64_t)w, (cuuint64_t)h, (cuuint64_t)n};
+    const cuuint64_t strides[3] = {(cuuint64_t)c * 2, (cuuint64_t)w * c * 2, (cuuint64_t)h * w * c * 2};
+    const cuuint32_t box[4] = {8, (cuuint32_t)boxW, (cuuint32_t)boxH, 1};
+    const cuuint32_t es[4] = {1, 1, 1, 1};
+    CUresult r = encode(m, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 4, const_cast<bf16*>(base), dims, strides, box, es,
+                        CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                        CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) return fail(I360B_CUDA_ERROR, "cuTensorMapEncodeTiled failed (%d)", (int)r);
+    return I360B_SUCCESS;
+}
+
+template <int CIN, int NPAD, int TW, int TH, int STAGES, int LD, int EP>
 int run_conv(const ConvArgs& a, cudaStream_t s)
 {
-    using S = ConvShape<CIN, NPAD, R>;
+    using S = ConvShape<CIN, NPAD, TW, TH, STAGES, LD>;
     static std::once_flag once;
     static int perSm = 1;
     static cudaError_t attrErr = cudaSuccess;
     std::call_once(once, [] {
-        attrErr = cudaFuncSetAttribute(k_conv3x3<CIN, NPAD, R, LD, EP>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       (int)S::kSmem);
+        auto* k = k_conv3x3<CIN, NPAD, TW, TH, STAGES, LD, EP>;
+        attrErr = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)S::kSmem);
         int occ = 1;
         if (attrErr == cudaSuccess)
-            attrErr = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_conv3x3<CIN, NPAD, R, LD, EP>, 128, S::kSmem);
+            attrErr = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k, S::kThreads, S::kSmem);
         perSm = std::max(1, std::min<int>(occ, 512 / (int)S::kTmem));
     });
     if (attrErr != cudaSuccess) return cuda_fail(attrErr, "conv3x3 attributes");
-    const long long tiles = (long long)a.n * ((a.h + R - 1) / R) * (a.w / kTileX);
+    const long long tiles = (long long)a.n * ((a.h + TH - 1) / TH) * ((a.w + TW - 1) / TW);
     if (tiles == 0) return I360B_SUCCESS;
-    k_conv3x3<CIN, NPAD, R, LD, EP><<<grid_for(tiles, perSm), 128, S::kSmem, s>>>(a);
+    CUtensorMap tm;
+    I360B_TRY(make_input_map(&tm, a.x, LD == LD_CONCAT ? a.cs : CIN, a.n, a.h, a.w, TW + 2, TH + 2));
+    k_conv3x3<CIN, NPAD, TW, TH, STAGES, LD, EP><<<grid_for(tiles, perSm), S::kThreads, S::kSmem, s>>>(tm, a);
     return check_launch("conv3x3 kernel");
 }
 
-// The (cin, npad) shapes the network uses, forward and backward.
+// The (cin, npad) shapes the network uses, forward and backward, with their
+// tile shape and ring depth.
 int dispatch_conv(int cin, int npad, int loader, int ep, const ConvArgs& a, cudaStream_t s)
 {
-#define I360B_CONV(CI, NP, R, LD, EP_)                                        \
-    if (cin == CI && npad == NP && loader == LD && ep == EP_) return run_conv<CI, NP, R, LD, EP_>(a, s);
+#define I360B_CONV(CI, NP, TW, TH, ST, LD, EP_)                \
+    if (cin == CI && npad == NP && loader == LD && ep == EP_) \
+        return run_conv<CI, NP, TW, TH, ST, LD, EP_>(a, s);
     // forward
-    I360B_CONV(16, 32, 4, LD_PLAIN, EP_RELU)
-    I360B_CONV(32, 32, 2, LD_PLAIN, EP_RELU)
-    I360B_CONV(32, 64, 2, LD_PLAIN, EP_RELU)
-    I360B_CONV(64, 64, 2, LD_PLAIN, EP_RELU)
-    I360B_CONV(96, 32, 1, LD_CONCAT, EP_RELU)
-    I360B_CONV(32, 16, 4, LD_PLAIN, EP_LOGITS)
-    I360B_CONV(32, 16, 4, LD_PLAIN, EP_COMPOSITE)
+    I360B_CONV(16, 32, 32, 32, 3, LD_PLAIN, EP_RELU)
+    I360B_CONV(32, 32, 16, 32, 3, LD_PLAIN, EP_RELU)
+    I360B_CONV(32, 64, 16, 32, 3, LD_PLAIN, EP_RELU)
+    I360B_CONV(64, 64, 16, 16, 3, LD_PLAIN, EP_RELU)
+    I360B_CONV(96, 32, 16, 16, 2, LD_CONCAT, EP_RELU)
+    I360B_CONV(32, 16, 32, 32, 2, LD_PLAIN, EP_LOGITS)
+    I360B_CONV(32, 16, 32, 32, 2, LD_PLAIN, EP_COMPOSITE)
     // backward data
-    I360B_CONV(16, 32, 4, LD_PLAIN, EP_MASK)
-    I360B_CONV(32, 32, 2, LD_PLAIN, EP_MASK)
-    I360B_CONV(32, 96, 2, LD_PLAIN, EP_RAW)
-    I360B_CONV(64, 64, 2, LD_PLAIN, EP_MASK)
-    I360B_CONV(64, 32, 2, LD_PLAIN, EP_RAW)
+    I360B_CONV(16, 32, 32, 32, 3, LD_PLAIN, EP_MASK)
+    I360B_CONV(32, 32, 16, 32, 3, LD_PLAIN, EP_MASK)
+    I360B_CONV(32, 96, 16, 16, 3, LD_PLAIN, EP_RAW)
+    I360B_CONV(64, 64, 16, 16, 3, LD_PLAIN, EP_MASK)
+    I360B_CONV(64, 32, 16, 16, 3, LD_PLAIN, EP_RAW)
 #undef I360B_CONV
     return fail(I360B_NOT_SUPPORTED, "conv3x3: no kernel for cin=%d cout=%d loader=%d epilogue=%d", cin, npad, loader,
                 ep);
@@ -1538,7 +1642,7 @@ extern "C" int i360b_conv3x3_forward(const void* dX, const void* dU, int skipCha
     if (!initialized()) return fail(I360B_CUDA_ERROR, "Not initialized.");
     I360B_TRY(ensure_ready());
     if (!dX || !dWeights || !dOut || (skipChannels > 0 && !dU)) return fail(I360B_INVALID_PARAM, "Null pointer argument.");
-    if (n <= 0 || h <= 0 || w <= 0 || w % kTileX != 0) return fail(I360B_INVALID_PARAM, "Invalid dimensions.");
+    if (n <= 0 || h <= 0 || w <= 0) return fail(I360B_INVALID_PARAM, "Invalid dimensions.");
     if ((epilogue == EP_RELU || epilogue == EP_LOGITS) && !dBias) return fail(I360B_INVALID_PARAM, "Null pointer argument.");
     if (epilogue == EP_MASK && !dAct) return fail(I360B_INVALID_PARAM, "Null pointer argument.");
     if (epilogue < EP_RELU || epilogue > EP_RAW) return fail(I360B_INVALID_PARAM, "unknown epilogue %d", epilogue);

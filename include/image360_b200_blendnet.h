@@ -139,7 +139,7 @@ I360B_API int i360b_render_plan_windows(i360b_render_plan* plan, int maxWindows,
 I360B_API int i360b_render_plan_tile_items(i360b_render_plan* plan, int tile, int maxItems,
                                            const unsigned short** dImages, int* boxes, int* numItems);
 
-/* ---- convolution primitives (NHWC bf16, width a multiple of 128) --------- */
+/* ---- convolution primitives (NHWC bf16) --------------------------------- */
 
 /* Epilogues of i360b_conv3x3_forward. */
 enum
@@ -155,12 +155,13 @@ enum
  * ([n][h][w][skipChannels]) and the nearest 2x upsample of dU
  * ([n][h/2][w/2][cin - skipChannels]).  dWeights is bf16 [cout][3][3][cin],
  * dBias fp32 [cout].  Supported (cin, cout): the layer shapes of the blend
- * network and of its backward pass. */
+ * network and of its backward pass.  Tensors 16-byte aligned. */
 I360B_API int i360b_conv3x3_forward(const void* dX, const void* dU, int skipChannels, int n, int h, int w, int cin,
                                     int cout, const void* dWeights, const float* dBias, int epilogue,
                                     const void* dAct, void* dOut, void* stream);
 /* Weight gradient of that convolution: dGradW[cout][3][3][cin] (fp32,
- * overwritten) = sum over pixels of dGrad[p][co] * input[p + tap][ci]. */
+ * overwritten) = sum over pixels of dGrad[p][co] * input[p + tap][ci];
+ * width a multiple of 128. */
 I360B_API int i360b_conv3x3_wgrad(const void* dX, const void* dU, int skipChannels, const void* dGrad, int n, int h,
                                   int w, int cin, int cout, float* dGradW, void* stream);
 
