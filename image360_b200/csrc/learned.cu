@@ -79,9 +79,13 @@ struct ConvArgs
 // Tile geometry of the 3x3 convolution: TW x TH output pixels per tile, split
 // into M blocks of 8 columns x 16 rows; the input halo of (TW+2) x (TH+2)
 // pixels is kept per 8-channel chunk with row pitch kP = TW+2 pixels.
-template <int CIN, int NPAD, int TW, int TH, int STAGES, int LD>
+template <int CIN, int NPAD, int TW, int TH, int STAGES, int LD, int EW = 4>
 struct ConvShape
 {
+    // Roles by warp: [0, EW) epilogue, EW producer, EW + 1 MMA, then (for a
+    // concatenated input) 4 upsampling warps.
+    static constexpr int kEpiWarps = EW;
+    static constexpr int kProducerWarp = EW, kMmaWarp = EW + 1, kExpandWarp = EW + 2;
     static constexpr int kC8 = CIN / 8;
     static constexpr int kP = TW + 2;
     static constexpr int kHaloPx = (TW + 2) * (TH + 2);
@@ -93,15 +97,23 @@ struct ConvShape
     static constexpr uint32_t kSlotCols = kMB * NPAD;
     static constexpr uint32_t kTmem = tc::tmem_cols(2 * kSlotCols);
     static constexpr int kKSteps = 9 * CIN / 16;
-    static constexpr int kThreads = LD == LD_CONCAT ? 320 : 192;
-    static constexpr uint32_t kBars = (2 * STAGES + 4) * 8 + 16;
-    static constexpr uint32_t kSmem = 128 + kW + STAGES * kStage + kBars;
+    static constexpr int kThreads = 32 * (EW + 2) + (LD == LD_CONCAT ? 128 : 0);
+    // Concatenated input: the half-resolution box behind a tile's halo,
+    // (TW/2+2) x (TH/2+2) pixels per 8-channel chunk, per ring stage.
+    static constexpr int kPh = TW / 2 + 2;
+    static constexpr int kHalfPx = (TW / 2 + 2) * (TH / 2 + 2);
+    static constexpr uint32_t kHalfBox = kHalfPx * 16;
+    static constexpr uint32_t kHalfChunk = (kHalfBox + 127) / 128 * 128;
+    static constexpr uint32_t kHalfStage = LD == LD_CONCAT ? kC8 * kHalfChunk : 0;  // upper bound on chunks
+    static constexpr uint32_t kBars = (3 * STAGES + 4) * 8 + 16;
+    static constexpr uint32_t kSmem = 128 + kW + STAGES * (kStage + kHalfStage) + kBars;
     static_assert(CIN % 16 == 0 && NPAD % 16 == 0 && NPAD >= 16 && NPAD <= 256, "MMA shape");
     static_assert(TW % 8 == 0 && TH % 16 == 0 && TW + 2 <= 256 && TH + 2 <= 256, "tile shape");
     static_assert(2 * kSlotCols <= 512, "TMEM capacity");
     static_assert(kW % 128 == 0, "ring alignment");
     static_assert(kChunk / 16 < (1u << 14) && kP < (1 << 14), "descriptor offset range");
     static_assert(kSmem <= 227u * 1024u, "shared memory");
+    static_assert(EW == 4 || (EW == 8 && kMB % 2 == 0), "epilogue warps split the M blocks in two");
 };
 
 __device__ __forceinline__ uint4 pack8_bf16(const float* v)
@@ -199,32 +211,36 @@ __device__ __forceinline__ void composite_pixel(const i360b_blend_job& J, int y,
 // 8-channel halves of a K step are one chunk apart (LBO).
 //
 // Roles:
-//   warp 4 lane 0  TMA producer: one 4-D box (8 channels x (TW+2) x (TH+2))
+//   warp EW lane 0 TMA producer: one 4-D box (8 channels x (TW+2) x (TH+2))
 //                  per chunk into a STAGES-deep ring, zero fill outside the
 //                  image;
-//   warps 6-9      (concatenated input only) cp.async producers of the
-//                  nearest-upsampled half-resolution channels;
-//   warp 5 lane 0  MMA issuer: MB x 9 CIN/16 tcgen05.mma per tile into one of
+//   warps EW+2..   (concatenated input only) expand the TMA-loaded
+//                  half-resolution box into the nearest-upsampled channels
+//                  of the halo (shared memory to shared memory);
+//   warp EW+1 lane 0 MMA issuer: MB x 9 CIN/16 tcgen05.mma per tile into one of
 //                  two TMEM accumulators; commits free the ring stage and
 //                  publish the accumulator;
-//   warps 0-3      epilogue: TMEM lanes 32w..32w+31 (rows 4w..4w+3 of each M
-//                  block) -> bias/ReLU, mask, raw or blend head -> global.
+//   warps 0..EW-1  epilogue (EW = 4 or 8): TMEM lanes 32q..32q+31, q = w % 4
+//                  (rows 4q..4q+3 of each M block) -> bias/ReLU, mask, raw or
+//                  blend head -> global.
 // Every wait is bounded; a timeout sets the error flag and the CTA winds
 // down after its loads have landed.
 // ---------------------------------------------------------------------------
-template <int CIN, int NPAD, int TW, int TH, int STAGES, int LD, int EP>
-__global__ void __launch_bounds__(ConvShape<CIN, NPAD, TW, TH, STAGES, LD>::kThreads, 1)
-    k_conv3x3(const __grid_constant__ CUtensorMap tmap, ConvArgs a)
+template <int CIN, int NPAD, int TW, int TH, int STAGES, int LD, int EP, int EW>
+__global__ void __launch_bounds__(ConvShape<CIN, NPAD, TW, TH, STAGES, LD, EW>::kThreads, 1)
+    k_conv3x3(const __grid_constant__ CUtensorMap tmap, const __grid_constant__ CUtensorMap tmapHalf, ConvArgs a)
 {
-    using S = ConvShape<CIN, NPAD, TW, TH, STAGES, LD>;
+    using S = ConvShape<CIN, NPAD, TW, TH, STAGES, LD, EW>;
     extern __shared__ unsigned char smemRaw[];
     unsigned char* smem =
         reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(smemRaw) + 127) & ~uintptr_t(127));
     unsigned char* wsm = smem;
     unsigned char* ring = smem + S::kW;
-    uint64_t* full = reinterpret_cast<uint64_t*>(ring + STAGES * S::kStage);
+    unsigned char* halfRing = ring + STAGES * S::kStage;
+    uint64_t* full = reinterpret_cast<uint64_t*>(halfRing + STAGES * S::kHalfStage);
     uint64_t* empty = full + STAGES;
-    uint64_t* accFull = empty + STAGES;
+    uint64_t* halfFull = empty + STAGES;
+    uint64_t* accFull = halfFull + STAGES;
     uint64_t* accEmpty = accFull + 2;
     uint32_t* tmemSlot = reinterpret_cast<uint32_t*>(accEmpty + 2);
 
@@ -249,11 +265,12 @@ __global__ void __launch_bounds__(ConvShape<CIN, NPAD, TW, TH, STAGES, LD>::kThr
         {
             tc::mbar_init(&full[s], LD == LD_CONCAT ? 1 + 128 : 1);
             tc::mbar_init(&empty[s], 1);
+            tc::mbar_init(&halfFull[s], 1);
         }
         for (int k = 0; k < 2; ++k)
         {
             tc::mbar_init(&accFull[k], 1);
-            tc::mbar_init(&accEmpty[k], 4);
+            tc::mbar_init(&accEmpty[k], EW);
         }
         tc::fence_mbar_init();
     }
@@ -274,7 +291,7 @@ __global__ void __launch_bounds__(ConvShape<CIN, NPAD, TW, TH, STAGES, LD>::kThr
     const uint32_t tmem = *tmemSlot;
     bool ok = true;
 
-    if (warp == 4)
+    if (warp == S::kProducerWarp)
     {
         if (lane == 0)
         {
@@ -290,6 +307,16 @@ __global__ void __launch_bounds__(ConvShape<CIN, NPAD, TW, TH, STAGES, LD>::kThr
                 int img, y0, x0;
                 coord(i, img, y0, x0);
                 unsigned char* st = ring + s * S::kStage;
+                if (LD == LD_CONCAT)
+                {
+                    // half-resolution rows/columns y0/2 - 1 .. (y0 + TH)/2 (x0, y0 even)
+                    unsigned char* hs = halfRing + s * S::kHalfStage;
+                    const int nu8 = S::kC8 - tmaChunks;
+                    tc::mbar_arrive_expect_tx(&halfFull[s], (uint32_t)nu8 * S::kHalfBox);
+                    for (int c = 0; c < nu8; ++c)
+                        tc::tma_load_4d(hs + c * S::kHalfChunk, &tmapHalf, c * 8, (x0 >> 1) - 1, (y0 >> 1) - 1, img,
+                                        &halfFull[s]);
+                }
                 tc::mbar_arrive_expect_tx(&full[s], (uint32_t)tmaChunks * S::kBox);
                 for (int c = 0; c < tmaChunks; ++c)
                     tc::tma_load_4d(st + c * S::kChunk, &tmap, c * 8, x0 - 1, y0 - 1, img, &full[s]);
@@ -297,46 +324,49 @@ __global__ void __launch_bounds__(ConvShape<CIN, NPAD, TW, TH, STAGES, LD>::kThr
             }
             // The last loads must land before the CTA may exit.
             for (int j = max(0, issued - STAGES); j < issued; ++j)
+            {
                 if (!tc::mbar_wait(&full[j % STAGES], (j / STAGES) & 1, kWaitSpins)) ok = false;
+                if (LD == LD_CONCAT && !tc::mbar_wait(&halfFull[j % STAGES], (j / STAGES) & 1, kWaitSpins)) ok = false;
+            }
         }
     }
-    else if (LD == LD_CONCAT && warp >= 6)
+    else if (LD == LD_CONCAT && warp >= S::kExpandWarp)
     {
-        const int ptid = tid - 192;
-        const int sc8 = a.cs >> 3, nu8 = S::kC8 - sc8, uc = CIN - a.cs;
-        const int hh = a.h >> 1, hw = a.w >> 1;
+        // Nearest 2x upsample of the half-resolution box into the halo chunks
+        // after the skip channels: halo pixel (hx, hy) reads box pixel
+        // ((hx - 1) >> 1) + 1, ((hy - 1) >> 1) + 1 (tile origin even).
+        const int ptid = tid - 32 * S::kExpandWarp;
+        const int sc8 = a.cs >> 3, nu8 = S::kC8 - sc8;
         for (int i = 0; i < myTiles; ++i)
         {
             const int s = i % STAGES;
-            if (!tc::mbar_wait(&empty[s], ((i / STAGES) & 1) ^ 1, kWaitSpins))
+            bool got = tc::mbar_wait(&halfFull[s], (i / STAGES) & 1, kWaitSpins);
+            if (!got)
             {
                 ok = false;
                 break;
             }
-            int img, y0, x0;
-            coord(i, img, y0, x0);
+            const unsigned char* hs = halfRing + s * S::kHalfStage;
             unsigned char* st = ring + s * S::kStage;
             const int nq = nu8 * S::kHaloPx;
             for (int q = ptid; q < nq; q += 128)
             {
-                const int cu = q % nu8, px = q / nu8;
-                const int hx = px % S::kP, hy = px / S::kP;
-                const int yy = y0 - 1 + hy, xx = x0 - 1 + hx;
-                const bool in = yy >= 0 && yy < a.h && xx >= 0 && xx < a.w;
-                const bf16* src =
-                    in ? a.u + ((((size_t)img * hh + (yy >> 1)) * hw + (xx >> 1)) * uc + cu * 8) : a.u;
-                tc::cp_async16(st + (sc8 + cu) * S::kChunk + px * 16, src, in ? 16 : 0);
+                const int cu = q / S::kHaloPx, px = q - cu * S::kHaloPx;
+                const int hy = px / S::kP, hx = px - hy * S::kP;
+                const int ly = ((hy - 1) >> 1) + 1, lx = ((hx - 1) >> 1) + 1;
+                *reinterpret_cast<uint4*>(st + (sc8 + cu) * S::kChunk + px * 16) =
+                    *reinterpret_cast<const uint4*>(hs + cu * S::kHalfChunk + (ly * S::kPh + lx) * 16);
             }
-            tc::cp_async_arrive_noinc(&full[s]);
+            tc::fence_proxy_async();  // generic smem writes -> tensor core
+            tc::mbar_arrive(&full[s]);
         }
-        tc::cp_async_wait<0>();
     }
-    else if (warp == 5)
+    else if (warp == S::kMmaWarp)
     {
         if (lane == 0)
         {
             constexpr uint32_t idesc = tc::idesc_bf16_f32(128, NPAD);
-            const uint32_t wb = tc::smem_u32(wsm);
+            const uint64_t bBase = tc::smem_desc(tc::smem_u32(wsm), NPAD * 16, 128);
             for (int i = 0; i < myTiles; ++i)
             {
                 const int s = i % STAGES, acc = i & 1;
@@ -346,21 +376,23 @@ __global__ void __launch_bounds__(ConvShape<CIN, NPAD, TW, TH, STAGES, LD>::kThr
                     ok = false;
                     break;
                 }
-                if (LD == LD_CONCAT) tc::fence_proxy_async();  // cp.async data -> tensor core
                 tc::fence_after_sync();
-                const uint32_t hb = tc::smem_u32(ring + s * S::kStage);
+                // Descriptors differ only in their start-address field: add
+                // the (compile-time) offset in 16-byte units to a base.
+                const uint64_t aBase = tc::smem_desc(tc::smem_u32(ring + s * S::kStage), S::kChunk, S::kP * 16);
+#pragma unroll
                 for (int b = 0; b < S::kMB; ++b)
                 {
                     const int bx = b % S::kBX, by = b / S::kBX;
                     const uint32_t d = tmem + acc * S::kSlotCols + b * NPAD;
-#pragma unroll 4
+#pragma unroll
                     for (int ks = 0; ks < S::kKSteps; ++ks)
                     {
                         const int k0 = ks * 16, tap = k0 / CIN, c8 = (k0 % CIN) >> 3;
                         const int dy = tap / 3, dx = tap % 3;
-                        const uint32_t aAddr = hb + c8 * S::kChunk + ((by * 16 + dy) * S::kP + bx * 8 + dx) * 16;
-                        tc::mma_bf16(d, tc::smem_desc(aAddr, S::kChunk, S::kP * 16),
-                                     tc::smem_desc(wb + 2 * ks * (NPAD * 16), NPAD * 16, 128), idesc, ks > 0 ? 1u : 0u);
+                        const uint32_t aOff = (c8 * S::kChunk + ((by * 16 + dy) * S::kP + bx * 8 + dx) * 16) >> 4;
+                        const uint32_t bOff = (2 * ks * (NPAD * 16)) >> 4;
+                        tc::mma_bf16(d, aBase + aOff, bBase + bOff, idesc, ks > 0 ? 1u : 0u);
                     }
                 }
                 tc::mma_commit(&empty[s]);
@@ -368,8 +400,11 @@ __global__ void __launch_bounds__(ConvShape<CIN, NPAD, TW, TH, STAGES, LD>::kThr
             }
         }
     }
-    else if (warp < 4)
+    else if (warp < EW)
     {
+        // Warp w reads TMEM lane quadrant w % 4; with 8 epilogue warps the
+        // two warps of a quadrant take alternate M blocks.
+        const int quad = warp & 3, half = warp >> 2;
         for (int i = 0; i < myTiles; ++i)
         {
             const int acc = i & 1;
@@ -383,11 +418,11 @@ __global__ void __launch_bounds__(ConvShape<CIN, NPAD, TW, TH, STAGES, LD>::kThr
             tc::fence_after_sync();
             int img, y0, x0;
             coord(i, img, y0, x0);
-            const uint32_t base = tmem + ((uint32_t)(warp * 32) << 16) + acc * S::kSlotCols;
-            for (int b = 0; b < S::kMB; ++b)
+            const uint32_t base = tmem + ((uint32_t)(quad * 32) << 16) + acc * S::kSlotCols;
+            for (int b = (EW == 8 ? half : 0); b < S::kMB; b += EW / 4)
             {
                 const int bx = b % S::kBX, by = b / S::kBX;
-                const int y = y0 + by * 16 + warp * 4 + (lane >> 3);
+                const int y = y0 + by * 16 + quad * 4 + (lane >> 3);
                 const int x = x0 + bx * 8 + (lane & 7);
                 const bool valid = y < a.h && x < a.w;
                 const size_t pix = ((size_t)img * a.h + y) * a.w + x;
@@ -947,15 +982,15 @@ int make_input_map(CUtensorMap* m, const bf16* base, int c, int n, int h, int w,
     return I360B_SUCCESS;
 }
 
-template <int CIN, int NPAD, int TW, int TH, int STAGES, int LD, int EP>
+template <int CIN, int NPAD, int TW, int TH, int STAGES, int LD, int EP, int EW>
 int run_conv(const ConvArgs& a, cudaStream_t s)
 {
-    using S = ConvShape<CIN, NPAD, TW, TH, STAGES, LD>;
+    using S = ConvShape<CIN, NPAD, TW, TH, STAGES, LD, EW>;
     static std::once_flag once;
     static int perSm = 1;
     static cudaError_t attrErr = cudaSuccess;
     std::call_once(once, [] {
-        auto* k = k_conv3x3<CIN, NPAD, TW, TH, STAGES, LD, EP>;
+        auto* k = k_conv3x3<CIN, NPAD, TW, TH, STAGES, LD, EP, EW>;
         attrErr = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)S::kSmem);
         int occ = 1;
         if (attrErr == cudaSuccess)
@@ -965,9 +1000,17 @@ int run_conv(const ConvArgs& a, cudaStream_t s)
     if (attrErr != cudaSuccess) return cuda_fail(attrErr, "conv3x3 attributes");
     const long long tiles = (long long)a.n * ((a.h + TH - 1) / TH) * ((a.w + TW - 1) / TW);
     if (tiles == 0) return I360B_SUCCESS;
-    CUtensorMap tm;
+    CUtensorMap tm, th;
     I360B_TRY(make_input_map(&tm, a.x, LD == LD_CONCAT ? a.cs : CIN, a.n, a.h, a.w, TW + 2, TH + 2));
-    k_conv3x3<CIN, NPAD, TW, TH, STAGES, LD, EP><<<grid_for(tiles, perSm), S::kThreads, S::kSmem, s>>>(tm, a);
+    if (LD == LD_CONCAT)
+    {
+        if (a.cs % 8 || a.h % 2 || a.w % 2 || CIN - a.cs > 8 * S::kC8)
+            return fail(I360B_INVALID_PARAM, "concatenated conv3x3 input: even sizes and 8-channel groups");
+        I360B_TRY(make_input_map(&th, a.u, CIN - a.cs, a.n, a.h / 2, a.w / 2, TW / 2 + 2, TH / 2 + 2));
+    }
+    else
+        th = tm;
+    k_conv3x3<CIN, NPAD, TW, TH, STAGES, LD, EP, EW><<<grid_for(tiles, perSm), S::kThreads, S::kSmem, s>>>(tm, th, a);
     return check_launch("conv3x3 kernel");
 }
 
@@ -975,23 +1018,23 @@ int run_conv(const ConvArgs& a, cudaStream_t s)
 // tile shape and ring depth.
 int dispatch_conv(int cin, int npad, int loader, int ep, const ConvArgs& a, cudaStream_t s)
 {
-#define I360B_CONV(CI, NP, TW, TH, ST, LD, EP_)                \
+#define I360B_CONV(CI, NP, TW, TH, ST, LD, EP_, EW)             \
     if (cin == CI && npad == NP && loader == LD && ep == EP_) \
-        return run_conv<CI, NP, TW, TH, ST, LD, EP_>(a, s);
+        return run_conv<CI, NP, TW, TH, ST, LD, EP_, EW>(a, s);
     // forward
-    I360B_CONV(16, 32, 32, 32, 3, LD_PLAIN, EP_RELU)
-    I360B_CONV(32, 32, 16, 32, 3, LD_PLAIN, EP_RELU)
-    I360B_CONV(32, 64, 16, 32, 3, LD_PLAIN, EP_RELU)
-    I360B_CONV(64, 64, 16, 16, 3, LD_PLAIN, EP_RELU)
-    I360B_CONV(96, 32, 16, 16, 2, LD_CONCAT, EP_RELU)
-    I360B_CONV(32, 16, 32, 32, 2, LD_PLAIN, EP_LOGITS)
-    I360B_CONV(32, 16, 32, 32, 2, LD_PLAIN, EP_COMPOSITE)
+    I360B_CONV(16, 32, 32, 32, 3, LD_PLAIN, EP_RELU, 8)
+    I360B_CONV(32, 32, 16, 32, 3, LD_PLAIN, EP_RELU, 8)
+    I360B_CONV(32, 64, 16, 32, 3, LD_PLAIN, EP_RELU, 8)
+    I360B_CONV(64, 64, 16, 16, 3, LD_PLAIN, EP_RELU, 8)
+    I360B_CONV(96, 32, 16, 16, 2, LD_CONCAT, EP_RELU, 8)
+    I360B_CONV(32, 16, 32, 32, 2, LD_PLAIN, EP_LOGITS, 8)
+    I360B_CONV(32, 16, 32, 32, 2, LD_PLAIN, EP_COMPOSITE, 8)
     // backward data
-    I360B_CONV(16, 32, 32, 32, 3, LD_PLAIN, EP_MASK)
-    I360B_CONV(32, 32, 16, 32, 3, LD_PLAIN, EP_MASK)
-    I360B_CONV(32, 96, 16, 16, 3, LD_PLAIN, EP_RAW)
-    I360B_CONV(64, 64, 16, 16, 3, LD_PLAIN, EP_MASK)
-    I360B_CONV(64, 32, 16, 16, 3, LD_PLAIN, EP_RAW)
+    I360B_CONV(16, 32, 32, 32, 3, LD_PLAIN, EP_MASK, 8)
+    I360B_CONV(32, 32, 16, 32, 3, LD_PLAIN, EP_MASK, 8)
+    I360B_CONV(32, 96, 16, 16, 3, LD_PLAIN, EP_RAW, 8)
+    I360B_CONV(64, 64, 16, 16, 3, LD_PLAIN, EP_MASK, 8)
+    I360B_CONV(64, 32, 16, 16, 3, LD_PLAIN, EP_RAW, 8)
 #undef I360B_CONV
     return fail(I360B_NOT_SUPPORTED, "conv3x3: no kernel for cin=%d cout=%d loader=%d epilogue=%d", cin, npad, loader,
                 ep);
