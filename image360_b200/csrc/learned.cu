@@ -106,7 +106,8 @@ struct ConvShape
     static constexpr uint32_t kHalfChunk = (kHalfBox + 127) / 128 * 128;
     static constexpr uint32_t kHalfStage = LD == LD_CONCAT ? kC8 * kHalfChunk : 0;  // upper bound on chunks
     static constexpr uint32_t kBars = (3 * STAGES + 4) * 8 + 16;
-    static constexpr uint32_t kSmem = 128 + kW + STAGES * (kStage + kHalfStage) + kBars;
+    static constexpr uint32_t kBias = NPAD * 4;
+    static constexpr uint32_t kSmem = 128 + kW + STAGES * (kStage + kHalfStage) + kBars + kBias;
     static_assert(CIN % 16 == 0 && NPAD % 16 == 0 && NPAD >= 16 && NPAD <= 256, "MMA shape");
     static_assert(TW % 8 == 0 && TH % 16 == 0 && TW + 2 <= 256 && TH + 2 <= 256, "tile shape");
     static_assert(2 * kSlotCols <= 512, "TMEM capacity");
@@ -156,25 +157,34 @@ __device__ __forceinline__ const bf16* input_chunk(const bf16* x, const bf16* u,
 }
 
 // Softmax-weighted composite of a pixel's covered layers (the network head).
-__device__ __forceinline__ void composite_pixel(const i360b_blend_job& J, int y, int x, const float* l, float* outDN,
-                                                float* wts, float (*v)[3], bool* cov, int& nCov)
+// The pixel's layer values (0 where a slot is absent).
+__device__ __forceinline__ void load_slots(const i360b_blend_job& J, int y, int x, float (*v)[3])
+{
+#pragma unroll
+    for (int i = 0; i < kSlots; ++i)
+    {
+        v[i][0] = v[i][1] = v[i][2] = 0.0f;
+        if (J.slot[i])
+        {
+            const unsigned short* p = J.slot[i] + (long long)y * J.rowStride + (long long)x * J.pixStride;
+            v[i][0] = __ldg(p);
+            v[i][1] = __ldg(p + 1);
+            v[i][2] = __ldg(p + 2);
+        }
+    }
+}
+
+// Softmax over the covered layers (value not (0,0,0)) of the logits, and the
+// weighted sum of the layers; v from load_slots.
+__device__ __forceinline__ void blend_slots(const float* l, const float (*v)[3], float* outDN, float* wts, bool* cov,
+                                            int& nCov)
 {
     float m = -INFINITY;
     nCov = 0;
 #pragma unroll
     for (int i = 0; i < kSlots; ++i)
     {
-        cov[i] = false;
-        v[i][0] = v[i][1] = v[i][2] = 0.0f;
-        if (J.slot[i])
-        {
-            const unsigned short* p = J.slot[i] + (long long)y * J.rowStride + (long long)x * J.pixStride;
-            const unsigned short r = p[0], g = p[1], b = p[2];
-            cov[i] = (r | g | b) != 0;
-            v[i][0] = r;
-            v[i][1] = g;
-            v[i][2] = b;
-        }
+        cov[i] = v[i][0] != 0.0f || v[i][1] != 0.0f || v[i][2] != 0.0f;
         if (cov[i])
         {
             m = fmaxf(m, l[i]);
@@ -198,6 +208,13 @@ __device__ __forceinline__ void composite_pixel(const i360b_blend_job& J, int y,
         outDN[1] += wts[i] * v[i][1];
         outDN[2] += wts[i] * v[i][2];
     }
+}
+
+__device__ __forceinline__ void composite_pixel(const i360b_blend_job& J, int y, int x, const float* l, float* outDN,
+                                                float* wts, float (*v)[3], bool* cov, int& nCov)
+{
+    load_slots(J, y, x, v);
+    blend_slots(l, v, outDN, wts, cov, nCov);
 }
 
 // ---------------------------------------------------------------------------
@@ -243,6 +260,7 @@ __global__ void __launch_bounds__(ConvShape<CIN, NPAD, TW, TH, STAGES, LD, EW>::
     uint64_t* accFull = halfFull + STAGES;
     uint64_t* accEmpty = accFull + 2;
     uint32_t* tmemSlot = reinterpret_cast<uint32_t*>(accEmpty + 2);
+    float* sBias = reinterpret_cast<float*>(tmemSlot + 4);
 
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const int tilesX = (a.w + TW - 1) / TW, tilesY = (a.h + TH - 1) / TH;
@@ -282,6 +300,7 @@ __global__ void __launch_bounds__(ConvShape<CIN, NPAD, TW, TH, STAGES, LD, EW>::
             tc::cp_async16(wsm + k8 * (NPAD * 16) + n * 16, a.wt + (size_t)n * 9 * CIN + k8 * 8, 16);
         }
         tc::cp_async_commit();
+        for (int c = tid; c < NPAD; c += blockDim.x) sBias[c] = a.bias ? a.bias[c] : 0.0f;
         tc::cp_async_wait<0>();
         tc::fence_proxy_async();
     }
@@ -426,53 +445,71 @@ __global__ void __launch_bounds__(ConvShape<CIN, NPAD, TW, TH, STAGES, LD, EW>::
                 const int x = x0 + bx * 8 + (lane & 7);
                 const bool valid = y < a.h && x < a.w;
                 const size_t pix = ((size_t)img * a.h + y) * a.w + x;
+                // Global inputs of the epilogue first, so their latency
+                // overlaps the TMEM loads.
+                float vv[4][3];
+                bool inJob = false;
+                if (EP == EP_COMPOSITE)
+                {
+                    const i360b_blend_job& J = a.jobs[img];
+                    inJob = valid && x < J.width && y < J.height;
+                    if (inJob) load_slots(J, y, x, vv);
+                }
+                uint4 mk[EP == EP_MASK ? NPAD / 8 : 1];
+                if (EP == EP_MASK && valid)
+                {
+                    const uint4* ap = reinterpret_cast<const uint4*>(a.act + pix * NPAD);
+#pragma unroll
+                    for (int q = 0; q < NPAD / 8; ++q) mk[q] = ap[q];
+                }
+                constexpr int kCols = (EP == EP_LOGITS || EP == EP_COMPOSITE) ? 16 : NPAD;
+                uint32_t r[kCols];
+#pragma unroll
+                for (int cb = 0; cb < kCols / 16; ++cb) tc::tmem_ld16_nowait(base + b * NPAD + cb * 16, r + cb * 16);
+                tc::tmem_wait_ld();
+#pragma unroll
+                for (int cb = 0; cb < kCols / 16; ++cb) tc::tmem_reg_fence16(r + cb * 16);
+                if (!valid) continue;
                 if (EP == EP_LOGITS || EP == EP_COMPOSITE)
                 {
-                    float v[16];
-                    tc::tmem_ld16(base + b * NPAD, v);
-                    if (!valid) continue;
                     float l[4];
 #pragma unroll
-                    for (int j = 0; j < 4; ++j) l[j] = v[j] + a.bias[j];
+                    for (int j = 0; j < 4; ++j) l[j] = __uint_as_float(r[j]) + sBias[j];
                     if (EP == EP_LOGITS)
                     {
                         reinterpret_cast<float4*>(a.out)[pix] = make_float4(l[0], l[1], l[2], l[3]);
                     }
-                    else
+                    else if (inJob)
                     {
                         const i360b_blend_job& J = a.jobs[img];
-                        if (x < J.width && y < J.height)
-                        {
-                            float o[3], wts[4], vv[4][3];
-                            bool cov[4];
-                            int nCov;
-                            composite_pixel(J, y, x, l, o, wts, vv, cov, nCov);
-                            unsigned short* q = J.out + (long long)y * J.outRowStride + (long long)x * 3;
+                        float o[3], wts[4];
+                        bool cov[4];
+                        int nCov;
+                        blend_slots(l, vv, o, wts, cov, nCov);
+                        unsigned short* q = J.out + (long long)y * J.outRowStride + (long long)x * 3;
 #pragma unroll
-                            for (int c = 0; c < 3; ++c)
-                                q[c] = (unsigned short)__float2uint_rn(fminf(fmaxf(o[c], 0.0f), 65535.0f));
-                        }
+                        for (int c = 0; c < 3; ++c)
+                            q[c] = (unsigned short)__float2uint_rn(fminf(fmaxf(o[c], 0.0f), 65535.0f));
                     }
                 }
                 else
                 {
-#pragma unroll 1
+#pragma unroll
                     for (int cb = 0; cb < NPAD / 16; ++cb)
                     {
                         float v[16];
-                        tc::tmem_ld16(base + b * NPAD + cb * 16, v);
-                        if (!valid) continue;
+#pragma unroll
+                        for (int j = 0; j < 16; ++j) v[j] = __uint_as_float(r[cb * 16 + j]);
                         if (EP == EP_RELU)
                         {
 #pragma unroll
-                            for (int j = 0; j < 16; ++j) v[j] = fmaxf(v[j] + a.bias[cb * 16 + j], 0.0f);
+                            for (int j = 0; j < 16; ++j) v[j] = fmaxf(v[j] + sBias[cb * 16 + j], 0.0f);
                         }
                         if (EP == EP_MASK)
                         {
-                            const uint4* ap = reinterpret_cast<const uint4*>(a.act + pix * NPAD + cb * 16);
                             float m[16];
-                            unpack8_bf16(ap[0], m);
-                            unpack8_bf16(ap[1], m + 8);
+                            unpack8_bf16(mk[2 * cb], m);
+                            unpack8_bf16(mk[2 * cb + 1], m + 8);
 #pragma unroll
                             for (int j = 0; j < 16; ++j) v[j] = m[j] > 0.0f ? v[j] : 0.0f;
                         }
