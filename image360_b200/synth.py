@@ -207,6 +207,58 @@ def tile_grid(pano_w: int, pano_h: int, tile: int, mats, fw: int, fh: int):
     return tiles
 
 
+C3_SIDES = (512, 768, 1024, 1536, 2048)
+
+
+@dataclass
+class UnevenTiles:
+    """Uneven output tiles, each overlapped by its own placements of frames
+    from a shared pool.  A "placement" is a pool frame with a homography of its
+    own (the same image may be placed on several tiles)."""
+    canvas_w: int
+    canvas_h: int
+    frame_of: np.ndarray    # (n_placements,) pool frame index of each placement
+    to_canvas: np.ndarray   # (n_placements, 3, 3) placement -> canvas
+    tiles: list             # [(x, y, w, h, [placement indices])]
+
+
+def uneven_tiles(n_tiles: int, n_frames: int, frame_w: int, frame_h: int, focal: float, seed: int,
+                 sides=C3_SIDES, k_max: int = 7, jitter_deg: float = 0.5) -> UnevenTiles:
+    """Tiles with width and height drawn uniformly from `sides`, laid out in
+    rows on one canvas; each tile draws K ~ U{1..k_max} distinct pool frames
+    and places each with its centre within +-0.35 of a frame size of the
+    tile centre (so any two placements of a tile overlap by at least 30% of a
+    frame along each axis) and a small roll/pitch/yaw."""
+    rng = np.random.default_rng(seed)
+    K = np.diag([focal, focal, 1.0])
+    Ki = np.linalg.inv(K)
+    j = math.radians(jitter_deg)
+    C = np.array([[1, 0, -frame_w / 2.0], [0, 1, -frame_h / 2.0], [0, 0, 1]])
+    row_w = 8 * max(sides)
+    x = y = row_h = 0
+    tiles, mats, frame_of = [], [], []
+    for _ in range(n_tiles):
+        w, h = int(rng.choice(sides)), int(rng.choice(sides))
+        if x + w > row_w:
+            x, y, row_h = 0, y + row_h, 0
+        k = int(rng.integers(1, k_max + 1))
+        cs = []
+        for f in rng.choice(n_frames, size=min(k, n_frames), replace=False):
+            cx = x + w / 2.0 + rng.uniform(-0.35, 0.35) * frame_w
+            cy = y + h / 2.0 + rng.uniform(-0.35, 0.35) * frame_h
+            R = _rot(rng.uniform(-j, j), rng.uniform(-j, j), rng.uniform(-j, j) * 0.5)
+            P = np.array([[1, 0, cx], [0, 1, cy], [0, 0, 1]])
+            Hm = P @ K @ R @ Ki @ C
+            cs.append(len(mats))
+            mats.append(Hm / Hm[2, 2])
+            frame_of.append(int(f))
+        tiles.append((x, y, w, h, cs))
+        x += w
+        row_h = max(row_h, h)
+    return UnevenTiles(canvas_w=row_w, canvas_h=y + row_h, frame_of=np.array(frame_of, np.int32),
+                       to_canvas=np.stack(mats), tiles=tiles)
+
+
 def make_panorama(cfg: PanoConfig, device="cpu", with_cfa: bool = True) -> Panorama:
     rng = np.random.default_rng(cfg.seed)
     mats, W, H = geometry(cfg, rng)

@@ -105,3 +105,33 @@ def test_launchers_match_host_api(backend, oracle_c):
     d_g = _dev_u16(g)
     assert backend.launch_gain(d_g.data_ptr(), 1001, 1.5) == 0
     assert np.array_equal(_host_u16(d_g), oracle_c.gain(g, 1.5))
+
+
+def test_render_plan_uneven_tiles_exact(backend, oracle_c):
+    """Uneven tiles (sides from the uneven-tile workload's set, scaled) each
+    overlapped by 1-7 placements of frames from a shared pool: the plan renders
+    every tile in one set of launches, bit-exact against the oracle."""
+    torch = _torch()
+    s = 0.05
+    cfg = synth.scaled(synth.C1, s, tile=64)
+    pano = synth.make_panorama(cfg)
+    black, cm, rc, filt = synth.demosaic_params(cfg)
+    pool = _demosaic_frames(backend, pano)
+    host_pool = [_host_u16(d) for d in pool]
+    sides = tuple(max(16, int(v * s)) for v in synth.C3_SIDES)
+    ut = synth.uneven_tiles(40, len(pool), cfg.frame_w, cfg.frame_h, cfg.focal, seed=7, sides=sides)
+    gains = (1.0 / pano.gains[ut.frame_of]).astype(np.float32)
+    frames = [(pool[f].data_ptr(), cfg.frame_w, cfg.frame_h, H, float(g))
+              for f, H, g in zip(ut.frame_of, ut.to_canvas, gains)]
+    outs = [torch.zeros((t[3], t[2], 3), dtype=torch.int16, device="cuda") for t in ut.tiles]
+    tiles = [(x, y, w, h, cs, o.data_ptr()) for (x, y, w, h, cs), o in zip(ut.tiles, outs)]
+    plan = RenderPlan(frames, tiles, 6, COORDS_REFERENCE)
+    assert plan.execute() == ComputeResult.SUCCESS and plan.wait() == ComputeResult.SUCCESS
+    inv = np.stack([synth.inverse_homography_f32(H) for H in ut.to_canvas])
+    _, ref = oracle_c.render_tiles(4, [host_pool[f] for f in ut.frame_of], inv, gains, ut.tiles, 6)
+    ks = [len(t[4]) for t in ut.tiles]
+    assert min(ks) == 1 and max(ks) >= 5
+    assert len({(t[2], t[3]) for t in ut.tiles}) > 5
+    for t, (o, r) in enumerate(zip(outs, ref)):
+        assert np.array_equal(_host_u16(o), r), (t, ut.tiles[t][:4])
+    plan.close()
