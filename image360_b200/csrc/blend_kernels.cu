@@ -1099,8 +1099,17 @@ __global__ void __launch_bounds__(256) k_down0(BlendArgs a, const Unit* __restri
     const int X0 = u.bx * kDnTW, Y0 = u.by * kDnTH;
     const int tid = threadIdx.x;
     const signed char k = (signed char)it.k;
-    for (int idx = tid; idx < HW * kDnSH; idx += 256)
+    // Footprint: every load of this thread is issued before any is used, so
+    // kPer x 2 pixels of gathers are in flight at once.
+    constexpr int kFoot = HW * kDnSH;
+    constexpr int kPer = (kFoot + 255) / 256;
+    unsigned short pv[kPer][2][3];
+    signed char po[kPer][2];
+#pragma unroll
+    for (int m = 0; m < kPer; ++m)
     {
+        const int idx = tid + 256 * m;
+        if (idx >= kFoot) break;
         const int r = idx / HW, cp = idx - r * HW;
         const int gy = min(max(2 * Y0 - 2 + r, 0), sh - 1);
 #pragma unroll
@@ -1109,23 +1118,29 @@ __global__ void __launch_bounds__(256) k_down0(BlendArgs a, const Unit* __restri
             const int gx = min(max(2 * X0 - 2 + 2 * cp + e, 0), sw - 1);
             const size_t p = (size_t)gy * sw + gx;
             const unsigned short* px = it.img + p * 3;
-            const int r0 = __ldg(px), r1 = __ldg(px + 1), r2 = __ldg(px + 2);
-            const int m = (r0 | r1 | r2) ? 1 : 0;
-            const int dwv = (m << 16) | (T.owner[p] == k ? 1 : 0);
-            if (e == 0)
-            {
-                E[0][r][cp] = r0;
-                E[1][r][cp] = r1;
-                E[2][r][cp] = r2;
-                E[3][r][cp] = dwv;
-            }
-            else
-            {
-                O[0][r][cp] = r0;
-                O[1][r][cp] = r1;
-                O[2][r][cp] = r2;
-                O[3][r][cp] = dwv;
-            }
+            pv[m][e][0] = __ldg(px);
+            pv[m][e][1] = __ldg(px + 1);
+            pv[m][e][2] = __ldg(px + 2);
+            po[m][e] = __ldg(T.owner + p);
+        }
+    }
+#pragma unroll
+    for (int m = 0; m < kPer; ++m)
+    {
+        const int idx = tid + 256 * m;
+        if (idx >= kFoot) break;
+        const int r = idx / HW, cp = idx - r * HW;
+#pragma unroll
+        for (int e = 0; e < 2; ++e)
+        {
+            const int r0 = pv[m][e][0], r1 = pv[m][e][1], r2 = pv[m][e][2];
+            const int mk = (r0 | r1 | r2) ? 1 : 0;
+            const int dwv = (mk << 16) | (po[m][e] == k ? 1 : 0);
+            int(*D)[kDnSH][HW] = e == 0 ? E : O;
+            D[0][r][cp] = r0;
+            D[1][r][cp] = r1;
+            D[2][r][cp] = r2;
+            D[3][r][cp] = dwv;
         }
     }
     __syncthreads();
