@@ -1175,7 +1175,7 @@ __global__ void __launch_bounds__(256) k_down0(BlendArgs a, const Unit* __restri
 // Laplacian = G_l - Up(G_l+1) or G_top (SeamBlend.cpp:184-201).
 // Contributors that own no pixel have an all-zero weight pyramid and add
 // exactly +-0, so summing every contributor equals the reference's sum.
-__global__ void __launch_bounds__(256) k_blend_level(BlendArgs a, const Unit* __restrict__ units, int level)
+__global__ void __launch_bounds__(256, 5) k_blend_level(BlendArgs a, const Unit* __restrict__ units, int level)
 {
     __shared__ ItemCache C;
     const Unit u = units[blockIdx.x];
@@ -1253,7 +1253,7 @@ __global__ void __launch_bounds__(256) k_collapse(BlendArgs a, const Unit* __res
 // is 1 for its owner and 0 for every other contributor, so the blended level-0
 // band is exactly the owner's Laplacian img - Up(G1); the output is
 // clamp(that + Up(recon_1)) + 0.5 truncated, and 0 where nobody owns.
-__global__ void __launch_bounds__(256) k_final0(BlendArgs a, const Unit* __restrict__ units)
+__global__ void __launch_bounds__(256, 5) k_final0(BlendArgs a, const Unit* __restrict__ units)
 {
     __shared__ ItemCache C;
     const Unit u = units[blockIdx.x];
