@@ -96,6 +96,8 @@ def load_library(path: str = LIB_PATH):
     L.i360b_render_plan_destroy.argtypes = [vp]
     L.i360b_render_plan_stats.argtypes = [vp, vp, ct.POINTER(RenderStats)]
     L.i360b_render_plan_profile.argtypes = [vp, vp, ct.POINTER(ct.c_float), i]
+    L.i360b_render_plan_autotune.argtypes = [vp, vp, ct.POINTER(ct.c_int), ct.POINTER(ct.c_int),
+                                             ct.POINTER(ct.c_float)]
     L.i360b_render_stage_name.restype = ct.c_char_p
     L.i360b_launch_demosaic.argtypes = [vp, i, i, ct.c_uint16, _f32p, _f32p, ct.c_uint32, vp, vp]
     L.i360b_launch_warp.argtypes = [vp, i, i, vp, i, i, _f32p, i, i, f, vp]
@@ -286,6 +288,15 @@ class RenderPlan:
         if rc != 0:
             raise RuntimeError(self.lib.i360b_get_last_error().decode())
         return {self.lib.i360b_render_stage_name(i).decode(): float(ms[i]) for i in range(10)}
+
+    def autotune(self, stream: int = 0) -> dict:
+        """Times every band height / chamfer ring depth on this plan and keeps
+        the fastest: {"band_rows", "dt_slots", "ms"}."""
+        r, k, ms = ct.c_int(), ct.c_int(), ct.c_float()
+        rc = self.lib.i360b_render_plan_autotune(self._h, stream or None, ct.byref(r), ct.byref(k), ct.byref(ms))
+        if rc != 0:
+            raise RuntimeError(self.lib.i360b_get_last_error().decode())
+        return {"band_rows": r.value, "dt_slots": k.value, "ms": ms.value}
 
     def execute(self, stream: int = 0) -> ComputeResult:
         return ComputeResult(self.lib.i360b_render_plan_execute(self._h, stream or None))

@@ -23,7 +23,7 @@ __device__ __forceinline__ bool cov_bit(const uint32_t* cov, int covWords, int x
 // ---------------------------------------------------------------------------
 // Coverage (SeamBlend.cpp:564-567): covered = any channel != 0, as bits, plus
 // the inclusive bounding box of covered pixels (SeamBlend.cpp:263-280).
-// A CTA owns a band of kBandRows full-width rows of one contributor; each warp
+// A CTA owns a band of a.bandRows full-width rows of one contributor; each warp
 // walks its rows 32 pixels at a time, so one ballot is one coverage word.
 // ---------------------------------------------------------------------------
 struct BoxAcc
@@ -87,9 +87,10 @@ __global__ void __launch_bounds__(256) k_coverage(BlendArgs a, const Unit* __res
     const TileDev& T = a.tiles[it.tile];
     const int W = T.w, H = T.h, lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     BoxAcc box;
-    for (int r = 0; r < kBandRows / 8; ++r)
+    const int rowsPerWarp = a.bandRows >> 3;
+    for (int r = 0; r < rowsPerWarp; ++r)
     {
-        const int y = u.by * kBandRows + warp * (kBandRows / 8) + r;
+        const int y = u.by * a.bandRows + warp * rowsPerWarp + r;
         if (y >= H) break;
         for (int x0 = 0; x0 < W; x0 += 32)
         {
@@ -155,9 +156,10 @@ __global__ void __launch_bounds__(256) k_warp_tiles(BlendArgs a, const Unit* __r
     const int W = T.w, H = T.h, lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     unsigned short* img = const_cast<unsigned short*>(it.img);
     BoxAcc box;
-    for (int r = 0; r < kBandRows / 8; ++r)
+    const int rowsPerWarp = a.bandRows >> 3;
+    for (int r = 0; r < rowsPerWarp; ++r)
     {
-        const int y = u.by * kBandRows + warp * (kBandRows / 8) + r;
+        const int y = u.by * a.bandRows + warp * rowsPerWarp + r;
         if (y >= H) break;
         const float dY = (float)(y + it.offY);
         const bool rowIn = y >= it.vy0 && y <= it.vy1;
@@ -508,8 +510,8 @@ __global__ void __launch_bounds__(256) k_owner(BlendArgs a, const Unit* __restri
     const int K = T.numItems;
     const long long full = (long long)T.w * T.h;
     const float kInf = (float)(T.w + T.h);
-    const long long base = (long long)u.by * kBandRows * T.w;
-    const long long n = min((long long)kBandRows * T.w, full - base);
+    const long long base = (long long)u.by * a.bandRows * T.w;
+    const long long n = min((long long)a.bandRows * T.w, full - base);
     for (long long q = threadIdx.x; q < n; q += blockDim.x)
     {
         const long long p = base + q;
@@ -1185,8 +1187,8 @@ __global__ void __launch_bounds__(256, 5) k_blend_level(BlendArgs a, const Unit*
     const int lw = T.lw[level], lh = T.lh[level];
     const bool top = level == T.bands - 1;
     const int uw = T.lw[level + 1], uh = T.lh[level + 1];
-    const long long base = (long long)u.by * kBandRows * lw;
-    const long long n = min((long long)kBandRows * lw, (long long)lw * lh - base);
+    const long long base = (long long)u.by * a.bandRows * lw;
+    const long long n = min((long long)a.bandRows * lw, (long long)lw * lh - base);
     for (long long q = threadIdx.x; q < n; q += blockDim.x)
     {
         const long long pl = base + q;
@@ -1230,8 +1232,8 @@ __global__ void __launch_bounds__(256) k_collapse(BlendArgs a, const Unit* __res
     const int lw = T.lw[level], lh = T.lh[level];
     const int uw = T.lw[level + 1], uh = T.lh[level + 1];
     const float* r = T.blend + T.loff[level + 1] * 3;
-    const long long base = (long long)u.by * kBandRows * lw;
-    const long long n = min((long long)kBandRows * lw, (long long)lw * lh - base);
+    const long long base = (long long)u.by * a.bandRows * lw;
+    const long long n = min((long long)a.bandRows * lw, (long long)lw * lh - base);
     for (long long q = threadIdx.x; q < n; q += blockDim.x)
     {
         const long long pl = base + q;
@@ -1262,8 +1264,8 @@ __global__ void __launch_bounds__(256, 5) k_final0(BlendArgs a, const Unit* __re
     const int W = T.w, H = T.h;
     const int uw = T.lw[1], uh = T.lh[1];
     const float* rc = T.blend + T.loff[1] * 3;
-    const long long base = (long long)u.by * kBandRows * W;
-    const long long n = min((long long)kBandRows * W, (long long)W * H - base);
+    const long long base = (long long)u.by * a.bandRows * W;
+    const long long n = min((long long)a.bandRows * W, (long long)W * H - base);
     constexpr int B = 4;  // pixels per thread in flight
     for (long long q0 = threadIdx.x; q0 < n; q0 += (long long)blockDim.x * B)
     {
@@ -1350,10 +1352,12 @@ int launch_warp_tiles(const BlendArgs& a, const Unit* units, int n, cudaStream_t
     return check_launch("tile warp kernel");
 }
 
-int launch_dt(const BlendArgs& a, const int* itemList, int n, bool backward, int maxW, int maxH, cudaStream_t s)
+int launch_dt(const BlendArgs& a, const int* itemList, int n, bool backward, int maxW, int maxH, int slotsWanted,
+              cudaStream_t s)
 {
     if (n <= 0) return I360B_SUCCESS;
     int slots = dt_rows_in_flight(maxW, maxH);
+    if (slotsWanted >= 2 && slotsWanted < slots) slots = slotsWanted;
     if (slots < 2)
         return fail(I360B_NOT_SUPPORTED, "Chunk %dx%d exceeds the distance-transform row ring.", maxW, maxH);
     size_t smem = (size_t)slots * dt_ring_stride(maxW) * sizeof(float) + dt_prog_bytes(maxH);

@@ -8,7 +8,7 @@
 namespace i360b
 {
 constexpr int kMaxBands = 8;
-constexpr int kBandRows = 16;  // rows per CTA of the per-pixel band kernels
+constexpr int kBandRows = 16;  // default rows per CTA of the per-pixel band kernels
 constexpr int kSeamRadius = 24;                 // SeamBlend.cpp:319
 constexpr int kSeamBand = 2 * kSeamRadius + 1;  // candidates per line
 constexpr float kSeamSmooth = 2.0f;             // SeamBlend.cpp:309
@@ -72,12 +72,14 @@ struct BlendArgs
     TileDev* tiles;
     int* error;                        // set non-zero by a kernel that gave up (bounded waits)
     unsigned long long* seamCycles;    // per-phase SM cycles of the seam kernel (5 counters)
+    int bandRows;                      // rows per band unit (a multiple of 8; the plan's tuning)
 };
 
 // Kernel launchers (blend_kernels.cu).
 int launch_coverage(const BlendArgs& a, const Unit* units, int n, cudaStream_t s);
 int launch_warp_tiles(const BlendArgs& a, const Unit* units, int n, cudaStream_t s);
-int launch_dt(const BlendArgs& a, const int* itemList, int n, bool backward, int maxW, int maxH, cudaStream_t s);
+int launch_dt(const BlendArgs& a, const int* itemList, int n, bool backward, int maxW, int maxH, int slots,
+              cudaStream_t s);
 int launch_owner(const BlendArgs& a, const Unit* units, int n, cudaStream_t s);
 int launch_seam(const BlendArgs& a, const int* tileList, int n, cudaStream_t s);
 int launch_down(const BlendArgs& a, const Unit* units, int n, int level, cudaStream_t s);

@@ -227,54 +227,9 @@ int Plan::build(const std::vector<TileSpec>& specs, int numBands, bool renderPat
     nItems = (int)items.size();
     // ---- work lists -------------------------------------------------------
     std::vector<Unit> units;
-    // Band units: kBandRows full-width rows each (per-pixel kernels).
-    auto addBands = [&](int id, int h) {
-        for (int by = 0; by < (h + kBandRows - 1) / kBandRows; ++by) units.push_back(Unit{id, 0, by, 0});
-    };
-    // Block units of the pyramid down kernel: 32 x 16 outputs each.
-    auto addBlocks = [&](int id, int w, int h) {
-        for (int by = 0; by < (h + 15) / 16; ++by)
-            for (int bx = 0; bx < (w + 31) / 32; ++bx) units.push_back(Unit{id, bx, by, 0});
-    };
-    lists.clear();
-    auto beginList = [&]() { return (int)units.size(); };
-    auto endList = [&](int start) { lists.push_back(Range{start, (int)units.size() - start}); };
-    int s;
-    s = beginList();  // 0: coverage / warp
-    for (int i = 0; i < nItems; ++i) addBands(i, tiles[items[i].tile].h);
-    endList(s);
-    s = beginList();  // 1: ownership
-    for (int t = 0; t < nTiles; ++t) addBands(t, tiles[t].h);
-    endList(s);
-    s = beginList();  // 2: level 0 output
-    for (int t = 0; t < nTiles; ++t) addBands(t, tiles[t].h);
-    endList(s);
-    for (int l = 0; l < kMaxBands - 1; ++l)  // 3 + l: down from level l
-    {
-        s = beginList();
-        for (int i = 0; i < nItems; ++i)
-        {
-            const TileDev& T = tiles[items[i].tile];
-            if (T.bands > l + 1) addBlocks(i, T.lw[l + 1], T.lh[l + 1]);
-        }
-        endList(s);
-    }
-    for (int l = 0; l < kMaxBands; ++l)  // 3 + (kMaxBands-1) + l: blend band at level l (l >= 1)
-    {
-        s = beginList();
-        if (l >= 1)
-            for (int t = 0; t < nTiles; ++t)
-                if (tiles[t].bands > l) addBands(t, tiles[t].lh[l]);
-        endList(s);
-    }
-    for (int l = 0; l < kMaxBands; ++l)  // 3 + 2*kMaxBands - 1 + l: collapse at level l (1 <= l <= bands-2)
-    {
-        s = beginList();
-        if (l >= 1)
-            for (int t = 0; t < nTiles; ++t)
-                if (tiles[t].bands > l + 1) addBands(t, tiles[t].lh[l]);
-        endList(s);
-    }
+    make_units(8, units);  // the largest list any band height needs
+    unitCap = (int)units.size();
+    make_units(bandRows, units);
     std::vector<int> ints;
     for (int i = 0; i < nItems; ++i) ints.push_back(i);
     int seamStart = (int)ints.size();
@@ -282,7 +237,7 @@ int Plan::build(const std::vector<TileSpec>& specs, int numBands, bool renderPat
         if (tiles[t].numItems >= 2) ints.push_back(t);
     nSeam = (int)ints.size() - seamStart;
     // ---- device allocation -----------------------------------------------
-    size_t unitBytes = align256(std::max<size_t>(units.size(), 1) * sizeof(Unit));
+    size_t unitBytes = align256(std::max<size_t>(unitCap, 1) * sizeof(Unit));
     size_t intBytes = align256(std::max<size_t>(ints.size(), 1) * sizeof(int));
     size_t itemBytes = align256(std::max(nItems, 1) * sizeof(ItemDev));
     size_t tileBytes = align256(std::max(nTiles, 1) * sizeof(TileDev));
@@ -373,6 +328,78 @@ int Plan::build(const std::vector<TileSpec>& specs, int numBands, bool renderPat
     return I360B_SUCCESS;
 }
 
+void Plan::make_units(int rows, std::vector<Unit>& units)
+{
+    units.clear();
+    // Band units: `rows` full-width rows each (per-pixel kernels).
+    auto addBands = [&](int id, int h) {
+        for (int by = 0; by < (h + rows - 1) / rows; ++by) units.push_back(Unit{id, 0, by, 0});
+    };
+    // Block units of the pyramid down kernel: 32 x 16 outputs each.
+    auto addBlocks = [&](int id, int w, int h) {
+        for (int by = 0; by < (h + 15) / 16; ++by)
+            for (int bx = 0; bx < (w + 31) / 32; ++bx) units.push_back(Unit{id, bx, by, 0});
+    };
+    lists.clear();
+    auto beginList = [&]() { return (int)units.size(); };
+    auto endList = [&](int start) { lists.push_back(Range{start, (int)units.size() - start}); };
+    int s;
+    s = beginList();  // 0: coverage / warp
+    for (int i = 0; i < nItems; ++i) addBands(i, tiles[items[i].tile].h);
+    endList(s);
+    s = beginList();  // 1: ownership
+    for (int t = 0; t < nTiles; ++t) addBands(t, tiles[t].h);
+    endList(s);
+    s = beginList();  // 2: level 0 output
+    for (int t = 0; t < nTiles; ++t) addBands(t, tiles[t].h);
+    endList(s);
+    for (int l = 0; l < kMaxBands - 1; ++l)  // 3 + l: down from level l
+    {
+        s = beginList();
+        for (int i = 0; i < nItems; ++i)
+        {
+            const TileDev& T = tiles[items[i].tile];
+            if (T.bands > l + 1) addBlocks(i, T.lw[l + 1], T.lh[l + 1]);
+        }
+        endList(s);
+    }
+    for (int l = 0; l < kMaxBands; ++l)  // 3 + (kMaxBands-1) + l: blend band at level l (l >= 1)
+    {
+        s = beginList();
+        if (l >= 1)
+            for (int t = 0; t < nTiles; ++t)
+                if (tiles[t].bands > l) addBands(t, tiles[t].lh[l]);
+        endList(s);
+    }
+    for (int l = 0; l < kMaxBands; ++l)  // 3 + 2*kMaxBands - 1 + l: collapse at level l (1 <= l <= bands-2)
+    {
+        s = beginList();
+        if (l >= 1)
+            for (int t = 0; t < nTiles; ++t)
+                if (tiles[t].bands > l + 1) addBands(t, tiles[t].lh[l]);
+        endList(s);
+    }
+}
+
+int Plan::set_tuning(int rows, int slots, cudaStream_t s)
+{
+    if (rows < 8 || rows > 64 || (rows & 7)) return fail(I360B_INVALID_PARAM, "band rows must be 8..64, a multiple of 8");
+    std::vector<Unit> units;
+    make_units(rows, units);
+    if ((int)units.size() > unitCap) return fail(I360B_INVALID_PARAM, "work list exceeds its capacity");
+    I360B_CUDA(cudaStreamSynchronize(s), "plan tuning");
+    I360B_CUDA(cudaMemcpyAsync(dUnits, units.data(), units.size() * sizeof(Unit), cudaMemcpyHostToDevice, s),
+               "plan tuning");
+    I360B_CUDA(cudaStreamSynchronize(s), "plan tuning");
+    bandRows = rows;
+    dtSlots = slots;
+    if (graphExec) cudaGraphExecDestroy(graphExec);
+    if (graph) cudaGraphDestroy(graph);
+    graphExec = nullptr;
+    graph = nullptr;
+    return I360B_SUCCESS;
+}
+
 Plan::~Plan()
 {
     if (graphExec) cudaGraphExecDestroy(graphExec);
@@ -396,7 +423,7 @@ int Plan::kernels_per_execute() const
 
 int Plan::enqueue_warp(cudaStream_t s)
 {
-    BlendArgs a{dItems, dTiles, dError, dSeamCycles};
+    BlendArgs a{dItems, dTiles, dError, dSeamCycles, bandRows};
     if (nItems > 0) k_init_bbox<<<(nItems + 127) / 128, 128, 0, s>>>(dItems, nItems);
     I360B_TRY(check_launch("bbox init kernel"));
     I360B_CUDA(cudaMemsetAsync(dError, 0, sizeof(int), s), "error flag reset");
@@ -407,7 +434,7 @@ int Plan::enqueue_warp(cudaStream_t s)
 
 int Plan::enqueue(cudaStream_t s, cudaEvent_t* ev)
 {
-    BlendArgs a{dItems, dTiles, dError, dSeamCycles};
+    BlendArgs a{dItems, dTiles, dError, dSeamCycles, bandRows};
     auto L = [&](int idx) { return lists[idx]; };
     auto mark = [&](int i) {
         if (ev) cudaEventRecord(ev[i], s);
@@ -416,9 +443,9 @@ int Plan::enqueue(cudaStream_t s, cudaEvent_t* ev)
     I360B_TRY(enqueue_warp(s));
     Range r;
     mark(1);
-    I360B_TRY(launch_dt(a, dInts, nItems, false, maxW, maxH, s));
+    I360B_TRY(launch_dt(a, dInts, nItems, false, maxW, maxH, dtSlots, s));
     mark(2);
-    I360B_TRY(launch_dt(a, dInts, nItems, true, maxW, maxH, s));
+    I360B_TRY(launch_dt(a, dInts, nItems, true, maxW, maxH, dtSlots, s));
     mark(3);
     r = L(1);
     I360B_TRY(launch_owner(a, dUnits + r.start, r.count, s));
@@ -690,6 +717,52 @@ extern "C" int i360b_render_plan_wait(i360b_render_plan* plan, void* stream)
     if (!plan) return fail(I360B_INVALID_PARAM, "Null plan.");
     I360B_TRY(ensure_ready());
     return plan->plan.check(static_cast<cudaStream_t>(stream));
+}
+
+extern "C" int i360b_render_plan_autotune(i360b_render_plan* plan, void* stream, int* bandRows, int* dtSlots,
+                                          float* bestMs)
+{
+    clear_error();
+    if (!plan) return fail(I360B_INVALID_PARAM, "Null plan.");
+    I360B_TRY(ensure_ready());
+    Plan& P = plan->plan;
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    const int maxSlots = dt_rows_in_flight(P.maxW, P.maxH);
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    I360B_CUDA(cudaEventCreate(&e0), "autotune events");
+    I360B_CUDA(cudaEventCreate(&e1), "autotune events");
+    int bestR = P.bandRows, bestS = P.dtSlots;
+    float best = INFINITY;
+    int rc = I360B_SUCCESS;
+    for (int rows : {8, 16, 32, 64})
+    {
+        for (int slots = 2; slots <= maxSlots && rc == I360B_SUCCESS; ++slots)
+        {
+            if ((rc = P.set_tuning(rows, slots, s)) != I360B_SUCCESS) break;
+            if ((rc = P.execute(s, true)) != I360B_SUCCESS) break;  // capture + warm-up
+            cudaEventRecord(e0, s);
+            for (int k = 0; k < 2 && rc == I360B_SUCCESS; ++k) rc = P.execute(s, true);
+            cudaEventRecord(e1, s);
+            if (rc == I360B_SUCCESS) rc = P.check(s);
+            float ms = 0.0f;
+            cudaEventElapsedTime(&ms, e0, e1);
+            if (rc == I360B_SUCCESS && ms < best)
+            {
+                best = ms;
+                bestR = rows;
+                bestS = slots;
+            }
+        }
+        if (rc != I360B_SUCCESS) break;
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (rc != I360B_SUCCESS) return rc;
+    I360B_TRY(P.set_tuning(bestR, bestS, s));
+    if (bandRows) *bandRows = bestR;
+    if (dtSlots) *dtSlots = bestS;
+    if (bestMs) *bestMs = best / 2.0f;
+    return I360B_SUCCESS;
 }
 
 extern "C" size_t i360b_render_plan_scratch_bytes(const i360b_render_plan* plan)

@@ -51,6 +51,10 @@ struct Plan
 {
     bool render = false;
     int nTiles = 0, nItems = 0, nSeam = 0, bandsReq = 0, maxW = 1, maxH = 1;
+    // Tuning: rows per band unit of the per-pixel kernels (8, 16, 32 or 64)
+    // and ring slots of the chamfer transform (0 = as many as fit).
+    int bandRows = kBandRows, dtSlots = 0;
+    int unitCap = 0;  // units the device list holds (sized for 8-row bands)
     std::vector<ItemDev> items;
     std::vector<TileDev> tiles;
     std::vector<Range> lists;
@@ -86,6 +90,11 @@ struct Plan
     // coverage pass, leaving every contributor's tile-space image in the arena.
     int enqueue_warp(cudaStream_t s);
     int kernels_per_execute() const;
+    // Work lists for band height `rows` (fills `lists`).
+    void make_units(int rows, std::vector<Unit>& units);
+    // Switches the band height and chamfer ring depth; the next execute
+    // recaptures the graph.  Synchronous on `s`.
+    int set_tuning(int rows, int slots, cudaStream_t s);
     int execute(cudaStream_t s, bool useGraph);
     // Waits for the stream and reports a kernel that gave up (bounded waits).
     int check(cudaStream_t s);

@@ -232,6 +232,16 @@ I360B_API int i360b_render_plan_stats(i360b_render_plan* plan, void* stream, i36
  * i360b_render_stage_name).  Synchronous. */
 I360B_API int i360b_render_plan_profile(i360b_render_plan* plan, void* stream, float* stageMs, int maxStages);
 I360B_API const char* i360b_render_stage_name(int stage);
+/* Autotuner: times the plan's own execute (two runs after a warm-up, CUDA
+ * events on `stream`) for every band-unit height of the per-pixel kernels
+ * (8, 16, 32, 64 rows) and every ring depth of the chamfer transform that
+ * fits (2 to 4 row groups), and keeps the fastest.  The output of every
+ * setting is identical (the settings only partition the same work), so
+ * tuning never changes results.  The chosen values and the best time of one
+ * execute are returned when the pointers are non-null.  Synchronous; the
+ * plan's outputs are overwritten with its render. */
+I360B_API int i360b_render_plan_autotune(i360b_render_plan* plan, void* stream, int* bandRows, int* dtSlots,
+                                         float* bestMs);
 /* Device bytes of scratch the plan holds. */
 I360B_API size_t i360b_render_plan_scratch_bytes(const i360b_render_plan* plan);
 I360B_API void i360b_render_plan_destroy(i360b_render_plan* plan);

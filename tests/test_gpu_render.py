@@ -134,4 +134,13 @@ def test_render_plan_uneven_tiles_exact(backend, oracle_c):
     assert len({(t[2], t[3]) for t in ut.tiles}) > 5
     for t, (o, r) in enumerate(zip(outs, ref)):
         assert np.array_equal(_host_u16(o), r), (t, ut.tiles[t][:4])
+    # The autotuner only re-partitions the same work: every setting it tries,
+    # and the one it keeps, renders the same bits.
+    tuned = plan.autotune()
+    assert tuned["band_rows"] in (8, 16, 32, 64) and 2 <= tuned["dt_slots"] <= 4 and tuned["ms"] > 0
+    for o in outs:
+        o.zero_()
+    assert plan.execute() == ComputeResult.SUCCESS and plan.wait() == ComputeResult.SUCCESS
+    for t, (o, r) in enumerate(zip(outs, ref)):
+        assert np.array_equal(_host_u16(o), r), ("after autotune", t)
     plan.close()
