@@ -21,7 +21,19 @@ IN_SCALE = 1.0 / 32768.0
 class BlendJob(ct.Structure):
     _fields_ = [("slot", ct.c_void_p * 4), ("pixStride", ct.c_longlong), ("rowStride", ct.c_longlong),
                 ("width", ct.c_int), ("height", ct.c_int), ("target", ct.c_void_p),
-                ("targetRowStride", ct.c_longlong), ("out", ct.c_void_p), ("outRowStride", ct.c_longlong)]
+                ("targetRowStride", ct.c_longlong), ("out", ct.c_void_p), ("outRowStride", ct.c_longlong),
+                ("edges", (ct.c_float * 16) * 4)]
+
+
+NO_EDGES = [float("nan"), 0.0, 0.0, 0.0] * 4  # one slot without boundary segments
+
+
+def set_edges(job: BlendJob, slot_edges):
+    """slot_edges: 4 entries (one per slot) of 16 floats or None (no segments)."""
+    for i in range(4):
+        e = slot_edges[i] if slot_edges is not None and slot_edges[i] is not None else NO_EDGES
+        for q in range(16):
+            job.edges[i][q] = float(e[q])
 
 
 def _bind():
@@ -75,11 +87,12 @@ def param_layout() -> list[tuple[int, int, int, int]]:
 
 
 def make_jobs(slots, width: int, height: int, pix_stride: int, row_stride: int, target=None, target_row_stride=0,
-              out=None, out_row_stride=0) -> ct.Array:
+              out=None, out_row_stride=0, edges=None) -> ct.Array:
     """A ctypes array of BlendJob from per-window slot pointers.
 
     ``slots``: list (one per window) of 4 device pointers or None.  ``target``
-    and ``out``: per-window device pointers (or None).
+    and ``out``: per-window device pointers (or None).  ``edges``: per window,
+    4 slot entries of 16 floats (boundary segments in window pixels) or None.
     """
     n = len(slots)
     arr = (BlendJob * n)()
@@ -95,19 +108,21 @@ def make_jobs(slots, width: int, height: int, pix_stride: int, row_stride: int, 
         j.targetRowStride = target_row_stride
         j.out = (out[k] if out is not None else None) or None
         j.outRowStride = out_row_stride
+        set_edges(j, edges[k] if edges is not None else None)
     return arr
 
 
-def batch_jobs(layers, target=None, out=None) -> ct.Array:
+def batch_jobs(layers, target=None, out=None, edges=None) -> ct.Array:
     """Jobs for a dense batch: ``layers`` uint16/int16 CUDA tensor [n][h][w][4][3]
-    (a layer that is all zero is simply uncovered), ``target``/``out`` [n][h][w][3]."""
+    (a layer that is all zero is simply uncovered), ``target``/``out`` [n][h][w][3],
+    ``edges`` optional [n][4][16] boundary segments."""
     n, h, w = layers.shape[:3]
     base = layers.data_ptr()
     es = layers.element_size()
     slots = [[base + (k * h * w * 12 + i * 3) * es for i in range(4)] for k in range(n)]
     tg = [target.data_ptr() + k * h * w * 3 * es for k in range(n)] if target is not None else None
     ot = [out.data_ptr() + k * h * w * 3 * es for k in range(n)] if out is not None else None
-    return make_jobs(slots, w, h, 12, 12 * w, tg, 3 * w, ot, 3 * w)
+    return make_jobs(slots, w, h, 12, 12 * w, tg, 3 * w, ot, 3 * w, edges)
 
 
 class BlendNet:

@@ -705,6 +705,29 @@ __global__ void k_wgrad_reduce(const float* __restrict__ partial, int slices, in
 // ---------------------------------------------------------------------------
 // Glue: input packing, pooling, loss, gradient routing, bias gradients, Adam.
 // ---------------------------------------------------------------------------
+// The mask channel of a covered pixel: 0.25 + 0.75 min(1, d / kFeather) with
+// d the distance from (x, y) to the nearest of the slot's boundary segments
+// (1 when it has none).
+constexpr float kFeather = 2048.0f;
+
+__device__ __forceinline__ float feathered_mask(const float* e, float x, float y)
+{
+    float d2 = INFINITY;
+#pragma unroll
+    for (int s = 0; s < 4; ++s)
+    {
+        const float ax = e[4 * s], ay = e[4 * s + 1];
+        if (ax != ax) continue;  // absent segment
+        const float dx = e[4 * s + 2] - ax, dy = e[4 * s + 3] - ay;
+        const float l2 = dx * dx + dy * dy;
+        float t = l2 > 0.0f ? ((x - ax) * dx + (y - ay) * dy) / l2 : 0.0f;
+        t = fminf(fmaxf(t, 0.0f), 1.0f);
+        const float qx = ax + t * dx - x, qy = ay + t * dy - y;
+        d2 = fminf(d2, qx * qx + qy * qy);
+    }
+    return 0.25f + 0.75f * fminf(1.0f, sqrtf(d2) / kFeather);
+}
+
 __global__ void k_pack_input(const i360b_blend_job* __restrict__ jobs, int n, int h, int w, bf16* __restrict__ x0)
 {
     const long long total = (long long)n * h * w;
@@ -730,7 +753,7 @@ __global__ void k_pack_input(const i360b_blend_job* __restrict__ jobs, int n, in
                 ch[4 * i] = r * kInScale;
                 ch[4 * i + 1] = g * kInScale;
                 ch[4 * i + 2] = b * kInScale;
-                ch[4 * i + 3] = 1.0f;
+                ch[4 * i + 3] = feathered_mask(J.edges[i], (float)x, (float)y);
             }
         }
         uint4* o = reinterpret_cast<uint4*>(x0 + idx * 16);
@@ -2029,6 +2052,22 @@ int learned_render(Plan& P, BlendNet& N, unsigned short* const* tileOut, int max
         {
             i360b_blend_job j{};
             for (int i = 0; i < 4; ++i) j.slot[i] = st.item[i] >= 0 ? P.items[st.item[i]].img + off : nullptr;
+            for (int i = 0; i < 4; ++i)
+                for (int e = 0; e < 4; ++e)
+                {
+                    const float* src = st.item[i] >= 0 ? &P.itemEdges[(size_t)st.item[i] * 16 + 4 * e] : nullptr;
+                    float* d = &j.edges[i][4 * e];
+                    if (!src)
+                    {
+                        d[0] = NAN;
+                        d[1] = d[2] = d[3] = 0.0f;
+                        continue;
+                    }
+                    d[0] = src[0] - st.ox;  // NaN stays NaN
+                    d[1] = src[1] - st.oy;
+                    d[2] = src[2] - st.ox;
+                    d[3] = src[3] - st.oy;
+                }
             j.pixStride = 3;
             j.rowStride = 3LL * T.w;
             j.width = st.w;
@@ -2206,7 +2245,7 @@ extern "C" int i360b_render_plan_windows(i360b_render_plan* plan, int maxWindows
 }
 
 extern "C" int i360b_render_plan_tile_items(i360b_render_plan* plan, int tile, int maxItems,
-                                            const unsigned short** dImages, int* boxes, int* numItems)
+                                            const unsigned short** dImages, int* boxes, float* edges, int* numItems)
 {
     clear_error();
     if (!plan || !numItems) return fail(I360B_INVALID_PARAM, "Null pointer argument.");
@@ -2226,6 +2265,8 @@ extern "C" int i360b_render_plan_tile_items(i360b_render_plan* plan, int tile, i
             boxes[4 * k + 2] = it.vx1;
             boxes[4 * k + 3] = it.vy1;
         }
+        if (edges)
+            for (int q = 0; q < 16; ++q) edges[16 * k + q] = P.itemEdges[(size_t)(T.firstItem + k) * 16 + q];
     }
     return I360B_SUCCESS;
 }

@@ -122,6 +122,7 @@ int Plan::build(const std::vector<TileSpec>& specs, int numBands, bool renderPat
     // ---- host layout ------------------------------------------------------
     tiles.assign(nTiles, TileDev{});
     items.clear();
+    itemEdges.clear();
     size_t bytes = 0;
     struct Off
     {
@@ -222,6 +223,7 @@ int Plan::build(const std::vector<TileSpec>& specs, int numBands, bool renderPat
             o.wg = bytes; bytes += align256(std::max<size_t>(pyrPx, 1) * 4);
             items.push_back(it);
             itemOff.push_back(o);
+            itemEdges.insert(itemEdges.end(), I.edges, I.edges + 16);
         }
     }
     nItems = (int)items.size();
@@ -600,6 +602,61 @@ int launch_blend_chunk_in(void* arena, size_t arenaBytes, const unsigned short* 
 // ---------------------------------------------------------------------------
 using namespace i360b;
 
+namespace
+{
+// The coverage boundary of a frame in tile coordinates: the warp writes
+// destination pixel (x, y) when its source position lies in [0, srcW-1) x
+// [0, srcH-1), so the boundary is that source rectangle mapped by the
+// frame->canvas homography (FP64) and shifted by the tile origin.  Each of
+// its 4 edges is clipped to the tile's pixel centres [0, w-1] x [0, h-1]
+// (Liang-Barsky); an edge outside the tile is absent (NaN x0).
+void coverage_edges(const double* m, int srcW, int srcH, int tx, int ty, int w, int h, float* out)
+{
+    const double sx[4] = {0.0, (double)(srcW - 1), (double)(srcW - 1), 0.0};
+    const double sy[4] = {0.0, 0.0, (double)(srcH - 1), (double)(srcH - 1)};
+    double px[4], py[4];
+    for (int q = 0; q < 4; ++q)
+    {
+        const double wq = m[6] * sx[q] + m[7] * sy[q] + m[8];
+        px[q] = (m[0] * sx[q] + m[1] * sy[q] + m[2]) / wq - tx;
+        py[q] = (m[3] * sx[q] + m[4] * sy[q] + m[5]) / wq - ty;
+    }
+    for (int e = 0; e < 4; ++e)
+    {
+        const double x0 = px[e], y0 = py[e], dx = px[(e + 1) & 3] - x0, dy = py[(e + 1) & 3] - y0;
+        double t0 = 0.0, t1 = 1.0;
+        const double pp[4] = {-dx, dx, -dy, dy};
+        const double qq[4] = {x0 - 0.0, (w - 1) - x0, y0 - 0.0, (h - 1) - y0};
+        bool in = true;
+        for (int k = 0; k < 4 && in; ++k)
+        {
+            if (pp[k] == 0.0)
+            {
+                if (qq[k] < 0.0) in = false;
+            }
+            else
+            {
+                const double r = qq[k] / pp[k];
+                if (pp[k] < 0.0) t0 = std::max(t0, r);
+                else t1 = std::min(t1, r);
+                if (t0 > t1) in = false;
+            }
+        }
+        float* o = out + 4 * e;
+        if (!in)
+        {
+            o[0] = __builtin_nanf("");
+            o[1] = o[2] = o[3] = 0.0f;
+            continue;
+        }
+        o[0] = (float)(x0 + t0 * dx);
+        o[1] = (float)(y0 + t0 * dy);
+        o[2] = (float)(x0 + t1 * dx);
+        o[3] = (float)(y0 + t1 * dy);
+    }
+}
+}  // namespace
+
 extern "C" int i360b_render_plan_create(const i360b_frame* frames, int numFrames, const i360b_tile* tiles,
                                         int numTiles, const int* contributors, int numBands, int coordMode,
                                         i360b_render_plan** outPlan)
@@ -686,6 +743,7 @@ extern "C" int i360b_render_plan_create(const i360b_frame* frames, int numFrames
                     it.vy0 = (int)std::max(-1.0, std::floor(mny - 2.0 - T.y));
                     it.vx1 = (int)std::min((double)T.width, std::ceil(mxx + 2.0 - T.x));
                     it.vy1 = (int)std::min((double)T.height, std::ceil(mxy + 2.0 - T.y));
+                    coverage_edges(m, F.width, F.height, T.x, T.y, T.width, T.height, it.edges);
                 }
             }
             specs[t].items.push_back(it);

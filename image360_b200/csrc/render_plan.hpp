@@ -19,6 +19,10 @@ struct ItemSpec
     float gain = 1.0f;
     // Tile-local box outside which the warp is surely empty (default: all).
     int vx0 = 0, vy0 = 0, vx1 = 0x3fffffff, vy1 = 0x3fffffff;
+    // The 4 edges of the coverage boundary clipped to the tile, {x0, y0, x1,
+    // y1} each in tile pixels; NaN x0 = absent (the learned blend's feature).
+    float edges[16] = {__builtin_nanf(""), 0, 0, 0, __builtin_nanf(""), 0, 0, 0,
+                       __builtin_nanf(""), 0, 0, 0, __builtin_nanf(""), 0, 0, 0};
 };
 
 struct TileSpec
@@ -69,6 +73,7 @@ struct Plan
     unsigned long long* dSeamCycles = nullptr;
     int* hostErr = nullptr;
     std::vector<SubTile> subTiles;  // built on first learned render
+    std::vector<float> itemEdges;   // 16 per item (ItemSpec::edges)
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t graphExec = nullptr;
 

@@ -40,7 +40,8 @@ def _bind():
     L.i360b_render_plan_learned.argtypes = [vp, vp, ct.POINTER(vp), i, vp, ct.POINTER(ct.c_float)]
     L.i360b_render_plan_judge.argtypes = [vp, ct.POINTER(vp), ct.c_double, ct.c_double, ct.POINTER(LearnedStats),
                                           ct.POINTER(ct.c_float), i, vp]
-    L.i360b_render_plan_tile_items.argtypes = [vp, i, i, ct.POINTER(vp), ct.POINTER(ct.c_int), ct.POINTER(ct.c_int)]
+    L.i360b_render_plan_tile_items.argtypes = [vp, i, i, ct.POINTER(vp), ct.POINTER(ct.c_int),
+                                               ct.POINTER(ct.c_float), ct.POINTER(ct.c_int)]
     L.i360b_render_plan_windows.argtypes = [vp, i, ct.POINTER(ct.c_int), ct.POINTER(ct.c_int)]
     L._learned_bound = True
     return L
@@ -94,18 +95,24 @@ class PanoramaRender:
         if self.plan.execute(stream) != 0 or self.plan.wait(stream) != 0:
             raise RuntimeError(self.be.get_last_error())
 
-    def tile_items(self, t: int):
-        """[(device image ptr, (x0, y0, x1, y1))] of tile t's contributors."""
+    def tile_items(self, t: int, with_edges: bool = False):
+        """[(device image ptr, (x0, y0, x1, y1))] of tile t's contributors;
+        with_edges adds each one's 16 boundary-segment floats (tile pixels)."""
         L = _bind()
         n = ct.c_int()
         imgs = (ct.c_void_p * 64)()
         boxes = (ct.c_int * 256)()
-        _check(L.i360b_render_plan_tile_items(self.plan._h, t, 64, imgs, boxes, ct.byref(n)))
-        return [(imgs[k], tuple(boxes[4 * k:4 * k + 4])) for k in range(min(n.value, 64))]
+        edges = (ct.c_float * (16 * 64))()
+        _check(L.i360b_render_plan_tile_items(self.plan._h, t, 64, imgs, boxes, edges, ct.byref(n)))
+        k = min(n.value, 64)
+        if with_edges:
+            return [(imgs[i], tuple(boxes[4 * i:4 * i + 4]), list(edges[16 * i:16 * i + 16])) for i in range(k)]
+        return [(imgs[i], tuple(boxes[4 * i:4 * i + 4])) for i in range(k)]
 
     def items(self):
+        """Per tile, [(image ptr, box, edges)] of its contributors (cached)."""
         if self._items is None:
-            self._items = [self.tile_items(t) for t in range(len(self.tiles))]
+            self._items = [self.tile_items(t, with_edges=True) for t in range(len(self.tiles))]
         return self._items
 
     def learned(self, net: bn.BlendNet, outs=None, max_batch: int = 256, stream=0) -> dict:
@@ -158,7 +165,7 @@ def sample_windows(render: PanoramaRender, n: int, rng: np.random.Generator, can
     cands = cands if cands is not None else window_candidates(render)
     if not cands:
         raise RuntimeError("no tile is reached by two contributors")
-    slots, targets = [], []
+    slots, targets, edges = [], [], []
     tries = 0
     while len(slots) < n:
         tries += 1
@@ -168,12 +175,13 @@ def sample_windows(render: PanoramaRender, n: int, rng: np.random.Generator, can
         _, _, w, h, _ = render.tiles[t]
         x = int(rng.integers(0, w - WINDOW + 1))
         y = int(rng.integers(0, h - WINDOW + 1))
-        hit = [p for p, (x0, y0, x1, y1) in render.items()[t]
+        hit = [(p, e) for p, (x0, y0, x1, y1), e in render.items()[t]
                if x0 < x + WINDOW and x1 >= x and y0 < y + WINDOW and y1 >= y]
         if not 2 <= len(hit) <= 4:
             continue
         off = (y * w + x) * 3 * 2  # bytes
-        slots.append([p + off for p in hit] + [None] * (4 - len(hit)))
+        slots.append([p + off for p, _ in hit] + [None] * (4 - len(hit)))
+        edges.append([_shift_edges(e, x, y) for _, e in hit] + [None] * (4 - len(hit)))
         targets.append((render.outs[t].data_ptr() + off, 3 * w))
     jobs = (bn.BlendJob * n)()
     for k in range(n):
@@ -187,7 +195,19 @@ def sample_windows(render: PanoramaRender, n: int, rng: np.random.Generator, can
         j.height = WINDOW
         j.target = targets[k][0]
         j.targetRowStride = targets[k][1]
+        bn.set_edges(j, edges[k])
     return jobs
+
+
+def _shift_edges(e, x, y):
+    """Boundary segments from tile to window coordinates (NaN stays NaN)."""
+    out = list(e)
+    for s in range(4):
+        out[4 * s] -= x
+        out[4 * s + 1] -= y
+        out[4 * s + 2] -= x
+        out[4 * s + 3] -= y
+    return out
 
 
 def train(net: bn.BlendNet, renders, steps: int, batch: int = 64, lr: float = 1e-3, seed: int = 0, log=None,

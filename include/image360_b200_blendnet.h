@@ -7,8 +7,11 @@
  * The network stands in for that blend on overlap windows:
  *
  *   input   16 channels per pixel: up to 4 warped RGB48 layers, each as R, G, B
- *           (value / 32768) and a coverage mask (1 where the layer is not
- *           (0,0,0), SeamBlend.cpp:565), in bf16;
+ *           (value / 32768) and a feathered coverage mask: 0 where the layer
+ *           is (0,0,0) (uncovered, SeamBlend.cpp:565), else
+ *           0.25 + 0.75 min(1, d / 2048) with d the distance from the pixel
+ *           to the nearest of the layer's boundary edges given in the job
+ *           (1 where none is given), in bf16;
  *   net     a 2-scale U-Net-lite of eight 3x3 convolutions with zero padding:
  *           16->32, 32->32 (full resolution, kept as the skip), 2x2 average
  *           pool, 32->64, 64->64, 64->64 (half resolution), nearest 2x
@@ -52,6 +55,11 @@ typedef struct i360b_blend_job
     /* Inference: RGB48 output (3 elements per pixel). */
     unsigned short* out;
     long long outRowStride;
+    /* Per slot, up to 4 line segments {x0, y0, x1, y1} in window pixel
+     * coordinates: the parts of the layer's coverage boundary inside the
+     * output tile (the distance of the feathered mask).  A segment whose x0
+     * is NaN is absent. */
+    float edges[4][16];
 } i360b_blend_job;
 
 typedef struct i360b_blendnet i360b_blendnet;
@@ -133,11 +141,14 @@ I360B_API int i360b_render_plan_judge(i360b_render_plan* plan, unsigned short* c
  * entries are written. */
 I360B_API int i360b_render_plan_windows(i360b_render_plan* plan, int maxWindows, int* info, int* numWindows);
 /* The warped contributor images of tile `tile` after an execute (device RGB48,
- * tile-sized) and their footprint boxes {x0, y0, x1, y1} in tile pixels
- * (outside the box the image is zero).  numItems receives the count; up to
- * maxItems entries are written. */
+ * tile-sized), their footprint boxes {x0, y0, x1, y1} in tile pixels
+ * (outside the box the image is zero) and, when `edges` is non-null, 16
+ * floats per contributor: the 4 edges of its coverage boundary clipped to the
+ * tile, as in i360b_blend_job (tile coordinates; NaN x0 = absent).
+ * numItems receives the count; up to maxItems entries are written. */
 I360B_API int i360b_render_plan_tile_items(i360b_render_plan* plan, int tile, int maxItems,
-                                           const unsigned short** dImages, int* boxes, int* numItems);
+                                           const unsigned short** dImages, int* boxes, float* edges,
+                                           int* numItems);
 
 /* ---- convolution primitives (NHWC bf16) --------------------------------- */
 

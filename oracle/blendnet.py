@@ -4,7 +4,8 @@ TEST INFRASTRUCTURE ONLY: imported by tests/ (gradient checks of the GPU
 kernels) and nothing else.  It restates, in float64, the network declared in
 include/image360_b200_blendnet.h: input packing of up to 4 RGB48 layers with
 coverage masks (coverage as in SeamBlend.cpp:565, a pixel is covered when it
-is not (0,0,0)), eight 3x3 zero-padded convolutions, 2x2 average pool,
+is not (0,0,0); the mask is feathered by the distance to the layer's
+footprint boundary when boundary segments are given), eight 3x3 zero-padded convolutions, 2x2 average pool,
 nearest 2x upsample with concatenation after the skip, ReLU, and the softmax
 blend head over the covered layers, plus the mean-squared-error loss against
 a target and the gradient of that loss with respect to every parameter.
@@ -92,14 +93,44 @@ def up2(x):
     return np.repeat(np.repeat(x, 2, axis=1), 2, axis=2)
 
 
-def pack_input(layers: np.ndarray, bf16: bool = True):
-    """layers uint16 [N][H][W][4][3] -> (x0 [N][H][W][16], coverage [N][H][W][4])."""
+FEATHER = 2048.0
+
+
+def feathered_mask(edges: np.ndarray, h: int, w: int) -> np.ndarray:
+    """Mask value of a covered pixel of one slot, [H][W]:
+    0.25 + 0.75 min(1, d / FEATHER), d the distance from the pixel to the
+    nearest of up to 4 boundary segments (x0, y0, x1, y1) in ``edges`` (16
+    floats; a NaN x0 marks an absent segment; no segment gives 1)."""
+    yy, xx = np.mgrid[0:h, 0:w].astype(np.float64)
+    d2 = np.full((h, w), np.inf)
+    for s in range(4):
+        ax, ay, bx, by = (float(v) for v in edges[4 * s:4 * s + 4])
+        if ax != ax:
+            continue
+        dx, dy = bx - ax, by - ay
+        l2 = dx * dx + dy * dy
+        t = np.clip(((xx - ax) * dx + (yy - ay) * dy) / l2, 0.0, 1.0) if l2 > 0 else np.zeros((h, w))
+        qx, qy = ax + t * dx - xx, ay + t * dy - yy
+        d2 = np.minimum(d2, qx * qx + qy * qy)
+    return 0.25 + 0.75 * np.minimum(1.0, np.sqrt(d2) / FEATHER)
+
+
+def pack_input(layers: np.ndarray, bf16: bool = True, edges: np.ndarray | None = None):
+    """layers uint16 [N][H][W][4][3] -> (x0 [N][H][W][16], coverage [N][H][W][4]).
+
+    Channel 4i+3 is slot i's mask: 0 where uncovered, else 1, or the feathered
+    mask when ``edges`` ([N][4][16] boundary segments per slot) is given."""
     v = layers.astype(np.float64)
     cov = (layers != 0).any(axis=-1)
+    n, h, w = layers.shape[:3]
     x0 = np.zeros(layers.shape[:3] + (16,))
     for i in range(4):
         x0[..., 4 * i:4 * i + 3] = np.where(cov[..., i:i + 1], v[..., i, :] * IN_SCALE, 0.0)
-        x0[..., 4 * i + 3] = cov[..., i]
+        if edges is None:
+            x0[..., 4 * i + 3] = cov[..., i]
+        else:
+            for k in range(n):
+                x0[k, ..., 4 * i + 3] = np.where(cov[k, ..., i], feathered_mask(edges[k][i], h, w), 0.0)
     return (bf16_round(x0) if bf16 else x0), cov
 
 
@@ -115,7 +146,7 @@ def head(logits: np.ndarray, layers: np.ndarray, cov: np.ndarray):
     return out, wts
 
 
-def forward(params: np.ndarray, layers: np.ndarray, bf16: bool = True):
+def forward(params: np.ndarray, layers: np.ndarray, bf16: bool = True, edges: np.ndarray | None = None):
     """Forward pass; returns (logits [N][H][W][4], cache for backward)."""
     R = bf16_round if bf16 else (lambda a: a)
     if bf16:  # the GPU keeps fp32 masters, bf16 weights and fp32 biases
@@ -123,7 +154,7 @@ def forward(params: np.ndarray, layers: np.ndarray, bf16: bool = True):
     else:
         P = [(W.astype(np.float64), b.astype(np.float64)) for W, b in split_params(params)]
     relu = lambda a: np.maximum(a, 0.0)
-    x0, cov = pack_input(layers, bf16)
+    x0, cov = pack_input(layers, bf16, edges)
     a1 = R(relu(conv3x3(x0, *P[0])))
     a2 = R(relu(conv3x3(a1, *P[1])))
     p2 = R(pool2(a2))
@@ -152,10 +183,11 @@ def loss_and_dlogits(logits, layers, target, cov):
     return loss, dl
 
 
-def gradients(params: np.ndarray, layers: np.ndarray, target: np.ndarray, bf16: bool = True):
+def gradients(params: np.ndarray, layers: np.ndarray, target: np.ndarray, bf16: bool = True,
+              edges: np.ndarray | None = None):
     """(loss, flat gradient with the layout of ``params``)."""
     R = bf16_round if bf16 else (lambda a: a)
-    logits, c = forward(params, layers, bf16)
+    logits, c = forward(params, layers, bf16, edges)
     loss, dl = loss_and_dlogits(logits, layers, target, c["cov"])
     P = c["P"]
     grads = [None] * 8
@@ -187,8 +219,8 @@ def gradients(params: np.ndarray, layers: np.ndarray, target: np.ndarray, bf16: 
     return loss, flat
 
 
-def blend(params: np.ndarray, layers: np.ndarray, bf16: bool = True) -> np.ndarray:
+def blend(params: np.ndarray, layers: np.ndarray, bf16: bool = True, edges: np.ndarray | None = None) -> np.ndarray:
     """Inference: RGB48 output of the network head, rounded to nearest."""
-    logits, c = forward(params, layers, bf16)
+    logits, c = forward(params, layers, bf16, edges)
     out, _ = head(logits, layers, c["cov"])
     return np.clip(np.rint(out), 0, 65535).astype(np.uint16)

@@ -101,3 +101,35 @@ def test_untrained_head_is_coverage_mean():
     mean = np.where(cnt[..., None] > 0, (layers.astype(np.float64) * cov[..., None]).sum(-2) /
                     np.maximum(cnt, 1)[..., None], 0.0)
     assert np.abs(out.astype(np.float64) - np.rint(mean)).max() <= 1
+
+
+def test_feathered_mask_distances():
+    nan = float("nan")
+    none = [nan, 0, 0, 0] * 4
+    assert np.all(ob.feathered_mask(np.array(none), 3, 5) == 1.0)
+    # One vertical segment x = 0, y in [0, 10]: the mask grows with x.
+    e = np.array([0, 0, 0, 10] + [nan, 0, 0, 0] * 3, np.float64)
+    m = ob.feathered_mask(e, 4, 8)
+    np.testing.assert_allclose(m[:, 0], 0.25)
+    np.testing.assert_allclose(m[2, 5], 0.25 + 0.75 * 5 / ob.FEATHER)
+    # Beyond the segment's end the distance is to the endpoint.
+    e2 = np.array([0, 0, 2, 0] + [nan, 0, 0, 0] * 3, np.float64)
+    m2 = ob.feathered_mask(e2, 4, 6)
+    np.testing.assert_allclose(m2[3, 5], 0.25 + 0.75 * np.sqrt(18.0) / ob.FEATHER)
+    far = np.array([-5000, -5000, -5000, -4000] + [nan, 0, 0, 0] * 3, np.float64)
+    assert np.all(ob.feathered_mask(far, 2, 2) == 1.0)
+
+
+def test_pack_input_without_edges_is_binary_and_edges_feather_covered_pixels():
+    _, layers, _ = _case(9)
+    x_plain, cov = ob.pack_input(layers, bf16=False)
+    nan = float("nan")
+    edges = np.array([[[nan, 0, 0, 0] * 4] * 4] * layers.shape[0], np.float64)
+    x_none, _ = ob.pack_input(layers, bf16=False, edges=edges)
+    np.testing.assert_array_equal(x_plain, x_none)
+    edges[0, 1, :4] = [0, 0, 0, 3]
+    x_f, _ = ob.pack_input(layers, bf16=False, edges=edges)
+    m = x_f[0, ..., 7]
+    assert np.all(m[~cov[0, ..., 1]] == 0)
+    assert np.all((m[cov[0, ..., 1]] >= 0.25) & (m[cov[0, ..., 1]] < 1))
+    np.testing.assert_array_equal(np.delete(x_f, 7, -1), np.delete(x_plain, 7, -1))

@@ -133,13 +133,24 @@ def _random_params(seed):
                                            rng.normal(0, 0.05, co)]) for ci, co in ob.LAYERS]).astype(np.float32)
 
 
-def _device_batch(layers, target=None):
+def _device_batch(layers, target=None, edges=None):
     import torch
     from image360_b200 import blendnet as bn
     dl = _t(layers.view(np.int16))
     dt = _t(target.view(np.int16)) if target is not None else None
     out = torch.zeros(layers.shape[:3] + (3,), dtype=torch.int16, device="cuda")
-    return dl, dt, out, bn.batch_jobs(dl, dt, out)
+    return dl, dt, out, bn.batch_jobs(dl, dt, out, None if edges is None else edges.tolist())
+
+
+def _edges(seed, n, h, w):
+    """Per window and slot, 1 to 4 random boundary segments near the window."""
+    rng = np.random.default_rng(seed)
+    e = np.full((n, 4, 16), np.nan)
+    for k in range(n):
+        for i in range(4):
+            for s in range(rng.integers(1, 5)):
+                e[k, i, 4 * s:4 * s + 4] = rng.uniform([-300, -50, -300, -50], [w + 300, h + 50, w + 300, h + 50])
+    return e
 
 
 def test_network_logits_and_gradients_match_oracle(backend):
@@ -168,6 +179,39 @@ def test_network_logits_and_gradients_match_oracle(backend):
             r = ref_g[o:o + c]
             e = np.linalg.norm(g[o:o + c] - r) / max(np.linalg.norm(r), 1e-30)
             assert e < 2e-2, (l + 1, what, e)
+    net.close()
+
+
+def test_feathered_masks_match_oracle(backend):
+    """Boundary segments give each covered pixel a feathered mask channel:
+    logits and gradients against the oracle computing the same feature."""
+    import torch
+    from image360_b200 import blendnet as bn
+    n, h, w = 2, 8, 256
+    layers = _layers(13, n, h, w)
+    target = _owner_target(layers)
+    edges = _edges(17, n, h, w)
+    params = _random_params(6)
+    net = bn.BlendNet(seed=6)
+    net.set_params(params)
+    dl, dt, _, jobs = _device_batch(layers, target, edges)
+    logits = torch.zeros((n, h, w, 4), dtype=torch.float32, device="cuda")
+    net.logits(jobs, n, w, h, logits)
+    ref_logits, _ = ob.forward(params.astype(np.float64), layers, bf16=True, edges=edges)
+    plain_logits, _ = ob.forward(params.astype(np.float64), layers, bf16=True)
+    got = logits.cpu().numpy()
+    d = np.abs(got - ref_logits)
+    assert d.max() <= 0.02 * np.abs(ref_logits).max() + 1e-3, d.max()
+    assert d.mean() <= 2e-3 * np.abs(ref_logits).mean() + 1e-5, d.mean()
+    # The feature reaches the logits: far more than the rounding noise above.
+    assert np.abs(plain_logits - ref_logits).mean() > 20 * d.mean()
+    g, loss = net.gradients(jobs, n, w, h)
+    ref_loss, ref_g = ob.gradients(params.astype(np.float64), layers, target, bf16=True, edges=edges)
+    assert abs(loss - ref_loss) <= 1e-3 * ref_loss, (loss, ref_loss)
+    for l, (wo, nw, bo, nb) in enumerate(bn.param_layout()):
+        r = ref_g[wo:wo + nw]
+        e = np.linalg.norm(g[wo:wo + nw] - r) / max(np.linalg.norm(r), 1e-30)
+        assert e < 2e-2, (l + 1, e)
     net.close()
 
 

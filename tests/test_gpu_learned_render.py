@@ -38,7 +38,7 @@ def _expected(scene, t, images):
     for oy in range(0, h, 256):
         for ox in range(0, w, 256):
             cw, ch = min(256, w - ox), min(256, h - oy)
-            hits = [k for k, (_, (x0, y0, x1, y1)) in enumerate(items)
+            hits = [k for k, (_, (x0, y0, x1, y1), *_) in enumerate(items)
                     if x0 < ox + cw and x1 >= ox and y0 < oy + ch and y1 >= oy]
             if len(hits) > 4:
                 # the 4 largest footprint overlaps, kept in contributor order
