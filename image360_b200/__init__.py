@@ -103,6 +103,12 @@ def load_library(path: str = LIB_PATH):
     L.i360b_launch_warp.argtypes = [vp, i, i, vp, i, i, _f32p, i, i, f, vp]
     L.i360b_launch_median.argtypes = [ct.POINTER(vp), i, vp, i, i, f, vp]
     L.i360b_launch_gain.argtypes = [vp, i, f, vp]
+    _i32p, _f64p = ct.POINTER(ct.c_int), ct.POINTER(ct.c_double)
+    L.i360b_compute_lab_stats.argtypes = [_u16p, i, i, _f64p, _f64p]
+    L.i360b_apply_reinhard_color_transfer.argtypes = [_u16p, i, i, _f64p, _f64p, _f64p, _f64p]
+    L.i360b_launch_lab_stats.argtypes = [ct.POINTER(vp), _i32p, _i32p, i, vp, vp]
+    L.i360b_launch_reinhard.argtypes = [ct.POINTER(vp), _i32p, _i32p, i, vp, vp, vp]
+    L.i360b_launch_color_correct.argtypes = [ct.POINTER(vp), _i32p, _i32p, i, i, vp, vp]
     L.i360b_launch_blend.argtypes = [ct.POINTER(vp), i, i, i, i, vp, vp]
     L.i360b_launch_blend_noalloc.argtypes = [ct.POINTER(vp), i, i, i, i, vp, vp]
     _lib = L
@@ -122,6 +128,14 @@ def _p16(a: np.ndarray):
 
 def _pf(a: np.ndarray):
     return a.ctypes.data_as(_f32p)
+
+
+def _pd(a: np.ndarray):
+    return a.ctypes.data_as(ct.POINTER(ct.c_double))
+
+
+def _ints(v):
+    return (ct.c_int * max(1, len(v)))(*[int(x) for x in v])
 
 
 class B200ComputeBackend:
@@ -177,6 +191,22 @@ class B200ComputeBackend:
         assert data.dtype == np.uint16 and data.flags.c_contiguous
         return ComputeResult(self.lib.i360b_apply_gain(_p16(data), data.size, ct.c_float(gain)))
 
+    # IComputeBackend.h:65-67
+    def compute_lab_stats(self, rgb: np.ndarray):
+        """(ComputeResult, mean[3], std[3]) of an (h, w, 3) uint16 image."""
+        rgb = np.ascontiguousarray(rgb, np.uint16)
+        mean, std = np.zeros(3), np.zeros(3)
+        r = self.lib.i360b_compute_lab_stats(_p16(rgb), rgb.shape[1], rgb.shape[0], _pd(mean), _pd(std))
+        return ComputeResult(r), mean, std
+
+    # IComputeBackend.h:69-73
+    def apply_reinhard_color_transfer(self, rgb: np.ndarray, src_mean, src_std, ref_mean, ref_std) -> ComputeResult:
+        """In place on an (h, w, 3) C-contiguous uint16 image."""
+        assert rgb.dtype == np.uint16 and rgb.flags.c_contiguous
+        a = [np.ascontiguousarray(v, np.float64).reshape(3) for v in (src_mean, src_std, ref_mean, ref_std)]
+        return ComputeResult(self.lib.i360b_apply_reinhard_color_transfer(_p16(rgb), rgb.shape[1], rgb.shape[0],
+                                                                          *[_pd(v) for v in a]))
+
     # IComputeBackend.h:46-49
     def demosaic_bayer(self, cfa: np.ndarray, black_level: int, cam_mul, rgb_cam, filters: int,
                        rgb_out: np.ndarray) -> ComputeResult:
@@ -217,6 +247,27 @@ class B200ComputeBackend:
 
     def launch_gain(self, d_data: int, n: int, gain: float, stream: int = 0) -> ComputeResult:
         return ComputeResult(self.lib.i360b_launch_gain(d_data, n, gain, stream or None))
+
+    def launch_lab_stats(self, d_images, widths, heights, d_stats: int, stream: int = 0) -> ComputeResult:
+        """Lab statistics of device images into d_stats (device, len * 6 doubles)."""
+        n = len(d_images)
+        return ComputeResult(self.lib.i360b_launch_lab_stats((ct.c_void_p * max(1, n))(*d_images), _ints(widths),
+                                                             _ints(heights), n, d_stats, stream or None))
+
+    def launch_reinhard(self, d_images, widths, heights, d_src_stats: int, d_ref_stats: int,
+                        stream: int = 0) -> ComputeResult:
+        n = len(d_images)
+        return ComputeResult(self.lib.i360b_launch_reinhard((ct.c_void_p * max(1, n))(*d_images), _ints(widths),
+                                                            _ints(heights), n, d_src_stats, d_ref_stats,
+                                                            stream or None))
+
+    def launch_color_correct(self, d_images, widths, heights, ref_index: int, d_stats: int = 0,
+                             stream: int = 0) -> ComputeResult:
+        """Frame-set colour correction toward frame ref_index, in place on the device."""
+        n = len(d_images)
+        return ComputeResult(self.lib.i360b_launch_color_correct((ct.c_void_p * max(1, n))(*d_images),
+                                                                 _ints(widths), _ints(heights), n, ref_index,
+                                                                 d_stats or None, stream or None))
 
     def launch_blend(self, d_warped, width: int, height: int, d_out: int, num_bands: int = 5,
                      stream: int = 0) -> ComputeResult:

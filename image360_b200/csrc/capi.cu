@@ -118,6 +118,60 @@ extern "C" int i360b_apply_gain(unsigned short* data, int numPixels, float gain)
     return sync(s, "ApplyGain");
 }
 
+extern "C" int i360b_compute_lab_stats(const unsigned short* rgb, int width, int height, double outMean[3],
+                                       double outStd[3])
+{
+    clear_error();
+    I360B_TRY(require_init());
+    if (!rgb || !outMean || !outStd) return fail(I360B_INVALID_PARAM, "Null pointer argument.");
+    if (width <= 0 || height <= 0) return fail(I360B_INVALID_PARAM, "Invalid dimensions.");
+    int rc;
+    cudaStream_t s = get_stream(&rc);
+    I360B_TRY(rc);
+    size_t b = (size_t)width * height * 6;
+    DevBuf d, st;
+    I360B_TRY(d.alloc(b, s, "ComputeLabStats"));
+    I360B_TRY(st.alloc(6 * sizeof(double), s, "ComputeLabStats"));
+    I360B_CUDA(cudaMemcpyAsync(d.p, rgb, b, cudaMemcpyHostToDevice, s), "ComputeLabStats upload");
+    const unsigned short* img = d.as<unsigned short>();
+    I360B_TRY(launch_lab_stats(&img, &width, &height, 1, st.as<double>(), s));
+    double h[6];
+    I360B_CUDA(cudaMemcpyAsync(h, st.p, sizeof(h), cudaMemcpyDeviceToHost, s), "ComputeLabStats download");
+    I360B_TRY(sync(s, "ComputeLabStats"));
+    for (int c = 0; c < 3; ++c)
+    {
+        outMean[c] = h[c];
+        outStd[c] = h[3 + c];
+    }
+    return I360B_SUCCESS;
+}
+
+extern "C" int i360b_apply_reinhard_color_transfer(unsigned short* rgbInOut, int width, int height,
+                                                   const double srcMean[3], const double srcStd[3],
+                                                   const double refMean[3], const double refStd[3])
+{
+    clear_error();
+    I360B_TRY(require_init());
+    if (!rgbInOut || !srcMean || !srcStd || !refMean || !refStd)
+        return fail(I360B_INVALID_PARAM, "Null pointer argument.");
+    if (width <= 0 || height <= 0) return fail(I360B_INVALID_PARAM, "Invalid dimensions.");
+    int rc;
+    cudaStream_t s = get_stream(&rc);
+    I360B_TRY(rc);
+    size_t b = (size_t)width * height * 6;
+    DevBuf d, st;
+    I360B_TRY(d.alloc(b, s, "ApplyReinhardColorTransfer"));
+    I360B_TRY(st.alloc(12 * sizeof(double), s, "ApplyReinhardColorTransfer"));
+    const double h[12] = {srcMean[0], srcMean[1], srcMean[2], srcStd[0], srcStd[1], srcStd[2],
+                          refMean[0], refMean[1], refMean[2], refStd[0], refStd[1], refStd[2]};
+    I360B_CUDA(cudaMemcpyAsync(st.p, h, sizeof(h), cudaMemcpyHostToDevice, s), "ApplyReinhardColorTransfer upload");
+    I360B_CUDA(cudaMemcpyAsync(d.p, rgbInOut, b, cudaMemcpyHostToDevice, s), "ApplyReinhardColorTransfer upload");
+    unsigned short* img = d.as<unsigned short>();
+    I360B_TRY(launch_reinhard(&img, &width, &height, 1, st.as<double>(), st.as<double>() + 6, s));
+    I360B_CUDA(cudaMemcpyAsync(rgbInOut, d.p, b, cudaMemcpyDeviceToHost, s), "ApplyReinhardColorTransfer download");
+    return sync(s, "ApplyReinhardColorTransfer");
+}
+
 extern "C" int i360b_demosaic_bayer(const unsigned short* cfaData, int width, int height, unsigned short blackLevel,
                                     const float camMul[4], const float rgbCam[12], uint32_t filters,
                                     unsigned short* rgbOut)
@@ -216,6 +270,30 @@ extern "C" int i360b_launch_gain(unsigned short* dData, int numValues, float gai
     if (!dData) return fail(I360B_INVALID_PARAM, "Null pointer argument.");
     if (numValues <= 0) return fail(I360B_INVALID_PARAM, "Invalid pixel count.");
     return launch_gain(dData, numValues, gain, static_cast<cudaStream_t>(stream));
+}
+
+extern "C" int i360b_launch_lab_stats(const unsigned short* const* dImages, const int* widths, const int* heights,
+                                      int n, double* dStats, void* stream)
+{
+    clear_error();
+    I360B_TRY(require_init());
+    return launch_lab_stats(dImages, widths, heights, n, dStats, static_cast<cudaStream_t>(stream));
+}
+
+extern "C" int i360b_launch_reinhard(unsigned short* const* dImages, const int* widths, const int* heights, int n,
+                                     const double* dSrcStats, const double* dRefStats, void* stream)
+{
+    clear_error();
+    I360B_TRY(require_init());
+    return launch_reinhard(dImages, widths, heights, n, dSrcStats, dRefStats, static_cast<cudaStream_t>(stream));
+}
+
+extern "C" int i360b_launch_color_correct(unsigned short* const* dImages, const int* widths, const int* heights,
+                                          int n, int refIndex, double* dStats, void* stream)
+{
+    clear_error();
+    I360B_TRY(require_init());
+    return launch_color_correct(dImages, widths, heights, n, refIndex, dStats, static_cast<cudaStream_t>(stream));
 }
 
 extern "C" int i360b_launch_blend(const unsigned short* const* dWarped, int numContributors, int width, int height,

@@ -89,6 +89,13 @@ int launch_warp(const unsigned short* src, int sw, int sh, unsigned short* dst, 
 int launch_median(const unsigned short* const* inputs, int n, unsigned short* out, int w, int h, float sigma,
                   cudaStream_t s);
 int launch_gain(unsigned short* data, long long n, float gain, cudaStream_t s);
+// Lab statistics / Reinhard transfer / frame-set colour correction (color.cu).
+int launch_lab_stats(const unsigned short* const* dImgs, const int* w, const int* h, int n, double* dStats,
+                     cudaStream_t s);
+int launch_reinhard(unsigned short* const* dImgs, const int* w, const int* h, int n, const double* dSrcStats,
+                    const double* dRefStats, cudaStream_t s);
+int launch_color_correct(unsigned short* const* dImgs, const int* w, const int* h, int n, int refIndex,
+                         double* dStats, cudaStream_t s);
 int launch_blend_chunk(const unsigned short* const* warped, int k, int w, int h, int bands, unsigned short* out,
                        cudaStream_t s);
 // The same blend with all device scratch carved from a caller-provided buffer

@@ -101,6 +101,24 @@ I360B_API int i360b_median_stack(const unsigned short* const* inputs, int numInp
  * unsigned shorts (RenderExecutor passes width*height*3). */
 I360B_API int i360b_apply_gain(unsigned short* data, int numPixels, float gain);
 
+/* IComputeBackend::ComputeLabStats (IComputeBackend.h:65-67; CPU semantics
+ * GainColorOps.cpp:103-130): mean and standard deviation of CIE L, a, b over
+ * an RGB48 image (sRGB 16-bit -> linear -> XYZ -> Lab per pixel).  The
+ * per-pixel conversion is the reference's FP32 arithmetic with correctly
+ * rounded powers and cube roots, the sums are FP64 (reduction order differs
+ * from the reference's sequential loop, so results agree to FP64 rounding). */
+I360B_API int i360b_compute_lab_stats(const unsigned short* rgb, int width, int height, double outMean[3],
+                                      double outStd[3]);
+
+/* IComputeBackend::ApplyReinhardColorTransfer (IComputeBackend.h:69-73; CPU
+ * semantics GainColorOps.cpp:132-156): in place, Lab of each pixel mapped to
+ * (lab - srcMean) * (refStd / srcStd) + refMean (srcStd <= 1e-6 taken as 1)
+ * and back to RGB48.  Outputs agree with the reference within 1 LSB (its libm
+ * powf/cbrtf are not correctly rounded). */
+I360B_API int i360b_apply_reinhard_color_transfer(unsigned short* rgbInOut, int width, int height,
+                                                  const double srcMean[3], const double srcStd[3],
+                                                  const double refMean[3], const double refStd[3]);
+
 /* IComputeBackend::DemosaicBayer (IComputeBackend.h:46-49).  rgbCam is the
  * 3x4 matrix as 12 floats, row-major. */
 I360B_API int i360b_demosaic_bayer(const unsigned short* cfaData, int width, int height, unsigned short blackLevel,
@@ -135,6 +153,28 @@ I360B_API int i360b_launch_median(const unsigned short* const* dInputs, int numI
 
 /* ApplyGain on a device buffer. */
 I360B_API int i360b_launch_gain(unsigned short* dData, int numValues, float gain, void* stream);
+
+/* ComputeLabStats of n device RGB48 images in one pass (dImages, widths and
+ * heights are HOST arrays, n <= 64).  dStats: DEVICE array of n * 6 doubles,
+ * per image {mean L, a, b, std L, a, b}. */
+I360B_API int i360b_launch_lab_stats(const unsigned short* const* dImages, const int* widths, const int* heights,
+                                     int n, double* dStats, void* stream);
+
+/* ApplyReinhardColorTransfer of n device RGB48 images in place, image i from
+ * its statistics dSrcStats[i * 6 ..] to dRefStats[0 .. 5] (DEVICE arrays in
+ * the i360b_launch_lab_stats layout). */
+I360B_API int i360b_launch_reinhard(unsigned short* const* dImages, const int* widths, const int* heights, int n,
+                                    const double* dSrcStats, const double* dRefStats, void* stream);
+
+/* The Optimize stage's colour correction of a frame set on the device
+ * (OptimizeExecutor.cpp:283-330): the Lab statistics of all n frames in one
+ * pass, then every frame except frames[refIndex] transferred in place to the
+ * reference frame's statistics in a second pass, with no host round trip.
+ * The reference frame passes through unchanged, as there.  dStats (optional,
+ * DEVICE, n * 6 doubles) receives the statistics measured before the
+ * transfer. */
+I360B_API int i360b_launch_color_correct(unsigned short* const* dImages, const int* widths, const int* heights,
+                                         int n, int refIndex, double* dStats, void* stream);
 
 /* Seam blend of one chunk whose K warped buffers are already on the device
  * (dWarped is a HOST array of K device pointers). */

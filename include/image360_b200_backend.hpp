@@ -116,14 +116,17 @@ namespace WindowsApp { namespace Compute
         {
             return R(i360b_not_supported("MatchFeatures"));
         }
-        ComputeResult ComputeLabStats(const unsigned short*, int, int, double[3], double[3]) override
+        ComputeResult ComputeLabStats(const unsigned short* rgb, int width, int height, double outMean[3],
+                                      double outStd[3]) override
         {
-            return R(i360b_not_supported("ComputeLabStats"));
+            return R(i360b_compute_lab_stats(rgb, width, height, outMean, outStd));
         }
-        ComputeResult ApplyReinhardColorTransfer(unsigned short*, int, int, const double[3], const double[3],
-                                                 const double[3], const double[3]) override
+        ComputeResult ApplyReinhardColorTransfer(unsigned short* rgbInOut, int width, int height,
+                                                 const double srcMean[3], const double srcStd[3],
+                                                 const double refMean[3], const double refStd[3]) override
         {
-            return R(i360b_not_supported("ApplyReinhardColorTransfer"));
+            return R(i360b_apply_reinhard_color_transfer(rgbInOut, width, height, srcMean, srcStd, refMean,
+                                                         refStd));
         }
         ComputeResult BlockMatchAlign(const unsigned short*, const unsigned short*, int, int, int, int, TileOffset*,
                                       int, int) override

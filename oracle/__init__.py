@@ -100,6 +100,15 @@ class _Oracle:
         ok = self.lib.or_invert_h(_p(H, _f32p), _p(out, _f32p))
         return (out if ok else None)
 
+    def lab_stats(self, rgb, f64=False):
+        """(mean[3], std[3]) of CIE L, a, b over an (h, w, 3) image."""
+        return _lab_stats(self.lib.or_lab_stats_f64 if f64 else self.lib.or_lab_stats, rgb)
+
+    def reinhard(self, rgb, src_mean, src_std, ref_mean, ref_std, f64=False):
+        """Reinhard transfer of a copy of ``rgb``."""
+        return _reinhard(self.lib.or_reinhard_f64 if f64 else self.lib.or_reinhard, rgb, src_mean, src_std,
+                         ref_mean, ref_std)
+
     def coverage(self, img):
         img = np.ascontiguousarray(img, np.uint16)
         h, w = img.shape[:2]
@@ -158,6 +167,20 @@ class _Oracle:
         """tiles: list of (x, y, w, h, [frame indices]). Returns (seconds, outputs)."""
         return _render_tiles(self.lib.or_render_tiles, None, threads, frames, inv_h, gains, tiles, bands,
                              want_out)
+
+
+def _lab_stats(fn, rgb):
+    rgb = np.ascontiguousarray(rgb, np.uint16)
+    mean, std = np.zeros(3), np.zeros(3)
+    fn(_p(rgb, _u16p), rgb.shape[1], rgb.shape[0], _p(mean, _f64p), _p(std, _f64p))
+    return mean, std
+
+
+def _reinhard(fn, rgb, src_mean, src_std, ref_mean, ref_std):
+    out = np.array(rgb, np.uint16, copy=True, order="C")
+    a = [np.ascontiguousarray(v, np.float64).reshape(3) for v in (src_mean, src_std, ref_mean, ref_std)]
+    fn(_p(out, _u16p), out.shape[1], out.shape[0], *[_p(v, _f64p) for v in a])
+    return out
 
 
 def _render_tiles(fn, tier, threads, frames, inv_h, gains, tiles, bands, want_out):
@@ -238,6 +261,12 @@ class _Reference:
         out = np.zeros(9, np.float32)
         ok = self.lib.ref_invert_h(_p(H, _f32p), _p(out, _f32p))
         return (out if ok else None)
+
+    def lab_stats(self, rgb):
+        return _lab_stats(self.lib.ref_lab_stats, rgb)
+
+    def reinhard(self, rgb, src_mean, src_std, ref_mean, ref_std):
+        return _reinhard(self.lib.ref_reinhard, rgb, src_mean, src_std, ref_mean, ref_std)
 
     def coverage_distance(self, cov):
         cov = np.ascontiguousarray(cov, np.uint8)

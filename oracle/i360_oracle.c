@@ -275,6 +275,201 @@ void or_gain(uint16_t* data, int n, float gain)
     for (int i = 0; i < n; ++i) data[i] = clamp_trunc_u16((float)data[i] * gain);
 }
 
+/* ------------------------------------------------------------------------ */
+/* Lab statistics and Reinhard colour transfer: GainColorOps.cpp:28-156.      */
+/* FP32 per pixel, FP64 sums and transfer; libm powf/cbrtf as the reference.  */
+/* ------------------------------------------------------------------------ */
+#define LAB_DELTA (6.0f / 29.0f)
+
+static float lab_decode(float c) /* GainColorOps.cpp:30-33 */
+{
+    if (c <= 0.04045f) return c / 12.92f;
+    return powf((c + 0.055f) / 1.055f, 2.4f);
+}
+
+static float lab_encode(float c) /* GainColorOps.cpp:35-38 */
+{
+    if (c <= 0.0031308f) return c * 12.92f;
+    return 1.055f * powf(c, 1.0f / 2.4f) - 0.055f;
+}
+
+static float lab_fwd(float t) /* GainColorOps.cpp:40-44 */
+{
+    const float d = LAB_DELTA;
+    if (t > d * d * d) return cbrtf(t);
+    return t / (3.0f * d * d) + 4.0f / 29.0f;
+}
+
+static float lab_inv(float t) /* GainColorOps.cpp:46-50 */
+{
+    const float d = LAB_DELTA;
+    if (t > d) return t * t * t;
+    return 3.0f * d * d * (t - 4.0f / 29.0f);
+}
+
+static void lab_of_pixel(const uint16_t* px, float* lab) /* GainColorOps.cpp:56-73 */
+{
+    float r = lab_decode(px[0] / 65535.0f);
+    float g = lab_decode(px[1] / 65535.0f);
+    float b = lab_decode(px[2] / 65535.0f);
+    float X = 0.4124564f * r + 0.3575761f * g + 0.1804375f * b;
+    float Y = 0.2126729f * r + 0.7151522f * g + 0.0721750f * b;
+    float Z = 0.0193339f * r + 0.1191920f * g + 0.9503041f * b;
+    float fx = lab_fwd(X / 0.95047f);
+    float fy = lab_fwd(Y / 1.0f);
+    float fz = lab_fwd(Z / 1.08883f);
+    lab[0] = 116.0f * fy - 16.0f;
+    lab[1] = 500.0f * (fx - fy);
+    lab[2] = 200.0f * (fy - fz);
+}
+
+static void pixel_of_lab(const float* lab, uint16_t* px) /* GainColorOps.cpp:75-100 */
+{
+    float fy = (lab[0] + 16.0f) / 116.0f;
+    float fx = fy + lab[1] / 500.0f;
+    float fz = fy - lab[2] / 200.0f;
+    float X = 0.95047f * lab_inv(fx);
+    float Y = 1.0f * lab_inv(fy);
+    float Z = 1.08883f * lab_inv(fz);
+    float lin[3];
+    lin[0] = 3.2404542f * X - 1.5371385f * Y - 0.4985314f * Z;
+    lin[1] = -0.9692660f * X + 1.8760108f * Y + 0.0415560f * Z;
+    lin[2] = 0.0556434f * X - 0.2040259f * Y + 1.0572252f * Z;
+    for (int c = 0; c < 3; ++c)
+    {
+        float v = lin[c] < 0.0f ? 0.0f : lin[c]; /* a NaN stays NaN, as (std::max)(v, 0.0f) */
+        px[c] = clamp_trunc_u16(lab_encode(v) * 65535.0f);
+    }
+}
+
+void or_lab_stats(const uint16_t* rgb, int w, int h, double* mean3, double* std3)
+{
+    if (!rgb || !mean3 || !std3 || w <= 0 || h <= 0) return;
+    const long long n = (long long)w * h;
+    double sum[3] = {0.0, 0.0, 0.0}, sq[3] = {0.0, 0.0, 0.0};
+    for (long long i = 0; i < n; ++i)
+    {
+        float lab[3];
+        lab_of_pixel(rgb + i * 3, lab);
+        for (int c = 0; c < 3; ++c)
+        {
+            double v = (double)lab[c];
+            sum[c] += v;
+            sq[c] += v * v;
+        }
+    }
+    for (int c = 0; c < 3; ++c)
+    {
+        double m = sum[c] / (double)n;
+        double var = sq[c] / (double)n - m * m;
+        mean3[c] = m;
+        std3[c] = sqrt(var > 0.0 ? var : 0.0);
+    }
+}
+
+void or_reinhard(uint16_t* rgb, int w, int h, const double* srcMean, const double* srcStd,
+                 const double* refMean, const double* refStd)
+{
+    if (!rgb || !srcMean || !srcStd || !refMean || !refStd || w <= 0 || h <= 0) return;
+    const long long n = (long long)w * h;
+    for (long long i = 0; i < n; ++i)
+    {
+        uint16_t* px = rgb + i * 3;
+        float lab[3];
+        lab_of_pixel(px, lab);
+        for (int c = 0; c < 3; ++c)
+        {
+            double s = srcStd[c] > 1e-6 ? srcStd[c] : 1.0;
+            lab[c] = (float)(((double)lab[c] - srcMean[c]) * (refStd[c] / s) + refMean[c]);
+        }
+        pixel_of_lab(lab, px);
+    }
+}
+
+/* FP64 restatement of the same conversions (exact powers and cube roots in
+ * double), quantised only at the RGB48 output, for error reporting. */
+static double lab_fwd_d(double t)
+{
+    const double d = 6.0 / 29.0;
+    return t > d * d * d ? cbrt(t) : t / (3.0 * d * d) + 4.0 / 29.0;
+}
+
+static double lab_inv_d(double t)
+{
+    const double d = 6.0 / 29.0;
+    return t > d ? t * t * t : 3.0 * d * d * (t - 4.0 / 29.0);
+}
+
+static void lab_of_pixel_d(const uint16_t* px, double* lab)
+{
+    double lin[3];
+    for (int c = 0; c < 3; ++c)
+    {
+        double v = px[c] / 65535.0;
+        lin[c] = v <= 0.04045 ? v / 12.92 : pow((v + 0.055) / 1.055, 2.4);
+    }
+    double X = 0.4124564 * lin[0] + 0.3575761 * lin[1] + 0.1804375 * lin[2];
+    double Y = 0.2126729 * lin[0] + 0.7151522 * lin[1] + 0.0721750 * lin[2];
+    double Z = 0.0193339 * lin[0] + 0.1191920 * lin[1] + 0.9503041 * lin[2];
+    double fx = lab_fwd_d(X / 0.95047), fy = lab_fwd_d(Y), fz = lab_fwd_d(Z / 1.08883);
+    lab[0] = 116.0 * fy - 16.0;
+    lab[1] = 500.0 * (fx - fy);
+    lab[2] = 200.0 * (fy - fz);
+}
+
+void or_lab_stats_f64(const uint16_t* rgb, int w, int h, double* mean3, double* std3)
+{
+    if (!rgb || !mean3 || !std3 || w <= 0 || h <= 0) return;
+    const long long n = (long long)w * h;
+    double sum[3] = {0.0, 0.0, 0.0}, sq[3] = {0.0, 0.0, 0.0};
+    for (long long i = 0; i < n; ++i)
+    {
+        double lab[3];
+        lab_of_pixel_d(rgb + i * 3, lab);
+        for (int c = 0; c < 3; ++c)
+        {
+            sum[c] += lab[c];
+            sq[c] += lab[c] * lab[c];
+        }
+    }
+    for (int c = 0; c < 3; ++c)
+    {
+        double m = sum[c] / (double)n;
+        double var = sq[c] / (double)n - m * m;
+        mean3[c] = m;
+        std3[c] = sqrt(var > 0.0 ? var : 0.0);
+    }
+}
+
+void or_reinhard_f64(uint16_t* rgb, int w, int h, const double* srcMean, const double* srcStd,
+                     const double* refMean, const double* refStd)
+{
+    if (!rgb || !srcMean || !srcStd || !refMean || !refStd || w <= 0 || h <= 0) return;
+    const long long n = (long long)w * h;
+    for (long long i = 0; i < n; ++i)
+    {
+        uint16_t* px = rgb + i * 3;
+        double lab[3];
+        lab_of_pixel_d(px, lab);
+        for (int c = 0; c < 3; ++c)
+        {
+            double s = srcStd[c] > 1e-6 ? srcStd[c] : 1.0;
+            lab[c] = (lab[c] - srcMean[c]) * (refStd[c] / s) + refMean[c];
+        }
+        double fy = (lab[0] + 16.0) / 116.0, fx = fy + lab[1] / 500.0, fz = fy - lab[2] / 200.0;
+        double X = 0.95047 * lab_inv_d(fx), Y = lab_inv_d(fy), Z = 1.08883 * lab_inv_d(fz);
+        double lin[3] = {3.2404542 * X - 1.5371385 * Y - 0.4985314 * Z,
+                         -0.9692660 * X + 1.8760108 * Y + 0.0415560 * Z,
+                         0.0556434 * X - 0.2040259 * Y + 1.0572252 * Z};
+        for (int c = 0; c < 3; ++c)
+        {
+            double v = lin[c] < 0.0 ? 0.0 : lin[c];
+            double e = v <= 0.0031308 ? v * 12.92 : 1.055 * pow(v, 1.0 / 2.4) - 0.055;
+            px[c] = clamp_trunc_u16_d(e * 65535.0);
+        }
+    }
+}
+
 int or_invert_h(const float* m, float* out)
 {
     if (!m || !out) return 0;

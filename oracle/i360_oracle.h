@@ -33,6 +33,14 @@ void or_median(const uint16_t* const* inputs, int n, uint16_t* out, int w, int h
 /* GainColorOps.cpp:16-26 (in place). */
 void or_gain(uint16_t* data, int n, float gain);
 
+/* GainColorOps.cpp:103-130: mean and standard deviation of CIE L, a, b over an
+ * RGB48 image (per-pixel conversion GainColorOps.cpp:56-73). */
+void or_lab_stats(const uint16_t* rgb, int w, int h, double* mean3, double* std3);
+
+/* GainColorOps.cpp:132-156 (in place; back conversion GainColorOps.cpp:75-100). */
+void or_reinhard(uint16_t* rgb, int w, int h, const double* srcMean, const double* srcStd,
+                 const double* refMean, const double* refStd);
+
 /* HomographyMath.cpp:94-116.  Returns 1 on success, 0 when singular. */
 int or_invert_h(const float* h, float* out);
 
@@ -76,6 +84,9 @@ void or_warp_f64(const uint16_t* src, int sw, int sh, uint16_t* dst, int dw, int
                  const double* invH, int offX, int offY);
 void or_compose_f64(const uint16_t* const* bufs, const int32_t* owner, int k, int w, int h, int bands,
                     uint16_t* out);
+void or_lab_stats_f64(const uint16_t* rgb, int w, int h, double* mean3, double* std3);
+void or_reinhard_f64(uint16_t* rgb, int w, int h, const double* srcMean, const double* srcStd,
+                     const double* refMean, const double* refStd);
 
 /* Render a list of output tiles the way RenderExecutor::Execute does per chunk
  * (RenderExecutor.cpp:70-140): warp each contributor with its dst->src matrix,

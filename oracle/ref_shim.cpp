@@ -126,6 +126,17 @@ extern "C"
     // ApplyGainCpu (GainColorOps.cpp:16-26).
     void ref_gain(uint16_t* data, int n, float gain) { ApplyGainCpu(data, n, gain); }
 
+    // GainColorOps.cpp:103-130 / 132-156.
+    void ref_lab_stats(const uint16_t* rgb, int w, int h, double* mean, double* sd)
+    {
+        ComputeLabStatsCpu(rgb, w, h, mean, sd);
+    }
+    void ref_reinhard(uint16_t* rgb, int w, int h, const double* sm, const double* ss, const double* rm,
+                      const double* rs)
+    {
+        ApplyReinhardColorTransferCpu(rgb, w, h, sm, ss, rm, rs);
+    }
+
     // InvertHomography3x3 (HomographyMath.cpp:94-116).
     int ref_invert_h(const float* h, float* out) { return InvertHomography3x3(h, out) ? 1 : 0; }
 

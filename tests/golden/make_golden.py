@@ -20,6 +20,10 @@ Contents (all outputs are the reference's scalar tier unless named *_avx):
                   reference's per-tile render (warp, gain, seam blend)
   c2s_*           median stack of 16 aligned 14-bit frames with 5% transient
                   outlier rectangles
+  ct_*            Lab statistics (ComputeLabStatsCpu) and Reinhard transfer
+                  (ApplyReinhardColorTransferCpu) of two demosaiced c1s frame
+                  crops (target -> reference), a full-range random image and a
+                  flat image (zero standard deviation)
 """
 from __future__ import annotations
 
@@ -154,6 +158,19 @@ def main():
     # sumSq multiply-add into an FMA, so on 14-bit data they can pick a
     # different clip set than the scalar tier on a few values; kept for record.
     g["c2s_out_avx"] = R.median(frames, 2.0, tier=R.tier)
+    # colour correction (GainColorOps.cpp:103-156)
+    tgt = np.ascontiguousarray(g["c1s_frames"][1][:48, :64])
+    ref = np.ascontiguousarray(g["c1s_frames"][0][:48, :64])
+    rng = np.random.default_rng(8080)
+    rand = rng.integers(0, 65536, (24, 32, 3)).astype(np.uint16)
+    flat = np.full((8, 8, 3), (31000, 12000, 5000), np.uint16)
+    rm, rs = R.lab_stats(ref)
+    g["ct_target"], g["ct_ref"], g["ct_rand"], g["ct_flat"] = tgt, ref, rand, flat
+    g["ct_ref_stats"] = np.concatenate([rm, rs])
+    for name, img in (("target", tgt), ("rand", rand), ("flat", flat)):
+        m, sd = R.lab_stats(img)
+        g[f"ct_{name}_stats"] = np.concatenate([m, sd])
+        g[f"ct_{name}_out"] = R.reinhard(img, m, sd, rm, rs)
     np.savez_compressed(OUT, **g)
     print(OUT, os.path.getsize(OUT), "bytes")
 

@@ -70,3 +70,14 @@ def test_median_with_outliers(oracle_c):
     g = golden()
     out = oracle_c.median(list(g["c2s_in"]), 2.0)
     assert np.array_equal(out, g["c2s_out"])
+
+
+@pytest.mark.parametrize("name", ["target", "rand", "flat"])
+def test_color_transfer(oracle_c, name):
+    g = golden()
+    img = g[f"ct_{name}"]
+    mean, std = oracle_c.lab_stats(img)
+    assert np.array_equal(np.concatenate([mean, std]), g[f"ct_{name}_stats"])
+    ref = g["ct_ref_stats"]
+    out = oracle_c.reinhard(img, mean, std, ref[:3], ref[3:])
+    assert np.array_equal(out, g[f"ct_{name}_out"])

@@ -91,3 +91,18 @@ def test_blend_empty(oracle_c, reference):
     z = np.zeros((10, 12, 3), np.uint16)
     assert not oracle_c.blend([z, z], 5).any()
     assert not reference.blend([z, z]).any()
+
+
+@pytest.mark.parametrize("seed", range(6))
+def test_lab_stats_and_reinhard(oracle_c, reference, seed):
+    rng = np.random.default_rng(900 + seed)
+    w, h = (int(v) for v in rng.integers(1, 90, 2))
+    hi = [65536, 16384, 4096, 65536, 2, 65536][seed]
+    img = rng.integers(0, hi, (h, w, 3), dtype=np.uint16)
+    ref = rng.integers(0, 65536, (17, 13, 3), dtype=np.uint16)
+    m, s = oracle_c.lab_stats(img)
+    rm, rs = reference.lab_stats(ref)
+    assert np.array_equal(np.concatenate([m, s]), np.concatenate(reference.lab_stats(img)))
+    if seed == 5:
+        s = np.array([0.0, 1e-7, 3.0])  # the srcStd <= 1e-6 rule
+    assert np.array_equal(oracle_c.reinhard(img, m, s, rm, rs), reference.reinhard(img, m, s, rm, rs))
