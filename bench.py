@@ -305,6 +305,8 @@ def run_ours(args, rank, world, local_rank):
         line["learned"] = lr
         line["config"]["blend"] = ("plain seam blend (value); learned blend measured in 'learned' "
                                    "(same frames, 256x256 overlap windows, judged per window at 45 dB)")
+    if not args.no_color:
+        line["color_correct"] = run_color(args, S, stream)
     if not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(S, args)
     return line
@@ -585,6 +587,93 @@ def cpu_baseline(S, args):
             "sample": desc, "sample_seconds": round(spent, 1), "threads_model": "hardware_concurrency()-1 tasks"}
 
 
+def run_color(args, S, stream):
+    """Optimize-stage colour correction of the step's 24 frames, timed alone
+    (OptimizeExecutor.cpp:283-330: Lab statistics of the reference and each
+    target frame, then the Reinhard transfer of every target in place):
+    i360b_launch_color_correct on copies of the demosaiced frames, restored
+    before every step outside the timed events (inputs far larger than L2),
+    with frame 0 as the reference."""
+    import torch
+    be, cfg = S["be"], S["cfg"]
+    sp = stream.cuda_stream
+    n, w, h = len(S["rgb"]), cfg.frame_w, cfg.frame_h
+    work = [torch.empty_like(r) for r in S["rgb"]]
+    ptrs = [t.data_ptr() for t in work]
+    stats = torch.zeros(n * 6, dtype=torch.float64, device=work[0].device)
+    times, stat_times = [], []
+    with torch.cuda.stream(stream):
+        for i in range(args.warmup + args.steps):
+            for a, b in zip(work, S["rgb"]):
+                a.copy_(b)
+            e = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
+            e[0].record(stream)
+            assert be.launch_lab_stats(ptrs, [w] * n, [h] * n, stats.data_ptr(), sp) == 0, be.get_last_error()
+            e[1].record(stream)
+            e[2].record(stream)
+            assert be.launch_color_correct(ptrs, [w] * n, [h] * n, 0, stats.data_ptr(), sp) == 0, be.get_last_error()
+            e[3].record(stream)
+            if i >= args.warmup:
+                times.append(e[2:])
+                stat_times.append(e[:2])
+    torch.cuda.synchronize()
+    ms = float(np.mean([a.elapsed_time(b) for a, b in times]))
+    ms_stats = float(np.mean([a.elapsed_time(b) for a, b in stat_times]))
+    px = n * w * h
+    alg = px * 6 + (n - 1) * w * h * 12  # statistics read every frame; transfer reads and writes each target
+    peaks, kind = measured_peaks()
+    gbps = alg / (ms / 1e3) / 1e9
+    tr_ms = ms - ms_stats
+    tr_gbps = (n - 1) * w * h * 12 / (tr_ms / 1e3) / 1e9
+    out = {"value": round(px / 1e6 / (ms / 1e3), 1), "unit": "frame Mpix/s", "ms_per_step": round(ms, 3),
+           "frames": n, "frame": f"{w}x{h}", "reference_frame": 0, "gpu_launches_per_step": 3,
+           "stats_ms": round(ms_stats, 3), "transfer_ms": round(tr_ms, 3),
+           "roofline": {"kernel": "k_lab_partials + k_reinhard", "bound": "issue (correctly rounded FP32 powers and cube roots)",
+                        "achieved": round(gbps, 1), "peak": peaks["hbm_gbs"], "unit": "GB/s",
+                        "frac": round(gbps / peaks["hbm_gbs"], 4), "algorithmic_bytes": alg,
+                        "transfer_GBps": round(tr_gbps, 1), "peak_source": kind + " (hbm_gbs, burst copy)"}}
+    if not args.no_cpu_baseline:
+        out["cpu_baseline"] = cpu_color_baseline(S, n, w, h)
+    return out
+
+
+def cpu_color_baseline(S, n, w, h):
+    """The reference's per-image colour task (OptimizeExecutor.cpp:308-327:
+    ComputeLabStats of the reference, of the target, ApplyReinhardColorTransfer
+    of the target) on hardware_concurrency()-1 host threads, on row strips of
+    the frames, extrapolated to the n-1 targets of the frame set."""
+    import ctypes as ct
+    from concurrent.futures import ThreadPoolExecutor
+
+    import oracle
+    impl, kind = _cpu_impl()
+    stats_fn = impl.lib.ref_lab_stats if kind == "reference" else impl.lib.or_lab_stats
+    tr_fn = impl.lib.ref_reinhard if kind == "reference" else impl.lib.or_reinhard
+    threads = max(1, (os.cpu_count() or 2) - 1)
+    rows = max(1, h // 16)
+    ref = np.ascontiguousarray(S["rgb"][0][:rows].cpu().numpy().view(np.uint16))
+    tgts = [np.ascontiguousarray(S["rgb"][1 + k % (n - 1)][rows * (k // (n - 1)):][:rows].cpu().numpy().view(np.uint16))
+            for k in range(threads)]
+    d = lambda a: a.ctypes.data_as(oracle._f64p)
+
+    def task(t):
+        rm, rs, tm, ts = (np.zeros(3) for _ in range(4))
+        stats_fn(ref.ctypes.data_as(oracle._u16p), w, rows, d(rm), d(rs))
+        stats_fn(t.ctypes.data_as(oracle._u16p), w, t.shape[0], d(tm), d(ts))
+        tr_fn(t.ctypes.data_as(oracle._u16p), w, t.shape[0], d(tm), d(ts), d(rm), d(rs))
+
+    t0 = time.time()
+    with ThreadPoolExecutor(threads) as ex:
+        list(ex.map(task, tgts))
+    spent = time.time() - t0
+    px_s = sum(t.shape[0] * w for t in tgts) / spent  # target pixels colour-corrected per second
+    job_s = (n - 1) * w * h / px_s
+    return {"value": round(n * w * h / 1e6 / job_s, 2), "unit": "frame Mpix/s", "cores": threads, "kind": kind,
+            "sample": f"{threads} per-image tasks on {w}x{rows} strips (reference strip stats, target strip stats, "
+                      f"target transfer), extrapolated to {n - 1} targets of {w}x{h}",
+            "sample_seconds": round(spent, 2), "job_seconds": round(job_s, 2)}
+
+
 def run_reference(args, rank, world):
     """The reference's own CPU implementation of the path on this host's
     cores, on the same workload, bounded per step; rank 0 only."""
@@ -639,6 +728,7 @@ def main():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-learned", action="store_true", help="skip the learned blend")
+    ap.add_argument("--no-color", action="store_true", help="skip the colour-correction leg")
     ap.add_argument("--no-autotune", action="store_true", help="keep the plan's default band height and ring depth")
     ap.add_argument("--train-steps", type=int, default=782, help="Adam steps (782 x 64 = 50k windows)")
     ap.add_argument("--train-batch", type=int, default=64)

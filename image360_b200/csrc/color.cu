@@ -5,24 +5,36 @@
 //
 // Arithmetic follows the reference's CPU implementation (GainColorOps.cpp:28-156)
 // step by step in FP32 with every product and sum rounded separately (this file
-// is built without FMA contraction), the statistics in FP64, and the transfer
-// in FP64 before its cast back to FP32.  The transcendental steps are evaluated
-// to the correctly rounded FP32 result:
+// is built without FMA contraction) and the statistics in FP64.  The
+// reference's FP64 transfer (lab - mean) * scale + refMean is carried in
+// float-float arithmetic (hi + lo pairs, ~48 bits) and rounded once to FP32,
+// which gives the FP64 result's FP32 rounding except when that lies within
+// ~2^-48 of a rounding boundary (about 1 value in 10^7, mostly where the sum
+// cancels toward 0).  The transcendental steps are evaluated to the correctly
+// rounded FP32 result:
 //   * sRGB decode of a 16-bit code, ((c + 0.055f) / 1.055f)^2.4f
 //     (GainColorOps.cpp:30-33): a 65536-entry table, each entry the FP64 power
 //     rounded to FP32, built on the device once per process;
-//   * the cube root of LabF (GainColorOps.cpp:40-44): cbrtf refined by one
-//     Newton step y -= (y^3 - t) / (3 y^2) in FP64;
-//   * the sRGB encode power c^(1/2.4f) (GainColorOps.cpp:35-38): powf refined
-//     by one Newton step on z^12 = c^5 in FP64, times the first-order factor
-//     1 + (e - 5/12) ln c for the FP32 exponent e = 1/2.4f (|e - 5/12| ~ 1e-8).
+//   * the cube root of LabF (GainColorOps.cpp:40-44): a 2^(log2(t)/3) seed
+//     refined by one Newton step y -= (y^3 - t) / (3 y^2) whose residual
+//     y^3 - t is formed exactly from FMA product error terms, in FP32;
+//   * the sRGB encode power c^(1/2.4f) (GainColorOps.cpp:35-38): a
+//     2^(e log2 c) seed refined by one Newton step on z^12 = c^5 whose
+//     residual is formed from FMA error terms in FP32, together with the
+//     first-order factor 1 + (e - 5/12) ln c for the FP32 exponent e = 1/2.4f
+//     (|e - 5/12| ~ 1e-8), rounded once.
+// Divisions by the conversion's constants use the reciprocal and one FMA
+// residual correction, which equals IEEE division for 2^-99 <= |x| < 2^100
+// (checked for every float in that range and each divisor by
+// tests/color_arith_check.c); outside it they divide.
 // The reference's libm powf/cbrtf are within about one ulp of those values, so
 // outputs agree within 1 LSB at 16 bits, and the statistics to FP64 summation
 // order.
 //
-// Layout: RGB48 interleaved, row-major, 6 bytes per pixel.  A thread handles 8
-// consecutive pixels (three 16-byte loads) when the image base is 16-byte
-// aligned, else one pixel at a time.  The statistics are reduced per block in
+// Layout: RGB48 interleaved, row-major, 6 bytes per pixel.  When the image base
+// is 16-byte aligned a block moves chunks of 2048 pixels through shared memory
+// with 16-byte loads and stores; the remainder (and unaligned images) go one
+// pixel per thread.  The statistics are reduced per block in
 // FP64 into a partials array and summed by one block in a fixed order, so they
 // are deterministic from run to run.
 #include "common.cuh"
@@ -45,8 +57,8 @@ constexpr float kXn = 0.95047f;
 constexpr float kYn = 1.0f;
 constexpr float kZn = 1.08883f;
 constexpr float kInvGamma = 1.0f / 2.4f;
-// FP32 exponent minus 5/12, for the correction factor of the encode power.
-constexpr double kInvGammaDelta = (double)kInvGamma - 5.0 / 12.0;
+// (FP32 exponent - 5/12) ln 2: the correction of the encode power per unit of log2 c.
+constexpr float kInvGammaDeltaLn2 = (float)(((double)kInvGamma - 5.0 / 12.0) * 0.69314718055994530942);
 
 constexpr int kMaxImages = 64;   // images per batched launch
 constexpr int kThreads = 256;
@@ -67,34 +79,76 @@ __global__ void k_build_decode_table()
     g_srgbDecode[i] = v;
 }
 
-// Correctly rounded cube root for t in (kDelta3, 2].
+// x / d for the constant divisor d with r = 1.0f / d (see the header comment).
+__device__ __forceinline__ float div_const(float x, float d, float r)
+{
+    const float ax = fabsf(x);
+    if (ax >= 0x1p-99f && ax < 0x1p100f)
+    {
+        const float q = fmul(x, r);
+        return __fmaf_rn(__fmaf_rn(-q, d, x), r, q);
+    }
+    return fdiv(x, d);
+}
+
+// x / d without the range guard, for x = 0 or x >= 2^-99 (the reciprocal
+// step gives +0 for x = 0, like the division).
+__device__ __forceinline__ float div_const_nonneg(float x, float d, float r)
+{
+    const float q = fmul(x, r);
+    return __fmaf_rn(__fmaf_rn(-q, d, x), r, q);
+}
+
+constexpr float kRcpXn = 1.0f / kXn;
+constexpr float kRcpZn = 1.0f / kZn;
+constexpr float kRcpThreeDelta2 = 1.0f / kThreeDelta2;
+
+// Correctly rounded cube root for t in (kDelta3, 2]: p + pl = y^2 and
+// c + cl = p y exactly (FMA error terms), c - t is exact (Sterbenz), so the
+// residual y^3 - t carries only the rounding of the tiny pl y term.
 __device__ __forceinline__ float cbrt_rn(float t)
 {
-    const float y = cbrtf(t);
-    const double yd = y;
-    const double e = yd * yd * yd - (double)t;
-    const float step = __fdividef((float)e, 3.0f * y * y);
-    return __double2float_rn(yd - (double)step);
+    const float y = exp2f(fmul(__log2f(t), 0.333333343f));
+    const float p = fmul(y, y), pl = __fmaf_rn(y, y, -p);
+    const float c = fmul(p, y), cl = __fmaf_rn(p, y, -c);
+    const float e = fadd(fsub(c, t), __fmaf_rn(pl, y, cl));
+    return fsub(y, __fdividef(e, fmul(3.0f, p)));
 }
 
 // c^(1/2.4f) correctly rounded for c in [0.0031308, 2]; above 2 the encoded
-// value exceeds 1 and clamps to 65535 whatever its last bits.
+// value exceeds 1 and clamps to 65535 whatever its last bits.  z^12 and c^5
+// are carried as hi + lo pairs from FMA error terms; their hi parts agree to a
+// few ulp, so hi - hi is exact (Sterbenz) and the residual keeps ~2^-46.
 __device__ __forceinline__ float encode_pow_rn(float c)
 {
-    const float y0 = powf(c, kInvGamma);
-    if (!(c <= 2.0f)) return y0;
-    const double z = y0, cd = c;
-    const double z2 = z * z, z4 = z2 * z2, z12 = z4 * z4 * z4;
-    const double c2 = cd * cd, c5 = c2 * c2 * cd;
-    const float q = __fdividef((float)(z12 - c5), (float)z12);
-    const double z1 = z - z * ((double)q * (1.0 / 12.0));
-    const double corr = kInvGammaDelta * (double)__logf(c);
-    return __double2float_rn(z1 + z1 * corr);
+    const float l2 = __log2f(c);
+    const float z = exp2f(fmul(l2, kInvGamma));
+    if (!(c <= 2.0f)) return z;
+    const float z2 = fmul(z, z), z2l = __fmaf_rn(z, z, -z2);
+    const float z4 = fmul(z2, z2), z4l = fadd(__fmaf_rn(z2, z2, -z4), fmul(fmul(2.0f, z2), z2l));
+    const float z8 = fmul(z4, z4), z8l = fadd(__fmaf_rn(z4, z4, -z8), fmul(fmul(2.0f, z4), z4l));
+    const float z12 = fmul(z8, z4), z12l = fadd(__fmaf_rn(z8, z4, -z12), fadd(fmul(z8, z4l), fmul(z4, z8l)));
+    const float c2 = fmul(c, c), c2l = __fmaf_rn(c, c, -c2);
+    const float c4 = fmul(c2, c2), c4l = fadd(__fmaf_rn(c2, c2, -c4), fmul(fmul(2.0f, c2), c2l));
+    const float c5 = fmul(c4, c), c5l = fadd(__fmaf_rn(c4, c, -c5), fmul(c4l, c));
+    const float q = __fdividef(fadd(fsub(z12, c5), fsub(z12l, c5l)), z12);
+    const float corr = fsub(fmul(kInvGammaDeltaLn2, l2), fmul(q, 1.0f / 12.0f));
+    return __fmaf_rn(z, corr, z);
+}
+
+// (unsigned short) of v clamped to [0, 65535], truncated (NaN -> 0): v + 2^23
+// rounded toward zero holds trunc(v) in its low mantissa bits (no conversion
+// instruction).
+__device__ __forceinline__ unsigned short trunc_u16(float v)
+{
+    v = v > 0.0f ? v : 0.0f;
+    v = v < 65535.0f ? v : 65535.0f;
+    return (unsigned short)(__float_as_uint(__fadd_rz(v, 8388608.0f)) & 0xffffu);
 }
 
 __device__ __forceinline__ float lab_f(float t)  // GainColorOps.cpp:40-44
 {
-    return t > kDelta3 ? cbrt_rn(t) : fadd(fdiv(t, kThreeDelta2), kFourOver29);
+    return t > kDelta3 ? cbrt_rn(t) : fadd(div_const_nonneg(t, kThreeDelta2, kRcpThreeDelta2), kFourOver29);
 }
 
 __device__ __forceinline__ float lab_f_inv(float t)  // GainColorOps.cpp:46-50
@@ -121,9 +175,12 @@ __device__ __forceinline__ Lab rgb_to_lab(unsigned r16, unsigned g16, unsigned b
     const float X = fadd(fadd(fmul(0.4124564f, r), fmul(0.3575761f, g)), fmul(0.1804375f, b));
     const float Y = fadd(fadd(fmul(0.2126729f, r), fmul(0.7151522f, g)), fmul(0.0721750f, b));
     const float Z = fadd(fadd(fmul(0.0193339f, r), fmul(0.1191920f, g)), fmul(0.9503041f, b));
-    const float fx = lab_f(fdiv(X, kXn));
-    const float fy = lab_f(fdiv(Y, kYn));
-    const float fz = lab_f(fdiv(Z, kZn));
+    // X, Y, Z are 0 or at least ~2e-8 (the smallest non-zero table entry,
+    // (1 / 65535) / 12.92, times the smallest coefficient of a row), inside
+    // the unguarded division's exact range.
+    const float fx = lab_f(div_const_nonneg(X, kXn, kRcpXn));
+    const float fy = lab_f(Y);  // Y / kYn with kYn = 1 is Y exactly
+    const float fz = lab_f(div_const_nonneg(Z, kZn, kRcpZn));
     Lab o;
     o.v[0] = fsub(fmul(116.0f, fy), 16.0f);
     o.v[1] = fmul(500.0f, fsub(fx, fy));
@@ -134,11 +191,11 @@ __device__ __forceinline__ Lab rgb_to_lab(unsigned r16, unsigned g16, unsigned b
 // GainColorOps.cpp:75-100.
 __device__ __forceinline__ void lab_to_rgb(const Lab& lab, unsigned short* out)
 {
-    const float fy = fdiv(fadd(lab.v[0], 16.0f), 116.0f);
-    const float fx = fadd(fy, fdiv(lab.v[1], 500.0f));
-    const float fz = fsub(fy, fdiv(lab.v[2], 200.0f));
+    const float fy = div_const(fadd(lab.v[0], 16.0f), 116.0f, 1.0f / 116.0f);
+    const float fx = fadd(fy, div_const(lab.v[1], 500.0f, 1.0f / 500.0f));
+    const float fz = fsub(fy, div_const(lab.v[2], 200.0f, 1.0f / 200.0f));
     const float X = fmul(kXn, lab_f_inv(fx));
-    const float Y = fmul(kYn, lab_f_inv(fy));
+    const float Y = lab_f_inv(fy);  // kYn * v with kYn = 1 is v exactly
     const float Z = fmul(kZn, lab_f_inv(fz));
     const float rl = fsub(fsub(fmul(3.2404542f, X), fmul(1.5371385f, Y)), fmul(0.4985314f, Z));
     const float gl = fadd(fadd(fmul(-0.9692660f, X), fmul(1.8760108f, Y)), fmul(0.0415560f, Z));
@@ -147,9 +204,9 @@ __device__ __forceinline__ void lab_to_rgb(const Lab& lab, unsigned short* out)
     const float r = srgb_encode(rl < 0.0f ? 0.0f : rl);
     const float g = srgb_encode(gl < 0.0f ? 0.0f : gl);
     const float b = srgb_encode(bl < 0.0f ? 0.0f : bl);
-    out[0] = clamp_trunc_u16(fmul(r, 65535.0f));
-    out[1] = clamp_trunc_u16(fmul(g, 65535.0f));
-    out[2] = clamp_trunc_u16(fmul(b, 65535.0f));
+    out[0] = trunc_u16(fmul(r, 65535.0f));
+    out[1] = trunc_u16(fmul(g, 65535.0f));
+    out[2] = trunc_u16(fmul(b, 65535.0f));
 }
 
 // A batch of images, each covered by a run of blocks.
@@ -174,29 +231,24 @@ __device__ __forceinline__ int image_of_block(const ImageSet& s, int b)
     return lo;
 }
 
-// Loads 8 pixels (48 bytes) from a 16-byte aligned address.
-__device__ __forceinline__ void load8(const unsigned short* p, unsigned short* v)
+// A block's chunk of kChunkPx consecutive pixels (kChunkPx * 6 bytes) staged in
+// shared memory: loaded and stored as 16-byte words by consecutive threads,
+// processed with thread t on pixels t, t + kThreads, ... so that a warp reads 32
+// consecutive pixels.  The per-pixel code is a rolled loop, small enough for
+// the instruction cache.
+constexpr int kChunkPx = kThreads * kPixPerThread;
+constexpr int kChunkWords = kChunkPx * 6 / 16;
+
+__device__ __forceinline__ void stage_load(uint4* stage, const unsigned short* src)
 {
-    const uint4* q = reinterpret_cast<const uint4*>(p);
-    uint4 a = __ldcs(q), b = __ldcs(q + 1), c = __ldcs(q + 2);
-    const uint32_t w[12] = {a.x, a.y, a.z, a.w, b.x, b.y, b.z, b.w, c.x, c.y, c.z, c.w};
-#pragma unroll
-    for (int i = 0; i < 12; ++i)
-    {
-        v[2 * i] = (unsigned short)(w[i] & 0xffffu);
-        v[2 * i + 1] = (unsigned short)(w[i] >> 16);
-    }
+    const uint4* q = reinterpret_cast<const uint4*>(src);
+    for (int i = threadIdx.x; i < kChunkWords; i += kThreads) stage[i] = __ldcs(q + i);
 }
 
-__device__ __forceinline__ void store8(unsigned short* p, const unsigned short* v)
+__device__ __forceinline__ void stage_store(const uint4* stage, unsigned short* dst)
 {
-    uint32_t w[12];
-#pragma unroll
-    for (int i = 0; i < 12; ++i) w[i] = (uint32_t)v[2 * i] | ((uint32_t)v[2 * i + 1] << 16);
-    uint4* q = reinterpret_cast<uint4*>(p);
-    __stcs(q, make_uint4(w[0], w[1], w[2], w[3]));
-    __stcs(q + 1, make_uint4(w[4], w[5], w[6], w[7]));
-    __stcs(q + 2, make_uint4(w[8], w[9], w[10], w[11]));
+    uint4* q = reinterpret_cast<uint4*>(dst);
+    for (int i = threadIdx.x; i < kChunkWords; i += kThreads) __stcs(q + i, stage[i]);
 }
 
 __device__ __forceinline__ void accumulate(const Lab& lab, double* acc)
@@ -220,17 +272,24 @@ __global__ void __launch_bounds__(kThreads) k_lab_partials(const __grid_constant
     const unsigned short* img = set.img[im];
     const long long npx = set.pixels[im];
     double acc[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
-    const long long stride = (long long)nb * kThreads;
+    __shared__ uint4 stage[kChunkWords];
     const bool vec = (reinterpret_cast<uintptr_t>(img) & 15) == 0;
-    const long long groups = vec ? npx / kPixPerThread : 0;
-    for (long long gi = (long long)bi * kThreads + threadIdx.x; gi < groups; gi += stride)
+    const long long chunks = vec ? npx / kChunkPx : 0;
+    for (long long ch = bi; ch < chunks; ch += nb)
     {
-        unsigned short v[24];
-        load8(img + gi * 24, v);
-#pragma unroll
-        for (int p = 0; p < kPixPerThread; ++p) accumulate(rgb_to_lab(v[3 * p], v[3 * p + 1], v[3 * p + 2]), acc);
+        stage_load(stage, img + ch * kChunkPx * 3);
+        __syncthreads();
+        const unsigned short* sp = reinterpret_cast<const unsigned short*>(stage);
+#pragma unroll 1
+        for (int p = 0; p < kPixPerThread; ++p)
+        {
+            const unsigned short* q = sp + (threadIdx.x + p * kThreads) * 3;
+            accumulate(rgb_to_lab(q[0], q[1], q[2]), acc);
+        }
+        __syncthreads();
     }
-    for (long long px = groups * kPixPerThread + (long long)bi * kThreads + threadIdx.x; px < npx; px += stride)
+    const long long stride = (long long)nb * kThreads;
+    for (long long px = chunks * kChunkPx + (long long)bi * kThreads + threadIdx.x; px < npx; px += stride)
     {
         const unsigned short* q = img + px * 3;
         accumulate(rgb_to_lab(q[0], q[1], q[2]), acc);
@@ -294,10 +353,23 @@ __global__ void k_lab_finish(const __grid_constant__ ImageSet set, const double*
 
 // Per-channel transfer coefficients (GainColorOps.cpp:146-151): lab' =
 // (lab - srcMean) * (refStd / stdSrc) + refMean, stdSrc = srcStd or 1 when
-// srcStd <= 1e-6.
+// srcStd <= 1e-6, the FP64 coefficients held as float pairs hi + lo.
+struct FloatPair
+{
+    float h, l;
+};
+
+__device__ __forceinline__ FloatPair split(double x)
+{
+    FloatPair p;
+    p.h = __double2float_rn(x);
+    p.l = __double2float_rn(x - (double)p.h);
+    return p;
+}
+
 struct Transfer
 {
-    double srcMean[3], scale[3], refMean[3];
+    FloatPair srcMean[3], scale[3], refMean[3];
 };
 
 __device__ __forceinline__ Transfer make_transfer(const double* src, const double* ref)
@@ -307,20 +379,35 @@ __device__ __forceinline__ Transfer make_transfer(const double* src, const doubl
     for (int c = 0; c < 3; ++c)
     {
         const double s = src[3 + c] > 1e-6 ? src[3 + c] : 1.0;
-        t.srcMean[c] = src[c];
-        t.scale[c] = ref[3 + c] / s;
-        t.refMean[c] = ref[c];
+        t.srcMean[c] = split(src[c]);
+        t.scale[c] = split(ref[3 + c] / s);
+        t.refMean[c] = split(ref[c]);
     }
     return t;
+}
+
+// (v - m) * k + r in float-float, rounded once: two-sum for the differences
+// and sums, an FMA error term for the product.
+__device__ __forceinline__ float transfer_value(float v, const FloatPair& m, const FloatPair& k, const FloatPair& r)
+{
+    const float s = fsub(v, m.h);
+    const float sb = fsub(s, v);
+    const float se = fsub(fadd(fsub(v, fsub(s, sb)), fsub(-m.h, sb)), m.l);
+    const float dh = fadd(s, se);
+    const float dl = fsub(se, fsub(dh, s));
+    const float ph = fmul(dh, k.h);
+    const float pl = fadd(__fmaf_rn(dh, k.h, -ph), fadd(fmul(dh, k.l), fmul(dl, k.h)));
+    const float th = fadd(ph, r.h);
+    const float tb = fsub(th, ph);
+    const float te = fadd(fadd(fsub(ph, fsub(th, tb)), fsub(r.h, tb)), fadd(pl, r.l));
+    return fadd(th, te);
 }
 
 __device__ __forceinline__ void transfer_pixel(const Transfer& t, const unsigned short* in, unsigned short* out)
 {
     Lab lab = rgb_to_lab(in[0], in[1], in[2]);
 #pragma unroll
-    for (int c = 0; c < 3; ++c)
-        lab.v[c] = __double2float_rn(__dadd_rn(__dmul_rn(__dsub_rn((double)lab.v[c], t.srcMean[c]), t.scale[c]),
-                                               t.refMean[c]));
+    for (int c = 0; c < 3; ++c) lab.v[c] = transfer_value(lab.v[c], t.srcMean[c], t.scale[c], t.refMean[c]);
     lab_to_rgb(lab, out);
 }
 
@@ -335,18 +422,31 @@ __global__ void __launch_bounds__(kThreads) k_reinhard(const __grid_constant__ I
     unsigned short* img = set.img[im];
     const long long npx = set.pixels[im];
     const Transfer t = make_transfer(stats + (size_t)set.statIndex[im] * 6, refStats);
-    const long long stride = (long long)nb * kThreads;
+    __shared__ uint4 stage[kChunkWords];
     const bool vec = (reinterpret_cast<uintptr_t>(img) & 15) == 0;
-    const long long groups = vec ? npx / kPixPerThread : 0;
-    for (long long gi = (long long)bi * kThreads + threadIdx.x; gi < groups; gi += stride)
+    const long long chunks = vec ? npx / kChunkPx : 0;
+    for (long long ch = bi; ch < chunks; ch += nb)
     {
-        unsigned short v[24], o[24];
-        load8(img + gi * 24, v);
-#pragma unroll
-        for (int p = 0; p < kPixPerThread; ++p) transfer_pixel(t, v + 3 * p, o + 3 * p);
-        store8(img + gi * 24, o);
+        // each thread stores back exactly the words it loaded, so no barrier
+        // is needed between one chunk's store and the next chunk's load
+        stage_load(stage, img + ch * kChunkPx * 3);
+        __syncthreads();
+        unsigned short* sp = reinterpret_cast<unsigned short*>(stage);
+#pragma unroll 1
+        for (int p = 0; p < kPixPerThread; ++p)
+        {
+            unsigned short* q = sp + (threadIdx.x + p * kThreads) * 3;
+            unsigned short o[3];
+            transfer_pixel(t, q, o);
+            q[0] = o[0];
+            q[1] = o[1];
+            q[2] = o[2];
+        }
+        __syncthreads();
+        stage_store(stage, img + ch * kChunkPx * 3);
     }
-    for (long long px = groups * kPixPerThread + (long long)bi * kThreads + threadIdx.x; px < npx; px += stride)
+    const long long stride = (long long)nb * kThreads;
+    for (long long px = chunks * kChunkPx + (long long)bi * kThreads + threadIdx.x; px < npx; px += stride)
     {
         unsigned short o[3];
         transfer_pixel(t, img + px * 3, o);
@@ -375,13 +475,14 @@ int ensure_decode_table(cudaStream_t s)
     return I360B_SUCCESS;
 }
 
-// Blocks per image: about 4 resident 256-thread blocks per SM over the whole
-// batch, shared in proportion to pixel count, at least one per image.
-int plan_blocks(ImageSet& set)
+// Blocks per image: one wave of resident blocks (`perSm` per SM) over the
+// whole batch, shared in proportion to pixel count, at least one per image and
+// no more than the image has chunks.
+int plan_blocks(ImageSet& set, int perSm)
 {
     long long total = 0;
     for (int i = 0; i < set.n; ++i) total += set.pixels[i];
-    const long long target = (long long)sm_count() * 8;
+    const long long target = (long long)sm_count() * (perSm > 0 ? perSm : 1);
     set.blockStart[0] = 0;
     for (int i = 0; i < set.n; ++i)
     {
@@ -404,6 +505,27 @@ int check_images(unsigned short* const* imgs, const int* w, const int* h, int n)
         if (w[i] <= 0 || h[i] <= 0) return fail(I360B_INVALID_PARAM, "Invalid dimensions.");
     }
     return I360B_SUCCESS;
+}
+
+// Resident blocks per SM of a colour kernel (occupancy query, once per process).
+template <typename K>
+int resident_blocks(K kernel)
+{
+    int n = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, kernel, kThreads, 0) != cudaSuccess) n = 4;
+    return n > 0 ? n : 1;
+}
+
+int stats_blocks_per_sm()
+{
+    static const int n = resident_blocks(k_lab_partials);
+    return n;
+}
+
+int transfer_blocks_per_sm()
+{
+    static const int n = resident_blocks(k_reinhard);
+    return n;
 }
 
 ImageSet make_set(unsigned short* const* imgs, const int* w, const int* h, int n)
@@ -448,7 +570,7 @@ int launch_lab_stats(const unsigned short* const* dImgs, const int* w, const int
     if (!dStats) return fail(I360B_INVALID_PARAM, "Null pointer argument.");
     I360B_TRY(ensure_decode_table(s));
     ImageSet set = make_set(const_cast<unsigned short* const*>(dImgs), w, h, n);
-    const int blocks = plan_blocks(set);
+    const int blocks = plan_blocks(set, stats_blocks_per_sm());
     return run_stats(set, blocks, dStats, s);
 }
 
@@ -459,7 +581,7 @@ int launch_reinhard(unsigned short* const* dImgs, const int* w, const int* h, in
     if (!dSrcStats || !dRefStats) return fail(I360B_INVALID_PARAM, "Null pointer argument.");
     I360B_TRY(ensure_decode_table(s));
     ImageSet set = make_set(dImgs, w, h, n);
-    const int blocks = plan_blocks(set);
+    const int blocks = plan_blocks(set, transfer_blocks_per_sm());
     k_reinhard<<<blocks, kThreads, 0, s>>>(set, dSrcStats, dRefStats);
     return check_launch("Reinhard transfer kernel");
 }
@@ -478,7 +600,7 @@ int launch_color_correct(unsigned short* const* dImgs, const int* w, const int* 
         dStats = static_cast<double*>(own.p);
     }
     ImageSet all = make_set(dImgs, w, h, n);
-    const int blocks = plan_blocks(all);
+    const int blocks = plan_blocks(all, stats_blocks_per_sm());
     I360B_TRY(run_stats(all, blocks, dStats, s));
     if (n == 1) return I360B_SUCCESS;
     // The reference image passes through unchanged (OptimizeExecutor.cpp:290-296).
@@ -491,7 +613,7 @@ int launch_color_correct(unsigned short* const* dImgs, const int* w, const int* 
         targets.statIndex[targets.n] = i;
         ++targets.n;
     }
-    const int tblocks = plan_blocks(targets);
+    const int tblocks = plan_blocks(targets, transfer_blocks_per_sm());
     k_reinhard<<<tblocks, kThreads, 0, s>>>(targets, dStats, dStats + (size_t)refIndex * 6);
     return check_launch("Reinhard transfer kernel");
 }

@@ -4,8 +4,9 @@ The render path computes in FP32 with uint16 storage at every stage boundary,
 exactly as the reference's CPU backend does (bit-exact parity is tested
 elsewhere).  These tests report how far that FP32 arithmetic lies from the
 same algorithm carried out in FP64 - demosaic, warp (FP32 adjugate inverse
-against the exact FP64 inverse of the frame homography) and the multi-band
-compose on the same owner map - as max and mean absolute error in DN, and
+against the exact FP64 inverse of the frame homography), the multi-band
+compose on the same owner map, and the Lab/Reinhard colour transfer of one
+frame to another's statistics - as max and mean absolute error in DN, and
 bound them.  The CPU test measures the FP32 restatement; the GPU test
 measures the GPU kernels' own outputs through the C-ABI.
 
@@ -46,10 +47,13 @@ def _warp_rect(cfg, H, size=256):
     return int(px.min()) + 5, int(py.min()) + 5, size, size
 
 
-def _fp64_rows(O, cfg, pano, d32, warp32, blend32, owner):
+def _fp64_rows(O, cfg, pano, d32, warp32, blend32, owner, color32):
     black, cm, rc, filt = synth.demosaic_params(cfg)
     rows = []
     d64 = [O.demosaic(c.numpy().view(np.uint16), black, cm, rc, filt, f64=True) for c in pano.cfa[:2]]
+    tm, ts = O.lab_stats(d64[1], f64=True)
+    rm, rs = O.lab_stats(d64[0], f64=True)
+    rows.append(("colour transfer (frame 1 -> 0)", _err(color32, O.reinhard(d64[1], tm, ts, rm, rs, f64=True))))
     e = [_err(a, b) for a, b in zip(d32, d64)]
     rows.append(("demosaic", (max(x[0] for x in e), float(np.mean([x[1] for x in e])))))
     for k, (x0, y0, w, h, got) in enumerate(warp32):
@@ -79,7 +83,8 @@ def test_fp32_restatement_against_fp64(oracle_c):
         warp32.append((x0, y0, w, h, O.warp(frames[k], w, h, synth.inverse_homography_f32(pano.to_canvas[k]), x0, y0)))
     bufs = _tile_bufs(O, cfg, pano, frames)
     out, owner = O.blend(bufs, cfg.bands, return_owner=True)
-    _report(_fp64_rows(O, cfg, pano, frames[:2], warp32, (bufs, out), owner))
+    color32 = O.reinhard(frames[1], *O.lab_stats(frames[1]), *O.lab_stats(frames[0]))
+    _report(_fp64_rows(O, cfg, pano, frames[:2], warp32, (bufs, out), owner, color32))
 
 
 @pytest.mark.gpu
@@ -105,4 +110,9 @@ def test_gpu_kernels_against_fp64(backend, oracle_c):
     got = np.zeros((h, w, 3), np.uint16)
     assert backend.blend_chunk_contributors(bufs, w, h, got, cfg.bands) == 0, backend.get_last_error()
     _, owner = O.blend(bufs, cfg.bands, return_owner=True)
-    _report(_fp64_rows(O, cfg, pano, frames[:2], warp32, (bufs, got), owner))
+    rc_t, tm, ts = backend.compute_lab_stats(frames[1])
+    rc_r, rm, rs = backend.compute_lab_stats(frames[0])
+    assert rc_t == 0 and rc_r == 0, backend.get_last_error()
+    color32 = np.array(frames[1], copy=True)
+    assert backend.apply_reinhard_color_transfer(color32, tm, ts, rm, rs) == 0, backend.get_last_error()
+    _report(_fp64_rows(O, cfg, pano, frames[:2], warp32, (bufs, got), owner, color32))
