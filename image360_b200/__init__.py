@@ -31,6 +31,10 @@ COORDS_REFERENCE = 0
 COORDS_FP64_ORIGIN = 1
 
 
+CULL_REFERENCE = 0  # I360B_CULL_REFERENCE: FP32 as OverlapCulling.cpp
+CULL_FP64 = 1       # I360B_CULL_FP64
+
+
 class ComputeResult(enum.IntEnum):
     """WindowsApp::Compute::ComputeResult (ComputeTypes.h:32-50)."""
     SUCCESS = 0
@@ -109,6 +113,8 @@ def load_library(path: str = LIB_PATH):
     L.i360b_launch_lab_stats.argtypes = [ct.POINTER(vp), _i32p, _i32p, i, vp, vp]
     L.i360b_launch_reinhard.argtypes = [ct.POINTER(vp), _i32p, _i32p, i, vp, vp, vp]
     L.i360b_launch_color_correct.argtypes = [ct.POINTER(vp), _i32p, _i32p, i, i, vp, vp]
+    L.i360b_cull_tiles.argtypes = [_f32p, _i32p, _i32p, i, _i32p, i, i, _i32p, _i32p, _i32p, i, _i32p]
+    L.i360b_launch_cull_tiles.argtypes = [vp, vp, vp, i, vp, i, i, vp, vp, vp, i, vp, vp]
     L.i360b_launch_blend.argtypes = [ct.POINTER(vp), i, i, i, i, vp, vp]
     L.i360b_launch_blend_noalloc.argtypes = [ct.POINTER(vp), i, i, i, i, vp, vp]
     _lib = L
@@ -247,6 +253,30 @@ class B200ComputeBackend:
 
     def launch_gain(self, d_data: int, n: int, gain: float, stream: int = 0) -> ComputeResult:
         return ComputeResult(self.lib.i360b_launch_gain(d_data, n, gain, stream or None))
+
+    # OverlapCulling.cpp:10-115 for every tile of a panorama
+    def cull_tiles(self, homographies, widths, heights, tiles, mode: int = 0, capacity: int | None = None):
+        """(ComputeResult, first, count, contrib, total): each tile's
+        contributors in frame order, contrib[first[t]:first[t] + count[t]].
+        homographies: (n, 3, 3) frame -> canvas; tiles: (t, 4) x, y, w, h."""
+        H = np.ascontiguousarray(homographies, np.float32).reshape(-1, 9)
+        fw = np.ascontiguousarray(widths, np.int32)
+        fh = np.ascontiguousarray(heights, np.int32)
+        T = np.ascontiguousarray(tiles, np.int32).reshape(-1, 4)
+        n, t = len(fw), len(T)
+        cap = n * t if capacity is None else int(capacity)
+        first, count = np.zeros(max(1, t), np.int32), np.zeros(max(1, t), np.int32)
+        contrib, total = np.zeros(max(1, cap), np.int32), np.zeros(1, np.int32)
+        ip = lambda a: a.ctypes.data_as(ct.POINTER(ct.c_int))
+        r = self.lib.i360b_cull_tiles(_pf(H), ip(fw), ip(fh), n, ip(T), t, int(mode), ip(first), ip(count),
+                                      ip(contrib), cap, ip(total))
+        return ComputeResult(r), first[:t], count[:t], contrib[:int(total[0])], int(total[0])
+
+    def launch_cull_tiles(self, d_h: int, d_widths: int, d_heights: int, n: int, d_tiles: int, t: int, mode: int,
+                          d_first: int, d_count: int, d_contrib: int, capacity: int, d_total: int,
+                          stream: int = 0) -> ComputeResult:
+        return ComputeResult(self.lib.i360b_launch_cull_tiles(d_h, d_widths, d_heights, n, d_tiles, t, mode, d_first,
+                                                              d_count, d_contrib, capacity, d_total, stream or None))
 
     def launch_lab_stats(self, d_images, widths, heights, d_stats: int, stream: int = 0) -> ComputeResult:
         """Lab statistics of device images into d_stats (device, len * 6 doubles)."""

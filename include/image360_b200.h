@@ -202,6 +202,42 @@ I360B_API int i360b_launch_blend_noalloc(const unsigned short* const* dWarped, i
 /* One source frame: a demosaiced RGB48 image in device memory and its
  * homography from frame pixels to canvas pixels (Homography, Types.h:138-141,
  * in double).  gain is applied after the warp (RenderExecutor.cpp:111-114). */
+/* ---- tile -> contributor culling ---------------------------------------- */
+
+/* Overlap test modes of i360b_cull_tiles / i360b_launch_cull_tiles. */
+enum
+{
+    /* OverlapCulling.cpp:10-45 in FP32: decisions identical to the CPU's. */
+    I360B_CULL_REFERENCE = 0,
+    /* corners and tile bounds in FP64 (canvases beyond 2^24 pixels). */
+    I360B_CULL_FP64 = 1
+};
+
+/* The contributor list of every output tile: ImageOverlapsChunk
+ * (OverlapCulling.cpp:10-45) for every (tile, frame) pair - the box of the
+ * frame's projected corners (0,0), (W,0), (0,H), (W,H) under its frame ->
+ * canvas homography against the tile rectangle, strict inequalities - with
+ * each tile's frames listed in frame order as FindOverlappingImages builds
+ * them (OverlapCulling.cpp:47-89), and its rule that a frame of unknown size
+ * (width or height <= 0) overlaps every tile.
+ *   homographies  numFrames x 9 floats, row-major, frame -> canvas
+ *   tiles         numTiles x 4 ints: x, y, width, height
+ *   first, count  per tile: its contributors are contrib[first .. first+count)
+ *   total         contributors over all tiles.
+ * The output is the CSR form i360b_tile takes (first, count).  Host buffers;
+ * returns INVALID_PARAM when contribCapacity < *total (first, count and
+ * *total are still written, so the caller can size contrib and call again). */
+I360B_API int i360b_cull_tiles(const float* homographies, const int* frameWidths, const int* frameHeights,
+                               int numFrames, const int* tiles, int numTiles, int mode, int* first, int* count,
+                               int* contrib, int contribCapacity, int* total);
+
+/* The same on device buffers, stream-ordered (dTotal is a device int);
+ * contributors beyond contribCapacity are not written - compare *dTotal with
+ * the capacity. */
+I360B_API int i360b_launch_cull_tiles(const float* dHomographies, const int* dFrameWidths, const int* dFrameHeights,
+                                      int numFrames, const int* dTiles, int numTiles, int mode, int* dFirst,
+                                      int* dCount, int* dContrib, int contribCapacity, int* dTotal, void* stream);
+
 typedef struct i360b_frame
 {
     const unsigned short* rgb;

@@ -100,6 +100,18 @@ class _Oracle:
         ok = self.lib.or_invert_h(_p(H, _f32p), _p(out, _f32p))
         return (out if ok else None)
 
+    def overlaps(self, H, image_w, image_h, x, y, w, h, f64=False):
+        """ImageOverlapsChunk (OverlapCulling.cpp:36-71) of one frame and chunk."""
+        H = np.ascontiguousarray(H, np.float32).reshape(9)
+        fn = self.lib.or_image_overlaps_chunk_f64 if f64 else self.lib.or_image_overlaps_chunk
+        return bool(fn(_p(H, _f32p), int(image_w), int(image_h), int(x), int(y), int(w), int(h)))
+
+    def cull(self, Hs, widths, heights, tiles, f64=False):
+        """Per tile, the frames (in frame order) that overlap it; a frame of
+        unknown size (w or h <= 0) overlaps every tile (OverlapCulling.cpp:100-106)."""
+        return [[f for f, (H, fw, fh) in enumerate(zip(Hs, widths, heights))
+                 if fw <= 0 or fh <= 0 or self.overlaps(H, fw, fh, x, y, w, h, f64)] for x, y, w, h in tiles]
+
     def lab_stats(self, rgb, f64=False):
         """(mean[3], std[3]) of CIE L, a, b over an (h, w, 3) image."""
         return _lab_stats(self.lib.or_lab_stats_f64 if f64 else self.lib.or_lab_stats, rgb)
@@ -261,6 +273,17 @@ class _Reference:
         out = np.zeros(9, np.float32)
         ok = self.lib.ref_invert_h(_p(H, _f32p), _p(out, _f32p))
         return (out if ok else None)
+
+    def overlaps(self, H, image_w, image_h, x, y, w, h):
+        H = np.ascontiguousarray(H, np.float32).reshape(9)
+        return bool(self.lib.ref_image_overlaps_chunk(_p(H, _f32p), int(image_w), int(image_h), int(x), int(y),
+                                                      int(w), int(h)))
+
+    def find_overlapping_unopenable(self, n):
+        """FindOverlappingImages over n images whose files cannot be opened."""
+        ids = np.zeros(max(1, n), np.int32)
+        k = self.lib.ref_find_overlapping_unopenable(int(n), _p(ids, _i32p))
+        return list(ids[:k])
 
     def lab_stats(self, rgb):
         return _lab_stats(self.lib.ref_lab_stats, rgb)

@@ -14,6 +14,7 @@
 #define _POSIX_C_SOURCE 200809L
 #include "i360_oracle.h"
 
+#include <float.h>
 #include <math.h>
 #include <pthread.h>
 #include <stdlib.h>
@@ -468,6 +469,51 @@ void or_reinhard_f64(uint16_t* rgb, int w, int h, const double* srcMean, const d
             px[c] = clamp_trunc_u16_d(e * 65535.0);
         }
     }
+}
+
+/* ------------------------------------------------------------------------ */
+/* Overlap culling: OverlapCulling.cpp:36-71.                                 */
+/* ------------------------------------------------------------------------ */
+int or_image_overlaps_chunk(const float* m, int imageW, int imageH, int chunkX, int chunkY, int chunkW, int chunkH)
+{
+    const float cx[4] = {0.0f, (float)imageW, 0.0f, (float)imageW};
+    const float cy[4] = {0.0f, 0.0f, (float)imageH, (float)imageH};
+    float minX = FLT_MAX, minY = FLT_MAX, maxX = -FLT_MAX, maxY = -FLT_MAX;
+    for (int k = 0; k < 4; ++k)
+    {
+        float den = m[6] * cx[k] + m[7] * cy[k] + m[8];
+        if (fabsf(den) < 1e-10f) den = den >= 0.0f ? 1e-10f : -1e-10f;
+        float px = (m[0] * cx[k] + m[1] * cy[k] + m[2]) / den;
+        float py = (m[3] * cx[k] + m[4] * cy[k] + m[5]) / den;
+        if (px < minX) minX = px;
+        if (py < minY) minY = py;
+        if (maxX < px) maxX = px;
+        if (maxY < py) maxY = py;
+    }
+    float x0 = (float)chunkX, y0 = (float)chunkY;
+    float x1 = x0 + (float)chunkW, y1 = y0 + (float)chunkH;
+    return minX < x1 && maxX > x0 && minY < y1 && maxY > y0;
+}
+
+int or_image_overlaps_chunk_f64(const float* m, int imageW, int imageH, int chunkX, int chunkY, int chunkW,
+                                int chunkH)
+{
+    const double cx[4] = {0.0, (double)imageW, 0.0, (double)imageW};
+    const double cy[4] = {0.0, 0.0, (double)imageH, (double)imageH};
+    double minX = DBL_MAX, minY = DBL_MAX, maxX = -DBL_MAX, maxY = -DBL_MAX;
+    for (int k = 0; k < 4; ++k)
+    {
+        double den = (double)m[6] * cx[k] + (double)m[7] * cy[k] + (double)m[8];
+        if (fabs(den) < 1e-10) den = den >= 0.0 ? 1e-10 : -1e-10;
+        double px = ((double)m[0] * cx[k] + (double)m[1] * cy[k] + (double)m[2]) / den;
+        double py = ((double)m[3] * cx[k] + (double)m[4] * cy[k] + (double)m[5]) / den;
+        if (px < minX) minX = px;
+        if (py < minY) minY = py;
+        if (maxX < px) maxX = px;
+        if (maxY < py) maxY = py;
+    }
+    double x1 = (double)chunkX + (double)chunkW, y1 = (double)chunkY + (double)chunkH;
+    return minX < x1 && maxX > (double)chunkX && minY < y1 && maxY > (double)chunkY;
 }
 
 int or_invert_h(const float* m, float* out)

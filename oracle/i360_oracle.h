@@ -41,6 +41,13 @@ void or_lab_stats(const uint16_t* rgb, int w, int h, double* mean3, double* std3
 void or_reinhard(uint16_t* rgb, int w, int h, const double* srcMean, const double* srcStd,
                  const double* refMean, const double* refStd);
 
+/* OverlapCulling.cpp:36-71 (ImageOverlapsChunk): 1 when the box of the
+ * frame's projected corners overlaps the chunk.  f64: the FP64 form. */
+int or_image_overlaps_chunk(const float* h9, int imageW, int imageH, int chunkX, int chunkY, int chunkW,
+                            int chunkH);
+int or_image_overlaps_chunk_f64(const float* h9, int imageW, int imageH, int chunkX, int chunkY, int chunkW,
+                                int chunkH);
+
 /* HomographyMath.cpp:94-116.  Returns 1 on success, 0 when singular. */
 int or_invert_h(const float* h, float* out);
 

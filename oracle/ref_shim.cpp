@@ -20,6 +20,7 @@
 #include "HeaderFiles/GainColorOps.h"
 #include "HeaderFiles/HomographyMath.h"
 #include "HeaderFiles/SeamBlendKernels.h"
+#include "HeaderFiles/OverlapCulling.h"
 
 #include <atomic>
 #include <chrono>
@@ -125,6 +126,35 @@ extern "C"
 
     // ApplyGainCpu (GainColorOps.cpp:16-26).
     void ref_gain(uint16_t* data, int n, float gain) { ApplyGainCpu(data, n, gain); }
+
+    // OverlapCulling.cpp:36-71.
+    int ref_image_overlaps_chunk(const float* h9, int iw, int ih, int cx, int cy, int cw, int ch)
+    {
+        Homography h;
+        for (int i = 0; i < 9; ++i) h.h[i] = h9[i];
+        ChunkModel c;
+        c.x_offset = cx;
+        c.y_offset = cy;
+        c.width = cw;
+        c.height = ch;
+        return ImageOverlapsChunk(h, iw, ih, c) ? 1 : 0;
+    }
+
+    // OverlapCulling.cpp:73-115 with files that cannot be opened (the image
+    // loader is stubbed in ref_loader_stub.cpp): writes the ids returned.
+    int ref_find_overlapping_unopenable(int n, int* idsOut)
+    {
+        ChunkModel c;
+        std::vector<InputImageModel> images(n);
+        for (int i = 0; i < n; ++i)
+        {
+            images[i].id = 100 + i;
+            images[i].file_path = L"/nonexistent/frame.dng";
+        }
+        auto r = FindOverlappingImages(c, images);
+        for (size_t i = 0; i < r.size(); ++i) idsOut[i] = r[i];
+        return static_cast<int>(r.size());
+    }
 
     // GainColorOps.cpp:103-130 / 132-156.
     void ref_lab_stats(const uint16_t* rgb, int w, int h, double* mean, double* sd)

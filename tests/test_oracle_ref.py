@@ -106,3 +106,42 @@ def test_lab_stats_and_reinhard(oracle_c, reference, seed):
     if seed == 5:
         s = np.array([0.0, 1e-7, 3.0])  # the srcStd <= 1e-6 rule
     assert np.array_equal(oracle_c.reinhard(img, m, s, rm, rs), reference.reinhard(img, m, s, rm, rs))
+
+
+def _culling_cases(seed, n=200):
+    """Random frame homographies around a canvas, with near-singular rows and
+    far translations, and chunks around them."""
+    rng = np.random.default_rng(seed)
+    for _ in range(n):
+        a = rng.uniform(-0.4, 0.4)
+        s = rng.uniform(0.5, 2.0)
+        H = np.array([s * np.cos(a), -s * np.sin(a), rng.uniform(-5000, 5000),
+                      s * np.sin(a), s * np.cos(a), rng.uniform(-5000, 5000),
+                      rng.uniform(-2e-4, 2e-4), rng.uniform(-2e-4, 2e-4), rng.choice([1.0, 1e-11, -0.5])],
+                     np.float32)
+        yield (H, int(rng.integers(1, 4000)), int(rng.integers(1, 3000)), int(rng.integers(-6000, 6000)),
+               int(rng.integers(-6000, 6000)), int(rng.integers(1, 4096)), int(rng.integers(1, 4096)))
+
+
+def test_overlap_culling(oracle_c, reference):
+    n = 0
+    for H, iw, ih, x, y, w, h in _culling_cases(11):
+        assert oracle_c.overlaps(H, iw, ih, x, y, w, h) == reference.overlaps(H, iw, ih, x, y, w, h)
+        n += 1
+    assert n == 200
+
+
+def test_overlap_culling_known_answers(oracle_c, reference):
+    """The reference's own culling tests (WindowsApp.Tests/OverlapCullingTests.cpp:18-113)."""
+    eye = np.eye(3, dtype=np.float32)
+    far = np.array([[1, 0, 100000], [0, 1, 100000], [0, 0, 1]], np.float32)
+    part = np.array([[1, 0, 3500], [0, 1, 3500], [0, 0, 1]], np.float32)
+    cases = [(eye, 1000, 800, 0, 0, True), (far, 1000, 800, 0, 0, False), (part, 1000, 1000, 4000, 4000, True),
+             (eye, 1000, 1000, 1000, 0, False)]
+    for H, iw, ih, cx, cy, want in cases:
+        assert reference.overlaps(H, iw, ih, cx, cy, 4096, 4096) is want
+        assert oracle_c.overlaps(H, iw, ih, cx, cy, 4096, 4096) is want
+        assert oracle_c.overlaps(H, iw, ih, cx, cy, 4096, 4096, f64=True) is want
+    # unopenable files: sizes unknown -> both images included
+    assert reference.find_overlapping_unopenable(2) == [100, 101]
+    assert oracle_c.cull([eye, far], [0, -1], [0, 5], [(0, 0, 4096, 4096)]) == [[0, 1]]
