@@ -307,6 +307,8 @@ def run_ours(args, rank, world, local_rank):
                                    "(same frames, 256x256 overlap windows, judged per window at 45 dB)")
     if not args.no_color:
         line["color_correct"] = run_color(args, S, stream)
+    if not args.no_export:
+        line["export_preview"] = run_export(args, S, stream)
     if not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(S, args)
     return line
@@ -587,6 +589,40 @@ def cpu_baseline(S, args):
             "sample": desc, "sample_seconds": round(spent, 1), "threads_model": "hardware_concurrency()-1 tasks"}
 
 
+def run_export(args, S, stream):
+    """The panorama export that follows the render: the preview composite of
+    PanoramaExporter::ExportPreviewJpeg at the size the reference's CLI asks
+    for (cli/main.cpp: maxDimension = canvas width, so scale 1 on a wide
+    panorama) from the plan's tile outputs, timed alone with CUDA events."""
+    import torch
+    plan, pano = S["plan"], S["pano"]
+    sp = stream.cuda_stream
+    W, H = pano.canvas_w, pano.canvas_h
+    cap = W * H * 3
+    out = torch.empty(cap, dtype=torch.uint8, device=S["outs"][0].device)
+    times = []
+    with torch.cuda.stream(stream):
+        for i in range(args.warmup + args.steps):
+            e = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
+            e[0].record(stream)
+            r, ow, oh = plan.export_preview(W, H, W, out.data_ptr(), cap, sp)
+            e[1].record(stream)
+            assert r == 0, S["be"].get_last_error()
+            if i >= args.warmup:
+                times.append(e)
+    torch.cuda.synchronize()
+    ms = float(np.mean([a.elapsed_time(b) for a, b in times]))
+    px = ow * oh
+    alg = px * (6 + 3)  # one RGB48 source sample read, one RGB8 pixel written
+    peaks, kind = measured_peaks()
+    gbps = alg / (ms / 1e3) / 1e9
+    return {"value": round(px / 1e6 / (ms / 1e3), 1), "unit": "preview Mpix/s", "ms_per_step": round(ms, 3),
+            "preview": f"{ow}x{oh} RGB8 (maxDimension {W})", "gpu_launches_per_step": 2,
+            "roofline": {"kernel": "k_export_place (zero fill included)", "bound": "hbm", "achieved": round(gbps, 1),
+                         "peak": peaks["hbm_gbs"], "unit": "GB/s", "frac": round(gbps / peaks["hbm_gbs"], 4),
+                         "algorithmic_bytes": alg, "peak_source": kind + " (hbm_gbs, burst copy)"}}
+
+
 def run_color(args, S, stream):
     """Optimize-stage colour correction of the step's 24 frames, timed alone
     (OptimizeExecutor.cpp:283-330: Lab statistics of the reference and each
@@ -729,6 +765,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-learned", action="store_true", help="skip the learned blend")
     ap.add_argument("--no-color", action="store_true", help="skip the colour-correction leg")
+    ap.add_argument("--no-export", action="store_true", help="skip the preview-export leg")
     ap.add_argument("--no-autotune", action="store_true", help="keep the plan's default band height and ring depth")
     ap.add_argument("--train-steps", type=int, default=782, help="Adam steps (782 x 64 = 50k windows)")
     ap.add_argument("--train-batch", type=int, default=64)

@@ -113,6 +113,11 @@ def load_library(path: str = LIB_PATH):
     L.i360b_launch_lab_stats.argtypes = [ct.POINTER(vp), _i32p, _i32p, i, vp, vp]
     L.i360b_launch_reinhard.argtypes = [ct.POINTER(vp), _i32p, _i32p, i, vp, vp, vp]
     L.i360b_launch_color_correct.argtypes = [ct.POINTER(vp), _i32p, _i32p, i, i, vp, vp]
+    L.i360b_launch_export_preview.argtypes = [ct.POINTER(vp), _i32p, i, i, i, i, vp, ct.c_longlong, _i32p, _i32p, vp]
+    L.i360b_render_plan_export_preview.argtypes = [vp, i, i, i, vp, ct.c_longlong, _i32p, _i32p, vp]
+    L.i360b_write_tiff16_chunks.argtypes = [ct.c_char_p, ct.POINTER(vp), _i32p, i, i, i, vp]
+    L.i360b_render_plan_write_tiff16.argtypes = [vp, ct.c_char_p, i, i, vp]
+    L.i360b_download_framed.argtypes = [vp, i, i, vp, vp]
     L.i360b_cull_tiles.argtypes = [_f32p, _i32p, _i32p, i, _i32p, i, i, _i32p, _i32p, _i32p, i, _i32p]
     L.i360b_launch_cull_tiles.argtypes = [vp, vp, vp, i, vp, i, i, vp, vp, vp, i, vp, vp]
     L.i360b_launch_blend.argtypes = [ct.POINTER(vp), i, i, i, i, vp, vp]
@@ -272,6 +277,35 @@ class B200ComputeBackend:
                                       ip(contrib), cap, ip(total))
         return ComputeResult(r), first[:t], count[:t], contrib[:int(total[0])], int(total[0])
 
+    # PanoramaExporter.cpp:46-102, Tiff16Writer.cpp:40-97, StorageEngine.cpp:130-144
+    def launch_export_preview(self, d_chunks, rects, total_w: int, total_h: int, max_dimension: int, d_out: int,
+                              capacity: int, stream: int = 0):
+        """(ComputeResult, width, height) of the RGB8 preview composite of the
+        chunk outputs d_chunks (device pointers or 0 / None) at rects."""
+        n = len(d_chunks)
+        arr = (ct.c_void_p * max(1, n))(*[p or None for p in d_chunks])
+        r = np.ascontiguousarray(rects, np.int32).reshape(-1)
+        w, h = ct.c_int(), ct.c_int()
+        rc = self.lib.i360b_launch_export_preview(arr, r.ctypes.data_as(ct.POINTER(ct.c_int)), n, int(total_w),
+                                                  int(total_h), int(max_dimension), d_out or None,
+                                                  ct.c_longlong(capacity), ct.byref(w), ct.byref(h), stream or None)
+        return ComputeResult(rc), w.value, h.value
+
+    def write_tiff16_chunks(self, path: str, d_chunks, rects, canvas_w: int, canvas_h: int,
+                            stream: int = 0) -> ComputeResult:
+        n = len(d_chunks)
+        arr = (ct.c_void_p * max(1, n))(*[p or None for p in d_chunks])
+        r = np.ascontiguousarray(rects, np.int32).reshape(-1)
+        return ComputeResult(self.lib.i360b_write_tiff16_chunks(os.fsencode(path), arr,
+                                                                r.ctypes.data_as(ct.POINTER(ct.c_int)), n,
+                                                                int(canvas_w), int(canvas_h), stream or None))
+
+    def download_framed(self, d_data: int, width: int, height: int, stream: int = 0):
+        """(ComputeResult, bytes): the framed pixel-buffer blob of a device RGB48 image."""
+        buf = np.zeros(8 + width * height * 6, np.uint8)
+        rc = self.lib.i360b_download_framed(d_data, int(width), int(height), buf.ctypes.data, stream or None)
+        return ComputeResult(rc), buf.tobytes()
+
     def launch_cull_tiles(self, d_h: int, d_widths: int, d_heights: int, n: int, d_tiles: int, t: int, mode: int,
                           d_first: int, d_count: int, d_contrib: int, capacity: int, d_total: int,
                           stream: int = 0) -> ComputeResult:
@@ -378,6 +412,21 @@ class RenderPlan:
         if rc != 0:
             raise RuntimeError(self.lib.i360b_get_last_error().decode())
         return {"band_rows": r.value, "dt_slots": k.value, "ms": ms.value}
+
+    def export_preview(self, total_w: int, total_h: int, max_dimension: int, d_out: int, capacity: int,
+                       stream: int = 0):
+        """Preview composite of the rendered tiles into device RGB8 d_out
+        (PanoramaExporter.cpp:46-102).  Returns (ComputeResult, width, height)."""
+        w, h = ct.c_int(), ct.c_int()
+        rc = self.lib.i360b_render_plan_export_preview(self._h, int(total_w), int(total_h), int(max_dimension),
+                                                       d_out or None, ct.c_longlong(capacity), ct.byref(w),
+                                                       ct.byref(h), stream or None)
+        return ComputeResult(rc), w.value, h.value
+
+    def write_tiff16(self, path: str, canvas_w: int, canvas_h: int, stream: int = 0) -> ComputeResult:
+        """16-bit RGB TIFF of the canvas of tile outputs (Tiff16Writer.cpp:40-97)."""
+        return ComputeResult(self.lib.i360b_render_plan_write_tiff16(self._h, os.fsencode(path), int(canvas_w),
+                                                                     int(canvas_h), stream or None))
 
     def execute(self, stream: int = 0) -> ComputeResult:
         return ComputeResult(self.lib.i360b_render_plan_execute(self._h, stream or None))

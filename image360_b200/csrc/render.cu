@@ -757,6 +757,14 @@ extern "C" int i360b_render_plan_create(const i360b_frame* frames, int numFrames
         delete p;
         return rc;
     }
+    p->plan.tileRects.resize((size_t)numTiles * 4);
+    p->plan.tileListed.resize(numTiles);
+    for (int t = 0; t < numTiles; ++t)
+    {
+        const int r[4] = {tiles[t].x, tiles[t].y, tiles[t].width, tiles[t].height};
+        for (int q = 0; q < 4; ++q) p->plan.tileRects[(size_t)t * 4 + q] = r[q];
+        p->plan.tileListed[t] = tiles[t].count;
+    }
     *outPlan = p;
     return I360B_SUCCESS;
 }

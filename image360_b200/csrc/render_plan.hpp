@@ -74,6 +74,8 @@ struct Plan
     int* hostErr = nullptr;
     std::vector<SubTile> subTiles;  // built on first learned render
     std::vector<float> itemEdges;   // 16 per item (ItemSpec::edges)
+    std::vector<int> tileRects;     // x, y, width, height per tile (canvas)
+    std::vector<int> tileListed;    // contributors listed per tile (0: no render output)
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t graphExec = nullptr;
 

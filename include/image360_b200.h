@@ -202,6 +202,38 @@ I360B_API int i360b_launch_blend_noalloc(const unsigned short* const* dWarped, i
 /* One source frame: a demosaiced RGB48 image in device memory and its
  * homography from frame pixels to canvas pixels (Homography, Types.h:138-141,
  * in double).  gain is applied after the warp (RenderExecutor.cpp:111-114). */
+/* ---- export of rendered chunk outputs ----------------------------------- */
+
+/* The preview composite of PanoramaExporter::ExportPreviewJpeg
+ * (PanoramaExporter.cpp:46-102) on the device: chunk outputs (RGB48,
+ * dChunks[c] with canvas rectangle rects[4c .. 4c+3] = x, y, width, height;
+ * a null pointer = a chunk with no render output) placed in chunk order into
+ * an RGB8 image whose longest edge is maxDimension (ComputeExportScale /
+ * ComputeChunkPlacement, PanoramaExporter.cpp:9-24), nearest source pixel,
+ * samples >> 8; the last chunk with a source pixel wins where placements
+ * overlap, as in the reference's loop.  *outW / *outH receive the size;
+ * returns INVALID_PARAM when capacity < outW * outH * 3 bytes.  The JPEG
+ * encode is the caller's codec (IImageCodec::Encode).  dChunks and rects are
+ * HOST arrays; dOut is device memory. */
+I360B_API int i360b_launch_export_preview(const unsigned short* const* dChunks, const int* rects, int numChunks,
+                                          int totalW, int totalH, int maxDimension, unsigned char* dOut,
+                                          long long capacity, int* outW, int* outH, void* stream);
+
+/* Writes the 16-bit RGB TIFF of WriteTiff16RGB (Tiff16Writer.cpp:40-97,
+ * byte for byte) of a canvasW x canvasH canvas holding the chunk outputs at
+ * their rectangles (zero elsewhere), assembled band by band on the device.
+ * Canvases whose samples exceed the format's 32-bit offsets (4 GiB) are
+ * rejected with INVALID_PARAM (the reference would write wrapped offsets).
+ * Synchronous. */
+I360B_API int i360b_write_tiff16_chunks(const char* path, const unsigned short* const* dChunks, const int* rects,
+                                        int numChunks, int canvasW, int canvasH, void* stream);
+
+/* StorageEngine::WritePixelBuffer's framing (StorageEngine.cpp:130-144) of a
+ * device RGB48 image into hostOut: int32 width, int32 height (little
+ * endian), then width * height * 3 samples - 8 + width * height * 6 bytes.
+ * Synchronous. */
+I360B_API int i360b_download_framed(const unsigned short* dData, int width, int height, void* hostOut, void* stream);
+
 /* ---- tile -> contributor culling ---------------------------------------- */
 
 /* Overlap test modes of i360b_cull_tiles / i360b_launch_cull_tiles. */
@@ -318,6 +350,16 @@ I360B_API const char* i360b_render_stage_name(int stage);
  * plan's outputs are overwritten with its render. */
 I360B_API int i360b_render_plan_autotune(i360b_render_plan* plan, void* stream, int* bandRows, int* dtSlots,
                                          float* bestMs);
+/* i360b_launch_export_preview over the plan's tiles in tile order (tiles that
+ * list no contributor have no render output and are skipped). */
+I360B_API int i360b_render_plan_export_preview(i360b_render_plan* plan, int totalW, int totalH, int maxDimension,
+                                               unsigned char* dOut, long long capacity, int* outW, int* outH,
+                                               void* stream);
+
+/* i360b_write_tiff16_chunks over the plan's tile outputs. */
+I360B_API int i360b_render_plan_write_tiff16(i360b_render_plan* plan, const char* path, int canvasW, int canvasH,
+                                             void* stream);
+
 /* Device bytes of scratch the plan holds. */
 I360B_API size_t i360b_render_plan_scratch_bytes(const i360b_render_plan* plan);
 I360B_API void i360b_render_plan_destroy(i360b_render_plan* plan);

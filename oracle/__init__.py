@@ -112,6 +112,34 @@ class _Oracle:
         return [[f for f, (H, fw, fh) in enumerate(zip(Hs, widths, heights))
                  if fw <= 0 or fh <= 0 or self.overlaps(H, fw, fh, x, y, w, h, f64)] for x, y, w, h in tiles]
 
+    def export_preview(self, tiles, rects, total_w, total_h, max_dimension):
+        """Preview composite (RGB8, (h, w, 3)) of chunk outputs in chunk order
+        (PanoramaExporter.cpp:46-102); a None tile has no render output."""
+        return _export_preview(self.lib.or_export_preview, tiles, rects, total_w, total_h, max_dimension)
+
+    def export_scale(self, total_w, total_h, max_dimension):
+        self.lib.or_export_scale.restype = ct.c_float
+        return self.lib.or_export_scale(int(total_w), int(total_h), int(max_dimension))
+
+    def chunk_placement(self, x, y, w, h, scale):
+        out = np.zeros(4, np.int32)
+        self.lib.or_chunk_placement(int(x), int(y), int(w), int(h), ct.c_float(scale), _p(out, _i32p))
+        return tuple(int(v) for v in out)
+
+    def framed(self, img):
+        img = np.ascontiguousarray(img, np.uint16)
+        out = np.zeros(8 + img.size * 2, np.uint8)
+        self.lib.or_frame_pixel_buffer(_p(img, _u16p), img.shape[1], img.shape[0], _p(out, _u8p))
+        return out.tobytes()
+
+    def tiff16(self, img):
+        img = np.ascontiguousarray(img, np.uint16)
+        h, w = img.shape[:2]
+        self.lib.or_tiff16_size.restype = ct.c_longlong
+        out = np.zeros(self.lib.or_tiff16_size(w, h), np.uint8)
+        self.lib.or_tiff16_bytes(_p(img, _u16p), w, h, _p(out, _u8p))
+        return out.tobytes()
+
     def lab_stats(self, rgb, f64=False):
         """(mean[3], std[3]) of CIE L, a, b over an (h, w, 3) image."""
         return _lab_stats(self.lib.or_lab_stats_f64 if f64 else self.lib.or_lab_stats, rgb)
@@ -179,6 +207,25 @@ class _Oracle:
         """tiles: list of (x, y, w, h, [frame indices]). Returns (seconds, outputs)."""
         return _render_tiles(self.lib.or_render_tiles, None, threads, frames, inv_h, gains, tiles, bands,
                              want_out)
+
+
+def _export_preview(fn, tiles, rects, total_w, total_h, max_dimension):
+    arr = (ct.POINTER(ct.c_uint16) * max(1, len(tiles)))()
+    keep = []
+    for i, t in enumerate(tiles):
+        if t is not None:
+            a = np.ascontiguousarray(t, np.uint16)
+            keep.append(a)
+            arr[i] = a.ctypes.data_as(ct.POINTER(ct.c_uint16))
+    r = np.ascontiguousarray(rects, np.int32).reshape(-1)
+    scale = np.float32(max_dimension) / np.float32(max(total_w, total_h, 1))
+    cap = (int(np.float32(total_w) * scale) + 2) * (int(np.float32(total_h) * scale) + 2) * 3
+    out = np.zeros(max(3, cap), np.uint8)
+    ow, oh = ct.c_int(), ct.c_int()
+    if not fn(arr, _p(r, _i32p), len(tiles), int(total_w), int(total_h), int(max_dimension), _p(out, _u8p),
+              ct.c_longlong(out.size), ct.byref(ow), ct.byref(oh)):
+        raise ValueError("invalid export arguments")
+    return out[:ow.value * oh.value * 3].reshape(oh.value, ow.value, 3)
 
 
 def _lab_stats(fn, rgb):
@@ -278,6 +325,57 @@ class _Reference:
         H = np.ascontiguousarray(H, np.float32).reshape(9)
         return bool(self.lib.ref_image_overlaps_chunk(_p(H, _f32p), int(image_w), int(image_h), int(x), int(y),
                                                       int(w), int(h)))
+
+    def export_preview(self, tiles, total_w, total_h, chunk_size, max_dimension, frame_chunk=-1):
+        """The reference's ExportPreviewJpeg composite (captured before the JPEG
+        encode) over a chunk grid of total_w x total_h in chunk_size tiles,
+        chunk outputs `tiles` in grid order (None: no render task), each stored
+        and read back through its StorageEngine.  With frame_chunk >= 0 also
+        returns that chunk's framed blob bytes."""
+        import tempfile
+        arr = (ct.POINTER(ct.c_uint16) * max(1, len(tiles)))()
+        keep = []
+        for i, t in enumerate(tiles):
+            if t is not None:
+                a = np.ascontiguousarray(t, np.uint16)
+                keep.append(a)
+                arr[i] = a.ctypes.data_as(ct.POINTER(ct.c_uint16))
+        scale = np.float32(max_dimension) / np.float32(max(total_w, total_h))
+        cap = (int(np.float32(total_w) * scale) + 2) * (int(np.float32(total_h) * scale) + 2) * 3
+        out = np.zeros(cap, np.uint8)
+        ow, oh = ct.c_int(), ct.c_int()
+        fcap = 8 + (max(t.size for t in keep) * 2 if keep else 0)
+        frame = np.zeros(max(1, fcap), np.uint8)
+        fbytes = ct.c_longlong(0)
+        with tempfile.TemporaryDirectory() as d:
+            ok = self.lib.ref_export_preview(arr, int(total_w), int(total_h), int(chunk_size), int(max_dimension),
+                                             os.path.join(d, "p").encode(), _p(out, _u8p), ct.c_longlong(cap),
+                                             ct.byref(ow), ct.byref(oh), int(frame_chunk), _p(frame, _u8p),
+                                             ct.c_longlong(fcap), ct.byref(fbytes))
+        if not ok:
+            raise RuntimeError("reference ExportPreviewJpeg failed")
+        img = out[:ow.value * oh.value * 3].reshape(oh.value, ow.value, 3)
+        return (img, frame[:fbytes.value].tobytes()) if frame_chunk >= 0 else img
+
+    def tiff16(self, img):
+        """The bytes WriteTiff16RGB writes for an (h, w, 3) image."""
+        import tempfile
+        img = np.ascontiguousarray(img, np.uint16)
+        with tempfile.TemporaryDirectory() as d:
+            path = os.path.join(d, "t.tif")
+            if not self.lib.ref_write_tiff16(path.encode(), _p(img, _u16p), img.shape[1], img.shape[0]):
+                raise RuntimeError("reference WriteTiff16RGB failed")
+            with open(path, "rb") as f:
+                return f.read()
+
+    def export_scale(self, total_w, total_h, max_dimension):
+        self.lib.ref_export_scale.restype = ct.c_float
+        return self.lib.ref_export_scale(int(total_w), int(total_h), int(max_dimension))
+
+    def chunk_placement(self, x, y, w, h, scale):
+        out = np.zeros(4, np.int32)
+        self.lib.ref_chunk_placement(int(x), int(y), int(w), int(h), ct.c_float(scale), _p(out, _i32p))
+        return tuple(int(v) for v in out)
 
     def find_overlapping_unopenable(self, n):
         """FindOverlappingImages over n images whose files cannot be opened."""

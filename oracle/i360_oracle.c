@@ -516,6 +516,118 @@ int or_image_overlaps_chunk_f64(const float* m, int imageW, int imageH, int chun
     return minX < x1 && maxX > (double)chunkX && minY < y1 && maxY > (double)chunkY;
 }
 
+/* ------------------------------------------------------------------------ */
+/* Export: PanoramaExporter.cpp:9-102, StorageEngine.cpp:130-144,             */
+/* Tiff16Writer.cpp:40-97.                                                    */
+/* ------------------------------------------------------------------------ */
+float or_export_scale(int totalW, int totalH, int maxDimension)
+{
+    int longest = totalW > totalH ? totalW : totalH;
+    if (longest <= 0) return 1.0f;
+    return (float)maxDimension / (float)longest;
+}
+
+void or_chunk_placement(int x, int y, int w, int h, float scale, int* out4)
+{
+    int dw = (int)((float)w * scale), dh = (int)((float)h * scale);
+    out4[0] = (int)((float)x * scale);
+    out4[1] = (int)((float)y * scale);
+    out4[2] = dw > 1 ? dw : 1;
+    out4[3] = dh > 1 ? dh : 1;
+}
+
+int or_export_preview(const uint16_t* const* tiles, const int32_t* rects, int numTiles, int totalW, int totalH,
+                      int maxDimension, uint8_t* out, long long capacity, int* outW, int* outH)
+{
+    if (maxDimension <= 0 || totalW <= 0 || totalH <= 0) return 0;
+    float scale = or_export_scale(totalW, totalH, maxDimension);
+    int ow = (int)((float)totalW * scale), oh = (int)((float)totalH * scale);
+    ow = ow > 1 ? ow : 1;
+    oh = oh > 1 ? oh : 1;
+    if ((long long)ow * oh * 3 > capacity) return 0;
+    memset(out, 0, (size_t)ow * oh * 3);
+    for (int c = 0; c < numTiles; ++c)
+    {
+        const uint16_t* src = tiles[c];
+        if (!src) continue;
+        const int32_t* r = rects + 4 * c;
+        int p[4];
+        or_chunk_placement(r[0], r[1], r[2], r[3], scale, p);
+        for (int dy = 0; dy < p[3]; ++dy)
+        {
+            int oy = p[1] + dy;
+            if (oy < 0 || oy >= oh) continue;
+            for (int dx = 0; dx < p[2]; ++dx)
+            {
+                int ox = p[0] + dx;
+                if (ox < 0 || ox >= ow) continue;
+                int sx = (int)((float)dx / scale), sy = (int)((float)dy / scale);
+                if (sx < 0 || sx >= r[2] || sy < 0 || sy >= r[3]) continue;
+                const uint16_t* s = src + ((size_t)sy * r[2] + sx) * 3;
+                uint8_t* d = out + ((size_t)oy * ow + ox) * 3;
+                d[0] = (uint8_t)(s[0] >> 8);
+                d[1] = (uint8_t)(s[1] >> 8);
+                d[2] = (uint8_t)(s[2] >> 8);
+            }
+        }
+    }
+    *outW = ow;
+    *outH = oh;
+    return 1;
+}
+
+static void put_u16(uint8_t* p, uint16_t v)
+{
+    p[0] = (uint8_t)(v & 0xff);
+    p[1] = (uint8_t)(v >> 8);
+}
+
+static void put_u32(uint8_t* p, uint32_t v)
+{
+    for (int i = 0; i < 4; ++i) p[i] = (uint8_t)(v >> (8 * i));
+}
+
+void or_frame_pixel_buffer(const uint16_t* data, int w, int h, uint8_t* out)
+{
+    put_u32(out, (uint32_t)w);
+    put_u32(out + 4, (uint32_t)h);
+    memcpy(out + 8, data, (size_t)w * h * 6);
+}
+
+long long or_tiff16_size(int w, int h)
+{
+    return 8 + (long long)w * h * 6 + 6 + 8 + 8 + 2 + 12 * 12 + 4;
+}
+
+void or_tiff16_bytes(const uint16_t* data, int w, int h, uint8_t* out)
+{
+    const uint32_t pix = (uint32_t)((size_t)w * h * 6);
+    const uint32_t bps = 8 + pix, xres = bps + 6, yres = xres + 8, ifd = yres + 8;
+    out[0] = 'I';
+    out[1] = 'I';
+    put_u16(out + 2, 42);
+    put_u32(out + 4, ifd);
+    memcpy(out + 8, data, pix);
+    uint8_t* p = out + bps;
+    put_u16(p, 16), put_u16(p + 2, 16), put_u16(p + 4, 16);
+    put_u32(p + 6, 72), put_u32(p + 10, 1), put_u32(p + 14, 72), put_u32(p + 18, 1);
+    p = out + ifd;
+    put_u16(p, 12);
+    const uint32_t e[12][4] = {{256, 4, 1, (uint32_t)w}, {257, 4, 1, (uint32_t)h}, {258, 3, 3, bps},
+                               {259, 3, 1, 1},          {262, 3, 1, 2},          {273, 4, 1, 8},
+                               {277, 3, 1, 3},          {278, 4, 1, (uint32_t)h}, {279, 4, 1, pix},
+                               {282, 5, 1, xres},       {283, 5, 1, yres},       {296, 3, 1, 2}};
+    for (int i = 0; i < 12; ++i)
+    {
+        uint8_t* q = p + 2 + 12 * i;
+        put_u16(q, (uint16_t)e[i][0]);
+        put_u16(q + 2, (uint16_t)e[i][1]);
+        put_u32(q + 4, e[i][2]);
+        put_u32(q + 8, e[i][3]);
+    }
+    put_u32(p + 2 + 12 * 12, 0);
+}
+
 int or_invert_h(const float* m, float* out)
 {
     if (!m || !out) return 0;

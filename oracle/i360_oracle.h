@@ -48,6 +48,26 @@ int or_image_overlaps_chunk(const float* h9, int imageW, int imageH, int chunkX,
 int or_image_overlaps_chunk_f64(const float* h9, int imageW, int imageH, int chunkX, int chunkY, int chunkW,
                                 int chunkH);
 
+/* PanoramaExporter.cpp:9-24. */
+float or_export_scale(int totalW, int totalH, int maxDimension);
+void or_chunk_placement(int x, int y, int w, int h, float scale, int* out4);
+
+/* The preview composite of PanoramaExporter.cpp:46-102: every chunk's RGB48
+ * output (tiles[c], the chunk rectangle rects[4c..4c+3]; null = no render
+ * output) placed in chunk order into an RGB8 canvas of the exported size,
+ * nearest source pixel, 16 -> 8 bits by >> 8.  Writes the size to
+ * outW/outH; returns 0 when the composite needs more than `capacity` bytes
+ * or the arguments are invalid. */
+int or_export_preview(const uint16_t* const* tiles, const int32_t* rects, int numTiles, int totalW, int totalH,
+                      int maxDimension, uint8_t* out, long long capacity, int* outW, int* outH);
+
+/* StorageEngine.cpp:130-144: int32 width, int32 height, the RGB48 samples. */
+void or_frame_pixel_buffer(const uint16_t* data, int w, int h, uint8_t* out);
+
+/* Tiff16Writer.cpp:40-97 as bytes (size or_tiff16_size(w, h)). */
+long long or_tiff16_size(int w, int h);
+void or_tiff16_bytes(const uint16_t* data, int w, int h, uint8_t* out);
+
 /* HomographyMath.cpp:94-116.  Returns 1 on success, 0 when singular. */
 int or_invert_h(const float* h, float* out);
 

@@ -21,8 +21,13 @@
 #include "HeaderFiles/HomographyMath.h"
 #include "HeaderFiles/SeamBlendKernels.h"
 #include "HeaderFiles/OverlapCulling.h"
+#include "HeaderFiles/PanoramaExporter.h"
+#include "HeaderFiles/StorageEngine.h"
+#include "HeaderFiles/TextEncoding.h"
+#include "HeaderFiles/Tiff16Writer.h"
 
 #include <atomic>
+#include <memory>
 #include <chrono>
 #include <cmath>
 #include <cstdint>
@@ -32,6 +37,39 @@
 #include <vector>
 
 using namespace WindowsApp::Core;
+
+namespace WindowsApp::Core
+{
+void RefStubAddRenderTask(const std::string& chunkId, int64_t blobId);  // ref_project_stub.cpp
+}
+
+namespace
+{
+// An image codec that keeps the RGB8 image it is asked to encode (the
+// preview composite) and returns it as the "encoded" bytes.
+class CapturingCodec final : public WindowsApp::Compute::IImageCodec
+{
+public:
+    std::vector<unsigned char> rgb;
+    int width = 0, height = 0;
+    WindowsApp::Compute::ComputeResult Initialize() override { return WindowsApp::Compute::ComputeResult::SUCCESS; }
+    void Shutdown() override {}
+    WindowsApp::Compute::ComputeResult Decode(const unsigned char*, size_t, unsigned char**, int*, int*) override
+    {
+        return WindowsApp::Compute::ComputeResult::NOT_SUPPORTED;
+    }
+    void FreeDecoded(unsigned char*) override {}
+    WindowsApp::Compute::ComputeResult Encode(const unsigned char* data, int w, int h, int, std::vector<unsigned char>& out) override
+    {
+        width = w;
+        height = h;
+        rgb.assign(data, data + static_cast<size_t>(w) * h * 3);
+        out = rgb;
+        return WindowsApp::Compute::ComputeResult::SUCCESS;
+    }
+    const char* GetLastError() const override { return ""; }
+};
+}  // namespace
 namespace SB = WindowsApp::Core::Kernels::SeamBlend;
 using WindowsApp::Compute::ComputeResult;
 
@@ -154,6 +192,82 @@ extern "C"
         auto r = FindOverlappingImages(c, images);
         for (size_t i = 0; i < r.size(); ++i) idsOut[i] = r[i];
         return static_cast<int>(r.size());
+    }
+
+    // PanoramaExporter.cpp:34-114 run on a project whose chunk grid is
+    // totalW x totalH in chunkSize tiles (ProjectManager.cpp:260-281 order);
+    // chunk c's render output is tiles[c] (RGB48, the chunk's size), or no
+    // render task when tiles[c] is null.  Each output goes through the
+    // reference's StorageEngine::WritePixelBuffer into shard files under
+    // `dir` (a file prefix); the preview composite (RGB8) is captured from the
+    // codec into rgbOut (capacity bytes).  Returns 1 on success and writes
+    // the composite size; the framed blob of chunk `frameChunk` (or none when
+    // -1) is copied to frameOut (frameCapacity bytes, size to *frameBytes).
+    int ref_export_preview(const uint16_t* const* tiles, int totalW, int totalH, int chunkSize, int maxDimension,
+                           const char* dir, uint8_t* rgbOut, long long capacity, int* outW, int* outH,
+                           int frameChunk, uint8_t* frameOut, long long frameCapacity, long long* frameBytes)
+    {
+        ProjectManager pm;
+        pm.CreateProject(L"", totalW, totalH, chunkSize);
+        StorageEngine se;
+        if (!se.Open(Utf8ToWide(dir), L"ref", pm)) return 0;
+        int c = 0;
+        for (const auto& chunk : pm.GetChunks())
+        {
+            if (tiles[c])
+            {
+                PixelBuffer pb;
+                pb.width = chunk.width;
+                pb.height = chunk.height;
+                pb.data.assign(tiles[c], tiles[c] + static_cast<size_t>(chunk.width) * chunk.height * 3);
+                auto id = se.WritePixelBuffer(pb, "rendered_chunk_rgb48");  // RenderExecutor.cpp:142
+                if (!id.has_value()) return 0;
+                RefStubAddRenderTask(chunk.id, *id);
+                if (c == frameChunk && frameOut && frameBytes)
+                {
+                    auto blob = se.ReadBlob(*id);
+                    if (!blob.has_value() || static_cast<long long>(blob->size()) > frameCapacity) return 0;
+                    std::memcpy(frameOut, blob->data(), blob->size());
+                    *frameBytes = static_cast<long long>(blob->size());
+                }
+            }
+            ++c;
+        }
+        auto codec = std::make_shared<CapturingCodec>();
+        PanoramaExporter ex(pm, se, codec);
+        std::string preview = std::string(dir) + "_preview.bin";
+        if (!ex.ExportPreviewJpeg(Utf8ToWide(preview), maxDimension, 90)) return 0;
+        se.Close();
+        if (static_cast<long long>(codec->rgb.size()) > capacity) return 0;
+        std::memcpy(rgbOut, codec->rgb.data(), codec->rgb.size());
+        *outW = codec->width;
+        *outH = codec->height;
+        return 1;
+    }
+
+    // Tiff16Writer.cpp:40-97.
+    int ref_write_tiff16(const char* path, const uint16_t* data, int w, int h)
+    {
+        return WriteTiff16RGB(Utf8ToWide(path), data, w, h) ? 1 : 0;
+    }
+
+    // PanoramaExporter.cpp:9-24.
+    float ref_export_scale(int totalW, int totalH, int maxDimension)
+    {
+        return ComputeExportScale(totalW, totalH, maxDimension);
+    }
+    void ref_chunk_placement(int x, int y, int w, int h, float scale, int* out4)
+    {
+        ChunkModel c;
+        c.x_offset = x;
+        c.y_offset = y;
+        c.width = w;
+        c.height = h;
+        ChunkPlacement p = ComputeChunkPlacement(c, scale);
+        out4[0] = p.destX;
+        out4[1] = p.destY;
+        out4[2] = p.destW;
+        out4[3] = p.destH;
     }
 
     // GainColorOps.cpp:103-130 / 132-156.

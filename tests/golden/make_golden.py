@@ -20,6 +20,11 @@ Contents (all outputs are the reference's scalar tier unless named *_avx):
                   reference's per-tile render (warp, gain, seam blend)
   c2s_*           median stack of 16 aligned 14-bit frames with 5% transient
                   outlier rectangles
+  ex_*            export: the reference's ExportPreviewJpeg composite (captured
+                  before the JPEG encode) of a 300x200 grid of 128-pixel chunk
+                  outputs with one chunk unrendered, at two sizes; its
+                  WriteTiff16RGB bytes of a 5x7 image; a framed chunk blob
+                  (StorageEngine::WritePixelBuffer)
   ct_*            Lab statistics (ComputeLabStatsCpu) and Reinhard transfer
                   (ApplyReinhardColorTransferCpu) of two demosaiced c1s frame
                   crops (target -> reference), a full-range random image and a
@@ -158,6 +163,21 @@ def main():
     # sumSq multiply-add into an FMA, so on 14-bit data they can pick a
     # different clip set than the scalar tier on a few values; kept for record.
     g["c2s_out_avx"] = R.median(frames, 2.0, tier=R.tier)
+    # export (PanoramaExporter.cpp:34-114, Tiff16Writer.cpp:40-97, StorageEngine.cpp:130-144)
+    rng = np.random.default_rng(5150)
+    chunks = []
+    for y in range(0, 200, 128):
+        for x in range(0, 300, 128):
+            chunks.append(rng.integers(0, 65536, (min(128, 200 - y), min(128, 300 - x), 3)).astype(np.uint16))
+    g["ex_chunks"] = np.concatenate([c.reshape(-1) for c in chunks])
+    g["ex_missing"] = np.array([4], np.int32)
+    listed = [None if i == 4 else c for i, c in enumerate(chunks)]
+    g["ex_preview_97"], blob = R.export_preview(listed, 300, 200, 128, 97, frame_chunk=2)
+    g["ex_preview_450"] = R.export_preview(listed, 300, 200, 128, 450)
+    g["ex_framed_2"] = np.frombuffer(blob, np.uint8)
+    img = rng.integers(0, 65536, (5, 7, 3)).astype(np.uint16)
+    g["ex_tiff_in"] = img
+    g["ex_tiff_bytes"] = np.frombuffer(R.tiff16(img), np.uint8)
     # colour correction (GainColorOps.cpp:103-156)
     tgt = np.ascontiguousarray(g["c1s_frames"][1][:48, :64])
     ref = np.ascontiguousarray(g["c1s_frames"][0][:48, :64])

@@ -81,3 +81,24 @@ def test_color_transfer(oracle_c, name):
     ref = g["ct_ref_stats"]
     out = oracle_c.reinhard(img, mean, std, ref[:3], ref[3:])
     assert np.array_equal(out, g[f"ct_{name}_out"])
+
+
+def _golden_chunks(g):
+    flat, out, off = g["ex_chunks"], [], 0
+    for y in range(0, 200, 128):
+        for x in range(0, 300, 128):
+            h, w = min(128, 200 - y), min(128, 300 - x)
+            out.append(((x, y, w, h), flat[off:off + h * w * 3].reshape(h, w, 3)))
+            off += h * w * 3
+    return out
+
+
+def test_export(oracle_c):
+    g = golden()
+    chunks = _golden_chunks(g)
+    rects = [r for r, _ in chunks]
+    tiles = [None if i in g["ex_missing"] else c for i, (_, c) in enumerate(chunks)]
+    assert np.array_equal(oracle_c.export_preview(tiles, rects, 300, 200, 97), g["ex_preview_97"])
+    assert np.array_equal(oracle_c.export_preview(tiles, rects, 300, 200, 450), g["ex_preview_450"])
+    assert oracle_c.framed(chunks[2][1]) == g["ex_framed_2"].tobytes()
+    assert oracle_c.tiff16(g["ex_tiff_in"]) == g["ex_tiff_bytes"].tobytes()

@@ -145,3 +145,59 @@ def test_overlap_culling_known_answers(oracle_c, reference):
     # unopenable files: sizes unknown -> both images included
     assert reference.find_overlapping_unopenable(2) == [100, 101]
     assert oracle_c.cull([eye, far], [0, -1], [0, 5], [(0, 0, 4096, 4096)]) == [[0, 1]]
+
+
+def _chunk_grid(rng, W, H, cs, missing_every=5):
+    tiles, rects = [], []
+    for y in range(0, H, cs):
+        for x in range(0, W, cs):
+            w, h = min(cs, W - x), min(cs, H - y)
+            rects.append((x, y, w, h))
+            skip = missing_every and (x // cs + 3 * (y // cs)) % missing_every == 3
+            tiles.append(None if skip else rng.integers(0, 65536, (h, w, 3)).astype(np.uint16))
+    return tiles, rects
+
+
+@pytest.mark.parametrize("W,H,cs", [(700, 300, 128), (333, 777, 100), (64, 64, 64)])
+def test_export_preview_composite(oracle_c, reference, W, H, cs):
+    """PanoramaExporter::ExportPreviewJpeg's composite, captured before the
+    JPEG encode, from chunk blobs written and read back by the reference's
+    StorageEngine."""
+    rng = np.random.default_rng(W + H)
+    tiles, rects = _chunk_grid(rng, W, H, cs)
+    for md in (1, 7, 100, 237, max(W, H), 1000):
+        assert np.array_equal(oracle_c.export_preview(tiles, rects, W, H, md),
+                              reference.export_preview(tiles, W, H, cs, md)), md
+
+
+def test_export_formats(oracle_c, reference):
+    rng = np.random.default_rng(3)
+    for h, w in ((1, 1), (2, 3), (17, 40)):
+        img = rng.integers(0, 65536, (h, w, 3)).astype(np.uint16)
+        assert oracle_c.tiff16(img) == reference.tiff16(img)
+    tiles, rects = _chunk_grid(rng, 300, 200, 128, missing_every=0)
+    _, blob = reference.export_preview(tiles, 300, 200, 128, 50, frame_chunk=1)
+    assert oracle_c.framed(tiles[1]) == blob
+
+
+def test_export_known_answers(oracle_c, reference):
+    """PanoramaExporterTests.cpp:16-67 and the TIFF layout checks of
+    tests/engine_smoke/main.cpp:447-520."""
+    for impl in (oracle_c, reference):
+        assert abs(impl.export_scale(8192, 4096, 2048) - 0.25) < 1e-5
+        assert abs(impl.export_scale(2048, 4096, 1024) - 0.25) < 1e-5
+        assert impl.chunk_placement(4096, 8192, 4096, 4096, 0.25) == (1024, 2048, 1024, 1024)
+        p = impl.chunk_placement(0, 0, 100, 100, 0.001)
+        assert p[2] >= 1 and p[3] >= 1
+    px = (1000 + np.arange(18) * 777).astype(np.uint16).reshape(2, 3, 3)
+    b = oracle_c.tiff16(px)
+    u16 = lambda o: int.from_bytes(b[o:o + 2], "little")
+    u32 = lambda o: int.from_bytes(b[o:o + 4], "little")
+    ifd = u32(4)
+    assert b[:2] == b"II" and u16(2) == 42 and ifd == 8 + 36 + 6 + 8 + 8
+    assert b[8:44] == px.tobytes() and u16(ifd) == 12
+    tags = [(u16(ifd + 2 + 12 * i), u32(ifd + 2 + 12 * i + 8)) for i in range(12)]
+    assert tags[0] == (256, 3) and tags[1] == (257, 2) and tags[3] == (259, 1) and tags[4] == (262, 2)
+    assert tags[5] == (273, 8) and tags[6] == (277, 3) and tags[7] == (278, 2) and tags[8] == (279, 36)
+    assert [u16(tags[2][1] + 2 * k) for k in range(3)] == [16, 16, 16]
+    assert b == reference.tiff16(px)
