@@ -113,6 +113,12 @@ def load_library(path: str = LIB_PATH):
     L.i360b_launch_lab_stats.argtypes = [ct.POINTER(vp), _i32p, _i32p, i, vp, vp]
     L.i360b_launch_reinhard.argtypes = [ct.POINTER(vp), _i32p, _i32p, i, vp, vp, vp]
     L.i360b_launch_color_correct.argtypes = [ct.POINTER(vp), _i32p, _i32p, i, i, vp, vp]
+    L.i360b_pipeline_create.argtypes = [vp, ct.POINTER(vp)]
+    L.i360b_pipeline_submit.argtypes = [vp, ct.POINTER(vp), ct.POINTER(vp)]
+    L.i360b_pipeline_wait.argtypes = [vp, ct.POINTER(ct.c_float)]
+    L.i360b_pipeline_autotune.argtypes = [vp, _i32p, _i32p, ct.POINTER(ct.c_float)]
+    L.i360b_pipeline_destroy.argtypes = [vp]
+    L.i360b_pipeline_destroy.restype = None
     L.i360b_launch_export_preview.argtypes = [ct.POINTER(vp), _i32p, i, i, i, i, vp, ct.c_longlong, _i32p, _i32p, vp]
     L.i360b_render_plan_export_preview.argtypes = [vp, i, i, i, vp, ct.c_longlong, _i32p, _i32p, vp]
     L.i360b_write_tiff16_chunks.argtypes = [ct.c_char_p, ct.POINTER(vp), _i32p, i, i, i, vp]
@@ -348,6 +354,94 @@ def launch_blend_noalloc(d_warped, width: int, height: int, d_out: int, num_band
     arr = (ct.c_void_p * max(1, len(d_warped)))(*d_warped)
     return ComputeResult(L.i360b_launch_blend_noalloc(arr, len(d_warped), width, height, num_bands, d_out,
                                                       stream or None))
+
+
+class PipelineDesc(ct.Structure):
+    _fields_ = [("numFrames", ct.c_int), ("frameWidth", ct.c_int), ("frameHeight", ct.c_int),
+                ("toCanvas", ct.POINTER(ct.c_double)), ("gains", ct.POINTER(ct.c_float)),
+                ("blackLevel", ct.c_uint16), ("camMul", ct.c_float * 4), ("rgbCam", ct.c_float * 12),
+                ("filters", ct.c_uint32), ("numTiles", ct.c_int), ("tileRects", ct.POINTER(ct.c_int)),
+                ("tileFirst", ct.POINTER(ct.c_int)), ("tileCount", ct.POINTER(ct.c_int)),
+                ("contributors", ct.POINTER(ct.c_int)), ("numBands", ct.c_int), ("coordMode", ct.c_int),
+                ("depth", ct.c_int)]
+
+
+class RenderPipeline:
+    """Pipelined device-resident render of successive CFA frame sets of one
+    panorama geometry (i360b_pipeline_*): submit() enqueues the upload of a
+    set's CFA frames, their demosaic, the render of every tile and the
+    download of the tile outputs, and returns; `depth` device slots overlap
+    the three stages of consecutive submissions.  Host buffers are given as
+    addresses (pinned memory, e.g. torch pin_memory() tensors) and must stay
+    valid until wait() returns.
+
+    to_canvas: (n, 3, 3) frame -> canvas; gains: (n,) ApplyGain factors;
+    demosaic: (black, camMul[4], rgbCam 3x4, filters); tiles: [(x, y, w, h,
+    [frame indices])]."""
+
+    def __init__(self, frame_w, frame_h, to_canvas, gains, demosaic, tiles, num_bands: int,
+                 coord_mode: int = COORDS_REFERENCE, depth: int = 2):
+        self.lib = load_library()
+        black, cm, rc, filt = demosaic
+        n = len(gains)
+        self._H = np.ascontiguousarray(to_canvas, np.float64).reshape(n * 9)
+        self._g = np.ascontiguousarray(gains, np.float32)
+        self._rects = np.ascontiguousarray([t[:4] for t in tiles], np.int32).reshape(-1)
+        counts = [len(t[4]) for t in tiles]
+        self._first = np.ascontiguousarray(np.concatenate([[0], np.cumsum(counts)[:-1]]), np.int32)
+        self._count = np.ascontiguousarray(counts, np.int32)
+        self._contrib = np.ascontiguousarray([c for t in tiles for c in t[4]] or [0], np.int32)
+        d = PipelineDesc()
+        d.numFrames, d.frameWidth, d.frameHeight = n, int(frame_w), int(frame_h)
+        ip = lambda a: a.ctypes.data_as(ct.POINTER(ct.c_int))
+        d.toCanvas = self._H.ctypes.data_as(ct.POINTER(ct.c_double))
+        d.gains = self._g.ctypes.data_as(ct.POINTER(ct.c_float))
+        d.blackLevel = int(black)
+        for i, v in enumerate(np.asarray(cm, np.float32).reshape(4)):
+            d.camMul[i] = float(v)
+        for i, v in enumerate(np.asarray(rc, np.float32).reshape(12)):
+            d.rgbCam[i] = float(v)
+        d.filters = int(filt)
+        d.numTiles = len(tiles)
+        d.tileRects, d.tileFirst, d.tileCount = ip(self._rects), ip(self._first), ip(self._count)
+        d.contributors = ip(self._contrib)
+        d.numBands, d.coordMode, d.depth = int(num_bands), int(coord_mode), int(depth)
+        self.num_frames, self.num_tiles = n, len(tiles)
+        self._h = ct.c_void_p()
+        rc_ = self.lib.i360b_pipeline_create(ct.byref(d), ct.byref(self._h))
+        if rc_ != 0:
+            raise RuntimeError(f"render pipeline: {ComputeResult(rc_).name}: {self.lib.i360b_get_last_error().decode()}")
+
+    def submit(self, host_cfa, host_tiles) -> ComputeResult:
+        """host_cfa: num_frames addresses; host_tiles: num_tiles addresses."""
+        assert len(host_cfa) == self.num_frames and len(host_tiles) == self.num_tiles
+        a = (ct.c_void_p * self.num_frames)(*host_cfa)
+        b = (ct.c_void_p * self.num_tiles)(*host_tiles)
+        return ComputeResult(self.lib.i360b_pipeline_submit(self._h, a, b))
+
+    def wait(self):
+        """(ComputeResult, device ms from the first upload to the last download)."""
+        ms = ct.c_float()
+        rc = self.lib.i360b_pipeline_wait(self._h, ct.byref(ms))
+        return ComputeResult(rc), ms.value
+
+    def autotune(self) -> dict:
+        r, k, ms = ct.c_int(), ct.c_int(), ct.c_float()
+        rc = self.lib.i360b_pipeline_autotune(self._h, ct.byref(r), ct.byref(k), ct.byref(ms))
+        if rc != 0:
+            raise RuntimeError(self.lib.i360b_get_last_error().decode())
+        return {"band_rows": r.value, "dt_slots": k.value, "ms": ms.value}
+
+    def close(self) -> None:
+        if self._h:
+            self.lib.i360b_pipeline_destroy(self._h)
+            self._h = ct.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 class RenderPlan:

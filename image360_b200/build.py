@@ -18,7 +18,7 @@ OBJDIR = os.path.join(HERE, "_build")
 
 # Exact-parity kernels: no FMA contraction anywhere (the reference's CPU code
 # rounds every product and sum separately).
-PARITY_SOURCES = ["context.cu", "pixel_ops.cu", "blend_kernels.cu", "render.cu", "capi.cu", "noalloc.cu", "color.cu", "cull.cu", "export.cu"]
+PARITY_SOURCES = ["context.cu", "pixel_ops.cu", "blend_kernels.cu", "render.cu", "capi.cu", "noalloc.cu", "color.cu", "cull.cu", "export.cu", "pipeline.cu"]
 # Everything else (tensor-core learned blend) may contract.
 FAST_SOURCES: list[str] = ["learned.cu"]
 

@@ -202,6 +202,51 @@ I360B_API int i360b_launch_blend_noalloc(const unsigned short* const* dWarped, i
 /* One source frame: a demosaiced RGB48 image in device memory and its
  * homography from frame pixels to canvas pixels (Homography, Types.h:138-141,
  * in double).  gain is applied after the warp (RenderExecutor.cpp:111-114). */
+/* ---- pipelined render executor ------------------------------------------ */
+
+/* A device-resident RenderExecutor (RenderExecutor.cpp:40-147) for a sequence
+ * of frame sets of one panorama geometry: each submission uploads its CFA
+ * frames once, demosaics them (DemosaicBayer), renders every tile (the
+ * render plan) and downloads every tile output once - no per-operation host
+ * round trips (CudaPipeline.cpp:207-267 copies every operand on every call).
+ * `depth` device slots (1-4) let the upload of one submission, the render of
+ * the previous one and the download of the one before run at the same time
+ * on three streams.  Host buffers must be pinned for the copies to overlap
+ * and must stay valid until i360b_pipeline_wait returns. */
+typedef struct i360b_pipeline_desc
+{
+    int numFrames, frameWidth, frameHeight;
+    const double* toCanvas; /* numFrames x 9, frame -> canvas, row-major */
+    const float* gains;     /* numFrames: ApplyGain after the warp (RenderExecutor.cpp:111) */
+    unsigned short blackLevel;
+    float camMul[4];
+    float rgbCam[12]; /* 3x4, row-major */
+    uint32_t filters;
+    int numTiles;
+    const int* tileRects;    /* numTiles x 4: x, y, width, height */
+    const int* tileFirst;    /* numTiles: contributors[first .. first+count) */
+    const int* tileCount;    /* numTiles */
+    const int* contributors; /* frame indices */
+    int numBands;
+    int coordMode; /* I360B_COORDS_* */
+    int depth;     /* device slots, 1-4 (2 overlaps all three stages) */
+} i360b_pipeline_desc;
+
+typedef struct i360b_pipeline i360b_pipeline;
+
+I360B_API int i360b_pipeline_create(const i360b_pipeline_desc* desc, i360b_pipeline** out);
+/* Enqueues one frame set: hostCfa[numFrames] (width x height samples each)
+ * in, hostTiles[numTiles] (RGB48 tile outputs) out.  Returns at once. */
+I360B_API int i360b_pipeline_submit(i360b_pipeline* pipeline, const unsigned short* const* hostCfa,
+                                    unsigned short* const* hostTiles);
+/* Waits for every submission; *elapsedMs (optional) receives the device
+ * time from the first upload since the previous wait to the last download. */
+I360B_API int i360b_pipeline_wait(i360b_pipeline* pipeline, float* elapsedMs);
+/* i360b_render_plan_autotune on the first slot's plan (after a submission:
+ * the plan needs real frames), applied to every slot. */
+I360B_API int i360b_pipeline_autotune(i360b_pipeline* pipeline, int* bandRows, int* dtSlots, float* bestMs);
+I360B_API void i360b_pipeline_destroy(i360b_pipeline* pipeline);
+
 /* ---- export of rendered chunk outputs ----------------------------------- */
 
 /* The preview composite of PanoramaExporter::ExportPreviewJpeg
