@@ -1172,12 +1172,114 @@ __global__ void __launch_bounds__(256) k_down0(BlendArgs a, const Unit* __restri
     }
 }
 
+// One pixel of a blended band (the general path).
+__device__ __noinline__ void blend_pixel(const TileDev& T, const ItemCache& C, int level, int K, long long pl)
+{
+    const int lw = T.lw[level];
+    const bool top = level == T.bands - 1;
+    const int uw = T.lw[level + 1], uh = T.lh[level + 1];
+    const int y = (int)(pl / lw), x = (int)(pl - (long long)y * lw);
+    UpCoef c;
+    if (!top) c = up_coef_s(T.usx[level], T.usy[level], uw, uh, x, y);
+    const size_t p = T.loff[level] + pl;
+    float acc0 = 0.0f, acc1 = 0.0f, acc2 = 0.0f;
+    for (int k = 0; k < K; ++k)
+    {
+        float wv = __ldg(C.wg[k] + p);
+        float3 g = gauss_of(C.nd[k][p]);
+        if (!top)
+        {
+            const float4* up = C.nd[k] + T.loff[level + 1];
+            float3 a00 = gauss_of(up[(size_t)c.y0 * uw + c.x0]);
+            float3 a10 = gauss_of(up[(size_t)c.y0 * uw + c.x1]);
+            float3 a01 = gauss_of(up[(size_t)c.y1 * uw + c.x0]);
+            float3 a11 = gauss_of(up[(size_t)c.y1 * uw + c.x1]);
+            g.x = fsub(g.x, up_mix(a00.x, a10.x, a01.x, a11.x, c.wx, c.wy));
+            g.y = fsub(g.y, up_mix(a00.y, a10.y, a01.y, a11.y, c.wx, c.wy));
+            g.z = fsub(g.z, up_mix(a00.z, a10.z, a01.z, a11.z, c.wx, c.wy));
+        }
+        acc0 = fadd(acc0, fmul(wv, g.x));
+        acc1 = fadd(acc1, fmul(wv, g.y));
+        acc2 = fadd(acc2, fmul(wv, g.z));
+    }
+    float* b = T.blend + p * 3;
+    b[0] = acc0;
+    b[1] = acc1;
+    b[2] = acc2;
+}
+
+// Four consecutive pixels of a band below the top: for each contributor the
+// Up(G_l+1) taps slide along in a two-column window (the level above is half
+// as wide, so x0 advances by at most one column per pixel), each column's
+// texels and reciprocals computed once per contributor; every pixel's sum
+// still runs over the contributors in index order with its own weights.
+__device__ __forceinline__ void blend_quad(const TileDev& T, const ItemCache& C, int level, int K, long long pl,
+                                           int y, int x)
+{
+    const int uw = T.lw[level + 1], uh = T.lh[level + 1];
+    int x0[4];
+    float wx[4];
+    UpCoef c = up_coef_s(T.usx[level], T.usy[level], uw, uh, x, y);
+    const int y0 = c.y0, y1 = c.y1;
+    const float wy = c.wy;
+    x0[0] = c.x0;
+    wx[0] = c.wx;
+#pragma unroll
+    for (int i = 1; i < 4; ++i)
+    {
+        const UpCoef ci = up_coef_s(T.usx[level], T.usy[level], uw, uh, x + i, y);
+        x0[i] = ci.x0;
+        wx[i] = ci.wx;
+    }
+    const size_t p = T.loff[level] + pl;
+    float acc[4][3];
+#pragma unroll
+    for (int i = 0; i < 4; ++i) acc[i][0] = acc[i][1] = acc[i][2] = 0.0f;
+    for (int k = 0; k < K; ++k)
+    {
+        const float4* up = C.nd[k] + T.loff[level + 1];
+        int cur = x0[0];
+        float3 L0 = gauss_of(__ldg(up + (size_t)y0 * uw + cur)), L1 = gauss_of(__ldg(up + (size_t)y1 * uw + cur));
+        int nx = min(cur + 1, uw - 1);
+        float3 R0 = gauss_of(__ldg(up + (size_t)y0 * uw + nx)), R1 = gauss_of(__ldg(up + (size_t)y1 * uw + nx));
+#pragma unroll
+        for (int i = 0; i < 4; ++i)
+        {
+            if (x0[i] != cur)
+            {
+                cur = x0[i];
+                L0 = R0;
+                L1 = R1;
+                nx = min(cur + 1, uw - 1);
+                R0 = gauss_of(__ldg(up + (size_t)y0 * uw + nx));
+                R1 = gauss_of(__ldg(up + (size_t)y1 * uw + nx));
+            }
+            const float wv = __ldg(C.wg[k] + p + i);
+            float3 g = gauss_of(__ldg(C.nd[k] + p + i));
+            g.x = fsub(g.x, up_mix(L0.x, R0.x, L1.x, R1.x, wx[i], wy));
+            g.y = fsub(g.y, up_mix(L0.y, R0.y, L1.y, R1.y, wx[i], wy));
+            g.z = fsub(g.z, up_mix(L0.z, R0.z, L1.z, R1.z, wx[i], wy));
+            acc[i][0] = fadd(acc[i][0], fmul(wv, g.x));
+            acc[i][1] = fadd(acc[i][1], fmul(wv, g.y));
+            acc[i][2] = fadd(acc[i][2], fmul(wv, g.z));
+        }
+    }
+    float* b = T.blend + p * 3;
+#pragma unroll
+    for (int i = 0; i < 4; ++i)
+    {
+        b[3 * i] = acc[i][0];
+        b[3 * i + 1] = acc[i][1];
+        b[3 * i + 2] = acc[i][2];
+    }
+}
+
 // Blended band of one level: sum over the tile's contributors, in index
 // order, of weight * Laplacian (SeamBlend.cpp:501-509), where
 // Laplacian = G_l - Up(G_l+1) or G_top (SeamBlend.cpp:184-201).
 // Contributors that own no pixel have an all-zero weight pyramid and add
 // exactly +-0, so summing every contributor equals the reference's sum.
-__global__ void __launch_bounds__(256, 5) k_blend_level(BlendArgs a, const Unit* __restrict__ units, int level)
+__global__ void __launch_bounds__(256, 3) k_blend_level(BlendArgs a, const Unit* __restrict__ units, int level)
 {
     __shared__ ItemCache C;
     const Unit u = units[blockIdx.x];
@@ -1186,40 +1288,22 @@ __global__ void __launch_bounds__(256, 5) k_blend_level(BlendArgs a, const Unit*
     const int K = T.numItems;
     const int lw = T.lw[level], lh = T.lh[level];
     const bool top = level == T.bands - 1;
-    const int uw = T.lw[level + 1], uh = T.lh[level + 1];
-    const long long base = (long long)u.by * a.bandRows * lw;
-    const long long n = min((long long)a.bandRows * lw, (long long)lw * lh - base);
-    for (long long q = threadIdx.x; q < n; q += blockDim.x)
+    const int row0 = u.by * a.bandRows;
+    const int rows = min(a.bandRows, lh - row0);
+    const int qpr = (lw + 3) >> 2;
+    const int nq = rows * qpr;
+    for (int qi = threadIdx.x; qi < nq; qi += blockDim.x)
     {
-        const long long pl = base + q;
-        const int y = (int)(pl / lw), x = (int)(pl - (long long)y * lw);
-        UpCoef c;
-        if (!top) c = up_coef_s(T.usx[level], T.usy[level], uw, uh, x, y);
-        const size_t p = T.loff[level] + pl;
-        float acc0 = 0.0f, acc1 = 0.0f, acc2 = 0.0f;
-        for (int k = 0; k < K; ++k)
+        const int r = qi / qpr;
+        const int y = row0 + r, x = (qi - r * qpr) * 4;
+        const long long pl = (long long)y * lw + x;
+        const int cnt = min(4, lw - x);
+        if (!top && cnt == 4)
         {
-            float wv = __ldg(C.wg[k] + p);
-            float3 g = gauss_of(C.nd[k][p]);
-            if (!top)
-            {
-                const float4* up = C.nd[k] + T.loff[level + 1];
-                float3 a00 = gauss_of(up[(size_t)c.y0 * uw + c.x0]);
-                float3 a10 = gauss_of(up[(size_t)c.y0 * uw + c.x1]);
-                float3 a01 = gauss_of(up[(size_t)c.y1 * uw + c.x0]);
-                float3 a11 = gauss_of(up[(size_t)c.y1 * uw + c.x1]);
-                g.x = fsub(g.x, up_mix(a00.x, a10.x, a01.x, a11.x, c.wx, c.wy));
-                g.y = fsub(g.y, up_mix(a00.y, a10.y, a01.y, a11.y, c.wx, c.wy));
-                g.z = fsub(g.z, up_mix(a00.z, a10.z, a01.z, a11.z, c.wx, c.wy));
-            }
-            acc0 = fadd(acc0, fmul(wv, g.x));
-            acc1 = fadd(acc1, fmul(wv, g.y));
-            acc2 = fadd(acc2, fmul(wv, g.z));
+            blend_quad(T, C, level, K, pl, y, x);
+            continue;
         }
-        float* b = T.blend + p * 3;
-        b[0] = acc0;
-        b[1] = acc1;
-        b[2] = acc2;
+        for (int i = 0; i < cnt; ++i) blend_pixel(T, C, level, K, pl + i);
     }
 }
 
@@ -1255,7 +1339,116 @@ __global__ void __launch_bounds__(256) k_collapse(BlendArgs a, const Unit* __res
 // is 1 for its owner and 0 for every other contributor, so the blended level-0
 // band is exactly the owner's Laplacian img - Up(G1); the output is
 // clamp(that + Up(recon_1)) + 0.5 truncated, and 0 where nobody owns.
-__global__ void __launch_bounds__(256, 5) k_final0(BlendArgs a, const Unit* __restrict__ units)
+__device__ __forceinline__ void final_store(unsigned short* o, const float* r)
+{
+#pragma unroll
+    for (int ch = 0; ch < 3; ++ch)
+    {
+        float v = r[ch];
+        v = v < 65535.0f ? v : 65535.0f;
+        v = 0.0f < v ? v : 0.0f;
+        o[ch] = (unsigned short)__float2uint_rz(fadd(v, 0.5f));
+    }
+}
+
+// One output pixel (the general path).
+__device__ __noinline__ void final_pixel(const TileDev& T, const ItemCache& C, const float* rc, int uw, int uh,
+                                            long long p, int own)
+{
+    unsigned short* o = T.out + p * 3;
+    if (own < 0)
+    {
+        o[0] = o[1] = o[2] = 0;
+        return;
+    }
+    const int W = T.w;
+    const int y = (int)(p / W), x = (int)(p - (long long)y * W);
+    const unsigned short* px = C.img[own] + p * 3;
+    float r[3] = {(float)__ldg(px), (float)__ldg(px + 1), (float)__ldg(px + 2)};
+    if (T.bands > 1)
+    {
+        const UpCoef c = up_coef_s(T.usx[0], T.usy[0], uw, uh, x, y);
+        const float4* g1 = C.nd[own] + T.loff[1];
+        const float3 a00 = gauss_of(__ldg(g1 + (size_t)c.y0 * uw + c.x0));
+        const float3 a10 = gauss_of(__ldg(g1 + (size_t)c.y0 * uw + c.x1));
+        const float3 a01 = gauss_of(__ldg(g1 + (size_t)c.y1 * uw + c.x0));
+        const float3 a11 = gauss_of(__ldg(g1 + (size_t)c.y1 * uw + c.x1));
+        const float lap[3] = {fsub(r[0], up_mix(a00.x, a10.x, a01.x, a11.x, c.wx, c.wy)),
+                              fsub(r[1], up_mix(a00.y, a10.y, a01.y, a11.y, c.wx, c.wy)),
+                              fsub(r[2], up_mix(a00.z, a10.z, a01.z, a11.z, c.wx, c.wy))};
+#pragma unroll
+        for (int ch = 0; ch < 3; ++ch)
+        {
+            const float up = up_mix(__ldg(rc + ((size_t)c.y0 * uw + c.x0) * 3 + ch),
+                                    __ldg(rc + ((size_t)c.y0 * uw + c.x1) * 3 + ch),
+                                    __ldg(rc + ((size_t)c.y1 * uw + c.x0) * 3 + ch),
+                                    __ldg(rc + ((size_t)c.y1 * uw + c.x1) * 3 + ch), c.wx, c.wy);
+            r[ch] = fadd(lap[ch], up);
+        }
+    }
+    final_store(o, r);
+}
+
+// A level-1 texel column (rows y0 and y1) of the owner's hole-filled Gaussian
+// and of the level-1 reconstruction.
+struct TapColumn
+{
+    float3 g0, g1, u0, u1;
+};
+
+__device__ __forceinline__ TapColumn tap_column(const float4* g1, const float* rc, int uw, int y0, int y1, int col)
+{
+    const size_t q0 = (size_t)y0 * uw + col, q1 = (size_t)y1 * uw + col;
+    TapColumn t;
+    t.g0 = gauss_of(__ldg(g1 + q0));
+    t.g1 = gauss_of(__ldg(g1 + q1));
+    t.u0 = make_float3(__ldg(rc + q0 * 3), __ldg(rc + q0 * 3 + 1), __ldg(rc + q0 * 3 + 2));
+    t.u1 = make_float3(__ldg(rc + q1 * 3), __ldg(rc + q1 * 3 + 1), __ldg(rc + q1 * 3 + 2));
+    return t;
+}
+
+// Four consecutive pixels of one row with one owner share their level-1
+// taps.  Level 1 is half as wide (align-corners scale <= 0.5), so from one
+// pixel to the next x0 advances by at most one column: a window of two
+// columns (x0 and min(x0 + 1, w - 1), which is always x1) slides along, each
+// column's texels and reciprocals computed once; every pixel still combines
+// its own four taps with its own weights in the reference's order.
+__device__ __forceinline__ void final_quad(const TileDev& T, const ItemCache& C, const float* rc, int uw, int uh,
+                                           long long p, int y, int x, int own)
+{
+    const float4* g1 = C.nd[own] + T.loff[1];
+    UpCoef c = up_coef_s(T.usx[0], T.usy[0], uw, uh, x, y);
+    int cur = c.x0;
+    TapColumn L = tap_column(g1, rc, uw, c.y0, c.y1, cur);
+    TapColumn R = tap_column(g1, rc, uw, c.y0, c.y1, c.x1);
+    const unsigned short* px = C.img[own] + p * 3;
+    unsigned short* o = T.out + p * 3;
+#pragma unroll
+    for (int i = 0; i < 4; ++i)
+    {
+        if (i > 0)
+        {
+            c = up_coef_s(T.usx[0], T.usy[0], uw, uh, x + i, y);
+            if (c.x0 != cur)  // advanced by one column
+            {
+                cur = c.x0;
+                L = R;
+                R = tap_column(g1, rc, uw, c.y0, c.y1, c.x1);
+            }
+        }
+        const float wx = c.wx, wy = c.wy;
+        float r[3] = {(float)__ldg(px + 3 * i), (float)__ldg(px + 3 * i + 1), (float)__ldg(px + 3 * i + 2)};
+        const float lap[3] = {fsub(r[0], up_mix(L.g0.x, R.g0.x, L.g1.x, R.g1.x, wx, wy)),
+                              fsub(r[1], up_mix(L.g0.y, R.g0.y, L.g1.y, R.g1.y, wx, wy)),
+                              fsub(r[2], up_mix(L.g0.z, R.g0.z, L.g1.z, R.g1.z, wx, wy))};
+        r[0] = fadd(lap[0], up_mix(L.u0.x, R.u0.x, L.u1.x, R.u1.x, wx, wy));
+        r[1] = fadd(lap[1], up_mix(L.u0.y, R.u0.y, L.u1.y, R.u1.y, wx, wy));
+        r[2] = fadd(lap[2], up_mix(L.u0.z, R.u0.z, L.u1.z, R.u1.z, wx, wy));
+        final_store(o + 3 * i, r);
+    }
+}
+
+__global__ void __launch_bounds__(256) k_final0(BlendArgs a, const Unit* __restrict__ units)
 {
     __shared__ ItemCache C;
     const Unit u = units[blockIdx.x];
@@ -1264,63 +1457,27 @@ __global__ void __launch_bounds__(256, 5) k_final0(BlendArgs a, const Unit* __re
     const int W = T.w, H = T.h;
     const int uw = T.lw[1], uh = T.lh[1];
     const float* rc = T.blend + T.loff[1] * 3;
-    const long long base = (long long)u.by * a.bandRows * W;
-    const long long n = min((long long)a.bandRows * W, (long long)W * H - base);
-    constexpr int B = 4;  // pixels per thread in flight
-    for (long long q0 = threadIdx.x; q0 < n; q0 += (long long)blockDim.x * B)
+    const int row0 = u.by * a.bandRows;
+    const int rows = min(a.bandRows, H - row0);
+    const int qpr = (W + 3) >> 2;  // quads per row
+    const int nq = rows * qpr;
+    for (int qi = threadIdx.x; qi < nq; qi += blockDim.x)
     {
-        int own[B];
-        long long pp[B];
+        const int y = row0 + qi / qpr;
+        const int x = (qi - (qi / qpr) * qpr) * 4;
+        const long long p = (long long)y * W + x;
+        const int cnt = min(4, W - x);
+        int own[4];
 #pragma unroll
-        for (int b = 0; b < B; ++b)
+        for (int i = 0; i < 4; ++i) own[i] = i < cnt ? (int)T.owner[p + i] : -2;
+        if (cnt == 4 && T.bands > 1 && own[0] >= 0 && own[1] == own[0] && own[2] == own[0] && own[3] == own[0])
         {
-            pp[b] = base + q0 + (long long)b * blockDim.x;
-            own[b] = (q0 + (long long)b * blockDim.x < n) ? (int)T.owner[pp[b]] : -2;
+            final_quad(T, C, rc, uw, uh, p, y, x, own[0]);
+            continue;
         }
 #pragma unroll
-        for (int b = 0; b < B; ++b)
-        {
-            if (own[b] == -2) continue;
-            const long long p = pp[b];
-            unsigned short* o = T.out + p * 3;
-            if (own[b] < 0)
-            {
-                o[0] = o[1] = o[2] = 0;
-                continue;
-            }
-            const int y = (int)(p / W), x = (int)(p - (long long)y * W);
-            const unsigned short* px = C.img[own[b]] + p * 3;
-            float r[3] = {(float)__ldg(px), (float)__ldg(px + 1), (float)__ldg(px + 2)};
-            if (T.bands > 1)
-            {
-                const UpCoef c = up_coef_s(T.usx[0], T.usy[0], uw, uh, x, y);
-                const float4* g1 = C.nd[own[b]] + T.loff[1];
-                const float3 a00 = gauss_of(__ldg(g1 + (size_t)c.y0 * uw + c.x0));
-                const float3 a10 = gauss_of(__ldg(g1 + (size_t)c.y0 * uw + c.x1));
-                const float3 a01 = gauss_of(__ldg(g1 + (size_t)c.y1 * uw + c.x0));
-                const float3 a11 = gauss_of(__ldg(g1 + (size_t)c.y1 * uw + c.x1));
-                const float lap[3] = {fsub(r[0], up_mix(a00.x, a10.x, a01.x, a11.x, c.wx, c.wy)),
-                                      fsub(r[1], up_mix(a00.y, a10.y, a01.y, a11.y, c.wx, c.wy)),
-                                      fsub(r[2], up_mix(a00.z, a10.z, a01.z, a11.z, c.wx, c.wy))};
-#pragma unroll
-                for (int ch = 0; ch < 3; ++ch)
-                {
-                    const float up = up_mix(__ldg(rc + ((size_t)c.y0 * uw + c.x0) * 3 + ch),
-                                            __ldg(rc + ((size_t)c.y0 * uw + c.x1) * 3 + ch),
-                                            __ldg(rc + ((size_t)c.y1 * uw + c.x0) * 3 + ch),
-                                            __ldg(rc + ((size_t)c.y1 * uw + c.x1) * 3 + ch), c.wx, c.wy);
-                    r[ch] = fadd(lap[ch], up);
-                }
-            }
-#pragma unroll
-            for (int ch = 0; ch < 3; ++ch)
-            {
-                float v = r[ch];
-                v = v < 65535.0f ? v : 65535.0f;
-                v = 0.0f < v ? v : 0.0f;
-                o[ch] = (unsigned short)__float2uint_rz(fadd(v, 0.5f));
-            }
-        }
+        for (int i = 0; i < 4; ++i)
+            if (i < cnt) final_pixel(T, C, rc, uw, uh, p + i, own[i]);
     }
 }
 }  // namespace
