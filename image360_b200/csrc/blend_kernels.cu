@@ -114,12 +114,27 @@ __global__ void __launch_bounds__(256) k_coverage(BlendArgs a, const Unit* __res
 // buffer (RenderExecutor.cpp:104-114), coverage and box emitted in the same
 // pass.  Arithmetic identical to k_warp in pixel_ops.cu.
 // ---------------------------------------------------------------------------
-__device__ __forceinline__ void warp_px(const ItemDev& it, float dX, float dY, unsigned short o[3])
+// The warp parameters of one item, read once per CTA into registers (the
+// item table is in global memory, where the compiler cannot tell it apart
+// from the image being written).
+struct WarpItem
+{
+    float H[9];
+    const unsigned short* src;
+    int srcW, srcH;
+    float gain;
+    bool applyGain;
+};
+
+// One destination pixel (WarpPerspectiveKernels.h:16-43 and WarpPerspective_Scalar.cpp:8-45,
+// then ApplyGain, GainColorOps.cpp:16-26).  hy = {H[1] dY, H[4] dY, H[7] dY}
+// for the row: the same rounded products, summed in the reference's order.
+__device__ __forceinline__ void warp_px(const WarpItem& it, float dX, const float* hy, unsigned short o[3])
 {
     const float* H = it.H;
-    float sx = fadd(fadd(fmul(H[0], dX), fmul(H[1], dY)), H[2]);
-    float sy = fadd(fadd(fmul(H[3], dX), fmul(H[4], dY)), H[5]);
-    float sw1 = fadd(fadd(fmul(H[6], dX), fmul(H[7], dY)), H[8]);
+    float sx = fadd(fadd(fmul(H[0], dX), hy[0]), H[2]);
+    float sy = fadd(fadd(fmul(H[3], dX), hy[1]), H[5]);
+    float sw1 = fadd(fadd(fmul(H[6], dX), hy[2]), H[8]);
     o[0] = o[1] = o[2] = 0;
     if (fabsf(sw1) < 1e-10f) return;
     sx = fdiv(sx, sw1);
@@ -136,14 +151,13 @@ __device__ __forceinline__ void warp_px(const ItemDev& it, float dX, float dY, u
     unsigned short b0 = __ldg(r1), b1 = __ldg(r1 + 1), b2 = __ldg(r1 + 2), b3 = __ldg(r1 + 3), b4 = __ldg(r1 + 4),
                    b5 = __ldg(r1 + 5);
     const unsigned short t00[3] = {a0, a1, a2}, t10[3] = {a3, a4, a5}, t01[3] = {b0, b1, b2}, t11[3] = {b3, b4, b5};
-    const bool applyGain = !gain_is_identity(it.gain);
 #pragma unroll
     for (int c = 0; c < 3; ++c)
     {
         float v = fadd(fadd(fadd(fmul(w00, (float)t00[c]), fmul(w10, (float)t10[c])), fmul(w01, (float)t01[c])),
                        fmul(w11, (float)t11[c]));
         unsigned short q = clamp_trunc_u16(v);
-        if (applyGain) q = clamp_trunc_u16(fmul((float)q, it.gain));
+        if (it.applyGain) q = clamp_trunc_u16(fmul((float)q, it.gain));
         o[c] = q;
     }
 }
@@ -155,21 +169,31 @@ __global__ void __launch_bounds__(256) k_warp_tiles(BlendArgs a, const Unit* __r
     const TileDev& T = a.tiles[it.tile];
     const int W = T.w, H = T.h, lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     unsigned short* img = const_cast<unsigned short*>(it.img);
+    WarpItem wi;
+#pragma unroll
+    for (int q = 0; q < 9; ++q) wi.H[q] = it.H[q];
+    wi.src = it.src;
+    wi.srcW = it.srcW;
+    wi.srcH = it.srcH;
+    wi.gain = it.gain;
+    wi.applyGain = !gain_is_identity(it.gain);
+    const int offX = it.offX, offY = it.offY, vx0 = it.vx0, vx1 = it.vx1, vy0 = it.vy0, vy1 = it.vy1;
     BoxAcc box;
     const int rowsPerWarp = a.bandRows >> 3;
     for (int r = 0; r < rowsPerWarp; ++r)
     {
         const int y = u.by * a.bandRows + warp * rowsPerWarp + r;
         if (y >= H) break;
-        const float dY = (float)(y + it.offY);
-        const bool rowIn = y >= it.vy0 && y <= it.vy1;
+        const float dY = (float)(y + offY);
+        const float hy[3] = {fmul(wi.H[1], dY), fmul(wi.H[4], dY), fmul(wi.H[7], dY)};
+        const bool rowIn = y >= vy0 && y <= vy1;
         for (int x0 = 0; x0 < W; x0 += 64)
         {
             // Two independent pixels per lane keep more gathers in flight.
             const int xa = x0 + lane, xb = x0 + 32 + lane;
             unsigned short oa[3] = {0, 0, 0}, ob[3] = {0, 0, 0};
-            if (rowIn && xa < W && xa >= it.vx0 && xa <= it.vx1) warp_px(it, (float)(xa + it.offX), dY, oa);
-            if (rowIn && xb < W && xb >= it.vx0 && xb <= it.vx1) warp_px(it, (float)(xb + it.offX), dY, ob);
+            if (rowIn && xa < W && xa >= vx0 && xa <= vx1) warp_px(wi, (float)(xa + offX), hy, oa);
+            if (rowIn && xb < W && xb >= vx0 && xb <= vx1) warp_px(wi, (float)(xb + offX), hy, ob);
             bool ca = (oa[0] | oa[1] | oa[2]) != 0, cb = (ob[0] | ob[1] | ob[2]) != 0;
             if (xa < W)
             {
@@ -1265,12 +1289,22 @@ __device__ __forceinline__ void blend_quad(const TileDev& T, const ItemCache& C,
         }
     }
     float* b = T.blend + p * 3;
-#pragma unroll
-    for (int i = 0; i < 4; ++i)
+    if ((reinterpret_cast<uintptr_t>(b) & 15) == 0)  // the quad's 48 bytes: three 16-byte stores
     {
-        b[3 * i] = acc[i][0];
-        b[3 * i + 1] = acc[i][1];
-        b[3 * i + 2] = acc[i][2];
+        float4* b4 = reinterpret_cast<float4*>(b);
+        b4[0] = make_float4(acc[0][0], acc[0][1], acc[0][2], acc[1][0]);
+        b4[1] = make_float4(acc[1][1], acc[1][2], acc[2][0], acc[2][1]);
+        b4[2] = make_float4(acc[2][2], acc[3][0], acc[3][1], acc[3][2]);
+    }
+    else
+    {
+#pragma unroll
+        for (int i = 0; i < 4; ++i)
+        {
+            b[3 * i] = acc[i][0];
+            b[3 * i + 1] = acc[i][1];
+            b[3 * i + 2] = acc[i][2];
+        }
     }
 }
 
@@ -1423,6 +1457,7 @@ __device__ __forceinline__ void final_quad(const TileDev& T, const ItemCache& C,
     TapColumn R = tap_column(g1, rc, uw, c.y0, c.y1, c.x1);
     const unsigned short* px = C.img[own] + p * 3;
     unsigned short* o = T.out + p * 3;
+    unsigned short res[12];
 #pragma unroll
     for (int i = 0; i < 4; ++i)
     {
@@ -1444,7 +1479,21 @@ __device__ __forceinline__ void final_quad(const TileDev& T, const ItemCache& C,
         r[0] = fadd(lap[0], up_mix(L.u0.x, R.u0.x, L.u1.x, R.u1.x, wx, wy));
         r[1] = fadd(lap[1], up_mix(L.u0.y, R.u0.y, L.u1.y, R.u1.y, wx, wy));
         r[2] = fadd(lap[2], up_mix(L.u0.z, R.u0.z, L.u1.z, R.u1.z, wx, wy));
-        final_store(o + 3 * i, r);
+        final_store(res + 3 * i, r);
+    }
+    // the quad's 24 bytes: three 8-byte stores when aligned
+    if ((reinterpret_cast<uintptr_t>(o) & 7) == 0)
+    {
+        uint2* o2 = reinterpret_cast<uint2*>(o);
+#pragma unroll
+        for (int k = 0; k < 3; ++k)
+            o2[k] = make_uint2((uint32_t)res[4 * k] | ((uint32_t)res[4 * k + 1] << 16),
+                               (uint32_t)res[4 * k + 2] | ((uint32_t)res[4 * k + 3] << 16));
+    }
+    else
+    {
+#pragma unroll
+        for (int k = 0; k < 12; ++k) o[k] = res[k];
     }
 }
 
