@@ -7,10 +7,12 @@
 // device on every call (CudaPipeline.cpp:207-267); here each submission makes
 // exactly one upload of its CFA frames and one download of its chunk outputs,
 // and `depth` device slots (CFA frames, demosaiced frames, a render plan and
-// its chunk outputs) let three streams work on different submissions at once:
-// the upload of set k+1, the demosaic and render of set k, the download of
-// set k-1.  Per slot, events order the three stages against the slot's
-// previous use: its upload waits until the previous render of the slot has
+// its chunk outputs, and a compute stream of its own) let different
+// submissions run at once: the upload of set k+1, the demosaic and render of
+// sets k and k-1 (the latency-bound stages of one render - the chamfer
+// wavefront, the seam search - overlap the bandwidth-bound stages of the
+// other), the download of set k-2.  Per slot, events order the three stages
+// against the slot's previous use: its upload waits until the previous render of the slot has
 // read the CFA, its render waits for its upload and for the previous download
 // of the slot's outputs, its download waits for its render.  Host buffers must
 // be pinned for the copies to overlap, and must stay valid until the
@@ -30,6 +32,7 @@ struct i360b_pipeline
         unsigned short* rgb = nullptr;   // numFrames x w x h x 3
         unsigned short* outs = nullptr;  // every tile's output, back to back
         i360b_render_plan* plan = nullptr;
+        cudaStream_t comp = nullptr;     // demosaic and render of this slot
         cudaEvent_t uploaded = nullptr, rendered = nullptr, downloaded = nullptr;
         bool used = false;
     };
@@ -40,18 +43,20 @@ struct i360b_pipeline
     std::vector<size_t> tileOff;    // element offset of each tile output in a slot's `outs`
     std::vector<size_t> tileBytes;  // bytes of each tile output
     std::vector<Slot> slots;
-    cudaStream_t up = nullptr, comp = nullptr, down = nullptr;
+    cudaStream_t up = nullptr, down = nullptr;
     cudaEvent_t start = nullptr, end = nullptr;
     long long submitted = 0;
     bool timing = false;
 
     ~i360b_pipeline()
     {
-        for (cudaStream_t s : {up, comp, down})
+        for (cudaStream_t s : {up, down})
             if (s) cudaStreamSynchronize(s);
         for (Slot& S : slots)
         {
+            if (S.comp) cudaStreamSynchronize(S.comp);
             if (S.plan) i360b_render_plan_destroy(S.plan);
+            if (S.comp) cudaStreamDestroy(S.comp);
             cudaFree(S.cfa);
             cudaFree(S.rgb);
             cudaFree(S.outs);
@@ -60,7 +65,7 @@ struct i360b_pipeline
         }
         for (cudaEvent_t e : {start, end})
             if (e) cudaEventDestroy(e);
-        for (cudaStream_t s : {up, comp, down})
+        for (cudaStream_t s : {up, down})
             if (s) cudaStreamDestroy(s);
     }
 };
@@ -76,6 +81,7 @@ int make_slot(i360b_pipeline& P, const i360b_pipeline_desc& d, i360b_pipeline::S
     I360B_CUDA(cudaMalloc(&S.outs, outElems * sizeof(unsigned short)), "pipeline chunk outputs");
     for (cudaEvent_t* e : {&S.uploaded, &S.rendered, &S.downloaded})
         I360B_CUDA(cudaEventCreateWithFlags(e, cudaEventDisableTiming), "pipeline event");
+    I360B_CUDA(cudaStreamCreateWithFlags(&S.comp, cudaStreamNonBlocking), "pipeline stream");
     std::vector<i360b_frame> frames(P.nFrames);
     for (int f = 0; f < P.nFrames; ++f)
     {
@@ -136,7 +142,7 @@ extern "C" int i360b_pipeline_create(const i360b_pipeline_desc* d, i360b_pipelin
         P->tileBytes.push_back(elems * sizeof(unsigned short));
         P->tileOff.push_back(P->tileOff.back() + ((elems + 127) & ~size_t(127)));  // 256-byte aligned outputs
     }
-    for (cudaStream_t* s : {&P->up, &P->comp, &P->down})
+    for (cudaStream_t* s : {&P->up, &P->down})
         I360B_CUDA(cudaStreamCreateWithFlags(s, cudaStreamNonBlocking), "pipeline stream");
     for (cudaEvent_t* e : {&P->start, &P->end}) I360B_CUDA(cudaEventCreate(e), "pipeline event");
     P->slots.resize(d->depth);
@@ -171,13 +177,13 @@ extern "C" int i360b_pipeline_submit(i360b_pipeline* P, const unsigned short* co
                    "pipeline upload");
     I360B_CUDA(cudaEventRecord(S.uploaded, P->up), "pipeline order");
     // demosaic and render: after the upload and the slot's previous download
-    I360B_CUDA(cudaStreamWaitEvent(P->comp, S.uploaded, 0), "pipeline order");
-    if (S.used) I360B_CUDA(cudaStreamWaitEvent(P->comp, S.downloaded, 0), "pipeline order");
+    I360B_CUDA(cudaStreamWaitEvent(S.comp, S.uploaded, 0), "pipeline order");
+    if (S.used) I360B_CUDA(cudaStreamWaitEvent(S.comp, S.downloaded, 0), "pipeline order");
     for (int f = 0; f < P->nFrames; ++f)
         I360B_TRY(launch_demosaic(S.cfa + px * f, P->w, P->h, P->black, P->camMul, P->rgbCam, P->filters,
-                                  S.rgb + px * 3 * f, P->comp));
-    I360B_TRY(S.plan->plan.execute(P->comp, true));
-    I360B_CUDA(cudaEventRecord(S.rendered, P->comp), "pipeline order");
+                                  S.rgb + px * 3 * f, S.comp));
+    I360B_TRY(S.plan->plan.execute(S.comp, true));
+    I360B_CUDA(cudaEventRecord(S.rendered, S.comp), "pipeline order");
     // download: after the render
     I360B_CUDA(cudaStreamWaitEvent(P->down, S.rendered, 0), "pipeline order");
     for (size_t t = 0; t < P->tileOff.size(); ++t)
@@ -200,7 +206,7 @@ extern "C" int i360b_pipeline_wait(i360b_pipeline* P, float* elapsedMs)
     if (P->timing && elapsedMs) I360B_CUDA(cudaEventElapsedTime(elapsedMs, P->start, P->end), "pipeline timing");
     P->timing = false;
     for (auto& S : P->slots)
-        if (S.used) I360B_TRY(S.plan->plan.check(P->comp));
+        if (S.used) I360B_TRY(S.plan->plan.check(S.comp));
     return I360B_SUCCESS;
 }
 
@@ -212,8 +218,9 @@ extern "C" int i360b_pipeline_autotune(i360b_pipeline* P, int* bandRows, int* dt
     I360B_TRY(i360b_pipeline_wait(P, nullptr));
     int rows = 0, ring = 0;
     float ms = 0.0f;
-    I360B_TRY(i360b_render_plan_autotune(P->slots[0].plan, P->comp, &rows, &ring, &ms));
-    for (size_t k = 1; k < P->slots.size(); ++k) I360B_TRY(P->slots[k].plan->plan.set_tuning(rows, ring, P->comp));
+    I360B_TRY(i360b_render_plan_autotune(P->slots[0].plan, P->slots[0].comp, &rows, &ring, &ms));
+    for (size_t k = 1; k < P->slots.size(); ++k)
+        I360B_TRY(P->slots[k].plan->plan.set_tuning(rows, ring, P->slots[k].comp));
     if (bandRows) *bandRows = rows;
     if (dtSlots) *dtSlots = ring;
     if (bestMs) *bestMs = ms;

@@ -209,9 +209,10 @@ I360B_API int i360b_launch_blend_noalloc(const unsigned short* const* dWarped, i
  * frames once, demosaics them (DemosaicBayer), renders every tile (the
  * render plan) and downloads every tile output once - no per-operation host
  * round trips (CudaPipeline.cpp:207-267 copies every operand on every call).
- * `depth` device slots (1-4) let the upload of one submission, the render of
- * the previous one and the download of the one before run at the same time
- * on three streams.  Host buffers must be pinned for the copies to overlap
+ * `depth` device slots (1-4), each with its own compute stream, let the
+ * upload of one submission, the renders of the previous ones and the
+ * download of an earlier one run at the same time (two renders overlap the
+ * latency-bound stages of one with the bandwidth-bound stages of the other).  Host buffers must be pinned for the copies to overlap
  * and must stay valid until i360b_pipeline_wait returns. */
 typedef struct i360b_pipeline_desc
 {
