@@ -227,17 +227,51 @@ int Plan::build(const std::vector<TileSpec>& specs, int numBands, bool renderPat
         }
     }
     nItems = (int)items.size();
+    // ---- chains: tiles split into two groups of about equal work ----------
+    nChains = nTiles >= 2 ? kMaxChains : 1;
+    tileChain.assign(nTiles, 0);
+    if (nChains > 1)
+    {
+        std::vector<int> order(nTiles);
+        for (int t = 0; t < nTiles; ++t) order[t] = t;
+        auto load = [&](int t) { return (double)tiles[t].w * tiles[t].h * (1 + tiles[t].numItems); };
+        std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return load(a) > load(b); });
+        double sum[kMaxChains] = {0.0, 0.0};
+        for (int t : order)
+        {
+            const int c = sum[1] < sum[0] ? 1 : 0;
+            tileChain[t] = c;
+            sum[c] += load(t);
+        }
+    }
     // ---- work lists -------------------------------------------------------
     std::vector<Unit> units;
     make_units(8, units);  // the largest list any band height needs
     unitCap = (int)units.size();
     make_units(bandRows, units);
     std::vector<int> ints;
-    for (int i = 0; i < nItems; ++i) ints.push_back(i);
+    for (int c = 0; c < nChains; ++c)
+    {
+        dtRange[c].start = (int)ints.size();
+        for (int i = 0; i < nItems; ++i)
+            if (tileChain[items[i].tile] == c) ints.push_back(i);
+        dtRange[c].count = (int)ints.size() - dtRange[c].start;
+    }
     int seamStart = (int)ints.size();
-    for (int t = 0; t < nTiles; ++t)
-        if (tiles[t].numItems >= 2) ints.push_back(t);
+    for (int c = 0; c < nChains; ++c)
+    {
+        seamRange[c].start = (int)ints.size() - seamStart;
+        for (int t = 0; t < nTiles; ++t)
+            if (tileChain[t] == c && tiles[t].numItems >= 2) ints.push_back(t);
+        seamRange[c].count = (int)ints.size() - seamStart - seamRange[c].start;
+    }
     nSeam = (int)ints.size() - seamStart;
+    if (nChains > 1)
+    {
+        I360B_CUDA(cudaStreamCreateWithFlags(&side, cudaStreamNonBlocking), "chain stream");
+        I360B_CUDA(cudaEventCreateWithFlags(&evFork, cudaEventDisableTiming), "chain event");
+        I360B_CUDA(cudaEventCreateWithFlags(&evJoin, cudaEventDisableTiming), "chain event");
+    }
     // ---- device allocation -----------------------------------------------
     size_t unitBytes = align256(std::max<size_t>(unitCap, 1) * sizeof(Unit));
     size_t intBytes = align256(std::max<size_t>(ints.size(), 1) * sizeof(int));
@@ -330,6 +364,9 @@ int Plan::build(const std::vector<TileSpec>& specs, int numBands, bool renderPat
     return I360B_SUCCESS;
 }
 
+// Lists per chain, kListsPerChain each (index chain * kListsPerChain + list).
+constexpr int kListsPerChain = 3 + (kMaxBands - 1) + kMaxBands + kMaxBands;
+
 void Plan::make_units(int rows, std::vector<Unit>& units)
 {
     units.clear();
@@ -345,41 +382,49 @@ void Plan::make_units(int rows, std::vector<Unit>& units)
     lists.clear();
     auto beginList = [&]() { return (int)units.size(); };
     auto endList = [&](int start) { lists.push_back(Range{start, (int)units.size() - start}); };
-    int s;
-    s = beginList();  // 0: coverage / warp
-    for (int i = 0; i < nItems; ++i) addBands(i, tiles[items[i].tile].h);
-    endList(s);
-    s = beginList();  // 1: ownership
-    for (int t = 0; t < nTiles; ++t) addBands(t, tiles[t].h);
-    endList(s);
-    s = beginList();  // 2: level 0 output
-    for (int t = 0; t < nTiles; ++t) addBands(t, tiles[t].h);
-    endList(s);
-    for (int l = 0; l < kMaxBands - 1; ++l)  // 3 + l: down from level l
+    for (int c = 0; c < nChains; ++c)
     {
-        s = beginList();
+        auto inT = [&](int t) { return tileChain.empty() || tileChain[t] == c; };
+        auto inI = [&](int i) { return inT(items[i].tile); };
+        int s;
+        s = beginList();  // 0: coverage / warp
         for (int i = 0; i < nItems; ++i)
+            if (inI(i)) addBands(i, tiles[items[i].tile].h);
+        endList(s);
+        s = beginList();  // 1: ownership
+        for (int t = 0; t < nTiles; ++t)
+            if (inT(t)) addBands(t, tiles[t].h);
+        endList(s);
+        s = beginList();  // 2: level 0 output
+        for (int t = 0; t < nTiles; ++t)
+            if (inT(t)) addBands(t, tiles[t].h);
+        endList(s);
+        for (int l = 0; l < kMaxBands - 1; ++l)  // 3 + l: down from level l
         {
-            const TileDev& T = tiles[items[i].tile];
-            if (T.bands > l + 1) addBlocks(i, T.lw[l + 1], T.lh[l + 1]);
+            s = beginList();
+            for (int i = 0; i < nItems; ++i)
+            {
+                const TileDev& T = tiles[items[i].tile];
+                if (inI(i) && T.bands > l + 1) addBlocks(i, T.lw[l + 1], T.lh[l + 1]);
+            }
+            endList(s);
         }
-        endList(s);
-    }
-    for (int l = 0; l < kMaxBands; ++l)  // 3 + (kMaxBands-1) + l: blend band at level l (l >= 1)
-    {
-        s = beginList();
-        if (l >= 1)
-            for (int t = 0; t < nTiles; ++t)
-                if (tiles[t].bands > l) addBands(t, tiles[t].lh[l]);
-        endList(s);
-    }
-    for (int l = 0; l < kMaxBands; ++l)  // 3 + 2*kMaxBands - 1 + l: collapse at level l (1 <= l <= bands-2)
-    {
-        s = beginList();
-        if (l >= 1)
-            for (int t = 0; t < nTiles; ++t)
-                if (tiles[t].bands > l + 1) addBands(t, tiles[t].lh[l]);
-        endList(s);
+        for (int l = 0; l < kMaxBands; ++l)  // 3 + (kMaxBands-1) + l: blend band at level l (l >= 1)
+        {
+            s = beginList();
+            if (l >= 1)
+                for (int t = 0; t < nTiles; ++t)
+                    if (inT(t) && tiles[t].bands > l) addBands(t, tiles[t].lh[l]);
+            endList(s);
+        }
+        for (int l = 0; l < kMaxBands; ++l)  // 3 + 2*kMaxBands - 1 + l: collapse at level l (1 <= l <= bands-2)
+        {
+            s = beginList();
+            if (l >= 1)
+                for (int t = 0; t < nTiles; ++t)
+                    if (inT(t) && tiles[t].bands > l + 1) addBands(t, tiles[t].lh[l]);
+            endList(s);
+        }
     }
 }
 
@@ -404,6 +449,10 @@ int Plan::set_tuning(int rows, int slots, cudaStream_t s)
 
 Plan::~Plan()
 {
+    if (side) cudaStreamSynchronize(side);
+    if (evFork) cudaEventDestroy(evFork);
+    if (evJoin) cudaEventDestroy(evJoin);
+    if (side) cudaStreamDestroy(side);
     if (graphExec) cudaGraphExecDestroy(graphExec);
     if (graph) cudaGraphDestroy(graph);
     if (hostErr) cudaFreeHost(hostErr);
@@ -417,65 +466,114 @@ const char* const kStageNames[kStages] = {"warp_gain_coverage", "chamfer_forward
 
 int Plan::kernels_per_execute() const
 {
-    int n = (nItems > 0 ? 1 : 0) + (lists[0].count > 0 ? 1 : 0) + (nItems > 0 ? 2 : 0) + (lists[1].count > 0 ? 1 : 0) +
-            (nSeam > 0 ? 1 : 0) + (lists[2].count > 0 ? 1 : 0);
-    for (size_t i = 3; i < lists.size(); ++i) n += lists[i].count > 0 ? 1 : 0;
+    int n = (nItems > 0 ? 1 : 0);  // bbox reset
+    for (int c = 0; c < nChains; ++c)
+    {
+        const Range* L = &lists[(size_t)c * kListsPerChain];
+        n += (L[0].count > 0 ? 1 : 0) + (dtRange[c].count > 0 ? 2 : 0) + (L[1].count > 0 ? 1 : 0) +
+             (seamRange[c].count > 0 ? 1 : 0) + (L[2].count > 0 ? 1 : 0);
+        for (int i = 3; i < kListsPerChain; ++i) n += L[i].count > 0 ? 1 : 0;
+    }
     return n;
 }
 
 int Plan::enqueue_warp(cudaStream_t s)
 {
-    BlendArgs a{dItems, dTiles, dError, dSeamCycles, bandRows};
     if (nItems > 0) k_init_bbox<<<(nItems + 127) / 128, 128, 0, s>>>(dItems, nItems);
     I360B_TRY(check_launch("bbox init kernel"));
     I360B_CUDA(cudaMemsetAsync(dError, 0, sizeof(int), s), "error flag reset");
-    const Range r = lists[0];
-    if (render) return launch_warp_tiles(a, dUnits + r.start, r.count, s);
-    return launch_coverage(a, dUnits + r.start, r.count, s);
+    for (int c = 0; c < nChains; ++c) I360B_TRY(enqueue_chain(c, 0, 0, s));
+    return I360B_SUCCESS;
+}
+
+int Plan::enqueue_chain(int c, int first, int last, cudaStream_t s)
+{
+    BlendArgs a{dItems, dTiles, dError, dSeamCycles, bandRows};
+    const Range* L = &lists[(size_t)c * kListsPerChain];
+    for (int stage = first; stage <= last; ++stage)
+    {
+        Range r;
+        switch (stage)
+        {
+        case 0:
+            r = L[0];
+            I360B_TRY(render ? launch_warp_tiles(a, dUnits + r.start, r.count, s)
+                             : launch_coverage(a, dUnits + r.start, r.count, s));
+            break;
+        case 1:
+        case 2:
+            I360B_TRY(launch_dt(a, dInts + dtRange[c].start, dtRange[c].count, stage == 2, maxW, maxH, dtSlots, s));
+            break;
+        case 3:
+            r = L[1];
+            I360B_TRY(launch_owner(a, dUnits + r.start, r.count, s));
+            break;
+        case 4:
+            I360B_TRY(launch_seam(a, seamList + seamRange[c].start, seamRange[c].count, s));
+            break;
+        case 5:
+        case 6:  // pyramid: level 0 -> 1 (stage 5), then the levels above (stage 6)
+            for (int l = stage == 5 ? 0 : 1; l < (stage == 5 ? 1 : kMaxBands - 1); ++l)
+            {
+                r = L[3 + l];
+                I360B_TRY(launch_down(a, dUnits + r.start, r.count, l, s));
+            }
+            break;
+        case 7:
+            for (int l = kMaxBands - 1; l >= 1; --l)
+            {
+                r = L[3 + (kMaxBands - 1) + l];
+                I360B_TRY(launch_blend_level(a, dUnits + r.start, r.count, l, s));
+            }
+            break;
+        case 8:
+            for (int l = kMaxBands - 1; l >= 1; --l)
+            {
+                r = L[3 + 2 * kMaxBands - 1 + l];
+                I360B_TRY(launch_collapse(a, dUnits + r.start, r.count, l, s));
+            }
+            break;
+        case 9:
+            r = L[2];
+            I360B_TRY(launch_final0(a, dUnits + r.start, r.count, s));
+            break;
+        }
+    }
+    return I360B_SUCCESS;
 }
 
 int Plan::enqueue(cudaStream_t s, cudaEvent_t* ev)
 {
-    BlendArgs a{dItems, dTiles, dError, dSeamCycles, bandRows};
-    auto L = [&](int idx) { return lists[idx]; };
+    if (!ev && nChains > 1)
+    {
+        // Stage 0's bbox reset and error flag for all items, then each chain's
+        // ten stages on its own stream (chain 1 forked onto `side`), joined.
+        if (nItems > 0) k_init_bbox<<<(nItems + 127) / 128, 128, 0, s>>>(dItems, nItems);
+        I360B_TRY(check_launch("bbox init kernel"));
+        I360B_CUDA(cudaMemsetAsync(dError, 0, sizeof(int), s), "error flag reset");
+        I360B_CUDA(cudaEventRecord(evFork, s), "chain fork");
+        I360B_CUDA(cudaStreamWaitEvent(side, evFork, 0), "chain fork");
+        I360B_TRY(enqueue_chain(0, 0, kStages - 1, s));
+        I360B_TRY(enqueue_chain(1, 0, kStages - 1, side));
+        I360B_CUDA(cudaEventRecord(evJoin, side), "chain join");
+        I360B_CUDA(cudaStreamWaitEvent(s, evJoin, 0), "chain join");
+        return I360B_SUCCESS;
+    }
+    // One stream, stage by stage (every chain's part of a stage before the
+    // next stage), so `ev[i]` brackets stage i (kStageNames order).
     auto mark = [&](int i) {
         if (ev) cudaEventRecord(ev[i], s);
     };
     mark(0);
-    I360B_TRY(enqueue_warp(s));
-    Range r;
-    mark(1);
-    I360B_TRY(launch_dt(a, dInts, nItems, false, maxW, maxH, dtSlots, s));
-    mark(2);
-    I360B_TRY(launch_dt(a, dInts, nItems, true, maxW, maxH, dtSlots, s));
-    mark(3);
-    r = L(1);
-    I360B_TRY(launch_owner(a, dUnits + r.start, r.count, s));
-    mark(4);
-    I360B_TRY(launch_seam(a, seamList, nSeam, s));
-    mark(5);
-    for (int l = 0; l < kMaxBands - 1; ++l)
+    if (nItems > 0) k_init_bbox<<<(nItems + 127) / 128, 128, 0, s>>>(dItems, nItems);
+    I360B_TRY(check_launch("bbox init kernel"));
+    I360B_CUDA(cudaMemsetAsync(dError, 0, sizeof(int), s), "error flag reset");
+    for (int stage = 0; stage < kStages; ++stage)
     {
-        r = L(3 + l);
-        I360B_TRY(launch_down(a, dUnits + r.start, r.count, l, s));
-        if (l == 0) mark(6);
+        if (stage > 0) mark(stage);
+        for (int c = 0; c < nChains; ++c) I360B_TRY(enqueue_chain(c, stage, stage, s));
     }
-    mark(7);
-    for (int l = kMaxBands - 1; l >= 1; --l)
-    {
-        r = L(3 + (kMaxBands - 1) + l);
-        I360B_TRY(launch_blend_level(a, dUnits + r.start, r.count, l, s));
-    }
-    mark(8);
-    for (int l = kMaxBands - 1; l >= 1; --l)
-    {
-        r = L(3 + 2 * kMaxBands - 1 + l);
-        I360B_TRY(launch_collapse(a, dUnits + r.start, r.count, l, s));
-    }
-    mark(9);
-    r = L(2);
-    I360B_TRY(launch_final0(a, dUnits + r.start, r.count, s));
-    mark(10);
+    mark(kStages);
     return I360B_SUCCESS;
 }
 

@@ -76,6 +76,17 @@ struct Plan
     std::vector<float> itemEdges;   // 16 per item (ItemSpec::edges)
     std::vector<int> tileRects;     // x, y, width, height per tile (canvas)
     std::vector<int> tileListed;    // contributors listed per tile (0: no render output)
+    // Tiles are independent, so they are split into chains of roughly equal
+    // work whose stages are enqueued on two streams inside the graph: the
+    // latency-bound stages of one chain (chamfer wavefront, seam search) run
+    // beside the bandwidth-bound stages of the other.
+    static constexpr int kMaxChains = 2;
+    int nChains = 1;
+    std::vector<int> tileChain;          // chain of each tile
+    Range dtRange[kMaxChains] = {};      // chamfer item lists in dInts, per chain
+    Range seamRange[kMaxChains] = {};    // seam tile lists in dInts, per chain
+    cudaStream_t side = nullptr;         // second chain's stream
+    cudaEvent_t evFork = nullptr, evJoin = nullptr;
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t graphExec = nullptr;
 
@@ -96,6 +107,8 @@ struct Plan
     // Only the first stage: bounding-box reset and the warp (render path) or
     // coverage pass, leaving every contributor's tile-space image in the arena.
     int enqueue_warp(cudaStream_t s);
+    // One chain's stages from `first` to `last` (kStageNames order, 0 = warp).
+    int enqueue_chain(int chain, int first, int last, cudaStream_t s);
     int kernels_per_execute() const;
     // Work lists for band height `rows` (fills `lists`).
     void make_units(int rows, std::vector<Unit>& units);
