@@ -559,8 +559,9 @@ int Plan::enqueue(cudaStream_t s, cudaEvent_t* ev)
         I360B_CUDA(cudaStreamWaitEvent(s, evJoin, 0), "chain join");
         return I360B_SUCCESS;
     }
-    // One stream, stage by stage (every chain's part of a stage before the
-    // next stage), so `ev[i]` brackets stage i (kStageNames order).
+    // Stage by stage (every chain's part of a stage, forked and joined,
+    // before the next stage), so `ev[i]` brackets stage i (kStageNames order)
+    // as it runs when the chains overlap.
     auto mark = [&](int i) {
         if (ev) cudaEventRecord(ev[i], s);
     };
@@ -571,7 +572,17 @@ int Plan::enqueue(cudaStream_t s, cudaEvent_t* ev)
     for (int stage = 0; stage < kStages; ++stage)
     {
         if (stage > 0) mark(stage);
-        for (int c = 0; c < nChains; ++c) I360B_TRY(enqueue_chain(c, stage, stage, s));
+        if (nChains > 1)
+        {
+            I360B_CUDA(cudaEventRecord(evFork, s), "chain fork");
+            I360B_CUDA(cudaStreamWaitEvent(side, evFork, 0), "chain fork");
+            I360B_TRY(enqueue_chain(0, stage, stage, s));
+            I360B_TRY(enqueue_chain(1, stage, stage, side));
+            I360B_CUDA(cudaEventRecord(evJoin, side), "chain join");
+            I360B_CUDA(cudaStreamWaitEvent(s, evJoin, 0), "chain join");
+        }
+        else
+            I360B_TRY(enqueue_chain(0, stage, stage, s));
     }
     mark(kStages);
     return I360B_SUCCESS;
