@@ -96,6 +96,7 @@ def load_library(path: str = LIB_PATH):
     L.i360b_render_plan_create.argtypes = [ct.POINTER(Frame), i, ct.POINTER(Tile), i, ct.POINTER(ct.c_int), i, i,
                                            ct.POINTER(vp)]
     L.i360b_render_plan_execute.argtypes = [vp, vp]
+    L.i360b_render_plan_execute_stages.argtypes = [vp, i, i, vp]
     L.i360b_render_plan_wait.argtypes = [vp, vp]
     L.i360b_render_plan_destroy.argtypes = [vp]
     L.i360b_render_plan_stats.argtypes = [vp, vp, ct.POINTER(RenderStats)]
@@ -524,6 +525,11 @@ class RenderPlan:
 
     def execute(self, stream: int = 0) -> ComputeResult:
         return ComputeResult(self.lib.i360b_render_plan_execute(self._h, stream or None))
+
+    def execute_stages(self, first: int, last: int, stream: int = 0) -> ComputeResult:
+        """Stages first..last (0 = warp, which alone reads the frames; 1-9 the blend)."""
+        return ComputeResult(self.lib.i360b_render_plan_execute_stages(self._h, int(first), int(last),
+                                                                       stream or None))
 
     def wait(self, stream: int = 0) -> ComputeResult:
         return ComputeResult(self.lib.i360b_render_plan_wait(self._h, stream or None))

@@ -440,6 +440,8 @@ int Plan::set_tuning(int rows, int slots, cudaStream_t s)
     I360B_CUDA(cudaStreamSynchronize(s), "plan tuning");
     bandRows = rows;
     dtSlots = slots;
+    for (auto& g : rangeGraphs) cudaGraphExecDestroy(g.second);
+    rangeGraphs.clear();
     if (graphExec) cudaGraphExecDestroy(graphExec);
     if (graph) cudaGraphDestroy(graph);
     graphExec = nullptr;
@@ -449,6 +451,7 @@ int Plan::set_tuning(int rows, int slots, cudaStream_t s)
 
 Plan::~Plan()
 {
+    for (auto& g : rangeGraphs) cudaGraphExecDestroy(g.second);
     if (side) cudaStreamSynchronize(side);
     if (evFork) cudaEventDestroy(evFork);
     if (evJoin) cudaEventDestroy(evJoin);
@@ -542,19 +545,24 @@ int Plan::enqueue_chain(int c, int first, int last, cudaStream_t s)
     return I360B_SUCCESS;
 }
 
-int Plan::enqueue(cudaStream_t s, cudaEvent_t* ev)
+int Plan::enqueue(cudaStream_t s, cudaEvent_t* ev) { return enqueue_range(s, 0, kStages - 1, ev); }
+
+int Plan::enqueue_range(cudaStream_t s, int first, int last, cudaEvent_t* ev)
 {
     if (!ev && nChains > 1)
     {
         // Stage 0's bbox reset and error flag for all items, then each chain's
-        // ten stages on its own stream (chain 1 forked onto `side`), joined.
-        if (nItems > 0) k_init_bbox<<<(nItems + 127) / 128, 128, 0, s>>>(dItems, nItems);
-        I360B_TRY(check_launch("bbox init kernel"));
-        I360B_CUDA(cudaMemsetAsync(dError, 0, sizeof(int), s), "error flag reset");
+        // stages on its own stream (chain 1 forked onto `side`), joined.
+        if (first == 0)
+        {
+            if (nItems > 0) k_init_bbox<<<(nItems + 127) / 128, 128, 0, s>>>(dItems, nItems);
+            I360B_TRY(check_launch("bbox init kernel"));
+            I360B_CUDA(cudaMemsetAsync(dError, 0, sizeof(int), s), "error flag reset");
+        }
         I360B_CUDA(cudaEventRecord(evFork, s), "chain fork");
         I360B_CUDA(cudaStreamWaitEvent(side, evFork, 0), "chain fork");
-        I360B_TRY(enqueue_chain(0, 0, kStages - 1, s));
-        I360B_TRY(enqueue_chain(1, 0, kStages - 1, side));
+        I360B_TRY(enqueue_chain(0, first, last, s));
+        I360B_TRY(enqueue_chain(1, first, last, side));
         I360B_CUDA(cudaEventRecord(evJoin, side), "chain join");
         I360B_CUDA(cudaStreamWaitEvent(s, evJoin, 0), "chain join");
         return I360B_SUCCESS;
@@ -565,13 +573,16 @@ int Plan::enqueue(cudaStream_t s, cudaEvent_t* ev)
     auto mark = [&](int i) {
         if (ev) cudaEventRecord(ev[i], s);
     };
-    mark(0);
-    if (nItems > 0) k_init_bbox<<<(nItems + 127) / 128, 128, 0, s>>>(dItems, nItems);
-    I360B_TRY(check_launch("bbox init kernel"));
-    I360B_CUDA(cudaMemsetAsync(dError, 0, sizeof(int), s), "error flag reset");
-    for (int stage = 0; stage < kStages; ++stage)
+    mark(first);
+    if (first == 0)
     {
-        if (stage > 0) mark(stage);
+        if (nItems > 0) k_init_bbox<<<(nItems + 127) / 128, 128, 0, s>>>(dItems, nItems);
+        I360B_TRY(check_launch("bbox init kernel"));
+        I360B_CUDA(cudaMemsetAsync(dError, 0, sizeof(int), s), "error flag reset");
+    }
+    for (int stage = first; stage <= last; ++stage)
+    {
+        if (stage > first) mark(stage);
         if (nChains > 1)
         {
             I360B_CUDA(cudaEventRecord(evFork, s), "chain fork");
@@ -584,7 +595,7 @@ int Plan::enqueue(cudaStream_t s, cudaEvent_t* ev)
         else
             I360B_TRY(enqueue_chain(0, stage, stage, s));
     }
-    mark(kStages);
+    mark(last + 1);
     return I360B_SUCCESS;
 }
 
@@ -604,6 +615,39 @@ int Plan::execute(cudaStream_t s, bool useGraph)
         I360B_CUDA(cudaGraphInstantiate(&graphExec, graph, 0), "graph instantiate");
     }
     I360B_CUDA(cudaGraphLaunch(graphExec, s), "graph launch");
+    return I360B_SUCCESS;
+}
+
+int Plan::execute_range(cudaStream_t s, int first, int last)
+{
+    if (first == 0 && last == kStages - 1) return execute(s, true);
+    if (first < 0 || last >= kStages || first > last) return fail(I360B_INVALID_PARAM, "Invalid stage range.");
+    const int key = first * kStages + last;
+    for (auto& g : rangeGraphs)
+        if (g.first == key)
+        {
+            I360B_CUDA(cudaGraphLaunch(g.second, s), "graph launch");
+            return I360B_SUCCESS;
+        }
+    cudaStream_t cap = nullptr;
+    I360B_CUDA(cudaStreamCreateWithFlags(&cap, cudaStreamNonBlocking), "graph capture stream");
+    I360B_CUDA(cudaStreamBeginCapture(cap, cudaStreamCaptureModeThreadLocal), "graph capture");
+    int rc = enqueue_range(cap, first, last, nullptr);
+    cudaGraph_t g = nullptr;
+    cudaError_t e = cudaStreamEndCapture(cap, &g);
+    cudaStreamDestroy(cap);
+    if (rc != I360B_SUCCESS)
+    {
+        if (g) cudaGraphDestroy(g);
+        return rc;
+    }
+    if (e != cudaSuccess) return cuda_fail(e, "graph capture");
+    cudaGraphExec_t x = nullptr;
+    e = cudaGraphInstantiate(&x, g, 0);
+    cudaGraphDestroy(g);
+    if (e != cudaSuccess) return cuda_fail(e, "graph instantiate");
+    rangeGraphs.push_back({key, x});
+    I360B_CUDA(cudaGraphLaunch(x, s), "graph launch");
     return I360B_SUCCESS;
 }
 
@@ -884,6 +928,15 @@ extern "C" int i360b_render_plan_execute(i360b_render_plan* plan, void* stream)
     if (!plan) return fail(I360B_INVALID_PARAM, "Null plan.");
     I360B_TRY(ensure_ready());
     return plan->plan.execute(static_cast<cudaStream_t>(stream), true);
+}
+
+extern "C" int i360b_render_plan_execute_stages(i360b_render_plan* plan, int firstStage, int lastStage,
+                                                void* stream)
+{
+    clear_error();
+    if (!plan) return fail(I360B_INVALID_PARAM, "Null plan.");
+    I360B_TRY(ensure_ready());
+    return plan->plan.execute_range(static_cast<cudaStream_t>(stream), firstStage, lastStage);
 }
 
 extern "C" int i360b_render_plan_wait(i360b_render_plan* plan, void* stream)

@@ -3,6 +3,7 @@
 
 #include "blend_kernels.cuh"
 
+#include <utility>
 #include <vector>
 
 namespace i360b
@@ -109,6 +110,11 @@ struct Plan
     int enqueue_warp(cudaStream_t s);
     // One chain's stages from `first` to `last` (kStageNames order, 0 = warp).
     int enqueue_chain(int chain, int first, int last, cudaStream_t s);
+    // Stages `first` to `last` of every chain (with ev, one stage at a time).
+    int enqueue_range(cudaStream_t s, int first, int last, cudaEvent_t* ev);
+    // Stages `first` to `last` as a graph of their own (cached per range).
+    int execute_range(cudaStream_t s, int first, int last);
+    std::vector<std::pair<int, cudaGraphExec_t>> rangeGraphs;
     int kernels_per_execute() const;
     // Work lists for band height `rows` (fills `lists`).
     void make_units(int rows, std::vector<Unit>& units);

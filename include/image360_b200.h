@@ -406,6 +406,14 @@ I360B_API int i360b_render_plan_export_preview(i360b_render_plan* plan, int tota
 I360B_API int i360b_render_plan_write_tiff16(i360b_render_plan* plan, const char* path, int canvasW, int canvasH,
                                              void* stream);
 
+/* Runs stages firstStage..lastStage of the plan (the order of
+ * i360b_render_stage_name: 0 = warp, gain and coverage, which alone reads the
+ * frames' RGB48 buffers; 1-9 the seam blend) as a CUDA graph of their own
+ * (captured on first use).  Running stage 0, then 1-9, is the same render as
+ * i360b_render_plan_execute; a caller that refills the frame buffers for the
+ * next render may do so as soon as stage 0 has completed. */
+I360B_API int i360b_render_plan_execute_stages(i360b_render_plan* plan, int firstStage, int lastStage, void* stream);
+
 /* Device bytes of scratch the plan holds. */
 I360B_API size_t i360b_render_plan_scratch_bytes(const i360b_render_plan* plan);
 I360B_API void i360b_render_plan_destroy(i360b_render_plan* plan);

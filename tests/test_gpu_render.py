@@ -144,3 +144,29 @@ def test_render_plan_uneven_tiles_exact(backend, oracle_c):
     for t, (o, r) in enumerate(zip(outs, ref)):
         assert np.array_equal(_host_u16(o), r), ("after autotune", t)
     plan.close()
+
+
+def test_render_plan_stage_ranges_equal_execute(backend):
+    """Stage 0 (warp) then stages 1-9 as separate graphs render the same bits
+    as the whole plan, on one stream and with the frames refilled between."""
+    torch = _torch()
+    cfg = synth.scaled(synth.C1, 0.02, tile=64)
+    pano = synth.make_panorama(cfg)
+    rgb = _demosaic_frames(backend, pano)
+    gains = (1.0 / pano.gains).astype(np.float32)
+    frames = [(r.data_ptr(), cfg.frame_w, cfg.frame_h, H, float(g)) for r, H, g in zip(rgb, pano.to_canvas, gains)]
+    outs_a = [torch.zeros((t[3], t[2], 3), dtype=torch.int16, device="cuda") for t in pano.tiles]
+    outs_b = [torch.zeros((t[3], t[2], 3), dtype=torch.int16, device="cuda") for t in pano.tiles]
+    pa = RenderPlan(frames, [(*t[:5], o.data_ptr()) for t, o in zip(pano.tiles, outs_a)], cfg.bands, COORDS_REFERENCE)
+    pb = RenderPlan(frames, [(*t[:5], o.data_ptr()) for t, o in zip(pano.tiles, outs_b)], cfg.bands, COORDS_REFERENCE)
+    assert pa.execute() == ComputeResult.SUCCESS and pa.wait() == ComputeResult.SUCCESS
+    for _ in range(2):
+        assert pb.execute_stages(0, 0) == ComputeResult.SUCCESS
+        assert pb.execute_stages(1, 9) == ComputeResult.SUCCESS
+        assert pb.wait() == ComputeResult.SUCCESS
+        assert all(torch.equal(a, b) for a, b in zip(outs_a, outs_b))
+        for o in outs_b:
+            o.zero_()
+    assert pb.execute_stages(3, 1) == ComputeResult.INVALID_PARAM
+    pa.close()
+    pb.close()
