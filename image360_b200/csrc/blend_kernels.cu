@@ -1196,6 +1196,143 @@ __global__ void __launch_bounds__(256) k_down0(BlendArgs a, const Unit* __restri
     }
 }
 
+// Level 0 -> 1 of a contributor's pyramids, streamed through registers.  The
+// same integer-exact sums as k_down0 (SeamBlend.cpp:60-79: 5-tap [1 4 6 4 1]
+// blur with clamped borders, then decimation; num = img * coverage, den =
+// coverage, weight = owner mask), computed without shared memory: a warp
+// makes one 32 x 16 block of level 1 (the same work units as k_down0), lane i
+// the output column X0 + i.  Each of the block's 36 footprint rows is read
+// once - lane i's two level-0 pixels 2X, 2X+1 as three 4-byte words, the halo
+// pixels 2X-2, 2X-1 and 2X+2 from the neighbouring lanes by shuffle - blurred
+// horizontally in registers and added into the output rows it feeds: an even
+// row 2m completes output row m-2 (weight 1), adds 6x to row m-1 and starts
+// row m; an odd row 2m+1 adds 4x to rows m-1 and m.  Warps whose footprint
+// touches the tile's side edges (clamping) or whose rows are not 4-byte
+// aligned read each footprint pixel with clamped scalar loads instead.
+constexpr int kDnWarps = 8;
+
+// One level-0 pixel packed for the shuffles: r | g << 16, b | coverage << 16 | owned << 17.
+struct PackedPx
+{
+    uint32_t rg, bw;
+};
+
+__device__ __forceinline__ PackedPx pack_px(int r, int g, int b, bool owned)
+{
+    const uint32_t mk = (r | g | b) ? 1u : 0u;
+    return PackedPx{(uint32_t)r | ((uint32_t)g << 16), (uint32_t)b | (mk << 16) | ((owned ? 1u : 0u) << 17)};
+}
+
+__device__ __forceinline__ PackedPx load_px(const unsigned short* img, const signed char* own, size_t p,
+                                            signed char k)
+{
+    const unsigned short* q = img + p * 3;
+    return pack_px(__ldg(q), __ldg(q + 1), __ldg(q + 2), __ldg(own + p) == k);
+}
+
+// The four channel sums r, g, b and (coverage << 16 | owned) of one pixel.
+__device__ __forceinline__ void px_channels(const PackedPx& v, int* c)
+{
+    c[0] = (int)(v.rg & 0xffffu);
+    c[1] = (int)(v.rg >> 16);
+    c[2] = (int)(v.bw & 0xffffu);
+    c[3] = (int)(((v.bw >> 16) & 1u) << 16 | (v.bw >> 17));
+}
+
+__global__ void __launch_bounds__(256) k_down0s(BlendArgs a, const Unit* __restrict__ units, int n)
+{
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int ui = blockIdx.x * kDnWarps + warp;
+    if (ui >= n) return;  // uniform per warp
+    const Unit u = units[ui];
+    const ItemDev& it = a.items[u.id];
+    const TileDev& T = a.tiles[it.tile];
+    const int sw = T.lw[0], sh = T.lh[0];
+    const int dw = T.lw[1], dh = T.lh[1];
+    const int X0 = u.bx * kDnTW, Y0 = u.by * kDnTH;
+    const int X = X0 + lane;
+    const unsigned short* img = it.img;
+    const signed char* own = T.owner;
+    const signed char k = (signed char)it.k;
+    const bool fast = (sw & 1) == 0 && 2 * X0 - 2 >= 0 && 2 * X0 + 2 * kDnTW <= sw - 1;
+    const size_t qrow = T.loff[1];
+    int P[4] = {0, 0, 0, 0}, Q[4] = {0, 0, 0, 0}, R[4] = {0, 0, 0, 0};
+    for (int r = 0; r < kDnSH; ++r)
+    {
+        const int gy = min(max(2 * Y0 - 2 + r, 0), sh - 1);
+        const size_t rowp = (size_t)gy * sw;
+        PackedPx px[5];  // columns 2X-2 .. 2X+2
+        if (fast)
+        {
+            const size_t p0 = rowp + 2 * X;
+            const uint32_t* w = reinterpret_cast<const uint32_t*>(img + p0 * 3);
+            const uint32_t w0 = __ldg(w), w1 = __ldg(w + 1), w2 = __ldg(w + 2);
+            const uint32_t ow = __ldg(reinterpret_cast<const unsigned short*>(own + p0));
+            px[2] = pack_px((int)(w0 & 0xffffu), (int)(w0 >> 16), (int)(w1 & 0xffffu),
+                            (signed char)(ow & 0xffu) == k);
+            px[3] = pack_px((int)(w1 >> 16), (int)(w2 & 0xffffu), (int)(w2 >> 16), (signed char)(ow >> 8) == k);
+            px[0].rg = __shfl_up_sync(kFull, px[2].rg, 1);
+            px[0].bw = __shfl_up_sync(kFull, px[2].bw, 1);
+            px[1].rg = __shfl_up_sync(kFull, px[3].rg, 1);
+            px[1].bw = __shfl_up_sync(kFull, px[3].bw, 1);
+            px[4].rg = __shfl_down_sync(kFull, px[2].rg, 1);
+            px[4].bw = __shfl_down_sync(kFull, px[2].bw, 1);
+            if (lane == 0)
+            {
+                px[0] = load_px(img, own, p0 - 2, k);
+                px[1] = load_px(img, own, p0 - 1, k);
+            }
+            if (lane == 31) px[4] = load_px(img, own, p0 + 2, k);
+        }
+        else
+        {
+#pragma unroll
+            for (int c = 0; c < 5; ++c)
+                px[c] = load_px(img, own, rowp + min(max(2 * X - 2 + c, 0), sw - 1), k);
+        }
+        int cv[5][4];
+#pragma unroll
+        for (int c = 0; c < 5; ++c) px_channels(px[c], cv[c]);
+        int t[4];
+#pragma unroll
+        for (int ch = 0; ch < 4; ++ch)
+            t[ch] = cv[0][ch] + 4 * cv[1][ch] + 6 * cv[2][ch] + 4 * cv[3][ch] + cv[4][ch];
+        if ((r & 1) == 0)
+        {
+            // even row 2m: last term of output m-2, middle of m-1, first of m
+#pragma unroll
+            for (int ch = 0; ch < 4; ++ch)
+            {
+                P[ch] += t[ch];
+                Q[ch] += 6 * t[ch];
+                R[ch] = t[ch];
+            }
+            const int j = (r >> 1) - 2;
+            const int Y = Y0 + j;
+            if (j >= 0 && X < dw && Y < dh)
+            {
+                const float s256 = 1.0f / 256.0f;
+                const size_t q = qrow + (size_t)Y * dw + X;
+                it.nd[q] = make_float4(fmul((float)P[0], s256), fmul((float)P[1], s256), fmul((float)P[2], s256),
+                                       fmul((float)(P[3] >> 16), s256));
+                it.wg[q] = fmul((float)(P[3] & 0xffff), s256);
+            }
+        }
+        else
+        {
+            // odd row 2m+1: second term of output m, fourth of m-1; then rotate
+#pragma unroll
+            for (int ch = 0; ch < 4; ++ch)
+            {
+                Q[ch] += 4 * t[ch];
+                R[ch] += 4 * t[ch];
+                P[ch] = Q[ch];
+                Q[ch] = R[ch];
+            }
+        }
+    }
+}
+
 // One pixel of a blended band (the general path).
 __device__ __noinline__ void blend_pixel(const TileDev& T, const ItemCache& C, int level, int K, long long pl)
 {
@@ -1607,9 +1744,7 @@ int launch_down(const BlendArgs& a, const Unit* units, int n, int level, cudaStr
     const int smem = (10 * kDnSH * (kDnSW / 2) + 5 * kDnSH * kDnTW) * (int)sizeof(float);
     if (level == 0)
     {
-        const int ismem = (8 * kDnSH * (kDnSW / 2) + 4 * kDnSH * kDnTW) * (int)sizeof(int);
-        cudaFuncSetAttribute(k_down0, cudaFuncAttributeMaxDynamicSharedMemorySize, ismem);
-        k_down0<<<n, 256, ismem, s>>>(a, units);
+        k_down0s<<<(n + kDnWarps - 1) / kDnWarps, 32 * kDnWarps, 0, s>>>(a, units, n);
     }
     else
     {
