@@ -1101,115 +1101,29 @@ __global__ void __launch_bounds__(256) k_down(BlendArgs a, const Unit* __restric
     }
 }
 
-// Level 0 -> 1 in integer arithmetic.  At level 0 every blur input is an
-// integer: pixel values (<= 65535, zero where uncovered), the 0/1 coverage
-// and the 0/1 ownership mask.  With the [1,4,6,4,1]/16 kernel each product
-// of the reference's FP32 sequence is exact, every horizontal partial sum is
-// a multiple of 1/16 below 2^16 and every vertical one a multiple of 1/256
-// below 2^16 (at most 24 significant bits), so no step rounds: the level-1
-// value IS (sum_ij c_i c_j v_ij) / 256.  Computing that sum in integers is
-// bit-identical to the FP32 chain of SeamBlend.cpp:15-79.  Coverage and
-// ownership sums (<= 256 each) share one int as den << 16 | weight.
-__global__ void __launch_bounds__(256) k_down0(BlendArgs a, const Unit* __restrict__ units)
-{
-    constexpr int HW = kDnSW / 2;
-    extern __shared__ int dn_ismem[];
-    auto E = reinterpret_cast<int (*)[kDnSH][HW]>(dn_ismem);
-    auto O = reinterpret_cast<int (*)[kDnSH][HW]>(dn_ismem + 4 * kDnSH * HW);
-    auto t = reinterpret_cast<int (*)[kDnSH][kDnTW]>(dn_ismem + 8 * kDnSH * HW);
-    const Unit u = units[blockIdx.x];
-    const ItemDev& it = a.items[u.id];
-    const TileDev& T = a.tiles[it.tile];
-    const int sw = T.lw[0], sh = T.lh[0];
-    const int dw = T.lw[1], dh = T.lh[1];
-    const int X0 = u.bx * kDnTW, Y0 = u.by * kDnTH;
-    const int tid = threadIdx.x;
-    const signed char k = (signed char)it.k;
-    // Footprint: every load of this thread is issued before any is used, so
-    // kPer x 2 pixels of gathers are in flight at once.
-    constexpr int kFoot = HW * kDnSH;
-    constexpr int kPer = (kFoot + 255) / 256;
-    unsigned short pv[kPer][2][3];
-    signed char po[kPer][2];
-#pragma unroll
-    for (int m = 0; m < kPer; ++m)
-    {
-        const int idx = tid + 256 * m;
-        if (idx >= kFoot) break;
-        const int r = idx / HW, cp = idx - r * HW;
-        const int gy = min(max(2 * Y0 - 2 + r, 0), sh - 1);
-#pragma unroll
-        for (int e = 0; e < 2; ++e)
-        {
-            const int gx = min(max(2 * X0 - 2 + 2 * cp + e, 0), sw - 1);
-            const size_t p = (size_t)gy * sw + gx;
-            const unsigned short* px = it.img + p * 3;
-            pv[m][e][0] = __ldg(px);
-            pv[m][e][1] = __ldg(px + 1);
-            pv[m][e][2] = __ldg(px + 2);
-            po[m][e] = __ldg(T.owner + p);
-        }
-    }
-#pragma unroll
-    for (int m = 0; m < kPer; ++m)
-    {
-        const int idx = tid + 256 * m;
-        if (idx >= kFoot) break;
-        const int r = idx / HW, cp = idx - r * HW;
-#pragma unroll
-        for (int e = 0; e < 2; ++e)
-        {
-            const int r0 = pv[m][e][0], r1 = pv[m][e][1], r2 = pv[m][e][2];
-            const int mk = (r0 | r1 | r2) ? 1 : 0;
-            const int dwv = (mk << 16) | (po[m][e] == k ? 1 : 0);
-            int(*D)[kDnSH][HW] = e == 0 ? E : O;
-            D[0][r][cp] = r0;
-            D[1][r][cp] = r1;
-            D[2][r][cp] = r2;
-            D[3][r][cp] = dwv;
-        }
-    }
-    __syncthreads();
-    for (int idx = tid; idx < 4 * kDnSH * kDnTW; idx += 256)
-    {
-        const int ch = idx / (kDnSH * kDnTW);
-        const int rem = idx - ch * kDnSH * kDnTW;
-        const int r = rem / kDnTW, i = rem - r * kDnTW;
-        t[ch][r][i] = E[ch][r][i] + 4 * O[ch][r][i] + 6 * E[ch][r][i + 1] + 4 * O[ch][r][i + 1] + E[ch][r][i + 2];
-    }
-    __syncthreads();
-    const int i = tid & 31;
-    for (int j = tid >> 5; j < kDnTH; j += 8)
-    {
-        const int X = X0 + i, Y = Y0 + j;
-        if (X >= dw || Y >= dh) continue;
-        int S[4];
-#pragma unroll
-        for (int ch = 0; ch < 4; ++ch)
-            S[ch] = t[ch][2 * j][i] + 4 * t[ch][2 * j + 1][i] + 6 * t[ch][2 * j + 2][i] + 4 * t[ch][2 * j + 3][i] +
-                    t[ch][2 * j + 4][i];
-        const float s256 = 1.0f / 256.0f;
-        const size_t q = T.loff[1] + (size_t)Y * dw + X;
-        it.nd[q] = make_float4(fmul((float)S[0], s256), fmul((float)S[1], s256), fmul((float)S[2], s256),
-                               fmul((float)(S[3] >> 16), s256));
-        it.wg[q] = fmul((float)(S[3] & 0xffff), s256);
-    }
-}
-
-// Level 0 -> 1 of a contributor's pyramids, streamed through registers.  The
-// same integer-exact sums as k_down0 (SeamBlend.cpp:60-79: 5-tap [1 4 6 4 1]
-// blur with clamped borders, then decimation; num = img * coverage, den =
-// coverage, weight = owner mask), computed without shared memory: a warp
-// makes one 32 x 16 block of level 1 (the same work units as k_down0), lane i
-// the output column X0 + i.  Each of the block's 36 footprint rows is read
-// once - lane i's two level-0 pixels 2X, 2X+1 as three 4-byte words, the halo
-// pixels 2X-2, 2X-1 and 2X+2 from the neighbouring lanes by shuffle - blurred
+// Level 0 -> 1 of a contributor's pyramids in integer arithmetic, streamed
+// through registers.  At level 0 every blur input is an integer: pixel values
+// (<= 65535, zero where uncovered), the 0/1 coverage and the 0/1 ownership
+// mask.  With the [1,4,6,4,1]/16 kernel each product of the reference's FP32
+// sequence is exact, every horizontal partial sum is a multiple of 1/16 below
+// 2^16 and every vertical one a multiple of 1/256 below 2^16 (at most 24
+// significant bits), so no step rounds: the level-1 value IS
+// (sum_ij c_i c_j v_ij) / 256, and computing that sum in integers is
+// bit-identical to the FP32 chain of SeamBlend.cpp:15-79 (blur with clamped
+// borders, then decimation; num = img * coverage, den = coverage, weight =
+// owner mask).  Coverage and ownership sums (<= 256 each) share one int as
+// den << 16 | weight.  No shared memory: a warp
+// makes one 64 x 16 block of level 1, lane i the output columns X0 + 2i and
+// X0 + 2i + 1.  Each of the block's 36 footprint rows is read once - lane i's
+// four level-0 pixels 2X .. 2X+3 as three 8-byte words, the halo pixels
+// 2X-2, 2X-1 and 2X+4 from the neighbouring lanes by shuffle - blurred
 // horizontally in registers and added into the output rows it feeds: an even
 // row 2m completes output row m-2 (weight 1), adds 6x to row m-1 and starts
 // row m; an odd row 2m+1 adds 4x to rows m-1 and m.  Warps whose footprint
-// touches the tile's side edges (clamping) or whose rows are not 4-byte
+// touches the tile's side edges (clamping) or whose rows are not 8-byte
 // aligned read each footprint pixel with clamped scalar loads instead.
 constexpr int kDnWarps = 8;
+constexpr int kDn0W = 64;  // level-1 columns per warp
 
 // One level-0 pixel packed for the shuffles: r | g << 16, b | coverage << 16 | owned << 17.
 struct PackedPx
@@ -1217,10 +1131,10 @@ struct PackedPx
     uint32_t rg, bw;
 };
 
-__device__ __forceinline__ PackedPx pack_px(int r, int g, int b, bool owned)
+__device__ __forceinline__ PackedPx pack_px(uint32_t r, uint32_t g, uint32_t b, bool owned)
 {
     const uint32_t mk = (r | g | b) ? 1u : 0u;
-    return PackedPx{(uint32_t)r | ((uint32_t)g << 16), (uint32_t)b | (mk << 16) | ((owned ? 1u : 0u) << 17)};
+    return PackedPx{r | (g << 16), b | (mk << 16) | ((owned ? 1u : 0u) << 17)};
 }
 
 __device__ __forceinline__ PackedPx load_px(const unsigned short* img, const signed char* own, size_t p,
@@ -1230,13 +1144,21 @@ __device__ __forceinline__ PackedPx load_px(const unsigned short* img, const sig
     return pack_px(__ldg(q), __ldg(q + 1), __ldg(q + 2), __ldg(own + p) == k);
 }
 
-// The four channel sums r, g, b and (coverage << 16 | owned) of one pixel.
+// The four channel values r, g, b and (coverage << 16 | owned) of one pixel.
 __device__ __forceinline__ void px_channels(const PackedPx& v, int* c)
 {
     c[0] = (int)(v.rg & 0xffffu);
     c[1] = (int)(v.rg >> 16);
     c[2] = (int)(v.bw & 0xffffu);
     c[3] = (int)(((v.bw >> 16) & 1u) << 16 | (v.bw >> 17));
+}
+
+__device__ __forceinline__ PackedPx shfl_px(const PackedPx& v, int delta, bool up)
+{
+    PackedPx o;
+    o.rg = up ? __shfl_up_sync(kFull, v.rg, delta) : __shfl_down_sync(kFull, v.rg, delta);
+    o.bw = up ? __shfl_up_sync(kFull, v.bw, delta) : __shfl_down_sync(kFull, v.bw, delta);
+    return o;
 }
 
 __global__ void __launch_bounds__(256) k_down0s(BlendArgs a, const Unit* __restrict__ units, int n)
@@ -1249,86 +1171,103 @@ __global__ void __launch_bounds__(256) k_down0s(BlendArgs a, const Unit* __restr
     const TileDev& T = a.tiles[it.tile];
     const int sw = T.lw[0], sh = T.lh[0];
     const int dw = T.lw[1], dh = T.lh[1];
-    const int X0 = u.bx * kDnTW, Y0 = u.by * kDnTH;
-    const int X = X0 + lane;
+    const int X0 = u.bx * kDn0W, Y0 = u.by * kDnTH;
+    const int X = X0 + 2 * lane;  // this lane's first column
     const unsigned short* img = it.img;
     const signed char* own = T.owner;
     const signed char k = (signed char)it.k;
-    const bool fast = (sw & 1) == 0 && 2 * X0 - 2 >= 0 && 2 * X0 + 2 * kDnTW <= sw - 1;
+    // 8-byte words need 4-pixel aligned rows on an 8-byte aligned image (a
+    // caller's warped buffer may sit at any even address).
+    const bool fast = (sw & 3) == 0 && ((reinterpret_cast<uintptr_t>(img) | reinterpret_cast<uintptr_t>(own)) & 7) == 0 &&
+                      2 * X0 - 2 >= 0 && 2 * X0 + 2 * kDn0W <= sw - 1;
     const size_t qrow = T.loff[1];
-    int P[4] = {0, 0, 0, 0}, Q[4] = {0, 0, 0, 0}, R[4] = {0, 0, 0, 0};
+    int P[2][4], Q[2][4], R[2][4];
+#pragma unroll
+    for (int c = 0; c < 2; ++c)
+#pragma unroll
+        for (int ch = 0; ch < 4; ++ch) P[c][ch] = Q[c][ch] = R[c][ch] = 0;
     for (int r = 0; r < kDnSH; ++r)
     {
         const int gy = min(max(2 * Y0 - 2 + r, 0), sh - 1);
         const size_t rowp = (size_t)gy * sw;
-        PackedPx px[5];  // columns 2X-2 .. 2X+2
+        PackedPx px[7];  // columns 2X-2 .. 2X+4
         if (fast)
         {
             const size_t p0 = rowp + 2 * X;
-            const uint32_t* w = reinterpret_cast<const uint32_t*>(img + p0 * 3);
-            const uint32_t w0 = __ldg(w), w1 = __ldg(w + 1), w2 = __ldg(w + 2);
-            const uint32_t ow = __ldg(reinterpret_cast<const unsigned short*>(own + p0));
-            px[2] = pack_px((int)(w0 & 0xffffu), (int)(w0 >> 16), (int)(w1 & 0xffffu),
-                            (signed char)(ow & 0xffu) == k);
-            px[3] = pack_px((int)(w1 >> 16), (int)(w2 & 0xffffu), (int)(w2 >> 16), (signed char)(ow >> 8) == k);
-            px[0].rg = __shfl_up_sync(kFull, px[2].rg, 1);
-            px[0].bw = __shfl_up_sync(kFull, px[2].bw, 1);
-            px[1].rg = __shfl_up_sync(kFull, px[3].rg, 1);
-            px[1].bw = __shfl_up_sync(kFull, px[3].bw, 1);
-            px[4].rg = __shfl_down_sync(kFull, px[2].rg, 1);
-            px[4].bw = __shfl_down_sync(kFull, px[2].bw, 1);
+            const uint2* w = reinterpret_cast<const uint2*>(img + p0 * 3);
+            const uint2 w0 = __ldg(w), w1 = __ldg(w + 1), w2 = __ldg(w + 2);
+            const uint32_t ow = __ldg(reinterpret_cast<const uint32_t*>(own + p0));
+            px[2] = pack_px(w0.x & 0xffffu, w0.x >> 16, w0.y & 0xffffu, (signed char)(ow & 0xffu) == k);
+            px[3] = pack_px(w0.y >> 16, w1.x & 0xffffu, w1.x >> 16, (signed char)((ow >> 8) & 0xffu) == k);
+            px[4] = pack_px(w1.y & 0xffffu, w1.y >> 16, w2.x & 0xffffu, (signed char)((ow >> 16) & 0xffu) == k);
+            px[5] = pack_px(w2.x >> 16, w2.y & 0xffffu, w2.y >> 16, (signed char)(ow >> 24) == k);
+            px[0] = shfl_px(px[4], 1, true);
+            px[1] = shfl_px(px[5], 1, true);
+            px[6] = shfl_px(px[2], 1, false);
             if (lane == 0)
             {
                 px[0] = load_px(img, own, p0 - 2, k);
                 px[1] = load_px(img, own, p0 - 1, k);
             }
-            if (lane == 31) px[4] = load_px(img, own, p0 + 2, k);
+            if (lane == 31) px[6] = load_px(img, own, p0 + 4, k);
         }
         else
         {
 #pragma unroll
-            for (int c = 0; c < 5; ++c)
+            for (int c = 0; c < 7; ++c)
                 px[c] = load_px(img, own, rowp + min(max(2 * X - 2 + c, 0), sw - 1), k);
         }
-        int cv[5][4];
+        int cv[7][4];
 #pragma unroll
-        for (int c = 0; c < 5; ++c) px_channels(px[c], cv[c]);
-        int t[4];
+        for (int c = 0; c < 7; ++c) px_channels(px[c], cv[c]);
+        int t[2][4];
 #pragma unroll
-        for (int ch = 0; ch < 4; ++ch)
-            t[ch] = cv[0][ch] + 4 * cv[1][ch] + 6 * cv[2][ch] + 4 * cv[3][ch] + cv[4][ch];
+        for (int c = 0; c < 2; ++c)
+#pragma unroll
+            for (int ch = 0; ch < 4; ++ch)
+                t[c][ch] = cv[2 * c][ch] + 4 * cv[2 * c + 1][ch] + 6 * cv[2 * c + 2][ch] + 4 * cv[2 * c + 3][ch] +
+                           cv[2 * c + 4][ch];
         if ((r & 1) == 0)
         {
             // even row 2m: last term of output m-2, middle of m-1, first of m
 #pragma unroll
-            for (int ch = 0; ch < 4; ++ch)
-            {
-                P[ch] += t[ch];
-                Q[ch] += 6 * t[ch];
-                R[ch] = t[ch];
-            }
+            for (int c = 0; c < 2; ++c)
+#pragma unroll
+                for (int ch = 0; ch < 4; ++ch)
+                {
+                    P[c][ch] += t[c][ch];
+                    Q[c][ch] += 6 * t[c][ch];
+                    R[c][ch] = t[c][ch];
+                }
             const int j = (r >> 1) - 2;
             const int Y = Y0 + j;
-            if (j >= 0 && X < dw && Y < dh)
+            if (j >= 0 && Y < dh)
             {
                 const float s256 = 1.0f / 256.0f;
-                const size_t q = qrow + (size_t)Y * dw + X;
-                it.nd[q] = make_float4(fmul((float)P[0], s256), fmul((float)P[1], s256), fmul((float)P[2], s256),
-                                       fmul((float)(P[3] >> 16), s256));
-                it.wg[q] = fmul((float)(P[3] & 0xffff), s256);
+#pragma unroll
+                for (int c = 0; c < 2; ++c)
+                {
+                    if (X + c >= dw) continue;
+                    const size_t q = qrow + (size_t)Y * dw + X + c;
+                    it.nd[q] = make_float4(fmul((float)P[c][0], s256), fmul((float)P[c][1], s256),
+                                           fmul((float)P[c][2], s256), fmul((float)(P[c][3] >> 16), s256));
+                    it.wg[q] = fmul((float)(P[c][3] & 0xffff), s256);
+                }
             }
         }
         else
         {
             // odd row 2m+1: second term of output m, fourth of m-1; then rotate
 #pragma unroll
-            for (int ch = 0; ch < 4; ++ch)
-            {
-                Q[ch] += 4 * t[ch];
-                R[ch] += 4 * t[ch];
-                P[ch] = Q[ch];
-                Q[ch] = R[ch];
-            }
+            for (int c = 0; c < 2; ++c)
+#pragma unroll
+                for (int ch = 0; ch < 4; ++ch)
+                {
+                    Q[c][ch] += 4 * t[c][ch];
+                    R[c][ch] += 4 * t[c][ch];
+                    P[c][ch] = Q[c][ch];
+                    Q[c][ch] = R[c][ch];
+                }
         }
     }
 }

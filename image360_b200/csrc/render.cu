@@ -374,10 +374,11 @@ void Plan::make_units(int rows, std::vector<Unit>& units)
     auto addBands = [&](int id, int h) {
         for (int by = 0; by < (h + rows - 1) / rows; ++by) units.push_back(Unit{id, 0, by, 0});
     };
-    // Block units of the pyramid down kernel: 32 x 16 outputs each.
-    auto addBlocks = [&](int id, int w, int h) {
+    // Block units of the pyramid down kernels: bw x 16 outputs each (64 wide
+    // for the level-0 step, whose lanes make two columns each; 32 above).
+    auto addBlocks = [&](int id, int w, int h, int bw) {
         for (int by = 0; by < (h + 15) / 16; ++by)
-            for (int bx = 0; bx < (w + 31) / 32; ++bx) units.push_back(Unit{id, bx, by, 0});
+            for (int bx = 0; bx < (w + bw - 1) / bw; ++bx) units.push_back(Unit{id, bx, by, 0});
     };
     lists.clear();
     auto beginList = [&]() { return (int)units.size(); };
@@ -405,7 +406,7 @@ void Plan::make_units(int rows, std::vector<Unit>& units)
             for (int i = 0; i < nItems; ++i)
             {
                 const TileDev& T = tiles[items[i].tile];
-                if (inI(i) && T.bands > l + 1) addBlocks(i, T.lw[l + 1], T.lh[l + 1]);
+                if (inI(i) && T.bands > l + 1) addBlocks(i, T.lw[l + 1], T.lh[l + 1], l == 0 ? 64 : 32);
             }
             endList(s);
         }
