@@ -162,7 +162,21 @@ __device__ __forceinline__ void warp_px(const WarpItem& it, float dX, const floa
     }
 }
 
-__global__ void __launch_bounds__(256) k_warp_tiles(BlendArgs a, const Unit* __restrict__ units)
+// Zeroes n u16 elements at p (any even address), the warp's lanes together:
+// at most 7 scalar stores either side of a 16-byte aligned body.
+__device__ __forceinline__ void warp_zero_u16(unsigned short* p, int n, int lane)
+{
+    if (n <= 0) return;
+    const int head = min(n, (int)(((16u - (unsigned)(reinterpret_cast<uintptr_t>(p) & 15u)) & 15u) >> 1));
+    if (lane < head) p[lane] = 0;
+    uint4* q = reinterpret_cast<uint4*>(p + head);
+    const int nq = (n - head) >> 3;
+    for (int j = lane; j < nq; j += 32) q[j] = make_uint4(0u, 0u, 0u, 0u);
+    const int t0 = head + (nq << 3);
+    if (lane < n - t0) p[t0 + lane] = 0;
+}
+
+__global__ void __launch_bounds__(256, 4) k_warp_tiles(BlendArgs a, const Unit* __restrict__ units)
 {
     const Unit u = units[blockIdx.x];
     const ItemDev& it = a.items[u.id];
@@ -186,25 +200,43 @@ __global__ void __launch_bounds__(256) k_warp_tiles(BlendArgs a, const Unit* __r
         if (y >= H) break;
         const float dY = (float)(y + offY);
         const float hy[3] = {fmul(wi.H[1], dY), fmul(wi.H[4], dY), fmul(wi.H[7], dY)};
-        const bool rowIn = y >= vy0 && y <= vy1;
-        for (int x0 = 0; x0 < W; x0 += 64)
+        // Columns [s0, s1) - whole 64-pixel segments - can hold a covered
+        // pixel; the rest of the row is (0,0,0) with zero coverage words,
+        // written as such without evaluating the mapping.
+        int s0 = 0, s1 = 0;
+        if (y >= vy0 && y <= vy1)
+        {
+            const int xs = max(vx0, 0), xe = min(vx1, W - 1);
+            if (xs <= xe)
+            {
+                s0 = xs & ~63;
+                s1 = min(W, (xe & ~63) + 64);
+            }
+        }
+        unsigned short* row = img + (size_t)y * W * 3;
+        uint32_t* covRow = it.cov + (size_t)y * T.covWords;
+        warp_zero_u16(row, s0 * 3, lane);
+        warp_zero_u16(row + (size_t)s1 * 3, (W - s1) * 3, lane);
+        for (int j = lane; j < (s0 >> 5); j += 32) covRow[j] = 0u;
+        for (int j = ((s1 + 31) >> 5) + lane; j < ((W + 31) >> 5); j += 32) covRow[j] = 0u;
+        for (int x0 = s0; x0 < s1; x0 += 64)
         {
             // Two independent pixels per lane keep more gathers in flight.
             const int xa = x0 + lane, xb = x0 + 32 + lane;
             unsigned short oa[3] = {0, 0, 0}, ob[3] = {0, 0, 0};
-            if (rowIn && xa < W && xa >= vx0 && xa <= vx1) warp_px(wi, (float)(xa + offX), hy, oa);
-            if (rowIn && xb < W && xb >= vx0 && xb <= vx1) warp_px(wi, (float)(xb + offX), hy, ob);
+            if (xa < W && xa >= vx0 && xa <= vx1) warp_px(wi, (float)(xa + offX), hy, oa);
+            if (xb < W && xb >= vx0 && xb <= vx1) warp_px(wi, (float)(xb + offX), hy, ob);
             bool ca = (oa[0] | oa[1] | oa[2]) != 0, cb = (ob[0] | ob[1] | ob[2]) != 0;
             if (xa < W)
             {
-                unsigned short* d = img + ((size_t)y * W + xa) * 3;
+                unsigned short* d = row + (size_t)xa * 3;
                 d[0] = oa[0];
                 d[1] = oa[1];
                 d[2] = oa[2];
             }
             if (xb < W)
             {
-                unsigned short* d = img + ((size_t)y * W + xb) * 3;
+                unsigned short* d = row + (size_t)xb * 3;
                 d[0] = ob[0];
                 d[1] = ob[1];
                 d[2] = ob[2];
@@ -212,8 +244,8 @@ __global__ void __launch_bounds__(256) k_warp_tiles(BlendArgs a, const Unit* __r
             unsigned ma = __ballot_sync(kFull, ca), mb = __ballot_sync(kFull, cb);
             if (lane == 0)
             {
-                it.cov[(size_t)y * T.covWords + (x0 >> 5)] = ma;
-                if (x0 + 32 < W) it.cov[(size_t)y * T.covWords + (x0 >> 5) + 1] = mb;
+                covRow[x0 >> 5] = ma;
+                if (x0 + 32 < W) covRow[(x0 >> 5) + 1] = mb;
             }
             box.add(ca, xa, y);
             box.add(cb, xb, y);
@@ -1176,11 +1208,32 @@ __global__ void __launch_bounds__(256) k_down0s(BlendArgs a, const Unit* __restr
     const unsigned short* img = it.img;
     const signed char* own = T.owner;
     const signed char k = (signed char)it.k;
+    const size_t qrow = T.loff[1];
+    // A footprint (rows 2Y0-2 .. 2Y0+33, columns 2X0-2 .. 2X0+129, before
+    // clamping) that misses the contributor's covered box reads only (0,0,0)
+    // pixels it does not own - ownership never leaves the covered box: the
+    // seam step reassigns pixels only inside two contributors' common box
+    // (SeamBlend.cpp:439-442, 580) - so its outputs are exactly zero.
+    {
+        const int bx0 = __ldg(it.bbox), by0 = __ldg(it.bbox + 1), bx1 = __ldg(it.bbox + 2), by1 = __ldg(it.bbox + 3);
+        if (2 * X0 + 2 * kDn0W + 1 < bx0 || 2 * X0 - 2 > bx1 || 2 * Y0 + 2 * kDnTH + 1 < by0 || 2 * Y0 - 2 > by1)
+        {
+            for (int j = 0; j < kDnTH && Y0 + j < dh; ++j)
+#pragma unroll
+                for (int c = 0; c < 2; ++c)
+                    if (X + c < dw)
+                    {
+                        const size_t q = qrow + (size_t)(Y0 + j) * dw + X + c;
+                        it.nd[q] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+                        it.wg[q] = 0.0f;
+                    }
+            return;
+        }
+    }
     // 8-byte words need 4-pixel aligned rows on an 8-byte aligned image (a
     // caller's warped buffer may sit at any even address).
     const bool fast = (sw & 3) == 0 && ((reinterpret_cast<uintptr_t>(img) | reinterpret_cast<uintptr_t>(own)) & 7) == 0 &&
                       2 * X0 - 2 >= 0 && 2 * X0 + 2 * kDn0W <= sw - 1;
-    const size_t qrow = T.loff[1];
     int P[2][4], Q[2][4], R[2][4];
 #pragma unroll
     for (int c = 0; c < 2; ++c)
