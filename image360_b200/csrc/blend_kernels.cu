@@ -537,7 +537,35 @@ struct ItemCache
     const float4* nd[kMaxTileItems];
     const float* wg[kMaxTileItems];
     int cnt[kMaxTileItems];
+    int4 box[kMaxTileItems];  // covered box (x0, y0, x1, y1), or its support at one level
 };
+
+// The box outside which a contributor's level-`level` pyramid values (num,
+// den and weight) are exactly zero, from its covered box at level 0.  At
+// level 0 the values vanish outside the covered box: num and den by
+// coverage, the weight because a contributor owns only pixels inside its
+// covered box (the ownership argmax needs d > 0, i.e. coverage, and the seam
+// step reassigns pixels only inside two contributors' common box,
+// SeamBlend.cpp:439-442, 580).  Output X of a blur + decimate step reads
+// pixels 2X-2 .. 2X+2 (clamped into the level, which stays inside that
+// range), so the support grows to [floor((x0-2)/2), floor((x1+2)/2)].  An
+// empty box (x0 > x1) stays empty.
+__device__ __forceinline__ int4 support_box(int4 b, int level)
+{
+    for (int l = 0; l < level; ++l)
+    {
+        b.x = (b.x - 2) >> 1;
+        b.y = (b.y - 2) >> 1;
+        b.z = (b.z + 2) >> 1;
+        b.w = (b.w + 2) >> 1;
+    }
+    return b;
+}
+
+__device__ __forceinline__ int4 covered_box(const int* bbox)
+{
+    return make_int4(__ldg(bbox), __ldg(bbox + 1), __ldg(bbox + 2), __ldg(bbox + 3));
+}
 
 __device__ __forceinline__ void load_item_cache(ItemCache& c, const BlendArgs& a, const TileDev& T)
 {
@@ -549,7 +577,16 @@ __device__ __forceinline__ void load_item_cache(ItemCache& c, const BlendArgs& a
         c.nd[k] = it.nd;
         c.wg[k] = it.wg;
         c.cnt[k] = it.bbox[4];
+        c.box[k] = make_int4(it.bbox[0], it.bbox[1], it.bbox[2], it.bbox[3]);
     }
+    __syncthreads();
+}
+
+// The cache's boxes as supports at `level` (after load_item_cache).
+__device__ __forceinline__ void level_boxes(ItemCache& c, const TileDev& T, int level)
+{
+    for (int k = threadIdx.x; k < T.numItems && k < kMaxTileItems; k += blockDim.x)
+        c.box[k] = support_box(c.box[k], level);
     __syncthreads();
 }
 
@@ -564,26 +601,35 @@ __global__ void __launch_bounds__(256) k_owner(BlendArgs a, const Unit* __restri
     const TileDev& T = a.tiles[u.id];
     load_item_cache(C, a, T);
     const int K = T.numItems;
-    const long long full = (long long)T.w * T.h;
-    const float kInf = (float)(T.w + T.h);
-    const long long base = (long long)u.by * a.bandRows * T.w;
-    const long long n = min((long long)a.bandRows * T.w, full - base);
-    for (long long q = threadIdx.x; q < n; q += blockDim.x)
+    const int W = T.w;
+    const long long full = (long long)W * T.h;
+    const float kInf = (float)(W + T.h);
+    const int row0 = u.by * a.bandRows;
+    const int rows = min(a.bandRows, T.h - row0);
+    for (int r = 0; r < rows; ++r)
     {
-        const long long p = base + q;
-        int best = -1;
-        float bestD = 0.0f;
-        for (int k = 0; k < K; ++k)
+        const int y = row0 + r;
+        for (int x = threadIdx.x; x < W; x += blockDim.x)
         {
-            const int cnt = C.cnt[k];
-            const float v = cnt == 0 ? 0.0f : ((long long)cnt == full ? kInf : __ldg(C.d[k] + p));
-            if (v > bestD)
+            const long long p = (long long)y * W + x;
+            int best = -1;
+            float bestD = 0.0f;
+            for (int k = 0; k < K; ++k)
             {
-                bestD = v;
-                best = k;
+                const int cnt = C.cnt[k];
+                const int4 B = C.box[k];
+                // d is 0 outside the covered box
+                const bool in = x >= B.x && x <= B.z && y >= B.y && y <= B.w;
+                const float v =
+                    cnt == 0 ? 0.0f : ((long long)cnt == full ? kInf : (in ? __ldg(C.d[k] + p) : 0.0f));
+                if (v > bestD)
+                {
+                    bestD = v;
+                    best = k;
+                }
             }
+            T.owner[p] = (signed char)best;
         }
-        T.owner[p] = (signed char)best;
     }
 }
 
@@ -1048,7 +1094,6 @@ __device__ __forceinline__ float3 gauss_of(float4 nd)
 constexpr int kDnTW = 32, kDnTH = 16;
 constexpr int kDnSW = 2 * kDnTW + 4, kDnSH = 2 * kDnTH + 4;
 
-template <bool L0>
 __global__ void __launch_bounds__(256) k_down(BlendArgs a, const Unit* __restrict__ units, int level)
 {
     // Footprint staged deinterleaved (even / odd columns in separate planes)
@@ -1066,8 +1111,23 @@ __global__ void __launch_bounds__(256) k_down(BlendArgs a, const Unit* __restric
     const int dw = T.lw[level + 1], dh = T.lh[level + 1];
     const int X0 = u.bx * kDnTW, Y0 = u.by * kDnTH;
     const int tid = threadIdx.x;
-    const float4* ndS = L0 ? nullptr : it.nd + T.loff[level];
-    const float* wgS = L0 ? nullptr : it.wg + T.loff[level];
+    // A footprint (rows 2Y0-2 .. 2Y0+33, columns 2X0-2 .. 2X0+65) outside
+    // the contributor's support at this level reads only zeros.
+    const int4 B = support_box(covered_box(it.bbox), level);
+    if (2 * X0 + 2 * kDnTW + 1 < B.x || 2 * X0 - 2 > B.z || 2 * Y0 + 2 * kDnTH + 1 < B.y || 2 * Y0 - 2 > B.w)
+    {
+        for (int idx = tid; idx < kDnTW * kDnTH; idx += 256)
+        {
+            const int X = X0 + (idx & (kDnTW - 1)), Y = Y0 + idx / kDnTW;
+            if (X >= dw || Y >= dh) continue;
+            const size_t q = T.loff[level + 1] + (size_t)Y * dw + X;
+            it.nd[q] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+            it.wg[q] = 0.0f;
+        }
+        return;
+    }
+    const float4* ndS = it.nd + T.loff[level];
+    const float* wgS = it.wg + T.loff[level];
     for (int idx = tid; idx < HW * kDnSH; idx += 256)
     {
         const int r = idx / HW, cp = idx - r * HW;
@@ -1078,26 +1138,12 @@ __global__ void __launch_bounds__(256) k_down(BlendArgs a, const Unit* __restric
             const int gx = min(max(2 * X0 - 2 + 2 * cp + e, 0), sw - 1);
             const size_t p = (size_t)gy * sw + gx;
             float v[5];
-            if (L0)
-            {
-                const unsigned short* px = it.img + p * 3;
-                const unsigned short r0 = px[0], r1 = px[1], r2 = px[2];
-                const float m = (r0 | r1 | r2) ? 1.0f : 0.0f;
-                v[0] = fmul((float)r0, m);
-                v[1] = fmul((float)r1, m);
-                v[2] = fmul((float)r2, m);
-                v[3] = m;
-                v[4] = (T.owner[p] == it.k) ? 1.0f : 0.0f;
-            }
-            else
-            {
-                const float4 q = ndS[p];
-                v[0] = q.x;
-                v[1] = q.y;
-                v[2] = q.z;
-                v[3] = q.w;
-                v[4] = wgS[p];
-            }
+            const float4 q = ndS[p];
+            v[0] = q.x;
+            v[1] = q.y;
+            v[2] = q.z;
+            v[3] = q.w;
+            v[4] = wgS[p];
 #pragma unroll
             for (int ch = 0; ch < 5; ++ch)
             {
@@ -1338,6 +1384,8 @@ __device__ __noinline__ void blend_pixel(const TileDev& T, const ItemCache& C, i
     float acc0 = 0.0f, acc1 = 0.0f, acc2 = 0.0f;
     for (int k = 0; k < K; ++k)
     {
+        const int4 B = C.box[k];
+        if (x < B.x || x > B.z || y < B.y || y > B.w) continue;  // weight 0: the term is +-0
         float wv = __ldg(C.wg[k] + p);
         float3 g = gauss_of(C.nd[k][p]);
         if (!top)
@@ -1390,6 +1438,8 @@ __device__ __forceinline__ void blend_quad(const TileDev& T, const ItemCache& C,
     for (int i = 0; i < 4; ++i) acc[i][0] = acc[i][1] = acc[i][2] = 0.0f;
     for (int k = 0; k < K; ++k)
     {
+        const int4 B = C.box[k];
+        if (x + 3 < B.x || x > B.z || y < B.y || y > B.w) continue;  // weight 0 on the quad: terms are +-0
         const float4* up = C.nd[k] + T.loff[level + 1];
         int cur = x0[0];
         float3 L0 = gauss_of(__ldg(up + (size_t)y0 * uw + cur)), L1 = gauss_of(__ldg(up + (size_t)y1 * uw + cur));
@@ -1440,14 +1490,17 @@ __device__ __forceinline__ void blend_quad(const TileDev& T, const ItemCache& C,
 // Blended band of one level: sum over the tile's contributors, in index
 // order, of weight * Laplacian (SeamBlend.cpp:501-509), where
 // Laplacian = G_l - Up(G_l+1) or G_top (SeamBlend.cpp:184-201).
-// Contributors that own no pixel have an all-zero weight pyramid and add
-// exactly +-0, so summing every contributor equals the reference's sum.
+// Where a contributor's weight is 0 its term is exactly +-0 (the hole-filled
+// Gaussian is finite), and adding +-0 to a sum that started at +0 changes
+// nothing, so skipping contributors outside their weight support (the whole
+// pyramid of one that owns no pixel) equals the reference's full sum.
 __global__ void __launch_bounds__(256, 3) k_blend_level(BlendArgs a, const Unit* __restrict__ units, int level)
 {
     __shared__ ItemCache C;
     const Unit u = units[blockIdx.x];
     const TileDev& T = a.tiles[u.id];
     load_item_cache(C, a, T);
+    level_boxes(C, T, level);
     const int K = T.numItems;
     const int lw = T.lw[level], lh = T.lh[level];
     const bool top = level == T.bands - 1;
@@ -1740,8 +1793,8 @@ int launch_down(const BlendArgs& a, const Unit* units, int n, int level, cudaStr
     }
     else
     {
-        cudaFuncSetAttribute(k_down<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-        k_down<false><<<n, 256, smem, s>>>(a, units, level);
+        cudaFuncSetAttribute(k_down, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+        k_down<<<n, 256, smem, s>>>(a, units, level);
     }
     return check_launch("pyramid down kernel");
 }
