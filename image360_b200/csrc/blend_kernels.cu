@@ -260,32 +260,46 @@ __global__ void __launch_bounds__(256, 4) k_warp_tiles(BlendArgs a, const Unit* 
 // The raster recurrence d[p] = min(init, left+1, up+1, upleft+sqrt2,
 // upright+sqrt2) is a DAG with a unique solution, so any schedule that applies
 // the same rounded operations (min is exact and order-free) reproduces the CPU
-// result bit for bit.
+// result bit for bit.  Neighbours outside the tile are skipped by the
+// reference; here they are virtual cells of value +inf, which min() ignores
+// (inf + c = inf), so one uniform step serves every pixel.
 //
-// Systolic wavefront: lane r of a warp owns row 32g + r and walks it one
-// column per step, kLag columns behind the lane above, so at every step the
-// three values it needs from the row above (x-1, x, x+1) have already been
-// produced; the newest one arrives by one __shfl_up_sync, the two older ones
-// are kept from earlier steps.  Lane 0 takes its row above from a shared-memory
-// ring written by lane 31 of the previous row group, with a bounded wait on
-// that group's published progress.  The backward pass is the same code on
-// mirrored coordinates with the forward result as init.
+// Systolic wavefront: lane r of a warp owns row 32g + r and at step t
+// computes column x = t - 2r - 2, two columns behind the lane above.  The
+// value it needs from the row above at x+1 is the lane above's output of the
+// previous step and arrives by one __shfl_up_sync; the values at x and x-1
+// are the ones received one and two steps earlier.  Lane 0 takes its row
+// above from a shared-memory ring slot written by lane 31 of the previous row
+// group.  A warp runs kDtChunk steps between hand-offs: before a chunk, lane
+// 0 waits (bounded) until the previous group has published every column the
+// chunk reads; after it, lane 31 publishes how many columns of its row are
+// final.  The initial values of a chunk (one or two coverage words, or eight
+// pairs of the forward result) are loaded before its first step, and only
+// chunks that touch the tile's edges test cells for being virtual.  The
+// backward pass is the same code on mirrored coordinates with the forward
+// result as init.
 //
 // Progress is published per row group (prog[g] = columns of row group g's
 // last row that are final), never per ring slot: group g + nslots reuses
 // group g's slot while group g + 1 may still be waiting for columns of group
 // g, so a per-slot counter would let g + nslots's progress release that wait
-// early.  The slot data itself is safe to reuse: group g + nslots writes
-// column x only after group g + 1 has read well past x (each group trails
-// the one above by more than kLag * 31 columns, and nslots >= 2).
+// early.  The slot data itself is safe to reuse: a group runs a chunk only
+// when the group above has finished at least 64 further steps, so when group
+// g + nslots (nslots >= 2) writes column x of the slot, group g + 1 has run
+// more than 64 steps past the one where it read x.
 // ---------------------------------------------------------------------------
-constexpr int kLag = 4;      // columns a row lags the row above
-constexpr int kDtRing = 4;   // row-group hand-off slots
+constexpr int kDtChunk = 16;  // steps between hand-offs
+constexpr int kDtRing = 4;    // row-group hand-off slots
+constexpr int kDtWarps = 16;  // warps per CTA
+constexpr int kDtStR = 20;    // staging row stride (floats): 16 columns + pad, 16-byte rows
+constexpr size_t kDtStageBytes = (size_t)kDtWarps * 32 * kDtStR * sizeof(float);
 
-__host__ __device__ __forceinline__ int dt_ring_stride(int W) { return (W + 7) & ~3; }
+// Ring slot: columns -4 .. W of a row (index = column + 4); columns < 0 and
+// column W hold +inf.
+__host__ __device__ __forceinline__ int dt_ring_stride(int W) { return (W + 8) & ~3; }
 
 template <bool BACK>
-__global__ void __launch_bounds__(512, 2) k_dt(BlendArgs a, const int* __restrict__ itemList, int nslots)
+__global__ void __launch_bounds__(32 * kDtWarps, 2) k_dt(BlendArgs a, const int* __restrict__ itemList, int nslots)
 {
     extern __shared__ float smem[];
     const ItemDev& it = a.items[itemList[blockIdx.x]];
@@ -299,54 +313,64 @@ __global__ void __launch_bounds__(512, 2) k_dt(BlendArgs a, const int* __restric
         if (cnt == 0 || (long long)cnt == (long long)W * H) return;
     }
     const int RS = dt_ring_stride(W);
-    float* ring = smem;
-    int* prog = reinterpret_cast<int*>(smem + (size_t)nslots * RS);
-    for (int i = threadIdx.x; i < (H + 31) >> 5; i += blockDim.x) prog[i] = -1;
+    float* ring = smem + kDtStageBytes / sizeof(float);
+    int* prog = reinterpret_cast<int*>(ring + (size_t)nslots * RS);
+    const float INF = f_inf();
+    const int nG = (H + 31) >> 5;
+    for (int i = threadIdx.x; i < nG; i += blockDim.x) prog[i] = -1;
+    for (int i = threadIdx.x; i < nslots * 5; i += blockDim.x)
+    {
+        const int sl = i / 5, e = i - sl * 5;
+        ring[(size_t)sl * RS + (e < 4 ? e : W + 4)] = INF;
+    }
     __syncthreads();
     const float kInf = (float)(W + H);
     const float kDiag = 1.41421356f;
-    const float INF = f_inf();
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int nG = (H + 31) >> 5;
     const int nwarps = blockDim.x >> 5;
-    const bool vec = (W & 3) == 0;  // 16-byte row alignment of d1/d and the ring
+    const float* src = BACK ? it.d1 : nullptr;
+    float* dst = BACK ? it.d : it.d1;
+    // 8-byte pairs of columns: even row length and 8-byte aligned buffers.
+    const bool pairs = (W & 1) == 0 && ((reinterpret_cast<uintptr_t>(dst) | reinterpret_cast<uintptr_t>(src)) & 7) == 0;
+    const int nSteps = W + 64;  // lane 31 computes column W - 1 at step W + 63
 
     for (int g = warp; g < nG; g += nwarps)
     {
-        const int vy = g * 32 + lane;
+        const int vy = g * 32 + lane;  // row in the pass's (mirrored) order
         const bool rowOk = vy < H;
-        const bool fullGroup = g > 0 && g * 32 + 31 < H;
-        const int ry = BACK ? H - 1 - vy : (rowOk ? vy : 0);
-        const int rys = rowOk ? (BACK ? ry : vy) : 0;
-        float* outRow = (BACK ? it.d : it.d1) + (size_t)rys * W;
-        const float* d1Row = it.d1 + (size_t)rys * W;
-        const uint32_t* covRow = it.cov + (size_t)rys * covWords;
-        const int slot = g % nslots, pslot = (g + nslots - 1) % nslots;  // ring slots of g and g - 1
-        float* ringOut = ring + slot * RS;
-        const float* ringIn = ring + pslot * RS;
-        float left = INF;               // own row, column x-1
-        float upm1 = INF, up0 = INF;    // row above, columns x-1 and x
-        float h0 = INF, h1 = INF, h2 = INF;  // own outputs 1, 2, 3 steps ago
-        int seen = -1;                  // lane 0: progress of the group above already observed
-        const int nSteps = W + 31 * kLag;
-        for (int t0 = 0; t0 < nSteps; t0 += kLag)
+        const bool fullGroup = g * 32 + 31 < H;
+        const bool hasAbove = g > 0;  // lane 0's row above: the ring, else virtual
+        const int ry = rowOk ? (BACK ? H - 1 - vy : vy) : 0;  // memory row
+        float* outRow = dst + (size_t)ry * W;
+        const float* inRow = BACK ? src + (size_t)ry * W : nullptr;
+        const uint32_t* covRow = it.cov + (size_t)ry * covWords;
+        // Staging rows of this warp: a chunk's 32 x 16 values cross between
+        // lanes (one row each) and 8-lane groups (one 64-byte row segment per
+        // global access) here.
+        float* st = smem + (size_t)warp * 32 * kDtStR;
+        const int sj = lane >> 3, sp = lane & 7;  // transposed role: rows sj + 4k, pair sp
+        float* ringOut = ring + (size_t)(g % nslots) * RS + 4;
+        const float* ringIn = ring + (size_t)((g + nslots - 1) % nslots) * RS + 4;
+        float left = INF, up0 = INF, upm1 = INF;  // own x-1; row above at x and x-1
+        int seen = -1;                            // lane 0: progress of the group above already observed
+        int wIdx = -4;                            // forward: coverage words wIdx .. wIdx+2 held
+        uint32_t wLo = 0, wHi = 0, wNx = 0;
+        for (int t0 = 0; t0 < nSteps; t0 += kDtChunk)
         {
-            // Lane 0 needs the row above up to column x+1 for every x of this block.
             int bad = 0;
-            if (g > 0 && lane == 0)
+            if (hasAbove && lane == 0)
             {
-                const int target = min(t0 + kLag + 1, W);
-                if (seen < target)
+                // this chunk reads columns up to t0 + kDtChunk - 1 of the row above
+                const int need = min(t0 + kDtChunk, W);
+                if (seen < need)
                 {
                     cuda::atomic_ref<int, cuda::thread_scope_block> pr(prog[g - 1]);
-                    long long tstart = clock64();
+                    const long long tstart = clock64();
                     int spins = 0;
-                    while ((seen = pr.load(cuda::memory_order_acquire)) < target)
+                    while ((seen = pr.load(cuda::memory_order_acquire)) < need)
                     {
-                        // The producer is normally one block ahead: poll first,
-                        // back off only if the wait is long.
-                        if (++spins > 256) __nanosleep(64);
-                        if ((spins & 255) == 0 && (*(volatile int*)a.error || clock64() - tstart > kSpinCycles))
+                        if (++spins > 32) __nanosleep(128);
+                        if ((spins & 63) == 0 && (*(volatile int*)a.error || clock64() - tstart > kSpinCycles))
                         {
                             atomicExch(a.error, 1);
                             bad = 1;
@@ -356,174 +380,145 @@ __global__ void __launch_bounds__(512, 2) k_dt(BlendArgs a, const int* __restric
                 }
             }
             if (__shfl_sync(kFull, bad, 0)) return;  // gave up waiting (error flag set)
-            const int xb = t0 - kLag * lane;       // my first column of this block (multiple of 4)
-            // Interior block of a full group below row 0: every lane's four
-            // columns lie in [1, W-2], so no edge condition applies and the
-            // step is branch-free.
-            if (fullGroup && t0 - kLag * 31 >= 1 && t0 + kLag < W)
+            const int xs = t0 - 2 * lane - 2;  // this lane's column at the chunk's first step
+            // Interior chunk: every lane's row and columns lie in the tile, so
+            // no cell is virtual (but lane 0's row above, in group 0).
+            if (fullGroup && pairs && t0 - 64 >= 0 && t0 + kDtChunk - 2 <= W)
             {
-                float iv[kLag];
+                float iv[kDtChunk];
                 if (BACK)
                 {
-                    if (vec)
-                    {
-                        const float4 q = __ldg(reinterpret_cast<const float4*>(d1Row + (W - kLag - xb)));
-                        iv[0] = q.w; iv[1] = q.z; iv[2] = q.y; iv[3] = q.x;
-                    }
-                    else
-                    {
+                    // Row j's 16 values sit at memory columns W-16-xs_j .. W-1-xs_j
+                    // (mirrored); 8 lanes load each row as 8-byte pairs.
+                    __syncwarp();
 #pragma unroll
-                        for (int q = 0; q < kLag; ++q) iv[q] = __ldg(d1Row + (W - 1 - xb - q));
+                    for (int k = 0; k < 8; ++k)
+                    {
+                        const int j = 4 * k + sj;
+                        const int vyj = g * 32 + j, xsj = t0 - 2 * j - 2;
+                        const float* rowj = src + (size_t)(H - 1 - vyj) * W + (W - 16 - xsj);
+                        *reinterpret_cast<float2*>(st + j * kDtStR + 2 * sp) =
+                            __ldg(reinterpret_cast<const float2*>(rowj + 2 * sp));
+                    }
+                    __syncwarp();
+                    const float4* r4 = reinterpret_cast<const float4*>(st + lane * kDtStR);
+#pragma unroll
+                    for (int m = 0; m < 4; ++m)
+                    {
+                        const float4 v = r4[m];  // memory columns 4m .. 4m+3 = chunk steps 15-4m .. 12-4m
+                        iv[15 - 4 * m] = v.x;
+                        iv[14 - 4 * m] = v.y;
+                        iv[13 - 4 * m] = v.z;
+                        iv[12 - 4 * m] = v.w;
                     }
                 }
                 else
                 {
-                    const uint32_t wd = __ldg(covRow + (xb >> 5)) >> (xb & 31);
+                    const int w0 = xs >> 5;
+                    if (w0 != wIdx)
+                    {
+                        if (w0 == wIdx + 1)
+                        {
+                            wLo = wHi;
+                            wHi = wNx;
+                        }
+                        else
+                        {
+                            wLo = __ldg(covRow + w0);
+                            wHi = w0 + 1 < covWords ? __ldg(covRow + w0 + 1) : 0u;
+                        }
+                        wNx = w0 + 2 < covWords ? __ldg(covRow + w0 + 2) : 0u;
+                        wIdx = w0;
+                    }
+                    const uint32_t bits = __funnelshift_r(wLo, wHi, xs & 31);
 #pragma unroll
-                    for (int q = 0; q < kLag; ++q) iv[q] = ((wd >> q) & 1u) ? kInf : 0.0f;
+                    for (int q = 0; q < kDtChunk; ++q) iv[q] = ((bits >> q) & 1u) ? kInf : 0.0f;
                 }
-                float dv[kLag];
 #pragma unroll
-                for (int q = 0; q < kLag; ++q)
+                for (int q = 0; q < kDtChunk; ++q)
                 {
-                    const float recv = __shfl_up_sync(kFull, h2, 1);
-                    const float rv = lane == 0 ? ringIn[xb + q + 1] : 0.0f;
-                    const float upp1 = lane == 0 ? rv : recv;
+                    const float recv = __shfl_up_sync(kFull, left, 1);
+                    const float upp1 = lane == 0 ? (hasAbove ? ringIn[xs + q + 1] : INF) : recv;
                     float av = fminf(iv[q], fadd(up0, 1.0f));
                     av = fminf(av, fadd(upm1, kDiag));
                     av = fminf(av, fadd(upp1, kDiag));
                     av = fminf(av, fadd(left, 1.0f));
-                    dv[q] = av;
-                    left = av;
                     upm1 = up0;
                     up0 = upp1;
-                    h2 = h1;
-                    h1 = h0;
-                    h0 = av;
+                    left = av;
+                    iv[q] = av;
                 }
-                if (vec)
-                {
-                    if (BACK)
-                        *reinterpret_cast<float4*>(outRow + (W - kLag - xb)) = make_float4(dv[3], dv[2], dv[1], dv[0]);
-                    else *reinterpret_cast<float4*>(outRow + xb) = make_float4(dv[0], dv[1], dv[2], dv[3]);
-                }
-                else
-                {
+                // Results through the staging rows (memory order: the backward
+                // pass reversed), then 64-byte row segments to the output.
+                __syncwarp();
+                float4* w4 = reinterpret_cast<float4*>(st + lane * kDtStR);
 #pragma unroll
-                    for (int q = 0; q < kLag; ++q) outRow[BACK ? W - 1 - xb - q : xb + q] = dv[q];
-                }
-                if (lane == 31)
+                for (int m = 0; m < 4; ++m)
                 {
-                    *reinterpret_cast<float4*>(ringOut + xb) = make_float4(dv[0], dv[1], dv[2], dv[3]);
-                    cuda::atomic_ref<int, cuda::thread_scope_block> pr(prog[g]);
-                    pr.store(xb + kLag, cuda::memory_order_release);
+                    if (BACK) w4[m] = make_float4(iv[15 - 4 * m], iv[14 - 4 * m], iv[13 - 4 * m], iv[12 - 4 * m]);
+                    else w4[m] = make_float4(iv[4 * m], iv[4 * m + 1], iv[4 * m + 2], iv[4 * m + 3]);
                 }
-                continue;
-            }
-            const bool inside = rowOk && xb >= 0 && xb + kLag <= W;
-            // Initial values of the block: one coverage word or 16 bytes of d1.
-            float iv[kLag];
-            if (inside)
-            {
-                if (BACK)
+                __syncwarp();
+#pragma unroll
+                for (int k = 0; k < 8; ++k)
                 {
-                    const int r0 = W - kLag - xb;  // real columns r0 .. r0+3 are x = xb+3 .. xb
-                    if (vec)
+                    const int j = 4 * k + sj;
+                    const int vyj = g * 32 + j, xsj = t0 - 2 * j - 2;
+                    const float2 v = *reinterpret_cast<const float2*>(st + j * kDtStR + 2 * sp);
+                    if (BACK)
                     {
-                        const float4 q = __ldg(reinterpret_cast<const float4*>(d1Row + r0));
-                        iv[0] = q.w; iv[1] = q.z; iv[2] = q.y; iv[3] = q.x;
+                        *reinterpret_cast<float2*>(dst + (size_t)(H - 1 - vyj) * W + (W - 16 - xsj) + 2 * sp) = v;
+                        // memory columns 2sp, 2sp+1 are chunk columns xs+15-2sp, xs+14-2sp
+                        if (j == 31) *reinterpret_cast<float2*>(ringOut + xsj + 14 - 2 * sp) = make_float2(v.y, v.x);
                     }
                     else
                     {
-#pragma unroll
-                        for (int q = 0; q < kLag; ++q) iv[q] = __ldg(d1Row + (W - 1 - xb - q));
+                        *reinterpret_cast<float2*>(dst + (size_t)vyj * W + xsj + 2 * sp) = v;
+                        if (j == 31) *reinterpret_cast<float2*>(ringOut + xsj + 2 * sp) = v;
                     }
-                }
-                else
-                {
-                    const uint32_t wd = __ldg(covRow + (xb >> 5)) >> (xb & 31);
-#pragma unroll
-                    for (int q = 0; q < kLag; ++q) iv[q] = ((wd >> q) & 1u) ? kInf : 0.0f;
                 }
             }
             else
             {
 #pragma unroll
-                for (int q = 0; q < kLag; ++q)
+                for (int q = 0; q < kDtChunk; ++q)
                 {
-                    const int x = xb + q;
-                    iv[q] = INF;
-                    if (rowOk && x >= 0 && x < W)
+                    const int x = xs + q;
+                    const bool ok = rowOk && x >= 0 && x < W;
+                    float iv = INF;
+                    if (ok)
+                        iv = BACK ? __ldg(inRow + (W - 1 - x))
+                                  : (((__ldg(covRow + (x >> 5)) >> (x & 31)) & 1u) ? kInf : 0.0f);
+                    const float recv = __shfl_up_sync(kFull, left, 1);
+                    // lane 0 reads columns >= -1 of the row above (ring holds +inf
+                    // outside [0, W)); group 0 has no row above
+                    float upp1 = recv;
+                    if (lane == 0) upp1 = hasAbove ? ringIn[min(max(x + 1, -1), W)] : INF;
+                    float av = fminf(iv, fadd(up0, 1.0f));
+                    av = fminf(av, fadd(upm1, kDiag));
+                    av = fminf(av, fadd(upp1, kDiag));
+                    av = fminf(av, fadd(left, 1.0f));
+                    const float d = ok ? av : INF;
+                    upm1 = up0;
+                    up0 = upp1;
+                    left = d;
+                    if (ok)
                     {
-                        const int rx = BACK ? W - 1 - x : x;
-                        iv[q] = BACK ? __ldg(d1Row + rx) : (((__ldg(covRow + (rx >> 5)) >> (rx & 31)) & 1u) ? kInf : 0.0f);
-                    }
-                }
-            }
-            float dv[kLag];
-#pragma unroll
-            for (int q = 0; q < kLag; ++q)
-            {
-                const int x = xb + q;
-                // Publish to the lane below my output of kLag-1 steps ago: its up[x+1].
-                float recv = __shfl_up_sync(kFull, h2, 1);
-                if (lane == 0) recv = (g > 0 && x + 1 >= 0 && x + 1 < W) ? ringIn[x + 1] : INF;
-                // Lanes 1..31 receive up[0] at their step x = -1; lane 0 starts
-                // at x = 0 and takes it from the ring (final: the first wait
-                // covered columns 0..kLag).
-                if (lane == 0 && x == 0 && g > 0) up0 = ringIn[0];
-                const float upp1 = recv;
-                float av = iv[q];
-                if (vy > 0)
-                {
-                    av = fminf(av, fadd(up0, 1.0f));
-                    if (x > 0) av = fminf(av, fadd(upm1, kDiag));
-                    if (x < W - 1) av = fminf(av, fadd(upp1, kDiag));
-                }
-                if (x > 0) av = fminf(av, fadd(left, 1.0f));
-                const bool ok = rowOk && x >= 0 && x < W;
-                const float d = ok ? av : INF;
-                dv[q] = d;
-                left = d;
-                upm1 = up0;
-                up0 = upp1;
-                h2 = h1;
-                h1 = h0;
-                h0 = d;
-            }
-            // Block results: one 16-byte store to the row (and to the ring for
-            // the last row of the group).
-            if (inside && vec)
-            {
-                if (BACK)
-                    *reinterpret_cast<float4*>(outRow + (W - kLag - xb)) = make_float4(dv[3], dv[2], dv[1], dv[0]);
-                else *reinterpret_cast<float4*>(outRow + xb) = make_float4(dv[0], dv[1], dv[2], dv[3]);
-                if (lane == 31) *reinterpret_cast<float4*>(ringOut + xb) = make_float4(dv[0], dv[1], dv[2], dv[3]);
-            }
-            else
-            {
-#pragma unroll
-                for (int q = 0; q < kLag; ++q)
-                {
-                    const int x = xb + q;
-                    if (rowOk && x >= 0 && x < W)
-                    {
-                        outRow[BACK ? W - 1 - x : x] = dv[q];
-                        if (lane == 31) ringOut[x] = dv[q];
+                        outRow[BACK ? W - 1 - x : x] = d;
+                        if (lane == 31) ringOut[x] = d;
                     }
                 }
             }
             // Lane 31 publishes how many columns of its row are final.
-            if (lane == 31 && xb + kLag - 1 >= 0)
+            if (lane == 31)
             {
-                __syncwarp(0x80000000u);
+                const int done = min(max(t0 - 64 + kDtChunk, 0), W);
                 cuda::atomic_ref<int, cuda::thread_scope_block> pr(prog[g]);
-                pr.store(min(xb + kLag, W), cuda::memory_order_release);
+                pr.store(done, cuda::memory_order_release);
             }
         }
     }
 }
-
 
 // A tile's contributor descriptors staged in shared memory: the per-pixel
 // loops below then index shared memory instead of chasing items[k] in global
@@ -1719,10 +1714,10 @@ size_t dt_prog_bytes(int maxH) { return (size_t)(((maxH + 31) >> 5) + 1) * sizeo
 int dt_rows_in_flight(int maxW, int maxH)
 {
     const size_t row = (size_t)dt_ring_stride(maxW) * sizeof(float);
-    const size_t prog = dt_prog_bytes(maxH);
-    auto fit = [&](size_t budget) { return budget > prog ? (int)((budget - prog) / row) : 0; };
-    int n = fit(100 * 1024);  // two CTAs per SM
-    if (n < 2) n = fit(210 * 1024);
+    const size_t fixed = dt_prog_bytes(maxH) + kDtStageBytes;
+    auto fit = [&](size_t budget) { return budget > fixed ? (int)((budget - fixed) / row) : 0; };
+    int n = fit(110 * 1024);  // two CTAs per SM
+    if (n < 2) n = fit(220 * 1024);
     return n > kDtRing ? kDtRing : n;
 }
 
@@ -1748,16 +1743,16 @@ int launch_dt(const BlendArgs& a, const int* itemList, int n, bool backward, int
     if (slotsWanted >= 2 && slotsWanted < slots) slots = slotsWanted;
     if (slots < 2)
         return fail(I360B_NOT_SUPPORTED, "Chunk %dx%d exceeds the distance-transform row ring.", maxW, maxH);
-    size_t smem = (size_t)slots * dt_ring_stride(maxW) * sizeof(float) + dt_prog_bytes(maxH);
+    size_t smem = kDtStageBytes + (size_t)slots * dt_ring_stride(maxW) * sizeof(float) + dt_prog_bytes(maxH);
     if (backward)
     {
         cudaFuncSetAttribute(k_dt<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        k_dt<true><<<n, 512, smem, s>>>(a, itemList, slots);
+        k_dt<true><<<n, 32 * kDtWarps, smem, s>>>(a, itemList, slots);
     }
     else
     {
         cudaFuncSetAttribute(k_dt<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        k_dt<false><<<n, 512, smem, s>>>(a, itemList, slots);
+        k_dt<false><<<n, 32 * kDtWarps, smem, s>>>(a, itemList, slots);
     }
     return check_launch("distance transform kernel");
 }
