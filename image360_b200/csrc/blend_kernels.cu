@@ -293,7 +293,6 @@ constexpr int kDtRing = 4;    // row-group hand-off slots
 constexpr int kDtWarps = 16;  // warps per CTA
 constexpr int kDtStR = 20;    // staging row stride (floats): 16 columns + pad, 16-byte rows
 constexpr size_t kDtStageBytes = (size_t)kDtWarps * 32 * kDtStR * sizeof(float);
-
 // Ring slot: columns -4 .. W of a row (index = column + 4); columns < 0 and
 // column W hold +inf.
 __host__ __device__ __forceinline__ int dt_ring_stride(int W) { return (W + 8) & ~3; }
@@ -383,37 +382,40 @@ __global__ void __launch_bounds__(32 * kDtWarps, 2) k_dt(BlendArgs a, const int*
             const int xs = t0 - 2 * lane - 2;  // this lane's column at the chunk's first step
             // Interior chunk: every lane's row and columns lie in the tile, so
             // no cell is virtual (but lane 0's row above, in group 0).
-            if (fullGroup && pairs && t0 - 64 >= 0 && t0 + kDtChunk - 2 <= W)
+            // Interior chunk: every lane's row and columns lie in the tile, so
+            // no cell is virtual (but lane 0's row above, in group 0).
+            // Elsewhere cells outside the tile are +inf and never stored; with
+            // an even row length a column pair is in or out as a whole.  The
+            // backward pass takes its edge chunks cell by cell (fewer registers
+            // in its staged path).
+            const bool interior = fullGroup && t0 - 64 >= 0 && t0 + kDtChunk - 2 <= W;
+            if (pairs && (!BACK || interior))
             {
-                float iv[kDtChunk];
+                // The chunk's initial values enter, and its results leave, this
+                // lane's staging row in memory order (the backward pass's columns
+                // reversed), four at a time.
+                float* const cur = st;
+                float4* myRow = reinterpret_cast<float4*>(cur + lane * kDtStR);
+                uint32_t bits = 0;
+                __syncwarp();  // the previous chunk's row-segment reads are done
                 if (BACK)
                 {
                     // Row j's 16 values sit at memory columns W-16-xs_j .. W-1-xs_j
                     // (mirrored); 8 lanes load each row as 8-byte pairs.
-                    __syncwarp();
 #pragma unroll
                     for (int k = 0; k < 8; ++k)
                     {
                         const int j = 4 * k + sj;
-                        const int vyj = g * 32 + j, xsj = t0 - 2 * j - 2;
-                        const float* rowj = src + (size_t)(H - 1 - vyj) * W + (W - 16 - xsj);
-                        *reinterpret_cast<float2*>(st + j * kDtStR + 2 * sp) =
-                            __ldg(reinterpret_cast<const float2*>(rowj + 2 * sp));
+                        const int vyj = g * 32 + j, m0 = W - 16 - (t0 - 2 * j - 2) + 2 * sp;
+                        *reinterpret_cast<float2*>(cur + j * kDtStR + 2 * sp) =
+                            __ldg(reinterpret_cast<const float2*>(src + (size_t)(H - 1 - vyj) * W + m0));
                     }
                     __syncwarp();
-                    const float4* r4 = reinterpret_cast<const float4*>(st + lane * kDtStR);
-#pragma unroll
-                    for (int m = 0; m < 4; ++m)
-                    {
-                        const float4 v = r4[m];  // memory columns 4m .. 4m+3 = chunk steps 15-4m .. 12-4m
-                        iv[15 - 4 * m] = v.x;
-                        iv[14 - 4 * m] = v.y;
-                        iv[13 - 4 * m] = v.z;
-                        iv[12 - 4 * m] = v.w;
-                    }
                 }
                 else
                 {
+                    // Coverage words xs>>5 and the next, held across chunks (the
+                    // word after them loaded a chunk early).
                     const int w0 = xs >> 5;
                     if (w0 != wIdx)
                     {
@@ -424,57 +426,106 @@ __global__ void __launch_bounds__(32 * kDtWarps, 2) k_dt(BlendArgs a, const int*
                         }
                         else
                         {
-                            wLo = __ldg(covRow + w0);
-                            wHi = w0 + 1 < covWords ? __ldg(covRow + w0 + 1) : 0u;
+                            wLo = w0 >= 0 && w0 < covWords ? __ldg(covRow + w0) : 0u;
+                            wHi = w0 + 1 >= 0 && w0 + 1 < covWords ? __ldg(covRow + w0 + 1) : 0u;
                         }
-                        wNx = w0 + 2 < covWords ? __ldg(covRow + w0 + 2) : 0u;
+                        wNx = w0 + 2 >= 0 && w0 + 2 < covWords ? __ldg(covRow + w0 + 2) : 0u;
                         wIdx = w0;
                     }
-                    const uint32_t bits = __funnelshift_r(wLo, wHi, xs & 31);
-#pragma unroll
-                    for (int q = 0; q < kDtChunk; ++q) iv[q] = ((bits >> q) & 1u) ? kInf : 0.0f;
+                    bits = __funnelshift_r(wLo, wHi, xs & 31);
                 }
+                // Lane 0's row above: columns t0-1 .. t0+14 (slot entries
+                // t0+3 .. t0+18) as five 16-byte reads, the same for every lane.
+                const float4* slot4 = reinterpret_cast<const float4*>(ringIn - 4) + (t0 >> 2);
+                float prevW = interior ? slot4[0].w : 0.0f;
 #pragma unroll
-                for (int q = 0; q < kDtChunk; ++q)
+                for (int m4 = 0; m4 < kDtChunk / 4; ++m4)
                 {
-                    const float recv = __shfl_up_sync(kFull, left, 1);
-                    const float upp1 = lane == 0 ? (hasAbove ? ringIn[xs + q + 1] : INF) : recv;
-                    float av = fminf(iv[q], fadd(up0, 1.0f));
-                    av = fminf(av, fadd(upm1, kDiag));
-                    av = fminf(av, fadd(upp1, kDiag));
-                    av = fminf(av, fadd(left, 1.0f));
-                    upm1 = up0;
-                    up0 = upp1;
-                    left = av;
-                    iv[q] = av;
-                }
-                // Results through the staging rows (memory order: the backward
-                // pass reversed), then 64-byte row segments to the output.
-                __syncwarp();
-                float4* w4 = reinterpret_cast<float4*>(st + lane * kDtStR);
+                    float in[4], o[4];
+                    if (BACK)
+                    {
+                        const float4 v = myRow[3 - m4];  // memory columns 12-4m4 .. 15-4m4
+                        in[0] = v.w;
+                        in[1] = v.z;
+                        in[2] = v.y;
+                        in[3] = v.x;
+                    }
+                    else
+                    {
 #pragma unroll
-                for (int m = 0; m < 4; ++m)
-                {
-                    if (BACK) w4[m] = make_float4(iv[15 - 4 * m], iv[14 - 4 * m], iv[13 - 4 * m], iv[12 - 4 * m]);
-                    else w4[m] = make_float4(iv[4 * m], iv[4 * m + 1], iv[4 * m + 2], iv[4 * m + 3]);
+                        for (int i = 0; i < 4; ++i) in[i] = ((bits >> (4 * m4 + i)) & 1u) ? kInf : 0.0f;
+                    }
+                    if (interior)
+                    {
+                        const float4 blk = slot4[m4 + 1];
+                        const float above[4] = {prevW, blk.x, blk.y, blk.z};
+                        prevW = blk.w;
+#pragma unroll
+                        for (int i = 0; i < 4; ++i)
+                        {
+                            const float recv = __shfl_up_sync(kFull, left, 1);
+                            const float upp1 = lane == 0 ? (hasAbove ? above[i] : INF) : recv;
+                            float av = fminf(in[i], fadd(up0, 1.0f));
+                            av = fminf(av, fadd(upm1, kDiag));
+                            av = fminf(av, fadd(upp1, kDiag));
+                            av = fminf(av, fadd(left, 1.0f));
+                            upm1 = up0;
+                            up0 = upp1;
+                            left = av;
+                            o[i] = av;
+                        }
+                    }
+                    else
+                    {
+#pragma unroll
+                        for (int i = 0; i < 4; ++i)
+                        {
+                            const int x = xs + 4 * m4 + i;
+                            const bool ok = rowOk && x >= 0 && x < W;
+                            const float recv = __shfl_up_sync(kFull, left, 1);
+                            // lane 0 reads columns >= -1 of the row above (the ring
+                            // holds +inf outside [0, W)); group 0 has no row above
+                            float upp1 = recv;
+                            if (lane == 0) upp1 = hasAbove ? ringIn[min(max(x + 1, -1), W)] : INF;
+                            float av = fminf(in[i], fadd(up0, 1.0f));
+                            av = fminf(av, fadd(upm1, kDiag));
+                            av = fminf(av, fadd(upp1, kDiag));
+                            av = fminf(av, fadd(left, 1.0f));
+                            const float d = ok ? av : INF;
+                            upm1 = up0;
+                            up0 = upp1;
+                            left = d;
+                            o[i] = d;
+                        }
+                    }
+                    if (BACK) myRow[3 - m4] = make_float4(o[3], o[2], o[1], o[0]);
+                    else myRow[m4] = make_float4(o[0], o[1], o[2], o[3]);
                 }
+                // 64-byte row segments to the output.
                 __syncwarp();
 #pragma unroll
                 for (int k = 0; k < 8; ++k)
                 {
                     const int j = 4 * k + sj;
                     const int vyj = g * 32 + j, xsj = t0 - 2 * j - 2;
-                    const float2 v = *reinterpret_cast<const float2*>(st + j * kDtStR + 2 * sp);
+                    const float2 v = *reinterpret_cast<const float2*>(cur + j * kDtStR + 2 * sp);
                     if (BACK)
                     {
-                        *reinterpret_cast<float2*>(dst + (size_t)(H - 1 - vyj) * W + (W - 16 - xsj) + 2 * sp) = v;
-                        // memory columns 2sp, 2sp+1 are chunk columns xs+15-2sp, xs+14-2sp
-                        if (j == 31) *reinterpret_cast<float2*>(ringOut + xsj + 14 - 2 * sp) = make_float2(v.y, v.x);
+                        const int m0 = W - 16 - xsj + 2 * sp;  // chunk columns xs_j+15-2sp, xs_j+14-2sp
+                        if (interior || (vyj < H && m0 >= 0 && m0 < W))
+                        {
+                            *reinterpret_cast<float2*>(dst + (size_t)(H - 1 - vyj) * W + m0) = v;
+                            if (j == 31) *reinterpret_cast<float2*>(ringOut + xsj + 14 - 2 * sp) = make_float2(v.y, v.x);
+                        }
                     }
                     else
                     {
-                        *reinterpret_cast<float2*>(dst + (size_t)vyj * W + xsj + 2 * sp) = v;
-                        if (j == 31) *reinterpret_cast<float2*>(ringOut + xsj + 2 * sp) = v;
+                        const int c0 = xsj + 2 * sp;
+                        if (interior || (vyj < H && c0 >= 0 && c0 < W))
+                        {
+                            *reinterpret_cast<float2*>(dst + (size_t)vyj * W + c0) = v;
+                            if (j == 31) *reinterpret_cast<float2*>(ringOut + c0) = v;
+                        }
                     }
                 }
             }
