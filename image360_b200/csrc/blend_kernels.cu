@@ -303,14 +303,26 @@ __global__ void __launch_bounds__(32 * kDtWarps, 2) k_dt(BlendArgs a, const int*
     extern __shared__ float smem[];
     const ItemDev& it = a.items[itemList[blockIdx.x]];
     const TileDev& T = a.tiles[it.tile];
-    const int W = T.w, H = T.h, covWords = T.covWords;
+    const int Wt = T.w, Ht = T.h, covWords = T.covWords;
     // A contributor that covers none or all of its tile has d == 0 or
     // d == kInf everywhere (no seed / nothing to seed); the ownership kernel
     // substitutes those values, so the transform is skipped.
     {
         const int cnt = it.bbox[4];
-        if (cnt == 0 || (long long)cnt == (long long)W * H) return;
+        if (cnt == 0 || (long long)cnt == (long long)Wt * Ht) return;
     }
+    // The transform runs on R: the covered box grown by one cell and clamped
+    // to the tile, its left edge rounded down to an even column and its right
+    // edge up to an odd one where the tile allows (rows of 8-byte pairs).
+    // Cells outside the box are uncovered, so d == 0 there; the cells of R
+    // outside the box are uncovered too and come out 0 whatever lies beyond
+    // R, and every cell inside the box reads only cells of R.  So the
+    // recurrence on R with +inf beyond it gives the tile transform's values
+    // on R.  Nothing is written outside R: the ownership kernel, the fields'
+    // only reader, takes d == 0 outside the covered box.
+    const int rx0 = max(it.bbox[0] - 1, 0) & ~1, rx1 = min((it.bbox[2] + 1) | 1, Wt - 1);
+    const int ry0 = max(it.bbox[1] - 1, 0), ry1 = min(it.bbox[3] + 1, Ht - 1);
+    const int W = rx1 - rx0 + 1, H = ry1 - ry0 + 1;  // R's extent; the recurrence below runs on R
     const int RS = dt_ring_stride(W);
     float* ring = smem + kDtStageBytes / sizeof(float);
     int* prog = reinterpret_cast<int*>(ring + (size_t)nslots * RS);
@@ -323,14 +335,15 @@ __global__ void __launch_bounds__(32 * kDtWarps, 2) k_dt(BlendArgs a, const int*
         ring[(size_t)sl * RS + (e < 4 ? e : W + 4)] = INF;
     }
     __syncthreads();
-    const float kInf = (float)(W + H);
+    const float kInf = (float)(Wt + Ht);
     const float kDiag = 1.41421356f;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int nwarps = blockDim.x >> 5;
     const float* src = BACK ? it.d1 : nullptr;
     float* dst = BACK ? it.d : it.d1;
     // 8-byte pairs of columns: even row length and 8-byte aligned buffers.
-    const bool pairs = (W & 1) == 0 && ((reinterpret_cast<uintptr_t>(dst) | reinterpret_cast<uintptr_t>(src)) & 7) == 0;
+    const bool pairs = (W & 1) == 0 && (Wt & 1) == 0 &&
+                       ((reinterpret_cast<uintptr_t>(dst) | reinterpret_cast<uintptr_t>(src)) & 7) == 0;
     const int nSteps = W + 64;  // lane 31 computes column W - 1 at step W + 63
 
     for (int g = warp; g < nG; g += nwarps)
@@ -339,10 +352,10 @@ __global__ void __launch_bounds__(32 * kDtWarps, 2) k_dt(BlendArgs a, const int*
         const bool rowOk = vy < H;
         const bool fullGroup = g * 32 + 31 < H;
         const bool hasAbove = g > 0;  // lane 0's row above: the ring, else virtual
-        const int ry = rowOk ? (BACK ? H - 1 - vy : vy) : 0;  // memory row
-        float* outRow = dst + (size_t)ry * W;
-        const float* inRow = BACK ? src + (size_t)ry * W : nullptr;
-        const uint32_t* covRow = it.cov + (size_t)ry * covWords;
+        const int ty = rowOk ? (BACK ? ry1 - vy : ry0 + vy) : ry0;  // tile row
+        float* outRow = dst + (size_t)ty * Wt;
+        const float* inRow = BACK ? src + (size_t)ty * Wt : nullptr;
+        const uint32_t* covRow = it.cov + (size_t)ty * covWords;
         // Staging rows of this warp: a chunk's 32 x 16 values cross between
         // lanes (one row each) and 8-lane groups (one 64-byte row segment per
         // global access) here.
@@ -400,15 +413,15 @@ __global__ void __launch_bounds__(32 * kDtWarps, 2) k_dt(BlendArgs a, const int*
                 __syncwarp();  // the previous chunk's row-segment reads are done
                 if (BACK)
                 {
-                    // Row j's 16 values sit at memory columns W-16-xs_j .. W-1-xs_j
+                    // Row j's 16 values sit at tile columns rx1-15-xs_j .. rx1-xs_j
                     // (mirrored); 8 lanes load each row as 8-byte pairs.
 #pragma unroll
                     for (int k = 0; k < 8; ++k)
                     {
                         const int j = 4 * k + sj;
-                        const int vyj = g * 32 + j, m0 = W - 16 - (t0 - 2 * j - 2) + 2 * sp;
+                        const int vyj = g * 32 + j, m0 = rx1 - 15 - (t0 - 2 * j - 2) + 2 * sp;
                         *reinterpret_cast<float2*>(cur + j * kDtStR + 2 * sp) =
-                            __ldg(reinterpret_cast<const float2*>(src + (size_t)(H - 1 - vyj) * W + m0));
+                            __ldg(reinterpret_cast<const float2*>(src + (size_t)(ry1 - vyj) * Wt + m0));
                     }
                     __syncwarp();
                 }
@@ -416,7 +429,8 @@ __global__ void __launch_bounds__(32 * kDtWarps, 2) k_dt(BlendArgs a, const int*
                 {
                     // Coverage words xs>>5 and the next, held across chunks (the
                     // word after them loaded a chunk early).
-                    const int w0 = xs >> 5;
+                    const int xa = rx0 + xs;  // tile column of the chunk's first step
+                    const int w0 = xa >> 5;
                     if (w0 != wIdx)
                     {
                         if (w0 == wIdx + 1)
@@ -432,7 +446,7 @@ __global__ void __launch_bounds__(32 * kDtWarps, 2) k_dt(BlendArgs a, const int*
                         wNx = w0 + 2 >= 0 && w0 + 2 < covWords ? __ldg(covRow + w0 + 2) : 0u;
                         wIdx = w0;
                     }
-                    bits = __funnelshift_r(wLo, wHi, xs & 31);
+                    bits = __funnelshift_r(wLo, wHi, xa & 31);
                 }
                 // Lane 0's row above: columns t0-1 .. t0+14 (slot entries
                 // t0+3 .. t0+18) as five 16-byte reads, the same for every lane.
@@ -511,10 +525,10 @@ __global__ void __launch_bounds__(32 * kDtWarps, 2) k_dt(BlendArgs a, const int*
                     const float2 v = *reinterpret_cast<const float2*>(cur + j * kDtStR + 2 * sp);
                     if (BACK)
                     {
-                        const int m0 = W - 16 - xsj + 2 * sp;  // chunk columns xs_j+15-2sp, xs_j+14-2sp
-                        if (interior || (vyj < H && m0 >= 0 && m0 < W))
+                        const int m0 = rx1 - 15 - xsj + 2 * sp;  // chunk columns xs_j+15-2sp, xs_j+14-2sp
+                        if (interior || (vyj < H && m0 >= rx0 && m0 < rx1))
                         {
-                            *reinterpret_cast<float2*>(dst + (size_t)(H - 1 - vyj) * W + m0) = v;
+                            *reinterpret_cast<float2*>(dst + (size_t)(ry1 - vyj) * Wt + m0) = v;
                             if (j == 31) *reinterpret_cast<float2*>(ringOut + xsj + 14 - 2 * sp) = make_float2(v.y, v.x);
                         }
                     }
@@ -523,7 +537,7 @@ __global__ void __launch_bounds__(32 * kDtWarps, 2) k_dt(BlendArgs a, const int*
                         const int c0 = xsj + 2 * sp;
                         if (interior || (vyj < H && c0 >= 0 && c0 < W))
                         {
-                            *reinterpret_cast<float2*>(dst + (size_t)vyj * W + c0) = v;
+                            *reinterpret_cast<float2*>(dst + (size_t)(ry0 + vyj) * Wt + rx0 + c0) = v;
                             if (j == 31) *reinterpret_cast<float2*>(ringOut + c0) = v;
                         }
                     }
@@ -538,8 +552,8 @@ __global__ void __launch_bounds__(32 * kDtWarps, 2) k_dt(BlendArgs a, const int*
                     const bool ok = rowOk && x >= 0 && x < W;
                     float iv = INF;
                     if (ok)
-                        iv = BACK ? __ldg(inRow + (W - 1 - x))
-                                  : (((__ldg(covRow + (x >> 5)) >> (x & 31)) & 1u) ? kInf : 0.0f);
+                        iv = BACK ? __ldg(inRow + (rx1 - x))
+                                  : (((__ldg(covRow + ((rx0 + x) >> 5)) >> ((rx0 + x) & 31)) & 1u) ? kInf : 0.0f);
                     const float recv = __shfl_up_sync(kFull, left, 1);
                     // lane 0 reads columns >= -1 of the row above (ring holds +inf
                     // outside [0, W)); group 0 has no row above
@@ -555,7 +569,7 @@ __global__ void __launch_bounds__(32 * kDtWarps, 2) k_dt(BlendArgs a, const int*
                     left = d;
                     if (ok)
                     {
-                        outRow[BACK ? W - 1 - x : x] = d;
+                        outRow[BACK ? rx1 - x : rx0 + x] = d;
                         if (lane == 31) ringOut[x] = d;
                     }
                 }
