@@ -176,7 +176,7 @@ __device__ __forceinline__ void warp_zero_u16(unsigned short* p, int n, int lane
     if (lane < n - t0) p[t0 + lane] = 0;
 }
 
-__global__ void __launch_bounds__(256, 4) k_warp_tiles(BlendArgs a, const Unit* __restrict__ units)
+__global__ void __launch_bounds__(256, 8) k_warp_tiles(BlendArgs a, const Unit* __restrict__ units)
 {
     const Unit u = units[blockIdx.x];
     const ItemDev& it = a.items[u.id];
@@ -1299,7 +1299,7 @@ __device__ __forceinline__ PackedPx shfl_px(const PackedPx& v, int delta, bool u
     return o;
 }
 
-__global__ void __launch_bounds__(256) k_down0s(BlendArgs a, const Unit* __restrict__ units, int n)
+__global__ void __launch_bounds__(256, 4) k_down0s(BlendArgs a, const Unit* __restrict__ units, int n)
 {
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int ui = blockIdx.x * kDnWarps + warp;
