@@ -703,7 +703,7 @@ __global__ void __launch_bounds__(256) k_owner(BlendArgs a, const Unit* __restri
 // memory.
 // ---------------------------------------------------------------------------
 constexpr int kSeamThreads = 1024;
-constexpr int kDpThreads = 128;
+constexpr int kDpThreads = 512;  // 8 threads per candidate (64 candidate slots)
 
 // First byte of a 16-byte chunk (positions t = tb + b) that satisfies the
 // predicate, or INT_MAX.
@@ -934,16 +934,17 @@ __global__ void __launch_bounds__(kSeamThreads, 1) k_seam(BlendArgs a, const int
                 __syncthreads();
             }
             // Phase 3b: dynamic program over contested lines
-            // (SeamBlend.cpp:362-407) on the first kDpThreads threads: thread
-            // pairs share a candidate k, each scanning half of the previous
-            // line's entries in four interleaved chains; the halves merge with
-            // the lowest-index rule of the reference's strict '<' scan.
-            // Penalties 2|t - pt| are exact small integers formed in float.
-            // Candidate costs are fetched kPre lines ahead.
+            // (SeamBlend.cpp:362-407) on the first kDpThreads threads: 8
+            // threads share a candidate k, each scanning every 8th entry of the
+            // previous line in index order; the parts merge to the lowest
+            // (value, index), which is what the reference's strict '<' scan in
+            // index order keeps.  Penalties 2|t - pt| are exact small integers
+            // formed in float.  Candidate costs are fetched kPre lines ahead.
             if (tid < kDpThreads)
             {
                 constexpr int kPre = 4;
-                const int k = tid >> 1, half = tid & 1;
+                constexpr int kParts = 8;
+                const int k = tid / kParts, part = tid % kParts;
                 const int nC = sNumContested;
                 float cq[kPre];
 #pragma unroll
@@ -975,60 +976,37 @@ __global__ void __launch_bounds__(kSeamThreads, 1) k_seam(BlendArgs a, const int
                     float b = FLT_MAX;
                     if (last >= 0 && k < lw)
                     {
-                        const int plo = sLo[last];
-                        const int hsplit = (lastW + 1) >> 1;
-                        const int pb = half ? hsplit : 0, pe = half ? lastW : hsplit;
-                        const float d0 = (float)(lo + k - plo - pb);  // t - pt at pk = pb
-                        float best[4] = {FLT_MAX, FLT_MAX, FLT_MAX, FLT_MAX};
-                        int bi[4] = {-1, -1, -1, -1};
-                        for (int pk = pb; pk < pe; pk += 4)
-                        {
+                        const float d0 = (float)(lo + k - sLo[last]);  // t - pt at pk = 0
 #pragma unroll
-                            for (int q = 0; q < 4; ++q)
+                        for (int i = 0; i < (kSeamBand + kParts - 1) / kParts; ++i)
+                        {
+                            const int kk = part + kParts * i;
+                            if (kk < lastW)
                             {
-                                const int kk = pk + q;
-                                if (kk < pe)
+                                const float dd = fsub(d0, (float)kk);
+                                const float pen = fadd(fabsf(dd), fabsf(dd));
+                                const float c2 = fadd(dpBuf[cur ^ 1][kk], pen);
+                                if (c2 < b)
                                 {
-                                    const float dd = fsub(d0, (float)(kk - pb));
-                                    const float pen = fadd(fabsf(dd), fabsf(dd));
-                                    const float c2 = fadd(dpBuf[cur ^ 1][kk], pen);
-                                    if (c2 < best[q])
-                                    {
-                                        best[q] = c2;
-                                        bi[q] = kk;
-                                    }
+                                    b = c2;
+                                    bp = kk;
                                 }
                             }
                         }
-                        b = best[0];
-                        bp = bi[0];
-#pragma unroll
-                        for (int q = 1; q < 4; ++q)
-                            if (bi[q] >= 0 && (best[q] < b || (best[q] == b && (bp < 0 || bi[q] < bp))))
-                            {
-                                b = best[q];
-                                bp = bi[q];
-                            }
                     }
-                    // Merge with the partner half (the lower half holds lower indices).
+#pragma unroll
+                    for (int m = 1; m < kParts; m <<= 1)
                     {
-                        const float ob = __shfl_xor_sync(0xffffffffu, b, 1);
-                        const int obp = __shfl_xor_sync(0xffffffffu, bp, 1);
-                        const float b0 = half ? ob : b, b1 = half ? b : ob;
-                        const int i0 = half ? obp : bp, i1 = half ? bp : obp;
-                        if (i0 >= 0 && (i1 < 0 || !(b1 < b0)))
+                        const float ob = __shfl_xor_sync(0xffffffffu, b, m);
+                        const int obp = __shfl_xor_sync(0xffffffffu, bp, m);
+                        if (obp >= 0 && (bp < 0 || ob < b || (ob == b && obp < bp)))
                         {
-                            b = b0;
-                            bp = i0;
-                        }
-                        else
-                        {
-                            b = b1;
-                            bp = i1;
+                            b = ob;
+                            bp = obp;
                         }
                     }
                     if (last >= 0 && k < lw) val = fadd(c, b);
-                    if (half == 0 && k < lw)
+                    if (part == 0 && k < lw)
                     {
                         dpBuf[cur][k] = val;
                         sBack[(size_t)line * kSeamBand + k] = (unsigned char)(bp < 0 ? 255 : bp);
