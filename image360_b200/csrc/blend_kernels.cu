@@ -705,20 +705,23 @@ __global__ void __launch_bounds__(256) k_owner(BlendArgs a, const Unit* __restri
 constexpr int kSeamThreads = 1024;
 constexpr int kDpThreads = 512;  // 8 threads per candidate (64 candidate slots)
 
-// First byte of a 16-byte chunk (positions t = tb + b) that satisfies the
-// predicate, or INT_MAX.
-template <typename Pred>
-__device__ __forceinline__ int first_in_chunk(uint4 v, int tb, int lineLen, Pred pred)
+// First position t = tb + b (b in 0..15) of a 16-byte chunk of owner bytes,
+// with 0 <= t < lineLen, whose byte equals a or b (owner indices 0..127), or
+// INT_MAX: four-byte SIMD compares instead of a byte loop.
+__device__ __forceinline__ int first_owner_in_chunk(uint4 v, unsigned repA, unsigned repB, int tb, int lineLen)
 {
+    const int b0 = max(0, -tb), b1 = min(16, lineLen - tb);
+    if (b0 >= b1) return 0x7fffffff;
     const unsigned w[4] = {v.x, v.y, v.z, v.w};
+    unsigned mask = 0;
 #pragma unroll
-    for (int b = 0; b < 16; ++b)
+    for (int i = 0; i < 4; ++i)
     {
-        const int t = tb + b;
-        const int o = (int)(signed char)((w[b >> 2] >> ((b & 3) * 8)) & 0xffu);
-        if (t >= 0 && t < lineLen && pred(o)) return t;
+        const unsigned m = (__vcmpeq4(w[i], repA) | __vcmpeq4(w[i], repB)) & 0x80808080u;
+        mask |= (((m >> 7) & 1u) | ((m >> 14) & 2u) | ((m >> 21) & 4u) | ((m >> 28) & 8u)) << (4 * i);
     }
-    return 0x7fffffff;
+    mask &= ((1u << b1) - 1u) & ~((1u << b0) - 1u);
+    return mask ? tb + __ffs(mask) - 1 : 0x7fffffff;
 }
 
 __global__ void __launch_bounds__(kSeamThreads, 1) k_seam(BlendArgs a, const int* __restrict__ tileList, int smemLines)
@@ -788,6 +791,7 @@ __global__ void __launch_bounds__(kSeamThreads, 1) k_seam(BlendArgs a, const int
             // Phase 1: crossover of each line (SeamBlend.cpp:334-345) and its band.
             if (rowScan)
             {
+                const unsigned repI = (unsigned)ci * 0x01010101u, repJ = (unsigned)cj * 0x01010101u;
                 for (int line = warp; line < numLines; line += nwarps)
                 {
                     const signed char* rowp = T.owner + pix(line, 0);
@@ -801,24 +805,21 @@ __global__ void __launch_bounds__(kSeamThreads, 1) k_seam(BlendArgs a, const int
                     {
                         const int c = c0 + lane;
                         int f = 0x7fffffff;
-                        if (c < nChunks)
-                            f = first_in_chunk(src[c], c * 16 - off, lineLen, [&](int o) { return o == ci || o == cj; });
+                        if (c < nChunks) f = first_owner_in_chunk(src[c], repI, repJ, c * 16 - off, lineLen);
                         p1 = __reduce_min_sync(kFull, f);
                     }
                     int cross = -1;
                     if (p1 != 0x7fffffff)
                     {
                         v1 = (int)T.owner[pix(line, p1)];
+                        const unsigned repO = (v1 == ci ? (unsigned)cj : (unsigned)ci) * 0x01010101u;  // the other of I, J
                         const int cStart = (p1 + off) >> 4;
                         int f2 = 0x7fffffff;
                         for (int c0 = cStart; c0 < nChunks && f2 == 0x7fffffff; c0 += 32)
                         {
                             const int c = c0 + lane;
                             int f = 0x7fffffff;
-                            if (c < nChunks)
-                                f = first_in_chunk(src[c], c * 16 - off, lineLen, [&](int o) {
-                                    return (o == ci || o == cj) && o != v1;
-                                });
+                            if (c < nChunks) f = first_owner_in_chunk(src[c], repO, repO, c * 16 - off, lineLen);
                             if (f <= p1) f = 0x7fffffff;  // only positions after the first I/J pixel
                             f2 = __reduce_min_sync(kFull, f);
                         }
