@@ -185,7 +185,7 @@ int Plan::build(const std::vector<TileSpec>& specs, int numBands, bool renderPat
         maxH = std::max(maxH, S.h);
         size_t px = (size_t)S.w * S.h;
         TOff& to = tileOff[t];
-        to.owner = bytes; bytes += align256(px);
+        to.owner = bytes; bytes += align256(px + 16);  // + 16: the seam scan's 16-byte chunk reads past a row end stay inside
         to.blend = bytes; bytes += align256(std::max<size_t>(pyrPx, 1) * 12);
         size_t ml = (size_t)T.maxLines;
         to.lo = bytes; bytes += align256(ml * 4);
