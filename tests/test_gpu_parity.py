@@ -136,6 +136,28 @@ def test_blend_random_exact(backend, oracle_c, seed):
         assert np.array_equal(out, ref), (seed, bands, int(np.abs(out.astype(int) - ref).max()))
 
 
+def _box_buf(rng, w, h, x0, y0, x1, y1):
+    img = np.zeros((h, w, 3), np.uint16)
+    img[y0:y1 + 1, x0:x1 + 1] = rng.integers(100, 30000, (y1 - y0 + 1, x1 - x0 + 1, 3)).astype(np.uint16)
+    return img
+
+
+@pytest.mark.parametrize("w,h", [(130, 70), (131, 97), (258, 66), (515, 40), (64, 200)])
+def test_blend_box_geometry_exact(backend, oracle_c, w, h):
+    """Covered boxes with odd and even edges, touching the tile's borders or
+    not, on tiles wide enough for interior distance-transform chunks (even
+    widths take the paired path, odd ones the cell path)."""
+    rng = np.random.default_rng(w * 1000 + h)
+    bufs = [_box_buf(rng, w, h, 0, 0, w // 2 + 1, h - 1),            # left, full height
+            _box_buf(rng, w, h, w // 3, 3, w - 1, h // 2 + 5),        # right edge, odd top
+            _box_buf(rng, w, h, w // 5 + 1, h // 4, 4 * w // 5, h - 2)]  # interior, odd left edge
+    for bands in (3, 6):
+        out = np.zeros((h, w, 3), np.uint16)
+        assert backend.blend_chunk_contributors(bufs, w, h, out, bands) == ComputeResult.SUCCESS, backend.get_last_error()
+        ref = oracle_c.blend(bufs, bands)
+        assert np.array_equal(out, ref), (w, h, bands, int(np.abs(out.astype(int) - ref).max()))
+
+
 def test_blend_empty_and_single(backend, oracle_c):
     w, h = 50, 30
     out = np.ones((h, w, 3), np.uint16)
