@@ -773,19 +773,6 @@ __global__ void __launch_bounds__(kSeamThreads, 1) k_seam(BlendArgs a, const int
                 const int y = rowScan ? oy0 + line : oy0 + t;
                 return cov_bit(I.cov, T.covWords, x, y) && cov_bit(J.cov, T.covWords, x, y);
             };
-            // Contested band of a line (SeamBlend.cpp:347-359).
-            auto band_of = [&](int line, int cross, int& lo, int& hi) {
-                lo = 1;
-                hi = 0;
-                if (cross < 0) return;
-                const int bLo = max(0, cross - kSeamRadius), bHi = min(lineLen - 1, cross + kSeamRadius);
-                for (int t = bLo; t <= bHi; ++t)
-                    if (both_cov(line, t))
-                    {
-                        if (hi < lo) lo = t;
-                        hi = t;
-                    }
-            };
 
             long long tp = clock64();
             // Phase 1: crossover of each line (SeamBlend.cpp:334-345) and its band.
@@ -867,8 +854,33 @@ __global__ void __launch_bounds__(kSeamThreads, 1) k_seam(BlendArgs a, const int
                             else if (o != first) cross = t0 + q;
                         }
                     }
-                    int lo, hi;
-                    band_of(line, cross, lo, hi);
+                    // Contested band (SeamBlend.cpp:347-359): the coverage bits
+                    // of 8 rows requested at once (both contributors' words, no
+                    // short circuit).
+                    int lo = 1, hi = 0;
+                    if (cross >= 0)
+                    {
+                        const int bLo = max(0, cross - kSeamRadius), bHi = min(lineLen - 1, cross + kSeamRadius);
+                        const int x = ox0 + line;
+                        for (int tb = bLo; tb <= bHi; tb += 8)
+                        {
+                            bool ok[8];
+#pragma unroll
+                            for (int q = 0; q < 8; ++q)
+                            {
+                                const int y = oy0 + min(tb + q, bHi);
+                                ok[q] = tb + q <= bHi &&
+                                        (cov_bit(I.cov, T.covWords, x, y) & cov_bit(J.cov, T.covWords, x, y));
+                            }
+#pragma unroll
+                            for (int q = 0; q < 8; ++q)
+                                if (ok[q])
+                                {
+                                    if (hi < lo) lo = tb + q;
+                                    hi = tb + q;
+                                }
+                        }
+                    }
                     sLo[line] = lo;
                     sHi[line] = hi;
                 }
