@@ -326,7 +326,10 @@ def run_ours(args, rank, world, local_rank):
                                "k's render, after its warp stage has read the frames",
                    "autotuned": tuned},
         "roofline": roof, "stages": per_stage, "gpu_launches": launches,
-        "seam_phase_cycles": stats["seamPhaseCycles"],
+        # SM cycles of the seam kernel's five phases (crossover scan, colour
+        # cost, DP, backtrack, reassign), summed over tiles, pairs and every
+        # execution of the plan since it was built (autotuning included).
+        "seam_phase_cycles_cumulative": stats["seamPhaseCycles"],
         "clocks": clk.summary(),
         "e2e": e2e,
     }
