@@ -666,29 +666,69 @@ __global__ void __launch_bounds__(256) k_owner(BlendArgs a, const Unit* __restri
     const float kInf = (float)(W + T.h);
     const int row0 = u.by * a.bandRows;
     const int rows = min(a.bandRows, T.h - row0);
+    // Four pixels per thread: 16-byte reads of d and one 4-byte owner store
+    // when rows are 4-pixel aligned.  A contributor with no covered pixel, or
+    // whose covered box misses the pixels, has d == 0 there and cannot win
+    // (the argmax needs d > 0), so it is skipped.
+    const bool vec = (W & 3) == 0;
     for (int r = 0; r < rows; ++r)
     {
         const int y = row0 + r;
-        for (int x = threadIdx.x; x < W; x += blockDim.x)
+        for (int x4 = threadIdx.x * 4; x4 < W; x4 += blockDim.x * 4)
         {
-            const long long p = (long long)y * W + x;
-            int best = -1;
-            float bestD = 0.0f;
+            const long long p = (long long)y * W + x4;
+            const int n = min(4, W - x4);
+            int best[4] = {-1, -1, -1, -1};
+            float bestD[4] = {0.0f, 0.0f, 0.0f, 0.0f};
             for (int k = 0; k < K; ++k)
             {
                 const int cnt = C.cnt[k];
-                const int4 B = C.box[k];
-                // d is 0 outside the covered box
-                const bool in = x >= B.x && x <= B.z && y >= B.y && y <= B.w;
-                const float v =
-                    cnt == 0 ? 0.0f : ((long long)cnt == full ? kInf : (in ? __ldg(C.d[k] + p) : 0.0f));
-                if (v > bestD)
+                if (cnt == 0) continue;
+                if ((long long)cnt == full)
                 {
-                    bestD = v;
-                    best = k;
+#pragma unroll
+                    for (int i = 0; i < 4; ++i)
+                        if (kInf > bestD[i])
+                        {
+                            bestD[i] = kInf;
+                            best[i] = k;
+                        }
+                    continue;
+                }
+                const int4 B = C.box[k];
+                if (y < B.y || y > B.w || x4 + 3 < B.x || x4 > B.z) continue;
+                float v[4];
+                if (vec)
+                {
+                    const float4 q = __ldg(reinterpret_cast<const float4*>(C.d[k] + p));
+                    v[0] = q.x;
+                    v[1] = q.y;
+                    v[2] = q.z;
+                    v[3] = q.w;
+                }
+                else
+                {
+#pragma unroll
+                    for (int i = 0; i < 4; ++i) v[i] = i < n ? __ldg(C.d[k] + p + i) : 0.0f;
+                }
+#pragma unroll
+                for (int i = 0; i < 4; ++i)
+                {
+                    const int x = x4 + i;
+                    const float vi = (x >= B.x && x <= B.z) ? v[i] : 0.0f;  // d is 0 outside the covered box
+                    if (vi > bestD[i])
+                    {
+                        bestD[i] = vi;
+                        best[i] = k;
+                    }
                 }
             }
-            T.owner[p] = (signed char)best;
+            if (vec)
+                *reinterpret_cast<uint32_t*>(T.owner + p) = (uint32_t)(best[0] & 0xff) | ((uint32_t)(best[1] & 0xff) << 8) |
+                                                            ((uint32_t)(best[2] & 0xff) << 16) |
+                                                            ((uint32_t)(best[3] & 0xff) << 24);
+            else
+                for (int i = 0; i < n; ++i) T.owner[p + i] = (signed char)best[i];
         }
     }
 }
