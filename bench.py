@@ -182,7 +182,9 @@ def _levels(w, h, bands):
 
 
 def stage_bytes(stats, S):
-    """Algorithmic bytes per stage (formulas stated in DESIGN.md)."""
+    """Algorithmic bytes per stage: the bytes each stage must move over the
+    workload's tiles and contributors (item pixels, covered pixels, pyramid
+    levels), counted over every item pixel."""
     cfg = S["cfg"]
     npx_in = len(S["cfa"]) * cfg.frame_w * cfg.frame_h
     cov = stats["coveredItemPixels"]
