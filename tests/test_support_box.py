@@ -64,3 +64,29 @@ def test_empty_box_stays_empty():
     for level in range(6):
         b = support(box, level)
         assert b[0] > b[2] and b[1] > b[3]
+
+
+@pytest.mark.parametrize("seed", range(10))
+def test_owned_pixels_lie_in_the_owners_covered_box(oracle_c, seed):
+    """The level-0 weight (owner mask) vanishes outside the covered box: the
+    ownership argmax needs coverage, and the seam refinement reassigns
+    pixels only inside two contributors' common box (SeamBlend.cpp:439-442,
+    580).  Checked on the oracle's final owner maps."""
+    rng = np.random.default_rng(50 + seed)
+    w, h = int(rng.integers(20, 120)), int(rng.integers(20, 120))
+    bufs = []
+    for _ in range(int(rng.integers(2, 6))):
+        img = np.zeros((h, w, 3), np.uint16)
+        for _ in range(int(rng.integers(1, 3))):  # one or two rectangles: non-convex coverage too
+            x0, y0 = int(rng.integers(0, w - 4)), int(rng.integers(0, h - 4))
+            x1, y1 = min(w - 1, x0 + int(rng.integers(3, w))), min(h - 1, y0 + int(rng.integers(3, h)))
+            img[y0:y1 + 1, x0:x1 + 1] = rng.integers(100, 30000, (y1 - y0 + 1, x1 - x0 + 1, 3)).astype(np.uint16)
+        bufs.append(img)
+    _, owner = oracle_c.blend(bufs, 5, return_owner=True)
+    for k, img in enumerate(bufs):
+        cov = img.any(axis=2)
+        ys, xs = np.nonzero(owner == k)
+        if len(ys) == 0:
+            continue
+        cy, cx = np.nonzero(cov)
+        assert ys.min() >= cy.min() and ys.max() <= cy.max() and xs.min() >= cx.min() and xs.max() <= cx.max()
