@@ -206,7 +206,9 @@ def stage_bytes(stats, S):
             collapse += 24 * n[l]
     return {
         "demosaic": npx_in * (2 + 6),
-        "warp_gain_coverage": cov * 6 + item_px * 6 + item_px // 8,
+        # 6 B of source read and 6 B written per covered item pixel (bilinear
+        # taps at about 1:1 scale read each source texel about once)
+        "warp_gain_coverage": cov * 12,
         "chamfer_forward": item_px // 8 + item_px * 4,
         "chamfer_backward": item_px * 8,
         "ownership": item_px * 4 + out,
@@ -288,16 +290,19 @@ def run_ours(args, rank, world, local_rank):
     blend_ms = sum(stages[s] for s in blend_stages)
     # Dominant memory-bound kernel: the tile warp (one launch per chain and
     # execute; the seam step above it in the launch list is a sequential
-    # dynamic program, not bandwidth-bound).  Traffic per step = the
-    # ncu-measured DRAM/algorithmic ratio of profiles/k_warp_tiles_traffic.json
-    # times this workload's algorithmic bytes.
+    # dynamic program, not bandwidth-bound).  Traffic per step: the ncu DRAM
+    # bytes of a smaller capture (profiles/k_warp_tiles_traffic.json), read
+    # bytes scaled by covered item pixels and written bytes by item pixels.
     dom = "warp_gain_coverage"
     ach = sb[dom] / (stages[dom] / 1e3) / 1e9
     traffic = None
     tp = os.path.join(ROOT, "profiles", "k_warp_tiles_traffic.json")
     if os.path.exists(tp):
         with open(tp) as f:
-            traffic = int(json.load(f)["dram_bytes_per_algorithmic_byte"] * sb[dom])
+            tj = json.load(f)
+        item_px = sum(t[2] * t[3] * len(t[4]) for t in S["pano"].tiles)
+        traffic = int(tj["read_bytes_per_covered_item_px"] * stats["coveredItemPixels"] +
+                      tj["write_bytes_per_item_px"] * item_px)
     roof = {"kernel": "k_warp_tiles (" + dom + ")", "bound": "hbm", "achieved": round(ach, 1), "peak": peaks["hbm_gbs"],
             "unit": "GB/s", "frac": round(ach / peaks["hbm_gbs"], 4), "traffic": traffic,
             "algorithmic_bytes": sb[dom], "ms": round(stages[dom], 3),
@@ -322,7 +327,8 @@ def run_ours(args, rank, world, local_rank):
                    "item_pixels": sum(t[2] * t[3] * len(t[4]) for t in S["pano"].tiles),
                    "covered_item_pixels": stats["coveredItemPixels"],
                    "output_mpix": round(out_px / 1e6, 2), "coords": "reference (bit-exact vs CPU backend)",
-                   "l2": "inputs and outputs larger than L2 (no flush)", "blend": "plain (learned blend not built)",
+                   "l2": "inputs and outputs larger than L2 (no flush)",
+                   "blend": "plain seam blend (--no-learned: learned blend not measured in this run)",
                    "parallelism": f"{world} independent panoramas",
                    "schedule": "steps back to back: step k+1's demosaic (own stream) overlaps stages 1-9 of step "
                                "k's render, after its warp stage has read the frames",
@@ -618,14 +624,21 @@ def cpu_demosaic_all(impl, kind, cfa_host, cfg, threads):
     return outs
 
 
-def cpu_sample(impl, kind, frames_host, pano, cfg, threads, n_tiles, n_frames_dem, cfa_host, gains):
-    """Times a bounded sample of the job on host cores; returns extrapolated
-    job seconds and a description."""
+def cpu_sample(impl, kind, frames_host, pano, cfg, threads, n_tiles, cfa_host, gains, seed=7):
+    """One bounded sample of the job on the host cores, timed as it runs (no
+    extrapolation): the demosaic of the frames in proportion to the sampled
+    tiles (frames / tiles of the panorama), then n_tiles tiles chosen with
+    `seed`, rendered as the reference's CPU backend does (one chunk task per
+    worker thread: warp + gain of every contributor, seam blend).  Returns
+    (output pixels of the sampled tiles, seconds, description)."""
     from image360_b200 import synth
     black, cm, rc, filt = synth.demosaic_params(cfg)
-    rng = np.random.default_rng(7)
-    # demosaic sample: n frames on `threads` workers
-    idx = list(range(min(n_frames_dem, len(cfa_host))))
+    rng = np.random.default_rng(seed)
+    n_dem = max(1, int(round(len(cfa_host) * n_tiles / len(pano.tiles))))
+    idx = [int(i) for i in rng.permutation(len(cfa_host))[:n_dem]]
+    order = rng.permutation(len(pano.tiles))[:n_tiles]
+    sample = [pano.tiles[i] for i in order]
+    inv = np.stack([synth.inverse_homography_f32(H) for H in pano.to_canvas])
     t0 = time.time()
     if kind == "reference":
         import ctypes as ct
@@ -640,36 +653,29 @@ def cpu_sample(impl, kind, frames_host, pano, cfg, threads, n_tiles, n_frames_de
         for i in idx:
             impl.demosaic(cfa_host[i], black, cm, rc, filt)
     t_dem = time.time() - t0
-    dem_job = t_dem * len(cfa_host) / len(idx) if kind == "reference" else t_dem * len(cfa_host) / len(idx) / 1.0
-    # render sample: tiles chosen with a fixed seed
-    order = rng.permutation(len(pano.tiles))[:n_tiles]
-    sample = [pano.tiles[i] for i in order]
-    inv = np.stack([synth.inverse_homography_f32(H) for H in pano.to_canvas])
-    if kind == "reference":
-        secs, _ = impl.render_tiles(threads, frames_host, inv, gains, sample, cfg.bands, want_out=False)
-    else:
-        secs, _ = impl.render_tiles(threads, frames_host, inv, gains, sample, cfg.bands, want_out=False)
-    work = lambda ts: sum(t[2] * t[3] * max(1, len(t[4])) for t in ts)
-    render_job = secs * work(pano.tiles) / work(sample)
-    return dem_job + render_job, t_dem + secs, (f"{len(idx)} frames demosaiced + {len(sample)} of {len(pano.tiles)} "
-                                               f"tiles rendered on {threads} threads, extrapolated by frames and "
-                                               f"by tile area x contributors")
+    secs, _ = impl.render_tiles(threads, frames_host, inv, gains, sample, cfg.bands, want_out=False)
+    px = sum(t[2] * t[3] for t in sample)
+    return px, t_dem + secs, (f"{len(idx)} of {len(cfa_host)} frames demosaiced + {len(sample)} of {len(pano.tiles)} "
+                              f"tiles rendered on {threads} threads (frames in proportion to the tiles), timed as run")
+
+
+def _cpu_threads():
+    """hardware_concurrency()-1 worker threads: the reference's CPU-backend
+    task window (ComputeBackendFactory.cpp:99-100)."""
+    return max(1, (os.cpu_count() or 2) - 1)
 
 
 def cpu_baseline(S, args):
-    import torch
     impl, kind = _cpu_impl()
-    threads = max(1, (os.cpu_count() or 2) - 1)
+    threads = _cpu_threads()
     cfg, pano = S["cfg"], S["pano"]
     frames_host = [r.cpu().numpy().view(np.uint16) for r in S["rgb"]]
     cfa_host = [c.cpu().numpy().view(np.uint16) for c in S["cfa"]]
     gains = (1.0 / pano.gains).astype(np.float32)
     n_tiles = max(threads, args.cpu_tiles)
-    job_s, spent, desc = cpu_sample(impl, kind, frames_host, pano, cfg, threads, n_tiles, max(2, threads // 2),
-                                    cfa_host, gains)
-    out_px = sum(t[2] * t[3] for t in pano.tiles)
-    return {"value": round(out_px / 1e6 / job_s, 3), "unit": UNIT, "cores": threads, "kind": kind,
-            "sample": desc, "sample_seconds": round(spent, 1), "threads_model": "hardware_concurrency()-1 tasks"}
+    px, secs, desc = cpu_sample(impl, kind, frames_host, pano, cfg, threads, n_tiles, cfa_host, gains)
+    return {"value": round(px / 1e6 / secs, 3), "unit": UNIT, "cores": threads, "kind": kind,
+            "sample": desc, "sample_seconds": round(secs, 1), "threads_model": "hardware_concurrency()-1 tasks"}
 
 
 def run_export(args, S, stream):
@@ -795,43 +801,43 @@ def cpu_color_baseline(S, n, w, h):
 
 def run_reference(args, rank, world):
     """The reference's own CPU implementation of the path on this host's
-    cores, on the same workload, bounded per step; rank 0 only."""
+    cores, on the same workload; rank 0 only.  Each step is one bounded
+    sample of the job (a proportional share of the frames demosaiced and
+    `--cpu-tiles` tiles rendered, a new seeded choice every step), timed as
+    it runs: value = the sampled tiles' output pixels / the steps' seconds."""
     if rank != 0:
         return None
     from image360_b200 import synth
     impl, kind = _cpu_impl()
-    threads = os.cpu_count() or 1
+    threads = _cpu_threads()
     cfg = synth.C1 if args.scale == 1.0 else synth.scaled(synth.C1, args.scale, tile=synth.C1.tile)
-    device = "cpu"
-    try:
-        import torch
-        if torch.cuda.is_available():
-            device = "cuda:0"  # synthetic input generation only; timed work is on the CPU
-    except Exception:
-        pass
-    pano = synth.make_panorama(cfg, device=device)
-    cfa_host = [c.cpu().numpy().view(np.uint16) for c in pano.cfa]
-    black, cm, rc, filt = synth.demosaic_params(cfg)
+    pano = synth.make_panorama(cfg, device="cpu")
+    cfa_host = [c.numpy().view(np.uint16) for c in pano.cfa]
     gains = (1.0 / pano.gains).astype(np.float32)
-    # every frame demosaiced once by the CPU code itself (untimed setup);
-    # the timed steps re-demosaic a sample of frames and render a sample of tiles
+    # every frame demosaiced once by the CPU code itself (untimed setup: the
+    # render of a sampled tile needs all of its contributors)
     frames_host = cpu_demosaic_all(impl, kind, cfa_host, cfg, threads)
-    times = []
+    n_tiles = max(1, min(args.cpu_tiles, len(pano.tiles)))
+    px_tot = secs_tot = 0.0
+    desc = ""
+    t_wall = time.time()
     for s in range(args.warmup + args.steps):
-        job_s, spent, desc = cpu_sample(impl, kind, frames_host, pano, cfg, threads, max(threads, args.cpu_tiles),
-                                        max(2, threads // 2), cfa_host, gains)
+        if s == args.warmup:
+            t_wall = time.time()
+        px, secs, desc = cpu_sample(impl, kind, frames_host, pano, cfg, threads, n_tiles, cfa_host, gains, seed=100 + s)
         if s >= args.warmup:
-            times.append(job_s)
-    out_px = sum(t[2] * t[3] for t in pano.tiles)
-    job = float(np.mean(times))
-    value = out_px / 1e6 / job
+            px_tot += px
+            secs_tot += secs
+    wall = time.time() - t_wall
+    value = px_tot / 1e6 / secs_tot
     return {"metric": METRIC, "value": round(value, 3), "unit": UNIT, "n_gpus": world, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": round(job * 1e3, 1), "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "u16 storage / fp32 arithmetic", "data": "synthetic (seeded scene, 14-bit RGGB)",
-            "impl": "reference",
+            "warmup": args.warmup, "ms_per_step": round(secs_tot / args.steps * 1e3, 1), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "u16 storage / fp32 arithmetic",
+            "data": "synthetic (seeded scene, 14-bit RGGB)", "impl": "reference",
             "config": {"workload": f"plain seam blend, 24 x {cfg.frame_w}x{cfg.frame_h} RGGB -> "
                                    f"{pano.canvas_w}x{pano.canvas_h} in {cfg.tile}^2 tiles, {cfg.bands} bands",
-                       "parallelism": f"{threads} host threads"},
+                       "step": f"one sample per step: {desc}", "parallelism": f"{threads} host threads",
+                       "timed_wall_seconds": round(wall, 1)},
             "cpu_baseline": {"value": round(value, 3), "unit": UNIT, "cores": threads, "kind": kind, "sample": desc},
             "e2e": {"value": round(value, 3), "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
 
@@ -843,7 +849,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--scale", type=float, default=1.0, help="geometry scale of the workload (1.0 = full size)")
-    ap.add_argument("--cpu-tiles", type=int, default=45, help="tiles in the CPU-baseline sample")
+    ap.add_argument("--cpu-tiles", type=int, default=15, help="tiles per CPU sample (one per host thread)")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-learned", action="store_true", help="skip the learned blend")

@@ -129,6 +129,8 @@ def load_library(path: str = LIB_PATH):
     L.i360b_launch_cull_tiles.argtypes = [vp, vp, vp, i, vp, i, i, vp, vp, vp, i, vp, vp]
     L.i360b_launch_blend.argtypes = [ct.POINTER(vp), i, i, i, i, vp, vp]
     L.i360b_launch_blend_noalloc.argtypes = [ct.POINTER(vp), i, i, i, i, vp, vp]
+    L.i360b_render_plan_set_wait_limit.argtypes = [vp, ct.c_longlong, vp]
+    L.i360b_debug_inject_failure.argtypes = [i, i]
     _lib = L
     return L
 
@@ -347,6 +349,17 @@ class B200ComputeBackend:
                                                          stream or None))
 
 
+INJECT_ALLOC = 1
+INJECT_LAUNCH = 2
+
+
+def inject_failure(kind: int, count: int = 1) -> ComputeResult:
+    """i360b_debug_inject_failure: the next `count` device allocations
+    (INJECT_ALLOC) or launch checks (INJECT_LAUNCH) of the library fail on the
+    host; count 0 disarms."""
+    return ComputeResult(load_library().i360b_debug_inject_failure(int(kind), int(count)))
+
+
 def launch_blend_noalloc(d_warped, width: int, height: int, d_out: int, num_bands: int = 5,
                          stream: int = 0) -> ComputeResult:
     """i360b_launch_blend_noalloc: the device blend with no device allocation
@@ -533,6 +546,10 @@ class RenderPlan:
 
     def wait(self, stream: int = 0) -> ComputeResult:
         return ComputeResult(self.lib.i360b_render_plan_wait(self._h, stream or None))
+
+    def set_wait_limit(self, cycles: int, stream: int = 0) -> ComputeResult:
+        """Bounded-wait limit of the plan's kernels in SM cycles (-1: default)."""
+        return ComputeResult(self.lib.i360b_render_plan_set_wait_limit(self._h, int(cycles), stream or None))
 
     def close(self) -> None:
         if self._h:

@@ -11,7 +11,6 @@ namespace i360b
 namespace
 {
 constexpr unsigned kFull = 0xffffffffu;
-constexpr long long kSpinCycles = 2000000000ll;  // ~1 s at B200 clocks: bounded waits
 
 __device__ __forceinline__ float f_inf() { return __int_as_float(0x7f800000); }
 
@@ -382,9 +381,11 @@ __global__ void __launch_bounds__(32 * kDtWarps, 2) k_dt(BlendArgs a, const int*
                     while ((seen = pr.load(cuda::memory_order_acquire)) < need)
                     {
                         if (++spins > 32) __nanosleep(128);
-                        if ((spins & 63) == 0 && (*(volatile int*)a.error || clock64() - tstart > kSpinCycles))
+                        if (((spins & 63) == 0 || a.spinLimit == 0) &&
+                            (*(volatile int*)a.error || clock64() - tstart > a.spinLimit))
                         {
                             atomicExch(a.error, 1);
+                            atomicExch(a.error + 1, 1);
                             bad = 1;
                             break;
                         }

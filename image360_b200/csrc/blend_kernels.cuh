@@ -66,13 +66,20 @@ struct Unit
     int level;
 };
 
+// Default limit of every bounded device wait, in SM cycles (~1 s at B200
+// clocks).
+constexpr long long kSpinCyclesDefault = 2000000000ll;
+
 struct BlendArgs
 {
     ItemDev* items;
     TileDev* tiles;
-    int* error;                        // set non-zero by a kernel that gave up (bounded waits)
+    // error[0]: set by a kernel that gave up (bounded waits) in this execution;
+    // error[1]: the same, kept across executions until the host reads it.
+    int* error;
     unsigned long long* seamCycles;    // per-phase SM cycles of the seam kernel (5 counters)
     int bandRows;                      // rows per band unit (a multiple of 8; the plan's tuning)
+    long long spinLimit;               // cycles a bounded wait may last (0: give up at the first miss)
 };
 
 // Kernel launchers (blend_kernels.cu).

@@ -50,8 +50,10 @@ int fail(int code, const char* fmt, ...);
 void clear_error();
 // Maps a CUDA error to a result code and records the message.
 int cuda_fail(cudaError_t e, const char* what);
-// Checks for a launch error of the kernel just enqueued.
+// Checks for a launch error of the kernel just enqueued (or an injected one).
 int check_launch(const char* what);
+// True when a test armed a host-side allocation failure (consumes one).
+bool inject_alloc_failure();
 
 bool initialized();
 int device();
@@ -64,6 +66,9 @@ void dev_free(void* p, cudaStream_t s);
 
 // Requires an initialised context (lazy-initialises on first use).
 int ensure_ready();
+// Device address of the allocation-free blend's static scratch array on the
+// current device (noalloc.cu); resolved once per device.
+int noalloc_scratch(void** out);
 
 #define I360B_TRY(expr)             \
     do                              \

@@ -51,10 +51,27 @@ int cuda_fail(cudaError_t e, const char* what)
     return fail(code, "%s: %s", what, cudaGetErrorString(e));
 }
 
+namespace
+{
+// Armed host-side failures (i360b_debug_inject_failure).
+std::atomic<int> g_injectAlloc{0}, g_injectLaunch{0};
+
+bool take_injected(std::atomic<int>& n)
+{
+    int v = n.load();
+    while (v > 0)
+        if (n.compare_exchange_weak(v, v - 1)) return true;
+    return false;
+}
+}  // namespace
+
+bool inject_alloc_failure() { return take_injected(g_injectAlloc); }
+
 int check_launch(const char* what)
 {
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return cuda_fail(e, what);
+    if (take_injected(g_injectLaunch)) return fail(I360B_KERNEL_LAUNCH_FAILED, "%s: launch failed (injected)", what);
     return I360B_SUCCESS;
 }
 
@@ -94,6 +111,11 @@ static int do_initialize()
     I360B_CUDA(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &threshold), "cudaMemPoolSetAttribute");
     I360B_CUDA(cudaDeviceGetAttribute(&g_sms, cudaDevAttrMultiProcessorCount, best), "cudaDeviceGetAttribute");
     g_device = best;
+    // Resolve the allocation-free blend's scratch array now, with the device
+    // current: this loads its module, so the array is reserved here rather
+    // than inside that entry point's first call.
+    void* scratch = nullptr;
+    I360B_TRY(noalloc_scratch(&scratch));
     g_init.store(true);
     return I360B_SUCCESS;
 }
@@ -128,6 +150,8 @@ int dev_alloc(void** p, size_t bytes, cudaStream_t s, const char* what)
 {
     *p = nullptr;
     if (bytes == 0) bytes = 256;
+    if (inject_alloc_failure())
+        return fail(I360B_OUT_OF_MEMORY, "%s: device allocation of %zu bytes failed (injected)", what, bytes);
     cudaError_t e = cudaMallocAsync(p, bytes, s);
     if (e != cudaSuccess)
     {
@@ -165,6 +189,16 @@ extern "C" void i360b_shutdown(void)
 }
 
 extern "C" int i360b_is_initialized(void) { return g_init.load() ? 1 : 0; }
+
+extern "C" int i360b_debug_inject_failure(int kind, int count)
+{
+    clear_error();
+    if (count < 0) return fail(I360B_INVALID_PARAM, "count must be >= 0.");
+    if (kind == I360B_INJECT_ALLOC) g_injectAlloc.store(count);
+    else if (kind == I360B_INJECT_LAUNCH) g_injectLaunch.store(count);
+    else return fail(I360B_INVALID_PARAM, "Unknown injection kind %d.", kind);
+    return I360B_SUCCESS;
+}
 
 extern "C" const char* i360b_get_last_error(void) { return t_err; }
 

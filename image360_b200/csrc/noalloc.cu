@@ -13,8 +13,11 @@
 // exceed it is rejected with I360B_INVALID_PARAM before anything is enqueued.
 // All calls share the array and each call overwrites what the previous one
 // left there, so calls whose GPU work overlaps (two threads, or two streams)
-// race; serialise them.  The first call on a device looks up the array's
-// device address with that device current.
+// race; serialise them.  i360b_initialize looks up the array's device
+// address on the device it selects (with that device current), which makes
+// the runtime load this file's module - and so reserve the 12 MiB - at
+// initialisation, not on the first call; a call on a device that was not set
+// up that way looks it up then.
 #include "common.cuh"
 
 #include <mutex>
@@ -31,6 +34,8 @@ __device__ __align__(256) unsigned char g_noallocScratch[kNoAllocScratchBytes];
 constexpr int kMaxDevices = 64;
 std::mutex g_noallocMu;
 void* g_noallocPtr[kMaxDevices] = {};
+
+}  // namespace
 
 // Device address of the scratch array on the current device (host code only
 // sees a stand-in for the symbol, never its device address).
@@ -50,7 +55,6 @@ int noalloc_scratch(void** out)
     *out = g_noallocPtr[dev];
     return I360B_SUCCESS;
 }
-}  // namespace
 }  // namespace i360b
 
 using namespace i360b;

@@ -291,6 +291,8 @@ int Plan::build(const std::vector<TileSpec>& specs, int numBands, bool renderPat
     }
     else
     {
+        if (inject_alloc_failure())
+            return fail(I360B_OUT_OF_MEMORY, "render plan: device allocation of %zu bytes failed (injected)", bytes);
         cudaError_t e = cudaMalloc(&arena, bytes);
         if (e != cudaSuccess)
         {
@@ -347,7 +349,7 @@ int Plan::build(const std::vector<TileSpec>& specs, int numBands, bool renderPat
         if (nTiles)
             I360B_CUDA(cudaMemcpyAsync(dTiles, tiles.data(), nTiles * sizeof(TileDev), cudaMemcpyHostToDevice, stream),
                        "plan upload");
-        I360B_CUDA(cudaMemsetAsync(dError, 0, sizeof(int), stream), "plan upload");
+        I360B_CUDA(cudaMemsetAsync(dError, 0, 2 * sizeof(int), stream), "plan upload");
         I360B_CUDA(cudaMemsetAsync(dSeamCycles, 0, 5 * sizeof(unsigned long long), stream), "plan upload");
         I360B_CUDA(cudaStreamSynchronize(stream), "plan upload");
     }
@@ -357,7 +359,7 @@ int Plan::build(const std::vector<TileSpec>& specs, int numBands, bool renderPat
         I360B_CUDA(cudaMemcpy(dInts, ints.data(), ints.size() * sizeof(int), cudaMemcpyHostToDevice), "plan upload");
         if (nItems) I360B_CUDA(cudaMemcpy(dItems, items.data(), nItems * sizeof(ItemDev), cudaMemcpyHostToDevice), "plan upload");
         if (nTiles) I360B_CUDA(cudaMemcpy(dTiles, tiles.data(), nTiles * sizeof(TileDev), cudaMemcpyHostToDevice), "plan upload");
-        I360B_CUDA(cudaMemset(dError, 0, sizeof(int)), "plan upload");
+        I360B_CUDA(cudaMemset(dError, 0, 2 * sizeof(int)), "plan upload");
         I360B_CUDA(cudaMemset(dSeamCycles, 0, 5 * sizeof(unsigned long long)), "plan upload");
     }
     seamList = dInts + seamStart;
@@ -441,12 +443,25 @@ int Plan::set_tuning(int rows, int slots, cudaStream_t s)
     I360B_CUDA(cudaStreamSynchronize(s), "plan tuning");
     bandRows = rows;
     dtSlots = slots;
+    drop_graphs();
+    return I360B_SUCCESS;
+}
+
+void Plan::drop_graphs()
+{
     for (auto& g : rangeGraphs) cudaGraphExecDestroy(g.second);
     rangeGraphs.clear();
     if (graphExec) cudaGraphExecDestroy(graphExec);
     if (graph) cudaGraphDestroy(graph);
     graphExec = nullptr;
     graph = nullptr;
+}
+
+int Plan::set_wait_limit(long long cycles, cudaStream_t s)
+{
+    I360B_CUDA(cudaStreamSynchronize(s), "plan wait limit");
+    spinLimit = cycles < 0 ? kSpinCyclesDefault : cycles;
+    drop_graphs();
     return I360B_SUCCESS;
 }
 
@@ -492,7 +507,7 @@ int Plan::enqueue_warp(cudaStream_t s)
 
 int Plan::enqueue_chain(int c, int first, int last, cudaStream_t s)
 {
-    BlendArgs a{dItems, dTiles, dError, dSeamCycles, bandRows};
+    BlendArgs a{dItems, dTiles, dError, dSeamCycles, bandRows, spinLimit};
     const Range* L = &lists[(size_t)c * kListsPerChain];
     for (int stage = first; stage <= last; ++stage)
     {
@@ -654,10 +669,18 @@ int Plan::execute_range(cudaStream_t s, int first, int last)
 
 int Plan::check(cudaStream_t s)
 {
-    if (!hostErr) I360B_CUDA(cudaMallocHost(&hostErr, sizeof(int)), "pinned flag");
-    I360B_CUDA(cudaMemcpyAsync(hostErr, dError, sizeof(int), cudaMemcpyDeviceToHost, s), "error flag readback");
+    if (!hostErr) I360B_CUDA(cudaMallocHost(&hostErr, 2 * sizeof(int)), "pinned flag");
+    I360B_CUDA(cudaMemcpyAsync(hostErr, dError, 2 * sizeof(int), cudaMemcpyDeviceToHost, s), "error flag readback");
     I360B_CUDA(cudaStreamSynchronize(s), "render synchronize");
-    if (*hostErr) return fail(I360B_KERNEL_LAUNCH_FAILED, "A render kernel gave up waiting (bounded spin); output invalid.");
+    // error[1] holds a give-up of any execution since the last check (each
+    // execution clears error[0] when it starts), so a failed run is reported
+    // even when later runs of the same plan succeeded.
+    if (hostErr[0] || hostErr[1])
+    {
+        I360B_CUDA(cudaMemsetAsync(dError + 1, 0, sizeof(int), s), "error flag reset");
+        I360B_CUDA(cudaStreamSynchronize(s), "error flag reset");
+        return fail(I360B_KERNEL_LAUNCH_FAILED, "A render kernel gave up waiting (bounded spin); output invalid.");
+    }
     return I360B_SUCCESS;
 }
 
@@ -744,7 +767,7 @@ int launch_blend_chunk_in(void* arena, size_t arenaBytes, const unsigned short* 
     I360B_TRY(p.enqueue(s));
     // Status of the bounded waits, read without a pinned staging buffer.
     int flag = 0;
-    I360B_CUDA(cudaMemcpyAsync(&flag, p.dError, sizeof(int), cudaMemcpyDeviceToHost, s), "error flag readback");
+    I360B_CUDA(cudaMemcpyAsync(&flag, p.dError + 1, sizeof(int), cudaMemcpyDeviceToHost, s), "error flag readback");
     I360B_CUDA(cudaStreamSynchronize(s), "blend synchronize");
     if (flag) return fail(I360B_KERNEL_LAUNCH_FAILED, "A blend kernel gave up waiting (bounded spin); output invalid.");
     return I360B_SUCCESS;
@@ -992,6 +1015,14 @@ extern "C" int i360b_render_plan_autotune(i360b_render_plan* plan, void* stream,
     if (dtSlots) *dtSlots = bestS;
     if (bestMs) *bestMs = best / 2.0f;
     return I360B_SUCCESS;
+}
+
+extern "C" int i360b_render_plan_set_wait_limit(i360b_render_plan* plan, long long cycles, void* stream)
+{
+    clear_error();
+    if (!plan) return fail(I360B_INVALID_PARAM, "Null plan.");
+    I360B_TRY(ensure_ready());
+    return plan->plan.set_wait_limit(cycles, static_cast<cudaStream_t>(stream));
 }
 
 extern "C" size_t i360b_render_plan_scratch_bytes(const i360b_render_plan* plan)

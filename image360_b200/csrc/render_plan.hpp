@@ -59,6 +59,9 @@ struct Plan
     // Tuning: rows per band unit of the per-pixel kernels (8, 16, 32 or 64)
     // and ring slots of the chamfer transform (0 = as many as fit).
     int bandRows = kBandRows, dtSlots = 0;
+    // Limit of the bounded device waits (SM cycles; 0 = give up at the first
+    // wait that is not satisfied at once, a test setting).
+    long long spinLimit = kSpinCyclesDefault;
     int unitCap = 0;  // units the device list holds (sized for 8-row bands)
     std::vector<ItemDev> items;
     std::vector<TileDev> tiles;
@@ -121,8 +124,12 @@ struct Plan
     // Switches the band height and chamfer ring depth; the next execute
     // recaptures the graph.  Synchronous on `s`.
     int set_tuning(int rows, int slots, cudaStream_t s);
+    // Changes the bounded-wait limit; the next execute recaptures the graph.
+    int set_wait_limit(long long cycles, cudaStream_t s);
+    void drop_graphs();
     int execute(cudaStream_t s, bool useGraph);
-    // Waits for the stream and reports a kernel that gave up (bounded waits).
+    // Waits for the stream and reports a kernel that gave up (bounded waits)
+    // in any execution since the previous check.
     int check(cudaStream_t s);
 };
 }  // namespace i360b

@@ -192,8 +192,9 @@ I360B_API int i360b_launch_blend(const unsigned short* const* dWarped, int numCo
  * 256x256 with 8 contributors fits - returns I360B_INVALID_PARAM.  The caller
  * passes device inputs and output as for i360b_launch_blend.  Synchronous: it
  * waits for `stream` before returning.  Every call reuses the same array, so
- * calls whose GPU work overlaps race; serialise them.  The first call on each
- * device looks up the array's device address. */
+ * calls whose GPU work overlaps race; serialise them.  i360b_initialize
+ * reserves the array on the device it selects and looks up its device
+ * address, so the entry point itself never touches the allocator. */
 I360B_API int i360b_launch_blend_noalloc(const unsigned short* const* dWarped, int numContributors, int width,
                                          int height, int numBands, unsigned short* dOut, void* stream);
 
@@ -413,6 +414,30 @@ I360B_API int i360b_render_plan_write_tiff16(i360b_render_plan* plan, const char
  * i360b_render_plan_execute; a caller that refills the frame buffers for the
  * next render may do so as soon as stage 0 has completed. */
 I360B_API int i360b_render_plan_execute_stages(i360b_render_plan* plan, int firstStage, int lastStage, void* stream);
+
+/* Sets how long each bounded device wait of the plan's kernels may last, in
+ * SM cycles (default about one second; a negative value restores it).  A
+ * kernel whose wait runs out sets the plan's error flag and returns, and
+ * i360b_render_plan_wait then reports I360B_KERNEL_LAUNCH_FAILED.  0 makes
+ * every wait that is not satisfied at once give up, which tests use to
+ * exercise that path without faulting the GPU.  No reference counterpart:
+ * the reference's kernels have no inter-block waits.  Synchronous on
+ * `stream`; the next execute recaptures the plan's graph. */
+I360B_API int i360b_render_plan_set_wait_limit(i360b_render_plan* plan, long long cycles, void* stream);
+
+/* Host-side failure injection for tests (StubTaskExecutor.h:27-56 injects at
+ * task level; this injects at the device-call level).  kind
+ * I360B_INJECT_ALLOC makes the next `count` device allocations of the library
+ * fail as out of memory (I360B_OUT_OF_MEMORY); I360B_INJECT_LAUNCH makes the
+ * next `count` launch checks report a failed launch
+ * (I360B_KERNEL_LAUNCH_FAILED).  Nothing reaches the GPU: the failure is
+ * decided on the host before the call.  count 0 disarms. */
+enum
+{
+    I360B_INJECT_ALLOC = 1,
+    I360B_INJECT_LAUNCH = 2
+};
+I360B_API int i360b_debug_inject_failure(int kind, int count);
 
 /* Device bytes of scratch the plan holds. */
 I360B_API size_t i360b_render_plan_scratch_bytes(const i360b_render_plan* plan);

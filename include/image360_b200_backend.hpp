@@ -6,7 +6,7 @@
 // Header-only.  Compile it inside the reference project, with
 // WindowsApp.Compute/HeaderFiles on the include path, and link
 // libimage360_b200.so.  ComputeBackendFactory then selects it like the other
-// backends (see INTEGRATION.md for the factory and CLI lines).
+// backends once a TryB200 branch names it (ComputeBackendFactory.cpp:108-135).
 //
 // Semantics follow the reference backends: Initialize() before use, every
 // operation returns a ComputeResult, GetLastError() describes the last failure

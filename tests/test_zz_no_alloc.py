@@ -58,6 +58,25 @@ def test_noalloc_blend_matches_allocating_blend_on_consecutive_calls(backend):
         assert torch.equal(ref, got), (seed, w, h, k)
 
 
+def test_noalloc_blend_allocates_nothing(backend):
+    """The defining property: once the library is initialised, a call changes
+    neither the device's free memory nor what torch's allocator holds (the
+    scratch array was reserved when the library was initialised)."""
+    import torch
+    w, h, k, bands = 192, 160, 4, 5
+    d_in = _device(_buffers(21, w, h, k))
+    ptrs = [t.data_ptr() for t in d_in]
+    out = torch.zeros((h, w, 3), dtype=torch.int16, device="cuda")
+    assert launch_blend_noalloc(ptrs, w, h, out.data_ptr(), bands) == ComputeResult.SUCCESS
+    torch.cuda.synchronize()
+    free0, alloc0 = torch.cuda.mem_get_info()[0], torch.cuda.memory_allocated()
+    for _ in range(3):
+        assert launch_blend_noalloc(ptrs, w, h, out.data_ptr(), bands) == ComputeResult.SUCCESS
+    torch.cuda.synchronize()
+    assert torch.cuda.mem_get_info()[0] == free0
+    assert torch.cuda.memory_allocated() == alloc0
+
+
 def test_noalloc_blend_rejects_chunks_beyond_its_scratch(backend):
     import torch
     w = h = 1024
