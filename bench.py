@@ -105,13 +105,25 @@ class ClockSampler:
 # ---------------------------------------------------------------------------
 # our arm
 # ---------------------------------------------------------------------------
-def setup_ours(cfg, rank, device):
+def setup_ours(cfg, rank, device, world=1, sharded=False):
+    """The rank's render: with `sharded`, its LPT share of one panorama (only
+    the frames its tiles need, tiles renumbered to them); otherwise a whole
+    panorama of its own seed."""
     import torch
 
-    from image360_b200 import COORDS_REFERENCE, B200ComputeBackend, RenderPlan, synth
+    from image360_b200 import COORDS_REFERENCE, B200ComputeBackend, RenderPlan, shard, synth
     t0 = time.time()
-    cfg = synth.PanoConfig(**{**cfg.__dict__, "seed": cfg.seed + 1000 * rank})
-    pano = synth.make_panorama(cfg, device=device)
+    if sharded:
+        geo = synth.make_panorama(cfg, with_cfa=False)
+        mine, need = shard.shard(geo.tiles, rank, world)
+        full = synth.make_panorama(cfg, device=device, frames=need)
+        pano = synth.Panorama(cfg=cfg, canvas_w=full.canvas_w, canvas_h=full.canvas_h,
+                              to_canvas=full.to_canvas[need], gains=full.gains[need],
+                              cfa=[full.cfa[f] for f in need], tiles=shard.local_view(geo.tiles, mine, need))
+        del full
+    else:
+        cfg = synth.PanoConfig(**{**cfg.__dict__, "seed": cfg.seed + 1000 * rank})
+        pano = synth.make_panorama(cfg, device=device)
     torch.cuda.synchronize()
     log(f"[rank {rank}] synthetic panorama {pano.canvas_w}x{pano.canvas_h}, {len(pano.cfa)} frames, "
         f"{len(pano.tiles)} tiles in {time.time() - t0:.1f}s")
@@ -181,28 +193,44 @@ def _levels(w, h, bands):
     return dims
 
 
-def stage_bytes(stats, S):
+def _sum_over_ranks(v, world, device):
+    """Sum of a per-rank count over the ranks (control plane, outside the
+    timed regions)."""
+    if world == 1:
+        return v
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([float(v)], device=device, dtype=torch.float64)
+    dist.all_reduce(t)
+    return int(t.item())
+
+
+def stage_bytes(stats, S, fused_levels=2):
     """Algorithmic bytes per stage: the bytes each stage must move over the
     workload's tiles and contributors (item pixels, covered pixels, pyramid
-    levels), counted over every item pixel."""
+    levels), counted over every item pixel.  With the fused pyramid
+    (fused_levels 2) the base stage reads level 0 and writes level 2, the
+    materialised stages start at level 2, and the fine stage reads the
+    owners' pixels and writes the output."""
     cfg = S["cfg"]
     npx_in = len(S["cfa"]) * cfg.frame_w * cfg.frame_h
     cov = stats["coveredItemPixels"]
     out = stats["outputPixels"]
     tiles = S["pano"].tiles
     item_px = sum(t[2] * t[3] * len(t[4]) for t in tiles)
-    down0 = down = bands_b = collapse = 0
+    lo = 2 if fused_levels == 2 else 1
+    base = down = bands_b = collapse = 0
     for (_, _, w, h, cs) in tiles:
         d = _levels(w, h, cfg.bands)
         n = [a * b for a, b in d]
         k = len(cs)
-        if len(n) > 1:
-            down0 += k * (7 * n[0] + 20 * n[1])
-        for l in range(1, len(n) - 1):
+        if len(n) > lo:
+            base += k * (7 * n[0] + 20 * n[lo])
+        for l in range(lo, len(n) - 1):
             down += k * 20 * (n[l] + n[l + 1])
-        for l in range(1, len(n)):
+        for l in range(lo, len(n)):
             bands_b += (k * 20 + 12) * n[l]
-        for l in range(1, len(n) - 1):
+        for l in range(lo, len(n) - 1):
             collapse += 24 * n[l]
     return {
         "demosaic": npx_in * (2 + 6),
@@ -212,11 +240,11 @@ def stage_bytes(stats, S):
         "chamfer_forward": item_px // 8 + item_px * 4,
         "chamfer_backward": item_px * 8,
         "ownership": item_px * 4 + out,
-        "pyramid_down0": down0,
+        "pyramid_base": base,
         "pyramid_down": down,
         "blend_bands": bands_b,
         "collapse": collapse,
-        "level0_output": out * 13,
+        "fine_output": out * 13,
         "blend_total": cov * 6 + out * 6,
     }
 
@@ -229,10 +257,14 @@ def run_ours(args, rank, world, local_rank):
     device = f"cuda:{local_rank}"
     torch.cuda.set_device(local_rank)
     cfg = synth.C1 if args.scale == 1.0 else synth.scaled(synth.C1, args.scale, tile=synth.C1.tile)
+    sharded = world > 1 and args.mode == "sharded"
+    if sharded:
+        # one panorama of 8 frame columns per rank, its tiles split by LPT
+        cfg = synth.PanoConfig(**{**cfg.__dict__, "cols": cfg.cols * world})
     net = untrained = train_info = None
-    if not args.no_learned:
+    if not args.no_learned and world == 1:
         net, untrained, train_info = prepare_network(args, cfg, rank)
-    S = setup_ours(cfg, rank, device)
+    S = setup_ours(cfg, rank, device, world, sharded)
     stream = torch.cuda.Stream(device=device)
     sp = stream.cuda_stream
     step = make_step(S, sp, overlap=True)
@@ -279,14 +311,23 @@ def run_ours(args, rank, world, local_rank):
         dist.barrier()
     out_px = stats["outputPixels"]
     ms_step = ms / args.steps
-    value = world * out_px / 1e6 / (ms_step / 1e3)
+    px_total = _sum_over_ranks(out_px, world, device)
+    value = px_total / 1e6 / (ms_step / 1e3)
     e2e = run_e2e(args, S, stream, world, device, tuned) if not args.no_e2e else None
+    shard_loads = None
+    if world > 1:
+        mine = {"rank": rank, "tiles": len(S["pano"].tiles), "frames": len(S["pano"].cfa),
+                "output_mpix": round(out_px / 1e6, 2), "ms_per_step": round(ms_step, 3),
+                "tile_cost": sum(t[2] * t[3] * max(1, len(t[4])) for t in S["pano"].tiles)}
+        gathered = [None] * world
+        dist.all_gather_object(gathered, mine)
+        shard_loads = gathered
     if rank != 0:
         return None
     peaks, peak_kind = measured_peaks()
-    sb = stage_bytes(stats, S)
-    blend_stages = ["chamfer_forward", "chamfer_backward", "ownership", "seam_dp", "pyramid_down0", "pyramid_down",
-                    "blend_bands", "collapse", "level0_output"]
+    sb = stage_bytes(stats, S, plan.tuning()["fused_levels"])
+    blend_stages = ["chamfer_forward", "chamfer_backward", "ownership", "seam_dp", "pyramid_base", "pyramid_down",
+                    "blend_bands", "collapse", "fine_output"]
     blend_ms = sum(stages[s] for s in blend_stages)
     # Dominant memory-bound kernel: the tile warp (one launch per chain and
     # execute; the seam step above it in the launch list is a sequential
@@ -329,7 +370,9 @@ def run_ours(args, rank, world, local_rank):
                    "output_mpix": round(out_px / 1e6, 2), "coords": "reference (bit-exact vs CPU backend)",
                    "l2": "inputs and outputs larger than L2 (no flush)",
                    "blend": "plain seam blend (--no-learned: learned blend not measured in this run)",
-                   "parallelism": f"{world} independent panoramas",
+                   "parallelism": (f"{world} ranks, one panorama of {cfg.rows}x{cfg.cols} frames, tiles split by "
+                                   f"LPT on area x contributors, no data-path collective" if sharded else
+                                   f"{world} independent panoramas" if world > 1 else "1 GPU"),
                    "schedule": "steps back to back: step k+1's demosaic (own stream) overlaps stages 1-9 of step "
                                "k's render, after its warp stage has read the frames",
                    "autotuned": tuned},
@@ -341,6 +384,8 @@ def run_ours(args, rank, world, local_rank):
         "clocks": clk.summary(),
         "e2e": e2e,
     }
+    if shard_loads is not None:
+        line["shards"] = shard_loads
     if net is not None:
         lr = run_learned(args, S, stream, net, untrained, train_info)
         lr["speedup_vs_plain"] = round(lr["value"] / value * world, 3)
@@ -348,13 +393,55 @@ def run_ours(args, rank, world, local_rank):
         line["learned"] = lr
         line["config"]["blend"] = ("plain seam blend (value); learned blend measured in 'learned' "
                                    "(same frames, 256x256 overlap windows, judged per window at 45 dB)")
+    if world > 1:
+        return line  # the secondary legs and the CPU checks run at N = 1 only
     if not args.no_color:
         line["color_correct"] = run_color(args, S, stream)
     if not args.no_export:
         line["export_preview"] = run_export(args, S, stream)
+    if not args.no_uneven:
+        line["uneven_tiles"] = run_uneven(args, S, stream)
+    if not args.no_stack:
+        line["median_stack"] = run_stack(args, device, stream)
     if not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(S, args)
+    if not args.no_parity:
+        line["parity"] = parity_check(S, sp)
     return line
+
+
+def parity_check(S, sp):
+    """Every tile of the benchmarked panorama (the plan's own outputs after
+    the timed steps) against the reference's CPU code run here on the same
+    demosaiced frames: warp + gain + seam blend of each tile as
+    RenderExecutor does it (RenderExecutor.cpp:101-140), scalar tier, on the
+    host threads.  Outside the timed region."""
+    import torch
+
+    from image360_b200 import synth
+    plan, pano, cfg = S["plan"], S["pano"], S["cfg"]
+    with torch.cuda.stream(torch.cuda.ExternalStream(sp)):
+        assert plan.execute(sp) == 0 and plan.wait(sp) == 0
+    torch.cuda.synchronize()
+    impl, kind = _cpu_impl()
+    threads = _cpu_threads()
+    frames = [r.cpu().numpy().view(np.uint16) for r in S["rgb"]]
+    gains = (1.0 / pano.gains).astype(np.float32)
+    inv = np.stack([synth.inverse_homography_f32(H) for H in pano.to_canvas])
+    t0 = time.time()
+    if kind == "reference":
+        _, ref = impl.render_tiles(threads, frames, inv, gains, pano.tiles, cfg.bands, tier=0)
+    else:
+        _, ref = impl.render_tiles(threads, frames, inv, gains, pano.tiles, cfg.bands)
+    secs = time.time() - t0
+    bad, worst = 0, 0
+    for o, r in zip(S["outs"], ref):
+        got = o.cpu().numpy().view(np.uint16)
+        if not np.array_equal(got, r):
+            bad += 1
+            worst = max(worst, int(np.abs(got.astype(np.int32) - r.astype(np.int32)).max()))
+    return {"checked": f"all {len(ref)} tiles vs the reference's CPU code ({kind}, scalar tier) on the same frames",
+            "exact": bad == 0, "tiles_differing": bad, "max_abs_diff": worst, "cpu_seconds": round(secs, 1)}
 
 
 def prepare_network(args, cfg, rank):
@@ -556,7 +643,8 @@ def run_e2e(args, S, stream, world, device, tuned=None):
         dist.all_reduce(tt, op=dist.ReduceOp.MAX)
         ms = float(tt.item())
     serial = run_e2e_serial(args, S, stream, world, device, host_cfa, host_out)
-    return {"value": round(world * px / 1e6 / (ms / 1e3), 2), "unit": UNIT, "h2d_bytes_per_step": h2d,
+    px_total = _sum_over_ranks(px, world, device)
+    return {"value": round(px_total / 1e6 / (ms / 1e3), 2), "unit": UNIT, "h2d_bytes_per_step": h2d,
             "d2h_bytes_per_step": d2h, "ms_per_step": round(ms, 3), "steps": k,
             "api": "i360b_pipeline_submit/wait, 2 device slots, pinned host buffers", "autotuned": pipe_tuned,
             "clocks": clk.summary(), "serial": serial}
@@ -593,8 +681,8 @@ def run_e2e_serial(args, S, stream, world, device, host_cfa, host_out):
         tt = torch.tensor([ms], device=device, dtype=torch.float64)
         dist.all_reduce(tt, op=dist.ReduceOp.MAX)
         ms = float(tt.item())
-    px = sum(o.shape[0] * o.shape[1] for o in S["outs"])
-    return {"value": round(world * px / 1e6 / (ms / 1e3), 2), "unit": UNIT, "ms_per_step": round(ms, 3)}
+    px = _sum_over_ranks(sum(o.shape[0] * o.shape[1] for o in S["outs"]), world, device)
+    return {"value": round(px / 1e6 / (ms / 1e3), 2), "unit": UNIT, "ms_per_step": round(ms, 3)}
 
 
 # ---------------------------------------------------------------------------
@@ -676,6 +764,213 @@ def cpu_baseline(S, args):
     px, secs, desc = cpu_sample(impl, kind, frames_host, pano, cfg, threads, n_tiles, cfa_host, gains)
     return {"value": round(px / 1e6 / secs, 3), "unit": UNIT, "cores": threads, "kind": kind,
             "sample": desc, "sample_seconds": round(secs, 1), "threads_model": "hardware_concurrency()-1 tasks"}
+
+
+def run_uneven(args, S, stream):
+    """The batched uneven-tile workload: 256 output tiles with sides drawn from
+    {512, 768, 1024, 1536, 2048}, each overlapped by 1-7 placements of frames
+    from the step's pool of 24 demosaiced 6000x4000 frames, 6 bands, rendered
+    by one plan (every stage one launch over all tiles, replayed as a CUDA
+    graph) with the autotuned band height, ring depth and level-fusion depth.
+    Timed with CUDA events on the stream; a seeded sample of 16 tiles is
+    checked bit for bit against the reference's CPU code."""
+    import torch
+
+    from image360_b200 import COORDS_REFERENCE, RenderPlan, synth
+    cfg, pano = S["cfg"], S["pano"]
+    sp = stream.cuda_stream
+    n = 256 if args.scale == 1.0 else max(8, int(256 * args.scale))
+    sides = synth.C3_SIDES if args.scale == 1.0 else tuple(max(16, int(v * args.scale)) for v in synth.C3_SIDES)
+    ut = synth.uneven_tiles(n, len(S["rgb"]), cfg.frame_w, cfg.frame_h, cfg.focal, seed=20260711, sides=sides)
+    gains = (1.0 / pano.gains[ut.frame_of]).astype(np.float32)
+    outs = [torch.empty((t[3], t[2], 3), dtype=torch.int16, device=S["rgb"][0].device) for t in ut.tiles]
+    frames = [(S["rgb"][f].data_ptr(), cfg.frame_w, cfg.frame_h, H, float(g))
+              for f, H, g in zip(ut.frame_of, ut.to_canvas, gains)]
+    plan = RenderPlan(frames, [(*t[:5], o.data_ptr()) for t, o in zip(ut.tiles, outs)], 6, COORDS_REFERENCE)
+    with torch.cuda.stream(stream):
+        for _ in range(args.warmup):
+            assert plan.execute(sp) == 0
+        assert plan.wait(sp) == 0
+    tuned = plan.autotune(sp) if not args.no_autotune else plan.tuning()
+    stats = plan.stats(sp)
+    stages = plan.profile(sp)
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
+    with torch.cuda.stream(stream):
+        ev[0].record(stream)
+        for _ in range(args.steps):
+            assert plan.execute(sp) == 0
+        ev[1].record(stream)
+    torch.cuda.synchronize()
+    assert plan.wait(sp) == 0
+    ms = ev[0].elapsed_time(ev[1]) / args.steps
+    px = stats["outputPixels"]
+    peaks, kind = measured_peaks()
+    blend_ms = sum(v for k, v in stages.items() if k != "warp_gain_coverage")
+    blend_bytes = stats["coveredItemPixels"] * 6 + px * 6
+    res = {"value": round(px / 1e6 / (ms / 1e3), 1), "unit": "output Mpix/s", "ms_per_step": round(ms, 3),
+           "steps": args.steps, "tiles": len(ut.tiles), "tile_contributors": stats["numItems"],
+           "output_mpix": round(px / 1e6, 1), "covered_item_pixels": stats["coveredItemPixels"],
+           "gpu_launches_per_step": stats["kernelsPerExecute"], "autotuned": tuned,
+           "stages_ms": {k: round(v, 3) for k, v in stages.items()},
+           "blend_roofline": {"achieved": round(blend_bytes / (blend_ms / 1e3) / 1e9, 1), "peak": peaks["hbm_gbs"],
+                              "unit": "GB/s", "frac": round(blend_bytes / (blend_ms / 1e3) / 1e9 / peaks["hbm_gbs"], 4),
+                              "algorithmic_bytes": blend_bytes,
+                              "bytes_formula": "sum of covered item pixels * 6 + output pixels * 6",
+                              "peak_source": kind + " (hbm_gbs, burst copy)"}}
+    if not args.no_parity:
+        impl, ikind = _cpu_impl()
+        rng = np.random.default_rng(5)
+        pick = sorted(int(i) for i in rng.permutation(len(ut.tiles))[:16])
+        host = {f: S["rgb"][f].cpu().numpy().view(np.uint16) for f in sorted(set(int(f) for f in ut.frame_of))}
+        fr = [host[int(f)] for f in ut.frame_of]
+        inv = np.stack([synth.inverse_homography_f32(H) for H in ut.to_canvas])
+        sub = [ut.tiles[i] for i in pick]
+        if ikind == "reference":
+            _, ref = impl.render_tiles(_cpu_threads(), fr, inv, gains, sub, 6, tier=0)
+        else:
+            _, ref = impl.render_tiles(_cpu_threads(), fr, inv, gains, sub, 6)
+        bad = sum(not np.array_equal(outs[i].cpu().numpy().view(np.uint16), r) for i, r in zip(pick, ref))
+        res["parity"] = {"checked": f"{len(pick)} seeded tiles vs the reference's CPU code ({ikind}, scalar tier)",
+                         "exact": bad == 0, "tiles_differing": int(bad)}
+    plan.close()
+    return res
+
+
+def run_stack(args, device, stream):
+    """The median-stack workload: 16 RGGB frames of 4000x3000 (14-bit, one
+    scene, near-identity homographies: translation U(-3, 3) px, rotation
+    +-0.2 degrees, 5% of each frame's pixels under white outlier rectangles).
+    A step demosaics the 16 frames and makes the per-pixel sigma-clipped
+    median of the frames warped onto the reference grid, with the fused
+    warp + median kernel (the warped frames are never written).  Timed with
+    CUDA events; the result is checked outside the timed region against the
+    reference's CPU code on the full stack (demosaic, WarpPerspective of
+    every frame, MedianStack), which is also timed as the CPU baseline."""
+    import torch
+
+    from image360_b200 import synth
+    cfg = synth.C2 if args.scale == 1.0 else synth.scaled_stack(synth.C2, args.scale)
+    t0 = time.time()
+    st = synth.make_stack(cfg, device=device)
+    torch.cuda.synchronize()
+    log(f"burst of {cfg.frames} frames {cfg.frame_w}x{cfg.frame_h} in {time.time() - t0:.1f}s, "
+        f"outliers {np.mean(st.outlier_frac):.3f}")
+    be = _backend()
+    black, cm, rc, filt = synth.demosaic_params(cfg)
+    w, h, n = cfg.frame_w, cfg.frame_h, cfg.frames
+    cfa = [c.view(torch.int16).contiguous() for c in st.cfa]
+    rgb = [torch.empty((h, w, 3), dtype=torch.int16, device=device) for _ in cfa]
+    out = torch.empty((h, w, 3), dtype=torch.int16, device=device)
+    Hs = np.stack([synth.inverse_homography_f32(H) for H in st.to_ref])
+    sp = stream.cuda_stream
+    rptr = [r.data_ptr() for r in rgb]
+
+    def demosaic():
+        for c, r in zip(cfa, rgb):
+            if be.launch_demosaic(c.data_ptr(), w, h, black, cm, rc, filt, r.data_ptr(), sp) != 0:
+                raise RuntimeError(be.get_last_error())
+
+    def median():
+        if be.launch_warp_median(rptr, w, h, Hs, out.data_ptr(), w, h, 0, 0, 2.0, sp) != 0:
+            raise RuntimeError(be.get_last_error())
+
+    ev = []
+    with torch.cuda.stream(stream):
+        for i in range(args.warmup + args.steps):
+            e = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
+            e[0].record(stream)
+            demosaic()
+            e[1].record(stream)
+            median()
+            e[2].record(stream)
+            if i >= args.warmup:
+                ev.append(e)
+    torch.cuda.synchronize()
+    ms_step = float(np.mean([a.elapsed_time(c) for a, _, c in ev]))
+    ms_dem = float(np.mean([a.elapsed_time(b) for a, b, _ in ev]))
+    ms_med = float(np.mean([b.elapsed_time(c) for _, b, c in ev]))
+    npx = w * h
+    med_bytes = npx * 3 * (n * 2 + 2)
+    dem_bytes = n * npx * (2 + 6)
+    peaks, kind = measured_peaks()
+    gbps = med_bytes / (ms_med / 1e3) / 1e9
+    res = {"value": round(npx / 1e6 / (ms_step / 1e3), 1), "unit": "stack output Mpix/s",
+           "ms_per_step": round(ms_step, 3), "steps": args.steps,
+           "workload": f"{n} x {w}x{h} RGGB {cfg.bits}-bit, translation +-{cfg.max_shift} px, rotation "
+                       f"+-{cfg.max_rot_deg} deg, outliers {np.mean(st.outlier_frac):.3f} of pixels; demosaic + "
+                       f"fused warp/median (sigma 2)",
+           "gpu_launches_per_step": n + 1,
+           "stages_ms": {"demosaic": round(ms_dem, 3), "warp_median": round(ms_med, 3)},
+           "demosaic_GBps": round(dem_bytes / (ms_dem / 1e3) / 1e9, 1),
+           "roofline": {"kernel": "k_warp_median", "bound": "hbm", "achieved": round(gbps, 1),
+                        "peak": peaks["hbm_gbs"], "unit": "GB/s", "frac": round(gbps / peaks["hbm_gbs"], 4),
+                        "algorithmic_bytes": med_bytes,
+                        "bytes_formula": "Npx * 3 * (N * 2 + 2): every frame's texels read once, the median written",
+                        "peak_source": kind + " (hbm_gbs, burst copy)"}}
+    if not args.no_cpu_baseline:
+        res["cpu_check"] = cpu_stack_check(st, cfg, Hs, out.cpu().numpy().view(np.uint16))
+    return res
+
+
+def _backend():
+    from image360_b200 import B200ComputeBackend
+    be = B200ComputeBackend()
+    assert be.initialize() == 0, be.get_last_error()
+    return be
+
+
+def cpu_stack_check(st, cfg, Hs, got):
+    """The reference's CPU code on the full stack, in row strips on
+    hardware_concurrency()-1 threads: demosaic of every frame, WarpPerspective
+    of every frame onto the reference grid, MedianStack.  Run with the
+    reference's scalar tier (the algorithm as written, which the GPU
+    reproduces: bit-exact expected) and timed with its run-time tier (what
+    the CPU backend picks on this host; its FMA-contracted statistics may
+    clip a different value set at a few scalars)."""
+    from concurrent.futures import ThreadPoolExecutor
+
+    from image360_b200 import synth
+    impl, kind = _cpu_impl()
+    threads = _cpu_threads()
+    black, cm, rc, filt = synth.demosaic_params(cfg)
+    w, h = cfg.frame_w, cfg.frame_h
+    cfa = [c.cpu().numpy().view(np.uint16) for c in st.cfa]
+    strips = [(y0, min(h, y0 + max(8, h // (4 * threads)))) for y0 in range(0, h, max(8, h // (4 * threads)))]
+
+    def run(tier):
+        kw = {} if tier is None else {"tier": tier}
+        t0 = time.time()
+        with ThreadPoolExecutor(threads) as ex:
+            # whole-frame demosaic tasks (the 3x3 stencil needs neighbouring rows)
+            rgb = list(ex.map(lambda c: impl.demosaic(c, black, cm, rc, filt, **kw), cfa))
+            warped = [np.zeros((h, w, 3), np.uint16) for _ in rgb]
+
+            def warp_strip(args):
+                k, (y0, y1) = args
+                warped[k][y0:y1] = impl.warp(rgb[k], w, y1 - y0, Hs[k], 0, y0, **kw)
+            list(ex.map(warp_strip, [(k, s) for k in range(len(rgb)) for s in strips]))
+            med = np.zeros((h, w, 3), np.uint16)
+
+            def med_strip(s):
+                y0, y1 = s
+                med[y0:y1] = impl.median([wp[y0:y1] for wp in warped], 2.0, **kw)
+            list(ex.map(med_strip, strips))
+        return med, time.time() - t0
+
+    exact_tier = 0 if kind == "reference" else None
+    ref_exact, secs_exact = run(exact_tier)
+    out = {"kind": kind, "cores": threads, "exact_vs_scalar_tier": bool(np.array_equal(got, ref_exact))}
+    if kind == "reference":
+        ref_auto, secs = run(impl.tier)
+        diff = np.abs(got.astype(np.int32) - ref_auto.astype(np.int32))
+        out.update({"auto_tier": int(impl.tier), "values_differing_from_auto_tier": int((diff > 0).sum()),
+                    "max_diff_vs_auto_tier": int(diff.max())})
+    else:
+        secs = secs_exact
+    out.update({"value": round(w * h / 1e6 / secs, 2), "unit": "stack output Mpix/s", "seconds": round(secs, 2),
+                "sample": f"full stack: {len(cfa)} frames demosaiced (one task each), warped and median-stacked in "
+                          f"{len(strips)} row strips per frame on {threads} threads"})
+    return out
 
 
 def run_export(args, S, stream):
@@ -811,6 +1106,8 @@ def run_reference(args, rank, world):
     impl, kind = _cpu_impl()
     threads = _cpu_threads()
     cfg = synth.C1 if args.scale == 1.0 else synth.scaled(synth.C1, args.scale, tile=synth.C1.tile)
+    if world > 1 and args.mode == "sharded":
+        cfg = synth.PanoConfig(**{**cfg.__dict__, "cols": cfg.cols * world})
     pano = synth.make_panorama(cfg, device="cpu")
     cfa_host = [c.numpy().view(np.uint16) for c in pano.cfa]
     gains = (1.0 / pano.gains).astype(np.float32)
@@ -848,6 +1145,9 @@ def main():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--mode", choices=["sharded", "replicas"], default="sharded",
+                    help="N > 1: one panorama of 8N frame columns split over the ranks (sharded), or one "
+                         "panorama per rank (replicas)")
     ap.add_argument("--scale", type=float, default=1.0, help="geometry scale of the workload (1.0 = full size)")
     ap.add_argument("--cpu-tiles", type=int, default=15, help="tiles per CPU sample (one per host thread)")
     ap.add_argument("--no-e2e", action="store_true")
@@ -855,6 +1155,9 @@ def main():
     ap.add_argument("--no-learned", action="store_true", help="skip the learned blend")
     ap.add_argument("--no-color", action="store_true", help="skip the colour-correction leg")
     ap.add_argument("--no-export", action="store_true", help="skip the preview-export leg")
+    ap.add_argument("--no-stack", action="store_true", help="skip the median-stack leg")
+    ap.add_argument("--no-uneven", action="store_true", help="skip the 256 uneven-tile leg")
+    ap.add_argument("--no-parity", action="store_true", help="skip the full-panorama check against the CPU code")
     ap.add_argument("--no-autotune", action="store_true", help="keep the plan's default band height and ring depth")
     ap.add_argument("--train-steps", type=int, default=782, help="Adam steps (782 x 64 = 50k windows)")
     ap.add_argument("--train-batch", type=int, default=64)

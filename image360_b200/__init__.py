@@ -107,6 +107,7 @@ def load_library(path: str = LIB_PATH):
     L.i360b_launch_demosaic.argtypes = [vp, i, i, ct.c_uint16, _f32p, _f32p, ct.c_uint32, vp, vp]
     L.i360b_launch_warp.argtypes = [vp, i, i, vp, i, i, _f32p, i, i, f, vp]
     L.i360b_launch_median.argtypes = [ct.POINTER(vp), i, vp, i, i, f, vp]
+    L.i360b_launch_warp_median.argtypes = [ct.POINTER(vp), i, i, i, _f32p, vp, i, i, i, i, f, vp]
     L.i360b_launch_gain.argtypes = [vp, i, f, vp]
     _i32p, _f64p = ct.POINTER(ct.c_int), ct.POINTER(ct.c_double)
     L.i360b_compute_lab_stats.argtypes = [_u16p, i, i, _f64p, _f64p]
@@ -130,6 +131,8 @@ def load_library(path: str = LIB_PATH):
     L.i360b_launch_blend.argtypes = [ct.POINTER(vp), i, i, i, i, vp, vp]
     L.i360b_launch_blend_noalloc.argtypes = [ct.POINTER(vp), i, i, i, i, vp, vp]
     L.i360b_render_plan_set_wait_limit.argtypes = [vp, ct.c_longlong, vp]
+    L.i360b_render_plan_get_tuning.argtypes = [vp, _i32p, _i32p, _i32p]
+    L.i360b_render_plan_set_tuning.argtypes = [vp, i, i, i, vp]
     L.i360b_debug_inject_failure.argtypes = [i, i]
     _lib = L
     return L
@@ -264,6 +267,17 @@ class B200ComputeBackend:
         arr = (ct.c_void_p * max(1, len(d_inputs)))(*d_inputs)
         return ComputeResult(self.lib.i360b_launch_median(arr, len(d_inputs), d_out, width, height, sigma,
                                                           stream or None))
+
+    def launch_warp_median(self, d_frames, src_w: int, src_h: int, homographies, d_out: int, dst_w: int, dst_h: int,
+                           offset_x: int = 0, offset_y: int = 0, sigma: float = 2.0,
+                           stream: int = 0) -> ComputeResult:
+        """Median stack of the frames warped onto one grid (homographies:
+        (n, 3, 3) or (n, 9) dst->src float32), without writing the warped
+        frames."""
+        arr = (ct.c_void_p * max(1, len(d_frames)))(*d_frames)
+        H = np.ascontiguousarray(homographies, np.float32).reshape(-1)
+        return ComputeResult(self.lib.i360b_launch_warp_median(arr, len(d_frames), src_w, src_h, _pf(H), d_out, dst_w,
+                                                               dst_h, offset_x, offset_y, sigma, stream or None))
 
     def launch_gain(self, d_data: int, n: int, gain: float, stream: int = 0) -> ComputeResult:
         return ComputeResult(self.lib.i360b_launch_gain(d_data, n, gain, stream or None))
@@ -513,13 +527,25 @@ class RenderPlan:
         return {self.lib.i360b_render_stage_name(i).decode(): float(ms[i]) for i in range(10)}
 
     def autotune(self, stream: int = 0) -> dict:
-        """Times every band height / chamfer ring depth on this plan and keeps
-        the fastest: {"band_rows", "dt_slots", "ms"}."""
+        """Times every level-fusion depth / band height / chamfer ring depth
+        on this plan and keeps the fastest: {"band_rows", "dt_slots",
+        "fused_levels", "ms"}."""
         r, k, ms = ct.c_int(), ct.c_int(), ct.c_float()
         rc = self.lib.i360b_render_plan_autotune(self._h, stream or None, ct.byref(r), ct.byref(k), ct.byref(ms))
         if rc != 0:
             raise RuntimeError(self.lib.i360b_get_last_error().decode())
-        return {"band_rows": r.value, "dt_slots": k.value, "ms": ms.value}
+        return {"band_rows": r.value, "dt_slots": k.value, "fused_levels": self.tuning()["fused_levels"],
+                "ms": ms.value}
+
+    def tuning(self) -> dict:
+        r, k, f = ct.c_int(), ct.c_int(), ct.c_int()
+        self.lib.i360b_render_plan_get_tuning(self._h, ct.byref(r), ct.byref(k), ct.byref(f))
+        return {"band_rows": r.value, "dt_slots": k.value, "fused_levels": f.value}
+
+    def set_tuning(self, band_rows: int = 16, dt_slots: int = 0, fused_levels: int = 2,
+                   stream: int = 0) -> ComputeResult:
+        return ComputeResult(self.lib.i360b_render_plan_set_tuning(self._h, int(band_rows), int(dt_slots),
+                                                                   int(fused_levels), stream or None))
 
     def export_preview(self, total_w: int, total_h: int, max_dimension: int, d_out: int, capacity: int,
                        stream: int = 0):

@@ -48,6 +48,8 @@ def _bind():
     L.i360b_blendnet_destroy.restype = None
     L.i360b_blendnet_get_params.argtypes = [vp, ct.POINTER(ct.c_float), i]
     L.i360b_blendnet_set_params.argtypes = [vp, ct.POINTER(ct.c_float), i]
+    L.i360b_blendnet_get_adam.argtypes = [vp, ct.POINTER(ct.c_float), ct.POINTER(ct.c_float), i, ct.POINTER(i)]
+    L.i360b_blendnet_set_adam.argtypes = [vp, ct.POINTER(ct.c_float), ct.POINTER(ct.c_float), i, i]
     L.i360b_blendnet_logits.argtypes = [vp, jp, i, i, i, vp]
     L.i360b_blendnet_gradients.argtypes = [vp, jp, i, i, i, ct.POINTER(ct.c_float), ct.POINTER(ct.c_double)]
     L.i360b_blendnet_train_step.argtypes = [vp, jp, i, i, i, f, ct.POINTER(ct.c_double), vp]
@@ -160,6 +162,31 @@ class BlendNet:
     def set_params(self, p: np.ndarray):
         p = np.ascontiguousarray(p, np.float32)
         _check(self._L.i360b_blendnet_set_params(self._h, p.ctypes.data_as(ct.POINTER(ct.c_float)), p.size))
+
+    def get_adam(self):
+        """(first moments, second moments, step) of the optimiser."""
+        m, v, st = np.zeros(param_count(), np.float32), np.zeros(param_count(), np.float32), ct.c_int()
+        fp = ct.POINTER(ct.c_float)
+        _check(self._L.i360b_blendnet_get_adam(self._h, m.ctypes.data_as(fp), v.ctypes.data_as(fp), m.size,
+                                               ct.byref(st)))
+        return m, v, st.value
+
+    def set_adam(self, m: np.ndarray, v: np.ndarray, step: int):
+        m = np.ascontiguousarray(m, np.float32)
+        v = np.ascontiguousarray(v, np.float32)
+        fp = ct.POINTER(ct.c_float)
+        _check(self._L.i360b_blendnet_set_adam(self._h, m.ctypes.data_as(fp), v.ctypes.data_as(fp), m.size,
+                                               int(step)))
+
+    def save_checkpoint(self, path: str):
+        """Weights and the Adam state (moments and step) in one .npz file."""
+        m, v, st = self.get_adam()
+        np.savez(path, params=self.get_params(), adam_m=m, adam_v=v, adam_step=np.array([st], np.int64))
+
+    def load_checkpoint(self, path: str):
+        with np.load(path) as z:
+            self.set_params(z["params"])
+            self.set_adam(z["adam_m"], z["adam_v"], int(z["adam_step"][0]))
 
     def logits(self, jobs, n: int, w: int, h: int, out):
         _check(self._L.i360b_blendnet_logits(self._h, jobs, n, w, h, _ptr(out)))

@@ -112,7 +112,21 @@ __global__ void __launch_bounds__(256) k_coverage(BlendArgs a, const Unit* __res
 // Tile warp: WarpPerspective + ApplyGain of one contributor into its tile
 // buffer (RenderExecutor.cpp:104-114), coverage and box emitted in the same
 // pass.  Arithmetic identical to k_warp in pixel_ops.cu.
+//
+// A CTA makes a 128x16 block of one contributor's tile.  The source pixels
+// its bilinear taps can reach - the box of the block corners' source
+// positions (the corners of a projective image of a rectangle with w > 0
+// bound it), widened by 2 pixels for the FP32 rounding of the per-pixel
+// positions - are staged in shared memory first: rows read as 16-byte words
+// (8 pixels per three words) and kept as 8-byte pixels (r | g << 16, b), so
+// that a pixel's two horizontal taps are one 16-byte or two 8-byte shared
+// loads.  A tap outside the staged box (never expected) is read from global
+// memory instead, so the result does not depend on the margin.  Lanes take
+// consecutive pixels, so one ballot is one coverage word.
 // ---------------------------------------------------------------------------
+constexpr int kWpW = kWarpBlockW, kWpH = kWarpBlockH;  // destination pixels per CTA
+constexpr int kWpSW = 160, kWpSH = 28; // staged source box (pixels) at most
+
 // The warp parameters of one item, read once per CTA into registers (the
 // item table is in global memory, where the compiler cannot tell it apart
 // from the image being written).
@@ -125,40 +139,52 @@ struct WarpItem
     bool applyGain;
 };
 
-// One destination pixel (WarpPerspectiveKernels.h:16-43 and WarpPerspective_Scalar.cpp:8-45,
-// then ApplyGain, GainColorOps.cpp:16-26).  hy = {H[1] dY, H[4] dY, H[7] dY}
-// for the row: the same rounded products, summed in the reference's order.
-__device__ __forceinline__ void warp_px(const WarpItem& it, float dX, const float* hy, unsigned short o[3])
+// The source position of destination (dX, dY) (WarpPerspective_Scalar.cpp:21-37);
+// hy = {H[1] dY, H[4] dY, H[7] dY} of the row: the same rounded products,
+// summed in the reference's order.  False where the pixel is (0,0,0) by the
+// |w| < 1e-10 or range rule.
+__device__ __forceinline__ bool warp_pos(const WarpItem& it, float dX, const float* hy, int& x0, int& y0, float& fx,
+                                         float& fy)
 {
     const float* H = it.H;
     float sx = fadd(fadd(fmul(H[0], dX), hy[0]), H[2]);
     float sy = fadd(fadd(fmul(H[3], dX), hy[1]), H[5]);
-    float sw1 = fadd(fadd(fmul(H[6], dX), hy[2]), H[8]);
-    o[0] = o[1] = o[2] = 0;
-    if (fabsf(sw1) < 1e-10f) return;
+    const float sw1 = fadd(fadd(fmul(H[6], dX), hy[2]), H[8]);
+    if (fabsf(sw1) < 1e-10f) return false;
     sx = fdiv(sx, sw1);
     sy = fdiv(sy, sw1);
-    if (!(sx >= 0.0f && sx < (float)(it.srcW - 1) && sy >= 0.0f && sy < (float)(it.srcH - 1))) return;
-    int x0 = (int)floorf(sx), y0 = (int)floorf(sy);
-    float fx = fsub(sx, (float)x0), fy = fsub(sy, (float)y0);
-    float gx = fsub(1.0f, fx), gy = fsub(1.0f, fy);
-    float w00 = fmul(gx, gy), w10 = fmul(fx, gy), w01 = fmul(gx, fy), w11 = fmul(fx, fy);
-    const unsigned short* r0 = it.src + ((size_t)y0 * it.srcW + x0) * 3;
-    const unsigned short* r1 = r0 + (size_t)it.srcW * 3;
-    unsigned short a0 = __ldg(r0), a1 = __ldg(r0 + 1), a2 = __ldg(r0 + 2), a3 = __ldg(r0 + 3), a4 = __ldg(r0 + 4),
-                   a5 = __ldg(r0 + 5);
-    unsigned short b0 = __ldg(r1), b1 = __ldg(r1 + 1), b2 = __ldg(r1 + 2), b3 = __ldg(r1 + 3), b4 = __ldg(r1 + 4),
-                   b5 = __ldg(r1 + 5);
-    const unsigned short t00[3] = {a0, a1, a2}, t10[3] = {a3, a4, a5}, t01[3] = {b0, b1, b2}, t11[3] = {b3, b4, b5};
+    if (!(sx >= 0.0f && sx < (float)(it.srcW - 1) && sy >= 0.0f && sy < (float)(it.srcH - 1))) return false;
+    x0 = (int)floorf(sx);
+    y0 = (int)floorf(sy);
+    fx = fsub(sx, (float)x0);
+    fy = fsub(sy, (float)y0);
+    return true;
+}
+
+// Bilinear mix + clamp/truncate + gain of one pixel from its four taps
+// (WarpPerspectiveKernels.h:16-43, GainColorOps.cpp:16-26).
+__device__ __forceinline__ void warp_mix(const WarpItem& it, float fx, float fy, const unsigned short* t00,
+                                         const unsigned short* t10, const unsigned short* t01,
+                                         const unsigned short* t11, unsigned short o[3])
+{
+    const float gx = fsub(1.0f, fx), gy = fsub(1.0f, fy);
+    const float w00 = fmul(gx, gy), w10 = fmul(fx, gy), w01 = fmul(gx, fy), w11 = fmul(fx, fy);
 #pragma unroll
     for (int c = 0; c < 3; ++c)
     {
-        float v = fadd(fadd(fadd(fmul(w00, (float)t00[c]), fmul(w10, (float)t10[c])), fmul(w01, (float)t01[c])),
-                       fmul(w11, (float)t11[c]));
+        const float v = fadd(fadd(fadd(fmul(w00, (float)t00[c]), fmul(w10, (float)t10[c])), fmul(w01, (float)t01[c])),
+                             fmul(w11, (float)t11[c]));
         unsigned short q = clamp_trunc_u16(v);
         if (it.applyGain) q = clamp_trunc_u16(fmul((float)q, it.gain));
         o[c] = q;
     }
+}
+
+__device__ __forceinline__ void px_of(uint2 v, unsigned short* t)
+{
+    t[0] = (unsigned short)(v.x & 0xffffu);
+    t[1] = (unsigned short)(v.x >> 16);
+    t[2] = (unsigned short)(v.y & 0xffffu);
 }
 
 // Zeroes n u16 elements at p (any even address), the warp's lanes together:
@@ -175,8 +201,15 @@ __device__ __forceinline__ void warp_zero_u16(unsigned short* p, int n, int lane
     if (lane < n - t0) p[t0 + lane] = 0;
 }
 
-__global__ void __launch_bounds__(256, 8) k_warp_tiles(BlendArgs a, const Unit* __restrict__ units)
+struct WarpSmem
 {
+    uint2 px[kWpSH][kWpSW];
+    int box[4];   // staged source box: x0 (8-aligned), y0, columns, rows; columns 0 = not staged
+};
+
+__global__ void __launch_bounds__(256) k_warp_tiles(BlendArgs a, const Unit* __restrict__ units)
+{
+    __shared__ __align__(16) WarpSmem S;
     const Unit u = units[blockIdx.x];
     const ItemDev& it = a.items[u.id];
     const TileDev& T = a.tiles[it.tile];
@@ -190,64 +223,161 @@ __global__ void __launch_bounds__(256, 8) k_warp_tiles(BlendArgs a, const Unit* 
     wi.srcH = it.srcH;
     wi.gain = it.gain;
     wi.applyGain = !gain_is_identity(it.gain);
-    const int offX = it.offX, offY = it.offY, vx0 = it.vx0, vx1 = it.vx1, vy0 = it.vy0, vy1 = it.vy1;
-    BoxAcc box;
-    const int rowsPerWarp = a.bandRows >> 3;
-    for (int r = 0; r < rowsPerWarp; ++r)
+    const int offX = it.offX, offY = it.offY;
+    const int X0 = u.bx * kWpW, Y0 = u.by * kWpH;
+    const int X1 = min(X0 + kWpW, W) - 1, Y1 = min(Y0 + kWpH, H) - 1;
+    // the block's part of the footprint box (tile-local; outside it the warp is (0,0,0))
+    const int fx0 = max(it.vx0, X0), fx1 = min(it.vx1, X1), fy0 = max(it.vy0, Y0), fy1 = min(it.vy1, Y1);
+    const bool any = fx0 <= fx1 && fy0 <= fy1;
+    if (threadIdx.x == 0)
     {
-        const int y = u.by * a.bandRows + warp * rowsPerWarp + r;
-        if (y >= H) break;
-        const float dY = (float)(y + offY);
-        const float hy[3] = {fmul(wi.H[1], dY), fmul(wi.H[4], dY), fmul(wi.H[7], dY)};
-        // Columns [s0, s1) - whole 64-pixel segments - can hold a covered
-        // pixel; the rest of the row is (0,0,0) with zero coverage words,
-        // written as such without evaluating the mapping.
-        int s0 = 0, s1 = 0;
-        if (y >= vy0 && y <= vy1)
+        // staged source box from the corners of the block's footprint part (FP64)
+        int bx = 0, by = 0, bc = 0, br = 0;
+        if (any)
         {
-            const int xs = max(vx0, 0), xe = min(vx1, W - 1);
-            if (xs <= xe)
+            double mnx = 1e300, mny = 1e300, mxx = -1e300, mxy = -1e300;
+            bool ok = true;
+            for (int c = 0; c < 4 && ok; ++c)
             {
-                s0 = xs & ~63;
-                s1 = min(W, (xe & ~63) + 64);
+                const double dx = (double)((c & 1) ? fx1 : fx0) + offX, dy = (double)((c & 2) ? fy1 : fy0) + offY;
+                const double w = (double)wi.H[6] * dx + (double)wi.H[7] * dy + (double)wi.H[8];
+                if (!(w > 1e-6)) ok = false;
+                const double sx = ((double)wi.H[0] * dx + (double)wi.H[1] * dy + (double)wi.H[2]) / w;
+                const double sy = ((double)wi.H[3] * dx + (double)wi.H[4] * dy + (double)wi.H[5]) / w;
+                mnx = fmin(mnx, sx);
+                mxx = fmax(mxx, sx);
+                mny = fmin(mny, sy);
+                mxy = fmax(mxy, sy);
+            }
+            if (ok && mxx > -1e9 && mnx < 1e9 && mxy > -1e9 && mny < 1e9)
+            {
+                const int sx0 = max(0, (int)floor(mnx) - 2), sx1 = min(wi.srcW - 1, (int)floor(mxx) + 3);
+                const int sy0 = max(0, (int)floor(mny) - 2), sy1 = min(wi.srcH - 1, (int)floor(mxy) + 3);
+                const int xa = sx0 & ~7;
+                if (sx0 <= sx1 && sy0 <= sy1 && sx1 - xa + 1 <= kWpSW && sy1 - sy0 + 1 <= kWpSH)
+                {
+                    bx = xa;
+                    by = sy0;
+                    bc = ((sx1 - xa) | 7) + 1;
+                    br = sy1 - sy0 + 1;
+                }
             }
         }
+        S.box[0] = bx;
+        S.box[1] = by;
+        S.box[2] = bc;
+        S.box[3] = br;
+    }
+    __syncthreads();
+    const int sbx = S.box[0], sby = S.box[1], sbc = S.box[2], sbr = S.box[3];
+    if (sbc > 0)
+    {
+        // 8-pixel groups: three 16-byte words when source rows are 16-byte aligned
+        const bool fast = (wi.srcW & 7) == 0 && (reinterpret_cast<uintptr_t>(wi.src) & 15) == 0;
+        const int ng = sbc >> 3;
+        for (int t = threadIdx.x; t < sbr * ng; t += blockDim.x)
+        {
+            const int r = t / ng, g = t - r * ng;
+            const int gx = sbx + 8 * g;
+            const unsigned short* s = wi.src + ((size_t)(sby + r) * wi.srcW + gx) * 3;
+            uint2* d = &S.px[r][8 * g];
+            if (fast && gx + 8 <= wi.srcW)
+            {
+                const uint4* s4 = reinterpret_cast<const uint4*>(s);
+                const uint4 q0 = __ldg(s4), q1 = __ldg(s4 + 1), q2 = __ldg(s4 + 2);
+                const uint32_t w[12] = {q0.x, q0.y, q0.z, q0.w, q1.x, q1.y, q1.z, q1.w, q2.x, q2.y, q2.z, q2.w};
+#pragma unroll
+                for (int e = 0; e < 8; e += 2)
+                {
+                    // pixels e, e+1 occupy u16 3e .. 3e+5 = words 3e/2 .. 3e/2+2
+                    const uint32_t a0 = w[3 * e / 2], a1 = w[3 * e / 2 + 1], a2 = w[3 * e / 2 + 2];
+                    d[e] = make_uint2(a0, a1 & 0xffffu);
+                    d[e + 1] = make_uint2((a1 >> 16) | (a2 << 16), a2 >> 16);
+                }
+            }
+            else
+            {
+#pragma unroll
+                for (int e = 0; e < 8; ++e)
+                    if (gx + e < wi.srcW)
+                        d[e] = make_uint2((uint32_t)__ldg(s + 3 * e) | ((uint32_t)__ldg(s + 3 * e + 1) << 16),
+                                          (uint32_t)__ldg(s + 3 * e + 2));
+            }
+        }
+    }
+    __syncthreads();
+    BoxAcc box;
+    for (int rr = 0; rr < kWpH / 8; ++rr)
+    {
+        const int y = Y0 + warp * (kWpH / 8) + rr;
+        if (y > Y1) break;
         unsigned short* row = img + (size_t)y * W * 3;
         uint32_t* covRow = it.cov + (size_t)y * T.covWords;
-        warp_zero_u16(row, s0 * 3, lane);
-        warp_zero_u16(row + (size_t)s1 * 3, (W - s1) * 3, lane);
-        for (int j = lane; j < (s0 >> 5); j += 32) covRow[j] = 0u;
-        for (int j = ((s1 + 31) >> 5) + lane; j < ((W + 31) >> 5); j += 32) covRow[j] = 0u;
-        for (int x0 = s0; x0 < s1; x0 += 64)
+        const bool rowIn = any && y >= fy0 && y <= fy1;
+        if (!rowIn)
         {
-            // Two independent pixels per lane keep more gathers in flight.
-            const int xa = x0 + lane, xb = x0 + 32 + lane;
-            unsigned short oa[3] = {0, 0, 0}, ob[3] = {0, 0, 0};
-            if (xa < W && xa >= vx0 && xa <= vx1) warp_px(wi, (float)(xa + offX), hy, oa);
-            if (xb < W && xb >= vx0 && xb <= vx1) warp_px(wi, (float)(xb + offX), hy, ob);
-            bool ca = (oa[0] | oa[1] | oa[2]) != 0, cb = (ob[0] | ob[1] | ob[2]) != 0;
-            if (xa < W)
+            warp_zero_u16(row + (size_t)X0 * 3, (X1 - X0 + 1) * 3, lane);
+            for (int j = (X0 >> 5) + lane; j <= (X1 >> 5); j += 32) covRow[j] = 0u;
+            continue;
+        }
+        const float dY = (float)(y + offY);
+        const float hy[3] = {fmul(wi.H[1], dY), fmul(wi.H[4], dY), fmul(wi.H[7], dY)};
+#pragma unroll
+        for (int i = 0; i < kWpW / 32; ++i)
+        {
+            const int x = X0 + 32 * i + lane;
+            unsigned short o[3] = {0, 0, 0};
+            int x0, y0;
+            float fx, fy;
+            if (x >= fx0 && x <= fx1 && warp_pos(wi, (float)(x + offX), hy, x0, y0, fx, fy))
             {
-                unsigned short* d = row + (size_t)xa * 3;
-                d[0] = oa[0];
-                d[1] = oa[1];
-                d[2] = oa[2];
+                const int cx = x0 - sbx, ry = y0 - sby;
+                unsigned short t00[3], t10[3], t01[3], t11[3];
+                if (cx >= 0 && cx + 1 < sbc && ry >= 0 && ry + 1 < sbr)
+                {
+                    if ((cx & 1) == 0)
+                    {
+                        const uint4 p0 = *reinterpret_cast<const uint4*>(&S.px[ry][cx]);
+                        const uint4 p1 = *reinterpret_cast<const uint4*>(&S.px[ry + 1][cx]);
+                        px_of(make_uint2(p0.x, p0.y), t00);
+                        px_of(make_uint2(p0.z, p0.w), t10);
+                        px_of(make_uint2(p1.x, p1.y), t01);
+                        px_of(make_uint2(p1.z, p1.w), t11);
+                    }
+                    else
+                    {
+                        px_of(S.px[ry][cx], t00);
+                        px_of(S.px[ry][cx + 1], t10);
+                        px_of(S.px[ry + 1][cx], t01);
+                        px_of(S.px[ry + 1][cx + 1], t11);
+                    }
+                }
+                else
+                {
+                    const unsigned short* r0 = wi.src + ((size_t)y0 * wi.srcW + x0) * 3;
+                    const unsigned short* r1 = r0 + (size_t)wi.srcW * 3;
+#pragma unroll
+                    for (int c = 0; c < 3; ++c)
+                    {
+                        t00[c] = __ldg(r0 + c);
+                        t10[c] = __ldg(r0 + 3 + c);
+                        t01[c] = __ldg(r1 + c);
+                        t11[c] = __ldg(r1 + 3 + c);
+                    }
+                }
+                warp_mix(wi, fx, fy, t00, t10, t01, t11, o);
             }
-            if (xb < W)
+            const bool cov = (o[0] | o[1] | o[2]) != 0;
+            if (x <= X1)
             {
-                unsigned short* d = row + (size_t)xb * 3;
-                d[0] = ob[0];
-                d[1] = ob[1];
-                d[2] = ob[2];
+                unsigned short* d = row + (size_t)x * 3;
+                d[0] = o[0];
+                d[1] = o[1];
+                d[2] = o[2];
             }
-            unsigned ma = __ballot_sync(kFull, ca), mb = __ballot_sync(kFull, cb);
-            if (lane == 0)
-            {
-                covRow[x0 >> 5] = ma;
-                if (x0 + 32 < W) covRow[(x0 >> 5) + 1] = mb;
-            }
-            box.add(ca, xa, y);
-            box.add(cb, xb, y);
+            const unsigned m = __ballot_sync(kFull, cov);
+            if (lane == 0 && x - lane <= X1) covRow[(x - lane) >> 5] = m;
+            box.add(cov, x, y);
         }
     }
     box.flush(it.bbox);
@@ -1803,6 +1933,507 @@ __global__ void __launch_bounds__(256) k_final0(BlendArgs a, const Unit* __restr
             if (i < cnt) final_pixel(T, C, rc, uw, uh, p + i, own[i]);
     }
 }
+
+// ---------------------------------------------------------------------------
+// Fused pyramid levels 0 and 1 (SeamBlend.cpp:125-201, 447-546).
+//
+// Level 1 of every contributor's pyramids (num, den and weight: 20 bytes per
+// level-1 pixel per contributor) and of the tile's blended bands is never
+// written to memory.  Two kernels replace the level-0 and level-1 steps of
+// the materialised pyramid:
+//
+//  k_base2  per contributor and 32x8 block of level 2: stages the level-0
+//           footprint in shared memory, computes the level-1 values of the
+//           block's level-1 rectangle exactly in integers (as k_down0s), then
+//           blurs and decimates them to level 2 in FP32 in the reference's
+//           order (as k_down).  Writes level 2 only.
+//  k_fine   per tile and 64x32 block of output pixels: for every contributor
+//           owning a pixel of the block's level-0 footprint, in index order,
+//           recomputes its level-1 values on the block's level-1 window from
+//           the staged level-0 footprint, accumulates the blended level-1 band
+//           (weight x (G1 - Up(G2))) and, for the pixels it owns, the level-0
+//           Laplacian img - Up(G1); then collapses level 1 with Up(recon2)
+//           read from the coarse levels and writes the output.
+//
+// Levels 2 and above stay materialised (a sixteenth of the pixels).  The
+// values are the materialised pyramid's bit for bit: the level-1 values are
+// the same exact integers / 256, every FP32 operation is the same in the same
+// order, and a blended-band term is skipped only where its weight is exactly
+// zero (the term is then +-0, and adding +-0 to the sum, which starts at +0
+// and is never -0, changes nothing).  A contributor that owns no pixel of a
+// block's footprint has weight zero on the whole level-1 window.
+// ---------------------------------------------------------------------------
+constexpr int kB2W = 32, kB2H = 8;                  // level-2 outputs per k_base2 CTA
+constexpr int kB1W = 2 * kB2W + 3, kB1H = 2 * kB2H + 3;  // its level-1 rectangle (at most)
+constexpr int kB0S = 2 * kB1W + 3 + 3;              // level-0 footprint row stride: at most 137 columns from
+                                                    // a 4-pixel aligned start, 35 whole groups
+constexpr int kB0H = 2 * kB1H + 3;                  // level-0 footprint rows (at most)
+constexpr int kRun = 7;                             // level-1 rows per streaming task
+
+constexpr int kFW = 64, kFH = 32;                   // output pixels per k_fine CTA
+constexpr int kF1W = 36, kF1H = 20;                 // its level-1 window (bound; checked)
+constexpr int kF0S = 2 * kF1W + 8;                  // level-0 footprint row stride: the footprint's
+                                                    // at most 78 columns rounded up to whole 4-pixel groups
+constexpr int kF0H = 2 * kF1H + 3;                  // level-0 footprint rows
+constexpr int kF2W = 22, kF2H = 14;                 // level-2 window (bound; checked)
+
+// Stages contributor k's level-0 pixels of tile rows [ry0, ry1] x columns
+// [cx0, cx1] as packed pixels (r | g << 16, b | cov << 16 | own << 17) at
+// sm[(y - ry0) * stride + (x - (cx0 & ~3))], in whole groups of four pixels
+// from the aligned start (stride must hold them: a multiple of 4 at least
+// cx1 - (cx0 & ~3) + 1).  `own` is the owner map of the same rows (global,
+// or shared with row stride ownStride when ownSm is set).  A group is read
+// as three 8-byte words when the image rows allow it.
+__device__ __forceinline__ void stage_level0(const unsigned short* img, const signed char* own, int ownStride,
+                                             bool ownSm, signed char k, int W, int ry0, int ry1, int cx0, int cx1,
+                                             PackedPx* sm, int stride)
+{
+    const int cxa = cx0 & ~3;
+    const int ng = ((cx1 - cxa) >> 2) + 1;
+    const int nr = ry1 - ry0 + 1;
+    const bool fast = (W & 3) == 0 && (reinterpret_cast<uintptr_t>(img) & 7) == 0;
+    for (int t = threadIdx.x; t < nr * ng; t += blockDim.x)
+    {
+        const int r = t / ng, g = t - r * ng;
+        const int c = cxa + 4 * g;
+        const size_t p = (size_t)(ry0 + r) * W + c;
+        PackedPx* d = sm + r * stride + 4 * g;
+        signed char o[4];
+#pragma unroll
+        for (int e = 0; e < 4; ++e)
+            o[e] = (c + e < W) ? (ownSm ? own[r * ownStride + (c + e - cxa)] : __ldg(own + p + e)) : (signed char)-1;
+        if (fast)
+        {
+            const uint2* w = reinterpret_cast<const uint2*>(img + p * 3);
+            const uint2 w0 = __ldg(w), w1 = __ldg(w + 1), w2 = __ldg(w + 2);
+            d[0] = pack_px(w0.x & 0xffffu, w0.x >> 16, w0.y & 0xffffu, o[0] == k);
+            d[1] = pack_px(w0.y >> 16, w1.x & 0xffffu, w1.x >> 16, o[1] == k);
+            d[2] = pack_px(w1.y & 0xffffu, w1.y >> 16, w2.x & 0xffffu, o[2] == k);
+            d[3] = pack_px(w2.x >> 16, w2.y & 0xffffu, w2.y >> 16, o[3] == k);
+        }
+        else
+        {
+#pragma unroll
+            for (int e = 0; e < 4; ++e)
+                if (c + e < W)
+                {
+                    const unsigned short* q = img + (p + e) * 3;
+                    d[e] = pack_px(__ldg(q), __ldg(q + 1), __ldg(q + 2), o[e] == k);
+                }
+        }
+    }
+}
+
+// Exact level-1 values (num r, g, b; den; weight) of level-1 column X1 and
+// rows Y1s .. Y1s + R - 1 from a staged footprint (tile rows from ry0,
+// columns from cxa), handed to emit(m, nr, ng, nb, den, wg) in row order.
+// Integer sums of the [1,4,6,4,1] x [1,4,6,4,1] stencil over clamped level-0
+// coordinates, streamed row by row (see k_down0s for why they are exact).
+template <typename Emit>
+__device__ __forceinline__ void level1_column(const PackedPx* sm, int stride, int ry0, int cxa, int W, int H,
+                                              int X1, int Y1s, int R, Emit emit)
+{
+    int col[5];
+#pragma unroll
+    for (int i = 0; i < 5; ++i) col[i] = min(max(2 * X1 - 2 + i, 0), W - 1) - cxa;
+    int P[4] = {0, 0, 0, 0}, Q[4] = {0, 0, 0, 0}, Rr[4] = {0, 0, 0, 0};
+    const float s256 = 1.0f / 256.0f;
+    for (int r = 0; r <= 2 * R + 2; ++r)
+    {
+        const int gy = min(max(2 * Y1s - 2 + r, 0), H - 1);
+        const PackedPx* row = sm + (gy - ry0) * stride;
+        int t[4] = {0, 0, 0, 0};
+#pragma unroll
+        for (int i = 0; i < 5; ++i)
+        {
+            int cv[4];
+            px_channels(row[col[i]], cv);
+            const int wgt = (i == 0 || i == 4) ? 1 : (i == 2 ? 6 : 4);
+#pragma unroll
+            for (int ch = 0; ch < 4; ++ch) t[ch] += wgt * cv[ch];
+        }
+        if ((r & 1) == 0)
+        {
+#pragma unroll
+            for (int ch = 0; ch < 4; ++ch)
+            {
+                P[ch] += t[ch];
+                Q[ch] += 6 * t[ch];
+                Rr[ch] = t[ch];
+            }
+            const int m = (r >> 1) - 2;
+            if (m >= 0)
+                emit(m, fmul((float)P[0], s256), fmul((float)P[1], s256), fmul((float)P[2], s256),
+                     fmul((float)(P[3] >> 16), s256), fmul((float)(P[3] & 0xffff), s256));
+        }
+        else
+        {
+#pragma unroll
+            for (int ch = 0; ch < 4; ++ch)
+            {
+                Q[ch] += 4 * t[ch];
+                Rr[ch] += 4 * t[ch];
+                P[ch] = Q[ch];
+                Q[ch] = Rr[ch];
+            }
+        }
+    }
+}
+
+struct Base2Smem
+{
+    PackedPx px[kB0H * kB0S];          // level-0 footprint; later the horizontal level-2 pass
+    float l1[5][kB1H][kB1W];           // level-1 rectangle: num r, g, b, den, weight
+};
+
+__global__ void __launch_bounds__(256) k_base2(BlendArgs a, const Unit* __restrict__ units)
+{
+    extern __shared__ __align__(16) unsigned char base2_raw[];
+    Base2Smem& S = *reinterpret_cast<Base2Smem*>(base2_raw);
+    float (*t)[kB1H][kB2W] = reinterpret_cast<float (*)[kB1H][kB2W]>(S.px);  // aliases the footprint
+    const Unit u = units[blockIdx.x];
+    const ItemDev& it = a.items[u.id];
+    const TileDev& T = a.tiles[it.tile];
+    const int W = T.w, H = T.h;
+    const int lw1 = T.lw[1], lh1 = T.lh[1], lw2 = T.lw[2], lh2 = T.lh[2];
+    const int X2a = u.bx * kB2W, Y2a = u.by * kB2H;
+    const int X2b = min(X2a + kB2W - 1, lw2 - 1), Y2b = min(Y2a + kB2H - 1, lh2 - 1);
+    const int X1lo = max(0, 2 * X2a - 2), X1hi = min(lw1 - 1, 2 * X2b + 2);
+    const int Y1lo = max(0, 2 * Y2a - 2), Y1hi = min(lh1 - 1, 2 * Y2b + 2);
+    const int cx0 = max(0, 2 * X1lo - 2), cx1 = min(W - 1, 2 * X1hi + 2);
+    const int ry0 = max(0, 2 * Y1lo - 2), ry1 = min(H - 1, 2 * Y1hi + 2);
+    const size_t q2 = T.loff[2];
+    // A footprint that misses the covered box reads only uncovered pixels the
+    // contributor does not own: its level-2 values are exactly zero.
+    const int4 cb = covered_box(it.bbox);
+    if (cb.x > cb.z || cx1 < cb.x || cx0 > cb.z || ry1 < cb.y || ry0 > cb.w)
+    {
+        for (int idx = threadIdx.x; idx < kB2W * kB2H; idx += blockDim.x)
+        {
+            const int X = X2a + (idx & (kB2W - 1)), Y = Y2a + idx / kB2W;
+            if (X > X2b || Y > Y2b) continue;
+            const size_t q = q2 + (size_t)Y * lw2 + X;
+            it.nd[q] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+            it.wg[q] = 0.0f;
+        }
+        return;
+    }
+    const int cxa = cx0 & ~3;
+    stage_level0(it.img, T.owner, 0, false, (signed char)it.k, W, ry0, ry1, cx0, cx1, S.px, kB0S);
+    __syncthreads();
+    // level-1 rectangle, a column run of kRun rows per task
+    const int nX1 = X1hi - X1lo + 1, nY1 = Y1hi - Y1lo + 1;
+    const int nRuns = (nY1 + kRun - 1) / kRun;
+    for (int task = threadIdx.x; task < nX1 * nRuns; task += blockDim.x)
+    {
+        const int run = task / nX1, cx = task - run * nX1;
+        const int Y1s = Y1lo + run * kRun;
+        const int R = min(kRun, Y1hi - Y1s + 1);
+        level1_column(S.px, kB0S, ry0, cxa, W, H, X1lo + cx, Y1s, R,
+                      [&](int m, float nr, float ng, float nb, float den, float wg) {
+                          const int ry = Y1s + m - Y1lo;
+                          S.l1[0][ry][cx] = nr;
+                          S.l1[1][ry][cx] = ng;
+                          S.l1[2][ry][cx] = nb;
+                          S.l1[3][ry][cx] = den;
+                          S.l1[4][ry][cx] = wg;
+                      });
+    }
+    __syncthreads();
+    // horizontal taps at the level-2 columns (over clamped level-1 columns)
+    const int nX2 = X2b - X2a + 1, nY2 = Y2b - Y2a + 1;
+    for (int idx = threadIdx.x; idx < 5 * nY1 * kB2W; idx += blockDim.x)
+    {
+        const int ch = idx / (nY1 * kB2W);
+        const int rem = idx - ch * nY1 * kB2W;
+        const int r = rem / kB2W, i = rem - r * kB2W;
+        if (i >= nX2) continue;
+        const int X2 = X2a + i;
+        float v[5];
+#pragma unroll
+        for (int q = 0; q < 5; ++q) v[q] = S.l1[ch][r][min(max(2 * X2 - 2 + q, 0), lw1 - 1) - X1lo];
+        t[ch][r][i] = blur5(v[0], v[1], v[2], v[3], v[4]);
+    }
+    __syncthreads();
+    for (int idx = threadIdx.x; idx < nX2 * nY2; idx += blockDim.x)
+    {
+        const int j = idx / nX2, i = idx - j * nX2;
+        const int Y2 = Y2a + j;
+        int rows[5];
+#pragma unroll
+        for (int q = 0; q < 5; ++q) rows[q] = min(max(2 * Y2 - 2 + q, 0), lh1 - 1) - Y1lo;
+        float o[5];
+#pragma unroll
+        for (int ch = 0; ch < 5; ++ch)
+            o[ch] = blur5(t[ch][rows[0]][i], t[ch][rows[1]][i], t[ch][rows[2]][i], t[ch][rows[3]][i], t[ch][rows[4]][i]);
+        const size_t q = q2 + (size_t)Y2 * lw2 + X2a + i;
+        it.nd[q] = make_float4(o[0], o[1], o[2], o[3]);
+        it.wg[q] = o[4];
+    }
+}
+
+struct FineSmem
+{
+    PackedPx px[kF0H * kF0S];                  // one contributor's level-0 footprint
+    signed char own[kF0H * kF0S];              // the tile's owner map over the footprint
+    float g1[3][kF1H][kF1W];                   // that contributor's G1 on the level-1 window; then recon1
+    float w1[kF1H][kF1W];                      // its level-1 weight
+    float g2[3][kF2H][kF2W];                   // its G2 on the level-2 window
+    float r2[3][kF2H][kF2W];                   // recon2 on the level-2 window
+    const unsigned short* img[kMaxTileItems];
+    const float4* nd[kMaxTileItems];
+    uint32_t set[kMaxTileItems / 32];          // contributors owning a footprint pixel
+};
+
+__global__ void __launch_bounds__(256) k_fine(BlendArgs a, const Unit* __restrict__ units)
+{
+    extern __shared__ __align__(16) unsigned char fine_raw[];
+    FineSmem& S = *reinterpret_cast<FineSmem*>(fine_raw);
+    const Unit u = units[blockIdx.x];
+    const TileDev& T = a.tiles[u.id];
+    const int W = T.w, H = T.h, K = min(T.numItems, kMaxTileItems);
+    const int X0 = u.bx * kFW, Y0 = u.by * kFH;
+    const int xe = min(X0 + kFW - 1, W - 1), ye = min(Y0 + kFH - 1, H - 1);
+    const int tid = threadIdx.x;
+    // this thread's outputs: 8 pixels of one row
+    const int oy = Y0 + (tid >> 3), ox = X0 + (tid & 7) * 8;
+    const bool rowOk = oy <= ye;
+    int own[8];
+#pragma unroll
+    for (int i = 0; i < 8; ++i) own[i] = (rowOk && ox + i <= xe) ? (int)__ldg(T.owner + (size_t)oy * W + ox + i) : -2;
+    for (int k = tid; k < K; k += blockDim.x)
+    {
+        const ItemDev& it = a.items[T.firstItem + k];
+        S.img[k] = it.img;
+        S.nd[k] = it.nd;
+    }
+    if (tid < kMaxTileItems / 32) S.set[tid] = 0u;
+    __syncthreads();  // the set is cleared before any thread adds to it
+    unsigned short* outRow = T.out + ((size_t)oy * W + ox) * 3;
+    if (T.bands == 1)
+    {
+        // one band: the output is the owner's pixel (SeamBlend.cpp:527-545)
+#pragma unroll
+        for (int i = 0; i < 8; ++i)
+        {
+            if (own[i] == -2) continue;
+            unsigned short* o = outRow + 3 * i;
+            if (own[i] < 0)
+            {
+                o[0] = o[1] = o[2] = 0;
+                continue;
+            }
+            const unsigned short* p = S.img[own[i]] + ((size_t)oy * W + ox + i) * 3;
+            const float r[3] = {(float)__ldg(p), (float)__ldg(p + 1), (float)__ldg(p + 2)};
+            final_store(o, r);
+        }
+        return;
+    }
+    const int lw1 = T.lw[1], lh1 = T.lh[1];
+    const bool top1 = T.bands == 2;
+    // level-1 window: the Up taps of the block's first and last pixels
+    // (monotonic in x and y)
+    const UpCoef ca = up_coef_s(T.usx[0], T.usy[0], lw1, lh1, X0, Y0);
+    const UpCoef cb = up_coef_s(T.usx[0], T.usy[0], lw1, lh1, xe, ye);
+    const int A0 = ca.x0, A1 = cb.x1, B0 = ca.y0, B1 = cb.y1;
+    const int nA = A1 - A0 + 1, nB = B1 - B0 + 1;
+    const int cx0 = max(0, 2 * A0 - 2), cx1 = min(W - 1, 2 * A1 + 2);
+    const int ry0 = max(0, 2 * B0 - 2), ry1 = min(H - 1, 2 * B1 + 2);
+    const int cxa = cx0 & ~3;
+    // level-2 window: the Up taps (level 2 -> 1) of the level-1 window's corners
+    int P0 = 0, P1 = -1, Q0 = 0, Q1 = -1;
+    const int lw2 = top1 ? 1 : T.lw[2], lh2 = top1 ? 1 : T.lh[2];
+    if (!top1)
+    {
+        const UpCoef pa = up_coef_s(T.usx[1], T.usy[1], lw2, lh2, A0, B0);
+        const UpCoef pb = up_coef_s(T.usx[1], T.usy[1], lw2, lh2, A1, B1);
+        P0 = pa.x0;
+        P1 = pb.x1;
+        Q0 = pa.y0;
+        Q1 = pb.y1;
+    }
+    const int nP = P1 - P0 + 1, nQ = Q1 - Q0 + 1;
+    if (nA > kF1W || nB > kF1H || ry1 - ry0 + 1 > kF0H || ((cx1 - cxa + 4) & ~3) > kF0S || nP > kF2W || nQ > kF2H)
+    {
+        // outside the proven window bounds: report instead of overrunning
+        if (tid == 0)
+        {
+            atomicExch(a.error, 1);
+            atomicExch(a.error + 1, 1);
+        }
+        return;
+    }
+    // owner map over the footprint, and the contributors it names
+    const int nr = ry1 - ry0 + 1, ncol = cx1 - cxa + 1;
+    for (int idx = tid; idx < nr * ncol; idx += blockDim.x)
+    {
+        const int r = idx / ncol, c = idx - r * ncol;
+        const int x = cxa + c;
+        const int o = x < W ? (int)__ldg(T.owner + (size_t)(ry0 + r) * W + x) : -1;
+        S.own[r * kF0S + c] = (signed char)o;
+        if (x >= cx0 && o >= 0 && o < K) atomicOr(&S.set[o >> 5], 1u << (o & 31));
+    }
+    // recon2 on the level-2 window
+    if (!top1)
+    {
+        const float* rc2 = T.blend + T.loff[2] * 3;
+        for (int idx = tid; idx < nP * nQ; idx += blockDim.x)
+        {
+            const int r = idx / nP, c = idx - r * nP;
+            const float* s = rc2 + ((size_t)(Q0 + r) * lw2 + P0 + c) * 3;
+            S.r2[0][r][c] = __ldg(s);
+            S.r2[1][r][c] = __ldg(s + 1);
+            S.r2[2][r][c] = __ldg(s + 2);
+        }
+    }
+    __syncthreads();
+    // this thread's level-1 window pixels: tid, tid + 256, tid + 512
+    float acc[3][3];
+#pragma unroll
+    for (int j = 0; j < 3; ++j) acc[j][0] = acc[j][1] = acc[j][2] = 0.0f;
+    float lap[8][3];
+#pragma unroll
+    for (int i = 0; i < 8; ++i) lap[i][0] = lap[i][1] = lap[i][2] = 0.0f;
+    const int nWin = nA * nB;
+    const int nRuns = (nB + kRun - 1) / kRun;
+    for (int w = 0; w < kMaxTileItems / 32; ++w)
+    {
+        uint32_t m = S.set[w];
+        while (m)
+        {
+            const int k = 32 * w + __ffs(m) - 1;
+            m &= m - 1;
+            stage_level0(S.img[k], S.own, kF0S, true, (signed char)k, W, ry0, ry1, cxa, cx1, S.px, kF0S);
+            if (!top1)
+            {
+                const float4* g2 = S.nd[k] + T.loff[2];
+                for (int idx = tid; idx < nP * nQ; idx += blockDim.x)
+                {
+                    const int r = idx / nP, c = idx - r * nP;
+                    const float3 g = gauss_of(__ldg(g2 + (size_t)(Q0 + r) * lw2 + P0 + c));
+                    S.g2[0][r][c] = g.x;
+                    S.g2[1][r][c] = g.y;
+                    S.g2[2][r][c] = g.z;
+                }
+            }
+            __syncthreads();
+            // level-1 values of contributor k on the window
+            for (int task = tid; task < nA * nRuns; task += blockDim.x)
+            {
+                const int run = task / nA, c = task - run * nA;
+                const int Y1s = B0 + run * kRun;
+                const int R = min(kRun, B1 - Y1s + 1);
+                level1_column(S.px, kF0S, ry0, cxa, W, H, A0 + c, Y1s, R,
+                              [&](int mm, float n0, float n1, float n2, float den, float wg) {
+                                  const int r = Y1s + mm - B0;
+                                  const float3 g = gauss_of(make_float4(n0, n1, n2, den));
+                                  S.g1[0][r][c] = g.x;
+                                  S.g1[1][r][c] = g.y;
+                                  S.g1[2][r][c] = g.z;
+                                  S.w1[r][c] = wg;
+                              });
+            }
+            __syncthreads();
+            // blended level-1 band: weight x Laplacian, in contributor order
+#pragma unroll
+            for (int j = 0; j < 3; ++j)
+            {
+                const int p = tid + 256 * j;
+                if (p >= nWin) continue;
+                const int r = p / nA, c = p - r * nA;
+                const float wv = S.w1[r][c];
+                if (wv == 0.0f) continue;  // the term is +-0
+                float g[3] = {S.g1[0][r][c], S.g1[1][r][c], S.g1[2][r][c]};
+                if (!top1)
+                {
+                    const UpCoef q = up_coef_s(T.usx[1], T.usy[1], lw2, lh2, A0 + c, B0 + r);
+                    const int x0 = q.x0 - P0, x1 = q.x1 - P0, y0 = q.y0 - Q0, y1 = q.y1 - Q0;
+#pragma unroll
+                    for (int ch = 0; ch < 3; ++ch)
+                        g[ch] = fsub(g[ch], up_mix(S.g2[ch][y0][x0], S.g2[ch][y0][x1], S.g2[ch][y1][x0],
+                                                   S.g2[ch][y1][x1], q.wx, q.wy));
+                }
+#pragma unroll
+                for (int ch = 0; ch < 3; ++ch) acc[j][ch] = fadd(acc[j][ch], fmul(wv, g[ch]));
+            }
+            // level-0 Laplacian of the pixels k owns: img - Up(G1)
+#pragma unroll
+            for (int i = 0; i < 8; ++i)
+            {
+                if (own[i] != k) continue;
+                const int x = ox + i;
+                const UpCoef q = up_coef_s(T.usx[0], T.usy[0], lw1, lh1, x, oy);
+                const int x0 = q.x0 - A0, x1 = q.x1 - A0, y0 = q.y0 - B0, y1 = q.y1 - B0;
+                int cv[4];
+                px_channels(S.px[(oy - ry0) * kF0S + (x - cxa)], cv);
+#pragma unroll
+                for (int ch = 0; ch < 3; ++ch)
+                    lap[i][ch] = fsub((float)cv[ch], up_mix(S.g1[ch][y0][x0], S.g1[ch][y0][x1], S.g1[ch][y1][x0],
+                                                            S.g1[ch][y1][x1], q.wx, q.wy));
+            }
+            __syncthreads();
+        }
+    }
+    // recon1 = blended1 + Up(recon2) on the window (in g1's place)
+#pragma unroll
+    for (int j = 0; j < 3; ++j)
+    {
+        const int p = tid + 256 * j;
+        if (p >= nWin) continue;
+        const int r = p / nA, c = p - r * nA;
+        float v[3] = {acc[j][0], acc[j][1], acc[j][2]};
+        if (!top1)
+        {
+            const UpCoef q = up_coef_s(T.usx[1], T.usy[1], lw2, lh2, A0 + c, B0 + r);
+            const int x0 = q.x0 - P0, x1 = q.x1 - P0, y0 = q.y0 - Q0, y1 = q.y1 - Q0;
+#pragma unroll
+            for (int ch = 0; ch < 3; ++ch)
+                v[ch] = fadd(v[ch], up_mix(S.r2[ch][y0][x0], S.r2[ch][y0][x1], S.r2[ch][y1][x0], S.r2[ch][y1][x1],
+                                           q.wx, q.wy));
+        }
+        S.g1[0][r][c] = v[0];
+        S.g1[1][r][c] = v[1];
+        S.g1[2][r][c] = v[2];
+    }
+    __syncthreads();
+    if (!rowOk) return;
+    // output: clamp(lap0 + Up(recon1)) + 0.5, zero where nobody owns
+    unsigned short res[24];
+#pragma unroll
+    for (int i = 0; i < 8; ++i)
+    {
+        res[3 * i] = res[3 * i + 1] = res[3 * i + 2] = 0;
+        if (own[i] < 0) continue;
+        const UpCoef q = up_coef_s(T.usx[0], T.usy[0], lw1, lh1, ox + i, oy);
+        const int x0 = q.x0 - A0, x1 = q.x1 - A0, y0 = q.y0 - B0, y1 = q.y1 - B0;
+        float r[3];
+#pragma unroll
+        for (int ch = 0; ch < 3; ++ch)
+            r[ch] = fadd(lap[i][ch], up_mix(S.g1[ch][y0][x0], S.g1[ch][y0][x1], S.g1[ch][y1][x0], S.g1[ch][y1][x1],
+                                            q.wx, q.wy));
+        final_store(res + 3 * i, r);
+    }
+    if (ox + 7 <= xe && (reinterpret_cast<uintptr_t>(outRow) & 15) == 0)
+    {
+        uint4* o4 = reinterpret_cast<uint4*>(outRow);
+#pragma unroll
+        for (int k = 0; k < 3; ++k)
+            o4[k] = make_uint4((uint32_t)res[8 * k] | ((uint32_t)res[8 * k + 1] << 16),
+                               (uint32_t)res[8 * k + 2] | ((uint32_t)res[8 * k + 3] << 16),
+                               (uint32_t)res[8 * k + 4] | ((uint32_t)res[8 * k + 5] << 16),
+                               (uint32_t)res[8 * k + 6] | ((uint32_t)res[8 * k + 7] << 16));
+    }
+    else
+    {
+        for (int i = 0; i < 8; ++i)
+            if (own[i] != -2)
+            {
+                outRow[3 * i] = res[3 * i];
+                outRow[3 * i + 1] = res[3 * i + 1];
+                outRow[3 * i + 2] = res[3 * i + 2];
+            }
+    }
+}
 }  // namespace
 
 // Shared-memory bytes of the per-row-group progress counters.
@@ -1910,5 +2541,23 @@ int launch_final0(const BlendArgs& a, const Unit* units, int n, cudaStream_t s)
     if (n <= 0) return I360B_SUCCESS;
     k_final0<<<n, 256, 0, s>>>(a, units);
     return check_launch("final level kernel");
+}
+
+int launch_base2(const BlendArgs& a, const Unit* units, int n, cudaStream_t s)
+{
+    if (n <= 0) return I360B_SUCCESS;
+    const int smem = (int)sizeof(Base2Smem);
+    cudaFuncSetAttribute(k_base2, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    k_base2<<<n, 256, smem, s>>>(a, units);
+    return check_launch("pyramid base kernel");
+}
+
+int launch_fine(const BlendArgs& a, const Unit* units, int n, cudaStream_t s)
+{
+    if (n <= 0) return I360B_SUCCESS;
+    const int smem = (int)sizeof(FineSmem);
+    cudaFuncSetAttribute(k_fine, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    k_fine<<<n, 256, smem, s>>>(a, units);
+    return check_launch("fine levels kernel");
 }
 }  // namespace i360b

@@ -93,5 +93,13 @@ int launch_down(const BlendArgs& a, const Unit* units, int n, int level, cudaStr
 int launch_blend_level(const BlendArgs& a, const Unit* units, int n, int level, cudaStream_t s);
 int launch_collapse(const BlendArgs& a, const Unit* units, int n, int level, cudaStream_t s);
 int launch_final0(const BlendArgs& a, const Unit* units, int n, cudaStream_t s);
+// Fused pyramid levels 0-1: level 2 of every contributor from level 0
+// (units: item, 32x8 blocks of level 2), then per tile the level-1 blend,
+// its collapse and the output (units: tile, 64x32 blocks of output pixels).
+constexpr int kBase2W = 32, kBase2H = 8, kFineW = 64, kFineH = 32;
+// Destination block of one tile-warp CTA (launch_warp_tiles units: item, block).
+constexpr int kWarpBlockW = 128, kWarpBlockH = 16;
+int launch_base2(const BlendArgs& a, const Unit* units, int n, cudaStream_t s);
+int launch_fine(const BlendArgs& a, const Unit* units, int n, cudaStream_t s);
 int dt_rows_in_flight(int maxW, int maxH);
 }  // namespace i360b

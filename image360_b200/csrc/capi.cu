@@ -263,6 +263,21 @@ extern "C" int i360b_launch_median(const unsigned short* const* dInputs, int num
     return launch_median(dInputs, numInputs, dOutput, width, height, sigmaThreshold, static_cast<cudaStream_t>(stream));
 }
 
+extern "C" int i360b_launch_warp_median(const unsigned short* const* dFrames, int numFrames, int srcW, int srcH,
+                                        const float* homographies, unsigned short* dOutput, int dstW, int dstH,
+                                        int offsetX, int offsetY, float sigmaThreshold, void* stream)
+{
+    clear_error();
+    I360B_TRY(require_init());
+    if (!dFrames || !dOutput || !homographies) return fail(I360B_INVALID_PARAM, "Null pointer argument.");
+    if (numFrames <= 0 || numFrames > 32) return fail(I360B_INVALID_PARAM, "numInputs must be 1-32.");
+    if (srcW <= 0 || srcH <= 0 || dstW <= 0 || dstH <= 0) return fail(I360B_INVALID_PARAM, "Invalid dimensions.");
+    for (int i = 0; i < numFrames; ++i)
+        if (!dFrames[i]) return fail(I360B_INVALID_PARAM, "Null pointer argument.");
+    return launch_warp_median(dFrames, numFrames, srcW, srcH, homographies, dOutput, dstW, dstH, offsetX, offsetY,
+                              sigmaThreshold, static_cast<cudaStream_t>(stream));
+}
+
 extern "C" int i360b_launch_gain(unsigned short* dData, int numValues, float gain, void* stream)
 {
     clear_error();

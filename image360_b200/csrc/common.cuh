@@ -93,6 +93,8 @@ int launch_warp(const unsigned short* src, int sw, int sh, unsigned short* dst, 
                 int offX, int offY, float gain, cudaStream_t s);
 int launch_median(const unsigned short* const* inputs, int n, unsigned short* out, int w, int h, float sigma,
                   cudaStream_t s);
+int launch_warp_median(const unsigned short* const* frames, int n, int sw, int sh, const float* H, unsigned short* out,
+                       int dw, int dh, int offX, int offY, float sigma, cudaStream_t s);
 int launch_gain(unsigned short* data, long long n, float gain, cudaStream_t s);
 // Lab statistics / Reinhard transfer / frame-set colour correction (color.cu).
 int launch_lab_stats(const unsigned short* const* dImgs, const int* w, const int* h, int n, double* dStats,

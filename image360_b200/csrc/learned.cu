@@ -1615,6 +1615,35 @@ extern "C" int i360b_blendnet_set_params(i360b_blendnet* net, const float* hostP
     return I360B_SUCCESS;
 }
 
+extern "C" int i360b_blendnet_get_adam(i360b_blendnet* net, float* hostM, float* hostV, int count, int* step)
+{
+    I360B_TRY(net_prologue(net));
+    if (!hostM || !hostV || !step || count != net->net.nParams)
+        return fail(I360B_INVALID_PARAM, "parameter count mismatch");
+    BlendNet& N = net->net;
+    std::lock_guard<std::mutex> lk(N.mu);
+    I360B_CUDA(cudaDeviceSynchronize(), "blend network");
+    I360B_CUDA(cudaMemcpy(hostM, N.adamM, (size_t)count * sizeof(float), cudaMemcpyDeviceToHost), "adam download");
+    I360B_CUDA(cudaMemcpy(hostV, N.adamV, (size_t)count * sizeof(float), cudaMemcpyDeviceToHost), "adam download");
+    *step = N.step;
+    return I360B_SUCCESS;
+}
+
+extern "C" int i360b_blendnet_set_adam(i360b_blendnet* net, const float* hostM, const float* hostV, int count,
+                                       int step)
+{
+    I360B_TRY(net_prologue(net));
+    if (!hostM || !hostV || count != net->net.nParams || step < 0)
+        return fail(I360B_INVALID_PARAM, "parameter count mismatch or negative step");
+    BlendNet& N = net->net;
+    std::lock_guard<std::mutex> lk(N.mu);
+    I360B_CUDA(cudaDeviceSynchronize(), "blend network");
+    I360B_CUDA(cudaMemcpy(N.adamM, hostM, (size_t)count * sizeof(float), cudaMemcpyHostToDevice), "adam upload");
+    I360B_CUDA(cudaMemcpy(N.adamV, hostV, (size_t)count * sizeof(float), cudaMemcpyHostToDevice), "adam upload");
+    N.step = step;
+    return I360B_SUCCESS;
+}
+
 extern "C" int i360b_blendnet_logits(i360b_blendnet* net, const i360b_blend_job* jobs, int n, int w, int h,
                                      float* dLogits)
 {

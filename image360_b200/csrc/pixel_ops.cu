@@ -242,10 +242,18 @@ __global__ void __launch_bounds__(256) k_warp(const unsigned short* __restrict__
 
 // ---------------------------------------------------------------------------
 // Median stack (MedianStackKernels.h:19-55, MedianStack_Scalar.cpp:8-24).
-// One output scalar per thread.  Statistics are accumulated sequentially in
-// input order in FP32 (sumSq exceeds 2^24, so the order is part of the
-// result).  Clipped-out values become INT_MAX and a register bitonic network
-// of the padded width sorts; the median is element keptCount/2.
+//
+// Two output scalars per thread, packed as the low and high halves of one
+// 32-bit word per input (one 4-byte load per input: a warp reads 128
+// contiguous bytes of each input).  Per scalar the statistics are
+// accumulated sequentially in input order in FP32 (sumSq exceeds 2^24, so
+// the order is part of the result), exactly as the reference.  The sort is a
+// bitonic network on the packed words with __vminu2/__vmaxu2, so one
+// compare-exchange instruction pair sorts both scalars' stacks.  A clipped
+// value, and every slot past the input count, becomes 0xFFFF: the maximum of
+// the type, so the first keptCount sorted positions hold exactly the sorted
+// kept values (ties with a kept 65535 do not change any value there), and
+// the median is element keptCount/2 - the reference's values[count / 2].
 // ---------------------------------------------------------------------------
 struct MedianInputs
 {
@@ -253,7 +261,7 @@ struct MedianInputs
 };
 
 template <int P>
-__device__ __forceinline__ void bitonic_sort(int (&v)[P])
+__device__ __forceinline__ void bitonic_sort_u16x2(uint32_t (&v)[P])
 {
 #pragma unroll
     for (int k = 2; k <= P; k <<= 1)
@@ -262,72 +270,185 @@ __device__ __forceinline__ void bitonic_sort(int (&v)[P])
 #pragma unroll
             for (int i = 0; i < P; ++i)
             {
-                int l = i ^ j;
+                const int l = i ^ j;
                 if (l > i)
                 {
-                    int a = v[i], b = v[l];
-                    int lo = min(a, b), hi = max(a, b);
-                    bool up = (i & k) == 0;
+                    const uint32_t lo = __vminu2(v[i], v[l]), hi = __vmaxu2(v[i], v[l]);
+                    const bool up = (i & k) == 0;
                     v[i] = up ? lo : hi;
                     v[l] = up ? hi : lo;
                 }
             }
 }
 
-template <int P>
-__global__ void __launch_bounds__(256) k_median(MedianInputs in, int n, long long total, float sigma,
-                                                unsigned short* __restrict__ out)
+// Sigma bounds of one scalar's stack (MedianStackKernels.h:22-27).
+__device__ __forceinline__ void clip_bounds(float sum, float sumSq, int n, float sigma, float& lo, float& hi)
 {
-    long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (idx >= total) return;
-    int v[P];
-#pragma unroll
-    for (int i = 0; i < P; ++i) v[i] = i < n ? (int)__ldg(in.p[i] + idx) : 0x7fffffff;
-    int count = n;
+    const float fn = (float)n;
+    const float mean = fdiv(sum, fn);
+    const float var = fsub(fdiv(sumSq, fn), fmul(mean, mean));
+    const float sd = __fsqrt_rn(var < 0.0f ? 0.0f : var);
+    lo = fsub(mean, fmul(sigma, sd));
+    hi = fadd(mean, fmul(sigma, sd));
+}
+
+// The sigma-clipped median of both halves of v[0..n) (v[i] for i >= n must
+// be 0xFFFFFFFF), packed the same way.  v is sorted in place.
+template <int P>
+__device__ __forceinline__ uint32_t median_pair(uint32_t (&v)[P], int n, float sigma)
+{
+    int cntL = n, cntH = n;
     if (n > 3)
     {
-        float sum = 0.0f, sumSq = 0.0f;
+        float sL = 0.0f, qL = 0.0f, sH = 0.0f, qH = 0.0f;
 #pragma unroll
         for (int i = 0; i < P; ++i)
             if (i < n)
             {
-                float f = (float)v[i];
-                sum = fadd(sum, f);
-                sumSq = fadd(sumSq, fmul(f, f));
+                const float a = (float)(v[i] & 0xffffu), b = (float)(v[i] >> 16);
+                sL = fadd(sL, a);
+                qL = fadd(qL, fmul(a, a));
+                sH = fadd(sH, b);
+                qH = fadd(qH, fmul(b, b));
             }
-        float fn = (float)n;
-        float mean = fdiv(sum, fn);
-        float var = fsub(fdiv(sumSq, fn), fmul(mean, mean));
-        float sd = __fsqrt_rn(var < 0.0f ? 0.0f : var);
-        float lo = fsub(mean, fmul(sigma, sd));
-        float hi = fadd(mean, fmul(sigma, sd));
-        int kept = 0;
+        float loL, hiL, loH, hiH;
+        clip_bounds(sL, qL, n, sigma, loL, hiL);
+        clip_bounds(sH, qH, n, sigma, loH, hiH);
+        uint32_t outL = 0, outH = 0;  // bit i: value i is clipped
+        int kL = 0, kH = 0;
 #pragma unroll
         for (int i = 0; i < P; ++i)
             if (i < n)
             {
-                float f = (float)v[i];
-                kept += (f >= lo && f <= hi) ? 1 : 0;
+                const float a = (float)(v[i] & 0xffffu), b = (float)(v[i] >> 16);
+                const bool keepA = a >= loL && a <= hiL, keepB = b >= loH && b <= hiH;
+                kL += keepA ? 1 : 0;
+                kH += keepB ? 1 : 0;
+                outL |= keepA ? 0u : (1u << i);
+                outH |= keepB ? 0u : (1u << i);
             }
-        if (kept > 0)
+        // if nothing is kept the reference keeps every value
+        if (kL == 0) outL = 0;
+        else cntL = kL;
+        if (kH == 0) outH = 0;
+        else cntH = kH;
+#pragma unroll
+        for (int i = 0; i < P; ++i)
         {
-#pragma unroll
-            for (int i = 0; i < P; ++i)
-                if (i < n)
-                {
-                    float f = (float)v[i];
-                    if (!(f >= lo && f <= hi)) v[i] = 0x7fffffff;
-                }
-            count = kept;
+            if ((outL >> i) & 1u) v[i] |= 0x0000ffffu;
+            if ((outH >> i) & 1u) v[i] |= 0xffff0000u;
         }
     }
-    bitonic_sort<P>(v);
-    int m = count >> 1;
-    int r = v[0];
+    bitonic_sort_u16x2<P>(v);
+    const int mL = cntL >> 1, mH = cntH >> 1;
+    uint32_t rL = v[0], rH = v[0];
 #pragma unroll
     for (int i = 1; i < P; ++i)
-        if (i == m) r = v[i];
-    out[idx] = (unsigned short)r;
+    {
+        rL = (i == mL) ? v[i] : rL;
+        rH = (i == mH) ? v[i] : rH;
+    }
+    return (rL & 0x0000ffffu) | (rH & 0xffff0000u);
+}
+
+// Packed path: scalars 2t and 2t+1 of every input (4-byte aligned inputs
+// and output, even scalar count).
+template <int P>
+__global__ void __launch_bounds__(256) k_median2(MedianInputs in, int n, long long pairs, float sigma,
+                                                 uint32_t* __restrict__ out)
+{
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= pairs) return;
+    uint32_t v[P];
+#pragma unroll
+    for (int i = 0; i < P; ++i)
+        v[i] = i < n ? __ldg(reinterpret_cast<const uint32_t*>(in.p[i]) + t) : 0xffffffffu;
+    out[t] = median_pair<P>(v, n, sigma);
+}
+
+// General path (any alignment or odd count): one scalar per thread, in the
+// low half of the packed words.
+template <int P>
+__global__ void __launch_bounds__(256) k_median1(MedianInputs in, int n, long long total, float sigma,
+                                                 unsigned short* __restrict__ out)
+{
+    const long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (idx >= total) return;
+    uint32_t v[P];
+#pragma unroll
+    for (int i = 0; i < P; ++i) v[i] = i < n ? ((uint32_t)__ldg(in.p[i] + idx) | 0xffff0000u) : 0xffffffffu;
+    out[idx] = (unsigned short)(median_pair<P>(v, n, sigma) & 0xffffu);
+}
+
+// ---------------------------------------------------------------------------
+// Warp + median stack fused: the median of n frames each warped onto the
+// same destination grid (IComputeBackend::WarpPerspective of every frame,
+// then MedianStack over the warped buffers: CpuComputeBackend.cpp:112-159).
+// Each destination pixel's n samples are computed with the warp's exact FP32
+// arithmetic and stacked in registers, so the warped frames are never
+// written; a thread makes two horizontally adjacent pixels and stacks their
+// channels as three packed pairs (r, g, b of pixel x in the low halves, of
+// pixel x+1 in the high halves).
+// ---------------------------------------------------------------------------
+struct StackParams
+{
+    const unsigned short* src[kMaxContributors];
+    float H[kMaxContributors][9];
+};
+
+template <int P>
+__global__ void __launch_bounds__(256) k_warp_median(StackParams S, int n, int sw, int sh,
+                                                     unsigned short* __restrict__ dst, int dw, int dh, int offX,
+                                                     int offY, float sigma)
+{
+    const int x = (blockIdx.x * 32 + threadIdx.x) * 2;
+    const int y = blockIdx.y * 8 + threadIdx.y;
+    if (x >= dw || y >= dh) return;
+    const bool two = x + 1 < dw;
+    const float dX = (float)(x + offX), dY = (float)(y + offY);
+    uint32_t r[P], g[P], b[P];
+#pragma unroll
+    for (int i = 0; i < P; ++i)
+    {
+        r[i] = g[i] = b[i] = 0xffffffffu;
+        if (i < n)
+        {
+            WarpParams W;
+#pragma unroll
+            for (int q = 0; q < 9; ++q) W.H[q] = S.H[i][q];
+            W.gain = 1.0f;
+            W.applyGain = 0;
+            unsigned short a[3], c[3] = {0, 0, 0};
+            warp_pixel(S.src[i], sw, sh, W, dX, dY, a);
+            if (two) warp_pixel(S.src[i], sw, sh, W, (float)(x + 1 + offX), dY, c);
+            r[i] = (uint32_t)a[0] | ((uint32_t)c[0] << 16);
+            g[i] = (uint32_t)a[1] | ((uint32_t)c[1] << 16);
+            b[i] = (uint32_t)a[2] | ((uint32_t)c[2] << 16);
+        }
+    }
+    const uint32_t mr = median_pair<P>(r, n, sigma);
+    const uint32_t mg = median_pair<P>(g, n, sigma);
+    const uint32_t mb = median_pair<P>(b, n, sigma);
+    unsigned short* o = dst + ((size_t)y * dw + x) * 3;
+    if (two && ((reinterpret_cast<uintptr_t>(o) & 3) == 0))
+    {
+        uint32_t* o32 = reinterpret_cast<uint32_t*>(o);
+        o32[0] = (mr & 0xffffu) | (mg << 16);
+        o32[1] = (mb & 0xffffu) | (mr & 0xffff0000u);
+        o32[2] = (mg >> 16) | (mb & 0xffff0000u);
+    }
+    else
+    {
+        o[0] = (unsigned short)(mr & 0xffffu);
+        o[1] = (unsigned short)(mg & 0xffffu);
+        o[2] = (unsigned short)(mb & 0xffffu);
+        if (two)
+        {
+            o[3] = (unsigned short)(mr >> 16);
+            o[4] = (unsigned short)(mg >> 16);
+            o[5] = (unsigned short)(mb >> 16);
+        }
+    }
 }
 
 // ---------------------------------------------------------------------------
@@ -398,15 +519,52 @@ int launch_median(const unsigned short* const* inputs, int n, unsigned short* ou
                   cudaStream_t s)
 {
     MedianInputs in;
-    int cnt = n < kMaxContributors ? n : kMaxContributors;
-    for (int i = 0; i < kMaxContributors; ++i) in.p[i] = i < cnt ? inputs[i] : nullptr;
-    long long total = (long long)w * h * 3;
-    unsigned blocks = (unsigned)((total + 255) / 256);
-    if (cnt <= 4) k_median<4><<<blocks, 256, 0, s>>>(in, cnt, total, sigma, out);
-    else if (cnt <= 8) k_median<8><<<blocks, 256, 0, s>>>(in, cnt, total, sigma, out);
-    else if (cnt <= 16) k_median<16><<<blocks, 256, 0, s>>>(in, cnt, total, sigma, out);
-    else k_median<32><<<blocks, 256, 0, s>>>(in, cnt, total, sigma, out);
+    const int cnt = n < kMaxContributors ? n : kMaxContributors;
+    uintptr_t align = reinterpret_cast<uintptr_t>(out);
+    for (int i = 0; i < kMaxContributors; ++i)
+    {
+        in.p[i] = i < cnt ? inputs[i] : nullptr;
+        if (i < cnt) align |= reinterpret_cast<uintptr_t>(inputs[i]);
+    }
+    const long long total = (long long)w * h * 3;
+    if ((total & 1) == 0 && (align & 3) == 0)
+    {
+        const long long pairs = total >> 1;
+        const unsigned blocks = (unsigned)((pairs + 255) / 256);
+        uint32_t* o = reinterpret_cast<uint32_t*>(out);
+        if (cnt <= 4) k_median2<4><<<blocks, 256, 0, s>>>(in, cnt, pairs, sigma, o);
+        else if (cnt <= 8) k_median2<8><<<blocks, 256, 0, s>>>(in, cnt, pairs, sigma, o);
+        else if (cnt <= 16) k_median2<16><<<blocks, 256, 0, s>>>(in, cnt, pairs, sigma, o);
+        else k_median2<32><<<blocks, 256, 0, s>>>(in, cnt, pairs, sigma, o);
+    }
+    else
+    {
+        const unsigned blocks = (unsigned)((total + 255) / 256);
+        if (cnt <= 4) k_median1<4><<<blocks, 256, 0, s>>>(in, cnt, total, sigma, out);
+        else if (cnt <= 8) k_median1<8><<<blocks, 256, 0, s>>>(in, cnt, total, sigma, out);
+        else if (cnt <= 16) k_median1<16><<<blocks, 256, 0, s>>>(in, cnt, total, sigma, out);
+        else k_median1<32><<<blocks, 256, 0, s>>>(in, cnt, total, sigma, out);
+    }
     return check_launch("median kernel");
+}
+
+int launch_warp_median(const unsigned short* const* frames, int n, int sw, int sh, const float* H, unsigned short* out,
+                       int dw, int dh, int offX, int offY, float sigma, cudaStream_t s)
+{
+    StackParams S;
+    const int cnt = n < kMaxContributors ? n : kMaxContributors;
+    for (int i = 0; i < kMaxContributors; ++i)
+    {
+        S.src[i] = i < cnt ? frames[i] : nullptr;
+        for (int q = 0; q < 9; ++q) S.H[i][q] = i < cnt ? H[(size_t)i * 9 + q] : 0.0f;
+    }
+    dim3 grid((unsigned)((dw + 63) / 64), (unsigned)((dh + 7) / 8));
+    dim3 block(32, 8);
+    if (cnt <= 4) k_warp_median<4><<<grid, block, 0, s>>>(S, cnt, sw, sh, out, dw, dh, offX, offY, sigma);
+    else if (cnt <= 8) k_warp_median<8><<<grid, block, 0, s>>>(S, cnt, sw, sh, out, dw, dh, offX, offY, sigma);
+    else if (cnt <= 16) k_warp_median<16><<<grid, block, 0, s>>>(S, cnt, sw, sh, out, dw, dh, offX, offY, sigma);
+    else k_warp_median<32><<<grid, block, 0, s>>>(S, cnt, sw, sh, out, dw, dh, offX, offY, sigma);
+    return check_launch("warp + median kernel");
 }
 
 int launch_gain(unsigned short* data, long long n, float gain, cudaStream_t s)

@@ -366,8 +366,12 @@ int Plan::build(const std::vector<TileSpec>& specs, int numBands, bool renderPat
     return I360B_SUCCESS;
 }
 
-// Lists per chain, kListsPerChain each (index chain * kListsPerChain + list).
-constexpr int kListsPerChain = 3 + (kMaxBands - 1) + kMaxBands + kMaxBands;
+// Lists per chain, kListsPerChain each (index chain * kListsPerChain + list):
+// warp, ownership, level-0 output, down from each level, blend and collapse
+// at each level, then the fused pyramid's level-2 base and fine blocks.
+constexpr int kListBase2 = 3 + (kMaxBands - 1) + kMaxBands + kMaxBands;
+constexpr int kListFine = kListBase2 + 1;
+constexpr int kListsPerChain = kListFine + 1;
 
 void Plan::make_units(int rows, std::vector<Unit>& units)
 {
@@ -390,9 +394,19 @@ void Plan::make_units(int rows, std::vector<Unit>& units)
         auto inT = [&](int t) { return tileChain.empty() || tileChain[t] == c; };
         auto inI = [&](int i) { return inT(items[i].tile); };
         int s;
-        s = beginList();  // 0: coverage / warp
+        s = beginList();  // 0: warp (render path: 128x16 blocks) / coverage (bands)
         for (int i = 0; i < nItems; ++i)
-            if (inI(i)) addBands(i, tiles[items[i].tile].h);
+        {
+            if (!inI(i)) continue;
+            const TileDev& T = tiles[items[i].tile];
+            if (render)
+            {
+                for (int by = 0; by < (T.h + kWarpBlockH - 1) / kWarpBlockH; ++by)
+                    for (int bx = 0; bx < (T.w + kWarpBlockW - 1) / kWarpBlockW; ++bx) units.push_back(Unit{i, bx, by, 0});
+            }
+            else
+                addBands(i, T.h);
+        }
         endList(s);
         s = beginList();  // 1: ownership
         for (int t = 0; t < nTiles; ++t)
@@ -428,6 +442,23 @@ void Plan::make_units(int rows, std::vector<Unit>& units)
                     if (inT(t) && tiles[t].bands > l + 1) addBands(t, tiles[t].lh[l]);
             endList(s);
         }
+        s = beginList();  // kListBase2: level-2 blocks of every contributor of a tile with >= 3 bands
+        for (int i = 0; i < nItems; ++i)
+        {
+            const TileDev& T = tiles[items[i].tile];
+            if (!inI(i) || T.bands < 3) continue;
+            for (int by = 0; by < (T.lh[2] + kBase2H - 1) / kBase2H; ++by)
+                for (int bx = 0; bx < (T.lw[2] + kBase2W - 1) / kBase2W; ++bx) units.push_back(Unit{i, bx, by, 0});
+        }
+        endList(s);
+        s = beginList();  // kListFine: output blocks of every tile
+        for (int t = 0; t < nTiles; ++t)
+        {
+            if (!inT(t)) continue;
+            for (int by = 0; by < (tiles[t].h + kFineH - 1) / kFineH; ++by)
+                for (int bx = 0; bx < (tiles[t].w + kFineW - 1) / kFineW; ++bx) units.push_back(Unit{t, bx, by, 0});
+        }
+        endList(s);
     }
 }
 
@@ -443,6 +474,15 @@ int Plan::set_tuning(int rows, int slots, cudaStream_t s)
     I360B_CUDA(cudaStreamSynchronize(s), "plan tuning");
     bandRows = rows;
     dtSlots = slots;
+    drop_graphs();
+    return I360B_SUCCESS;
+}
+
+int Plan::set_fusion(int levels, cudaStream_t s)
+{
+    if (levels != 0 && levels != 2) return fail(I360B_INVALID_PARAM, "fused pyramid levels must be 0 or 2");
+    I360B_CUDA(cudaStreamSynchronize(s), "plan fusion");
+    fusedLevels = levels;
     drop_graphs();
     return I360B_SUCCESS;
 }
@@ -478,20 +518,29 @@ Plan::~Plan()
     if (arena && ownsArena) cudaFree(arena);
 }
 
+// Stages 5-9 with the fused pyramid: level 0 -> 2 of every contributor;
+// down from level 2; blended bands >= 2; collapse to level 2; level-1 blend,
+// collapse and output.  Materialised: level 0 -> 1; down from level 1; bands
+// >= 1; collapse to level 1; level-0 output.
 const char* const kStageNames[kStages] = {"warp_gain_coverage", "chamfer_forward", "chamfer_backward",
-                                          "ownership",          "seam_dp",         "pyramid_down0",
+                                          "ownership",          "seam_dp",         "pyramid_base",
                                           "pyramid_down",       "blend_bands",     "collapse",
-                                          "level0_output"};
+                                          "fine_output"};
 
 int Plan::kernels_per_execute() const
 {
     int n = (nItems > 0 ? 1 : 0);  // bbox reset
+    const int lo = fusedLevels == 2 ? 2 : 1;
     for (int c = 0; c < nChains; ++c)
     {
         const Range* L = &lists[(size_t)c * kListsPerChain];
         n += (L[0].count > 0 ? 1 : 0) + (dtRange[c].count > 0 ? 2 : 0) + (L[1].count > 0 ? 1 : 0) +
-             (seamRange[c].count > 0 ? 1 : 0) + (L[2].count > 0 ? 1 : 0);
-        for (int i = 3; i < kListsPerChain; ++i) n += L[i].count > 0 ? 1 : 0;
+             (seamRange[c].count > 0 ? 1 : 0);
+        n += fusedLevels == 2 ? (L[kListBase2].count > 0 ? 1 : 0) + (L[kListFine].count > 0 ? 1 : 0)
+                              : (L[3].count > 0 ? 1 : 0) + (L[2].count > 0 ? 1 : 0);
+        for (int l = lo; l < kMaxBands - 1; ++l) n += L[3 + l].count > 0 ? 1 : 0;               // down
+        for (int l = lo; l < kMaxBands; ++l) n += L[3 + (kMaxBands - 1) + l].count > 0 ? 1 : 0;  // blend
+        for (int l = lo; l < kMaxBands; ++l) n += L[3 + 2 * kMaxBands - 1 + l].count > 0 ? 1 : 0;  // collapse
     }
     return n;
 }
@@ -509,6 +558,8 @@ int Plan::enqueue_chain(int c, int first, int last, cudaStream_t s)
 {
     BlendArgs a{dItems, dTiles, dError, dSeamCycles, bandRows, spinLimit};
     const Range* L = &lists[(size_t)c * kListsPerChain];
+    const bool fused = fusedLevels == 2;
+    const int lo = fused ? 2 : 1;  // lowest level the materialised stages handle
     for (int stage = first; stage <= last; ++stage)
     {
         Range r;
@@ -530,31 +581,42 @@ int Plan::enqueue_chain(int c, int first, int last, cudaStream_t s)
         case 4:
             I360B_TRY(launch_seam(a, seamList + seamRange[c].start, seamRange[c].count, s));
             break;
-        case 5:
-        case 6:  // pyramid: level 0 -> 1 (stage 5), then the levels above (stage 6)
-            for (int l = stage == 5 ? 0 : 1; l < (stage == 5 ? 1 : kMaxBands - 1); ++l)
+        case 5:  // pyramid base: level 0 -> 2 (fused) or level 0 -> 1
+            if (fused)
+            {
+                r = L[kListBase2];
+                I360B_TRY(launch_base2(a, dUnits + r.start, r.count, s));
+            }
+            else
+            {
+                r = L[3];
+                I360B_TRY(launch_down(a, dUnits + r.start, r.count, 0, s));
+            }
+            break;
+        case 6:  // the levels above the base
+            for (int l = lo; l < kMaxBands - 1; ++l)
             {
                 r = L[3 + l];
                 I360B_TRY(launch_down(a, dUnits + r.start, r.count, l, s));
             }
             break;
         case 7:
-            for (int l = kMaxBands - 1; l >= 1; --l)
+            for (int l = kMaxBands - 1; l >= lo; --l)
             {
                 r = L[3 + (kMaxBands - 1) + l];
                 I360B_TRY(launch_blend_level(a, dUnits + r.start, r.count, l, s));
             }
             break;
         case 8:
-            for (int l = kMaxBands - 1; l >= 1; --l)
+            for (int l = kMaxBands - 1; l >= lo; --l)
             {
                 r = L[3 + 2 * kMaxBands - 1 + l];
                 I360B_TRY(launch_collapse(a, dUnits + r.start, r.count, l, s));
             }
             break;
-        case 9:
-            r = L[2];
-            I360B_TRY(launch_final0(a, dUnits + r.start, r.count, s));
+        case 9:  // fused: level-1 blend + collapse + output; else the level-0 output
+            r = fused ? L[kListFine] : L[2];
+            I360B_TRY(fused ? launch_fine(a, dUnits + r.start, r.count, s) : launch_final0(a, dUnits + r.start, r.count, s));
             break;
         }
     }
@@ -983,38 +1045,69 @@ extern "C" int i360b_render_plan_autotune(i360b_render_plan* plan, void* stream,
     cudaEvent_t e0 = nullptr, e1 = nullptr;
     I360B_CUDA(cudaEventCreate(&e0), "autotune events");
     I360B_CUDA(cudaEventCreate(&e1), "autotune events");
-    int bestR = P.bandRows, bestS = P.dtSlots;
+    int bestR = P.bandRows, bestS = P.dtSlots, bestF = P.fusedLevels;
     float best = INFINITY;
     int rc = I360B_SUCCESS;
-    for (int rows : {8, 16, 32, 64})
+    for (int fused : {2, 0})
     {
-        for (int slots = 2; slots <= maxSlots && rc == I360B_SUCCESS; ++slots)
+        if ((rc = P.set_fusion(fused, s)) != I360B_SUCCESS) break;
+        for (int rows : {8, 16, 32, 64})
         {
-            if ((rc = P.set_tuning(rows, slots, s)) != I360B_SUCCESS) break;
-            if ((rc = P.execute(s, true)) != I360B_SUCCESS) break;  // capture + warm-up
-            cudaEventRecord(e0, s);
-            for (int k = 0; k < 2 && rc == I360B_SUCCESS; ++k) rc = P.execute(s, true);
-            cudaEventRecord(e1, s);
-            if (rc == I360B_SUCCESS) rc = P.check(s);
-            float ms = 0.0f;
-            cudaEventElapsedTime(&ms, e0, e1);
-            if (rc == I360B_SUCCESS && ms < best)
+            for (int slots = 2; slots <= maxSlots && rc == I360B_SUCCESS; ++slots)
             {
-                best = ms;
-                bestR = rows;
-                bestS = slots;
+                if ((rc = P.set_tuning(rows, slots, s)) != I360B_SUCCESS) break;
+                if ((rc = P.execute(s, true)) != I360B_SUCCESS) break;  // capture + warm-up
+                cudaEventRecord(e0, s);
+                for (int k = 0; k < 2 && rc == I360B_SUCCESS; ++k) rc = P.execute(s, true);
+                cudaEventRecord(e1, s);
+                if (rc == I360B_SUCCESS) rc = P.check(s);
+                float ms = 0.0f;
+                cudaEventElapsedTime(&ms, e0, e1);
+                if (rc == I360B_SUCCESS && ms < best)
+                {
+                    best = ms;
+                    bestR = rows;
+                    bestS = slots;
+                    bestF = fused;
+                }
             }
+            if (rc != I360B_SUCCESS) break;
         }
         if (rc != I360B_SUCCESS) break;
     }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
     if (rc != I360B_SUCCESS) return rc;
+    I360B_TRY(P.set_fusion(bestF, s));
     I360B_TRY(P.set_tuning(bestR, bestS, s));
     if (bandRows) *bandRows = bestR;
     if (dtSlots) *dtSlots = bestS;
     if (bestMs) *bestMs = best / 2.0f;
     return I360B_SUCCESS;
+}
+
+extern "C" int i360b_render_plan_get_tuning(i360b_render_plan* plan, int* bandRows, int* dtSlots, int* fusedLevels)
+{
+    clear_error();
+    if (!plan) return fail(I360B_INVALID_PARAM, "Null plan.");
+    if (bandRows) *bandRows = plan->plan.bandRows;
+    if (dtSlots) *dtSlots = plan->plan.dtSlots;
+    if (fusedLevels) *fusedLevels = plan->plan.fusedLevels;
+    return I360B_SUCCESS;
+}
+
+extern "C" int i360b_render_plan_set_tuning(i360b_render_plan* plan, int bandRows, int dtSlots, int fusedLevels,
+                                            void* stream)
+{
+    clear_error();
+    if (!plan) return fail(I360B_INVALID_PARAM, "Null plan.");
+    I360B_TRY(ensure_ready());
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    const int maxSlots = dt_rows_in_flight(plan->plan.maxW, plan->plan.maxH);
+    if (dtSlots != 0 && (dtSlots < 2 || dtSlots > maxSlots))
+        return fail(I360B_INVALID_PARAM, "dtSlots must be 0 or 2-%d for this plan.", maxSlots);
+    I360B_TRY(plan->plan.set_fusion(fusedLevels, s));
+    return plan->plan.set_tuning(bandRows, dtSlots, s);
 }
 
 extern "C" int i360b_render_plan_set_wait_limit(i360b_render_plan* plan, long long cycles, void* stream)

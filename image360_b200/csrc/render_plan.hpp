@@ -59,6 +59,10 @@ struct Plan
     // Tuning: rows per band unit of the per-pixel kernels (8, 16, 32 or 64)
     // and ring slots of the chamfer transform (0 = as many as fit).
     int bandRows = kBandRows, dtSlots = 0;
+    // Pyramid levels computed on chip (level-fusion depth): 2 = levels 0 and
+    // 1 fused (k_base2 + k_fine, only levels >= 2 in memory), 0 = every level
+    // materialised (k_down0s, k_blend_level / k_collapse at level 1, k_final0).
+    int fusedLevels = 2;
     // Limit of the bounded device waits (SM cycles; 0 = give up at the first
     // wait that is not satisfied at once, a test setting).
     long long spinLimit = kSpinCyclesDefault;
@@ -124,6 +128,8 @@ struct Plan
     // Switches the band height and chamfer ring depth; the next execute
     // recaptures the graph.  Synchronous on `s`.
     int set_tuning(int rows, int slots, cudaStream_t s);
+    // Switches the level-fusion depth (0 or 2); recaptures on next execute.
+    int set_fusion(int levels, cudaStream_t s);
     // Changes the bounded-wait limit; the next execute recaptures the graph.
     int set_wait_limit(long long cycles, cudaStream_t s);
     void drop_graphs();

@@ -13,6 +13,7 @@ copied.
 from __future__ import annotations
 
 import argparse
+import os
 import ctypes as ct
 import math
 import time
@@ -234,12 +235,15 @@ def training_config(base: synth.PanoConfig, seed: int) -> synth.PanoConfig:
 
 
 def train_on_scenes(base: synth.PanoConfig, scenes: int, steps: int, batch: int = 64, lr: float = 1e-3,
-                    seed: int = 1, log=None) -> bn.BlendNet:
-    """Trains a new network on ``scenes`` seeded panoramas of configuration
-    ``base`` (seeds 7000 + 31 k, disjoint from the benchmark's), one scene
-    resident at a time, ``steps`` Adam steps in total."""
+                    seed: int = 1, log=None, resume: str = "") -> bn.BlendNet:
+    """Trains a new network (or the one in checkpoint ``resume``, weights
+    and Adam state) on ``scenes`` seeded panoramas of configuration ``base``
+    (seeds 7000 + 31 k, disjoint from the benchmark's), one scene resident at
+    a time, ``steps`` Adam steps in total."""
     import torch
     net = bn.BlendNet(seed=seed)
+    if resume:
+        net.load_checkpoint(resume)
     done = 0
     for k in range(scenes):
         t0 = time.time()
@@ -268,12 +272,18 @@ def main():
     ap.add_argument("--lr", type=float, default=1e-3)
     ap.add_argument("--scale", type=float, default=1.0, help="scene scale (1 = full-size 24-frame panorama)")
     ap.add_argument("--seed", type=int, default=1)
-    ap.add_argument("--out", default="")
+    ap.add_argument("--out", default="", help="weights (fp32 raw) to write")
+    ap.add_argument("--checkpoint", default="", help="checkpoint (.npz: weights + Adam state) to resume from and "
+                                                     "write back")
     ap.add_argument("--eval", action="store_true", help="learned render + judge of a held-out panorama")
     args = ap.parse_args()
     log = lambda *a: print(*a, flush=True)
     base = synth.C1 if args.scale == 1.0 else synth.scaled(synth.C1, args.scale)
-    net = train_on_scenes(base, args.scenes, args.steps, args.batch, args.lr, args.seed, log)
+    net = train_on_scenes(base, args.scenes, args.steps, args.batch, args.lr, args.seed, log,
+                          resume=args.checkpoint if args.checkpoint and os.path.exists(args.checkpoint) else "")
+    if args.checkpoint:
+        net.save_checkpoint(args.checkpoint)
+        log(f"checkpoint (weights + Adam state) -> {args.checkpoint}")
     if args.out:
         net.get_params().tofile(args.out)
         log(f"weights -> {args.out}")

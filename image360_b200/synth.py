@@ -116,19 +116,50 @@ def geometry(cfg: PanoConfig, rng: np.random.Generator):
     return np.stack(mats), out_w, out_h
 
 
-def render_scene(w: int, h: int, cfg: PanoConfig, rng: np.random.Generator, device) -> torch.Tensor:
-    """(h, w, 3) float32 scene in [0, 1]."""
-    img = torch.zeros((h, w, 3), dtype=torch.float32, device=device)
-    img += torch.tensor(rng.uniform(0.15, 0.35, 3), dtype=torch.float32, device=device)
+def scene_primitives(w: int, h: int, cfg, rng: np.random.Generator) -> dict:
+    """The seeded drawing list of a w x h scene canvas: background colour,
+    anisotropic Gaussian blobs, windowed gratings, hard-edged rectangles (in
+    canvas coordinates, drawn in this order)."""
+    bg = rng.uniform(0.15, 0.35, 3)
     scale = min(w, h)
+    blobs, grats, rects = [], [], []
     for _ in range(cfg.n_blobs):
         cx, cy = rng.uniform(0, w), rng.uniform(0, h)
         sx, sy = rng.uniform(0.01, 0.12) * scale, rng.uniform(0.01, 0.12) * scale
         th = rng.uniform(0, math.pi)
-        amp = torch.tensor(rng.uniform(-0.25, 0.45, 3), dtype=torch.float32, device=device)
+        amp = rng.uniform(-0.25, 0.45, 3)
+        blobs.append((cx, cy, sx, sy, th, amp))
+    for _ in range(cfg.n_gratings):
+        cx, cy = rng.uniform(0, w), rng.uniform(0, h)
+        rad = rng.uniform(0.05, 0.25) * scale
+        period = rng.uniform(4.0, 64.0)
+        th = rng.uniform(0, math.pi)
+        amp = float(rng.uniform(0.05, 0.2))
+        grats.append((cx, cy, rad, period, th, amp))
+    for _ in range(cfg.n_rects):
+        rw, rh = rng.uniform(0.005, 0.08) * scale, rng.uniform(0.005, 0.08) * scale
+        x0 = int(rng.uniform(0, w)); y0 = int(rng.uniform(0, h))
+        x1, y1 = int(min(w, x0 + rw + 1)), int(min(h, y0 + rh + 1))
+        rects.append((x0, y0, x1, y1, rng.uniform(0.0, 0.9, 3)))
+    return {"w": w, "h": h, "bg": bg, "blobs": blobs, "gratings": grats, "rects": rects}
+
+
+def rasterize(prims: dict, wx: int, wy: int, ww: int, wh: int, device) -> torch.Tensor:
+    """(wh, ww, 3) float32 of the scene over canvas window [wx, wx+ww) x
+    [wy, wy+wh): every primitive is a function of canvas coordinates, so any
+    window equals the same crop of the whole canvas."""
+    w, h = prims["w"], prims["h"]
+    img = torch.zeros((wh, ww, 3), dtype=torch.float32, device=device)
+    img += torch.tensor(prims["bg"], dtype=torch.float32, device=device)
+
+    def clip(x0, x1, y0, y1):
+        return max(x0, wx), min(x1, wx + ww), max(y0, wy), min(y1, wy + wh)
+
+    for cx, cy, sx, sy, th, amp in prims["blobs"]:
         rad = 3.0 * max(sx, sy)
         x0, x1 = int(max(0, cx - rad)), int(min(w, cx + rad + 1))
         y0, y1 = int(max(0, cy - rad)), int(min(h, cy + rad + 1))
+        x0, x1, y0, y1 = clip(x0, x1, y0, y1)
         if x1 <= x0 or y1 <= y0:
             continue
         yy, xx = torch.meshgrid(torch.arange(y0, y1, device=device, dtype=torch.float32) - cy,
@@ -136,28 +167,29 @@ def render_scene(w: int, h: int, cfg: PanoConfig, rng: np.random.Generator, devi
         u = xx * math.cos(th) + yy * math.sin(th)
         v = -xx * math.sin(th) + yy * math.cos(th)
         g = torch.exp(-0.5 * ((u / sx) ** 2 + (v / sy) ** 2))
-        img[y0:y1, x0:x1] += g[..., None] * amp
-    for _ in range(cfg.n_gratings):
-        cx, cy = rng.uniform(0, w), rng.uniform(0, h)
-        rad = rng.uniform(0.05, 0.25) * scale
-        period = rng.uniform(4.0, 64.0)
-        th = rng.uniform(0, math.pi)
-        amp = float(rng.uniform(0.05, 0.2))
+        img[y0 - wy:y1 - wy, x0 - wx:x1 - wx] += g[..., None] * torch.tensor(amp, dtype=torch.float32, device=device)
+    for cx, cy, rad, period, th, amp in prims["gratings"]:
         x0, x1 = int(max(0, cx - rad)), int(min(w, cx + rad + 1))
         y0, y1 = int(max(0, cy - rad)), int(min(h, cy + rad + 1))
+        x0, x1, y0, y1 = clip(x0, x1, y0, y1)
         if x1 <= x0 or y1 <= y0:
             continue
         yy, xx = torch.meshgrid(torch.arange(y0, y1, device=device, dtype=torch.float32) - cy,
                                 torch.arange(x0, x1, device=device, dtype=torch.float32) - cx, indexing="ij")
         win = torch.exp(-0.5 * (xx ** 2 + yy ** 2) / (0.4 * rad) ** 2)
         s = torch.sin(2 * math.pi * (xx * math.cos(th) + yy * math.sin(th)) / period)
-        img[y0:y1, x0:x1] += (amp * win * s)[..., None]
-    for _ in range(cfg.n_rects):
-        rw, rh = rng.uniform(0.005, 0.08) * scale, rng.uniform(0.005, 0.08) * scale
-        x0 = int(rng.uniform(0, w)); y0 = int(rng.uniform(0, h))
-        x1, y1 = int(min(w, x0 + rw + 1)), int(min(h, y0 + rh + 1))
-        img[y0:y1, x0:x1] = torch.tensor(rng.uniform(0.0, 0.9, 3), dtype=torch.float32, device=device)
+        img[y0 - wy:y1 - wy, x0 - wx:x1 - wx] += (amp * win * s)[..., None]
+    for x0, y0, x1, y1, col in prims["rects"]:
+        x0, x1, y0, y1 = clip(x0, x1, y0, y1)
+        if x1 <= x0 or y1 <= y0:
+            continue
+        img[y0 - wy:y1 - wy, x0 - wx:x1 - wx] = torch.tensor(col, dtype=torch.float32, device=device)
     return img.clamp_(0.0, 1.0)
+
+
+def render_scene(w: int, h: int, cfg, rng: np.random.Generator, device) -> torch.Tensor:
+    """(h, w, 3) float32 scene in [0, 1]."""
+    return rasterize(scene_primitives(w, h, cfg, rng), 0, 0, w, h, device)
 
 
 def _sample_bilinear(scene: torch.Tensor, X: torch.Tensor, Y: torch.Tensor) -> torch.Tensor:
@@ -259,7 +291,11 @@ def uneven_tiles(n_tiles: int, n_frames: int, frame_w: int, frame_h: int, focal:
                        to_canvas=np.stack(mats), tiles=tiles)
 
 
-def make_panorama(cfg: PanoConfig, device="cpu", with_cfa: bool = True) -> Panorama:
+def make_panorama(cfg: PanoConfig, device="cpu", with_cfa: bool = True, frames=None) -> Panorama:
+    """The panorama's geometry and tiles, and the CFA of every frame (or only
+    of the frame indices in `frames`; the others are None).  Each frame is
+    sampled from the scene rasterised over its own canvas footprint and has
+    its own noise seed, so a frame is the same whichever others are made."""
     rng = np.random.default_rng(cfg.seed)
     mats, W, H = geometry(cfg, rng)
     gains = rng.uniform(cfg.gain_lo, cfg.gain_hi, len(mats))
@@ -268,21 +304,117 @@ def make_panorama(cfg: PanoConfig, device="cpu", with_cfa: bool = True) -> Panor
     if not with_cfa:
         return pano
     pad = 64
-    scene = render_scene(W + 2 * pad, H + 2 * pad, cfg, rng, device)
-    gen = torch.Generator(device=device)
-    gen.manual_seed(cfg.seed)
+    prims = scene_primitives(W + 2 * pad, H + 2 * pad, cfg, rng)
+    want = set(range(len(mats))) if frames is None else {int(f) for f in frames}
     yy, xx = torch.meshgrid(torch.arange(cfg.frame_h, device=device, dtype=torch.float64),
                             torch.arange(cfg.frame_w, device=device, dtype=torch.float64), indexing="ij")
     for k, Hm in enumerate(mats):
+        if k not in want:
+            pano.cfa.append(None)
+            continue
         Ht = torch.tensor(Hm, dtype=torch.float64, device=device)
         den = Ht[2, 0] * xx + Ht[2, 1] * yy + Ht[2, 2]
-        X = ((Ht[0, 0] * xx + Ht[0, 1] * yy + Ht[0, 2]) / den + pad).float()
-        Y = ((Ht[1, 0] * xx + Ht[1, 1] * yy + Ht[1, 2]) / den + pad).float()
-        frame = _sample_bilinear(scene, X, Y)
+        Xc = (Ht[0, 0] * xx + Ht[0, 1] * yy + Ht[0, 2]) / den + pad
+        Yc = (Ht[1, 0] * xx + Ht[1, 1] * yy + Ht[1, 2]) / den + pad
+        wx0 = max(0, int(math.floor(float(Xc.min()))) - 2)
+        wy0 = max(0, int(math.floor(float(Yc.min()))) - 2)
+        wx1 = min(W + 2 * pad, int(math.ceil(float(Xc.max()))) + 3)
+        wy1 = min(H + 2 * pad, int(math.ceil(float(Yc.max()))) + 3)
+        scene = rasterize(prims, wx0, wy0, wx1 - wx0, wy1 - wy0, device)
+        frame = _sample_bilinear(scene, (Xc - wx0).float(), (Yc - wy0).float())
+        gen = torch.Generator(device=device)
+        gen.manual_seed(cfg.seed * 1009 + k)
         pano.cfa.append(mosaic(frame, cfg, float(gains[k]), gen))
-        del frame, X, Y, den
-    del scene
+        del frame, Xc, Yc, den, scene
     return pano
+
+
+@dataclass
+class StackConfig:
+    """A burst of frames of one view for the median stack: each frame is the
+    reference view moved by a near-identity homography (rotation about the
+    frame centre, translation), with transient outlier rectangles."""
+    frame_w: int
+    frame_h: int
+    frames: int
+    bits: int
+    black: int
+    sigma_read: float
+    max_shift: float = 3.0       # translation U(-max_shift, max_shift) px per axis
+    max_rot_deg: float = 0.2     # rotation U(-max_rot_deg, max_rot_deg)
+    outlier_frac: float = 0.05   # fraction of each frame's pixels inside outlier rectangles
+    n_blobs: int = 200
+    n_gratings: int = 50
+    n_rects: int = 100
+    seed: int = 20260710
+    # sensor of the burst (the panorama workload's)
+    gain_lo: float = 1.0
+    gain_hi: float = 1.0
+    jitter_deg: float = 0.0
+    margin: int = 0
+
+
+# Median stack plus warp: 16 frames of 4000x3000, 14-bit RGGB (black 512,
+# sigma_read 3 DN as the panorama workload), one exposure.
+C2 = StackConfig(frame_w=4000, frame_h=3000, frames=16, bits=14, black=512, sigma_read=3.0)
+
+
+def scaled_stack(cfg: StackConfig, s: float, **kw) -> StackConfig:
+    d = dict(cfg.__dict__)
+    d.update(frame_w=max(8, int(round(cfg.frame_w * s))), frame_h=max(8, int(round(cfg.frame_h * s))),
+             n_blobs=max(4, int(cfg.n_blobs * s * 4)), n_gratings=max(2, int(cfg.n_gratings * s * 4)),
+             n_rects=max(4, int(cfg.n_rects * s * 4)))
+    d.update(kw)
+    return StackConfig(**d)
+
+
+@dataclass
+class Stack:
+    cfg: StackConfig
+    to_ref: np.ndarray      # (n, 3, 3) float64, frame pixel -> reference-grid pixel
+    cfa: list = field(default_factory=list)         # n x (h, w) uint16 tensors
+    outlier_frac: list = field(default_factory=list)  # measured fraction per frame
+
+
+def make_stack(cfg: StackConfig, device="cpu") -> Stack:
+    """The burst: one scene canvas, frame k = the view through
+    H_k = T(t_k) R(theta_k) about the centre, with rectangles of value 1.0
+    (white) over about cfg.outlier_frac of its pixels, mosaicked to RGGB."""
+    rng = np.random.default_rng(cfg.seed)
+    w, h = cfg.frame_w, cfg.frame_h
+    pad = int(math.ceil(cfg.max_shift + 0.01 * max(w, h))) + 8
+    scene_cfg = PanoConfig(frame_w=w, frame_h=h, rows=1, cols=1, overlap=0.0, focal=1.0, bits=cfg.bits,
+                           black=cfg.black, gain_lo=1.0, gain_hi=1.0, sigma_read=cfg.sigma_read, tile=w, bands=1,
+                           n_blobs=cfg.n_blobs, n_gratings=cfg.n_gratings, n_rects=cfg.n_rects, seed=cfg.seed)
+    scene = render_scene(w + 2 * pad, h + 2 * pad, scene_cfg, rng, device)
+    gen = torch.Generator(device=device)
+    gen.manual_seed(cfg.seed)
+    yy, xx = torch.meshgrid(torch.arange(h, device=device, dtype=torch.float64),
+                            torch.arange(w, device=device, dtype=torch.float64), indexing="ij")
+    st = Stack(cfg=cfg, to_ref=np.zeros((cfg.frames, 3, 3)))
+    cx, cy = (w - 1) / 2.0, (h - 1) / 2.0
+    for k in range(cfg.frames):
+        th = math.radians(rng.uniform(-cfg.max_rot_deg, cfg.max_rot_deg))
+        tx, ty = rng.uniform(-cfg.max_shift, cfg.max_shift, 2)
+        c, s_ = math.cos(th), math.sin(th)
+        H = np.array([[c, -s_, cx - c * cx + s_ * cy + tx], [s_, c, cy - s_ * cx - c * cy + ty], [0.0, 0.0, 1.0]])
+        st.to_ref[k] = H
+        X = (H[0, 0] * xx + H[0, 1] * yy + H[0, 2] + pad).float()
+        Y = (H[1, 0] * xx + H[1, 1] * yy + H[1, 2] + pad).float()
+        frame = _sample_bilinear(scene, X, Y)
+        mask = torch.zeros((h, w), dtype=torch.bool, device=device)
+        target = cfg.outlier_frac * w * h
+        while int(mask.sum()) < target:
+            rw = int(rng.integers(max(2, w // 100), max(3, w // 12)))
+            rh = int(rng.integers(max(2, h // 100), max(3, h // 12)))
+            x0, y0 = int(rng.integers(0, w - rw + 1)), int(rng.integers(0, h - rh + 1))
+            mask[y0:y0 + rh, x0:x0 + rw] = True
+        frame[mask] = 1.0
+        st.outlier_frac.append(float(mask.float().mean()))
+        st.cfa.append(mosaic(frame, scene_cfg, 1.0, gen))
+        del frame, X, Y, mask
+    del scene
+    return st
 
 
 def demosaic_params(cfg: PanoConfig):

@@ -151,6 +151,18 @@ I360B_API int i360b_launch_warp(const unsigned short* dSrc, int srcW, int srcH, 
 I360B_API int i360b_launch_median(const unsigned short* const* dInputs, int numInputs, unsigned short* dOutput, int width,
                         int height, float sigmaThreshold, void* stream);
 
+/* The median stack of a burst: WarpPerspective of every frame onto one
+ * dstW x dstH grid (homographies: numFrames * 9 floats, each dst->src
+ * row-major as WarpPerspective takes it; offsets added to every destination
+ * coordinate), then MedianStack over the warped frames
+ * (CpuComputeBackend.cpp:112-159, MedianStackKernels.h:19-55), in one pass
+ * that never writes the warped frames: the result equals those two
+ * operations bit for bit.  dFrames is a HOST array of numFrames (1-32)
+ * device RGB48 frames of srcW x srcH. */
+I360B_API int i360b_launch_warp_median(const unsigned short* const* dFrames, int numFrames, int srcW, int srcH,
+                                       const float* homographies, unsigned short* dOutput, int dstW, int dstH,
+                                       int offsetX, int offsetY, float sigmaThreshold, void* stream);
+
 /* ApplyGain on a device buffer. */
 I360B_API int i360b_launch_gain(unsigned short* dData, int numValues, float gain, void* stream);
 
@@ -384,19 +396,33 @@ typedef struct i360b_render_stats
 I360B_API int i360b_render_plan_stats(i360b_render_plan* plan, void* stream, i360b_render_stats* out);
 /* Runs the plan once without the graph, timing each stage with CUDA events on
  * `stream`; stageMs receives up to maxStages values (10 stages, names from
- * i360b_render_stage_name).  Synchronous. */
+ * i360b_render_stage_name; stages 5-9 are the pyramid base, the levels above
+ * it, the blended bands, the collapse and the fine levels with the output,
+ * whose split depends on the level-fusion depth).  Synchronous. */
 I360B_API int i360b_render_plan_profile(i360b_render_plan* plan, void* stream, float* stageMs, int maxStages);
 I360B_API const char* i360b_render_stage_name(int stage);
 /* Autotuner: times the plan's own execute (two runs after a warm-up, CUDA
- * events on `stream`) for every band-unit height of the per-pixel kernels
- * (8, 16, 32, 64 rows) and every ring depth of the chamfer transform that
- * fits (2 to 4 row groups), and keeps the fastest.  The output of every
+ * events on `stream`) for both level-fusion depths (0, 2), every band-unit
+ * height of the per-pixel kernels (8, 16, 32, 64 rows) and every ring depth
+ * of the chamfer transform that fits (2 to 4 row groups), and keeps the
+ * fastest (read the fusion depth back with i360b_render_plan_get_tuning).  The output of every
  * setting is identical (the settings only partition the same work), so
  * tuning never changes results.  The chosen values and the best time of one
  * execute are returned when the pointers are non-null.  Synchronous; the
  * plan's outputs are overwritten with its render. */
 I360B_API int i360b_render_plan_autotune(i360b_render_plan* plan, void* stream, int* bandRows, int* dtSlots,
                                          float* bestMs);
+/* The plan's tuning: rows per band unit of the per-pixel kernels (8, 16, 32
+ * or 64), chamfer ring slots (0 = as many as fit, else 2 to the number that
+ * fits), and the level-fusion depth of the pyramid: 2 computes levels 0 and
+ * 1 on chip (only levels >= 2 of the pyramids are written to memory), 0
+ * materialises every level.  Every setting renders the same bits.  No
+ * reference counterpart (the reference's blend is a fixed CPU loop).
+ * set_tuning is synchronous on `stream`; the next execute recaptures the
+ * plan's graph.  The autotuner searches all three. */
+I360B_API int i360b_render_plan_get_tuning(i360b_render_plan* plan, int* bandRows, int* dtSlots, int* fusedLevels);
+I360B_API int i360b_render_plan_set_tuning(i360b_render_plan* plan, int bandRows, int dtSlots, int fusedLevels,
+                                           void* stream);
 /* i360b_launch_export_preview over the plan's tiles in tile order (tiles that
  * list no contributor have no render output and are skipped). */
 I360B_API int i360b_render_plan_export_preview(i360b_render_plan* plan, int totalW, int totalH, int maxDimension,

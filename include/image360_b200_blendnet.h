@@ -73,6 +73,13 @@ I360B_API int i360b_blendnet_create(unsigned long long seed, i360b_blendnet** ou
 I360B_API void i360b_blendnet_destroy(i360b_blendnet* net);
 I360B_API int i360b_blendnet_get_params(i360b_blendnet* net, float* hostParams, int count);
 I360B_API int i360b_blendnet_set_params(i360b_blendnet* net, const float* hostParams, int count);
+/* The optimiser state for checkpoints: Adam's first and second moments
+ * (param_count floats each) and the step count its bias correction uses.
+ * Saving it with the weights lets a resumed training continue exactly where
+ * it stopped.  Synchronous. */
+I360B_API int i360b_blendnet_get_adam(i360b_blendnet* net, float* hostM, float* hostV, int count, int* step);
+I360B_API int i360b_blendnet_set_adam(i360b_blendnet* net, const float* hostM, const float* hostV, int count,
+                                      int step);
 /* Forward pass of `n` windows of w x h; writes the 4 logits per pixel as fp32
  * [n][h][w][4] to dLogits.  Synchronous. */
 I360B_API int i360b_blendnet_logits(i360b_blendnet* net, const i360b_blend_job* jobs, int n, int w, int h,

@@ -274,6 +274,35 @@ def test_training_lowers_the_loss(backend):
     net.close()
 
 
+def test_checkpoint_resumes_training_exactly(backend, tmp_path):
+    """A checkpoint holds the weights and the Adam state (moments and step):
+    training 3 steps, saving, training 3 more equals loading the checkpoint
+    into a fresh network and training the same 3 steps."""
+    from image360_b200 import blendnet as bn
+    n, h, w = 2, 16, 256
+    layers = _layers(43, n, h, w)
+    target = _owner_target(layers)
+    dl, dt, _, jobs = _device_batch(layers, target)
+    a = bn.BlendNet(seed=6)
+    for _ in range(3):
+        a.train_step(jobs, n, w, h, 1e-3)
+    ck = str(tmp_path / "net.npz")
+    a.save_checkpoint(ck)
+    m, v, st = a.get_adam()
+    assert st == 3 and np.abs(m).max() > 0 and np.abs(v).max() > 0
+    for _ in range(3):
+        a.train_step(jobs, n, w, h, 1e-3)
+    b = bn.BlendNet(seed=99)
+    b.load_checkpoint(ck)
+    assert b.get_adam()[2] == 3
+    for _ in range(3):
+        b.train_step(jobs, n, w, h, 1e-3)
+    pa, pb = a.get_params(), b.get_params()
+    assert np.allclose(pa, pb, rtol=1e-6, atol=1e-9), float(np.abs(pa - pb).max())
+    a.close()
+    b.close()
+
+
 def test_invalid_windows_are_rejected(backend):
     from image360_b200 import blendnet as bn
     net = bn.BlendNet(seed=5)
