@@ -407,7 +407,62 @@ def run_ours(args, rank, world, local_rank):
         line["cpu_baseline"] = cpu_baseline(S, args)
     if not args.no_parity:
         line["parity"] = parity_check(S, sp)
+    if not args.no_native:
+        line["native_fp16"] = run_native(args, S, stream, step)
     return line
+
+
+def run_native(args, S, stream, step):
+    """The native mode of the same step: the render's stored pyramid levels in
+    FP16 (FP32 arithmetic), timed like the headline, and its error against
+    the FP64 restatement of the blend (the oracle's compose in FP64 on the
+    same warped contributors and owner map) on two seeded tiles with several
+    contributors.  The plan goes back to the exact mode afterwards."""
+    import torch
+
+    import oracle
+    from image360_b200 import PRECISION_EXACT, PRECISION_FP16, synth
+    plan, pano, cfg = S["plan"], S["pano"], S["cfg"]
+    sp = stream.cuda_stream
+    assert plan.set_precision(PRECISION_FP16, sp) == 0
+    with torch.cuda.stream(stream):
+        for _ in range(args.warmup):
+            step()
+        t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        t0.record(stream)
+        for _ in range(args.steps):
+            step()
+        t1.record(stream)
+    torch.cuda.synchronize()
+    assert plan.wait(sp) == 0
+    ms = t0.elapsed_time(t1) / args.steps
+    stages = plan.profile(sp)
+    O = oracle.oracle()
+    rng = np.random.default_rng(9)
+    multi = [i for i, t in enumerate(pano.tiles) if len(t[4]) >= 3] or list(range(len(pano.tiles)))
+    pick = sorted(int(i) for i in rng.permutation(multi)[:2])
+    gains = (1.0 / pano.gains).astype(np.float32)
+    errs = []
+    for i in pick:
+        x, y, w, h, cs = pano.tiles[i]
+        got = S["outs"][i].cpu().numpy().view(np.uint16)
+        bufs = [O.gain(O.warp(S["rgb"][k].cpu().numpy().view(np.uint16), w, h,
+                              synth.inverse_homography_f32(pano.to_canvas[k]), x, y), gains[k]) for k in cs]
+        _, owner = O.blend(bufs, cfg.bands, return_owner=True)
+        ref = O.compose(bufs, None, owner, cfg.bands, f64=True)
+        d = np.abs(got.astype(np.int64) - ref.astype(np.int64))
+        errs.append((int(d.max()), float(d.mean())))
+    assert plan.set_precision(PRECISION_EXACT, sp) == 0
+    with torch.cuda.stream(stream):
+        assert plan.execute(sp) == 0 and plan.wait(sp) == 0
+    torch.cuda.synchronize()
+    out_px = sum(t[2] * t[3] for t in pano.tiles)
+    return {"value": round(out_px / 1e6 / (ms / 1e3), 2), "unit": UNIT, "ms_per_step": round(ms, 3),
+            "storage": "pyramid levels >= 2 in FP16 (num / 256, den, weight), FP32 arithmetic; warped pixels u16",
+            "stages_ms": {k: round(v, 3) for k, v in stages.items()},
+            "error_vs_fp64": {"tiles": [pano.tiles[i][:4] for i in pick], "max_dn": max(e[0] for e in errs),
+                              "mean_dn": round(float(np.mean([e[1] for e in errs])), 5),
+                              "reference": "oracle FP64 compose on the same warped contributors and owner map"}}
 
 
 def parity_check(S, sp):
@@ -1158,6 +1213,7 @@ def main():
     ap.add_argument("--no-stack", action="store_true", help="skip the median-stack leg")
     ap.add_argument("--no-uneven", action="store_true", help="skip the 256 uneven-tile leg")
     ap.add_argument("--no-parity", action="store_true", help="skip the full-panorama check against the CPU code")
+    ap.add_argument("--no-native", action="store_true", help="skip the FP16-storage (native mode) leg")
     ap.add_argument("--no-autotune", action="store_true", help="keep the plan's default band height and ring depth")
     ap.add_argument("--train-steps", type=int, default=782, help="Adam steps (782 x 64 = 50k windows)")
     ap.add_argument("--train-batch", type=int, default=64)

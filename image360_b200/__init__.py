@@ -133,6 +133,7 @@ def load_library(path: str = LIB_PATH):
     L.i360b_render_plan_set_wait_limit.argtypes = [vp, ct.c_longlong, vp]
     L.i360b_render_plan_get_tuning.argtypes = [vp, _i32p, _i32p, _i32p]
     L.i360b_render_plan_set_tuning.argtypes = [vp, i, i, i, vp]
+    L.i360b_render_plan_set_precision.argtypes = [vp, i, vp]
     L.i360b_debug_inject_failure.argtypes = [i, i]
     _lib = L
     return L
@@ -363,6 +364,8 @@ class B200ComputeBackend:
                                                          stream or None))
 
 
+PRECISION_EXACT = 0
+PRECISION_FP16 = 1
 INJECT_ALLOC = 1
 INJECT_LAUNCH = 2
 
@@ -541,6 +544,11 @@ class RenderPlan:
         r, k, f = ct.c_int(), ct.c_int(), ct.c_int()
         self.lib.i360b_render_plan_get_tuning(self._h, ct.byref(r), ct.byref(k), ct.byref(f))
         return {"band_rows": r.value, "dt_slots": k.value, "fused_levels": f.value}
+
+    def set_precision(self, mode: int, stream: int = 0) -> ComputeResult:
+        """PRECISION_EXACT (FP32 pyramid levels, bit-exact) or PRECISION_FP16
+        (stored levels in FP16, FP32 arithmetic: the native mode)."""
+        return ComputeResult(self.lib.i360b_render_plan_set_precision(self._h, int(mode), stream or None))
 
     def set_tuning(self, band_rows: int = 16, dt_slots: int = 0, fused_levels: int = 2,
                    stream: int = 0) -> ComputeResult:

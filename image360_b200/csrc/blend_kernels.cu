@@ -4,6 +4,7 @@
 #include "blend_kernels.cuh"
 
 #include <cuda/atomic>
+#include <cuda_fp16.h>
 #include <cfloat>
 
 namespace i360b
@@ -1310,6 +1311,41 @@ __device__ __forceinline__ float3 gauss_of(float4 nd)
     return make_float3(fmul(nd.x, inv), fmul(nd.y, inv), fmul(nd.z, inv));
 }
 
+// A contributor's pyramid value (num.rgb, den) and weight at index q of a
+// materialised level.  Exact mode: FP32 as computed.  FP16 storage (the
+// native mode): the same buffers hold half4 (num / 256, den) and a half
+// weight - num is scaled by 2^-8 (exactly) so that sums of 16-bit samples
+// stay inside the half range; all arithmetic stays FP32.
+__device__ __forceinline__ float4 nd_at(const float4* nd, size_t q, int half)
+{
+    if (!half) return __ldg(nd + q);
+    const uint2 v = __ldg(reinterpret_cast<const uint2*>(nd) + q);
+    const float2 a = __half22float2(*reinterpret_cast<const __half2*>(&v.x));
+    const float2 b = __half22float2(*reinterpret_cast<const __half2*>(&v.y));
+    return make_float4(a.x * 256.0f, a.y * 256.0f, b.x * 256.0f, b.y);
+}
+
+__device__ __forceinline__ float wg_at(const float* wg, size_t q, int half)
+{
+    if (!half) return __ldg(wg + q);
+    return __half2float(__ushort_as_half(__ldg(reinterpret_cast<const unsigned short*>(wg) + q)));
+}
+
+__device__ __forceinline__ void pyr_store(float4* nd, float* wg, size_t q, float4 v, float w, int half)
+{
+    if (!half)
+    {
+        nd[q] = v;
+        wg[q] = w;
+        return;
+    }
+    const __half2 a = __floats2half2_rn(v.x * (1.0f / 256.0f), v.y * (1.0f / 256.0f));
+    const __half2 b = __floats2half2_rn(v.z * (1.0f / 256.0f), v.w);
+    reinterpret_cast<uint2*>(nd)[q] = make_uint2(*reinterpret_cast<const uint32_t*>(&a),
+                                                 *reinterpret_cast<const uint32_t*>(&b));
+    reinterpret_cast<unsigned short*>(wg)[q] = __half_as_ushort(__float2half_rn(w));
+}
+
 // Blur + decimate one level (SeamBlend.cpp:60-79) for num(3), den and weight
 // together.  A CTA makes a 32x8 block of level l+1 from a 68x20 footprint of
 // level l staged in shared memory with replicated borders.
@@ -1343,13 +1379,11 @@ __global__ void __launch_bounds__(256) k_down(BlendArgs a, const Unit* __restric
             const int X = X0 + (idx & (kDnTW - 1)), Y = Y0 + idx / kDnTW;
             if (X >= dw || Y >= dh) continue;
             const size_t q = T.loff[level + 1] + (size_t)Y * dw + X;
-            it.nd[q] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-            it.wg[q] = 0.0f;
+            pyr_store(it.nd, it.wg, q, make_float4(0.0f, 0.0f, 0.0f, 0.0f), 0.0f, a.half);
         }
         return;
     }
-    const float4* ndS = it.nd + T.loff[level];
-    const float* wgS = it.wg + T.loff[level];
+    const size_t lq = T.loff[level];
     for (int idx = tid; idx < HW * kDnSH; idx += 256)
     {
         const int r = idx / HW, cp = idx - r * HW;
@@ -1360,12 +1394,12 @@ __global__ void __launch_bounds__(256) k_down(BlendArgs a, const Unit* __restric
             const int gx = min(max(2 * X0 - 2 + 2 * cp + e, 0), sw - 1);
             const size_t p = (size_t)gy * sw + gx;
             float v[5];
-            const float4 q = ndS[p];
+            const float4 q = nd_at(it.nd, lq + p, a.half);
             v[0] = q.x;
             v[1] = q.y;
             v[2] = q.z;
             v[3] = q.w;
-            v[4] = wgS[p];
+            v[4] = wg_at(it.wg, lq + p, a.half);
 #pragma unroll
             for (int ch = 0; ch < 5; ++ch)
             {
@@ -1396,8 +1430,7 @@ __global__ void __launch_bounds__(256) k_down(BlendArgs a, const Unit* __restric
             o[ch] = blur5(t[ch][2 * j][i], t[ch][2 * j + 1][i], t[ch][2 * j + 2][i], t[ch][2 * j + 3][i],
                           t[ch][2 * j + 4][i]);
         const size_t q = T.loff[level + 1] + (size_t)Y * dw + X;
-        it.nd[q] = make_float4(o[0], o[1], o[2], o[3]);
-        it.wg[q] = o[4];
+        pyr_store(it.nd, it.wg, q, make_float4(o[0], o[1], o[2], o[3]), o[4], a.half);
     }
 }
 
@@ -1594,7 +1627,7 @@ __global__ void __launch_bounds__(256, 4) k_down0s(BlendArgs a, const Unit* __re
 }
 
 // One pixel of a blended band (the general path).
-__device__ __noinline__ void blend_pixel(const TileDev& T, const ItemCache& C, int level, int K, long long pl)
+__device__ __noinline__ void blend_pixel(const TileDev& T, const ItemCache& C, int level, int K, long long pl, int half)
 {
     const int lw = T.lw[level];
     const bool top = level == T.bands - 1;
@@ -1608,15 +1641,15 @@ __device__ __noinline__ void blend_pixel(const TileDev& T, const ItemCache& C, i
     {
         const int4 B = C.box[k];
         if (x < B.x || x > B.z || y < B.y || y > B.w) continue;  // weight 0: the term is +-0
-        float wv = __ldg(C.wg[k] + p);
-        float3 g = gauss_of(C.nd[k][p]);
+        float wv = wg_at(C.wg[k], p, half);
+        float3 g = gauss_of(nd_at(C.nd[k], p, half));
         if (!top)
         {
-            const float4* up = C.nd[k] + T.loff[level + 1];
-            float3 a00 = gauss_of(up[(size_t)c.y0 * uw + c.x0]);
-            float3 a10 = gauss_of(up[(size_t)c.y0 * uw + c.x1]);
-            float3 a01 = gauss_of(up[(size_t)c.y1 * uw + c.x0]);
-            float3 a11 = gauss_of(up[(size_t)c.y1 * uw + c.x1]);
+            const size_t up = T.loff[level + 1];
+            float3 a00 = gauss_of(nd_at(C.nd[k], up + (size_t)c.y0 * uw + c.x0, half));
+            float3 a10 = gauss_of(nd_at(C.nd[k], up + (size_t)c.y0 * uw + c.x1, half));
+            float3 a01 = gauss_of(nd_at(C.nd[k], up + (size_t)c.y1 * uw + c.x0, half));
+            float3 a11 = gauss_of(nd_at(C.nd[k], up + (size_t)c.y1 * uw + c.x1, half));
             g.x = fsub(g.x, up_mix(a00.x, a10.x, a01.x, a11.x, c.wx, c.wy));
             g.y = fsub(g.y, up_mix(a00.y, a10.y, a01.y, a11.y, c.wx, c.wy));
             g.z = fsub(g.z, up_mix(a00.z, a10.z, a01.z, a11.z, c.wx, c.wy));
@@ -1637,7 +1670,7 @@ __device__ __noinline__ void blend_pixel(const TileDev& T, const ItemCache& C, i
 // texels and reciprocals computed once per contributor; every pixel's sum
 // still runs over the contributors in index order with its own weights.
 __device__ __forceinline__ void blend_quad(const TileDev& T, const ItemCache& C, int level, int K, long long pl,
-                                           int y, int x)
+                                           int y, int x, int half)
 {
     const int uw = T.lw[level + 1], uh = T.lh[level + 1];
     int x0[4];
@@ -1662,11 +1695,14 @@ __device__ __forceinline__ void blend_quad(const TileDev& T, const ItemCache& C,
     {
         const int4 B = C.box[k];
         if (x + 3 < B.x || x > B.z || y < B.y || y > B.w) continue;  // weight 0 on the quad: terms are +-0
-        const float4* up = C.nd[k] + T.loff[level + 1];
+        const float4* nd = C.nd[k];
+        const size_t up = T.loff[level + 1];
         int cur = x0[0];
-        float3 L0 = gauss_of(__ldg(up + (size_t)y0 * uw + cur)), L1 = gauss_of(__ldg(up + (size_t)y1 * uw + cur));
+        float3 L0 = gauss_of(nd_at(nd, up + (size_t)y0 * uw + cur, half)),
+               L1 = gauss_of(nd_at(nd, up + (size_t)y1 * uw + cur, half));
         int nx = min(cur + 1, uw - 1);
-        float3 R0 = gauss_of(__ldg(up + (size_t)y0 * uw + nx)), R1 = gauss_of(__ldg(up + (size_t)y1 * uw + nx));
+        float3 R0 = gauss_of(nd_at(nd, up + (size_t)y0 * uw + nx, half)),
+               R1 = gauss_of(nd_at(nd, up + (size_t)y1 * uw + nx, half));
 #pragma unroll
         for (int i = 0; i < 4; ++i)
         {
@@ -1676,11 +1712,11 @@ __device__ __forceinline__ void blend_quad(const TileDev& T, const ItemCache& C,
                 L0 = R0;
                 L1 = R1;
                 nx = min(cur + 1, uw - 1);
-                R0 = gauss_of(__ldg(up + (size_t)y0 * uw + nx));
-                R1 = gauss_of(__ldg(up + (size_t)y1 * uw + nx));
+                R0 = gauss_of(nd_at(nd, up + (size_t)y0 * uw + nx, half));
+                R1 = gauss_of(nd_at(nd, up + (size_t)y1 * uw + nx, half));
             }
-            const float wv = __ldg(C.wg[k] + p + i);
-            float3 g = gauss_of(__ldg(C.nd[k] + p + i));
+            const float wv = wg_at(C.wg[k], p + i, half);
+            float3 g = gauss_of(nd_at(nd, p + i, half));
             g.x = fsub(g.x, up_mix(L0.x, R0.x, L1.x, R1.x, wx[i], wy));
             g.y = fsub(g.y, up_mix(L0.y, R0.y, L1.y, R1.y, wx[i], wy));
             g.z = fsub(g.z, up_mix(L0.z, R0.z, L1.z, R1.z, wx[i], wy));
@@ -1738,10 +1774,10 @@ __global__ void __launch_bounds__(256, 3) k_blend_level(BlendArgs a, const Unit*
         const int cnt = min(4, lw - x);
         if (!top && cnt == 4)
         {
-            blend_quad(T, C, level, K, pl, y, x);
+            blend_quad(T, C, level, K, pl, y, x, a.half);
             continue;
         }
-        for (int i = 0; i < cnt; ++i) blend_pixel(T, C, level, K, pl + i);
+        for (int i = 0; i < cnt; ++i) blend_pixel(T, C, level, K, pl + i, a.half);
     }
 }
 
@@ -2113,8 +2149,7 @@ __global__ void __launch_bounds__(256) k_base2(BlendArgs a, const Unit* __restri
             const int X = X2a + (idx & (kB2W - 1)), Y = Y2a + idx / kB2W;
             if (X > X2b || Y > Y2b) continue;
             const size_t q = q2 + (size_t)Y * lw2 + X;
-            it.nd[q] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-            it.wg[q] = 0.0f;
+            pyr_store(it.nd, it.wg, q, make_float4(0.0f, 0.0f, 0.0f, 0.0f), 0.0f, a.half);
         }
         return;
     }
@@ -2167,8 +2202,7 @@ __global__ void __launch_bounds__(256) k_base2(BlendArgs a, const Unit* __restri
         for (int ch = 0; ch < 5; ++ch)
             o[ch] = blur5(t[ch][rows[0]][i], t[ch][rows[1]][i], t[ch][rows[2]][i], t[ch][rows[3]][i], t[ch][rows[4]][i]);
         const size_t q = q2 + (size_t)Y2 * lw2 + X2a + i;
-        it.nd[q] = make_float4(o[0], o[1], o[2], o[3]);
-        it.wg[q] = o[4];
+        pyr_store(it.nd, it.wg, q, make_float4(o[0], o[1], o[2], o[3]), o[4], a.half);
     }
 }
 
@@ -2306,11 +2340,11 @@ __global__ void __launch_bounds__(256) k_fine(BlendArgs a, const Unit* __restric
             stage_level0(S.img[k], S.own, kF0S, true, (signed char)k, W, ry0, ry1, cxa, cx1, S.px, kF0S);
             if (!top1)
             {
-                const float4* g2 = S.nd[k] + T.loff[2];
+                const size_t g2 = T.loff[2];
                 for (int idx = tid; idx < nP * nQ; idx += blockDim.x)
                 {
                     const int r = idx / nP, c = idx - r * nP;
-                    const float3 g = gauss_of(__ldg(g2 + (size_t)(Q0 + r) * lw2 + P0 + c));
+                    const float3 g = gauss_of(nd_at(S.nd[k], g2 + (size_t)(Q0 + r) * lw2 + P0 + c, a.half));
                     S.g2[0][r][c] = g.x;
                     S.g2[1][r][c] = g.y;
                     S.g2[2][r][c] = g.z;

@@ -80,6 +80,7 @@ struct BlendArgs
     unsigned long long* seamCycles;    // per-phase SM cycles of the seam kernel (5 counters)
     int bandRows;                      // rows per band unit (a multiple of 8; the plan's tuning)
     long long spinLimit;               // cycles a bounded wait may last (0: give up at the first miss)
+    int half;                          // materialised pyramid levels stored as FP16 (the native mode)
 };
 
 // Kernel launchers (blend_kernels.cu).

@@ -478,9 +478,22 @@ int Plan::set_tuning(int rows, int slots, cudaStream_t s)
     return I360B_SUCCESS;
 }
 
+int Plan::set_precision(int mode, cudaStream_t s)
+{
+    if (mode != I360B_PRECISION_EXACT && mode != I360B_PRECISION_FP16)
+        return fail(I360B_INVALID_PARAM, "Unknown precision mode %d.", mode);
+    I360B_CUDA(cudaStreamSynchronize(s), "plan precision");
+    storage16 = mode == I360B_PRECISION_FP16 ? 1 : 0;
+    if (storage16) fusedLevels = 2;
+    drop_graphs();
+    return I360B_SUCCESS;
+}
+
 int Plan::set_fusion(int levels, cudaStream_t s)
 {
     if (levels != 0 && levels != 2) return fail(I360B_INVALID_PARAM, "fused pyramid levels must be 0 or 2");
+    if (storage16 && levels != 2)
+        return fail(I360B_INVALID_PARAM, "FP16 pyramid storage needs the fused levels (2).");
     I360B_CUDA(cudaStreamSynchronize(s), "plan fusion");
     fusedLevels = levels;
     drop_graphs();
@@ -556,7 +569,7 @@ int Plan::enqueue_warp(cudaStream_t s)
 
 int Plan::enqueue_chain(int c, int first, int last, cudaStream_t s)
 {
-    BlendArgs a{dItems, dTiles, dError, dSeamCycles, bandRows, spinLimit};
+    BlendArgs a{dItems, dTiles, dError, dSeamCycles, bandRows, spinLimit, storage16};
     const Range* L = &lists[(size_t)c * kListsPerChain];
     const bool fused = fusedLevels == 2;
     const int lo = fused ? 2 : 1;  // lowest level the materialised stages handle
@@ -1050,6 +1063,7 @@ extern "C" int i360b_render_plan_autotune(i360b_render_plan* plan, void* stream,
     int rc = I360B_SUCCESS;
     for (int fused : {2, 0})
     {
+        if (fused != 2 && P.storage16) continue;  // FP16 storage exists only with the fused levels
         if ((rc = P.set_fusion(fused, s)) != I360B_SUCCESS) break;
         for (int rows : {8, 16, 32, 64})
         {
@@ -1108,6 +1122,14 @@ extern "C" int i360b_render_plan_set_tuning(i360b_render_plan* plan, int bandRow
         return fail(I360B_INVALID_PARAM, "dtSlots must be 0 or 2-%d for this plan.", maxSlots);
     I360B_TRY(plan->plan.set_fusion(fusedLevels, s));
     return plan->plan.set_tuning(bandRows, dtSlots, s);
+}
+
+extern "C" int i360b_render_plan_set_precision(i360b_render_plan* plan, int mode, void* stream)
+{
+    clear_error();
+    if (!plan) return fail(I360B_INVALID_PARAM, "Null plan.");
+    I360B_TRY(ensure_ready());
+    return plan->plan.set_precision(mode, static_cast<cudaStream_t>(stream));
 }
 
 extern "C" int i360b_render_plan_set_wait_limit(i360b_render_plan* plan, long long cycles, void* stream)

@@ -63,6 +63,10 @@ struct Plan
     // 1 fused (k_base2 + k_fine, only levels >= 2 in memory), 0 = every level
     // materialised (k_down0s, k_blend_level / k_collapse at level 1, k_final0).
     int fusedLevels = 2;
+    // Storage of the materialised pyramid levels: 0 FP32 (exact, the
+    // reference's values bit for bit), 1 FP16 with FP32 arithmetic (the
+    // native mode; needs the fused levels, so level 1 is never stored).
+    int storage16 = 0;
     // Limit of the bounded device waits (SM cycles; 0 = give up at the first
     // wait that is not satisfied at once, a test setting).
     long long spinLimit = kSpinCyclesDefault;
@@ -130,6 +134,8 @@ struct Plan
     int set_tuning(int rows, int slots, cudaStream_t s);
     // Switches the level-fusion depth (0 or 2); recaptures on next execute.
     int set_fusion(int levels, cudaStream_t s);
+    // Switches the pyramid storage precision (0 exact, 1 FP16).
+    int set_precision(int mode, cudaStream_t s);
     // Changes the bounded-wait limit; the next execute recaptures the graph.
     int set_wait_limit(long long cycles, cudaStream_t s);
     void drop_graphs();

@@ -423,6 +423,22 @@ I360B_API int i360b_render_plan_autotune(i360b_render_plan* plan, void* stream, 
 I360B_API int i360b_render_plan_get_tuning(i360b_render_plan* plan, int* bandRows, int* dtSlots, int* fusedLevels);
 I360B_API int i360b_render_plan_set_tuning(i360b_render_plan* plan, int bandRows, int dtSlots, int fusedLevels,
                                            void* stream);
+/* Precision of the render's stored pyramid levels.  EXACT keeps them in
+ * FP32 and renders the CPU backend's output bit for bit.  FP16 is the native
+ * mode: the levels a plan keeps in memory (levels >= 2 with the fused
+ * pyramid, which it selects) are stored as FP16 with every operation in
+ * FP32, halving their traffic; its output is no longer bit-exact, and its
+ * error against the FP64 restatement of the blend is what the tests and the
+ * bench report.  Warped pixels stay 16-bit integers in both modes (the same
+ * two bytes as FP16, without FP16's rounding of values above 2048).  No
+ * reference counterpart.  Synchronous on `stream`; the next execute
+ * recaptures the plan's graph. */
+enum
+{
+    I360B_PRECISION_EXACT = 0,
+    I360B_PRECISION_FP16 = 1
+};
+I360B_API int i360b_render_plan_set_precision(i360b_render_plan* plan, int mode, void* stream);
 /* i360b_launch_export_preview over the plan's tiles in tile order (tiles that
  * list no contributor have no render output and are skipped). */
 I360B_API int i360b_render_plan_export_preview(i360b_render_plan* plan, int totalW, int totalH, int maxDimension,

@@ -116,3 +116,50 @@ def test_gpu_kernels_against_fp64(backend, oracle_c):
     color32 = np.array(frames[1], copy=True)
     assert backend.apply_reinhard_color_transfer(color32, tm, ts, rm, rs) == 0, backend.get_last_error()
     _report(_fp64_rows(O, cfg, pano, frames[:2], warp32, (bufs, got), owner, color32))
+
+
+@pytest.mark.gpu
+def test_fp16_storage_mode_error_against_fp64(backend, oracle_c):
+    """The native mode (stored pyramid levels in FP16, FP32 arithmetic) on a
+    scaled panorama: every tile's output against the FP64 compose of the
+    same warped contributors on the same owner map (the stages before the
+    pyramid are exact in both modes), beside the exact mode's error.
+    Reported, and bounded: the FP16 rounding of the coarse levels (relative
+    2^-12) moves the output by at most a few DN where a coarse band is
+    large, and by far less on average."""
+    import torch
+
+    from image360_b200 import COORDS_REFERENCE, PRECISION_EXACT, PRECISION_FP16, RenderPlan
+    O = oracle_c
+    cfg, pano = _scene()
+    black, cm, rc, filt = synth.demosaic_params(cfg)
+    host = [O.demosaic(c.numpy().view(np.uint16), black, cm, rc, filt) for c in pano.cfa]
+    dev = [torch.from_numpy(f.view(np.int16)).cuda() for f in host]
+    gains = (1.0 / pano.gains).astype(np.float32)
+    outs = [torch.zeros((t[3], t[2], 3), dtype=torch.int16, device="cuda") for t in pano.tiles]
+    frames = [(d.data_ptr(), cfg.frame_w, cfg.frame_h, H, float(g)) for d, H, g in zip(dev, pano.to_canvas, gains)]
+    plan = RenderPlan(frames, [(*t[:5], o.data_ptr()) for t, o in zip(pano.tiles, outs)], cfg.bands, COORDS_REFERENCE)
+    res = {}
+    for mode in (PRECISION_EXACT, PRECISION_FP16):
+        assert plan.set_precision(mode) == 0
+        assert plan.execute() == 0 and plan.wait() == 0
+        res[mode] = [o.cpu().numpy().view(np.uint16).copy() for o in outs]
+    assert plan.set_precision(PRECISION_FP16) == 0
+    assert plan.set_tuning(16, 0, 0) != 0  # FP16 storage exists only with the fused levels
+    plan.close()
+    rows = {PRECISION_EXACT: [], PRECISION_FP16: []}
+    for t, (x, y, w, h, cs) in enumerate(pano.tiles):
+        if len(cs) < 2:
+            continue
+        bufs = [O.gain(O.warp(host[k], w, h, synth.inverse_homography_f32(pano.to_canvas[k]), x, y), gains[k])
+                for k in cs]
+        _, owner = O.blend(bufs, cfg.bands, return_owner=True)
+        ref = O.compose(bufs, None, owner, cfg.bands, f64=True)
+        for mode in rows:
+            rows[mode].append(_err(res[mode][t], ref))
+    ex = (max(r[0] for r in rows[PRECISION_EXACT]), float(np.mean([r[1] for r in rows[PRECISION_EXACT]])))
+    fp = (max(r[0] for r in rows[PRECISION_FP16]), float(np.mean([r[1] for r in rows[PRECISION_FP16]])))
+    print(f"\ncompose vs FP64 over {len(rows[PRECISION_FP16])} tiles: exact max {ex[0]} mean {ex[1]:.5f}; "
+          f"fp16 storage max {fp[0]} mean {fp[1]:.5f}")
+    assert ex[0] <= 1 and ex[1] < 0.02, ex
+    assert fp[0] <= 48 and fp[1] < 1.0, fp
