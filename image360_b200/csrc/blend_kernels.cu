@@ -2007,6 +2007,8 @@ constexpr int kB0H = 2 * kB1H + 3;                  // level-0 footprint rows (a
 constexpr int kRun = 7;                             // level-1 rows per streaming task
 
 constexpr int kFW = 64, kFH = 32;                   // output pixels per k_fine CTA
+constexpr int kFRun = 3;                            // k_fine's level-1 rows per streaming task (more tasks than
+                                                    // threads would idle otherwise: the window is ~34 wide)
 constexpr int kF1W = 36, kF1H = 20;                 // its level-1 window (bound; checked)
 constexpr int kF0S = 2 * kF1W + 8;                  // level-0 footprint row stride: the footprint's
                                                     // at most 78 columns rounded up to whole 4-pixel groups
@@ -2217,6 +2219,12 @@ struct FineSmem
     const unsigned short* img[kMaxTileItems];
     const float4* nd[kMaxTileItems];
     uint32_t set[kMaxTileItems / 32];          // contributors owning a footprint pixel
+    // Up taps, tabulated: the align-corners coefficients are separable (the x
+    // part depends on x only, the y part on y only), so the block's columns
+    // and rows (level 0 -> 1) and the window's (level 1 -> 2) are computed
+    // once: tap indices relative to the window, and the fraction.
+    short2 tx0[kFW], ty0[kFH], tx1[kF1W], ty1[kF1H];
+    float fx0[kFW], fy0[kFH], fx1[kF1W], fy1[kF1H];
 };
 
 __global__ void __launch_bounds__(256) k_fine(BlendArgs a, const Unit* __restrict__ units)
@@ -2297,6 +2305,37 @@ __global__ void __launch_bounds__(256) k_fine(BlendArgs a, const Unit* __restric
         }
         return;
     }
+    // Up tap tables (see FineSmem); indices relative to the windows
+    for (int i = tid; i < kFW + kFH + kF1W + kF1H; i += blockDim.x)
+    {
+        if (i < kFW)
+        {
+            const UpCoef q = up_coef_s(T.usx[0], T.usy[0], lw1, lh1, min(X0 + i, xe), Y0);
+            S.tx0[i] = make_short2((short)(q.x0 - A0), (short)(q.x1 - A0));
+            S.fx0[i] = q.wx;
+        }
+        else if (i < kFW + kFH)
+        {
+            const int j = i - kFW;
+            const UpCoef q = up_coef_s(T.usx[0], T.usy[0], lw1, lh1, X0, min(Y0 + j, ye));
+            S.ty0[j] = make_short2((short)(q.y0 - B0), (short)(q.y1 - B0));
+            S.fy0[j] = q.wy;
+        }
+        else if (!top1 && i < kFW + kFH + kF1W)
+        {
+            const int c = i - kFW - kFH;
+            const UpCoef q = up_coef_s(T.usx[1], T.usy[1], lw2, lh2, min(A0 + c, A1), B0);
+            S.tx1[c] = make_short2((short)(q.x0 - P0), (short)(q.x1 - P0));
+            S.fx1[c] = q.wx;
+        }
+        else if (!top1)
+        {
+            const int r = i - kFW - kFH - kF1W;
+            const UpCoef q = up_coef_s(T.usx[1], T.usy[1], lw2, lh2, A0, min(B0 + r, B1));
+            S.ty1[r] = make_short2((short)(q.y0 - Q0), (short)(q.y1 - Q0));
+            S.fy1[r] = q.wy;
+        }
+    }
     // owner map over the footprint, and the contributors it names
     const int nr = ry1 - ry0 + 1, ncol = cx1 - cxa + 1;
     for (int idx = tid; idx < nr * ncol; idx += blockDim.x)
@@ -2329,7 +2368,7 @@ __global__ void __launch_bounds__(256) k_fine(BlendArgs a, const Unit* __restric
 #pragma unroll
     for (int i = 0; i < 8; ++i) lap[i][0] = lap[i][1] = lap[i][2] = 0.0f;
     const int nWin = nA * nB;
-    const int nRuns = (nB + kRun - 1) / kRun;
+    const int nRuns = (nB + kFRun - 1) / kFRun;
     for (int w = 0; w < kMaxTileItems / 32; ++w)
     {
         uint32_t m = S.set[w];
@@ -2355,8 +2394,8 @@ __global__ void __launch_bounds__(256) k_fine(BlendArgs a, const Unit* __restric
             for (int task = tid; task < nA * nRuns; task += blockDim.x)
             {
                 const int run = task / nA, c = task - run * nA;
-                const int Y1s = B0 + run * kRun;
-                const int R = min(kRun, B1 - Y1s + 1);
+                const int Y1s = B0 + run * kFRun;
+                const int R = min(kFRun, B1 - Y1s + 1);
                 level1_column(S.px, kF0S, ry0, cxa, W, H, A0 + c, Y1s, R,
                               [&](int mm, float n0, float n1, float n2, float den, float wg) {
                                   const int r = Y1s + mm - B0;
@@ -2380,12 +2419,12 @@ __global__ void __launch_bounds__(256) k_fine(BlendArgs a, const Unit* __restric
                 float g[3] = {S.g1[0][r][c], S.g1[1][r][c], S.g1[2][r][c]};
                 if (!top1)
                 {
-                    const UpCoef q = up_coef_s(T.usx[1], T.usy[1], lw2, lh2, A0 + c, B0 + r);
-                    const int x0 = q.x0 - P0, x1 = q.x1 - P0, y0 = q.y0 - Q0, y1 = q.y1 - Q0;
+                    const short2 xt = S.tx1[c], yt = S.ty1[r];
+                    const float wx = S.fx1[c], wy = S.fy1[r];
 #pragma unroll
                     for (int ch = 0; ch < 3; ++ch)
-                        g[ch] = fsub(g[ch], up_mix(S.g2[ch][y0][x0], S.g2[ch][y0][x1], S.g2[ch][y1][x0],
-                                                   S.g2[ch][y1][x1], q.wx, q.wy));
+                        g[ch] = fsub(g[ch], up_mix(S.g2[ch][yt.x][xt.x], S.g2[ch][yt.x][xt.y], S.g2[ch][yt.y][xt.x],
+                                                   S.g2[ch][yt.y][xt.y], wx, wy));
                 }
 #pragma unroll
                 for (int ch = 0; ch < 3; ++ch) acc[j][ch] = fadd(acc[j][ch], fmul(wv, g[ch]));
@@ -2396,14 +2435,14 @@ __global__ void __launch_bounds__(256) k_fine(BlendArgs a, const Unit* __restric
             {
                 if (own[i] != k) continue;
                 const int x = ox + i;
-                const UpCoef q = up_coef_s(T.usx[0], T.usy[0], lw1, lh1, x, oy);
-                const int x0 = q.x0 - A0, x1 = q.x1 - A0, y0 = q.y0 - B0, y1 = q.y1 - B0;
+                const short2 xt = S.tx0[x - X0], yt = S.ty0[oy - Y0];
+                const float wx = S.fx0[x - X0], wy = S.fy0[oy - Y0];
                 int cv[4];
                 px_channels(S.px[(oy - ry0) * kF0S + (x - cxa)], cv);
 #pragma unroll
                 for (int ch = 0; ch < 3; ++ch)
-                    lap[i][ch] = fsub((float)cv[ch], up_mix(S.g1[ch][y0][x0], S.g1[ch][y0][x1], S.g1[ch][y1][x0],
-                                                            S.g1[ch][y1][x1], q.wx, q.wy));
+                    lap[i][ch] = fsub((float)cv[ch], up_mix(S.g1[ch][yt.x][xt.x], S.g1[ch][yt.x][xt.y],
+                                                            S.g1[ch][yt.y][xt.x], S.g1[ch][yt.y][xt.y], wx, wy));
             }
             __syncthreads();
         }
@@ -2418,12 +2457,12 @@ __global__ void __launch_bounds__(256) k_fine(BlendArgs a, const Unit* __restric
         float v[3] = {acc[j][0], acc[j][1], acc[j][2]};
         if (!top1)
         {
-            const UpCoef q = up_coef_s(T.usx[1], T.usy[1], lw2, lh2, A0 + c, B0 + r);
-            const int x0 = q.x0 - P0, x1 = q.x1 - P0, y0 = q.y0 - Q0, y1 = q.y1 - Q0;
+            const short2 xt = S.tx1[c], yt = S.ty1[r];
+            const float wx = S.fx1[c], wy = S.fy1[r];
 #pragma unroll
             for (int ch = 0; ch < 3; ++ch)
-                v[ch] = fadd(v[ch], up_mix(S.r2[ch][y0][x0], S.r2[ch][y0][x1], S.r2[ch][y1][x0], S.r2[ch][y1][x1],
-                                           q.wx, q.wy));
+                v[ch] = fadd(v[ch], up_mix(S.r2[ch][yt.x][xt.x], S.r2[ch][yt.x][xt.y], S.r2[ch][yt.y][xt.x],
+                                           S.r2[ch][yt.y][xt.y], wx, wy));
         }
         S.g1[0][r][c] = v[0];
         S.g1[1][r][c] = v[1];
@@ -2438,13 +2477,13 @@ __global__ void __launch_bounds__(256) k_fine(BlendArgs a, const Unit* __restric
     {
         res[3 * i] = res[3 * i + 1] = res[3 * i + 2] = 0;
         if (own[i] < 0) continue;
-        const UpCoef q = up_coef_s(T.usx[0], T.usy[0], lw1, lh1, ox + i, oy);
-        const int x0 = q.x0 - A0, x1 = q.x1 - A0, y0 = q.y0 - B0, y1 = q.y1 - B0;
+        const short2 xt = S.tx0[ox + i - X0], yt = S.ty0[oy - Y0];
+        const float wx = S.fx0[ox + i - X0], wy = S.fy0[oy - Y0];
         float r[3];
 #pragma unroll
         for (int ch = 0; ch < 3; ++ch)
-            r[ch] = fadd(lap[i][ch], up_mix(S.g1[ch][y0][x0], S.g1[ch][y0][x1], S.g1[ch][y1][x0], S.g1[ch][y1][x1],
-                                            q.wx, q.wy));
+            r[ch] = fadd(lap[i][ch], up_mix(S.g1[ch][yt.x][xt.x], S.g1[ch][yt.x][xt.y], S.g1[ch][yt.y][xt.x],
+                                            S.g1[ch][yt.y][xt.y], wx, wy));
         final_store(res + 3 * i, r);
     }
     if (ox + 7 <= xe && (reinterpret_cast<uintptr_t>(outRow) & 15) == 0)
