@@ -277,6 +277,12 @@ def run_ours(args, rank, world, local_rank):
     # The plan's autotuner picks the band height and chamfer ring depth on
     # this workload (untimed; every setting renders the same bits).
     tuned = plan.autotune(sp) if not args.no_autotune else None
+    if args.fusion is not None or args.warp_shape is not None:
+        t = plan.tuning()
+        assert plan.set_tuning(t["band_rows"], t["dt_slots"],
+                               t["fused_levels"] if args.fusion is None else args.fusion,
+                               t["warp_shape"] if args.warp_shape is None else args.warp_shape, sp) == 0
+        tuned = {**(tuned or {}), **plan.tuning(), "forced": True}
     torch.cuda.synchronize()
     stats = plan.stats(sp)
     stages = plan.profile(sp)
@@ -1231,6 +1237,10 @@ def main():
     ap.add_argument("--no-uneven", action="store_true", help="skip the 256 uneven-tile leg")
     ap.add_argument("--no-parity", action="store_true", help="skip the full-panorama check against the CPU code")
     ap.add_argument("--no-native", action="store_true", help="skip the FP16-storage (native mode) leg")
+    ap.add_argument("--fusion", type=int, choices=[0, 2], default=None,
+                    help="force the level-fusion depth after autotuning (measurement of one form)")
+    ap.add_argument("--warp-shape", type=int, choices=[0, 1], default=None,
+                    help="force the tile-warp form after autotuning")
     ap.add_argument("--no-autotune", action="store_true", help="keep the plan's default band height and ring depth")
     ap.add_argument("--train-steps", type=int, default=782, help="Adam steps (782 x 64 = 50k windows)")
     ap.add_argument("--train-batch", type=int, default=64)

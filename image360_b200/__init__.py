@@ -131,8 +131,8 @@ def load_library(path: str = LIB_PATH):
     L.i360b_launch_blend.argtypes = [ct.POINTER(vp), i, i, i, i, vp, vp]
     L.i360b_launch_blend_noalloc.argtypes = [ct.POINTER(vp), i, i, i, i, vp, vp]
     L.i360b_render_plan_set_wait_limit.argtypes = [vp, ct.c_longlong, vp]
-    L.i360b_render_plan_get_tuning.argtypes = [vp, _i32p, _i32p, _i32p]
-    L.i360b_render_plan_set_tuning.argtypes = [vp, i, i, i, vp]
+    L.i360b_render_plan_get_tuning.argtypes = [vp, _i32p, _i32p, _i32p, _i32p]
+    L.i360b_render_plan_set_tuning.argtypes = [vp, i, i, i, i, vp]
     L.i360b_render_plan_set_precision.argtypes = [vp, i, vp]
     L.i360b_debug_inject_failure.argtypes = [i, i]
     _lib = L
@@ -537,23 +537,24 @@ class RenderPlan:
         rc = self.lib.i360b_render_plan_autotune(self._h, stream or None, ct.byref(r), ct.byref(k), ct.byref(ms))
         if rc != 0:
             raise RuntimeError(self.lib.i360b_get_last_error().decode())
-        return {"band_rows": r.value, "dt_slots": k.value, "fused_levels": self.tuning()["fused_levels"],
-                "ms": ms.value}
+        t = self.tuning()
+        return {"band_rows": r.value, "dt_slots": k.value, "fused_levels": t["fused_levels"],
+                "warp_shape": t["warp_shape"], "ms": ms.value}
 
     def tuning(self) -> dict:
-        r, k, f = ct.c_int(), ct.c_int(), ct.c_int()
-        self.lib.i360b_render_plan_get_tuning(self._h, ct.byref(r), ct.byref(k), ct.byref(f))
-        return {"band_rows": r.value, "dt_slots": k.value, "fused_levels": f.value}
+        r, k, f, w = ct.c_int(), ct.c_int(), ct.c_int(), ct.c_int()
+        self.lib.i360b_render_plan_get_tuning(self._h, ct.byref(r), ct.byref(k), ct.byref(f), ct.byref(w))
+        return {"band_rows": r.value, "dt_slots": k.value, "fused_levels": f.value, "warp_shape": w.value}
 
     def set_precision(self, mode: int, stream: int = 0) -> ComputeResult:
         """PRECISION_EXACT (FP32 pyramid levels, bit-exact) or PRECISION_FP16
         (stored levels in FP16, FP32 arithmetic: the native mode)."""
         return ComputeResult(self.lib.i360b_render_plan_set_precision(self._h, int(mode), stream or None))
 
-    def set_tuning(self, band_rows: int = 16, dt_slots: int = 0, fused_levels: int = 2,
+    def set_tuning(self, band_rows: int = 16, dt_slots: int = 0, fused_levels: int = 2, warp_shape: int = 1,
                    stream: int = 0) -> ComputeResult:
         return ComputeResult(self.lib.i360b_render_plan_set_tuning(self._h, int(band_rows), int(dt_slots),
-                                                                   int(fused_levels), stream or None))
+                                                                   int(fused_levels), int(warp_shape), stream or None))
 
     def export_preview(self, total_w: int, total_h: int, max_dimension: int, d_out: int, capacity: int,
                        stream: int = 0):

@@ -126,7 +126,7 @@ __global__ void __launch_bounds__(256) k_coverage(BlendArgs a, const Unit* __res
 // consecutive pixels, so one ballot is one coverage word.
 // ---------------------------------------------------------------------------
 constexpr int kWpW = kWarpBlockW, kWpH = kWarpBlockH;  // destination pixels per CTA
-constexpr int kWpSW = 160, kWpSH = 28; // staged source box (pixels) at most
+constexpr int kWpSW = 160, kWpSH = 44; // staged source box (pixels) at most
 
 // The warp parameters of one item, read once per CTA into registers (the
 // item table is in global memory, where the compiler cannot tell it apart
@@ -202,20 +202,30 @@ __device__ __forceinline__ void warp_zero_u16(unsigned short* p, int n, int lane
     if (lane < n - t0) p[t0 + lane] = 0;
 }
 
-struct WarpSmem
+// One destination pixel read straight from the source frame (the row-band
+// form below): the four taps by 2-byte loads through L1.
+__device__ __forceinline__ void warp_px(const WarpItem& it, float dX, const float* hy, unsigned short o[3])
 {
-    uint2 px[kWpSH][kWpSW];
-    int box[4];   // staged source box: x0 (8-aligned), y0, columns, rows; columns 0 = not staged
-};
+    o[0] = o[1] = o[2] = 0;
+    int x0, y0;
+    float fx, fy;
+    if (!warp_pos(it, dX, hy, x0, y0, fx, fy)) return;
+    const unsigned short* r0 = it.src + ((size_t)y0 * it.srcW + x0) * 3;
+    const unsigned short* r1 = r0 + (size_t)it.srcW * 3;
+    unsigned short t00[3], t10[3], t01[3], t11[3];
+#pragma unroll
+    for (int c = 0; c < 3; ++c)
+    {
+        t00[c] = __ldg(r0 + c);
+        t10[c] = __ldg(r0 + 3 + c);
+        t01[c] = __ldg(r1 + c);
+        t11[c] = __ldg(r1 + 3 + c);
+    }
+    warp_mix(it, fx, fy, t00, t10, t01, t11, o);
+}
 
-__global__ void __launch_bounds__(256) k_warp_tiles(BlendArgs a, const Unit* __restrict__ units)
+__device__ __forceinline__ WarpItem warp_item(const ItemDev& it)
 {
-    __shared__ __align__(16) WarpSmem S;
-    const Unit u = units[blockIdx.x];
-    const ItemDev& it = a.items[u.id];
-    const TileDev& T = a.tiles[it.tile];
-    const int W = T.w, H = T.h, lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    unsigned short* img = const_cast<unsigned short*>(it.img);
     WarpItem wi;
 #pragma unroll
     for (int q = 0; q < 9; ++q) wi.H[q] = it.H[q];
@@ -224,53 +234,138 @@ __global__ void __launch_bounds__(256) k_warp_tiles(BlendArgs a, const Unit* __r
     wi.srcH = it.srcH;
     wi.gain = it.gain;
     wi.applyGain = !gain_is_identity(it.gain);
+    return wi;
+}
+
+// Row-band form (warp shape 0): a CTA makes a.bandRows full-width rows of one
+// contributor, each warp whole rows in 64-pixel segments with two pixels per
+// lane in flight, gathering taps from the frame through L1; rows and segments
+// outside the frame's footprint box are written as zeros without evaluating
+// the mapping.
+__global__ void __launch_bounds__(256, 8) k_warp_rows(BlendArgs a, const Unit* __restrict__ units)
+{
+    const Unit u = units[blockIdx.x];
+    const ItemDev& it = a.items[u.id];
+    const TileDev& T = a.tiles[it.tile];
+    const int W = T.w, H = T.h, lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    unsigned short* img = const_cast<unsigned short*>(it.img);
+    const WarpItem wi = warp_item(it);
+    const int offX = it.offX, offY = it.offY, vx0 = it.vx0, vx1 = it.vx1, vy0 = it.vy0, vy1 = it.vy1;
+    BoxAcc box;
+    const int rowsPerWarp = a.bandRows >> 3;
+    for (int r = 0; r < rowsPerWarp; ++r)
+    {
+        const int y = u.by * a.bandRows + warp * rowsPerWarp + r;
+        if (y >= H) break;
+        const float dY = (float)(y + offY);
+        const float hy[3] = {fmul(wi.H[1], dY), fmul(wi.H[4], dY), fmul(wi.H[7], dY)};
+        int s0 = 0, s1 = 0;
+        if (y >= vy0 && y <= vy1)
+        {
+            const int xs = max(vx0, 0), xe = min(vx1, W - 1);
+            if (xs <= xe)
+            {
+                s0 = xs & ~63;
+                s1 = min(W, (xe & ~63) + 64);
+            }
+        }
+        unsigned short* row = img + (size_t)y * W * 3;
+        uint32_t* covRow = it.cov + (size_t)y * T.covWords;
+        warp_zero_u16(row, s0 * 3, lane);
+        warp_zero_u16(row + (size_t)s1 * 3, (W - s1) * 3, lane);
+        for (int j = lane; j < (s0 >> 5); j += 32) covRow[j] = 0u;
+        for (int j = ((s1 + 31) >> 5) + lane; j < ((W + 31) >> 5); j += 32) covRow[j] = 0u;
+        for (int x0 = s0; x0 < s1; x0 += 64)
+        {
+            const int xa = x0 + lane, xb = x0 + 32 + lane;
+            unsigned short oa[3] = {0, 0, 0}, ob[3] = {0, 0, 0};
+            if (xa < W && xa >= vx0 && xa <= vx1) warp_px(wi, (float)(xa + offX), hy, oa);
+            if (xb < W && xb >= vx0 && xb <= vx1) warp_px(wi, (float)(xb + offX), hy, ob);
+            const bool ca = (oa[0] | oa[1] | oa[2]) != 0, cb = (ob[0] | ob[1] | ob[2]) != 0;
+            if (xa < W)
+            {
+                unsigned short* d = row + (size_t)xa * 3;
+                d[0] = oa[0];
+                d[1] = oa[1];
+                d[2] = oa[2];
+            }
+            if (xb < W)
+            {
+                unsigned short* d = row + (size_t)xb * 3;
+                d[0] = ob[0];
+                d[1] = ob[1];
+                d[2] = ob[2];
+            }
+            const unsigned ma = __ballot_sync(kFull, ca), mb = __ballot_sync(kFull, cb);
+            if (lane == 0)
+            {
+                covRow[x0 >> 5] = ma;
+                if (x0 + 32 < W) covRow[(x0 >> 5) + 1] = mb;
+            }
+            box.add(ca, xa, y);
+            box.add(cb, xb, y);
+        }
+    }
+    box.flush(it.bbox);
+}
+
+// Staged-block form (warp shape 1).
+struct WarpSmem
+{
+    uint2 px[kWpSH][kWpSW];
+    float ext[4][4];  // per corner: source x, y (FP32, rounded outward by the caller's margin), ok flag
+};
+
+__global__ void __launch_bounds__(256) k_warp_tiles(BlendArgs a, const Unit* __restrict__ units)
+{
+    extern __shared__ __align__(16) unsigned char warp_raw[];
+    WarpSmem& S = *reinterpret_cast<WarpSmem*>(warp_raw);
+    const Unit u = units[blockIdx.x];
+    const ItemDev& it = a.items[u.id];
+    const TileDev& T = a.tiles[it.tile];
+    const int W = T.w, H = T.h, lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    unsigned short* img = const_cast<unsigned short*>(it.img);
+    const WarpItem wi = warp_item(it);
     const int offX = it.offX, offY = it.offY;
     const int X0 = u.bx * kWpW, Y0 = u.by * kWpH;
     const int X1 = min(X0 + kWpW, W) - 1, Y1 = min(Y0 + kWpH, H) - 1;
     // the block's part of the footprint box (tile-local; outside it the warp is (0,0,0))
     const int fx0 = max(it.vx0, X0), fx1 = min(it.vx1, X1), fy0 = max(it.vy0, Y0), fy1 = min(it.vy1, Y1);
     const bool any = fx0 <= fx1 && fy0 <= fy1;
-    if (threadIdx.x == 0)
+    // The staged source box: the source positions of the corners of the
+    // block's footprint part, one corner per thread of the first four.
+    if (any && threadIdx.x < 4)
     {
-        // staged source box from the corners of the block's footprint part (FP64)
-        int bx = 0, by = 0, bc = 0, br = 0;
-        if (any)
-        {
-            double mnx = 1e300, mny = 1e300, mxx = -1e300, mxy = -1e300;
-            bool ok = true;
-            for (int c = 0; c < 4 && ok; ++c)
-            {
-                const double dx = (double)((c & 1) ? fx1 : fx0) + offX, dy = (double)((c & 2) ? fy1 : fy0) + offY;
-                const double w = (double)wi.H[6] * dx + (double)wi.H[7] * dy + (double)wi.H[8];
-                if (!(w > 1e-6)) ok = false;
-                const double sx = ((double)wi.H[0] * dx + (double)wi.H[1] * dy + (double)wi.H[2]) / w;
-                const double sy = ((double)wi.H[3] * dx + (double)wi.H[4] * dy + (double)wi.H[5]) / w;
-                mnx = fmin(mnx, sx);
-                mxx = fmax(mxx, sx);
-                mny = fmin(mny, sy);
-                mxy = fmax(mxy, sy);
-            }
-            if (ok && mxx > -1e9 && mnx < 1e9 && mxy > -1e9 && mny < 1e9)
-            {
-                const int sx0 = max(0, (int)floor(mnx) - 2), sx1 = min(wi.srcW - 1, (int)floor(mxx) + 3);
-                const int sy0 = max(0, (int)floor(mny) - 2), sy1 = min(wi.srcH - 1, (int)floor(mxy) + 3);
-                const int xa = sx0 & ~7;
-                if (sx0 <= sx1 && sy0 <= sy1 && sx1 - xa + 1 <= kWpSW && sy1 - sy0 + 1 <= kWpSH)
-                {
-                    bx = xa;
-                    by = sy0;
-                    bc = ((sx1 - xa) | 7) + 1;
-                    br = sy1 - sy0 + 1;
-                }
-            }
-        }
-        S.box[0] = bx;
-        S.box[1] = by;
-        S.box[2] = bc;
-        S.box[3] = br;
+        const int c = threadIdx.x;
+        const float dx = (float)(((c & 1) ? fx1 : fx0) + offX), dy = (float)(((c & 2) ? fy1 : fy0) + offY);
+        const float w = wi.H[6] * dx + wi.H[7] * dy + wi.H[8];
+        const float sx = (wi.H[0] * dx + wi.H[1] * dy + wi.H[2]) / w;
+        const float sy = (wi.H[3] * dx + wi.H[4] * dy + wi.H[5]) / w;
+        S.ext[c][0] = sx;
+        S.ext[c][1] = sy;
+        S.ext[c][2] = (w > 1e-6f && fabsf(sx) < 1e8f && fabsf(sy) < 1e8f) ? 1.0f : 0.0f;
     }
     __syncthreads();
-    const int sbx = S.box[0], sby = S.box[1], sbc = S.box[2], sbr = S.box[3];
+    int sbx = 0, sby = 0, sbc = 0, sbr = 0;  // staged box: x0 (8-aligned), y0, columns, rows; sbc 0 = none
+    if (any && S.ext[0][2] > 0.0f && S.ext[1][2] > 0.0f && S.ext[2][2] > 0.0f && S.ext[3][2] > 0.0f)
+    {
+        const float mnx = fminf(fminf(S.ext[0][0], S.ext[1][0]), fminf(S.ext[2][0], S.ext[3][0]));
+        const float mxx = fmaxf(fmaxf(S.ext[0][0], S.ext[1][0]), fmaxf(S.ext[2][0], S.ext[3][0]));
+        const float mny = fminf(fminf(S.ext[0][1], S.ext[1][1]), fminf(S.ext[2][1], S.ext[3][1]));
+        const float mxy = fmaxf(fmaxf(S.ext[0][1], S.ext[1][1]), fmaxf(S.ext[2][1], S.ext[3][1]));
+        // 3 pixels of margin: the per-pixel positions are computed by the
+        // reference's FP32 formula, these by a contracted one
+        const int sx0 = max(0, (int)floorf(mnx) - 3), sx1 = min(wi.srcW - 1, (int)floorf(mxx) + 4);
+        const int sy0 = max(0, (int)floorf(mny) - 3), sy1 = min(wi.srcH - 1, (int)floorf(mxy) + 4);
+        const int xa = sx0 & ~7;
+        if (sx0 <= sx1 && sy0 <= sy1 && sx1 - xa + 1 <= kWpSW && sy1 - sy0 + 1 <= kWpSH)
+        {
+            sbx = xa;
+            sby = sy0;
+            sbc = ((sx1 - xa) | 7) + 1;
+            sbr = sy1 - sy0 + 1;
+        }
+    }
     if (sbc > 0)
     {
         // 8-pixel groups: three 16-byte words when source rows are 16-byte aligned
@@ -280,11 +375,11 @@ __global__ void __launch_bounds__(256) k_warp_tiles(BlendArgs a, const Unit* __r
         {
             const int r = t / ng, g = t - r * ng;
             const int gx = sbx + 8 * g;
-            const unsigned short* s = wi.src + ((size_t)(sby + r) * wi.srcW + gx) * 3;
+            const unsigned short* src = wi.src + ((size_t)(sby + r) * wi.srcW + gx) * 3;
             uint2* d = &S.px[r][8 * g];
             if (fast && gx + 8 <= wi.srcW)
             {
-                const uint4* s4 = reinterpret_cast<const uint4*>(s);
+                const uint4* s4 = reinterpret_cast<const uint4*>(src);
                 const uint4 q0 = __ldg(s4), q1 = __ldg(s4 + 1), q2 = __ldg(s4 + 2);
                 const uint32_t w[12] = {q0.x, q0.y, q0.z, q0.w, q1.x, q1.y, q1.z, q1.w, q2.x, q2.y, q2.z, q2.w};
 #pragma unroll
@@ -301,8 +396,8 @@ __global__ void __launch_bounds__(256) k_warp_tiles(BlendArgs a, const Unit* __r
 #pragma unroll
                 for (int e = 0; e < 8; ++e)
                     if (gx + e < wi.srcW)
-                        d[e] = make_uint2((uint32_t)__ldg(s + 3 * e) | ((uint32_t)__ldg(s + 3 * e + 1) << 16),
-                                          (uint32_t)__ldg(s + 3 * e + 2));
+                        d[e] = make_uint2((uint32_t)__ldg(src + 3 * e) | ((uint32_t)__ldg(src + 3 * e + 1) << 16),
+                                          (uint32_t)__ldg(src + 3 * e + 2));
             }
         }
     }
@@ -336,22 +431,10 @@ __global__ void __launch_bounds__(256) k_warp_tiles(BlendArgs a, const Unit* __r
                 unsigned short t00[3], t10[3], t01[3], t11[3];
                 if (cx >= 0 && cx + 1 < sbc && ry >= 0 && ry + 1 < sbr)
                 {
-                    if ((cx & 1) == 0)
-                    {
-                        const uint4 p0 = *reinterpret_cast<const uint4*>(&S.px[ry][cx]);
-                        const uint4 p1 = *reinterpret_cast<const uint4*>(&S.px[ry + 1][cx]);
-                        px_of(make_uint2(p0.x, p0.y), t00);
-                        px_of(make_uint2(p0.z, p0.w), t10);
-                        px_of(make_uint2(p1.x, p1.y), t01);
-                        px_of(make_uint2(p1.z, p1.w), t11);
-                    }
-                    else
-                    {
-                        px_of(S.px[ry][cx], t00);
-                        px_of(S.px[ry][cx + 1], t10);
-                        px_of(S.px[ry + 1][cx], t01);
-                        px_of(S.px[ry + 1][cx + 1], t11);
-                    }
+                    px_of(S.px[ry][cx], t00);
+                    px_of(S.px[ry][cx + 1], t10);
+                    px_of(S.px[ry + 1][cx], t01);
+                    px_of(S.px[ry + 1][cx + 1], t11);
                 }
                 else
                 {
@@ -2529,10 +2612,16 @@ int launch_coverage(const BlendArgs& a, const Unit* units, int n, cudaStream_t s
     return check_launch("coverage kernel");
 }
 
-int launch_warp_tiles(const BlendArgs& a, const Unit* units, int n, cudaStream_t s)
+int launch_warp_tiles(const BlendArgs& a, const Unit* units, int n, int shape, cudaStream_t s)
 {
     if (n <= 0) return I360B_SUCCESS;
-    k_warp_tiles<<<n, 256, 0, s>>>(a, units);
+    if (shape == 1)
+    {
+        const int smem = (int)sizeof(WarpSmem);
+        cudaFuncSetAttribute(k_warp_tiles, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+        k_warp_tiles<<<n, 256, smem, s>>>(a, units);
+    }
+    else k_warp_rows<<<n, 256, 0, s>>>(a, units);
     return check_launch("tile warp kernel");
 }
 

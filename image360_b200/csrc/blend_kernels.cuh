@@ -85,7 +85,9 @@ struct BlendArgs
 
 // Kernel launchers (blend_kernels.cu).
 int launch_coverage(const BlendArgs& a, const Unit* units, int n, cudaStream_t s);
-int launch_warp_tiles(const BlendArgs& a, const Unit* units, int n, cudaStream_t s);
+// shape 1: staged 128x32 blocks (units: item, block); 0: row bands (units:
+// item, band of BlendArgs::bandRows rows).
+int launch_warp_tiles(const BlendArgs& a, const Unit* units, int n, int shape, cudaStream_t s);
 int launch_dt(const BlendArgs& a, const int* itemList, int n, bool backward, int maxW, int maxH, int slots,
               cudaStream_t s);
 int launch_owner(const BlendArgs& a, const Unit* units, int n, cudaStream_t s);
@@ -99,7 +101,7 @@ int launch_final0(const BlendArgs& a, const Unit* units, int n, cudaStream_t s);
 // its collapse and the output (units: tile, 64x32 blocks of output pixels).
 constexpr int kBase2W = 32, kBase2H = 8, kFineW = 64, kFineH = 32;
 // Destination block of one tile-warp CTA (launch_warp_tiles units: item, block).
-constexpr int kWarpBlockW = 128, kWarpBlockH = 16;
+constexpr int kWarpBlockW = 128, kWarpBlockH = 32;
 int launch_base2(const BlendArgs& a, const Unit* units, int n, cudaStream_t s);
 int launch_fine(const BlendArgs& a, const Unit* units, int n, cudaStream_t s);
 int dt_rows_in_flight(int maxW, int maxH);

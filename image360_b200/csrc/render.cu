@@ -246,8 +246,19 @@ int Plan::build(const std::vector<TileSpec>& specs, int numBands, bool renderPat
     }
     // ---- work lists -------------------------------------------------------
     std::vector<Unit> units;
-    make_units(8, units);  // the largest list any band height needs
-    unitCap = (int)units.size();
+    {
+        // the largest list any band height and warp form needs
+        const int shape = warpShape;
+        size_t cap = 0;
+        for (int ws : {0, 1})
+        {
+            warpShape = ws;
+            make_units(8, units);
+            cap = std::max(cap, units.size());
+        }
+        warpShape = shape;
+        unitCap = (int)cap;
+    }
     make_units(bandRows, units);
     std::vector<int> ints;
     for (int c = 0; c < nChains; ++c)
@@ -399,7 +410,7 @@ void Plan::make_units(int rows, std::vector<Unit>& units)
         {
             if (!inI(i)) continue;
             const TileDev& T = tiles[items[i].tile];
-            if (render)
+            if (render && warpShape == 1)
             {
                 for (int by = 0; by < (T.h + kWarpBlockH - 1) / kWarpBlockH; ++by)
                     for (int bx = 0; bx < (T.w + kWarpBlockW - 1) / kWarpBlockW; ++bx) units.push_back(Unit{i, bx, by, 0});
@@ -476,6 +487,16 @@ int Plan::set_tuning(int rows, int slots, cudaStream_t s)
     dtSlots = slots;
     drop_graphs();
     return I360B_SUCCESS;
+}
+
+int Plan::set_warp_shape(int shape, cudaStream_t s)
+{
+    if (shape != 0 && shape != 1) return fail(I360B_INVALID_PARAM, "warp shape must be 0 or 1");
+    const int old = warpShape;
+    warpShape = shape;
+    const int rc = set_tuning(bandRows, dtSlots, s);  // remakes and uploads the work lists
+    if (rc != I360B_SUCCESS) warpShape = old;
+    return rc;
 }
 
 int Plan::set_precision(int mode, cudaStream_t s)
@@ -580,7 +601,7 @@ int Plan::enqueue_chain(int c, int first, int last, cudaStream_t s)
         {
         case 0:
             r = L[0];
-            I360B_TRY(render ? launch_warp_tiles(a, dUnits + r.start, r.count, s)
+            I360B_TRY(render ? launch_warp_tiles(a, dUnits + r.start, r.count, warpShape, s)
                              : launch_coverage(a, dUnits + r.start, r.count, s));
             break;
         case 1:
@@ -1058,40 +1079,64 @@ extern "C" int i360b_render_plan_autotune(i360b_render_plan* plan, void* stream,
     cudaEvent_t e0 = nullptr, e1 = nullptr;
     I360B_CUDA(cudaEventCreate(&e0), "autotune events");
     I360B_CUDA(cudaEventCreate(&e1), "autotune events");
-    int bestR = P.bandRows, bestS = P.dtSlots, bestF = P.fusedLevels;
+    int bestR = P.bandRows, bestS = P.dtSlots, bestF = P.fusedLevels, bestW = P.warpShape;
     float best = INFINITY;
     int rc = I360B_SUCCESS;
-    for (int fused : {2, 0})
+    auto trial = [&](float& ms) -> int {
+        int r = P.execute(s, true);  // capture + warm-up
+        if (r != I360B_SUCCESS) return r;
+        cudaEventRecord(e0, s);
+        for (int k = 0; k < 2 && r == I360B_SUCCESS; ++k) r = P.execute(s, true);
+        cudaEventRecord(e1, s);
+        if (r == I360B_SUCCESS) r = P.check(s);
+        ms = 0.0f;
+        cudaEventElapsedTime(&ms, e0, e1);
+        return r;
+    };
+    // 1: warp form x fusion depth at the current band height and ring depth
+    for (int shape : {1, 0})
     {
-        if (fused != 2 && P.storage16) continue;  // FP16 storage exists only with the fused levels
-        if ((rc = P.set_fusion(fused, s)) != I360B_SUCCESS) break;
+        for (int fused : {2, 0})
+        {
+            if (fused != 2 && P.storage16) continue;  // FP16 storage exists only with the fused levels
+            if ((rc = P.set_warp_shape(shape, s)) != I360B_SUCCESS || (rc = P.set_fusion(fused, s)) != I360B_SUCCESS)
+                break;
+            float ms;
+            if ((rc = trial(ms)) != I360B_SUCCESS) break;
+            if (ms < best)
+            {
+                best = ms;
+                bestW = shape;
+                bestF = fused;
+            }
+        }
+        if (rc != I360B_SUCCESS) break;
+    }
+    // 2: band height x ring depth with those
+    if (rc == I360B_SUCCESS && (rc = P.set_warp_shape(bestW, s)) == I360B_SUCCESS &&
+        (rc = P.set_fusion(bestF, s)) == I360B_SUCCESS)
+    {
         for (int rows : {8, 16, 32, 64})
         {
             for (int slots = 2; slots <= maxSlots && rc == I360B_SUCCESS; ++slots)
             {
                 if ((rc = P.set_tuning(rows, slots, s)) != I360B_SUCCESS) break;
-                if ((rc = P.execute(s, true)) != I360B_SUCCESS) break;  // capture + warm-up
-                cudaEventRecord(e0, s);
-                for (int k = 0; k < 2 && rc == I360B_SUCCESS; ++k) rc = P.execute(s, true);
-                cudaEventRecord(e1, s);
-                if (rc == I360B_SUCCESS) rc = P.check(s);
-                float ms = 0.0f;
-                cudaEventElapsedTime(&ms, e0, e1);
-                if (rc == I360B_SUCCESS && ms < best)
+                float ms;
+                if ((rc = trial(ms)) != I360B_SUCCESS) break;
+                if (ms < best)
                 {
                     best = ms;
                     bestR = rows;
                     bestS = slots;
-                    bestF = fused;
                 }
             }
             if (rc != I360B_SUCCESS) break;
         }
-        if (rc != I360B_SUCCESS) break;
     }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
     if (rc != I360B_SUCCESS) return rc;
+    I360B_TRY(P.set_warp_shape(bestW, s));
     I360B_TRY(P.set_fusion(bestF, s));
     I360B_TRY(P.set_tuning(bestR, bestS, s));
     if (bandRows) *bandRows = bestR;
@@ -1100,18 +1145,20 @@ extern "C" int i360b_render_plan_autotune(i360b_render_plan* plan, void* stream,
     return I360B_SUCCESS;
 }
 
-extern "C" int i360b_render_plan_get_tuning(i360b_render_plan* plan, int* bandRows, int* dtSlots, int* fusedLevels)
+extern "C" int i360b_render_plan_get_tuning(i360b_render_plan* plan, int* bandRows, int* dtSlots, int* fusedLevels,
+                                            int* warpShape)
 {
     clear_error();
     if (!plan) return fail(I360B_INVALID_PARAM, "Null plan.");
     if (bandRows) *bandRows = plan->plan.bandRows;
     if (dtSlots) *dtSlots = plan->plan.dtSlots;
     if (fusedLevels) *fusedLevels = plan->plan.fusedLevels;
+    if (warpShape) *warpShape = plan->plan.warpShape;
     return I360B_SUCCESS;
 }
 
 extern "C" int i360b_render_plan_set_tuning(i360b_render_plan* plan, int bandRows, int dtSlots, int fusedLevels,
-                                            void* stream)
+                                            int warpShape, void* stream)
 {
     clear_error();
     if (!plan) return fail(I360B_INVALID_PARAM, "Null plan.");
@@ -1120,7 +1167,9 @@ extern "C" int i360b_render_plan_set_tuning(i360b_render_plan* plan, int bandRow
     const int maxSlots = dt_rows_in_flight(plan->plan.maxW, plan->plan.maxH);
     if (dtSlots != 0 && (dtSlots < 2 || dtSlots > maxSlots))
         return fail(I360B_INVALID_PARAM, "dtSlots must be 0 or 2-%d for this plan.", maxSlots);
+    if (warpShape != 0 && warpShape != 1) return fail(I360B_INVALID_PARAM, "warp shape must be 0 or 1");
     I360B_TRY(plan->plan.set_fusion(fusedLevels, s));
+    plan->plan.warpShape = warpShape;
     return plan->plan.set_tuning(bandRows, dtSlots, s);
 }
 

@@ -67,6 +67,9 @@ struct Plan
     // reference's values bit for bit), 1 FP16 with FP32 arithmetic (the
     // native mode; needs the fused levels, so level 1 is never stored).
     int storage16 = 0;
+    // Tile-warp form: 1 = staged 128x32 blocks (source footprint in shared
+    // memory), 0 = row bands gathering through L1.
+    int warpShape = 1;
     // Limit of the bounded device waits (SM cycles; 0 = give up at the first
     // wait that is not satisfied at once, a test setting).
     long long spinLimit = kSpinCyclesDefault;
@@ -136,6 +139,8 @@ struct Plan
     int set_fusion(int levels, cudaStream_t s);
     // Switches the pyramid storage precision (0 exact, 1 FP16).
     int set_precision(int mode, cudaStream_t s);
+    // Switches the tile-warp form (0 or 1); remakes the work lists.
+    int set_warp_shape(int shape, cudaStream_t s);
     // Changes the bounded-wait limit; the next execute recaptures the graph.
     int set_wait_limit(long long cycles, cudaStream_t s);
     void drop_graphs();

@@ -402,10 +402,11 @@ I360B_API int i360b_render_plan_stats(i360b_render_plan* plan, void* stream, i36
 I360B_API int i360b_render_plan_profile(i360b_render_plan* plan, void* stream, float* stageMs, int maxStages);
 I360B_API const char* i360b_render_stage_name(int stage);
 /* Autotuner: times the plan's own execute (two runs after a warm-up, CUDA
- * events on `stream`) for both level-fusion depths (0, 2), every band-unit
- * height of the per-pixel kernels (8, 16, 32, 64 rows) and every ring depth
- * of the chamfer transform that fits (2 to 4 row groups), and keeps the
- * fastest (read the fusion depth back with i360b_render_plan_get_tuning).  The output of every
+ * events on `stream`), first for both tile-warp forms and level-fusion
+ * depths, then with the faster pair for every band-unit height of the
+ * per-pixel kernels (8, 16, 32, 64 rows) and every ring depth of the chamfer
+ * transform that fits (2 to 4 row groups), and keeps the fastest (read the
+ * fusion depth and warp form back with i360b_render_plan_get_tuning).  The output of every
  * setting is identical (the settings only partition the same work), so
  * tuning never changes results.  The chosen values and the best time of one
  * execute are returned when the pointers are non-null.  Synchronous; the
@@ -414,15 +415,18 @@ I360B_API int i360b_render_plan_autotune(i360b_render_plan* plan, void* stream, 
                                          float* bestMs);
 /* The plan's tuning: rows per band unit of the per-pixel kernels (8, 16, 32
  * or 64), chamfer ring slots (0 = as many as fit, else 2 to the number that
- * fits), and the level-fusion depth of the pyramid: 2 computes levels 0 and
- * 1 on chip (only levels >= 2 of the pyramids are written to memory), 0
- * materialises every level.  Every setting renders the same bits.  No
- * reference counterpart (the reference's blend is a fixed CPU loop).
- * set_tuning is synchronous on `stream`; the next execute recaptures the
- * plan's graph.  The autotuner searches all three. */
-I360B_API int i360b_render_plan_get_tuning(i360b_render_plan* plan, int* bandRows, int* dtSlots, int* fusedLevels);
+ * fits), the level-fusion depth of the pyramid (2 computes levels 0 and 1 on
+ * chip, so only levels >= 2 of the pyramids are written to memory; 0
+ * materialises every level) and the tile warp's form (1: 128x32 blocks whose
+ * source footprint is staged in shared memory; 0: row bands gathering
+ * through L1).  Every setting renders the same bits.  No reference
+ * counterpart (the reference's blend is a fixed CPU loop).  set_tuning is
+ * synchronous on `stream`; the next execute recaptures the plan's graph.
+ * The autotuner searches all four. */
+I360B_API int i360b_render_plan_get_tuning(i360b_render_plan* plan, int* bandRows, int* dtSlots, int* fusedLevels,
+                                           int* warpShape);
 I360B_API int i360b_render_plan_set_tuning(i360b_render_plan* plan, int bandRows, int dtSlots, int fusedLevels,
-                                           void* stream);
+                                           int warpShape, void* stream);
 /* Precision of the render's stored pyramid levels.  EXACT keeps them in
  * FP32 and renders the CPU backend's output bit for bit.  FP16 is the native
  * mode: the levels a plan keeps in memory (levels >= 2 with the fused

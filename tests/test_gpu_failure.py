@@ -109,7 +109,7 @@ def test_two_threads_keep_their_own_errors(backend, oracle_c):
     bufs = []
     for k in range(3):
         b = np.zeros((40, 64, 3), np.uint16)
-        b[:, 10 * k:40 + 10 * k] = rng.integers(100, 30000, (40, 30, 3))
+        b[:, 10 * k:40 + 10 * k] = rng.integers(100, 30000, (40, 40, 3))
         bufs.append(b)
     want_blend = oracle_c.blend(bufs, 4)
     errors = []
