@@ -2087,11 +2087,11 @@ constexpr int kB1W = 2 * kB2W + 3, kB1H = 2 * kB2H + 3;  // its level-1 rectangl
 constexpr int kB0S = 2 * kB1W + 3 + 3;              // level-0 footprint row stride: at most 137 columns from
                                                     // a 4-pixel aligned start, 35 whole groups
 constexpr int kB0H = 2 * kB1H + 3;                  // level-0 footprint rows (at most)
-constexpr int kRun = 7;                             // level-1 rows per streaming task
+constexpr int kRun = 4;                             // k_base2's level-1 rows per streaming task
 
 constexpr int kFW = 64, kFH = 32;                   // output pixels per k_fine CTA
-constexpr int kFRun = 3;                            // k_fine's level-1 rows per streaming task (more tasks than
-                                                    // threads would idle otherwise: the window is ~34 wide)
+constexpr int kFRun = 2;                            // k_fine's level-1 rows per streaming task (column pairs x
+                                                    // 2 rows: ~150 tasks on a ~34 x 18 window)
 constexpr int kF1W = 36, kF1H = 20;                 // its level-1 window (bound; checked)
 constexpr int kF0S = 2 * kF1W + 8;                  // level-0 footprint row stride: the footprint's
                                                     // at most 78 columns rounded up to whole 4-pixel groups
@@ -2100,29 +2100,32 @@ constexpr int kF2W = 22, kF2H = 14;                 // level-2 window (bound; ch
 
 // Stages contributor k's level-0 pixels of tile rows [ry0, ry1] x columns
 // [cx0, cx1] as packed pixels (r | g << 16, b | cov << 16 | own << 17) at
-// sm[(y - ry0) * stride + (x - (cx0 & ~3))], in whole groups of four pixels
-// from the aligned start (stride must hold them: a multiple of 4 at least
-// cx1 - (cx0 & ~3) + 1).  `own` is the owner map of the same rows (global,
-// or shared with row stride ownStride when ownSm is set).  A group is read
-// as three 8-byte words when the image rows allow it.
+// sm[(y - rowBase) * stride + (x - colBase)] (colBase a multiple of 4, at
+// most cx0), in whole groups of four pixels from cx0 & ~3 (stride must hold
+// them: a multiple of 4 at least cx1 - colBase + 1).  `own` is the owner map
+// of the same rows: global, or shared with row stride ownStride and the same
+// bases when ownSm is set.  A group is read as three 8-byte words when the
+// image rows allow it.
 __device__ __forceinline__ void stage_level0(const unsigned short* img, const signed char* own, int ownStride,
                                              bool ownSm, signed char k, int W, int ry0, int ry1, int cx0, int cx1,
-                                             PackedPx* sm, int stride)
+                                             PackedPx* sm, int stride, int rowBase, int colBase)
 {
-    const int cxa = cx0 & ~3;
-    const int ng = ((cx1 - cxa) >> 2) + 1;
+    const int cs = cx0 & ~3;
+    const int ng = ((cx1 - cs) >> 2) + 1;
     const int nr = ry1 - ry0 + 1;
     const bool fast = (W & 3) == 0 && (reinterpret_cast<uintptr_t>(img) & 7) == 0;
     for (int t = threadIdx.x; t < nr * ng; t += blockDim.x)
     {
         const int r = t / ng, g = t - r * ng;
-        const int c = cxa + 4 * g;
-        const size_t p = (size_t)(ry0 + r) * W + c;
-        PackedPx* d = sm + r * stride + 4 * g;
+        const int c = cs + 4 * g;
+        const int y = ry0 + r;
+        const size_t p = (size_t)y * W + c;
+        PackedPx* d = sm + (y - rowBase) * stride + (c - colBase);
         signed char o[4];
 #pragma unroll
         for (int e = 0; e < 4; ++e)
-            o[e] = (c + e < W) ? (ownSm ? own[r * ownStride + (c + e - cxa)] : __ldg(own + p + e)) : (signed char)-1;
+            o[e] = (c + e < W) ? (ownSm ? own[(y - rowBase) * ownStride + (c + e - colBase)] : __ldg(own + p + e))
+                               : (signed char)-1;
         if (fast)
         {
             const uint2* w = reinterpret_cast<const uint2*>(img + p * 3);
@@ -2145,58 +2148,71 @@ __device__ __forceinline__ void stage_level0(const unsigned short* img, const si
     }
 }
 
-// Exact level-1 values (num r, g, b; den; weight) of level-1 column X1 and
-// rows Y1s .. Y1s + R - 1 from a staged footprint (tile rows from ry0,
-// columns from cxa), handed to emit(m, nr, ng, nb, den, wg) in row order.
-// Integer sums of the [1,4,6,4,1] x [1,4,6,4,1] stencil over clamped level-0
-// coordinates, streamed row by row (see k_down0s for why they are exact).
+// Exact level-1 values (num r, g, b; den; weight) of level-1 columns X1 and
+// X1 + 1 and rows Y1s .. Y1s + R - 1 from a staged footprint (tile rows from
+// ry0, columns from cxa), handed to emit(col, m, nr, ng, nb, den, wg) in row
+// order (col 0 for X1, 1 for X1 + 1, only when `two`).  Integer sums of the
+// [1,4,6,4,1] x [1,4,6,4,1] stencil over clamped level-0 coordinates,
+// streamed row by row (see k_down0s for why they are exact).  The two
+// columns share three of their five taps: column X1 reads clamped columns
+// 2 X1 - 2 .. 2 X1 + 2 and X1 + 1 reads 2 X1 .. 2 X1 + 4, which are taps 2..6
+// of the same seven (clamping commutes with the shift).  Taps past cmax
+// (beyond the staged columns: only a second column that is not emitted
+// reaches them) read column cmax instead.
 template <typename Emit>
-__device__ __forceinline__ void level1_column(const PackedPx* sm, int stride, int ry0, int cxa, int W, int H,
-                                              int X1, int Y1s, int R, Emit emit)
+__device__ __forceinline__ void level1_pair(const PackedPx* sm, int stride, int ry0, int cxa, int cmax, int W, int H,
+                                            int X1, bool two, int Y1s, int R, Emit emit)
 {
-    int col[5];
+    int col[7];
 #pragma unroll
-    for (int i = 0; i < 5; ++i) col[i] = min(max(2 * X1 - 2 + i, 0), W - 1) - cxa;
-    int P[4] = {0, 0, 0, 0}, Q[4] = {0, 0, 0, 0}, Rr[4] = {0, 0, 0, 0};
+    for (int i = 0; i < 7; ++i) col[i] = min(min(max(2 * X1 - 2 + i, 0), W - 1), cmax) - cxa;
+    int P[2][4] = {}, Q[2][4] = {}, Rr[2][4] = {};
     const float s256 = 1.0f / 256.0f;
     for (int r = 0; r <= 2 * R + 2; ++r)
     {
         const int gy = min(max(2 * Y1s - 2 + r, 0), H - 1);
         const PackedPx* row = sm + (gy - ry0) * stride;
-        int t[4] = {0, 0, 0, 0};
+        int cv[7][4];
 #pragma unroll
-        for (int i = 0; i < 5; ++i)
-        {
-            int cv[4];
-            px_channels(row[col[i]], cv);
-            const int wgt = (i == 0 || i == 4) ? 1 : (i == 2 ? 6 : 4);
+        for (int i = 0; i < 7; ++i) px_channels(row[col[i]], cv[i]);
+        int t[2][4];
 #pragma unroll
-            for (int ch = 0; ch < 4; ++ch) t[ch] += wgt * cv[ch];
-        }
+        for (int c = 0; c < 2; ++c)
+#pragma unroll
+            for (int ch = 0; ch < 4; ++ch)
+                t[c][ch] = cv[2 * c][ch] + 4 * cv[2 * c + 1][ch] + 6 * cv[2 * c + 2][ch] + 4 * cv[2 * c + 3][ch] +
+                           cv[2 * c + 4][ch];
         if ((r & 1) == 0)
         {
 #pragma unroll
-            for (int ch = 0; ch < 4; ++ch)
-            {
-                P[ch] += t[ch];
-                Q[ch] += 6 * t[ch];
-                Rr[ch] = t[ch];
-            }
+            for (int c = 0; c < 2; ++c)
+#pragma unroll
+                for (int ch = 0; ch < 4; ++ch)
+                {
+                    P[c][ch] += t[c][ch];
+                    Q[c][ch] += 6 * t[c][ch];
+                    Rr[c][ch] = t[c][ch];
+                }
             const int m = (r >> 1) - 2;
             if (m >= 0)
-                emit(m, fmul((float)P[0], s256), fmul((float)P[1], s256), fmul((float)P[2], s256),
-                     fmul((float)(P[3] >> 16), s256), fmul((float)(P[3] & 0xffff), s256));
+#pragma unroll
+                for (int c = 0; c < 2; ++c)
+                    if (c == 0 || two)
+                        emit(c, m, fmul((float)P[c][0], s256), fmul((float)P[c][1], s256), fmul((float)P[c][2], s256),
+                             fmul((float)(P[c][3] >> 16), s256), fmul((float)(P[c][3] & 0xffff), s256));
         }
         else
         {
 #pragma unroll
-            for (int ch = 0; ch < 4; ++ch)
-            {
-                Q[ch] += 4 * t[ch];
-                Rr[ch] += 4 * t[ch];
-                P[ch] = Q[ch];
-                Q[ch] = Rr[ch];
-            }
+            for (int c = 0; c < 2; ++c)
+#pragma unroll
+                for (int ch = 0; ch < 4; ++ch)
+                {
+                    Q[c][ch] += 4 * t[c][ch];
+                    Rr[c][ch] += 4 * t[c][ch];
+                    P[c][ch] = Q[c][ch];
+                    Q[c][ch] = Rr[c][ch];
+                }
         }
     }
 }
@@ -2239,25 +2255,26 @@ __global__ void __launch_bounds__(256) k_base2(BlendArgs a, const Unit* __restri
         return;
     }
     const int cxa = cx0 & ~3;
-    stage_level0(it.img, T.owner, 0, false, (signed char)it.k, W, ry0, ry1, cx0, cx1, S.px, kB0S);
+    stage_level0(it.img, T.owner, 0, false, (signed char)it.k, W, ry0, ry1, cx0, cx1, S.px, kB0S, ry0, cxa);
     __syncthreads();
-    // level-1 rectangle, a column run of kRun rows per task
+    // level-1 rectangle: a pair of columns and a run of kRun rows per task
     const int nX1 = X1hi - X1lo + 1, nY1 = Y1hi - Y1lo + 1;
+    const int nPairs = (nX1 + 1) >> 1;
     const int nRuns = (nY1 + kRun - 1) / kRun;
-    for (int task = threadIdx.x; task < nX1 * nRuns; task += blockDim.x)
+    for (int task = threadIdx.x; task < nPairs * nRuns; task += blockDim.x)
     {
-        const int run = task / nX1, cx = task - run * nX1;
+        const int run = task / nPairs, cx = 2 * (task - run * nPairs);
         const int Y1s = Y1lo + run * kRun;
         const int R = min(kRun, Y1hi - Y1s + 1);
-        level1_column(S.px, kB0S, ry0, cxa, W, H, X1lo + cx, Y1s, R,
-                      [&](int m, float nr, float ng, float nb, float den, float wg) {
-                          const int ry = Y1s + m - Y1lo;
-                          S.l1[0][ry][cx] = nr;
-                          S.l1[1][ry][cx] = ng;
-                          S.l1[2][ry][cx] = nb;
-                          S.l1[3][ry][cx] = den;
-                          S.l1[4][ry][cx] = wg;
-                      });
+        level1_pair(S.px, kB0S, ry0, cxa, cx1, W, H, X1lo + cx, cx + 1 < nX1, Y1s, R,
+                    [&](int c, int m, float nr, float ng, float nb, float den, float wg) {
+                        const int ry = Y1s + m - Y1lo;
+                        S.l1[0][ry][cx + c] = nr;
+                        S.l1[1][ry][cx + c] = ng;
+                        S.l1[2][ry][cx + c] = nb;
+                        S.l1[3][ry][cx + c] = den;
+                        S.l1[4][ry][cx + c] = wg;
+                    });
     }
     __syncthreads();
     // horizontal taps at the level-2 columns (over clamped level-1 columns)
@@ -2293,7 +2310,7 @@ __global__ void __launch_bounds__(256) k_base2(BlendArgs a, const Unit* __restri
 
 struct FineSmem
 {
-    PackedPx px[kF0H * kF0S];                  // one contributor's level-0 footprint
+    PackedPx px[kF0H * kF0S];                  // one contributor's level-0 footprint (the part it needs)
     signed char own[kF0H * kF0S];              // the tile's owner map over the footprint
     float g1[3][kF1H][kF1W];                   // that contributor's G1 on the level-1 window; then recon1
     float w1[kF1H][kF1W];                      // its level-1 weight
@@ -2302,6 +2319,7 @@ struct FineSmem
     const unsigned short* img[kMaxTileItems];
     const float4* nd[kMaxTileItems];
     uint32_t set[kMaxTileItems / 32];          // contributors owning a footprint pixel
+    int obox[4];                               // the footprint pixels one contributor owns: x0, y0, x1, y1
     // Up taps, tabulated: the align-corners coefficients are separable (the x
     // part depends on x only, the y part on y only), so the block's columns
     // and rows (level 0 -> 1) and the window's (level 1 -> 2) are computed
@@ -2310,6 +2328,16 @@ struct FineSmem
     float fx0[kFW], fy0[kFH], fx1[kF1W], fy1[kF1H];
 };
 
+// Per 64x32 block of output pixels (see the section comment).  Threads own
+// pixels tid + 256 j (j < 8): lanes take consecutive columns of one row, so
+// shared-memory reads of neighbouring pixels and the output stores are
+// contiguous across a warp.  For each contributor owning a footprint pixel,
+// in index order: the footprint rows and columns within 6 of the pixels it
+// owns are staged (a level-1 task reads at most 6 beyond its own pixels), and
+// only the level-1 tasks (pairs of columns x kFRun rows) whose level-0
+// footprint holds one of those pixels are computed - elsewhere its level-1
+// weight is exactly zero, so its blended-band term is +-0 (skipped) and no
+// pixel it owns takes a tap there.
 __global__ void __launch_bounds__(256) k_fine(BlendArgs a, const Unit* __restrict__ units)
 {
     extern __shared__ __align__(16) unsigned char fine_raw[];
@@ -2320,12 +2348,16 @@ __global__ void __launch_bounds__(256) k_fine(BlendArgs a, const Unit* __restric
     const int X0 = u.bx * kFW, Y0 = u.by * kFH;
     const int xe = min(X0 + kFW - 1, W - 1), ye = min(Y0 + kFH - 1, H - 1);
     const int tid = threadIdx.x;
-    // this thread's outputs: 8 pixels of one row
-    const int oy = Y0 + (tid >> 3), ox = X0 + (tid & 7) * 8;
-    const bool rowOk = oy <= ye;
-    int own[8];
+    // this thread's outputs: column ox of rows oy0 + 4 j
+    const int ox = X0 + (tid & (kFW - 1)), oy0 = Y0 + (tid >> 6);
+    constexpr int kPx = kFW * kFH / 256;  // 8
+    int own[kPx];
 #pragma unroll
-    for (int i = 0; i < 8; ++i) own[i] = (rowOk && ox + i <= xe) ? (int)__ldg(T.owner + (size_t)oy * W + ox + i) : -2;
+    for (int j = 0; j < kPx; ++j)
+    {
+        const int y = oy0 + 4 * j;
+        own[j] = (ox <= xe && y <= ye) ? (int)__ldg(T.owner + (size_t)y * W + ox) : -2;
+    }
     for (int k = tid; k < K; k += blockDim.x)
     {
         const ItemDev& it = a.items[T.firstItem + k];
@@ -2334,21 +2366,21 @@ __global__ void __launch_bounds__(256) k_fine(BlendArgs a, const Unit* __restric
     }
     if (tid < kMaxTileItems / 32) S.set[tid] = 0u;
     __syncthreads();  // the set is cleared before any thread adds to it
-    unsigned short* outRow = T.out + ((size_t)oy * W + ox) * 3;
     if (T.bands == 1)
     {
         // one band: the output is the owner's pixel (SeamBlend.cpp:527-545)
 #pragma unroll
-        for (int i = 0; i < 8; ++i)
+        for (int j = 0; j < kPx; ++j)
         {
-            if (own[i] == -2) continue;
-            unsigned short* o = outRow + 3 * i;
-            if (own[i] < 0)
+            if (own[j] == -2) continue;
+            const size_t q = (size_t)(oy0 + 4 * j) * W + ox;
+            unsigned short* o = T.out + q * 3;
+            if (own[j] < 0)
             {
                 o[0] = o[1] = o[2] = 0;
                 continue;
             }
-            const unsigned short* p = S.img[own[i]] + ((size_t)oy * W + ox + i) * 3;
+            const unsigned short* p = S.img[own[j]] + q * 3;
             const float r[3] = {(float)__ldg(p), (float)__ldg(p + 1), (float)__ldg(p + 2)};
             final_store(o, r);
         }
@@ -2436,10 +2468,10 @@ __global__ void __launch_bounds__(256) k_fine(BlendArgs a, const Unit* __restric
         for (int idx = tid; idx < nP * nQ; idx += blockDim.x)
         {
             const int r = idx / nP, c = idx - r * nP;
-            const float* s = rc2 + ((size_t)(Q0 + r) * lw2 + P0 + c) * 3;
-            S.r2[0][r][c] = __ldg(s);
-            S.r2[1][r][c] = __ldg(s + 1);
-            S.r2[2][r][c] = __ldg(s + 2);
+            const float* src = rc2 + ((size_t)(Q0 + r) * lw2 + P0 + c) * 3;
+            S.r2[0][r][c] = __ldg(src);
+            S.r2[1][r][c] = __ldg(src + 1);
+            S.r2[2][r][c] = __ldg(src + 2);
         }
     }
     __syncthreads();
@@ -2447,11 +2479,14 @@ __global__ void __launch_bounds__(256) k_fine(BlendArgs a, const Unit* __restric
     float acc[3][3];
 #pragma unroll
     for (int j = 0; j < 3; ++j) acc[j][0] = acc[j][1] = acc[j][2] = 0.0f;
-    float lap[8][3];
+    float lap[kPx][3];
 #pragma unroll
-    for (int i = 0; i < 8; ++i) lap[i][0] = lap[i][1] = lap[i][2] = 0.0f;
+    for (int j = 0; j < kPx; ++j) lap[j][0] = lap[j][1] = lap[j][2] = 0.0f;
     const int nWin = nA * nB;
+    const int nPairs = (nA + 1) >> 1;
     const int nRuns = (nB + kFRun - 1) / kFRun;
+    const short2 xt0 = S.tx0[tid & (kFW - 1)];
+    const float wx0 = S.fx0[tid & (kFW - 1)];
     for (int w = 0; w < kMaxTileItems / 32; ++w)
     {
         uint32_t m = S.set[w];
@@ -2459,7 +2494,44 @@ __global__ void __launch_bounds__(256) k_fine(BlendArgs a, const Unit* __restric
         {
             const int k = 32 * w + __ffs(m) - 1;
             m &= m - 1;
-            stage_level0(S.img[k], S.own, kF0S, true, (signed char)k, W, ry0, ry1, cxa, cx1, S.px, kF0S);
+            // the footprint pixels k owns (footprint-relative box)
+            if (tid == 0)
+            {
+                S.obox[0] = S.obox[1] = 0x7fffffff;
+                S.obox[2] = S.obox[3] = -1;
+            }
+            __syncthreads();
+            {
+                int bx0 = 0x7fffffff, by0 = 0x7fffffff, bx1 = -1, by1 = -1;
+                for (int idx = tid; idx < nr * ncol; idx += blockDim.x)
+                {
+                    const int r = idx / ncol, c = idx - r * ncol;
+                    if (S.own[r * kF0S + c] == (signed char)k)
+                    {
+                        bx0 = min(bx0, c);
+                        bx1 = max(bx1, c);
+                        by0 = min(by0, r);
+                        by1 = max(by1, r);
+                    }
+                }
+                bx0 = __reduce_min_sync(kFull, bx0);
+                by0 = __reduce_min_sync(kFull, by0);
+                bx1 = __reduce_max_sync(kFull, bx1);
+                by1 = __reduce_max_sync(kFull, by1);
+                if ((tid & 31) == 0 && bx1 >= 0)
+                {
+                    atomicMin(&S.obox[0], bx0);
+                    atomicMin(&S.obox[1], by0);
+                    atomicMax(&S.obox[2], bx1);
+                    atomicMax(&S.obox[3], by1);
+                }
+            }
+            __syncthreads();
+            const int ob0 = S.obox[0], ob1 = S.obox[1], ob2 = S.obox[2], ob3 = S.obox[3];
+            // stage the footprint within 6 of the owned box
+            const int sy0 = max(ry0, ry0 + ob1 - 6), sy1 = min(ry1, ry0 + ob3 + 6);
+            const int sx0 = max(cx0, cxa + ob0 - 6), sx1 = min(cx1, cxa + ob2 + 6);
+            stage_level0(S.img[k], S.own, kF0S, true, (signed char)k, W, sy0, sy1, sx0, sx1, S.px, kF0S, ry0, cxa);
             if (!top1)
             {
                 const size_t g2 = T.loff[2];
@@ -2473,21 +2545,35 @@ __global__ void __launch_bounds__(256) k_fine(BlendArgs a, const Unit* __restric
                 }
             }
             __syncthreads();
-            // level-1 values of contributor k on the window
-            for (int task = tid; task < nA * nRuns; task += blockDim.x)
+            // level-1 values of contributor k on the window: the tasks whose
+            // level-0 footprint meets the owned box; zero weight elsewhere
+            for (int task = tid; task < nPairs * nRuns; task += blockDim.x)
             {
-                const int run = task / nA, c = task - run * nA;
+                const int run = task / nPairs, c = 2 * (task - run * nPairs);
                 const int Y1s = B0 + run * kFRun;
                 const int R = min(kFRun, B1 - Y1s + 1);
-                level1_column(S.px, kF0S, ry0, cxa, W, H, A0 + c, Y1s, R,
-                              [&](int mm, float n0, float n1, float n2, float den, float wg) {
-                                  const int r = Y1s + mm - B0;
-                                  const float3 g = gauss_of(make_float4(n0, n1, n2, den));
-                                  S.g1[0][r][c] = g.x;
-                                  S.g1[1][r][c] = g.y;
-                                  S.g1[2][r][c] = g.z;
-                                  S.w1[r][c] = wg;
-                              });
+                const bool two = c + 1 < nA;
+                const int X1 = A0 + c;
+                const int fr0 = max(2 * Y1s - 2, 0) - ry0, fr1 = min(2 * (Y1s + R - 1) + 2, H - 1) - ry0;
+                const int fc0 = max(2 * X1 - 2, 0) - cxa, fc1 = min(2 * (X1 + (two ? 1 : 0)) + 2, W - 1) - cxa;
+                if (fr1 < ob1 || fr0 > ob3 || fc1 < ob0 || fc0 > ob2)
+                {
+                    for (int rr = 0; rr < R; ++rr)
+                    {
+                        S.w1[Y1s + rr - B0][c] = 0.0f;
+                        if (two) S.w1[Y1s + rr - B0][c + 1] = 0.0f;
+                    }
+                    continue;
+                }
+                level1_pair(S.px, kF0S, ry0, cxa, cx1, W, H, X1, two, Y1s, R,
+                            [&](int cc, int mm, float n0, float n1, float n2, float den, float wg) {
+                                const int r = Y1s + mm - B0;
+                                const float3 g = gauss_of(make_float4(n0, n1, n2, den));
+                                S.g1[0][r][c + cc] = g.x;
+                                S.g1[1][r][c + cc] = g.y;
+                                S.g1[2][r][c + cc] = g.z;
+                                S.w1[r][c + cc] = wg;
+                            });
             }
             __syncthreads();
             // blended level-1 band: weight x Laplacian, in contributor order
@@ -2514,18 +2600,18 @@ __global__ void __launch_bounds__(256) k_fine(BlendArgs a, const Unit* __restric
             }
             // level-0 Laplacian of the pixels k owns: img - Up(G1)
 #pragma unroll
-            for (int i = 0; i < 8; ++i)
+            for (int j = 0; j < kPx; ++j)
             {
-                if (own[i] != k) continue;
-                const int x = ox + i;
-                const short2 xt = S.tx0[x - X0], yt = S.ty0[oy - Y0];
-                const float wx = S.fx0[x - X0], wy = S.fy0[oy - Y0];
+                if (own[j] != k) continue;
+                const int y = oy0 + 4 * j;
+                const short2 yt = S.ty0[y - Y0];
+                const float wy = S.fy0[y - Y0];
                 int cv[4];
-                px_channels(S.px[(oy - ry0) * kF0S + (x - cxa)], cv);
+                px_channels(S.px[(y - ry0) * kF0S + (ox - cxa)], cv);
 #pragma unroll
                 for (int ch = 0; ch < 3; ++ch)
-                    lap[i][ch] = fsub((float)cv[ch], up_mix(S.g1[ch][yt.x][xt.x], S.g1[ch][yt.x][xt.y],
-                                                            S.g1[ch][yt.y][xt.x], S.g1[ch][yt.y][xt.y], wx, wy));
+                    lap[j][ch] = fsub((float)cv[ch], up_mix(S.g1[ch][yt.x][xt0.x], S.g1[ch][yt.x][xt0.y],
+                                                            S.g1[ch][yt.y][xt0.x], S.g1[ch][yt.y][xt0.y], wx0, wy));
             }
             __syncthreads();
         }
@@ -2552,42 +2638,28 @@ __global__ void __launch_bounds__(256) k_fine(BlendArgs a, const Unit* __restric
         S.g1[2][r][c] = v[2];
     }
     __syncthreads();
-    if (!rowOk) return;
     // output: clamp(lap0 + Up(recon1)) + 0.5, zero where nobody owns
-    unsigned short res[24];
 #pragma unroll
-    for (int i = 0; i < 8; ++i)
+    for (int j = 0; j < kPx; ++j)
     {
-        res[3 * i] = res[3 * i + 1] = res[3 * i + 2] = 0;
-        if (own[i] < 0) continue;
-        const short2 xt = S.tx0[ox + i - X0], yt = S.ty0[oy - Y0];
-        const float wx = S.fx0[ox + i - X0], wy = S.fy0[oy - Y0];
-        float r[3];
+        if (own[j] == -2) continue;
+        const int y = oy0 + 4 * j;
+        unsigned short res[3] = {0, 0, 0};
+        if (own[j] >= 0)
+        {
+            const short2 yt = S.ty0[y - Y0];
+            const float wy = S.fy0[y - Y0];
+            float r[3];
 #pragma unroll
-        for (int ch = 0; ch < 3; ++ch)
-            r[ch] = fadd(lap[i][ch], up_mix(S.g1[ch][yt.x][xt.x], S.g1[ch][yt.x][xt.y], S.g1[ch][yt.y][xt.x],
-                                            S.g1[ch][yt.y][xt.y], wx, wy));
-        final_store(res + 3 * i, r);
-    }
-    if (ox + 7 <= xe && (reinterpret_cast<uintptr_t>(outRow) & 15) == 0)
-    {
-        uint4* o4 = reinterpret_cast<uint4*>(outRow);
-#pragma unroll
-        for (int k = 0; k < 3; ++k)
-            o4[k] = make_uint4((uint32_t)res[8 * k] | ((uint32_t)res[8 * k + 1] << 16),
-                               (uint32_t)res[8 * k + 2] | ((uint32_t)res[8 * k + 3] << 16),
-                               (uint32_t)res[8 * k + 4] | ((uint32_t)res[8 * k + 5] << 16),
-                               (uint32_t)res[8 * k + 6] | ((uint32_t)res[8 * k + 7] << 16));
-    }
-    else
-    {
-        for (int i = 0; i < 8; ++i)
-            if (own[i] != -2)
-            {
-                outRow[3 * i] = res[3 * i];
-                outRow[3 * i + 1] = res[3 * i + 1];
-                outRow[3 * i + 2] = res[3 * i + 2];
-            }
+            for (int ch = 0; ch < 3; ++ch)
+                r[ch] = fadd(lap[j][ch], up_mix(S.g1[ch][yt.x][xt0.x], S.g1[ch][yt.x][xt0.y], S.g1[ch][yt.y][xt0.x],
+                                                S.g1[ch][yt.y][xt0.y], wx0, wy));
+            final_store(res, r);
+        }
+        unsigned short* o = T.out + ((size_t)y * W + ox) * 3;
+        o[0] = res[0];
+        o[1] = res[1];
+        o[2] = res[2];
     }
 }
 }  // namespace
