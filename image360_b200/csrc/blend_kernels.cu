@@ -155,10 +155,10 @@ __device__ __forceinline__ bool warp_pos(const WarpItem& it, float dX, const flo
     sx = fdiv(sx, sw1);
     sy = fdiv(sy, sw1);
     if (!(sx >= 0.0f && sx < (float)(it.srcW - 1) && sy >= 0.0f && sy < (float)(it.srcH - 1))) return false;
-    x0 = (int)floorf(sx);
-    y0 = (int)floorf(sy);
-    fx = fsub(sx, (float)x0);
-    fy = fsub(sy, (float)y0);
+    x0 = (int)f2u_floor(sx);  // 0 <= sx, sy < 2^23 here
+    y0 = (int)f2u_floor(sy);
+    fx = fsub(sx, u2f((uint32_t)x0));
+    fy = fsub(sy, u2f((uint32_t)y0));
     return true;
 }
 
@@ -173,10 +173,10 @@ __device__ __forceinline__ void warp_mix(const WarpItem& it, float fx, float fy,
 #pragma unroll
     for (int c = 0; c < 3; ++c)
     {
-        const float v = fadd(fadd(fadd(fmul(w00, (float)t00[c]), fmul(w10, (float)t10[c])), fmul(w01, (float)t01[c])),
-                             fmul(w11, (float)t11[c]));
+        const float v = fadd(fadd(fadd(fmul(w00, u2f(t00[c])), fmul(w10, u2f(t10[c]))), fmul(w01, u2f(t01[c]))),
+                             fmul(w11, u2f(t11[c])));
         unsigned short q = clamp_trunc_u16(v);
-        if (it.applyGain) q = clamp_trunc_u16(fmul((float)q, it.gain));
+        if (it.applyGain) q = clamp_trunc_u16(fmul(u2f(q), it.gain));
         o[c] = q;
     }
 }
@@ -1904,7 +1904,7 @@ __device__ __forceinline__ void final_store(unsigned short* o, const float* r)
         float v = r[ch];
         v = v < 65535.0f ? v : 65535.0f;
         v = 0.0f < v ? v : 0.0f;
-        o[ch] = (unsigned short)__float2uint_rz(fadd(v, 0.5f));
+        o[ch] = (unsigned short)f2u_floor(fadd(v, 0.5f));  // v + 0.5 in [0.5, 65535.5]
     }
 }
 
@@ -1921,7 +1921,7 @@ __device__ __noinline__ void final_pixel(const TileDev& T, const ItemCache& C, c
     const int W = T.w;
     const int y = (int)(p / W), x = (int)(p - (long long)y * W);
     const unsigned short* px = C.img[own] + p * 3;
-    float r[3] = {(float)__ldg(px), (float)__ldg(px + 1), (float)__ldg(px + 2)};
+    float r[3] = {u2f(__ldg(px)), u2f(__ldg(px + 1)), u2f(__ldg(px + 2))};
     if (T.bands > 1)
     {
         const UpCoef c = up_coef_s(T.usx[0], T.usy[0], uw, uh, x, y);
@@ -1995,7 +1995,7 @@ __device__ __forceinline__ void final_quad(const TileDev& T, const ItemCache& C,
             }
         }
         const float wx = c.wx, wy = c.wy;
-        float r[3] = {(float)__ldg(px + 3 * i), (float)__ldg(px + 3 * i + 1), (float)__ldg(px + 3 * i + 2)};
+        float r[3] = {u2f(__ldg(px + 3 * i)), u2f(__ldg(px + 3 * i + 1)), u2f(__ldg(px + 3 * i + 2))};
         const float lap[3] = {fsub(r[0], up_mix(L.g0.x, R.g0.x, L.g1.x, R.g1.x, wx, wy)),
                               fsub(r[1], up_mix(L.g0.y, R.g0.y, L.g1.y, R.g1.y, wx, wy)),
                               fsub(r[2], up_mix(L.g0.z, R.g0.z, L.g1.z, R.g1.z, wx, wy))};
@@ -2381,7 +2381,7 @@ __global__ void __launch_bounds__(256) k_fine(BlendArgs a, const Unit* __restric
                 continue;
             }
             const unsigned short* p = S.img[own[j]] + q * 3;
-            const float r[3] = {(float)__ldg(p), (float)__ldg(p + 1), (float)__ldg(p + 2)};
+            const float r[3] = {u2f(__ldg(p)), u2f(__ldg(p + 1)), u2f(__ldg(p + 2))};
             final_store(o, r);
         }
         return;
@@ -2610,7 +2610,7 @@ __global__ void __launch_bounds__(256) k_fine(BlendArgs a, const Unit* __restric
                 px_channels(S.px[(y - ry0) * kF0S + (ox - cxa)], cv);
 #pragma unroll
                 for (int ch = 0; ch < 3; ++ch)
-                    lap[j][ch] = fsub((float)cv[ch], up_mix(S.g1[ch][yt.x][xt0.x], S.g1[ch][yt.x][xt0.y],
+                    lap[j][ch] = fsub(u2f((uint32_t)cv[ch]), up_mix(S.g1[ch][yt.x][xt0.x], S.g1[ch][yt.x][xt0.y],
                                                             S.g1[ch][yt.y][xt0.x], S.g1[ch][yt.y][xt0.y], wx0, wy));
             }
             __syncthreads();

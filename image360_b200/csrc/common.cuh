@@ -21,6 +21,18 @@ __device__ __forceinline__ float fsub(float a, float b) { return __fsub_rn(a, b)
 __device__ __forceinline__ float fmul(float a, float b) { return __fmul_rn(a, b); }
 __device__ __forceinline__ float fdiv(float a, float b) { return __fdiv_rn(a, b); }
 
+// Exact integer <-> float conversions on the FMA and ALU pipes.  The
+// conversion instructions (I2F/F2I) issue on the XU pipe at a fraction of the
+// FMA rate, and the pixel kernels convert every sample both ways; these
+// identities give the same values:
+//  u2f: for 0 <= v < 2^23 the float with bits 0x4B000000 | v is 2^23 + v,
+//       exactly, so subtracting 2^23 (exact) leaves v.
+//  f2u_floor: for 0 <= x < 2^23, x + 2^23 rounded toward zero lies in
+//       [2^23, 2^24), where floats are the integers, so it is 2^23 + floor(x)
+//       and its mantissa bits are floor(x).
+__device__ __forceinline__ float u2f(uint32_t v) { return __fsub_rn(__uint_as_float(0x4B000000u | v), 8388608.0f); }
+__device__ __forceinline__ uint32_t f2u_floor(float x) { return __float_as_uint(__fadd_rz(x, 8388608.0f)) & 0x7FFFFFu; }
+
 // (unsigned short)min(max(v, 0), 65535): clamp then truncate toward zero, the
 // quantisation at every stage boundary of the reference (e.g.
 // WarpPerspectiveKernels.h:41, BayerDemosaicKernels.h:58,73, GainColorOps.cpp:23).
@@ -28,7 +40,7 @@ __device__ __forceinline__ unsigned short clamp_trunc_u16(float v)
 {
     v = v > 0.0f ? v : 0.0f;  // NaN -> 0
     v = v < 65535.0f ? v : 65535.0f;
-    return static_cast<unsigned short>(__float2uint_rz(v));
+    return static_cast<unsigned short>(f2u_floor(v));  // truncation = floor on [0, 65535]
 }
 
 // ApplyGain's skip rule (GainColorOps.cpp:22 and RenderExecutor.cpp:111).

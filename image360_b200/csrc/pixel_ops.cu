@@ -65,7 +65,7 @@ __device__ __forceinline__ void demosaic_generic(const float (*s)[kDmTW + 2], in
     {
         float v = acc[c];
         if (c == my) v = s[ly + 1][lx + 1];
-        else if (cnt[c] != 0) v = fdiv(v, (float)cnt[c]);
+        else if (cnt[c] != 0) v = fdiv(v, u2f((uint32_t)cnt[c]));
         rgb[c] = v;
     }
 }
@@ -85,9 +85,9 @@ __global__ void __launch_bounds__(256) k_demosaic(const unsigned short* __restri
         {
             unsigned short raw = __ldg(cfa + (size_t)gy * w + gx);
             raw = raw > P.black ? (unsigned short)(raw - P.black) : (unsigned short)0;
-            v = clamp_trunc_u16(fmul((float)raw, P.camMul[bayer_color(gy, gx, P.filters)]));
+            v = clamp_trunc_u16(fmul(u2f(raw), P.camMul[bayer_color(gy, gx, P.filters)]));
         }
-        s[r][c] = (float)v;
+        s[r][c] = u2f(v);
     }
     __syncthreads();
     const bool evenW = (w & 1) == 0;
@@ -146,7 +146,7 @@ __global__ void __launch_bounds__(256) k_demosaic(const unsigned short* __restri
             }
             // Truncate to uint16 (DemosaicPixel), then the 3x4 colour matrix
             // (ApplyColorMatrixPixel, BayerDemosaicKernels.h:64-75).
-            const float r = (float)clamp_trunc_u16(R), g = (float)clamp_trunc_u16(G), b = (float)clamp_trunc_u16(B);
+            const float r = u2f(clamp_trunc_u16(R)), g = u2f(clamp_trunc_u16(G)), b = u2f(clamp_trunc_u16(B));
 #pragma unroll
             for (int row = 0; row < 3; ++row)
             {
@@ -207,8 +207,8 @@ __device__ __forceinline__ void warp_pixel(const unsigned short* __restrict__ sr
     // out-of-int-range positions are invalid, as the reference's int
     // conversion makes them.
     if (!(sx >= 0.0f && sx < (float)(sw - 1) && sy >= 0.0f && sy < (float)(sh - 1))) return;
-    int x0 = (int)floorf(sx), y0 = (int)floorf(sy);
-    float fx = fsub(sx, (float)x0), fy = fsub(sy, (float)y0);
+    int x0 = (int)f2u_floor(sx), y0 = (int)f2u_floor(sy);  // 0 <= sx, sy < 2^23 here
+    float fx = fsub(sx, u2f((uint32_t)x0)), fy = fsub(sy, u2f((uint32_t)y0));
     float gx = fsub(1.0f, fx), gy = fsub(1.0f, fy);
     float w00 = fmul(gx, gy), w10 = fmul(fx, gy), w01 = fmul(gx, fy), w11 = fmul(fx, fy);
     const unsigned short* r0 = src + ((size_t)y0 * sw + x0) * 3;
@@ -216,11 +216,11 @@ __device__ __forceinline__ void warp_pixel(const unsigned short* __restrict__ sr
 #pragma unroll
     for (int c = 0; c < 3; ++c)
     {
-        float v = fadd(fadd(fadd(fmul(w00, (float)__ldg(r0 + c)), fmul(w10, (float)__ldg(r0 + 3 + c))),
-                            fmul(w01, (float)__ldg(r1 + c))),
-                       fmul(w11, (float)__ldg(r1 + 3 + c)));
+        float v = fadd(fadd(fadd(fmul(w00, u2f(__ldg(r0 + c))), fmul(w10, u2f(__ldg(r0 + 3 + c)))),
+                            fmul(w01, u2f(__ldg(r1 + c)))),
+                       fmul(w11, u2f(__ldg(r1 + 3 + c))));
         unsigned short q = clamp_trunc_u16(v);
-        if (P.applyGain) q = clamp_trunc_u16(fmul((float)q, P.gain));
+        if (P.applyGain) q = clamp_trunc_u16(fmul(u2f(q), P.gain));
         o[c] = q;
     }
 }
@@ -305,7 +305,7 @@ __device__ __forceinline__ uint32_t median_pair(uint32_t (&v)[P], int n, float s
         for (int i = 0; i < P; ++i)
             if (i < n)
             {
-                const float a = (float)(v[i] & 0xffffu), b = (float)(v[i] >> 16);
+                const float a = u2f(v[i] & 0xffffu), b = u2f(v[i] >> 16);
                 sL = fadd(sL, a);
                 qL = fadd(qL, fmul(a, a));
                 sH = fadd(sH, b);
@@ -320,7 +320,7 @@ __device__ __forceinline__ uint32_t median_pair(uint32_t (&v)[P], int n, float s
         for (int i = 0; i < P; ++i)
             if (i < n)
             {
-                const float a = (float)(v[i] & 0xffffu), b = (float)(v[i] >> 16);
+                const float a = u2f(v[i] & 0xffffu), b = u2f(v[i] >> 16);
                 const bool keepA = a >= loL && a <= hiL, keepB = b >= loH && b <= hiH;
                 kL += keepA ? 1 : 0;
                 kH += keepB ? 1 : 0;
@@ -463,12 +463,12 @@ __global__ void __launch_bounds__(256) k_gain(unsigned short* __restrict__ d, lo
         uint4 q = *reinterpret_cast<uint4*>(d + i8);
         unsigned short* s = reinterpret_cast<unsigned short*>(&q);
 #pragma unroll
-        for (int k = 0; k < 8; ++k) s[k] = clamp_trunc_u16(fmul((float)s[k], gain));
+        for (int k = 0; k < 8; ++k) s[k] = clamp_trunc_u16(fmul(u2f(s[k]), gain));
         *reinterpret_cast<uint4*>(d + i8) = q;
     }
     else
     {
-        for (long long i = i8; i < n && i < i8 + 8; ++i) d[i] = clamp_trunc_u16(fmul((float)d[i], gain));
+        for (long long i = i8; i < n && i < i8 + 8; ++i) d[i] = clamp_trunc_u16(fmul(u2f(d[i]), gain));
     }
 }
 }  // namespace
