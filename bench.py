@@ -211,22 +211,27 @@ def stage_bytes(stats, S, fused_levels=2):
     levels), counted over every item pixel.  With the fused pyramid
     (fused_levels 2) the base stage reads level 0 and writes level 2, the
     materialised stages start at level 2, and the fine stage reads the
-    owners' pixels and writes the output."""
+    owners' pixels and writes the output.  With fused_levels 1 the base
+    stage writes level 1, the down steps start there, the blend and collapse
+    start at level 2, and the fine stage also reads level 1."""
     cfg = S["cfg"]
     npx_in = len(S["cfa"]) * cfg.frame_w * cfg.frame_h
     cov = stats["coveredItemPixels"]
     out = stats["outputPixels"]
     tiles = S["pano"].tiles
     item_px = sum(t[2] * t[3] * len(t[4]) for t in tiles)
-    lo = 2 if fused_levels == 2 else 1
-    base = down = bands_b = collapse = 0
+    lo = 2 if fused_levels >= 1 else 1
+    lo_down = 2 if fused_levels == 2 else 1
+    base = down = bands_b = collapse = level1 = 0
     for (_, _, w, h, cs) in tiles:
         d = _levels(w, h, cfg.bands)
         n = [a * b for a, b in d]
         k = len(cs)
-        if len(n) > lo:
-            base += k * (7 * n[0] + 20 * n[lo])
-        for l in range(lo, len(n) - 1):
+        if len(n) > lo_down:
+            base += k * (7 * n[0] + 20 * n[lo_down])
+        if fused_levels == 1 and len(n) > 1:
+            level1 += k * 20 * n[1]
+        for l in range(lo_down, len(n) - 1):
             down += k * 20 * (n[l] + n[l + 1])
         for l in range(lo, len(n)):
             bands_b += (k * 20 + 12) * n[l]
@@ -244,7 +249,7 @@ def stage_bytes(stats, S, fused_levels=2):
         "pyramid_down": down,
         "blend_bands": bands_b,
         "collapse": collapse,
-        "fine_output": out * 13,
+        "fine_output": out * 13 + level1,
         "blend_total": cov * 6 + out * 6,
     }
 
@@ -1237,7 +1242,7 @@ def main():
     ap.add_argument("--no-uneven", action="store_true", help="skip the 256 uneven-tile leg")
     ap.add_argument("--no-parity", action="store_true", help="skip the full-panorama check against the CPU code")
     ap.add_argument("--no-native", action="store_true", help="skip the FP16-storage (native mode) leg")
-    ap.add_argument("--fusion", type=int, choices=[0, 2], default=None,
+    ap.add_argument("--fusion", type=int, choices=[0, 1, 2], default=None,
                     help="force the level-fusion depth after autotuning (measurement of one form)")
     ap.add_argument("--warp-shape", type=int, choices=[0, 1], default=None,
                     help="force the tile-warp form after autotuning")

@@ -6,6 +6,7 @@
 #include <cuda/atomic>
 #include <cuda_fp16.h>
 #include <cfloat>
+#include <cstddef>
 
 namespace i360b
 {
@@ -2114,9 +2115,18 @@ __device__ __forceinline__ void stage_level0(const unsigned short* img, const si
     const int ng = ((cx1 - cs) >> 2) + 1;
     const int nr = ry1 - ry0 + 1;
     const bool fast = (W & 3) == 0 && (reinterpret_cast<uintptr_t>(img) & 7) == 0;
-    for (int t = threadIdx.x; t < nr * ng; t += blockDim.x)
+    // (row, group) pairs without a division: threads step through the groups
+    // of a row and on to later rows
+    int r = threadIdx.x / ng, g = threadIdx.x - r * ng;
+    const int dr = blockDim.x / ng, dg = blockDim.x - dr * ng;
+    for (; r < nr; r += dr, g += dg)
     {
-        const int r = t / ng, g = t - r * ng;
+        if (g >= ng)
+        {
+            g -= ng;
+            ++r;
+            if (r >= nr) break;
+        }
         const int c = cs + 4 * g;
         const int y = ry0 + r;
         const size_t p = (size_t)y * W + c;
@@ -2310,34 +2320,42 @@ __global__ void __launch_bounds__(256) k_base2(BlendArgs a, const Unit* __restri
 
 struct FineSmem
 {
-    PackedPx px[kF0H * kF0S];                  // one contributor's level-0 footprint (the part it needs)
-    signed char own[kF0H * kF0S];              // the tile's owner map over the footprint
-    float g1[3][kF1H][kF1W];                   // that contributor's G1 on the level-1 window; then recon1
+    float g1[3][kF1H][kF1W];                   // a contributor's G1 on the level-1 window; then recon1
     float w1[kF1H][kF1W];                      // its level-1 weight
     float g2[3][kF2H][kF2W];                   // its G2 on the level-2 window
     float r2[3][kF2H][kF2W];                   // recon2 on the level-2 window
     const unsigned short* img[kMaxTileItems];
     const float4* nd[kMaxTileItems];
+    const float* wg[kMaxTileItems];
     uint32_t set[kMaxTileItems / 32];          // contributors owning a footprint pixel
-    int obox[4];                               // the footprint pixels one contributor owns: x0, y0, x1, y1
+    int ob[kMaxTileItems][4];                  // the footprint pixels each owns: x0, y0, x1, y1 (footprint-relative)
     // Up taps, tabulated: the align-corners coefficients are separable (the x
     // part depends on x only, the y part on y only), so the block's columns
     // and rows (level 0 -> 1) and the window's (level 1 -> 2) are computed
     // once: tap indices relative to the window, and the fraction.
     short2 tx0[kFW], ty0[kFH], tx1[kF1W], ty1[kF1H];
     float fx0[kFW], fy0[kFH], fx1[kF1W], fy1[kF1H];
+    // Level 1 recomputed from level 0 only (the form with level 1 in memory
+    // is launched without these):
+    PackedPx px[kF0H * kF0S];                  // one contributor's level-0 footprint (the part it needs)
+    signed char own[kF0H * kF0S];              // the tile's owner map over the footprint
 };
 
 // Per 64x32 block of output pixels (see the section comment).  Threads own
 // pixels tid + 256 j (j < 8): lanes take consecutive columns of one row, so
 // shared-memory reads of neighbouring pixels and the output stores are
 // contiguous across a warp.  For each contributor owning a footprint pixel,
-// in index order: the footprint rows and columns within 6 of the pixels it
+// in index order, its level-1 values on the window come either from memory
+// (L1MEM: level 1 materialised by the level-0 step; G1 read where the weight
+// is non-zero, the only places they are used) or are recomputed from level 0
+// in shared memory: the footprint rows and columns within 6 of the pixels it
 // owns are staged (a level-1 task reads at most 6 beyond its own pixels), and
 // only the level-1 tasks (pairs of columns x kFRun rows) whose level-0
 // footprint holds one of those pixels are computed - elsewhere its level-1
 // weight is exactly zero, so its blended-band term is +-0 (skipped) and no
-// pixel it owns takes a tap there.
+// pixel it owns takes a tap there (each Up tap of a level-0 pixel has that
+// pixel in its 5-tap footprint).
+template <bool L1MEM>
 __global__ void __launch_bounds__(256) k_fine(BlendArgs a, const Unit* __restrict__ units)
 {
     extern __shared__ __align__(16) unsigned char fine_raw[];
@@ -2347,7 +2365,7 @@ __global__ void __launch_bounds__(256) k_fine(BlendArgs a, const Unit* __restric
     const int W = T.w, H = T.h, K = min(T.numItems, kMaxTileItems);
     const int X0 = u.bx * kFW, Y0 = u.by * kFH;
     const int xe = min(X0 + kFW - 1, W - 1), ye = min(Y0 + kFH - 1, H - 1);
-    const int tid = threadIdx.x;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     // this thread's outputs: column ox of rows oy0 + 4 j
     const int ox = X0 + (tid & (kFW - 1)), oy0 = Y0 + (tid >> 6);
     constexpr int kPx = kFW * kFH / 256;  // 8
@@ -2363,9 +2381,12 @@ __global__ void __launch_bounds__(256) k_fine(BlendArgs a, const Unit* __restric
         const ItemDev& it = a.items[T.firstItem + k];
         S.img[k] = it.img;
         S.nd[k] = it.nd;
+        S.wg[k] = it.wg;
+        S.ob[k][0] = S.ob[k][1] = 0x7fffffff;
+        S.ob[k][2] = S.ob[k][3] = -1;
     }
     if (tid < kMaxTileItems / 32) S.set[tid] = 0u;
-    __syncthreads();  // the set is cleared before any thread adds to it
+    __syncthreads();  // the set and boxes are cleared before any thread adds to them
     if (T.bands == 1)
     {
         // one band: the output is the owner's pixel (SeamBlend.cpp:527-545)
@@ -2451,15 +2472,35 @@ __global__ void __launch_bounds__(256) k_fine(BlendArgs a, const Unit* __restric
             S.fy1[r] = q.wy;
         }
     }
-    // owner map over the footprint, and the contributors it names
+    // owner map over the footprint (a warp per row): the contributors it
+    // names and, for the recomputing form, the box of the pixels each owns
+    // (lanes grouped by owner, one atomic update per group)
     const int nr = ry1 - ry0 + 1, ncol = cx1 - cxa + 1;
-    for (int idx = tid; idx < nr * ncol; idx += blockDim.x)
+    for (int r = warp; r < nr; r += 8)
     {
-        const int r = idx / ncol, c = idx - r * ncol;
-        const int x = cxa + c;
-        const int o = x < W ? (int)__ldg(T.owner + (size_t)(ry0 + r) * W + x) : -1;
-        S.own[r * kF0S + c] = (signed char)o;
-        if (x >= cx0 && o >= 0 && o < K) atomicOr(&S.set[o >> 5], 1u << (o & 31));
+        for (int c0 = 0; c0 < ncol; c0 += 32)
+        {
+            const int c = c0 + lane;
+            const int x = cxa + c;
+            int o = -1;
+            if (c < ncol && x < W) o = (int)__ldg(T.owner + (size_t)(ry0 + r) * W + x);
+            if (!L1MEM && c < ncol) S.own[r * kF0S + c] = (signed char)o;
+            const bool named = x >= cx0 && o >= 0 && o < K;
+            if (named) atomicOr(&S.set[o >> 5], 1u << (o & 31));
+            if (!L1MEM)
+            {
+                const int key = (o >= 0 && o < K && c < ncol) ? o : -1;
+                const unsigned grp = __match_any_sync(kFull, key);
+                const int cmin = __reduce_min_sync(grp, c), cmax = __reduce_max_sync(grp, c);
+                if (key >= 0 && lane == __ffs(grp) - 1)
+                {
+                    atomicMin(&S.ob[key][0], cmin);
+                    atomicMax(&S.ob[key][2], cmax);
+                    atomicMin(&S.ob[key][1], r);
+                    atomicMax(&S.ob[key][3], r);
+                }
+            }
+        }
     }
     // recon2 on the level-2 window
     if (!top1)
@@ -2494,44 +2535,6 @@ __global__ void __launch_bounds__(256) k_fine(BlendArgs a, const Unit* __restric
         {
             const int k = 32 * w + __ffs(m) - 1;
             m &= m - 1;
-            // the footprint pixels k owns (footprint-relative box)
-            if (tid == 0)
-            {
-                S.obox[0] = S.obox[1] = 0x7fffffff;
-                S.obox[2] = S.obox[3] = -1;
-            }
-            __syncthreads();
-            {
-                int bx0 = 0x7fffffff, by0 = 0x7fffffff, bx1 = -1, by1 = -1;
-                for (int idx = tid; idx < nr * ncol; idx += blockDim.x)
-                {
-                    const int r = idx / ncol, c = idx - r * ncol;
-                    if (S.own[r * kF0S + c] == (signed char)k)
-                    {
-                        bx0 = min(bx0, c);
-                        bx1 = max(bx1, c);
-                        by0 = min(by0, r);
-                        by1 = max(by1, r);
-                    }
-                }
-                bx0 = __reduce_min_sync(kFull, bx0);
-                by0 = __reduce_min_sync(kFull, by0);
-                bx1 = __reduce_max_sync(kFull, bx1);
-                by1 = __reduce_max_sync(kFull, by1);
-                if ((tid & 31) == 0 && bx1 >= 0)
-                {
-                    atomicMin(&S.obox[0], bx0);
-                    atomicMin(&S.obox[1], by0);
-                    atomicMax(&S.obox[2], bx1);
-                    atomicMax(&S.obox[3], by1);
-                }
-            }
-            __syncthreads();
-            const int ob0 = S.obox[0], ob1 = S.obox[1], ob2 = S.obox[2], ob3 = S.obox[3];
-            // stage the footprint within 6 of the owned box
-            const int sy0 = max(ry0, ry0 + ob1 - 6), sy1 = min(ry1, ry0 + ob3 + 6);
-            const int sx0 = max(cx0, cxa + ob0 - 6), sx1 = min(cx1, cxa + ob2 + 6);
-            stage_level0(S.img[k], S.own, kF0S, true, (signed char)k, W, sy0, sy1, sx0, sx1, S.px, kF0S, ry0, cxa);
             if (!top1)
             {
                 const size_t g2 = T.loff[2];
@@ -2544,38 +2547,71 @@ __global__ void __launch_bounds__(256) k_fine(BlendArgs a, const Unit* __restric
                     S.g2[2][r][c] = g.z;
                 }
             }
-            __syncthreads();
-            // level-1 values of contributor k on the window: the tasks whose
-            // level-0 footprint meets the owned box; zero weight elsewhere
-            for (int task = tid; task < nPairs * nRuns; task += blockDim.x)
+            if (L1MEM)
             {
-                const int run = task / nPairs, c = 2 * (task - run * nPairs);
-                const int Y1s = B0 + run * kFRun;
-                const int R = min(kFRun, B1 - Y1s + 1);
-                const bool two = c + 1 < nA;
-                const int X1 = A0 + c;
-                const int fr0 = max(2 * Y1s - 2, 0) - ry0, fr1 = min(2 * (Y1s + R - 1) + 2, H - 1) - ry0;
-                const int fc0 = max(2 * X1 - 2, 0) - cxa, fc1 = min(2 * (X1 + (two ? 1 : 0)) + 2, W - 1) - cxa;
-                if (fr1 < ob1 || fr0 > ob3 || fc1 < ob0 || fc0 > ob2)
+                // level 1 from memory: the weight everywhere on the window,
+                // G1 where the weight is non-zero (where it is used)
+                const size_t l1 = T.loff[1];
+#pragma unroll
+                for (int j = 0; j < 3; ++j)
                 {
-                    for (int rr = 0; rr < R; ++rr)
+                    const int p = tid + 256 * j;
+                    if (p >= nWin) continue;
+                    const int r = p / nA, c = p - r * nA;
+                    const size_t q = l1 + (size_t)(B0 + r) * lw1 + A0 + c;
+                    const float wv = wg_at(S.wg[k], q, a.half);
+                    S.w1[r][c] = wv;
+                    if (wv != 0.0f)
                     {
-                        S.w1[Y1s + rr - B0][c] = 0.0f;
-                        if (two) S.w1[Y1s + rr - B0][c + 1] = 0.0f;
+                        const float3 g = gauss_of(nd_at(S.nd[k], q, a.half));
+                        S.g1[0][r][c] = g.x;
+                        S.g1[1][r][c] = g.y;
+                        S.g1[2][r][c] = g.z;
                     }
-                    continue;
                 }
-                level1_pair(S.px, kF0S, ry0, cxa, cx1, W, H, X1, two, Y1s, R,
-                            [&](int cc, int mm, float n0, float n1, float n2, float den, float wg) {
-                                const int r = Y1s + mm - B0;
-                                const float3 g = gauss_of(make_float4(n0, n1, n2, den));
-                                S.g1[0][r][c + cc] = g.x;
-                                S.g1[1][r][c + cc] = g.y;
-                                S.g1[2][r][c + cc] = g.z;
-                                S.w1[r][c + cc] = wg;
-                            });
+                __syncthreads();
             }
-            __syncthreads();
+            else
+            {
+                const int ob0 = S.ob[k][0], ob1 = S.ob[k][1], ob2 = S.ob[k][2], ob3 = S.ob[k][3];
+                // stage the footprint within 6 of the owned box
+                const int sy0 = max(ry0, ry0 + ob1 - 6), sy1 = min(ry1, ry0 + ob3 + 6);
+                const int sx0 = max(cx0, cxa + ob0 - 6), sx1 = min(cx1, cxa + ob2 + 6);
+                stage_level0(S.img[k], S.own, kF0S, true, (signed char)k, W, sy0, sy1, sx0, sx1, S.px, kF0S, ry0,
+                             cxa);
+                __syncthreads();
+                // level-1 values of contributor k on the window: the tasks whose
+                // level-0 footprint meets the owned box; zero weight elsewhere
+                for (int task = tid; task < nPairs * nRuns; task += blockDim.x)
+                {
+                    const int run = task / nPairs, c = 2 * (task - run * nPairs);
+                    const int Y1s = B0 + run * kFRun;
+                    const int R = min(kFRun, B1 - Y1s + 1);
+                    const bool two = c + 1 < nA;
+                    const int X1 = A0 + c;
+                    const int fr0 = max(2 * Y1s - 2, 0) - ry0, fr1 = min(2 * (Y1s + R - 1) + 2, H - 1) - ry0;
+                    const int fc0 = max(2 * X1 - 2, 0) - cxa, fc1 = min(2 * (X1 + (two ? 1 : 0)) + 2, W - 1) - cxa;
+                    if (fr1 < ob1 || fr0 > ob3 || fc1 < ob0 || fc0 > ob2)
+                    {
+                        for (int rr = 0; rr < R; ++rr)
+                        {
+                            S.w1[Y1s + rr - B0][c] = 0.0f;
+                            if (two) S.w1[Y1s + rr - B0][c + 1] = 0.0f;
+                        }
+                        continue;
+                    }
+                    level1_pair(S.px, kF0S, ry0, cxa, cx1, W, H, X1, two, Y1s, R,
+                                [&](int cc, int mm, float n0, float n1, float n2, float den, float wg) {
+                                    const int r = Y1s + mm - B0;
+                                    const float3 g = gauss_of(make_float4(n0, n1, n2, den));
+                                    S.g1[0][r][c + cc] = g.x;
+                                    S.g1[1][r][c + cc] = g.y;
+                                    S.g1[2][r][c + cc] = g.z;
+                                    S.w1[r][c + cc] = wg;
+                                });
+                }
+                __syncthreads();
+            }
             // blended level-1 band: weight x Laplacian, in contributor order
 #pragma unroll
             for (int j = 0; j < 3; ++j)
@@ -2606,12 +2642,26 @@ __global__ void __launch_bounds__(256) k_fine(BlendArgs a, const Unit* __restric
                 const int y = oy0 + 4 * j;
                 const short2 yt = S.ty0[y - Y0];
                 const float wy = S.fy0[y - Y0];
-                int cv[4];
-                px_channels(S.px[(y - ry0) * kF0S + (ox - cxa)], cv);
+                float v[3];
+                if (L1MEM)
+                {
+                    const unsigned short* q = S.img[k] + ((size_t)y * W + ox) * 3;
+                    v[0] = u2f(__ldg(q));
+                    v[1] = u2f(__ldg(q + 1));
+                    v[2] = u2f(__ldg(q + 2));
+                }
+                else
+                {
+                    int cv[4];
+                    px_channels(S.px[(y - ry0) * kF0S + (ox - cxa)], cv);
+                    v[0] = u2f((uint32_t)cv[0]);
+                    v[1] = u2f((uint32_t)cv[1]);
+                    v[2] = u2f((uint32_t)cv[2]);
+                }
 #pragma unroll
                 for (int ch = 0; ch < 3; ++ch)
-                    lap[j][ch] = fsub(u2f((uint32_t)cv[ch]), up_mix(S.g1[ch][yt.x][xt0.x], S.g1[ch][yt.x][xt0.y],
-                                                            S.g1[ch][yt.y][xt0.x], S.g1[ch][yt.y][xt0.y], wx0, wy));
+                    lap[j][ch] = fsub(v[ch], up_mix(S.g1[ch][yt.x][xt0.x], S.g1[ch][yt.x][xt0.y], S.g1[ch][yt.y][xt0.x],
+                                                    S.g1[ch][yt.y][xt0.y], wx0, wy));
             }
             __syncthreads();
         }
@@ -2786,12 +2836,22 @@ int launch_base2(const BlendArgs& a, const Unit* units, int n, cudaStream_t s)
     return check_launch("pyramid base kernel");
 }
 
-int launch_fine(const BlendArgs& a, const Unit* units, int n, cudaStream_t s)
+int launch_fine(const BlendArgs& a, const Unit* units, int n, bool level1InMemory, cudaStream_t s)
 {
     if (n <= 0) return I360B_SUCCESS;
-    const int smem = (int)sizeof(FineSmem);
-    cudaFuncSetAttribute(k_fine, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-    k_fine<<<n, 256, smem, s>>>(a, units);
+    if (level1InMemory)
+    {
+        // the level-0 staging arrays (the struct's tail) are not used
+        const int smem = (int)offsetof(FineSmem, px);
+        cudaFuncSetAttribute(k_fine<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+        k_fine<true><<<n, 256, smem, s>>>(a, units);
+    }
+    else
+    {
+        const int smem = (int)sizeof(FineSmem);
+        cudaFuncSetAttribute(k_fine<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+        k_fine<false><<<n, 256, smem, s>>>(a, units);
+    }
     return check_launch("fine levels kernel");
 }
 }  // namespace i360b

@@ -103,6 +103,6 @@ constexpr int kBase2W = 32, kBase2H = 8, kFineW = 64, kFineH = 32;
 // Destination block of one tile-warp CTA (launch_warp_tiles units: item, block).
 constexpr int kWarpBlockW = 128, kWarpBlockH = 32;
 int launch_base2(const BlendArgs& a, const Unit* units, int n, cudaStream_t s);
-int launch_fine(const BlendArgs& a, const Unit* units, int n, cudaStream_t s);
+int launch_fine(const BlendArgs& a, const Unit* units, int n, bool level1InMemory, cudaStream_t s);
 int dt_rows_in_flight(int maxW, int maxH);
 }  // namespace i360b

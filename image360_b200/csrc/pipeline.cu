@@ -219,10 +219,11 @@ extern "C" int i360b_pipeline_autotune(i360b_pipeline* P, int* bandRows, int* dt
     int rows = 0, ring = 0;
     float ms = 0.0f;
     I360B_TRY(i360b_render_plan_autotune(P->slots[0].plan, P->slots[0].comp, &rows, &ring, &ms));
-    const int fused = P->slots[0].plan->plan.fusedLevels;
+    const int fused = P->slots[0].plan->plan.fusedLevels, shape = P->slots[0].plan->plan.warpShape;
     for (size_t k = 1; k < P->slots.size(); ++k)
     {
         I360B_TRY(P->slots[k].plan->plan.set_fusion(fused, P->slots[k].comp));
+        I360B_TRY(P->slots[k].plan->plan.set_warp_shape(shape, P->slots[k].comp));
         I360B_TRY(P->slots[k].plan->plan.set_tuning(rows, ring, P->slots[k].comp));
     }
     if (bandRows) *bandRows = rows;

@@ -512,7 +512,7 @@ int Plan::set_precision(int mode, cudaStream_t s)
 
 int Plan::set_fusion(int levels, cudaStream_t s)
 {
-    if (levels != 0 && levels != 2) return fail(I360B_INVALID_PARAM, "fused pyramid levels must be 0 or 2");
+    if (levels < 0 || levels > 2) return fail(I360B_INVALID_PARAM, "fused pyramid levels must be 0, 1 or 2");
     if (storage16 && levels != 2)
         return fail(I360B_INVALID_PARAM, "FP16 pyramid storage needs the fused levels (2).");
     I360B_CUDA(cudaStreamSynchronize(s), "plan fusion");
@@ -552,10 +552,12 @@ Plan::~Plan()
     if (arena && ownsArena) cudaFree(arena);
 }
 
-// Stages 5-9 with the fused pyramid: level 0 -> 2 of every contributor;
-// down from level 2; blended bands >= 2; collapse to level 2; level-1 blend,
-// collapse and output.  Materialised: level 0 -> 1; down from level 1; bands
-// >= 1; collapse to level 1; level-0 output.
+// Stages 5-9 with the fused pyramid (depth 2): level 0 -> 2 of every
+// contributor; down from level 2; blended bands >= 2; collapse to level 2;
+// level-1 blend, collapse and output from level 0.  Depth 1: level 0 -> 1;
+// down from level 1; bands >= 2; collapse to level 2; level-1 blend, collapse
+// and output reading level 1.  Materialised (depth 0): level 0 -> 1; down
+// from level 1; bands >= 1; collapse to level 1; level-0 output.
 const char* const kStageNames[kStages] = {"warp_gain_coverage", "chamfer_forward", "chamfer_backward",
                                           "ownership",          "seam_dp",         "pyramid_base",
                                           "pyramid_down",       "blend_bands",     "collapse",
@@ -564,15 +566,15 @@ const char* const kStageNames[kStages] = {"warp_gain_coverage", "chamfer_forward
 int Plan::kernels_per_execute() const
 {
     int n = (nItems > 0 ? 1 : 0);  // bbox reset
-    const int lo = fusedLevels == 2 ? 2 : 1;
+    const int lo = fusedLevels > 0 ? 2 : 1, downLo = fusedLevels == 2 ? 2 : 1;
     for (int c = 0; c < nChains; ++c)
     {
         const Range* L = &lists[(size_t)c * kListsPerChain];
         n += (L[0].count > 0 ? 1 : 0) + (dtRange[c].count > 0 ? 2 : 0) + (L[1].count > 0 ? 1 : 0) +
              (seamRange[c].count > 0 ? 1 : 0);
-        n += fusedLevels == 2 ? (L[kListBase2].count > 0 ? 1 : 0) + (L[kListFine].count > 0 ? 1 : 0)
-                              : (L[3].count > 0 ? 1 : 0) + (L[2].count > 0 ? 1 : 0);
-        for (int l = lo; l < kMaxBands - 1; ++l) n += L[3 + l].count > 0 ? 1 : 0;               // down
+        n += fusedLevels == 2 ? (L[kListBase2].count > 0 ? 1 : 0) : (L[3].count > 0 ? 1 : 0);
+        n += fusedLevels > 0 ? (L[kListFine].count > 0 ? 1 : 0) : (L[2].count > 0 ? 1 : 0);
+        for (int l = downLo; l < kMaxBands - 1; ++l) n += L[3 + l].count > 0 ? 1 : 0;           // down
         for (int l = lo; l < kMaxBands; ++l) n += L[3 + (kMaxBands - 1) + l].count > 0 ? 1 : 0;  // blend
         for (int l = lo; l < kMaxBands; ++l) n += L[3 + 2 * kMaxBands - 1 + l].count > 0 ? 1 : 0;  // collapse
     }
@@ -592,8 +594,9 @@ int Plan::enqueue_chain(int c, int first, int last, cudaStream_t s)
 {
     BlendArgs a{dItems, dTiles, dError, dSeamCycles, bandRows, spinLimit, storage16};
     const Range* L = &lists[(size_t)c * kListsPerChain];
-    const bool fused = fusedLevels == 2;
-    const int lo = fused ? 2 : 1;  // lowest level the materialised stages handle
+    const bool base2 = fusedLevels == 2, fine = fusedLevels > 0;
+    const int lo = fine ? 2 : 1;        // lowest level of the materialised blend and collapse
+    const int downLo = base2 ? 2 : 1;   // lowest level the down steps start from
     for (int stage = first; stage <= last; ++stage)
     {
         Range r;
@@ -615,8 +618,8 @@ int Plan::enqueue_chain(int c, int first, int last, cudaStream_t s)
         case 4:
             I360B_TRY(launch_seam(a, seamList + seamRange[c].start, seamRange[c].count, s));
             break;
-        case 5:  // pyramid base: level 0 -> 2 (fused) or level 0 -> 1
-            if (fused)
+        case 5:  // pyramid base: level 0 -> 2 (depth 2) or level 0 -> 1
+            if (base2)
             {
                 r = L[kListBase2];
                 I360B_TRY(launch_base2(a, dUnits + r.start, r.count, s));
@@ -628,7 +631,7 @@ int Plan::enqueue_chain(int c, int first, int last, cudaStream_t s)
             }
             break;
         case 6:  // the levels above the base
-            for (int l = lo; l < kMaxBands - 1; ++l)
+            for (int l = downLo; l < kMaxBands - 1; ++l)
             {
                 r = L[3 + l];
                 I360B_TRY(launch_down(a, dUnits + r.start, r.count, l, s));
@@ -648,9 +651,10 @@ int Plan::enqueue_chain(int c, int first, int last, cudaStream_t s)
                 I360B_TRY(launch_collapse(a, dUnits + r.start, r.count, l, s));
             }
             break;
-        case 9:  // fused: level-1 blend + collapse + output; else the level-0 output
-            r = fused ? L[kListFine] : L[2];
-            I360B_TRY(fused ? launch_fine(a, dUnits + r.start, r.count, s) : launch_final0(a, dUnits + r.start, r.count, s));
+        case 9:  // depths 1, 2: level-1 blend + collapse + output; else the level-0 output
+            r = fine ? L[kListFine] : L[2];
+            I360B_TRY(fine ? launch_fine(a, dUnits + r.start, r.count, !base2, s)
+                           : launch_final0(a, dUnits + r.start, r.count, s));
             break;
         }
     }
@@ -1096,7 +1100,7 @@ extern "C" int i360b_render_plan_autotune(i360b_render_plan* plan, void* stream,
     // 1: warp form x fusion depth at the current band height and ring depth
     for (int shape : {1, 0})
     {
-        for (int fused : {2, 0})
+        for (int fused : {2, 1, 0})
         {
             if (fused != 2 && P.storage16) continue;  // FP16 storage exists only with the fused levels
             if ((rc = P.set_warp_shape(shape, s)) != I360B_SUCCESS || (rc = P.set_fusion(fused, s)) != I360B_SUCCESS)

@@ -60,8 +60,10 @@ struct Plan
     // and ring slots of the chamfer transform (0 = as many as fit).
     int bandRows = kBandRows, dtSlots = 0;
     // Pyramid levels computed on chip (level-fusion depth): 2 = levels 0 and
-    // 1 fused (k_base2 + k_fine, only levels >= 2 in memory), 0 = every level
-    // materialised (k_down0s, k_blend_level / k_collapse at level 1, k_final0).
+    // 1 fused (k_base2 + k_fine, only levels >= 2 in memory), 1 = level 1
+    // materialised by k_down0s and read by k_fine (the level-1 blend,
+    // collapse and output fused), 0 = every level materialised (k_down0s,
+    // k_blend_level / k_collapse at level 1, k_final0).
     int fusedLevels = 2;
     // Storage of the materialised pyramid levels: 0 FP32 (exact, the
     // reference's values bit for bit), 1 FP16 with FP32 arithmetic (the

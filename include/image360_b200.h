@@ -416,8 +416,9 @@ I360B_API int i360b_render_plan_autotune(i360b_render_plan* plan, void* stream, 
 /* The plan's tuning: rows per band unit of the per-pixel kernels (8, 16, 32
  * or 64), chamfer ring slots (0 = as many as fit, else 2 to the number that
  * fits), the level-fusion depth of the pyramid (2 computes levels 0 and 1 on
- * chip, so only levels >= 2 of the pyramids are written to memory; 0
- * materialises every level) and the tile warp's form (1: 128x32 blocks whose
+ * chip, so only levels >= 2 of the pyramids are written to memory; 1 writes
+ * level 1 too and fuses the level-1 blend, the collapse and the output into
+ * one kernel that reads it; 0 materialises every level) and the tile warp's form (1: 128x32 blocks whose
  * source footprint is staged in shared memory; 0: row bands gathering
  * through L1).  Every setting renders the same bits.  No reference
  * counterpart (the reference's blend is a fixed CPU loop).  set_tuning is

@@ -1,7 +1,7 @@
 """The fused pyramid (levels 0 and 1 on chip: k_base2 + k_fine) against the
 oracle, and against the materialised pyramid, bit for bit:
 
-* both level-fusion depths and both tile-warp forms on tiles with 1 to 8
+* the three level-fusion depths and both tile-warp forms on tiles with 1 to 8
   bands (one band: the output
   is the owner's pixel; two: level 1 is the top level; three and more: the
   coarse levels come from memory);
@@ -48,7 +48,7 @@ def test_fusion_depths_match_oracle(backend, oracle_c, bands):
     plan, outs = _plan(dev, cfg, pano.to_canvas, gains, pano.tiles, bands)
     inv = np.stack([synth.inverse_homography_f32(H) for H in pano.to_canvas])
     _, ref = oracle_c.render_tiles(4, host, inv, gains, pano.tiles, bands)
-    for fused, shape in ((2, 1), (0, 1), (2, 0), (0, 0)):
+    for fused, shape in ((2, 1), (1, 1), (0, 1), (2, 0), (1, 0), (0, 0)):
         assert plan.set_tuning(16, 0, fused, shape) == ComputeResult.SUCCESS
         assert plan.tuning()["fused_levels"] == fused and plan.tuning()["warp_shape"] == shape
         for o in outs:
@@ -58,7 +58,7 @@ def test_fusion_depths_match_oracle(backend, oracle_c, bands):
             got = _host(o)
             assert np.array_equal(got, r), (fused, shape, bands, t, pano.tiles[t][:4],
                                             int(np.abs(got.astype(int) - r).max()))
-    assert plan.set_tuning(16, 0, 1) == ComputeResult.INVALID_PARAM
+    assert plan.set_tuning(16, 0, 3) == ComputeResult.INVALID_PARAM
     assert plan.set_tuning(16, 0, 2, 5) == ComputeResult.INVALID_PARAM
     plan.close()
 
@@ -110,7 +110,7 @@ def test_autotuner_picks_fusion_depth_without_changing_bits(backend, oracle_c):
     inv = np.stack([synth.inverse_homography_f32(H) for H in pano.to_canvas])
     _, ref = oracle_c.render_tiles(4, host, inv, gains, pano.tiles, 6)
     tuned = plan.autotune()
-    assert tuned["fused_levels"] in (0, 2) and tuned["band_rows"] in (8, 16, 32, 64) and tuned["warp_shape"] in (0, 1)
+    assert tuned["fused_levels"] in (0, 1, 2) and tuned["band_rows"] in (8, 16, 32, 64) and tuned["warp_shape"] in (0, 1)
     for o in outs:
         o.fill_(-1)
     assert plan.execute() == ComputeResult.SUCCESS and plan.wait() == ComputeResult.SUCCESS
