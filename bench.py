@@ -288,6 +288,9 @@ def run_ours(args, rank, world, local_rank):
                                t["fused_levels"] if args.fusion is None else args.fusion,
                                t["warp_shape"] if args.warp_shape is None else args.warp_shape, sp) == 0
         tuned = {**(tuned or {}), **plan.tuning(), "forced": True}
+    if args.chain_lag is not None:
+        assert plan.set_chain_lag(args.chain_lag, sp) == 0
+        tuned = {**(tuned or {}), "chain_lag": plan.chain_lag(), "forced": True}
     torch.cuda.synchronize()
     stats = plan.stats(sp)
     stages = plan.profile(sp)
@@ -1246,6 +1249,9 @@ def main():
                     help="force the level-fusion depth after autotuning (measurement of one form)")
     ap.add_argument("--warp-shape", type=int, choices=[0, 1], default=None,
                     help="force the tile-warp form after autotuning")
+    ap.add_argument("--chain-lag", type=int, default=None,
+                    help="force the chain stagger after autotuning (-1: chains together; L: the second chain "
+                         "starts after the first finishes stage L)")
     ap.add_argument("--no-autotune", action="store_true", help="keep the plan's default band height and ring depth")
     ap.add_argument("--train-steps", type=int, default=782, help="Adam steps (782 x 64 = 50k windows)")
     ap.add_argument("--train-batch", type=int, default=64)

@@ -97,6 +97,8 @@ def load_library(path: str = LIB_PATH):
                                            ct.POINTER(vp)]
     L.i360b_render_plan_execute.argtypes = [vp, vp]
     L.i360b_render_plan_execute_stages.argtypes = [vp, i, i, vp]
+    L.i360b_render_plan_set_chain_lag.argtypes = [vp, i, vp]
+    L.i360b_render_plan_get_chain_lag.argtypes = [vp, ct.POINTER(i)]
     L.i360b_render_plan_wait.argtypes = [vp, vp]
     L.i360b_render_plan_destroy.argtypes = [vp]
     L.i360b_render_plan_stats.argtypes = [vp, vp, ct.POINTER(RenderStats)]
@@ -539,7 +541,17 @@ class RenderPlan:
             raise RuntimeError(self.lib.i360b_get_last_error().decode())
         t = self.tuning()
         return {"band_rows": r.value, "dt_slots": k.value, "fused_levels": t["fused_levels"],
-                "warp_shape": t["warp_shape"], "ms": ms.value}
+                "warp_shape": t["warp_shape"], "chain_lag": self.chain_lag(), "ms": ms.value}
+
+    def chain_lag(self) -> int:
+        """The chain stagger: the stage of the first chain after which the
+        second starts (-1: together)."""
+        v = ct.c_int()
+        self.lib.i360b_render_plan_get_chain_lag(self._h, ct.byref(v))
+        return v.value
+
+    def set_chain_lag(self, stage: int, stream: int = 0) -> ComputeResult:
+        return ComputeResult(self.lib.i360b_render_plan_set_chain_lag(self._h, int(stage), stream or None))
 
     def tuning(self) -> dict:
         r, k, f, w = ct.c_int(), ct.c_int(), ct.c_int(), ct.c_int()

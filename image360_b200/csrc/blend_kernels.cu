@@ -980,6 +980,54 @@ __device__ __forceinline__ int first_owner_in_chunk(uint4 v, unsigned repA, unsi
     return mask ? tb + __ffs(mask) - 1 : 0x7fffffff;
 }
 
+// Bytes of a 16-byte chunk equal to the owner index replicated in rep, as a
+// 16-bit mask (bit b: byte b).
+__device__ __forceinline__ unsigned chunk_byte_mask(uint4 v, unsigned rep)
+{
+    const unsigned w[4] = {v.x, v.y, v.z, v.w};
+    unsigned mask = 0;
+#pragma unroll
+    for (int i = 0; i < 4; ++i)
+    {
+        const unsigned m = __vcmpeq4(w[i], rep) & 0x80808080u;
+        mask |= (((m >> 7) & 1u) | ((m >> 14) & 2u) | ((m >> 21) & 4u) | ((m >> 28) & 8u)) << (4 * i);
+    }
+    return mask;
+}
+
+// Contested band of a column line (SeamBlend.cpp:347-359): the positions
+// within kSeamRadius of the crossover covered by both contributors, as
+// lo..hi (lo > hi: none).  The coverage bits of 8 rows are requested at once
+// (both contributors' words, no short circuit).
+__device__ __forceinline__ void seam_column_band(const uint32_t* covI, const uint32_t* covJ, int covWords, int x,
+                                                 int oy0, int cross, int lineLen, int& outLo, int& outHi)
+{
+    int lo = 1, hi = 0;
+    if (cross >= 0)
+    {
+        const int bLo = max(0, cross - kSeamRadius), bHi = min(lineLen - 1, cross + kSeamRadius);
+        for (int tb = bLo; tb <= bHi; tb += 8)
+        {
+            bool ok[8];
+#pragma unroll
+            for (int q = 0; q < 8; ++q)
+            {
+                const int y = oy0 + min(tb + q, bHi);
+                ok[q] = tb + q <= bHi && (cov_bit(covI, covWords, x, y) & cov_bit(covJ, covWords, x, y));
+            }
+#pragma unroll
+            for (int q = 0; q < 8; ++q)
+                if (ok[q])
+                {
+                    if (hi < lo) lo = tb + q;
+                    hi = tb + q;
+                }
+        }
+    }
+    outLo = lo;
+    outHi = hi;
+}
+
 __global__ void __launch_bounds__(kSeamThreads, 1) k_seam(BlendArgs a, const int* __restrict__ tileList, int smemLines)
 {
     extern __shared__ unsigned char sm_seam[];
@@ -1090,6 +1138,57 @@ __global__ void __launch_bounds__(kSeamThreads, 1) k_seam(BlendArgs a, const int
                     }
                 }
             }
+            else if ((w & 15) == 0 && (reinterpret_cast<uintptr_t>(T.owner) & 15) == 0)
+            {
+                // Lines are columns.  The crossover of a column (the first
+                // pixel of the other owner after its first I/J pixel) is the
+                // later of the column's first I row and first J row, so both
+                // are found by one parallel pass over the overlap box instead
+                // of a walk down each column: 16-byte chunks of each row (their
+                // column offset is the same on every row, the row pitch being a
+                // multiple of 16), threads over (chunk, row segment), each
+                // segment scanned top-down and its first finds merged by
+                // atomicMin into the line arrays (used for the first rows
+                // here, overwritten with the band below).
+                int* fI = sLo;
+                int* fJ = sHi;
+                for (int l = tid; l < numLines; l += kSeamThreads) fI[l] = fJ[l] = 0x7fffffff;
+                __syncthreads();
+                const signed char* rowp0 = T.owner + pix(0, 0);
+                const int off = (int)(reinterpret_cast<uintptr_t>(rowp0) & 15);
+                const signed char* base0 = rowp0 - off;
+                const int nCh = (off + numLines + 15) >> 4;
+                const int nSeg = max(1, kSeamThreads / nCh);
+                const int segRows = (lineLen + nSeg - 1) / nSeg;
+                const unsigned repI = (unsigned)ci * 0x01010101u, repJ = (unsigned)cj * 0x01010101u;
+                for (int job = tid; job < nCh * nSeg; job += kSeamThreads)
+                {
+                    const int seg = job / nCh, c = job - seg * nCh;
+                    const int tb = 16 * c - off;  // column of the chunk's byte 0
+                    const int b0 = max(0, -tb), b1 = min(16, numLines - tb);
+                    const unsigned valid = ((1u << b1) - 1u) & ~((1u << b0) - 1u);
+                    unsigned foundI = 0, foundJ = 0;
+                    const int t1 = min(lineLen, (seg + 1) * segRows);
+                    for (int t = seg * segRows; t < t1 && (foundI & foundJ) != valid; ++t)
+                    {
+                        const uint4 v = *reinterpret_cast<const uint4*>(base0 + (size_t)t * w + 16 * c);
+                        const unsigned nI = chunk_byte_mask(v, repI) & valid & ~foundI;
+                        const unsigned nJ = chunk_byte_mask(v, repJ) & valid & ~foundJ;
+                        for (unsigned m = nI; m; m &= m - 1) atomicMin(&fI[tb + __ffs(m) - 1], t);
+                        for (unsigned m = nJ; m; m &= m - 1) atomicMin(&fJ[tb + __ffs(m) - 1], t);
+                        foundI |= nI;
+                        foundJ |= nJ;
+                    }
+                }
+                __syncthreads();
+                for (int line = tid; line < numLines; line += kSeamThreads)
+                {
+                    const int a1 = fI[line], a2 = fJ[line];
+                    const int cross = (a1 != 0x7fffffff && a2 != 0x7fffffff) ? max(a1, a2) : -1;
+                    seam_column_band(I.cov, J.cov, T.covWords, ox0 + line, oy0, cross, lineLen, sLo[line],
+                                     sHi[line]);
+                }
+            }
             else
             {
                 for (int line = tid; line < numLines; line += kSeamThreads)
@@ -1110,35 +1209,7 @@ __global__ void __launch_bounds__(kSeamThreads, 1) k_seam(BlendArgs a, const int
                             else if (o != first) cross = t0 + q;
                         }
                     }
-                    // Contested band (SeamBlend.cpp:347-359): the coverage bits
-                    // of 8 rows requested at once (both contributors' words, no
-                    // short circuit).
-                    int lo = 1, hi = 0;
-                    if (cross >= 0)
-                    {
-                        const int bLo = max(0, cross - kSeamRadius), bHi = min(lineLen - 1, cross + kSeamRadius);
-                        const int x = ox0 + line;
-                        for (int tb = bLo; tb <= bHi; tb += 8)
-                        {
-                            bool ok[8];
-#pragma unroll
-                            for (int q = 0; q < 8; ++q)
-                            {
-                                const int y = oy0 + min(tb + q, bHi);
-                                ok[q] = tb + q <= bHi &&
-                                        (cov_bit(I.cov, T.covWords, x, y) & cov_bit(J.cov, T.covWords, x, y));
-                            }
-#pragma unroll
-                            for (int q = 0; q < 8; ++q)
-                                if (ok[q])
-                                {
-                                    if (hi < lo) lo = tb + q;
-                                    hi = tb + q;
-                                }
-                        }
-                    }
-                    sLo[line] = lo;
-                    sHi[line] = hi;
+                    seam_column_band(I.cov, J.cov, T.covWords, ox0 + line, oy0, cross, lineLen, sLo[line], sHi[line]);
                 }
             }
             __syncthreads();
@@ -1366,17 +1437,23 @@ struct UpCoef
 
 // Align-corners bilinear resize coefficients (SeamBlend.cpp:85-115); the
 // scales sx, sy = (src-1)/(dst-1) are computed once per tile and level.
+// Coordinates and scales are non-negative and below 2^23, so the int/float
+// conversions (and the truncation, which is the floor there) are the exact
+// ones of u2f / f2u_floor.
+__device__ __forceinline__ void up_coef_x(float sx, int sw, int x, int& x0, float& wx)
+{
+    const float fx = fmul(sx, u2f((uint32_t)x));
+    x0 = min((int)f2u_floor(fx), sw - 1);
+    wx = fsub(fx, u2f((uint32_t)x0));
+}
+
 __device__ __forceinline__ UpCoef up_coef_s(float sx, float sy, int sw, int sh, int x, int y)
 {
     UpCoef c;
-    float fy = fmul(sy, (float)y);
-    c.y0 = min(__float2int_rz(fy), sh - 1);
+    up_coef_x(sy, sh, y, c.y0, c.wy);
     c.y1 = min(c.y0 + 1, sh - 1);
-    c.wy = fsub(fy, (float)c.y0);
-    float fx = fmul(sx, (float)x);
-    c.x0 = min(__float2int_rz(fx), sw - 1);
+    up_coef_x(sx, sw, x, c.x0, c.wx);
     c.x1 = min(c.x0 + 1, sw - 1);
-    c.wx = fsub(fx, (float)c.x0);
     return c;
 }
 
@@ -1975,28 +2052,55 @@ __device__ __forceinline__ void final_quad(const TileDev& T, const ItemCache& C,
                                            long long p, int y, int x, int own)
 {
     const float4* g1 = C.nd[own] + T.loff[1];
-    UpCoef c = up_coef_s(T.usx[0], T.usy[0], uw, uh, x, y);
+    const float sx = T.usx[0];
+    UpCoef c = up_coef_s(sx, T.usy[0], uw, uh, x, y);
     int cur = c.x0;
     TapColumn L = tap_column(g1, rc, uw, c.y0, c.y1, cur);
     TapColumn R = tap_column(g1, rc, uw, c.y0, c.y1, c.x1);
     const unsigned short* px = C.img[own] + p * 3;
+    // the quad's 12 source values: three 8-byte loads when aligned
+    uint32_t pw[6];
+    if ((reinterpret_cast<uintptr_t>(px) & 7) == 0)
+    {
+        const uint2* q = reinterpret_cast<const uint2*>(px);
+#pragma unroll
+        for (int k = 0; k < 3; ++k)
+        {
+            const uint2 v = __ldg(q + k);
+            pw[2 * k] = v.x;
+            pw[2 * k + 1] = v.y;
+        }
+    }
+    else
+    {
+#pragma unroll
+        for (int k = 0; k < 6; ++k) pw[k] = (uint32_t)__ldg(px + 2 * k) | ((uint32_t)__ldg(px + 2 * k + 1) << 16);
+    }
     unsigned short* o = T.out + p * 3;
     unsigned short res[12];
+    const float wy = c.wy;
 #pragma unroll
     for (int i = 0; i < 4; ++i)
     {
+        float wx = c.wx;
         if (i > 0)
         {
-            c = up_coef_s(T.usx[0], T.usy[0], uw, uh, x + i, y);
-            if (c.x0 != cur)  // advanced by one column
+            int x0;
+            up_coef_x(sx, uw, x + i, x0, wx);
+            if (x0 != cur)  // advanced by one column
             {
-                cur = c.x0;
+                cur = x0;
                 L = R;
-                R = tap_column(g1, rc, uw, c.y0, c.y1, c.x1);
+                R = tap_column(g1, rc, uw, c.y0, c.y1, min(x0 + 1, uw - 1));
             }
         }
-        const float wx = c.wx, wy = c.wy;
-        float r[3] = {u2f(__ldg(px + 3 * i)), u2f(__ldg(px + 3 * i + 1)), u2f(__ldg(px + 3 * i + 2))};
+        float r[3];
+#pragma unroll
+        for (int ch = 0; ch < 3; ++ch)
+        {
+            const int e = 3 * i + ch;  // value index in the quad
+            r[ch] = u2f((pw[e >> 1] >> (16 * (e & 1))) & 0xffffu);
+        }
         const float lap[3] = {fsub(r[0], up_mix(L.g0.x, R.g0.x, L.g1.x, R.g1.x, wx, wy)),
                               fsub(r[1], up_mix(L.g0.y, R.g0.y, L.g1.y, R.g1.y, wx, wy)),
                               fsub(r[2], up_mix(L.g0.z, R.g0.z, L.g1.z, R.g1.z, wx, wy))};
@@ -2034,6 +2138,10 @@ __global__ void __launch_bounds__(256) k_final0(BlendArgs a, const Unit* __restr
     const int rows = min(a.bandRows, H - row0);
     const int qpr = (W + 3) >> 2;  // quads per row
     const int nq = rows * qpr;
+    const signed char* owner = T.owner;
+    // a quad's four owner bytes as one word: rows of a multiple of 4 pixels
+    // on a 4-byte aligned map
+    const bool ownWord = (W & 3) == 0 && (reinterpret_cast<uintptr_t>(owner) & 3) == 0;
     for (int qi = threadIdx.x; qi < nq; qi += blockDim.x)
     {
         const int y = row0 + qi / qpr;
@@ -2041,8 +2149,17 @@ __global__ void __launch_bounds__(256) k_final0(BlendArgs a, const Unit* __restr
         const long long p = (long long)y * W + x;
         const int cnt = min(4, W - x);
         int own[4];
+        if (ownWord)
+        {
+            const uint32_t w = __ldg(reinterpret_cast<const uint32_t*>(owner + p));
 #pragma unroll
-        for (int i = 0; i < 4; ++i) own[i] = i < cnt ? (int)T.owner[p + i] : -2;
+            for (int i = 0; i < 4; ++i) own[i] = (int)(signed char)(w >> (8 * i));
+        }
+        else
+        {
+#pragma unroll
+            for (int i = 0; i < 4; ++i) own[i] = i < cnt ? (int)owner[p + i] : -2;
+        }
         if (cnt == 4 && T.bands > 1 && own[0] >= 0 && own[1] == own[0] && own[2] == own[0] && own[3] == own[0])
         {
             final_quad(T, C, rc, uw, uh, p, y, x, own[0]);

@@ -282,6 +282,7 @@ int Plan::build(const std::vector<TileSpec>& specs, int numBands, bool renderPat
         I360B_CUDA(cudaStreamCreateWithFlags(&side, cudaStreamNonBlocking), "chain stream");
         I360B_CUDA(cudaEventCreateWithFlags(&evFork, cudaEventDisableTiming), "chain event");
         I360B_CUDA(cudaEventCreateWithFlags(&evJoin, cudaEventDisableTiming), "chain event");
+        I360B_CUDA(cudaEventCreateWithFlags(&evLag, cudaEventDisableTiming), "chain event");
     }
     // ---- device allocation -----------------------------------------------
     size_t unitBytes = align256(std::max<size_t>(unitCap, 1) * sizeof(Unit));
@@ -510,6 +511,15 @@ int Plan::set_precision(int mode, cudaStream_t s)
     return I360B_SUCCESS;
 }
 
+int Plan::set_chain_lag(int stage, cudaStream_t s)
+{
+    if (stage < -1 || stage >= kStages - 1) return fail(I360B_INVALID_PARAM, "chain stagger must be -1 or a stage 0-8");
+    I360B_CUDA(cudaStreamSynchronize(s), "plan stagger");
+    chainLag = stage;
+    drop_graphs();
+    return I360B_SUCCESS;
+}
+
 int Plan::set_fusion(int levels, cudaStream_t s)
 {
     if (levels < 0 || levels > 2) return fail(I360B_INVALID_PARAM, "fused pyramid levels must be 0, 1 or 2");
@@ -545,6 +555,7 @@ Plan::~Plan()
     if (side) cudaStreamSynchronize(side);
     if (evFork) cudaEventDestroy(evFork);
     if (evJoin) cudaEventDestroy(evJoin);
+    if (evLag) cudaEventDestroy(evLag);
     if (side) cudaStreamDestroy(side);
     if (graphExec) cudaGraphExecDestroy(graphExec);
     if (graph) cudaGraphDestroy(graph);
@@ -675,9 +686,20 @@ int Plan::enqueue_range(cudaStream_t s, int first, int last, cudaEvent_t* ev)
             I360B_TRY(check_launch("bbox init kernel"));
             I360B_CUDA(cudaMemsetAsync(dError, 0, sizeof(int), s), "error flag reset");
         }
-        I360B_CUDA(cudaEventRecord(evFork, s), "chain fork");
-        I360B_CUDA(cudaStreamWaitEvent(side, evFork, 0), "chain fork");
-        I360B_TRY(enqueue_chain(0, first, last, s));
+        if (chainLag >= first && chainLag < last)
+        {
+            // staggered: chain 1 starts once chain 0 has finished stage chainLag
+            I360B_TRY(enqueue_chain(0, first, chainLag, s));
+            I360B_CUDA(cudaEventRecord(evLag, s), "chain stagger");
+            I360B_CUDA(cudaStreamWaitEvent(side, evLag, 0), "chain stagger");
+            I360B_TRY(enqueue_chain(0, chainLag + 1, last, s));
+        }
+        else
+        {
+            I360B_CUDA(cudaEventRecord(evFork, s), "chain fork");
+            I360B_CUDA(cudaStreamWaitEvent(side, evFork, 0), "chain fork");
+            I360B_TRY(enqueue_chain(0, first, last, s));
+        }
         I360B_TRY(enqueue_chain(1, first, last, side));
         I360B_CUDA(cudaEventRecord(evJoin, side), "chain join");
         I360B_CUDA(cudaStreamWaitEvent(s, evJoin, 0), "chain join");
@@ -1146,6 +1168,22 @@ extern "C" int i360b_render_plan_autotune(i360b_render_plan* plan, void* stream,
     if (bandRows) *bandRows = bestR;
     if (dtSlots) *dtSlots = bestS;
     if (bestMs) *bestMs = best / 2.0f;
+    return I360B_SUCCESS;
+}
+
+extern "C" int i360b_render_plan_set_chain_lag(i360b_render_plan* plan, int stage, void* stream)
+{
+    clear_error();
+    if (!plan) return fail(I360B_INVALID_PARAM, "Null plan.");
+    I360B_TRY(ensure_ready());
+    return plan->plan.set_chain_lag(stage, static_cast<cudaStream_t>(stream));
+}
+
+extern "C" int i360b_render_plan_get_chain_lag(i360b_render_plan* plan, int* stage)
+{
+    clear_error();
+    if (!plan || !stage) return fail(I360B_INVALID_PARAM, "Null pointer argument.");
+    *stage = plan->plan.nChains > 1 ? plan->plan.chainLag : -1;
     return I360B_SUCCESS;
 }
 

@@ -103,7 +103,13 @@ struct Plan
     Range dtRange[kMaxChains] = {};      // chamfer item lists in dInts, per chain
     Range seamRange[kMaxChains] = {};    // seam tile lists in dInts, per chain
     cudaStream_t side = nullptr;         // second chain's stream
-    cudaEvent_t evFork = nullptr, evJoin = nullptr;
+    cudaEvent_t evFork = nullptr, evJoin = nullptr, evLag = nullptr;
+    // Chain stagger: with chainLag = L >= 0, chain 1's first stage of a run
+    // waits until chain 0 has finished stage L, so the seam search of one
+    // chain (a CTA per tile, most SMs free) runs beside the other chain's
+    // full-GPU stages instead of beside its own seam search.  -1: both
+    // chains start together.  Ordering only: the render is the same.
+    int chainLag = -1;
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t graphExec = nullptr;
 
@@ -137,12 +143,14 @@ struct Plan
     // Switches the band height and chamfer ring depth; the next execute
     // recaptures the graph.  Synchronous on `s`.
     int set_tuning(int rows, int slots, cudaStream_t s);
-    // Switches the level-fusion depth (0 or 2); recaptures on next execute.
+    // Switches the level-fusion depth (0, 1 or 2); recaptures on next execute.
     int set_fusion(int levels, cudaStream_t s);
     // Switches the pyramid storage precision (0 exact, 1 FP16).
     int set_precision(int mode, cudaStream_t s);
     // Switches the tile-warp form (0 or 1); remakes the work lists.
     int set_warp_shape(int shape, cudaStream_t s);
+    // Sets the chain stagger (-1 or a stage 0-8); recaptures on next execute.
+    int set_chain_lag(int stage, cudaStream_t s);
     // Changes the bounded-wait limit; the next execute recaptures the graph.
     int set_wait_limit(long long cycles, cudaStream_t s);
     void drop_graphs();

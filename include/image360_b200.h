@@ -428,6 +428,19 @@ I360B_API int i360b_render_plan_get_tuning(i360b_render_plan* plan, int* bandRow
                                            int* warpShape);
 I360B_API int i360b_render_plan_set_tuning(i360b_render_plan* plan, int bandRows, int dtSlots, int fusedLevels,
                                            int warpShape, void* stream);
+/* Chain stagger.  A plan splits its tiles into two chains of about equal
+ * work whose stages run on two streams inside its graph.  With stage L >= 0
+ * the second chain starts only once the first has finished stage L (of the
+ * stages a run covers), so the seam search of one chain (a CTA per tile,
+ * most SMs free) overlaps the other chain's full-GPU stages; -1 starts both
+ * together (the default: on the 90-tile panorama a stagger measured no
+ * faster for whole runs and slower for runs split after stage 0, so the
+ * autotuner leaves it).  Ordering only: every setting renders the same
+ * bits.  A plan with one chain reports -1.
+ * Synchronous on `stream`; the next execute recaptures the plan's graph.
+ * No reference counterpart. */
+I360B_API int i360b_render_plan_set_chain_lag(i360b_render_plan* plan, int stage, void* stream);
+I360B_API int i360b_render_plan_get_chain_lag(i360b_render_plan* plan, int* stage);
 /* Precision of the render's stored pyramid levels.  EXACT keeps them in
  * FP32 and renders the CPU backend's output bit for bit.  FP16 is the native
  * mode: the levels a plan keeps in memory (levels >= 2 with the fused

@@ -111,9 +111,28 @@ def test_autotuner_picks_fusion_depth_without_changing_bits(backend, oracle_c):
     _, ref = oracle_c.render_tiles(4, host, inv, gains, pano.tiles, 6)
     tuned = plan.autotune()
     assert tuned["fused_levels"] in (0, 1, 2) and tuned["band_rows"] in (8, 16, 32, 64) and tuned["warp_shape"] in (0, 1)
+    assert tuned["chain_lag"] == -1
     for o in outs:
         o.fill_(-1)
     assert plan.execute() == ComputeResult.SUCCESS and plan.wait() == ComputeResult.SUCCESS
     for o, r in zip(outs, ref):
         assert np.array_equal(_host(o), r)
+    # the chain stagger orders work only: whole runs and the split run (stage
+    # 0, then 1-9) render the same bits at every setting
+    for lag in (-1, 0, 3, 8):
+        assert plan.set_chain_lag(lag) == ComputeResult.SUCCESS
+        assert plan.chain_lag() == lag
+        for split in (False, True):
+            for o in outs:
+                o.fill_(-1)
+            if split:
+                assert plan.execute_stages(0, 0) == ComputeResult.SUCCESS
+                assert plan.execute_stages(1, 9) == ComputeResult.SUCCESS
+            else:
+                assert plan.execute() == ComputeResult.SUCCESS
+            assert plan.wait() == ComputeResult.SUCCESS
+            for o, r in zip(outs, ref):
+                assert np.array_equal(_host(o), r), (lag, split)
+    assert plan.set_chain_lag(9) == ComputeResult.INVALID_PARAM
+    assert plan.set_chain_lag(-2) == ComputeResult.INVALID_PARAM
     plan.close()
