@@ -995,6 +995,22 @@ __device__ __forceinline__ unsigned chunk_byte_mask(uint4 v, unsigned rep)
     return mask;
 }
 
+// Bytes o .. o + 15 of the 32 bytes a, b (0 <= o < 16).
+__device__ __forceinline__ uint4 bytes16_at(uint4 a, uint4 b, int o)
+{
+    const unsigned sh = (unsigned)(o & 3) * 8u;
+    uint32_t w0, w1, w2, w3, w4;
+    switch (o >> 2)
+    {
+    case 0: w0 = a.x; w1 = a.y; w2 = a.z; w3 = a.w; w4 = b.x; break;
+    case 1: w0 = a.y; w1 = a.z; w2 = a.w; w3 = b.x; w4 = b.y; break;
+    case 2: w0 = a.z; w1 = a.w; w2 = b.x; w3 = b.y; w4 = b.z; break;
+    default: w0 = a.w; w1 = b.x; w2 = b.y; w3 = b.z; w4 = b.w; break;
+    }
+    return make_uint4(__funnelshift_r(w0, w1, sh), __funnelshift_r(w1, w2, sh), __funnelshift_r(w2, w3, sh),
+                      __funnelshift_r(w3, w4, sh));
+}
+
 // Contested band of a column line (SeamBlend.cpp:347-359): the positions
 // within kSeamRadius of the crossover covered by both contributors, as
 // lo..hi (lo > hi: none).  The coverage bits of 8 rows are requested at once
@@ -1138,25 +1154,27 @@ __global__ void __launch_bounds__(kSeamThreads, 1) k_seam(BlendArgs a, const int
                     }
                 }
             }
-            else if ((w & 15) == 0 && (reinterpret_cast<uintptr_t>(T.owner) & 15) == 0)
+            else if ((reinterpret_cast<uintptr_t>(T.owner) & 15) == 0)
             {
                 // Lines are columns.  The crossover of a column (the first
                 // pixel of the other owner after its first I/J pixel) is the
                 // later of the column's first I row and first J row, so both
                 // are found by one parallel pass over the overlap box instead
-                // of a walk down each column: 16-byte chunks of each row (their
-                // column offset is the same on every row, the row pitch being a
-                // multiple of 16), threads over (chunk, row segment), each
-                // segment scanned top-down and its first finds merged by
-                // atomicMin into the line arrays (used for the first rows
-                // here, overwritten with the band below).
+                // of a walk down each column: 16-byte chunks of each row,
+                // threads over (chunk, row segment), each segment scanned
+                // top-down and its first finds merged by atomicMin into the
+                // line arrays (used for the first rows here, overwritten with
+                // the band below).  With a row pitch that is a multiple of 16
+                // the chunks are the aligned ones (the same column offset on
+                // every row); otherwise a chunk is 16 columns of the box, read
+                // as the aligned chunk(s) holding them.
                 int* fI = sLo;
                 int* fJ = sHi;
                 for (int l = tid; l < numLines; l += kSeamThreads) fI[l] = fJ[l] = 0x7fffffff;
                 __syncthreads();
+                const bool pitch16 = (w & 15) == 0;
                 const signed char* rowp0 = T.owner + pix(0, 0);
-                const int off = (int)(reinterpret_cast<uintptr_t>(rowp0) & 15);
-                const signed char* base0 = rowp0 - off;
+                const int off = pitch16 ? (int)(reinterpret_cast<uintptr_t>(rowp0) & 15) : 0;
                 const int nCh = (off + numLines + 15) >> 4;
                 const int nSeg = max(1, kSeamThreads / nCh);
                 const int segRows = (lineLen + nSeg - 1) / nSeg;
@@ -1171,7 +1189,18 @@ __global__ void __launch_bounds__(kSeamThreads, 1) k_seam(BlendArgs a, const int
                     const int t1 = min(lineLen, (seg + 1) * segRows);
                     for (int t = seg * segRows; t < t1 && (foundI & foundJ) != valid; ++t)
                     {
-                        const uint4 v = *reinterpret_cast<const uint4*>(base0 + (size_t)t * w + 16 * c);
+                        // byte b of v: column tb + b of row t
+                        const signed char* at = rowp0 + (size_t)t * w + tb;
+                        const int o = (int)(reinterpret_cast<uintptr_t>(at) & 15);
+                        const uint4* ch = reinterpret_cast<const uint4*>(at - o);
+                        uint4 v = ch[0];
+                        if (o != 0)
+                        {
+                            // the second chunk only when a byte of the box lies
+                            // in it (so the read stays within the map's padding)
+                            const uint4 nx = o + b1 > 16 ? ch[1] : make_uint4(0u, 0u, 0u, 0u);
+                            v = bytes16_at(v, nx, o);
+                        }
                         const unsigned nI = chunk_byte_mask(v, repI) & valid & ~foundI;
                         const unsigned nJ = chunk_byte_mask(v, repJ) & valid & ~foundJ;
                         for (unsigned m = nI; m; m &= m - 1) atomicMin(&fI[tb + __ffs(m) - 1], t);

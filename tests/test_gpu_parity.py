@@ -212,3 +212,25 @@ def test_blend_wide_chunk(backend, oracle_c):
     out = np.zeros((w, h, 3), np.uint16)
     assert backend.blend_chunk_contributors([at, bt], h, w, out, 5) == ComputeResult.SUCCESS, backend.get_last_error()
     assert np.array_equal(out, oracle_c.blend([at, bt], 5))
+
+
+@pytest.mark.parametrize("w", [16, 17, 23, 30, 32, 45, 48, 61, 64, 100, 161])
+def test_blend_column_scan_pitches(backend, oracle_c, w):
+    """Tall overlaps (the seam search scans columns) on chunks of every row
+    pitch modulo 16, with the overlap box starting at different columns: the
+    column pass reads 16-byte chunks at every alignment.  A third contributor
+    owns part of the overlap, so some columns hold only one of the pair."""
+    rng = np.random.default_rng(w)
+    h = 150 + w
+    bufs = []
+    for x0, x1 in ((0, w // 2 + 3), (w // 3, w - 1), (w // 4, w // 2)):
+        b = np.zeros((h, w, 3), np.uint16)
+        y0 = int(rng.integers(0, 10))
+        b[y0:, x0:x1 + 1] = rng.integers(100, 30000, (h - y0, x1 - x0 + 1, 3))
+        bufs.append(b)
+    bufs[2][: h // 2] = 0
+    for bands in (3, 5):
+        out = np.zeros((h, w, 3), np.uint16)
+        assert backend.blend_chunk_contributors(bufs, w, h, out, bands) == ComputeResult.SUCCESS, backend.get_last_error()
+        ref = oracle_c.blend(bufs, bands)
+        assert np.array_equal(out, ref), (w, bands, int(np.abs(out.astype(int) - ref).max()))
