@@ -106,7 +106,8 @@ class ClockSampler:
 # our arm
 # ---------------------------------------------------------------------------
 def setup_ours(cfg, rank, device, world=1, sharded=False):
-    """The rank's render: with `sharded`, its LPT share of one panorama (only
+    """The rank's render: with `sharded`, its share of one panorama (a
+    contiguous band of tile columns balanced by area x contributors, only
     the frames its tiles need, tiles renumbered to them); otherwise a whole
     panorama of its own seed."""
     import torch
@@ -264,7 +265,8 @@ def run_ours(args, rank, world, local_rank):
     cfg = synth.C1 if args.scale == 1.0 else synth.scaled(synth.C1, args.scale, tile=synth.C1.tile)
     sharded = world > 1 and args.mode == "sharded"
     if sharded:
-        # one panorama of 8 frame columns per rank, its tiles split by LPT
+        # one panorama of 8 frame columns per rank, its tiles split into
+        # contiguous column bands balanced by cost
         cfg = synth.PanoConfig(**{**cfg.__dict__, "cols": cfg.cols * world})
     net = untrained = train_info = None
     if not args.no_learned and world == 1:
@@ -343,22 +345,23 @@ def run_ours(args, rank, world, local_rank):
     blend_stages = ["chamfer_forward", "chamfer_backward", "ownership", "seam_dp", "pyramid_base", "pyramid_down",
                     "blend_bands", "collapse", "fine_output"]
     blend_ms = sum(stages[s] for s in blend_stages)
-    # Dominant memory-bound kernel: the tile warp (one launch per chain and
-    # execute; the seam step above it in the launch list is a sequential
+    # Dominant memory-bound kernel: the tile warp in the form the plan runs
+    # (one launch per chain and execute; the seam step is a sequential
     # dynamic program, not bandwidth-bound).  Traffic per step: the ncu DRAM
-    # bytes of a smaller capture (profiles/k_warp_tiles_traffic.json), read
-    # bytes scaled by covered item pixels and written bytes by item pixels.
+    # bytes of a smaller capture of that form (profiles/<kernel>_traffic.json),
+    # read bytes scaled by covered item pixels and written bytes by item pixels.
     dom = "warp_gain_coverage"
+    kname = "k_warp_tiles" if plan.tuning()["warp_shape"] == 1 else "k_warp_rows"
     ach = sb[dom] / (stages[dom] / 1e3) / 1e9
     traffic = None
-    tp = os.path.join(ROOT, "profiles", "k_warp_tiles_traffic.json")
+    tp = os.path.join(ROOT, "profiles", kname + "_traffic.json")
     if os.path.exists(tp):
         with open(tp) as f:
             tj = json.load(f)
         item_px = sum(t[2] * t[3] * len(t[4]) for t in S["pano"].tiles)
         traffic = int(tj["read_bytes_per_covered_item_px"] * stats["coveredItemPixels"] +
                       tj["write_bytes_per_item_px"] * item_px)
-    roof = {"kernel": "k_warp_tiles (" + dom + ")", "bound": "hbm", "achieved": round(ach, 1), "peak": peaks["hbm_gbs"],
+    roof = {"kernel": kname + " (" + dom + ")", "bound": "hbm", "achieved": round(ach, 1), "peak": peaks["hbm_gbs"],
             "unit": "GB/s", "frac": round(ach / peaks["hbm_gbs"], 4), "traffic": traffic,
             "algorithmic_bytes": sb[dom], "ms": round(stages[dom], 3),
             "peak_source": peak_kind + " (hbm_gbs, burst copy)"}
@@ -385,7 +388,7 @@ def run_ours(args, rank, world, local_rank):
                    "l2": "inputs and outputs larger than L2 (no flush)",
                    "blend": "plain seam blend (--no-learned: learned blend not measured in this run)",
                    "parallelism": (f"{world} ranks, one panorama of {cfg.rows}x{cfg.cols} frames, tiles split by "
-                                   f"LPT on area x contributors, no data-path collective" if sharded else
+                                   f"contiguous tile-column bands balanced on area x contributors, no data-path collective" if sharded else
                                    f"{world} independent panoramas" if world > 1 else "1 GPU"),
                    "schedule": "steps back to back: step k+1's demosaic (own stream) overlaps stages 1-9 of step "
                                "k's render, after its warp stage has read the frames",

@@ -242,7 +242,11 @@ __device__ __forceinline__ WarpItem warp_item(const ItemDev& it)
 // contributor, each warp whole rows in 64-pixel segments with two pixels per
 // lane in flight, gathering taps from the frame through L1; rows and segments
 // outside the frame's footprint box are written as zeros without evaluating
-// the mapping.
+// the mapping.  The warps take the band's rows interleaved (warp w: rows w,
+// w + 8, ...), so at any time the CTA's warps walk eight neighbouring rows
+// side by side and the source rows they share (a bilinear tap pair reads two
+// rows, each also read by the next output row) are reused from L1 rather
+// than fetched again from DRAM after the whole GPU has streamed past them.
 __global__ void __launch_bounds__(256, 8) k_warp_rows(BlendArgs a, const Unit* __restrict__ units)
 {
     const Unit u = units[blockIdx.x];
@@ -256,7 +260,7 @@ __global__ void __launch_bounds__(256, 8) k_warp_rows(BlendArgs a, const Unit* _
     const int rowsPerWarp = a.bandRows >> 3;
     for (int r = 0; r < rowsPerWarp; ++r)
     {
-        const int y = u.by * a.bandRows + warp * rowsPerWarp + r;
+        const int y = u.by * a.bandRows + r * 8 + warp;
         if (y >= H) break;
         const float dY = (float)(y + offY);
         const float hy[3] = {fmul(wi.H[1], dY), fmul(wi.H[4], dY), fmul(wi.H[7], dY)};

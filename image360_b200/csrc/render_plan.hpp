@@ -64,14 +64,14 @@ struct Plan
     // materialised by k_down0s and read by k_fine (the level-1 blend,
     // collapse and output fused), 0 = every level materialised (k_down0s,
     // k_blend_level / k_collapse at level 1, k_final0).
-    int fusedLevels = 2;
+    int fusedLevels = 0;  // the fastest on the 90-tile panorama (the autotuner times all three)
     // Storage of the materialised pyramid levels: 0 FP32 (exact, the
     // reference's values bit for bit), 1 FP16 with FP32 arithmetic (the
     // native mode; needs the fused levels, so level 1 is never stored).
     int storage16 = 0;
     // Tile-warp form: 1 = staged 128x32 blocks (source footprint in shared
     // memory), 0 = row bands gathering through L1.
-    int warpShape = 1;
+    int warpShape = 0;  // the faster form on the 90-tile panorama (the autotuner times both)
     // Limit of the bounded device waits (SM cycles; 0 = give up at the first
     // wait that is not satisfied at once, a test setting).
     long long spinLimit = kSpinCyclesDefault;

@@ -70,13 +70,17 @@ def test_fused_odd_tile_sides_exact(backend, oracle_c):
     gains = (1.0 / pano.gains[ut.frame_of]).astype(np.float32)
     dv = [dev[f] for f in ut.frame_of]
     plan, outs = _plan(dv, cfg, ut.to_canvas, gains, ut.tiles, 6)
-    assert plan.tuning()["fused_levels"] == 2
-    assert plan.execute() == ComputeResult.SUCCESS and plan.wait() == ComputeResult.SUCCESS
+    assert plan.tuning()["fused_levels"] == 0 and plan.tuning()["warp_shape"] == 0  # the defaults
     inv = np.stack([synth.inverse_homography_f32(H) for H in ut.to_canvas])
     _, ref = oracle_c.render_tiles(4, [host[f] for f in ut.frame_of], inv, gains, ut.tiles, 6)
     assert len({t[2] % 4 for t in ut.tiles}) > 1
-    for t, (o, r) in enumerate(zip(outs, ref)):
-        assert np.array_equal(_host(o), r), (t, ut.tiles[t][:4])
+    for fused, shape in ((2, 1), (1, 0), (0, 0)):
+        assert plan.set_tuning(16, 0, fused, shape) == ComputeResult.SUCCESS
+        for o in outs:
+            o.fill_(-1)
+        assert plan.execute() == ComputeResult.SUCCESS and plan.wait() == ComputeResult.SUCCESS
+        for t, (o, r) in enumerate(zip(outs, ref)):
+            assert np.array_equal(_host(o), r), (fused, shape, t, ut.tiles[t][:4])
     plan.close()
 
 
