@@ -1719,8 +1719,7 @@ __global__ void __launch_bounds__(256, 4) k_down0s(BlendArgs a, const Unit* __re
                     if (X + c < dw)
                     {
                         const size_t q = qrow + (size_t)(Y0 + j) * dw + X + c;
-                        it.nd[q] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-                        it.wg[q] = 0.0f;
+                        pyr_store(it.nd, it.wg, q, make_float4(0.0f, 0.0f, 0.0f, 0.0f), 0.0f, a.half);
                     }
             return;
         }
@@ -1797,9 +1796,10 @@ __global__ void __launch_bounds__(256, 4) k_down0s(BlendArgs a, const Unit* __re
                 {
                     if (X + c >= dw) continue;
                     const size_t q = qrow + (size_t)Y * dw + X + c;
-                    it.nd[q] = make_float4(fmul((float)P[c][0], s256), fmul((float)P[c][1], s256),
-                                           fmul((float)P[c][2], s256), fmul((float)(P[c][3] >> 16), s256));
-                    it.wg[q] = fmul((float)(P[c][3] & 0xffff), s256);
+                    pyr_store(it.nd, it.wg, q,
+                              make_float4(fmul((float)P[c][0], s256), fmul((float)P[c][1], s256),
+                                          fmul((float)P[c][2], s256), fmul((float)(P[c][3] >> 16), s256)),
+                              fmul((float)(P[c][3] & 0xffff), s256), a.half);
                 }
             }
         }
@@ -2021,7 +2021,7 @@ __device__ __forceinline__ void final_store(unsigned short* o, const float* r)
 
 // One output pixel (the general path).
 __device__ __noinline__ void final_pixel(const TileDev& T, const ItemCache& C, const float* rc, int uw, int uh,
-                                            long long p, int own)
+                                            long long p, int own, int half)
 {
     unsigned short* o = T.out + p * 3;
     if (own < 0)
@@ -2036,11 +2036,12 @@ __device__ __noinline__ void final_pixel(const TileDev& T, const ItemCache& C, c
     if (T.bands > 1)
     {
         const UpCoef c = up_coef_s(T.usx[0], T.usy[0], uw, uh, x, y);
-        const float4* g1 = C.nd[own] + T.loff[1];
-        const float3 a00 = gauss_of(__ldg(g1 + (size_t)c.y0 * uw + c.x0));
-        const float3 a10 = gauss_of(__ldg(g1 + (size_t)c.y0 * uw + c.x1));
-        const float3 a01 = gauss_of(__ldg(g1 + (size_t)c.y1 * uw + c.x0));
-        const float3 a11 = gauss_of(__ldg(g1 + (size_t)c.y1 * uw + c.x1));
+        const float4* nd = C.nd[own];
+        const size_t l1 = T.loff[1];
+        const float3 a00 = gauss_of(nd_at(nd, l1 + (size_t)c.y0 * uw + c.x0, half));
+        const float3 a10 = gauss_of(nd_at(nd, l1 + (size_t)c.y0 * uw + c.x1, half));
+        const float3 a01 = gauss_of(nd_at(nd, l1 + (size_t)c.y1 * uw + c.x0, half));
+        const float3 a11 = gauss_of(nd_at(nd, l1 + (size_t)c.y1 * uw + c.x1, half));
         const float lap[3] = {fsub(r[0], up_mix(a00.x, a10.x, a01.x, a11.x, c.wx, c.wy)),
                               fsub(r[1], up_mix(a00.y, a10.y, a01.y, a11.y, c.wx, c.wy)),
                               fsub(r[2], up_mix(a00.z, a10.z, a01.z, a11.z, c.wx, c.wy))};
@@ -2064,12 +2065,13 @@ struct TapColumn
     float3 g0, g1, u0, u1;
 };
 
-__device__ __forceinline__ TapColumn tap_column(const float4* g1, const float* rc, int uw, int y0, int y1, int col)
+__device__ __forceinline__ TapColumn tap_column(const float4* nd, size_t l1, const float* rc, int uw, int y0, int y1,
+                                                int col, int half)
 {
     const size_t q0 = (size_t)y0 * uw + col, q1 = (size_t)y1 * uw + col;
     TapColumn t;
-    t.g0 = gauss_of(__ldg(g1 + q0));
-    t.g1 = gauss_of(__ldg(g1 + q1));
+    t.g0 = gauss_of(nd_at(nd, l1 + q0, half));
+    t.g1 = gauss_of(nd_at(nd, l1 + q1, half));
     t.u0 = make_float3(__ldg(rc + q0 * 3), __ldg(rc + q0 * 3 + 1), __ldg(rc + q0 * 3 + 2));
     t.u1 = make_float3(__ldg(rc + q1 * 3), __ldg(rc + q1 * 3 + 1), __ldg(rc + q1 * 3 + 2));
     return t;
@@ -2082,14 +2084,15 @@ __device__ __forceinline__ TapColumn tap_column(const float4* g1, const float* r
 // column's texels and reciprocals computed once; every pixel still combines
 // its own four taps with its own weights in the reference's order.
 __device__ __forceinline__ void final_quad(const TileDev& T, const ItemCache& C, const float* rc, int uw, int uh,
-                                           long long p, int y, int x, int own)
+                                           long long p, int y, int x, int own, int half)
 {
-    const float4* g1 = C.nd[own] + T.loff[1];
+    const float4* g1 = C.nd[own];
+    const size_t l1 = T.loff[1];
     const float sx = T.usx[0];
     UpCoef c = up_coef_s(sx, T.usy[0], uw, uh, x, y);
     int cur = c.x0;
-    TapColumn L = tap_column(g1, rc, uw, c.y0, c.y1, cur);
-    TapColumn R = tap_column(g1, rc, uw, c.y0, c.y1, c.x1);
+    TapColumn L = tap_column(g1, l1, rc, uw, c.y0, c.y1, cur, half);
+    TapColumn R = tap_column(g1, l1, rc, uw, c.y0, c.y1, c.x1, half);
     const unsigned short* px = C.img[own] + p * 3;
     // the quad's 12 source values: three 8-byte loads when aligned
     uint32_t pw[6];
@@ -2124,7 +2127,7 @@ __device__ __forceinline__ void final_quad(const TileDev& T, const ItemCache& C,
             {
                 cur = x0;
                 L = R;
-                R = tap_column(g1, rc, uw, c.y0, c.y1, min(x0 + 1, uw - 1));
+                R = tap_column(g1, l1, rc, uw, c.y0, c.y1, min(x0 + 1, uw - 1), half);
             }
         }
         float r[3];
@@ -2195,12 +2198,12 @@ __global__ void __launch_bounds__(256) k_final0(BlendArgs a, const Unit* __restr
         }
         if (cnt == 4 && T.bands > 1 && own[0] >= 0 && own[1] == own[0] && own[2] == own[0] && own[3] == own[0])
         {
-            final_quad(T, C, rc, uw, uh, p, y, x, own[0]);
+            final_quad(T, C, rc, uw, uh, p, y, x, own[0], a.half);
             continue;
         }
 #pragma unroll
         for (int i = 0; i < 4; ++i)
-            if (i < cnt) final_pixel(T, C, rc, uw, uh, p + i, own[i]);
+            if (i < cnt) final_pixel(T, C, rc, uw, uh, p + i, own[i], a.half);
     }
 }
 

@@ -506,7 +506,6 @@ int Plan::set_precision(int mode, cudaStream_t s)
         return fail(I360B_INVALID_PARAM, "Unknown precision mode %d.", mode);
     I360B_CUDA(cudaStreamSynchronize(s), "plan precision");
     storage16 = mode == I360B_PRECISION_FP16 ? 1 : 0;
-    if (storage16) fusedLevels = 2;
     drop_graphs();
     return I360B_SUCCESS;
 }
@@ -523,8 +522,6 @@ int Plan::set_chain_lag(int stage, cudaStream_t s)
 int Plan::set_fusion(int levels, cudaStream_t s)
 {
     if (levels < 0 || levels > 2) return fail(I360B_INVALID_PARAM, "fused pyramid levels must be 0, 1 or 2");
-    if (storage16 && levels != 2)
-        return fail(I360B_INVALID_PARAM, "FP16 pyramid storage needs the fused levels (2).");
     I360B_CUDA(cudaStreamSynchronize(s), "plan fusion");
     fusedLevels = levels;
     drop_graphs();
@@ -1124,7 +1121,6 @@ extern "C" int i360b_render_plan_autotune(i360b_render_plan* plan, void* stream,
     {
         for (int fused : {2, 1, 0})
         {
-            if (fused != 2 && P.storage16) continue;  // FP16 storage exists only with the fused levels
             if ((rc = P.set_warp_shape(shape, s)) != I360B_SUCCESS || (rc = P.set_fusion(fused, s)) != I360B_SUCCESS)
                 break;
             float ms;

@@ -65,9 +65,9 @@ struct Plan
     // collapse and output fused), 0 = every level materialised (k_down0s,
     // k_blend_level / k_collapse at level 1, k_final0).
     int fusedLevels = 0;  // the fastest on the 90-tile panorama (the autotuner times all three)
-    // Storage of the materialised pyramid levels: 0 FP32 (exact, the
-    // reference's values bit for bit), 1 FP16 with FP32 arithmetic (the
-    // native mode; needs the fused levels, so level 1 is never stored).
+    // Storage of the materialised pyramid levels (levels >= 1, or >= 2 at
+    // fusion depth 2): 0 FP32 (exact, the reference's values bit for bit),
+    // 1 FP16 with FP32 arithmetic (the native mode).
     int storage16 = 0;
     // Tile-warp form: 1 = staged 128x32 blocks (source footprint in shared
     // memory), 0 = row bands gathering through L1.

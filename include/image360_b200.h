@@ -443,9 +443,10 @@ I360B_API int i360b_render_plan_set_chain_lag(i360b_render_plan* plan, int stage
 I360B_API int i360b_render_plan_get_chain_lag(i360b_render_plan* plan, int* stage);
 /* Precision of the render's stored pyramid levels.  EXACT keeps them in
  * FP32 and renders the CPU backend's output bit for bit.  FP16 is the native
- * mode: the levels a plan keeps in memory (levels >= 2 with the fused
- * pyramid, which it selects) are stored as FP16 with every operation in
- * FP32, halving their traffic; its output is no longer bit-exact, and its
+ * mode: the levels a plan keeps in memory (levels >= 1, or >= 2 at
+ * level-fusion depth 2; any depth may be combined with it) are stored as
+ * FP16 (num / 256, den, weight) with every operation in FP32, halving their
+ * traffic; its output is no longer bit-exact, and its
  * error against the FP64 restatement of the blend is what the tests and the
  * bench report.  Warped pixels stay 16-bit integers in both modes (the same
  * two bytes as FP16, without FP16's rounding of values above 2048).  No

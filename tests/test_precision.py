@@ -120,8 +120,9 @@ def test_gpu_kernels_against_fp64(backend, oracle_c):
 
 @pytest.mark.gpu
 def test_fp16_storage_mode_error_against_fp64(backend, oracle_c):
-    """The native mode (stored pyramid levels in FP16, FP32 arithmetic) on a
-    scaled panorama: every tile's output against the FP64 compose of the
+    """The native mode (stored pyramid levels in FP16, FP32 arithmetic), at
+    each level-fusion depth (levels >= 1 stored at depths 0 and 1, >= 2 at
+    depth 2), on a scaled panorama: every tile's output against the FP64 compose of the
     same warped contributors on the same owner map (the stages before the
     pyramid are exact in both modes), beside the exact mode's error.
     Reported, and bounded: the FP16 rounding of the coarse levels (relative
@@ -140,14 +141,14 @@ def test_fp16_storage_mode_error_against_fp64(backend, oracle_c):
     frames = [(d.data_ptr(), cfg.frame_w, cfg.frame_h, H, float(g)) for d, H, g in zip(dev, pano.to_canvas, gains)]
     plan = RenderPlan(frames, [(*t[:5], o.data_ptr()) for t, o in zip(pano.tiles, outs)], cfg.bands, COORDS_REFERENCE)
     res = {}
-    for mode in (PRECISION_EXACT, PRECISION_FP16):
-        assert plan.set_precision(mode) == 0
+    FP16_D1, FP16_D2 = 10, 11  # FP16 storage at fusion depths 1 and 2 (depth 0 is PRECISION_FP16's row)
+    for mode, depth in ((PRECISION_EXACT, 0), (PRECISION_FP16, 0), (FP16_D1, 1), (FP16_D2, 2)):
+        assert plan.set_precision(PRECISION_FP16 if mode != PRECISION_EXACT else mode) == 0
+        assert plan.set_tuning(16, 0, depth, 0) == 0
         assert plan.execute() == 0 and plan.wait() == 0
         res[mode] = [o.cpu().numpy().view(np.uint16).copy() for o in outs]
-    assert plan.set_precision(PRECISION_FP16) == 0
-    assert plan.set_tuning(16, 0, 0) != 0  # FP16 storage exists only with the fused levels
     plan.close()
-    rows = {PRECISION_EXACT: [], PRECISION_FP16: []}
+    rows = {PRECISION_EXACT: [], PRECISION_FP16: [], FP16_D1: [], FP16_D2: []}
     for t, (x, y, w, h, cs) in enumerate(pano.tiles):
         if len(cs) < 2:
             continue
@@ -157,9 +158,11 @@ def test_fp16_storage_mode_error_against_fp64(backend, oracle_c):
         ref = O.compose(bufs, None, owner, cfg.bands, f64=True)
         for mode in rows:
             rows[mode].append(_err(res[mode][t], ref))
-    ex = (max(r[0] for r in rows[PRECISION_EXACT]), float(np.mean([r[1] for r in rows[PRECISION_EXACT]])))
-    fp = (max(r[0] for r in rows[PRECISION_FP16]), float(np.mean([r[1] for r in rows[PRECISION_FP16]])))
+    stat = {m: (max(r[0] for r in v), float(np.mean([r[1] for r in v]))) for m, v in rows.items()}
+    ex = stat[PRECISION_EXACT]
     print(f"\ncompose vs FP64 over {len(rows[PRECISION_FP16])} tiles: exact max {ex[0]} mean {ex[1]:.5f}; "
-          f"fp16 storage max {fp[0]} mean {fp[1]:.5f}")
+          + "; ".join(f"fp16 storage at depth {d} max {stat[m][0]} mean {stat[m][1]:.5f}"
+                      for m, d in ((PRECISION_FP16, 0), (FP16_D1, 1), (FP16_D2, 2))))
     assert ex[0] <= 1 and ex[1] < 0.02, ex
-    assert fp[0] <= 48 and fp[1] < 1.0, fp
+    for m in (PRECISION_FP16, FP16_D1, FP16_D2):
+        assert stat[m][0] <= 48 and stat[m][1] < 1.0, (m, stat[m])
