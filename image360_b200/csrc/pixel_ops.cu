@@ -76,18 +76,49 @@ __global__ void __launch_bounds__(256) k_demosaic(const unsigned short* __restri
     __shared__ float s[kDmTH + 2][kDmTW + 2];
     const int tx0 = blockIdx.x * kDmTW, ty0 = blockIdx.y * kDmTH;
     const int tid = threadIdx.y * 32 + threadIdx.x;
-    for (int i = tid; i < (kDmTH + 2) * (kDmTW + 2); i += 256)
+    // Black level and white balance of one CFA value (BayerDemosaicKernels.h
+    // BLS/WB steps), as the float the interpolation reads.
+    auto level = [&](unsigned short raw, int gy, int gx) {
+        raw = raw > P.black ? (unsigned short)(raw - P.black) : (unsigned short)0;
+        return u2f(clamp_trunc_u16(fmul(u2f(raw), P.camMul[bayer_color(gy, gx, P.filters)])));
+    };
+    if ((w & 3) == 0 && (reinterpret_cast<uintptr_t>(cfa) & 7) == 0 && tx0 >= 4 && tx0 + kDmTW + 4 <= w)
     {
-        int r = i / (kDmTW + 2), c = i % (kDmTW + 2);
-        int gx = tx0 - 1 + c, gy = ty0 - 1 + r;
-        unsigned short v = 0;
-        if (gx >= 0 && gy >= 0 && gx < w && gy < h)
+        // Interior column of tiles on 8-byte aligned rows: the footprint
+        // (columns tx0-1 .. tx0+64) read as 8-byte words of four values,
+        // columns tx0-4 .. tx0+67.
+        constexpr int kWords = kDmTW / 4 + 2;
+        for (int i = tid; i < (kDmTH + 2) * kWords; i += 256)
         {
-            unsigned short raw = __ldg(cfa + (size_t)gy * w + gx);
-            raw = raw > P.black ? (unsigned short)(raw - P.black) : (unsigned short)0;
-            v = clamp_trunc_u16(fmul(u2f(raw), P.camMul[bayer_color(gy, gx, P.filters)]));
+            const int r = i / kWords, wi = i - r * kWords;
+            const int gy = ty0 - 1 + r, gx0 = tx0 - 4 + 4 * wi;
+            float v[4] = {0.0f, 0.0f, 0.0f, 0.0f};
+            if (gy >= 0 && gy < h)
+            {
+                const uint2 q = __ldg(reinterpret_cast<const uint2*>(cfa + (size_t)gy * w + gx0));
+                v[0] = level((unsigned short)(q.x & 0xffffu), gy, gx0);
+                v[1] = level((unsigned short)(q.x >> 16), gy, gx0 + 1);
+                v[2] = level((unsigned short)(q.y & 0xffffu), gy, gx0 + 2);
+                v[3] = level((unsigned short)(q.y >> 16), gy, gx0 + 3);
+            }
+#pragma unroll
+            for (int k = 0; k < 4; ++k)
+            {
+                const int c = gx0 + k - (tx0 - 1);
+                if (c >= 0 && c < kDmTW + 2) s[r][c] = v[k];
+            }
         }
-        s[r][c] = u2f(v);
+    }
+    else
+    {
+        for (int i = tid; i < (kDmTH + 2) * (kDmTW + 2); i += 256)
+        {
+            int r = i / (kDmTW + 2), c = i % (kDmTW + 2);
+            int gx = tx0 - 1 + c, gy = ty0 - 1 + r;
+            float v = 0.0f;
+            if (gx >= 0 && gy >= 0 && gx < w && gy < h) v = level(__ldg(cfa + (size_t)gy * w + gx), gy, gx);
+            s[r][c] = v;
+        }
     }
     __syncthreads();
     const bool evenW = (w & 1) == 0;

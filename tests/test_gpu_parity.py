@@ -23,7 +23,7 @@ def test_initialize_and_info(backend):
     assert info["multiProcessorCount"] > 0
 
 
-@pytest.mark.parametrize("w,h", [(24, 20), (1, 1), (2, 3), (37, 29), (640, 480), (1001, 77)])
+@pytest.mark.parametrize("w,h", [(24, 20), (1, 1), (2, 3), (37, 29), (640, 480), (1001, 77), (1032, 40)])
 @pytest.mark.parametrize("filters", [synth.RGGB, 0x16161616, 0x61616161, 0x49494949, 0x1E1E1E1E, 0xB4B4B4B4, 0x94616194])
 def test_demosaic_exact(backend, oracle_c, w, h, filters):
     rng = np.random.default_rng(w * 1000 + h)
@@ -32,6 +32,26 @@ def test_demosaic_exact(backend, oracle_c, w, h, filters):
     assert backend.demosaic_bayer(cfa, 64, CAM_MUL, RGB_CAM, filters, out) == ComputeResult.SUCCESS
     ref = oracle_c.demosaic(cfa, 64, CAM_MUL, RGB_CAM, filters)
     assert np.array_equal(out, ref)
+
+
+def test_demosaic_device_buffers_any_alignment(backend, oracle_c):
+    """The device-pointer entry on a CFA starting 2 bytes past an 8-byte
+    boundary (the word-load staging is skipped) and on an aligned one (taken
+    for interior tile columns), both exact."""
+    import torch
+    w, h = 520, 37
+    rng = np.random.default_rng(3)
+    cfa = rng.integers(0, 16384, (h, w), dtype=np.uint16)
+    ref = oracle_c.demosaic(cfa, 64, CAM_MUL, RGB_CAM, synth.RGGB)
+    for shift in (0, 1):
+        raw = torch.zeros(w * h + 4, dtype=torch.int16, device="cuda")
+        raw[shift:shift + w * h] = torch.from_numpy(cfa.reshape(-1).view(np.int16)).cuda()
+        out = torch.zeros((h, w, 3), dtype=torch.int16, device="cuda")
+        rc = backend.launch_demosaic(raw.data_ptr() + 2 * shift, w, h, 64, CAM_MUL, RGB_CAM, synth.RGGB,
+                                     out.data_ptr())
+        assert rc == ComputeResult.SUCCESS, backend.get_last_error()
+        torch.cuda.synchronize()
+        assert np.array_equal(out.cpu().numpy().view(np.uint16), ref), shift
 
 
 def test_demosaic_engine_smoke_vector(backend, oracle_c):
