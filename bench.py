@@ -296,6 +296,9 @@ def run_ours(args, rank, world, local_rank):
     if args.chain_lag is not None:
         assert plan.set_chain_lag(args.chain_lag, sp) == 0
         tuned = {**(tuned or {}), "chain_lag": plan.chain_lag(), "forced": True}
+    if args.chain_split is not None:
+        assert plan.set_chain_split(args.chain_split, sp) == 0
+        tuned = {**(tuned or {}), "chain_split": plan.chain_split(), "forced": True}
     torch.cuda.synchronize()
     stats = plan.stats(sp)
     stages = plan.profile(sp)
@@ -1266,6 +1269,9 @@ def main():
     ap.add_argument("--chain-lag", type=int, default=None,
                     help="force the chain stagger after autotuning (-1: chains together; L: the second chain "
                          "starts after the first finishes stage L)")
+    ap.add_argument("--chain-split", type=int, default=None,
+                    help="force the chain split after autotuning (0: balanced; p: the p%% of tiles with the "
+                         "slowest seam step in the first chain)")
     ap.add_argument("--no-autotune", action="store_true", help="keep the plan's default band height and ring depth")
     ap.add_argument("--train-steps", type=int, default=782, help="Adam steps (782 x 64 = 50k windows)")
     ap.add_argument("--train-batch", type=int, default=64)

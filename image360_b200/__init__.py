@@ -99,6 +99,8 @@ def load_library(path: str = LIB_PATH):
     L.i360b_render_plan_execute_stages.argtypes = [vp, i, i, vp]
     L.i360b_render_plan_set_chain_lag.argtypes = [vp, i, vp]
     L.i360b_render_plan_get_chain_lag.argtypes = [vp, ct.POINTER(i)]
+    L.i360b_render_plan_set_chain_split.argtypes = [vp, i, vp]
+    L.i360b_render_plan_get_chain_split.argtypes = [vp, ct.POINTER(i)]
     L.i360b_render_plan_wait.argtypes = [vp, vp]
     L.i360b_render_plan_destroy.argtypes = [vp]
     L.i360b_render_plan_stats.argtypes = [vp, vp, ct.POINTER(RenderStats)]
@@ -541,7 +543,18 @@ class RenderPlan:
             raise RuntimeError(self.lib.i360b_get_last_error().decode())
         t = self.tuning()
         return {"band_rows": r.value, "dt_slots": k.value, "fused_levels": t["fused_levels"],
-                "warp_shape": t["warp_shape"], "chain_lag": self.chain_lag(), "ms": ms.value}
+                "warp_shape": t["warp_shape"], "chain_lag": self.chain_lag(), "chain_split": self.chain_split(),
+                "ms": ms.value}
+
+    def chain_split(self) -> int:
+        """The chain split: 0 balanced, p = the p percent of tiles with the
+        slowest seam step in the first chain."""
+        v = ct.c_int()
+        self.lib.i360b_render_plan_get_chain_split(self._h, ct.byref(v))
+        return v.value
+
+    def set_chain_split(self, percent: int, stream: int = 0) -> ComputeResult:
+        return ComputeResult(self.lib.i360b_render_plan_set_chain_split(self._h, int(percent), stream or None))
 
     def chain_lag(self) -> int:
         """The chain stagger: the stage of the first chain after which the

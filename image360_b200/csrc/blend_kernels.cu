@@ -1053,7 +1053,9 @@ __global__ void __launch_bounds__(kSeamThreads, 1) k_seam(BlendArgs a, const int
     extern __shared__ unsigned char sm_seam[];
     __shared__ float dpBuf[2][64];
     __shared__ int sLast, sBestK;
-    const TileDev& T = a.tiles[tileList[blockIdx.x]];
+    const int tileIndex = tileList[blockIdx.x];
+    const TileDev& T = a.tiles[tileIndex];
+    const long long tileStart = clock64();
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, tid = threadIdx.x;
     constexpr int nwarps = kSeamThreads / 32;
     const int K = T.numItems;
@@ -1450,6 +1452,7 @@ __global__ void __launch_bounds__(kSeamThreads, 1) k_seam(BlendArgs a, const int
             if (tid == 0) atomicAdd(a.seamCycles + 4, (unsigned long long)(clock64() - tp));
         }
     }
+    if (tid == 0) a.seamTile[tileIndex] = (unsigned long long)(clock64() - tileStart);
 }
 
 // ---------------------------------------------------------------------------

@@ -78,6 +78,7 @@ struct BlendArgs
     // error[1]: the same, kept across executions until the host reads it.
     int* error;
     unsigned long long* seamCycles;    // per-phase SM cycles of the seam kernel (5 counters)
+    unsigned long long* seamTile;      // SM cycles of each tile's seam step in the last execution
     int bandRows;                      // rows per band unit (a multiple of 8; the plan's tuning)
     long long spinLimit;               // cycles a bounded wait may last (0: give up at the first miss)
     int half;                          // materialised pyramid levels stored as FP16 (the native mode)

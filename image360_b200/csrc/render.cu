@@ -229,21 +229,7 @@ int Plan::build(const std::vector<TileSpec>& specs, int numBands, bool renderPat
     nItems = (int)items.size();
     // ---- chains: tiles split into two groups of about equal work ----------
     nChains = nTiles >= 2 ? kMaxChains : 1;
-    tileChain.assign(nTiles, 0);
-    if (nChains > 1)
-    {
-        std::vector<int> order(nTiles);
-        for (int t = 0; t < nTiles; ++t) order[t] = t;
-        auto load = [&](int t) { return (double)tiles[t].w * tiles[t].h * (1 + tiles[t].numItems); };
-        std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return load(a) > load(b); });
-        double sum[kMaxChains] = {0.0, 0.0};
-        for (int t : order)
-        {
-            const int c = sum[1] < sum[0] ? 1 : 0;
-            tileChain[t] = c;
-            sum[c] += load(t);
-        }
-    }
+    balanced_chains();
     // ---- work lists -------------------------------------------------------
     std::vector<Unit> units;
     {
@@ -261,22 +247,7 @@ int Plan::build(const std::vector<TileSpec>& specs, int numBands, bool renderPat
     }
     make_units(bandRows, units);
     std::vector<int> ints;
-    for (int c = 0; c < nChains; ++c)
-    {
-        dtRange[c].start = (int)ints.size();
-        for (int i = 0; i < nItems; ++i)
-            if (tileChain[items[i].tile] == c) ints.push_back(i);
-        dtRange[c].count = (int)ints.size() - dtRange[c].start;
-    }
-    int seamStart = (int)ints.size();
-    for (int c = 0; c < nChains; ++c)
-    {
-        seamRange[c].start = (int)ints.size() - seamStart;
-        for (int t = 0; t < nTiles; ++t)
-            if (tileChain[t] == c && tiles[t].numItems >= 2) ints.push_back(t);
-        seamRange[c].count = (int)ints.size() - seamStart - seamRange[c].start;
-    }
-    nSeam = (int)ints.size() - seamStart;
+    const int seamStart = chain_lists(ints);
     if (nChains > 1)
     {
         I360B_CUDA(cudaStreamCreateWithFlags(&side, cudaStreamNonBlocking), "chain stream");
@@ -290,7 +261,7 @@ int Plan::build(const std::vector<TileSpec>& specs, int numBands, bool renderPat
     size_t itemBytes = align256(std::max(nItems, 1) * sizeof(ItemDev));
     size_t tileBytes = align256(std::max(nTiles, 1) * sizeof(TileDev));
     size_t metaOff = bytes;
-    bytes += unitBytes + intBytes + itemBytes + tileBytes + 256 + 256;
+    bytes += unitBytes + intBytes + itemBytes + tileBytes + 256 + 256 + align256(std::max(nTiles, 1) * 8);
     arenaBytes = bytes;
     if (extArena)
     {
@@ -347,6 +318,7 @@ int Plan::build(const std::vector<TileSpec>& specs, int numBands, bool renderPat
     dTiles = reinterpret_cast<TileDev*>(base + metaOff + unitBytes + intBytes + itemBytes);
     dError = reinterpret_cast<int*>(base + metaOff + unitBytes + intBytes + itemBytes + tileBytes);
     dSeamCycles = reinterpret_cast<unsigned long long*>(base + metaOff + unitBytes + intBytes + itemBytes + tileBytes + 256);
+    dSeamTile = reinterpret_cast<unsigned long long*>(base + metaOff + unitBytes + intBytes + itemBytes + tileBytes + 512);
     if (extArena)
     {
         // Caller-provided scratch: upload the tables on the caller's stream
@@ -363,6 +335,8 @@ int Plan::build(const std::vector<TileSpec>& specs, int numBands, bool renderPat
                        "plan upload");
         I360B_CUDA(cudaMemsetAsync(dError, 0, 2 * sizeof(int), stream), "plan upload");
         I360B_CUDA(cudaMemsetAsync(dSeamCycles, 0, 5 * sizeof(unsigned long long), stream), "plan upload");
+        I360B_CUDA(cudaMemsetAsync(dSeamTile, 0, std::max(nTiles, 1) * sizeof(unsigned long long), stream),
+                   "plan upload");
         I360B_CUDA(cudaStreamSynchronize(stream), "plan upload");
     }
     else
@@ -373,6 +347,7 @@ int Plan::build(const std::vector<TileSpec>& specs, int numBands, bool renderPat
         if (nTiles) I360B_CUDA(cudaMemcpy(dTiles, tiles.data(), nTiles * sizeof(TileDev), cudaMemcpyHostToDevice), "plan upload");
         I360B_CUDA(cudaMemset(dError, 0, 2 * sizeof(int)), "plan upload");
         I360B_CUDA(cudaMemset(dSeamCycles, 0, 5 * sizeof(unsigned long long)), "plan upload");
+        I360B_CUDA(cudaMemset(dSeamTile, 0, std::max(nTiles, 1) * sizeof(unsigned long long)), "plan upload");
     }
     seamList = dInts + seamStart;
     return I360B_SUCCESS;
@@ -510,6 +485,87 @@ int Plan::set_precision(int mode, cudaStream_t s)
     return I360B_SUCCESS;
 }
 
+void Plan::balanced_chains()
+{
+    tileChain.assign(nTiles, 0);
+    if (nChains < 2) return;
+    std::vector<int> order(nTiles);
+    for (int t = 0; t < nTiles; ++t) order[t] = t;
+    auto load = [&](int t) { return (double)tiles[t].w * tiles[t].h * (1 + tiles[t].numItems); };
+    std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return load(a) > load(b); });
+    double sum[kMaxChains] = {0.0, 0.0};
+    for (int t : order)
+    {
+        const int c = sum[1] < sum[0] ? 1 : 0;
+        tileChain[t] = c;
+        sum[c] += load(t);
+    }
+}
+
+int Plan::chain_lists(std::vector<int>& ints)
+{
+    ints.clear();
+    for (int c = 0; c < nChains; ++c)
+    {
+        dtRange[c].start = (int)ints.size();
+        for (int i = 0; i < nItems; ++i)
+            if (tileChain[items[i].tile] == c) ints.push_back(i);
+        dtRange[c].count = (int)ints.size() - dtRange[c].start;
+    }
+    const int seamStart = (int)ints.size();
+    for (int c = 0; c < nChains; ++c)
+    {
+        seamRange[c].start = (int)ints.size() - seamStart;
+        for (int t = 0; t < nTiles; ++t)
+            if (tileChain[t] == c && tiles[t].numItems >= 2) ints.push_back(t);
+        seamRange[c].count = (int)ints.size() - seamStart - seamRange[c].start;
+    }
+    nSeam = (int)ints.size() - seamStart;
+    return seamStart;
+}
+
+int Plan::set_chain_split(int percent, cudaStream_t s)
+{
+    if (percent < 0 || percent > 50) return fail(I360B_INVALID_PARAM, "chain split must be 0 (balanced) to 50 percent");
+    I360B_CUDA(cudaStreamSynchronize(s), "plan chain split");
+    if (nChains < 2)
+    {
+        chainSplit = 0;
+        return I360B_SUCCESS;
+    }
+    if (percent == 0)
+        balanced_chains();
+    else
+    {
+        // the seam step's cycles per tile from the last execution: the
+        // slowest seams first, in the first chain
+        std::vector<unsigned long long> cyc(nTiles);
+        I360B_CUDA(cudaMemcpy(cyc.data(), dSeamTile, nTiles * sizeof(unsigned long long), cudaMemcpyDeviceToHost),
+                   "plan chain split");
+        bool any = false;
+        for (unsigned long long v : cyc) any = any || v != 0;
+        if (!any) return fail(I360B_INVALID_PARAM, "chain split by seam time needs an execution of the plan first");
+        std::vector<int> order(nTiles);
+        for (int t = 0; t < nTiles; ++t) order[t] = t;
+        std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return cyc[a] > cyc[b]; });
+        const int n0 = std::max(1, std::min(nTiles - 1, (nTiles * percent + 50) / 100));
+        tileChain.assign(nTiles, 1);
+        for (int k = 0; k < n0; ++k) tileChain[order[k]] = 0;
+    }
+    std::vector<int> ints;
+    const int seamStart = chain_lists(ints);
+    std::vector<Unit> units;
+    make_units(bandRows, units);
+    if ((int)units.size() > unitCap) return fail(I360B_INVALID_PARAM, "work list exceeds its capacity");
+    I360B_CUDA(cudaMemcpy(dInts, ints.data(), ints.size() * sizeof(int), cudaMemcpyHostToDevice), "plan chain split");
+    I360B_CUDA(cudaMemcpy(dUnits, units.data(), units.size() * sizeof(Unit), cudaMemcpyHostToDevice),
+               "plan chain split");
+    seamList = dInts + seamStart;
+    chainSplit = percent;
+    drop_graphs();
+    return I360B_SUCCESS;
+}
+
 int Plan::set_chain_lag(int stage, cudaStream_t s)
 {
     if (stage < -1 || stage >= kStages - 1) return fail(I360B_INVALID_PARAM, "chain stagger must be -1 or a stage 0-8");
@@ -600,7 +656,7 @@ int Plan::enqueue_warp(cudaStream_t s)
 
 int Plan::enqueue_chain(int c, int first, int last, cudaStream_t s)
 {
-    BlendArgs a{dItems, dTiles, dError, dSeamCycles, bandRows, spinLimit, storage16};
+    BlendArgs a{dItems, dTiles, dError, dSeamCycles, dSeamTile, bandRows, spinLimit, storage16};
     const Range* L = &lists[(size_t)c * kListsPerChain];
     const bool base2 = fusedLevels == 2, fine = fusedLevels > 0;
     const int lo = fine ? 2 : 1;        // lowest level of the materialised blend and collapse
@@ -1105,11 +1161,18 @@ extern "C" int i360b_render_plan_autotune(i360b_render_plan* plan, void* stream,
     int bestR = P.bandRows, bestS = P.dtSlots, bestF = P.fusedLevels, bestW = P.warpShape;
     float best = INFINITY;
     int rc = I360B_SUCCESS;
+    // One trial: a warm-up run (which also captures the graphs), then two
+    // timed runs, each in the form that lets a caller refill the frames early:
+    // stage 0, then stages 1-9 (execute_stages).
+    auto run = [&]() -> int {
+        int r = P.execute_range(s, 0, 0);
+        return r == I360B_SUCCESS ? P.execute_range(s, 1, kStages - 1) : r;
+    };
     auto trial = [&](float& ms) -> int {
-        int r = P.execute(s, true);  // capture + warm-up
+        int r = run();
         if (r != I360B_SUCCESS) return r;
         cudaEventRecord(e0, s);
-        for (int k = 0; k < 2 && r == I360B_SUCCESS; ++k) r = P.execute(s, true);
+        for (int k = 0; k < 2 && r == I360B_SUCCESS; ++k) r = run();
         cudaEventRecord(e1, s);
         if (r == I360B_SUCCESS) r = P.check(s);
         ms = 0.0f;
@@ -1155,11 +1218,28 @@ extern "C" int i360b_render_plan_autotune(i360b_render_plan* plan, void* stream,
             if (rc != I360B_SUCCESS) break;
         }
     }
+    // 3: chain split by seam time (two chains only), with the best of the above
+    int bestP = P.chainSplit;
+    if (rc == I360B_SUCCESS && P.nChains > 1 && (rc = P.set_tuning(bestR, bestS, s)) == I360B_SUCCESS)
+    {
+        for (int pct : {0, 10, 20, 30})
+        {
+            if ((rc = P.set_chain_split(pct, s)) != I360B_SUCCESS) break;
+            float ms;
+            if ((rc = trial(ms)) != I360B_SUCCESS) break;
+            if (ms < best)
+            {
+                best = ms;
+                bestP = pct;
+            }
+        }
+    }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
     if (rc != I360B_SUCCESS) return rc;
     I360B_TRY(P.set_warp_shape(bestW, s));
     I360B_TRY(P.set_fusion(bestF, s));
+    I360B_TRY(P.set_chain_split(bestP, s));
     I360B_TRY(P.set_tuning(bestR, bestS, s));
     if (bandRows) *bandRows = bestR;
     if (dtSlots) *dtSlots = bestS;
@@ -1173,6 +1253,22 @@ extern "C" int i360b_render_plan_set_chain_lag(i360b_render_plan* plan, int stag
     if (!plan) return fail(I360B_INVALID_PARAM, "Null plan.");
     I360B_TRY(ensure_ready());
     return plan->plan.set_chain_lag(stage, static_cast<cudaStream_t>(stream));
+}
+
+extern "C" int i360b_render_plan_set_chain_split(i360b_render_plan* plan, int percent, void* stream)
+{
+    clear_error();
+    if (!plan) return fail(I360B_INVALID_PARAM, "Null plan.");
+    I360B_TRY(ensure_ready());
+    return plan->plan.set_chain_split(percent, static_cast<cudaStream_t>(stream));
+}
+
+extern "C" int i360b_render_plan_get_chain_split(i360b_render_plan* plan, int* percent)
+{
+    clear_error();
+    if (!plan || !percent) return fail(I360B_INVALID_PARAM, "Null pointer argument.");
+    *percent = plan->plan.chainSplit;
+    return I360B_SUCCESS;
 }
 
 extern "C" int i360b_render_plan_get_chain_lag(i360b_render_plan* plan, int* stage)

@@ -88,6 +88,7 @@ struct Plan
     TileDev* dTiles = nullptr;
     int* dError = nullptr;
     unsigned long long* dSeamCycles = nullptr;
+    unsigned long long* dSeamTile = nullptr;  // seam cycles per tile, last execution
     int* hostErr = nullptr;
     std::vector<SubTile> subTiles;  // built on first learned render
     std::vector<float> itemEdges;   // 16 per item (ItemSpec::edges)
@@ -110,6 +111,12 @@ struct Plan
     // full-GPU stages instead of beside its own seam search.  -1: both
     // chains start together.  Ordering only: the render is the same.
     int chainLag = -1;
+    // Chain split: 0 = two chains of about equal work (area x contributors);
+    // p > 0 = the p percent of tiles whose seam step took longest in the
+    // last execution form the first chain, so their seam searches (a CTA per
+    // tile, sequential over lines) start early and run beside the second
+    // chain's full-GPU stages instead of deciding the end of one stage.
+    int chainSplit = 0;
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t graphExec = nullptr;
 
@@ -151,6 +158,12 @@ struct Plan
     int set_warp_shape(int shape, cudaStream_t s);
     // Sets the chain stagger (-1 or a stage 0-8); recaptures on next execute.
     int set_chain_lag(int stage, cudaStream_t s);
+    // Splits the tiles into the chains (see chainSplit); remakes the lists.
+    int set_chain_split(int percent, cudaStream_t s);
+    void balanced_chains();
+    // The chamfer item and seam tile lists per chain into `ints`; returns
+    // where the seam tiles start.
+    int chain_lists(std::vector<int>& ints);
     // Changes the bounded-wait limit; the next execute recaptures the graph.
     int set_wait_limit(long long cycles, cudaStream_t s);
     void drop_graphs();

@@ -401,12 +401,16 @@ I360B_API int i360b_render_plan_stats(i360b_render_plan* plan, void* stream, i36
  * whose split depends on the level-fusion depth).  Synchronous. */
 I360B_API int i360b_render_plan_profile(i360b_render_plan* plan, void* stream, float* stageMs, int maxStages);
 I360B_API const char* i360b_render_stage_name(int stage);
-/* Autotuner: times the plan's own execute (two runs after a warm-up, CUDA
- * events on `stream`), first for both tile-warp forms and level-fusion
+/* Autotuner: times the plan's own render (two runs after a warm-up, CUDA
+ * events on `stream`; each run as stage 0 then stages 1-9, the form
+ * i360b_render_plan_execute_stages offers for early frame refills), first
+ * for both tile-warp forms and level-fusion
  * depths, then with the faster pair for every band-unit height of the
  * per-pixel kernels (8, 16, 32, 64 rows) and every ring depth of the chamfer
- * transform that fits (2 to 4 row groups), and keeps the fastest (read the
- * fusion depth and warp form back with i360b_render_plan_get_tuning).  The output of every
+ * transform that fits (2 to 4 row groups), then the chain split, and keeps
+ * the fastest (read the fusion depth and warp form back with
+ * i360b_render_plan_get_tuning, the split with
+ * i360b_render_plan_get_chain_split).  The output of every
  * setting is identical (the settings only partition the same work), so
  * tuning never changes results.  The chosen values and the best time of one
  * execute are returned when the pointers are non-null.  Synchronous; the
@@ -440,6 +444,19 @@ I360B_API int i360b_render_plan_set_tuning(i360b_render_plan* plan, int bandRows
  * Synchronous on `stream`; the next execute recaptures the plan's graph.
  * No reference counterpart. */
 I360B_API int i360b_render_plan_set_chain_lag(i360b_render_plan* plan, int stage, void* stream);
+/* Chain split.  0: the two chains carry about equal work (area x
+ * contributors), the default.  p in 1..50: the p percent of tiles whose seam
+ * step took longest in the plan's last execution (the seam search runs one
+ * CTA per tile, sequentially over contested lines, so its slowest tile sets
+ * the stage's length while most SMs are free) form the first chain, the rest
+ * the second: the slow seam searches start early and run beside the other
+ * chain's full-GPU stages.  INVALID_PARAM for p outside 0..50, or for p > 0
+ * before the plan has executed once.  Ordering only: every setting renders
+ * the same bits.  The autotuner tries 0, 10, 20 and 30.  Synchronous on
+ * `stream`; the next execute recaptures the plan's graph.  No reference
+ * counterpart. */
+I360B_API int i360b_render_plan_set_chain_split(i360b_render_plan* plan, int percent, void* stream);
+I360B_API int i360b_render_plan_get_chain_split(i360b_render_plan* plan, int* percent);
 I360B_API int i360b_render_plan_get_chain_lag(i360b_render_plan* plan, int* stage);
 /* Precision of the render's stored pyramid levels.  EXACT keeps them in
  * FP32 and renders the CPU backend's output bit for bit.  FP16 is the native

@@ -113,6 +113,7 @@ def test_autotuner_picks_fusion_depth_without_changing_bits(backend, oracle_c):
     plan, outs = _plan(dev, cfg, pano.to_canvas, gains, pano.tiles, 6)
     inv = np.stack([synth.inverse_homography_f32(H) for H in pano.to_canvas])
     _, ref = oracle_c.render_tiles(4, host, inv, gains, pano.tiles, 6)
+    assert plan.set_chain_split(10) == ComputeResult.INVALID_PARAM  # no seam times before a first execution
     tuned = plan.autotune()
     assert tuned["fused_levels"] in (0, 1, 2) and tuned["band_rows"] in (8, 16, 32, 64) and tuned["warp_shape"] in (0, 1)
     assert tuned["chain_lag"] == -1
@@ -139,4 +140,19 @@ def test_autotuner_picks_fusion_depth_without_changing_bits(backend, oracle_c):
                 assert np.array_equal(_host(o), r), (lag, split)
     assert plan.set_chain_lag(9) == ComputeResult.INVALID_PARAM
     assert plan.set_chain_lag(-2) == ComputeResult.INVALID_PARAM
+    assert plan.set_chain_lag(-1) == ComputeResult.SUCCESS
+    # the chain split by seam time also orders work only
+    assert tuned["chain_split"] in (0, 10, 20, 30)
+    for pct in (0, 1, 30, 50):
+        assert plan.set_chain_split(pct) == ComputeResult.SUCCESS
+        assert plan.chain_split() == pct
+        for o in outs:
+            o.fill_(-1)
+        assert plan.execute_stages(0, 0) == ComputeResult.SUCCESS
+        assert plan.execute_stages(1, 9) == ComputeResult.SUCCESS
+        assert plan.wait() == ComputeResult.SUCCESS
+        for o, r in zip(outs, ref):
+            assert np.array_equal(_host(o), r), pct
+    assert plan.set_chain_split(51) == ComputeResult.INVALID_PARAM
+    assert plan.set_chain_split(-1) == ComputeResult.INVALID_PARAM
     plan.close()
