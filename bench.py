@@ -209,6 +209,16 @@ def _sum_over_ranks(v, world, device):
     return int(t.item())
 
 
+def _seam_tile_ms(cyc, clocks):
+    mhz = clocks.get("sm_mhz") or 1965.0
+    ms = cyc[cyc > 0] / (mhz * 1e3)
+    if not len(ms):
+        return None
+    return {"tiles": int(len(ms)), "max": round(float(ms[0]), 3), "p90": round(float(np.percentile(ms, 90)), 3),
+            "median": round(float(np.median(ms)), 3), "sum": round(float(ms.sum()), 2),
+            "slowest": [round(float(v), 3) for v in ms[:12]]}
+
+
 def stage_bytes(stats, S, fused_levels=2):
     """Algorithmic bytes per stage: the bytes each stage must move over the
     workload's tiles and contributors (item pixels, covered pixels, pyramid
@@ -302,6 +312,7 @@ def run_ours(args, rank, world, local_rank):
     torch.cuda.synchronize()
     stats = plan.stats(sp)
     stages = plan.profile(sp)
+    seam_cyc = np.sort(plan.seam_tile_cycles(sp).astype(np.float64))[::-1]
     # demosaic stage timed alone with events on the launching stream
     ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
     be, (black, cm, rc, filt) = S["be"], S["demosaic"]
@@ -405,6 +416,10 @@ def run_ours(args, rank, world, local_rank):
         # execution of the plan since it was built (autotuning included).
         "seam_phase_cycles_cumulative": stats["seamPhaseCycles"],
         "clocks": clk.summary(),
+        # the seam step's SM cycles per tile (last execution), slowest first,
+        # as ms at the sampled SM clock: the stage lasts as long as its
+        # slowest tile, which the chain split schedules first
+        "seam_tile_ms": _seam_tile_ms(seam_cyc, clk.summary()),
         "e2e": e2e,
     }
     if shard_loads is not None:

@@ -101,6 +101,7 @@ def load_library(path: str = LIB_PATH):
     L.i360b_render_plan_get_chain_lag.argtypes = [vp, ct.POINTER(i)]
     L.i360b_render_plan_set_chain_split.argtypes = [vp, i, vp]
     L.i360b_render_plan_get_chain_split.argtypes = [vp, ct.POINTER(i)]
+    L.i360b_render_plan_seam_tile_cycles.argtypes = [vp, ct.POINTER(ct.c_ulonglong), i, vp]
     L.i360b_render_plan_wait.argtypes = [vp, vp]
     L.i360b_render_plan_destroy.argtypes = [vp]
     L.i360b_render_plan_stats.argtypes = [vp, vp, ct.POINTER(RenderStats)]
@@ -506,6 +507,7 @@ class RenderPlan:
             tl[i].dOut = out
             contrib.extend(int(c) for c in cs)
         carr = (ct.c_int * max(1, len(contrib)))(*contrib)
+        self.num_tiles = len(tiles)
         self._h = ct.c_void_p()
         rc = self.lib.i360b_render_plan_create(fr, len(frames), tl, len(tiles), carr, num_bands, coord_mode,
                                                ct.byref(self._h))
@@ -552,6 +554,14 @@ class RenderPlan:
         v = ct.c_int()
         self.lib.i360b_render_plan_get_chain_split(self._h, ct.byref(v))
         return v.value
+
+    def seam_tile_cycles(self, stream: int = 0) -> np.ndarray:
+        """SM cycles of each tile's seam step in the last execution."""
+        out = (ct.c_ulonglong * max(1, self.num_tiles))()
+        rc = self.lib.i360b_render_plan_seam_tile_cycles(self._h, out, self.num_tiles, stream or None)
+        if rc != 0:
+            raise RuntimeError(self.lib.i360b_get_last_error().decode())
+        return np.array(out[:self.num_tiles], dtype=np.uint64)
 
     def set_chain_split(self, percent: int, stream: int = 0) -> ComputeResult:
         return ComputeResult(self.lib.i360b_render_plan_set_chain_split(self._h, int(percent), stream or None))

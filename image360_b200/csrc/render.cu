@@ -1263,6 +1263,22 @@ extern "C" int i360b_render_plan_set_chain_split(i360b_render_plan* plan, int pe
     return plan->plan.set_chain_split(percent, static_cast<cudaStream_t>(stream));
 }
 
+extern "C" int i360b_render_plan_seam_tile_cycles(i360b_render_plan* plan, unsigned long long* cycles, int maxTiles,
+                                                  void* stream)
+{
+    clear_error();
+    if (!plan || (!cycles && maxTiles > 0)) return fail(I360B_INVALID_PARAM, "Null pointer argument.");
+    I360B_TRY(ensure_ready());
+    Plan& P = plan->plan;
+    const int n = std::min(maxTiles, P.nTiles);
+    if (n <= 0) return I360B_SUCCESS;
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    I360B_CUDA(cudaMemcpyAsync(cycles, P.dSeamTile, n * sizeof(unsigned long long), cudaMemcpyDeviceToHost, s),
+               "seam tile cycles");
+    I360B_CUDA(cudaStreamSynchronize(s), "seam tile cycles");
+    return I360B_SUCCESS;
+}
+
 extern "C" int i360b_render_plan_get_chain_split(i360b_render_plan* plan, int* percent)
 {
     clear_error();

@@ -457,6 +457,11 @@ I360B_API int i360b_render_plan_set_chain_lag(i360b_render_plan* plan, int stage
  * counterpart. */
 I360B_API int i360b_render_plan_set_chain_split(i360b_render_plan* plan, int percent, void* stream);
 I360B_API int i360b_render_plan_get_chain_split(i360b_render_plan* plan, int* percent);
+/* SM cycles each tile's seam step took in the plan's last execution (0 for
+ * tiles with fewer than two contributors or before a first execution), for
+ * the first maxTiles tiles in plan order.  Synchronous on `stream`. */
+I360B_API int i360b_render_plan_seam_tile_cycles(i360b_render_plan* plan, unsigned long long* cycles, int maxTiles,
+                                                 void* stream);
 I360B_API int i360b_render_plan_get_chain_lag(i360b_render_plan* plan, int* stage);
 /* Precision of the render's stored pyramid levels.  EXACT keeps them in
  * FP32 and renders the CPU backend's output bit for bit.  FP16 is the native

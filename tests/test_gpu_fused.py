@@ -153,6 +153,9 @@ def test_autotuner_picks_fusion_depth_without_changing_bits(backend, oracle_c):
         assert plan.wait() == ComputeResult.SUCCESS
         for o, r in zip(outs, ref):
             assert np.array_equal(_host(o), r), pct
+    cyc = plan.seam_tile_cycles()
+    assert len(cyc) == len(pano.tiles)
+    assert all((c > 0) == (len(t[4]) >= 2) for c, t in zip(cyc, pano.tiles))
     assert plan.set_chain_split(51) == ComputeResult.INVALID_PARAM
     assert plan.set_chain_split(-1) == ComputeResult.INVALID_PARAM
     plan.close()
