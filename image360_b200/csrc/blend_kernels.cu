@@ -1522,6 +1522,25 @@ __device__ __forceinline__ float4 nd_at(const float4* nd, size_t q, int half)
     return make_float4(a.x * 256.0f, a.y * 256.0f, b.x * 256.0f, b.y);
 }
 
+// Levels >= 2 of a contributor's pyramid hold, once the band blend of their
+// level has run, the hole-filled Gaussian G = num * (1/den) in place of num
+// (exact mode): the blend of the level below and the fused fine kernel read
+// Up(G) taps, each level-l+1 value about sixteen times, and the reciprocal is
+// then computed once per value instead of once per tap.  The stored G is the
+// value gauss_of would compute, so the taps are bit-identical.  FP16 storage
+// keeps (num, den) and computes G at every read.
+__device__ __forceinline__ bool g_stored(int level, int half) { return level >= 2 && !half; }
+
+__device__ __forceinline__ float3 g_at(const float4* nd, size_t q, int level, int half)
+{
+    if (g_stored(level, half))
+    {
+        const float4 v = __ldg(nd + q);
+        return make_float3(v.x, v.y, v.z);
+    }
+    return gauss_of(nd_at(nd, q, half));
+}
+
 __device__ __forceinline__ float wg_at(const float* wg, size_t q, int half)
 {
     if (!half) return __ldg(wg + q);
@@ -1840,13 +1859,14 @@ __device__ __noinline__ void blend_pixel(const TileDev& T, const ItemCache& C, i
         if (x < B.x || x > B.z || y < B.y || y > B.w) continue;  // weight 0: the term is +-0
         float wv = wg_at(C.wg[k], p, half);
         float3 g = gauss_of(nd_at(C.nd[k], p, half));
+        if (g_stored(level, half)) const_cast<float4*>(C.nd[k])[p] = make_float4(g.x, g.y, g.z, 0.0f);
         if (!top)
         {
             const size_t up = T.loff[level + 1];
-            float3 a00 = gauss_of(nd_at(C.nd[k], up + (size_t)c.y0 * uw + c.x0, half));
-            float3 a10 = gauss_of(nd_at(C.nd[k], up + (size_t)c.y0 * uw + c.x1, half));
-            float3 a01 = gauss_of(nd_at(C.nd[k], up + (size_t)c.y1 * uw + c.x0, half));
-            float3 a11 = gauss_of(nd_at(C.nd[k], up + (size_t)c.y1 * uw + c.x1, half));
+            float3 a00 = g_at(C.nd[k], up + (size_t)c.y0 * uw + c.x0, level + 1, half);
+            float3 a10 = g_at(C.nd[k], up + (size_t)c.y0 * uw + c.x1, level + 1, half);
+            float3 a01 = g_at(C.nd[k], up + (size_t)c.y1 * uw + c.x0, level + 1, half);
+            float3 a11 = g_at(C.nd[k], up + (size_t)c.y1 * uw + c.x1, level + 1, half);
             g.x = fsub(g.x, up_mix(a00.x, a10.x, a01.x, a11.x, c.wx, c.wy));
             g.y = fsub(g.y, up_mix(a00.y, a10.y, a01.y, a11.y, c.wx, c.wy));
             g.z = fsub(g.z, up_mix(a00.z, a10.z, a01.z, a11.z, c.wx, c.wy));
@@ -1895,11 +1915,11 @@ __device__ __forceinline__ void blend_quad(const TileDev& T, const ItemCache& C,
         const float4* nd = C.nd[k];
         const size_t up = T.loff[level + 1];
         int cur = x0[0];
-        float3 L0 = gauss_of(nd_at(nd, up + (size_t)y0 * uw + cur, half)),
-               L1 = gauss_of(nd_at(nd, up + (size_t)y1 * uw + cur, half));
+        float3 L0 = g_at(nd, up + (size_t)y0 * uw + cur, level + 1, half),
+               L1 = g_at(nd, up + (size_t)y1 * uw + cur, level + 1, half);
         int nx = min(cur + 1, uw - 1);
-        float3 R0 = gauss_of(nd_at(nd, up + (size_t)y0 * uw + nx, half)),
-               R1 = gauss_of(nd_at(nd, up + (size_t)y1 * uw + nx, half));
+        float3 R0 = g_at(nd, up + (size_t)y0 * uw + nx, level + 1, half),
+               R1 = g_at(nd, up + (size_t)y1 * uw + nx, level + 1, half);
 #pragma unroll
         for (int i = 0; i < 4; ++i)
         {
@@ -1909,11 +1929,12 @@ __device__ __forceinline__ void blend_quad(const TileDev& T, const ItemCache& C,
                 L0 = R0;
                 L1 = R1;
                 nx = min(cur + 1, uw - 1);
-                R0 = gauss_of(nd_at(nd, up + (size_t)y0 * uw + nx, half));
-                R1 = gauss_of(nd_at(nd, up + (size_t)y1 * uw + nx, half));
+                R0 = g_at(nd, up + (size_t)y0 * uw + nx, level + 1, half);
+                R1 = g_at(nd, up + (size_t)y1 * uw + nx, level + 1, half);
             }
             const float wv = wg_at(C.wg[k], p + i, half);
             float3 g = gauss_of(nd_at(nd, p + i, half));
+            if (g_stored(level, half)) const_cast<float4*>(nd)[p + i] = make_float4(g.x, g.y, g.z, 0.0f);
             g.x = fsub(g.x, up_mix(L0.x, R0.x, L1.x, R1.x, wx[i], wy));
             g.y = fsub(g.y, up_mix(L0.y, R0.y, L1.y, R1.y, wx[i], wy));
             g.z = fsub(g.z, up_mix(L0.z, R0.z, L1.z, R1.z, wx[i], wy));
@@ -2697,7 +2718,7 @@ __global__ void __launch_bounds__(256) k_fine(BlendArgs a, const Unit* __restric
                 for (int idx = tid; idx < nP * nQ; idx += blockDim.x)
                 {
                     const int r = idx / nP, c = idx - r * nP;
-                    const float3 g = gauss_of(nd_at(S.nd[k], g2 + (size_t)(Q0 + r) * lw2 + P0 + c, a.half));
+                    const float3 g = g_at(S.nd[k], g2 + (size_t)(Q0 + r) * lw2 + P0 + c, 2, a.half);
                     S.g2[0][r][c] = g.x;
                     S.g2[1][r][c] = g.y;
                     S.g2[2][r][c] = g.z;

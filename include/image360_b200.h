@@ -495,7 +495,11 @@ I360B_API int i360b_render_plan_write_tiff16(i360b_render_plan* plan, const char
  * frames' RGB48 buffers; 1-9 the seam blend) as a CUDA graph of their own
  * (captured on first use).  Running stage 0, then 1-9, is the same render as
  * i360b_render_plan_execute; a caller that refills the frame buffers for the
- * next render may do so as soon as stage 0 has completed. */
+ * next render may do so as soon as stage 0 has completed.  Stages run in
+ * order and consume what the stages before them wrote: in particular the
+ * band blend (stage 7) turns the stored coarse pyramid levels into their
+ * Gaussian values in place, so a range starting after stage 5 must follow a
+ * run of the stages before it. */
 I360B_API int i360b_render_plan_execute_stages(i360b_render_plan* plan, int firstStage, int lastStage, void* stream);
 
 /* Sets how long each bounded device wait of the plan's kernels may last, in
