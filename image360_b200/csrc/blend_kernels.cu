@@ -1522,23 +1522,39 @@ __device__ __forceinline__ float4 nd_at(const float4* nd, size_t q, int half)
     return make_float4(a.x * 256.0f, a.y * 256.0f, b.x * 256.0f, b.y);
 }
 
-// Levels >= 2 of a contributor's pyramid hold, once the band blend of their
-// level has run, the hole-filled Gaussian G = num * (1/den) in place of num
-// (exact mode): the blend of the level below and the fused fine kernel read
-// Up(G) taps, each level-l+1 value about sixteen times, and the reciprocal is
-// then computed once per value instead of once per tap.  The stored G is the
-// value gauss_of would compute, so the taps are bit-identical.  FP16 storage
-// keeps (num, den) and computes G at every read.
-__device__ __forceinline__ bool g_stored(int level, int half) { return level >= 2 && !half; }
+// The levels gmin and above of a contributor's pyramid hold, once the band
+// blend of their level has run, the hole-filled Gaussian G = num * (1/den) in
+// place of num: the blend of the level below, the level-0 output (level 1)
+// and the fused fine kernel (level 2) read Up(G) taps, each value about
+// sixteen times, and the reciprocal is then computed once per value instead
+// of once per tap.  The stored G is the value gauss_of would compute, so the
+// taps are bit-identical in the exact mode (with FP16 storage G / 256 is
+// stored as FP16, like num / 256 before).  gmin is 1 with every level
+// materialised (the level-1 blend runs before the output) and 2 with the
+// fused levels (level 1 has no blend of its own).
+__device__ __forceinline__ bool g_stored(int level, int gmin) { return level >= gmin; }
 
-__device__ __forceinline__ float3 g_at(const float4* nd, size_t q, int level, int half)
+__device__ __forceinline__ float3 g_at(const float4* nd, size_t q, int level, int gmin, int half)
 {
-    if (g_stored(level, half))
+    if (g_stored(level, gmin))
     {
-        const float4 v = __ldg(nd + q);
+        const float4 v = nd_at(nd, q, half);
         return make_float3(v.x, v.y, v.z);
     }
     return gauss_of(nd_at(nd, q, half));
+}
+
+__device__ __forceinline__ void g_store(const float4* nd, size_t q, float3 g, int half)
+{
+    if (!half)
+    {
+        const_cast<float4*>(nd)[q] = make_float4(g.x, g.y, g.z, 0.0f);
+        return;
+    }
+    const __half2 a = __floats2half2_rn(g.x * (1.0f / 256.0f), g.y * (1.0f / 256.0f));
+    const __half2 b = __floats2half2_rn(g.z * (1.0f / 256.0f), 0.0f);
+    reinterpret_cast<uint2*>(const_cast<float4*>(nd))[q] =
+        make_uint2(*reinterpret_cast<const uint32_t*>(&a), *reinterpret_cast<const uint32_t*>(&b));
 }
 
 __device__ __forceinline__ float wg_at(const float* wg, size_t q, int half)
@@ -1843,7 +1859,8 @@ __global__ void __launch_bounds__(256, 4) k_down0s(BlendArgs a, const Unit* __re
 }
 
 // One pixel of a blended band (the general path).
-__device__ __noinline__ void blend_pixel(const TileDev& T, const ItemCache& C, int level, int K, long long pl, int half)
+__device__ __noinline__ void blend_pixel(const TileDev& T, const ItemCache& C, int level, int K, long long pl, int half,
+                                        int gmin)
 {
     const int lw = T.lw[level];
     const bool top = level == T.bands - 1;
@@ -1859,14 +1876,14 @@ __device__ __noinline__ void blend_pixel(const TileDev& T, const ItemCache& C, i
         if (x < B.x || x > B.z || y < B.y || y > B.w) continue;  // weight 0: the term is +-0
         float wv = wg_at(C.wg[k], p, half);
         float3 g = gauss_of(nd_at(C.nd[k], p, half));
-        if (g_stored(level, half)) const_cast<float4*>(C.nd[k])[p] = make_float4(g.x, g.y, g.z, 0.0f);
+        if (g_stored(level, gmin)) g_store(C.nd[k], p, g, half);
         if (!top)
         {
             const size_t up = T.loff[level + 1];
-            float3 a00 = g_at(C.nd[k], up + (size_t)c.y0 * uw + c.x0, level + 1, half);
-            float3 a10 = g_at(C.nd[k], up + (size_t)c.y0 * uw + c.x1, level + 1, half);
-            float3 a01 = g_at(C.nd[k], up + (size_t)c.y1 * uw + c.x0, level + 1, half);
-            float3 a11 = g_at(C.nd[k], up + (size_t)c.y1 * uw + c.x1, level + 1, half);
+            float3 a00 = g_at(C.nd[k], up + (size_t)c.y0 * uw + c.x0, level + 1, gmin, half);
+            float3 a10 = g_at(C.nd[k], up + (size_t)c.y0 * uw + c.x1, level + 1, gmin, half);
+            float3 a01 = g_at(C.nd[k], up + (size_t)c.y1 * uw + c.x0, level + 1, gmin, half);
+            float3 a11 = g_at(C.nd[k], up + (size_t)c.y1 * uw + c.x1, level + 1, gmin, half);
             g.x = fsub(g.x, up_mix(a00.x, a10.x, a01.x, a11.x, c.wx, c.wy));
             g.y = fsub(g.y, up_mix(a00.y, a10.y, a01.y, a11.y, c.wx, c.wy));
             g.z = fsub(g.z, up_mix(a00.z, a10.z, a01.z, a11.z, c.wx, c.wy));
@@ -1887,7 +1904,7 @@ __device__ __noinline__ void blend_pixel(const TileDev& T, const ItemCache& C, i
 // texels and reciprocals computed once per contributor; every pixel's sum
 // still runs over the contributors in index order with its own weights.
 __device__ __forceinline__ void blend_quad(const TileDev& T, const ItemCache& C, int level, int K, long long pl,
-                                           int y, int x, int half)
+                                           int y, int x, int half, int gmin)
 {
     const int uw = T.lw[level + 1], uh = T.lh[level + 1];
     int x0[4];
@@ -1915,11 +1932,11 @@ __device__ __forceinline__ void blend_quad(const TileDev& T, const ItemCache& C,
         const float4* nd = C.nd[k];
         const size_t up = T.loff[level + 1];
         int cur = x0[0];
-        float3 L0 = g_at(nd, up + (size_t)y0 * uw + cur, level + 1, half),
-               L1 = g_at(nd, up + (size_t)y1 * uw + cur, level + 1, half);
+        float3 L0 = g_at(nd, up + (size_t)y0 * uw + cur, level + 1, gmin, half),
+               L1 = g_at(nd, up + (size_t)y1 * uw + cur, level + 1, gmin, half);
         int nx = min(cur + 1, uw - 1);
-        float3 R0 = g_at(nd, up + (size_t)y0 * uw + nx, level + 1, half),
-               R1 = g_at(nd, up + (size_t)y1 * uw + nx, level + 1, half);
+        float3 R0 = g_at(nd, up + (size_t)y0 * uw + nx, level + 1, gmin, half),
+               R1 = g_at(nd, up + (size_t)y1 * uw + nx, level + 1, gmin, half);
 #pragma unroll
         for (int i = 0; i < 4; ++i)
         {
@@ -1929,12 +1946,12 @@ __device__ __forceinline__ void blend_quad(const TileDev& T, const ItemCache& C,
                 L0 = R0;
                 L1 = R1;
                 nx = min(cur + 1, uw - 1);
-                R0 = g_at(nd, up + (size_t)y0 * uw + nx, level + 1, half);
-                R1 = g_at(nd, up + (size_t)y1 * uw + nx, level + 1, half);
+                R0 = g_at(nd, up + (size_t)y0 * uw + nx, level + 1, gmin, half);
+                R1 = g_at(nd, up + (size_t)y1 * uw + nx, level + 1, gmin, half);
             }
             const float wv = wg_at(C.wg[k], p + i, half);
             float3 g = gauss_of(nd_at(nd, p + i, half));
-            if (g_stored(level, half)) const_cast<float4*>(nd)[p + i] = make_float4(g.x, g.y, g.z, 0.0f);
+            if (g_stored(level, gmin)) g_store(nd, p + i, g, half);
             g.x = fsub(g.x, up_mix(L0.x, R0.x, L1.x, R1.x, wx[i], wy));
             g.y = fsub(g.y, up_mix(L0.y, R0.y, L1.y, R1.y, wx[i], wy));
             g.z = fsub(g.z, up_mix(L0.z, R0.z, L1.z, R1.z, wx[i], wy));
@@ -1992,10 +2009,10 @@ __global__ void __launch_bounds__(256, 3) k_blend_level(BlendArgs a, const Unit*
         const int cnt = min(4, lw - x);
         if (!top && cnt == 4)
         {
-            blend_quad(T, C, level, K, pl, y, x, a.half);
+            blend_quad(T, C, level, K, pl, y, x, a.half, a.gmin);
             continue;
         }
-        for (int i = 0; i < cnt; ++i) blend_pixel(T, C, level, K, pl + i, a.half);
+        for (int i = 0; i < cnt; ++i) blend_pixel(T, C, level, K, pl + i, a.half, a.gmin);
     }
 }
 
@@ -2045,7 +2062,7 @@ __device__ __forceinline__ void final_store(unsigned short* o, const float* r)
 
 // One output pixel (the general path).
 __device__ __noinline__ void final_pixel(const TileDev& T, const ItemCache& C, const float* rc, int uw, int uh,
-                                            long long p, int own, int half)
+                                            long long p, int own, int half, int gmin)
 {
     unsigned short* o = T.out + p * 3;
     if (own < 0)
@@ -2062,10 +2079,10 @@ __device__ __noinline__ void final_pixel(const TileDev& T, const ItemCache& C, c
         const UpCoef c = up_coef_s(T.usx[0], T.usy[0], uw, uh, x, y);
         const float4* nd = C.nd[own];
         const size_t l1 = T.loff[1];
-        const float3 a00 = gauss_of(nd_at(nd, l1 + (size_t)c.y0 * uw + c.x0, half));
-        const float3 a10 = gauss_of(nd_at(nd, l1 + (size_t)c.y0 * uw + c.x1, half));
-        const float3 a01 = gauss_of(nd_at(nd, l1 + (size_t)c.y1 * uw + c.x0, half));
-        const float3 a11 = gauss_of(nd_at(nd, l1 + (size_t)c.y1 * uw + c.x1, half));
+        const float3 a00 = g_at(nd, l1 + (size_t)c.y0 * uw + c.x0, 1, gmin, half);
+        const float3 a10 = g_at(nd, l1 + (size_t)c.y0 * uw + c.x1, 1, gmin, half);
+        const float3 a01 = g_at(nd, l1 + (size_t)c.y1 * uw + c.x0, 1, gmin, half);
+        const float3 a11 = g_at(nd, l1 + (size_t)c.y1 * uw + c.x1, 1, gmin, half);
         const float lap[3] = {fsub(r[0], up_mix(a00.x, a10.x, a01.x, a11.x, c.wx, c.wy)),
                               fsub(r[1], up_mix(a00.y, a10.y, a01.y, a11.y, c.wx, c.wy)),
                               fsub(r[2], up_mix(a00.z, a10.z, a01.z, a11.z, c.wx, c.wy))};
@@ -2090,12 +2107,12 @@ struct TapColumn
 };
 
 __device__ __forceinline__ TapColumn tap_column(const float4* nd, size_t l1, const float* rc, int uw, int y0, int y1,
-                                                int col, int half)
+                                                int col, int half, int gmin)
 {
     const size_t q0 = (size_t)y0 * uw + col, q1 = (size_t)y1 * uw + col;
     TapColumn t;
-    t.g0 = gauss_of(nd_at(nd, l1 + q0, half));
-    t.g1 = gauss_of(nd_at(nd, l1 + q1, half));
+    t.g0 = g_at(nd, l1 + q0, 1, gmin, half);
+    t.g1 = g_at(nd, l1 + q1, 1, gmin, half);
     t.u0 = make_float3(__ldg(rc + q0 * 3), __ldg(rc + q0 * 3 + 1), __ldg(rc + q0 * 3 + 2));
     t.u1 = make_float3(__ldg(rc + q1 * 3), __ldg(rc + q1 * 3 + 1), __ldg(rc + q1 * 3 + 2));
     return t;
@@ -2108,15 +2125,15 @@ __device__ __forceinline__ TapColumn tap_column(const float4* nd, size_t l1, con
 // column's texels and reciprocals computed once; every pixel still combines
 // its own four taps with its own weights in the reference's order.
 __device__ __forceinline__ void final_quad(const TileDev& T, const ItemCache& C, const float* rc, int uw, int uh,
-                                           long long p, int y, int x, int own, int half)
+                                           long long p, int y, int x, int own, int half, int gmin)
 {
     const float4* g1 = C.nd[own];
     const size_t l1 = T.loff[1];
     const float sx = T.usx[0];
     UpCoef c = up_coef_s(sx, T.usy[0], uw, uh, x, y);
     int cur = c.x0;
-    TapColumn L = tap_column(g1, l1, rc, uw, c.y0, c.y1, cur, half);
-    TapColumn R = tap_column(g1, l1, rc, uw, c.y0, c.y1, c.x1, half);
+    TapColumn L = tap_column(g1, l1, rc, uw, c.y0, c.y1, cur, half, gmin);
+    TapColumn R = tap_column(g1, l1, rc, uw, c.y0, c.y1, c.x1, half, gmin);
     const unsigned short* px = C.img[own] + p * 3;
     // the quad's 12 source values: three 8-byte loads when aligned
     uint32_t pw[6];
@@ -2151,7 +2168,7 @@ __device__ __forceinline__ void final_quad(const TileDev& T, const ItemCache& C,
             {
                 cur = x0;
                 L = R;
-                R = tap_column(g1, l1, rc, uw, c.y0, c.y1, min(x0 + 1, uw - 1), half);
+                R = tap_column(g1, l1, rc, uw, c.y0, c.y1, min(x0 + 1, uw - 1), half, gmin);
             }
         }
         float r[3];
@@ -2222,12 +2239,12 @@ __global__ void __launch_bounds__(256) k_final0(BlendArgs a, const Unit* __restr
         }
         if (cnt == 4 && T.bands > 1 && own[0] >= 0 && own[1] == own[0] && own[2] == own[0] && own[3] == own[0])
         {
-            final_quad(T, C, rc, uw, uh, p, y, x, own[0], a.half);
+            final_quad(T, C, rc, uw, uh, p, y, x, own[0], a.half, a.gmin);
             continue;
         }
 #pragma unroll
         for (int i = 0; i < 4; ++i)
-            if (i < cnt) final_pixel(T, C, rc, uw, uh, p + i, own[i], a.half);
+            if (i < cnt) final_pixel(T, C, rc, uw, uh, p + i, own[i], a.half, a.gmin);
     }
 }
 
@@ -2718,7 +2735,7 @@ __global__ void __launch_bounds__(256) k_fine(BlendArgs a, const Unit* __restric
                 for (int idx = tid; idx < nP * nQ; idx += blockDim.x)
                 {
                     const int r = idx / nP, c = idx - r * nP;
-                    const float3 g = g_at(S.nd[k], g2 + (size_t)(Q0 + r) * lw2 + P0 + c, 2, a.half);
+                    const float3 g = g_at(S.nd[k], g2 + (size_t)(Q0 + r) * lw2 + P0 + c, 2, a.gmin, a.half);
                     S.g2[0][r][c] = g.x;
                     S.g2[1][r][c] = g.y;
                     S.g2[2][r][c] = g.z;

@@ -82,6 +82,7 @@ struct BlendArgs
     int bandRows;                      // rows per band unit (a multiple of 8; the plan's tuning)
     long long spinLimit;               // cycles a bounded wait may last (0: give up at the first miss)
     int half;                          // materialised pyramid levels stored as FP16 (the native mode)
+    int gmin;                          // lowest level whose band blend stores G in place of num (see g_at)
 };
 
 // Kernel launchers (blend_kernels.cu).

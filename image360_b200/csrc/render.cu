@@ -656,7 +656,9 @@ int Plan::enqueue_warp(cudaStream_t s)
 
 int Plan::enqueue_chain(int c, int first, int last, cudaStream_t s)
 {
-    BlendArgs a{dItems, dTiles, dError, dSeamCycles, dSeamTile, bandRows, spinLimit, storage16};
+    // levels whose band blend stores G in place (see g_at in blend_kernels.cu)
+    const int gmin = fusedLevels == 0 ? 1 : 2;
+    BlendArgs a{dItems, dTiles, dError, dSeamCycles, dSeamTile, bandRows, spinLimit, storage16, gmin};
     const Range* L = &lists[(size_t)c * kListsPerChain];
     const bool base2 = fusedLevels == 2, fine = fusedLevels > 0;
     const int lo = fine ? 2 : 1;        // lowest level of the materialised blend and collapse
