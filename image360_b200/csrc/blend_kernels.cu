@@ -1531,7 +1531,15 @@ __device__ __forceinline__ float4 nd_at(const float4* nd, size_t q, int half)
 // taps are bit-identical in the exact mode (with FP16 storage G / 256 is
 // stored as FP16, like num / 256 before).  gmin is 1 with every level
 // materialised (the level-1 blend runs before the output) and 2 with the
-// fused levels (level 1 has no blend of its own).
+// fused levels (level 1 has no blend of its own).  In the exact mode G is
+// stored only where the contributor's weight at that level is non-zero:
+// every reader takes Up(G) taps only for a pixel of non-zero weight one level
+// below (a blend term, or an owned level-0 pixel), each such tap has that
+// pixel in its 5-tap footprint (align-corners: |x - 2 x0| <= 2), and the
+// weight there is then a sum containing a positive product - non-zero.  A
+// tap elsewhere only enters a term of weight zero, which is +-0 for any
+// finite value.  (FP16 weights can round to zero, so that mode stores G
+// wherever the blend passes.)
 __device__ __forceinline__ bool g_stored(int level, int gmin) { return level >= gmin; }
 
 __device__ __forceinline__ float3 g_at(const float4* nd, size_t q, int level, int gmin, int half)
@@ -1875,8 +1883,11 @@ __device__ __noinline__ void blend_pixel(const TileDev& T, const ItemCache& C, i
         const int4 B = C.box[k];
         if (x < B.x || x > B.z || y < B.y || y > B.w) continue;  // weight 0: the term is +-0
         float wv = wg_at(C.wg[k], p, half);
+        const bool store = g_stored(level, gmin) && (half || wv != 0.0f);
+        if (wv == 0.0f && !store) continue;  // the term is +-0 and no reader needs G here
         float3 g = gauss_of(nd_at(C.nd[k], p, half));
-        if (g_stored(level, gmin)) g_store(C.nd[k], p, g, half);
+        if (store) g_store(C.nd[k], p, g, half);
+        if (wv == 0.0f) continue;
         if (!top)
         {
             const size_t up = T.loff[level + 1];
@@ -1925,10 +1936,15 @@ __device__ __forceinline__ void blend_quad(const TileDev& T, const ItemCache& C,
     float acc[4][3];
 #pragma unroll
     for (int i = 0; i < 4; ++i) acc[i][0] = acc[i][1] = acc[i][2] = 0.0f;
+    const bool storeAll = g_stored(level, gmin) && half;  // FP16: G stored wherever the blend passes
     for (int k = 0; k < K; ++k)
     {
         const int4 B = C.box[k];
         if (x + 3 < B.x || x > B.z || y < B.y || y > B.w) continue;  // weight 0 on the quad: terms are +-0
+        float wv[4];
+#pragma unroll
+        for (int i = 0; i < 4; ++i) wv[i] = wg_at(C.wg[k], p + i, half);
+        if (!storeAll && wv[0] == 0.0f && wv[1] == 0.0f && wv[2] == 0.0f && wv[3] == 0.0f) continue;
         const float4* nd = C.nd[k];
         const size_t up = T.loff[level + 1];
         int cur = x0[0];
@@ -1949,15 +1965,16 @@ __device__ __forceinline__ void blend_quad(const TileDev& T, const ItemCache& C,
                 R0 = g_at(nd, up + (size_t)y0 * uw + nx, level + 1, gmin, half);
                 R1 = g_at(nd, up + (size_t)y1 * uw + nx, level + 1, gmin, half);
             }
-            const float wv = wg_at(C.wg[k], p + i, half);
+            if (wv[i] == 0.0f && !storeAll) continue;
             float3 g = gauss_of(nd_at(nd, p + i, half));
             if (g_stored(level, gmin)) g_store(nd, p + i, g, half);
+            if (wv[i] == 0.0f) continue;
             g.x = fsub(g.x, up_mix(L0.x, R0.x, L1.x, R1.x, wx[i], wy));
             g.y = fsub(g.y, up_mix(L0.y, R0.y, L1.y, R1.y, wx[i], wy));
             g.z = fsub(g.z, up_mix(L0.z, R0.z, L1.z, R1.z, wx[i], wy));
-            acc[i][0] = fadd(acc[i][0], fmul(wv, g.x));
-            acc[i][1] = fadd(acc[i][1], fmul(wv, g.y));
-            acc[i][2] = fadd(acc[i][2], fmul(wv, g.z));
+            acc[i][0] = fadd(acc[i][0], fmul(wv[i], g.x));
+            acc[i][1] = fadd(acc[i][1], fmul(wv[i], g.y));
+            acc[i][2] = fadd(acc[i][2], fmul(wv[i], g.z));
         }
     }
     float* b = T.blend + p * 3;
