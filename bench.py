@@ -1282,8 +1282,8 @@ def main():
     ap.add_argument("--warp-shape", type=int, choices=[0, 1], default=None,
                     help="force the tile-warp form after autotuning")
     ap.add_argument("--chain-lag", type=int, default=None,
-                    help="force the chain stagger after autotuning (-1: chains together; L: the second chain "
-                         "starts after the first finishes stage L)")
+                    help="force the chain stagger after autotuning (-1: chains together; L: the other chains "
+                         "start after the first finishes stage L)")
     ap.add_argument("--chain-split", type=int, default=None,
                     help="force the chain split after autotuning (0: balanced; p: the p%% of tiles with the "
                          "slowest seam step in the first chain)")

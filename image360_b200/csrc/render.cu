@@ -227,8 +227,9 @@ int Plan::build(const std::vector<TileSpec>& specs, int numBands, bool renderPat
         }
     }
     nItems = (int)items.size();
-    // ---- chains: tiles split into two groups of about equal work ----------
-    nChains = nTiles >= 2 ? kMaxChains : 1;
+    // ---- chains: tiles split into groups of about equal work -------------
+    nChains = std::min(nTiles, (int)kMaxChains);
+    if (nChains < 1) nChains = 1;
     balanced_chains();
     // ---- work lists -------------------------------------------------------
     std::vector<Unit> units;
@@ -250,10 +251,13 @@ int Plan::build(const std::vector<TileSpec>& specs, int numBands, bool renderPat
     const int seamStart = chain_lists(ints);
     if (nChains > 1)
     {
-        I360B_CUDA(cudaStreamCreateWithFlags(&side, cudaStreamNonBlocking), "chain stream");
         I360B_CUDA(cudaEventCreateWithFlags(&evFork, cudaEventDisableTiming), "chain event");
-        I360B_CUDA(cudaEventCreateWithFlags(&evJoin, cudaEventDisableTiming), "chain event");
         I360B_CUDA(cudaEventCreateWithFlags(&evLag, cudaEventDisableTiming), "chain event");
+        for (int c = 1; c < nChains; ++c)
+        {
+            I360B_CUDA(cudaStreamCreateWithFlags(&side[c - 1], cudaStreamNonBlocking), "chain stream");
+            I360B_CUDA(cudaEventCreateWithFlags(&evJoin[c - 1], cudaEventDisableTiming), "chain event");
+        }
     }
     // ---- device allocation -----------------------------------------------
     size_t unitBytes = align256(std::max<size_t>(unitCap, 1) * sizeof(Unit));
@@ -493,10 +497,12 @@ void Plan::balanced_chains()
     for (int t = 0; t < nTiles; ++t) order[t] = t;
     auto load = [&](int t) { return (double)tiles[t].w * tiles[t].h * (1 + tiles[t].numItems); };
     std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return load(a) > load(b); });
-    double sum[kMaxChains] = {0.0, 0.0};
+    double sum[kMaxChains] = {};
     for (int t : order)
     {
-        const int c = sum[1] < sum[0] ? 1 : 0;
+        int c = 0;
+        for (int q = 1; q < nChains; ++q)
+            if (sum[q] < sum[c]) c = q;
         tileChain[t] = c;
         sum[c] += load(t);
     }
@@ -548,9 +554,16 @@ int Plan::set_chain_split(int percent, cudaStream_t s)
         std::vector<int> order(nTiles);
         for (int t = 0; t < nTiles; ++t) order[t] = t;
         std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return cyc[a] > cyc[b]; });
-        const int n0 = std::max(1, std::min(nTiles - 1, (nTiles * percent + 50) / 100));
-        tileChain.assign(nTiles, 1);
-        for (int k = 0; k < n0; ++k) tileChain[order[k]] = 0;
+        // chain c < nChains - 1 takes the next `percent` of the tiles in that
+        // order (at least one), the last chain the rest
+        const int per = std::max(1, (nTiles * percent + 50) / 100);
+        tileChain.assign(nTiles, nChains - 1);
+        for (int k = 0; k < nTiles; ++k)
+        {
+            const int c = k / per;
+            if (c >= nChains - 1 || nTiles - k <= 1) break;  // the last chain keeps at least one tile
+            tileChain[order[k]] = c;
+        }
     }
     std::vector<int> ints;
     const int seamStart = chain_lists(ints);
@@ -605,11 +618,14 @@ int Plan::set_wait_limit(long long cycles, cudaStream_t s)
 Plan::~Plan()
 {
     for (auto& g : rangeGraphs) cudaGraphExecDestroy(g.second);
-    if (side) cudaStreamSynchronize(side);
+    for (int c = 0; c + 1 < kMaxChains; ++c)
+    {
+        if (side[c]) cudaStreamSynchronize(side[c]);
+        if (evJoin[c]) cudaEventDestroy(evJoin[c]);
+        if (side[c]) cudaStreamDestroy(side[c]);
+    }
     if (evFork) cudaEventDestroy(evFork);
-    if (evJoin) cudaEventDestroy(evJoin);
     if (evLag) cudaEventDestroy(evLag);
-    if (side) cudaStreamDestroy(side);
     if (graphExec) cudaGraphExecDestroy(graphExec);
     if (graph) cudaGraphDestroy(graph);
     if (hostErr) cudaFreeHost(hostErr);
@@ -734,7 +750,7 @@ int Plan::enqueue_range(cudaStream_t s, int first, int last, cudaEvent_t* ev)
     if (!ev && nChains > 1)
     {
         // Stage 0's bbox reset and error flag for all items, then each chain's
-        // stages on its own stream (chain 1 forked onto `side`), joined.
+        // stages on its own stream (chains 1.. forked onto `side`), joined.
         if (first == 0)
         {
             if (nItems > 0) k_init_bbox<<<(nItems + 127) / 128, 128, 0, s>>>(dItems, nItems);
@@ -743,21 +759,24 @@ int Plan::enqueue_range(cudaStream_t s, int first, int last, cudaEvent_t* ev)
         }
         if (chainLag >= first && chainLag < last)
         {
-            // staggered: chain 1 starts once chain 0 has finished stage chainLag
+            // staggered: the other chains start once chain 0 has finished stage chainLag
             I360B_TRY(enqueue_chain(0, first, chainLag, s));
             I360B_CUDA(cudaEventRecord(evLag, s), "chain stagger");
-            I360B_CUDA(cudaStreamWaitEvent(side, evLag, 0), "chain stagger");
+            for (int c = 1; c < nChains; ++c) I360B_CUDA(cudaStreamWaitEvent(side[c - 1], evLag, 0), "chain stagger");
             I360B_TRY(enqueue_chain(0, chainLag + 1, last, s));
         }
         else
         {
             I360B_CUDA(cudaEventRecord(evFork, s), "chain fork");
-            I360B_CUDA(cudaStreamWaitEvent(side, evFork, 0), "chain fork");
+            for (int c = 1; c < nChains; ++c) I360B_CUDA(cudaStreamWaitEvent(side[c - 1], evFork, 0), "chain fork");
             I360B_TRY(enqueue_chain(0, first, last, s));
         }
-        I360B_TRY(enqueue_chain(1, first, last, side));
-        I360B_CUDA(cudaEventRecord(evJoin, side), "chain join");
-        I360B_CUDA(cudaStreamWaitEvent(s, evJoin, 0), "chain join");
+        for (int c = 1; c < nChains; ++c)
+        {
+            I360B_TRY(enqueue_chain(c, first, last, side[c - 1]));
+            I360B_CUDA(cudaEventRecord(evJoin[c - 1], side[c - 1]), "chain join");
+            I360B_CUDA(cudaStreamWaitEvent(s, evJoin[c - 1], 0), "chain join");
+        }
         return I360B_SUCCESS;
     }
     // Stage by stage (every chain's part of a stage, forked and joined,
@@ -779,11 +798,14 @@ int Plan::enqueue_range(cudaStream_t s, int first, int last, cudaEvent_t* ev)
         if (nChains > 1)
         {
             I360B_CUDA(cudaEventRecord(evFork, s), "chain fork");
-            I360B_CUDA(cudaStreamWaitEvent(side, evFork, 0), "chain fork");
+            for (int c = 1; c < nChains; ++c) I360B_CUDA(cudaStreamWaitEvent(side[c - 1], evFork, 0), "chain fork");
             I360B_TRY(enqueue_chain(0, stage, stage, s));
-            I360B_TRY(enqueue_chain(1, stage, stage, side));
-            I360B_CUDA(cudaEventRecord(evJoin, side), "chain join");
-            I360B_CUDA(cudaStreamWaitEvent(s, evJoin, 0), "chain join");
+            for (int c = 1; c < nChains; ++c)
+            {
+                I360B_TRY(enqueue_chain(c, stage, stage, side[c - 1]));
+                I360B_CUDA(cudaEventRecord(evJoin[c - 1], side[c - 1]), "chain join");
+                I360B_CUDA(cudaStreamWaitEvent(s, evJoin[c - 1], 0), "chain join");
+            }
         }
         else
             I360B_TRY(enqueue_chain(0, stage, stage, s));
@@ -1220,11 +1242,11 @@ extern "C" int i360b_render_plan_autotune(i360b_render_plan* plan, void* stream,
             if (rc != I360B_SUCCESS) break;
         }
     }
-    // 3: chain split by seam time (two chains only), with the best of the above
+    // 3: chain split by seam time (several chains only), with the best of the above
     int bestP = P.chainSplit;
     if (rc == I360B_SUCCESS && P.nChains > 1 && (rc = P.set_tuning(bestR, bestS, s)) == I360B_SUCCESS)
     {
-        for (int pct : {0, 10, 20, 30})
+        for (int pct : {0, 5, 10, 15, 20, 30})
         {
             if ((rc = P.set_chain_split(pct, s)) != I360B_SUCCESS) break;
             float ms;

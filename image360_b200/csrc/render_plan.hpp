@@ -94,28 +94,27 @@ struct Plan
     std::vector<float> itemEdges;   // 16 per item (ItemSpec::edges)
     std::vector<int> tileRects;     // x, y, width, height per tile (canvas)
     std::vector<int> tileListed;    // contributors listed per tile (0: no render output)
-    // Tiles are independent, so they are split into chains of roughly equal
-    // work whose stages are enqueued on two streams inside the graph: the
+    // Tiles are independent, so they are split into up to three chains whose
+    // stages are enqueued on their own streams inside the graph: the
     // latency-bound stages of one chain (chamfer wavefront, seam search) run
-    // beside the bandwidth-bound stages of the other.
-    static constexpr int kMaxChains = 2;
+    // beside the full-GPU stages of the others.
+    static constexpr int kMaxChains = 3;
     int nChains = 1;
     std::vector<int> tileChain;          // chain of each tile
     Range dtRange[kMaxChains] = {};      // chamfer item lists in dInts, per chain
     Range seamRange[kMaxChains] = {};    // seam tile lists in dInts, per chain
-    cudaStream_t side = nullptr;         // second chain's stream
-    cudaEvent_t evFork = nullptr, evJoin = nullptr, evLag = nullptr;
-    // Chain stagger: with chainLag = L >= 0, chain 1's first stage of a run
-    // waits until chain 0 has finished stage L, so the seam search of one
-    // chain (a CTA per tile, most SMs free) runs beside the other chain's
-    // full-GPU stages instead of beside its own seam search.  -1: both
-    // chains start together.  Ordering only: the render is the same.
+    cudaStream_t side[kMaxChains - 1] = {};     // the streams of chains 1..
+    cudaEvent_t evFork = nullptr, evLag = nullptr, evJoin[kMaxChains - 1] = {};
+    // Chain stagger: with chainLag = L >= 0, the other chains' first stage of
+    // a run waits until chain 0 has finished stage L.  -1: all chains start
+    // together.  Ordering only: the render is the same.
     int chainLag = -1;
-    // Chain split: 0 = two chains of about equal work (area x contributors);
-    // p > 0 = the p percent of tiles whose seam step took longest in the
-    // last execution form the first chain, so their seam searches (a CTA per
-    // tile, sequential over lines) start early and run beside the second
-    // chain's full-GPU stages instead of deciding the end of one stage.
+    // Chain split: 0 = chains of about equal work (area x contributors);
+    // p > 0 = tiles in order of their seam step's time in the last execution,
+    // slowest first: the first p percent form chain 0, the next p percent
+    // chain 1, the rest the last chain - so the slow seam searches (a CTA per
+    // tile, sequential over lines) start early and run beside the full-GPU
+    // stages of the chains behind them instead of deciding the end of a stage.
     int chainSplit = 0;
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t graphExec = nullptr;

@@ -432,27 +432,26 @@ I360B_API int i360b_render_plan_get_tuning(i360b_render_plan* plan, int* bandRow
                                            int* warpShape);
 I360B_API int i360b_render_plan_set_tuning(i360b_render_plan* plan, int bandRows, int dtSlots, int fusedLevels,
                                            int warpShape, void* stream);
-/* Chain stagger.  A plan splits its tiles into two chains of about equal
- * work whose stages run on two streams inside its graph.  With stage L >= 0
- * the second chain starts only once the first has finished stage L (of the
- * stages a run covers), so the seam search of one chain (a CTA per tile,
- * most SMs free) overlaps the other chain's full-GPU stages; -1 starts both
- * together (the default: on the 90-tile panorama a stagger measured no
- * faster for whole runs and slower for runs split after stage 0, so the
- * autotuner leaves it).  Ordering only: every setting renders the same
- * bits.  A plan with one chain reports -1.
+/* Chain stagger.  A plan splits its tiles into up to three chains whose
+ * stages run on their own streams inside its graph.  With stage L >= 0 the
+ * other chains start only once the first has finished stage L (of the
+ * stages a run covers); -1 starts them together (the default: on the
+ * 90-tile panorama a stagger measured no faster for whole runs and slower
+ * for runs split after stage 0, so the autotuner leaves it).  Ordering only:
+ * every setting renders the same bits.  A plan with one chain reports -1.
  * Synchronous on `stream`; the next execute recaptures the plan's graph.
  * No reference counterpart. */
 I360B_API int i360b_render_plan_set_chain_lag(i360b_render_plan* plan, int stage, void* stream);
-/* Chain split.  0: the two chains carry about equal work (area x
- * contributors), the default.  p in 1..50: the p percent of tiles whose seam
- * step took longest in the plan's last execution (the seam search runs one
+/* Chain split.  0: the chains carry about equal work (area x contributors),
+ * the default.  p in 1..50: the tiles ordered by the time their seam step
+ * took in the plan's last execution, slowest first (the seam search runs one
  * CTA per tile, sequentially over contested lines, so its slowest tile sets
- * the stage's length while most SMs are free) form the first chain, the rest
- * the second: the slow seam searches start early and run beside the other
- * chain's full-GPU stages.  INVALID_PARAM for p outside 0..50, or for p > 0
- * before the plan has executed once.  Ordering only: every setting renders
- * the same bits.  The autotuner tries 0, 10, 20 and 30.  Synchronous on
+ * the stage's length while most SMs are free): the first p percent form the
+ * first chain, the next p percent the second (with three chains), the rest
+ * the last.  The slow seam searches start early and run beside the full-GPU
+ * stages of the chains behind them.  INVALID_PARAM for p outside 0..50, or
+ * for p > 0 before the plan has executed once.  Ordering only: every setting
+ * renders the same bits.  The autotuner tries 0, 5, 10, 15, 20 and 30.  Synchronous on
  * `stream`; the next execute recaptures the plan's graph.  No reference
  * counterpart. */
 I360B_API int i360b_render_plan_set_chain_split(i360b_render_plan* plan, int percent, void* stream);
