@@ -1048,11 +1048,187 @@ __device__ __forceinline__ void seam_column_band(const uint32_t* covI, const uin
     outHi = hi;
 }
 
+// The seam DP of one pair on one warp while its values stay small integers
+// (SeamBlend.cpp:362-407).  Candidate costs are sums of absolute differences
+// of 16-bit values, so every value of the DP - cost, previous value, penalty
+// 2|t - pt| - is an integer; while they stay below 2^23 every FP32 operation
+// of the reference on them is exact (the warp form runs on lines shorter
+// than 2^20 pixels, so penalties stay below 2^21, and a cost is at most
+// 3 x 65535 < 2^18), and the minimum it scans for,
+//   b(t) = min over kk (dp[kk] + 2 |t - pt(kk)|), lowest kk on ties,
+// is an L1 distance transform: with positions in line coordinates,
+//   min over pt(kk) <= t of (dp - 2 pt)[kk] + 2 t   (a prefix minimum), and
+//   min over pt(kk) >= t of (dp + 2 pt)[kk] - 2 t   (a suffix minimum).
+// Both are warp scans over the previous line's 49 candidates, on keys
+// value * 64 + kk, so the minimum of a key is the lowest-index minimum; each
+// candidate then looks its two minima up.  Lane l holds candidates l and
+// l + 32.  After each line its largest value is checked against 2^23; where
+// it is not below, the warp stops, leaves that line's values in dpBuf[cur ^ 1], and
+// returns the line to continue from, which the general form then does with
+// the reference's own FP32 operations.  Returns via the out parameters the
+// first line not processed, and the last line, its width and cur.
+__device__ __forceinline__ void seam_dp_warp(const int* sList, const int* sLo, const int* sHi, int* sPrev,
+                                          unsigned char* sBack, const float* costs, int nC, int lineLen,
+                                          float (*dpBuf)[64], int lane, int& outStart, int& outLast,
+                                          int& outLastW, int& outCur)
+{
+    if (lineLen >= (1 << 20))
+    {
+        outStart = 0;  // all lines to the general form
+        outLast = -1;
+        outLastW = 0;
+        outCur = 0;
+        return;
+    }
+    constexpr int kPre = 4;
+    constexpr int kInf = 0x7fffffff;
+    const int k0 = lane, k1 = lane + 32;
+    float cq0[kPre], cq1[kPre];
+#pragma unroll
+    for (int q = 0; q < kPre; ++q)
+    {
+        cq0[q] = cq1[q] = 0.0f;
+        if (q < nC)
+        {
+            const int l = sList[q];
+            const int w = sHi[l] - sLo[l] + 1;
+            if (k0 < w) cq0[q] = costs[(size_t)l * kSeamBand + k0];
+            if (k1 < w && k1 < kSeamBand) cq1[q] = costs[(size_t)l * kSeamBand + k1];
+        }
+    }
+    float dp0 = 0.0f, dp1 = 0.0f;  // the previous line's values of candidates k0, k1
+    int last = -1, lastLo = 0, lastW = 0, cur = 0;
+    int ci2 = 0;
+    for (; ci2 < nC; ++ci2)
+    {
+        const int line = sList[ci2];
+        const int lo = sLo[line], lw = sHi[line] - lo + 1;
+        const float c0 = cq0[0], c1 = cq1[0];
+#pragma unroll
+        for (int q = 0; q + 1 < kPre; ++q)
+        {
+            cq0[q] = cq0[q + 1];
+            cq1[q] = cq1[q + 1];
+        }
+        cq0[kPre - 1] = cq1[kPre - 1] = 0.0f;
+        if (ci2 + kPre < nC)
+        {
+            const int l = sList[ci2 + kPre];
+            const int w = sHi[l] - sLo[l] + 1;
+            if (k0 < w) cq0[kPre - 1] = costs[(size_t)l * kSeamBand + k0];
+            if (k1 < w && k1 < kSeamBand) cq1[kPre - 1] = costs[(size_t)l * kSeamBand + k1];
+        }
+        float v0 = c0, v1 = c1;
+        int bp0 = -1, bp1 = -1;
+        if (last >= 0)
+        {
+            // keys of the previous candidates: slot a = kk (lane), slot b = kk + 32
+            int pa = kInf, pb = kInf, sa = kInf, sb = kInf;
+            if (k0 < lastW)
+            {
+                const int d = __float2int_rn(dp0);
+                pa = (d - 2 * k0) * 64 + k0;
+                sa = (d + 2 * k0) * 64 + k0;
+            }
+            if (k1 < lastW)
+            {
+                const int d = __float2int_rn(dp1);
+                pb = (d - 2 * k1) * 64 + k1;
+                sb = (d + 2 * k1) * 64 + k1;
+            }
+#pragma unroll
+            for (int d = 1; d < 32; d <<= 1)
+            {
+                const int ta = __shfl_up_sync(kFull, pa, d), tb = __shfl_up_sync(kFull, pb, d);
+                const int ua = __shfl_down_sync(kFull, sa, d), ub = __shfl_down_sync(kFull, sb, d);
+                if (lane >= d)
+                {
+                    pa = min(pa, ta);
+                    pb = min(pb, tb);
+                }
+                if (lane + d < 32)
+                {
+                    sa = min(sa, ua);
+                    sb = min(sb, ub);
+                }
+            }
+            pb = min(pb, __shfl_sync(kFull, pa, 31));  // prefixes of slot b include all of slot a
+            sa = min(sa, __shfl_sync(kFull, sb, 0));   // suffixes of slot a include all of slot b
+            // each candidate: b(t) at t = lo + k, position j = t - lastLo in the previous line
+#pragma unroll
+            for (int h = 0; h < 2; ++h)
+            {
+                const int kc = h == 0 ? k0 : k1;
+                const int j = lo + kc - lastLo;
+                const int iF = min(max(j, 0), lastW - 1), iB = min(max(j, 0), lastW - 1);
+                const int fa = __shfl_sync(kFull, pa, iF & 31), fb = __shfl_sync(kFull, pb, iF & 31);
+                const int ba = __shfl_sync(kFull, sa, iB & 31), bb = __shfl_sync(kFull, sb, iB & 31);
+                if (kc >= lw) continue;
+                int bv = 0, bi = -1;
+                if (j >= 0)
+                {
+                    const int key = iF < 32 ? fa : fb;
+                    bv = (key >> 6) + 2 * j;
+                    bi = key & 63;
+                }
+                if (j <= lastW - 1)
+                {
+                    const int key = iB < 32 ? ba : bb;
+                    const int v = (key >> 6) - 2 * j, i = key & 63;
+                    if (bi < 0 || v < bv || (v == bv && i < bi))
+                    {
+                        bv = v;
+                        bi = i;
+                    }
+                }
+                const float val = fadd(h == 0 ? c0 : c1, (float)bv);
+                if (h == 0)
+                {
+                    v0 = val;
+                    bp0 = bi;
+                }
+                else
+                {
+                    v1 = val;
+                    bp1 = bi;
+                }
+            }
+        }
+        if (k0 < lw) sBack[(size_t)line * kSeamBand + k0] = (unsigned char)(bp0 < 0 ? 255 : bp0);
+        if (k1 < lw) sBack[(size_t)line * kSeamBand + k1] = (unsigned char)(bp1 < 0 ? 255 : bp1);
+        if (lane == 0) sPrev[line] = last;
+        dp0 = v0;
+        dp1 = v1;
+        last = line;
+        lastLo = lo;
+        lastW = lw;
+        cur ^= 1;
+        // The next line is exact if this line's values are below 2^23 (with
+        // costs below 2^18 and penalties below 2^21 its sums stay below
+        // 2^24); values are non-negative, so their bits order as the values.
+        const unsigned mv = __reduce_max_sync(kFull, max(k0 < lw ? __float_as_uint(v0) : 0u,
+                                                         k1 < lw ? __float_as_uint(v1) : 0u));
+        if (mv >= __float_as_uint(8388608.0f))
+        {
+            ++ci2;
+            break;
+        }
+    }
+    // the last line's values where the general form and the final choice read them
+    if (k0 < lastW) dpBuf[cur ^ 1][k0] = dp0;
+    if (k1 < lastW) dpBuf[cur ^ 1][k1] = dp1;
+    outStart = ci2;
+    outLast = last;
+    outLastW = lastW;
+    outCur = cur;
+}
+
 __global__ void __launch_bounds__(kSeamThreads, 1) k_seam(BlendArgs a, const int* __restrict__ tileList, int smemLines)
 {
     extern __shared__ unsigned char sm_seam[];
     __shared__ float dpBuf[2][64];
     __shared__ int sLast, sBestK;
+    __shared__ int sDpStart, sDpLast, sDpLastW, sDpCur;  // where the warp form of the DP stopped
     const int tileIndex = tileList[blockIdx.x];
     const TileDev& T = a.tiles[tileIndex];
     const long long tileStart = clock64();
@@ -1309,31 +1485,47 @@ __global__ void __launch_bounds__(kSeamThreads, 1) k_seam(BlendArgs a, const int
                 __syncthreads();
             }
             // Phase 3b: dynamic program over contested lines
-            // (SeamBlend.cpp:362-407) on the first kDpThreads threads: 8
-            // threads share a candidate k, each scanning every 8th entry of the
-            // previous line in index order; the parts merge to the lowest
-            // (value, index), which is what the reference's strict '<' scan in
-            // index order keeps.  Penalties 2|t - pt| are exact small integers
-            // formed in float.  Candidate costs are fetched kPre lines ahead.
-            if (tid < kDpThreads)
+            // (SeamBlend.cpp:362-407).  First on one warp while its values
+            // are small integers (seam_dp_warp); from the line where that
+            // stops, on the first kDpThreads threads: 8 threads share a
+            // candidate k, each scanning every 8th entry of the previous line
+            // in index order; the parts merge to the lowest (value, index),
+            // which is what the reference's strict '<' scan in index order
+            // keeps.  Penalties 2|t - pt| are exact small integers formed in
+            // float.  Candidate costs are fetched kPre lines ahead.
+            if (warp == 0)
+            {
+                int st, la, lw, cu;
+                seam_dp_warp(sList, sLo, sHi, sPrev, sBack, T.cost, sNumContested, lineLen, dpBuf, lane, st, la, lw,
+                             cu);
+                if (lane == 0)
+                {
+                    sDpStart = st;
+                    sDpLast = la;
+                    sDpLastW = lw;
+                    sDpCur = cu;
+                }
+            }
+            __syncthreads();
+            if (tid < kDpThreads && sDpStart < sNumContested)
             {
                 constexpr int kPre = 4;
                 constexpr int kParts = 8;
                 const int k = tid / kParts, part = tid % kParts;
-                const int nC = sNumContested;
+                const int nC = sNumContested, start = sDpStart;
                 float cq[kPre];
 #pragma unroll
                 for (int q = 0; q < kPre; ++q)
                 {
                     cq[q] = 0.0f;
-                    if (q < nC)
+                    if (start + q < nC)
                     {
-                        const int l = sList[q];
+                        const int l = sList[start + q];
                         if (k <= sHi[l] - sLo[l]) cq[q] = T.cost[(size_t)l * kSeamBand + k];
                     }
                 }
-                int last = -1, cur = 0, lastW = 0;
-                for (int ci2 = 0; ci2 < nC; ++ci2)
+                int last = sDpLast, cur = sDpCur, lastW = sDpLastW;
+                for (int ci2 = start; ci2 < nC; ++ci2)
                 {
                     const int line = sList[ci2];
                     const int lo = sLo[line], lw = sHi[line] - lo + 1;
@@ -1394,20 +1586,28 @@ __global__ void __launch_bounds__(kSeamThreads, 1) k_seam(BlendArgs a, const int
                 }
                 if (tid == 0)
                 {
-                    sLast = last;
-                    int bestK = 0;
-                    if (last >= 0)
-                    {
-                        float best = FLT_MAX;
-                        for (int q = 0; q < lastW; ++q)
-                            if (dpBuf[cur ^ 1][q] < best)
-                            {
-                                best = dpBuf[cur ^ 1][q];
-                                bestK = q;
-                            }
-                    }
-                    sBestK = bestK;
+                    sDpLast = last;
+                    sDpLastW = lastW;
+                    sDpCur = cur;
                 }
+            }
+            __syncthreads();
+            if (tid == 0)
+            {
+                const int last = sDpLast, lastW = sDpLastW, cur = sDpCur;
+                sLast = last;
+                int bestK = 0;
+                if (last >= 0)
+                {
+                    float best = FLT_MAX;
+                    for (int q = 0; q < lastW; ++q)
+                        if (dpBuf[cur ^ 1][q] < best)
+                        {
+                            best = dpBuf[cur ^ 1][q];
+                            bestK = q;
+                        }
+                }
+                sBestK = bestK;
             }
             __syncthreads();
             if (tid == 0) { long long now = clock64(); atomicAdd(a.seamCycles + 2, (unsigned long long)(now - tp)); tp = now; }

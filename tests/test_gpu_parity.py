@@ -254,3 +254,29 @@ def test_blend_column_scan_pitches(backend, oracle_c, w):
         assert backend.blend_chunk_contributors(bufs, w, h, out, bands) == ComputeResult.SUCCESS, backend.get_last_error()
         ref = oracle_c.blend(bufs, bands)
         assert np.array_equal(out, ref), (w, bands, int(np.abs(out.astype(int) - ref).max()))
+
+
+@pytest.mark.parametrize("hi,noise", [(60000, 0), (60000, 3000), (400, 50), (2, 1)])
+def test_blend_seam_dp_value_ranges(backend, oracle_c, hi, noise):
+    """The seam DP runs on one warp while its values stay small integers and
+    continues with the reference's general FP32 scan from the line where
+    they grow past 2^23.  Two layers with slanted edges, so the seam crosses
+    every line of their overlap: large uniform differences (every candidate
+    ties) reach that bound after a few dozen contested lines, small ones
+    never do; both must choose exactly the reference's seam, in both scan
+    directions."""
+    rng = np.random.default_rng(hi + noise)
+    w, h = 300, 200
+    yy, xx = np.mgrid[0:h, 0:w]
+    a = np.zeros((h, w, 3), np.uint16)
+    b = np.zeros((h, w, 3), np.uint16)
+    ma = xx <= 0.6 * yy + 120
+    mb = xx >= 0.6 * yy + 40
+    a[ma] = np.clip(hi + rng.integers(-noise, noise + 1, (int(ma.sum()), 3)), 1, 65535)
+    b[mb] = np.clip(1 + rng.integers(0, noise + 1, (int(mb.sum()), 3)), 1, 65535)
+    for bufs, ww, hh in (([a, b], w, h),
+                         ([np.ascontiguousarray(a.transpose(1, 0, 2)), np.ascontiguousarray(b.transpose(1, 0, 2))], h, w)):
+        out = np.zeros((hh, ww, 3), np.uint16)
+        assert backend.blend_chunk_contributors(bufs, ww, hh, out, 4) == ComputeResult.SUCCESS, backend.get_last_error()
+        ref = oracle_c.blend(bufs, 4)
+        assert np.array_equal(out, ref), (hi, noise, int(np.abs(out.astype(int) - ref).max()))
