@@ -842,6 +842,34 @@ __device__ __forceinline__ int4 support_box(int4 b, int level)
     return b;
 }
 
+// The contributor's weight support at `level` (zero weight outside): its
+// owned box grown as support_box does.
+__device__ __forceinline__ int4 owned_support(const int* bbox, int level)
+{
+    return support_box(make_int4(__ldg(bbox + kOwnedBox), __ldg(bbox + kOwnedBox + 1), __ldg(bbox + kOwnedBox + 2),
+                                 __ldg(bbox + kOwnedBox + 3)),
+                       level);
+}
+
+// Where a contributor's num/den at `level` must be right (below the top level
+// `top` of its tile): the readers take G only where the weight is non-zero -
+// the band blend of the level, the Up taps of the level below (a non-zero
+// weight one level down has non-zero weights at its taps) and, at level 1,
+// the output's taps of owned pixels - and the down step makes level l+1 at a
+// position X from level l at 2X-2 .. 2X+2.  So the box is the owned weight
+// support grown by m(level) with m(top) = 0 and m(l) = 5 + 2 m(l+1) (the
+// footprint of a grown box at l+1 reaches at most 5 beyond the support at l,
+// support_box rounding included): m(l) = 5 (2^(top-l) - 1).  Outside it a
+// pyramid step may leave num/den wrong or unwritten; the weight is right
+// everywhere (level 0's is the owner mask, and each level's weight depends
+// only on the weight below).
+__device__ __forceinline__ int4 needed_box(const int* bbox, int level, int top)
+{
+    const int4 b = owned_support(bbox, level);
+    const int m = 5 * ((1 << max(top - level, 0)) - 1);
+    return make_int4(b.x - m, b.y - m, b.z + m, b.w + m);
+}
+
 __device__ __forceinline__ int4 covered_box(const int* bbox)
 {
     return make_int4(__ldg(bbox), __ldg(bbox + 1), __ldg(bbox + 2), __ldg(bbox + 3));
@@ -862,11 +890,12 @@ __device__ __forceinline__ void load_item_cache(ItemCache& c, const BlendArgs& a
     __syncthreads();
 }
 
-// The cache's boxes as supports at `level` (after load_item_cache).
-__device__ __forceinline__ void level_boxes(ItemCache& c, const TileDev& T, int level)
+// The cache's boxes as the contributors' weight supports at `level` (after
+// load_item_cache): outside them a contributor's weight is zero.
+__device__ __forceinline__ void level_boxes(ItemCache& c, const BlendArgs& a, const TileDev& T, int level)
 {
     for (int k = threadIdx.x; k < T.numItems && k < kMaxTileItems; k += blockDim.x)
-        c.box[k] = support_box(c.box[k], level);
+        c.box[k] = owned_support(a.items[T.firstItem + k].bbox, level);
     __syncthreads();
 }
 
@@ -877,9 +906,15 @@ __device__ __forceinline__ void level_boxes(ItemCache& c, const TileDev& T, int 
 __global__ void __launch_bounds__(256) k_owner(BlendArgs a, const Unit* __restrict__ units)
 {
     __shared__ ItemCache C;
+    __shared__ int obox[kMaxTileItems][4];  // the band's owned boxes, merged into the items' at the end
     const Unit u = units[blockIdx.x];
     const TileDev& T = a.tiles[u.id];
-    load_item_cache(C, a, T);
+    for (int k = threadIdx.x; k < kMaxTileItems; k += blockDim.x)
+    {
+        obox[k][0] = obox[k][1] = 0x7fffffff;
+        obox[k][2] = obox[k][3] = -1;
+    }
+    load_item_cache(C, a, T);  // (its barrier also orders the box initialisation)
     const int K = T.numItems;
     const int W = T.w;
     const long long full = (long long)W * T.h;
@@ -949,8 +984,41 @@ __global__ void __launch_bounds__(256) k_owner(BlendArgs a, const Unit* __restri
                                                             ((uint32_t)(best[3] & 0xff) << 24);
             else
                 for (int i = 0; i < n; ++i) T.owner[p + i] = (signed char)best[i];
+            // owned boxes: four pixels of one owner (the common case) as one
+            // key, the lanes of a key merged before one shared-memory update
+            const bool one = n == 4 && best[1] == best[0] && best[2] == best[0] && best[3] == best[0];
+            const int key = one ? best[0] : -2;
+            const unsigned act = __activemask();
+            const unsigned grp = __match_any_sync(act, key);
+            const int xmin = __reduce_min_sync(grp, x4), xmax = __reduce_max_sync(grp, x4 + 3);
+            if (key >= 0 && (threadIdx.x & 31) == __ffs(grp) - 1)
+            {
+                atomicMin(&obox[key][0], xmin);
+                atomicMax(&obox[key][2], xmax);
+                atomicMin(&obox[key][1], y);
+                atomicMax(&obox[key][3], y);
+            }
+            if (!one)
+                for (int i = 0; i < n; ++i)
+                    if (best[i] >= 0)
+                    {
+                        atomicMin(&obox[best[i]][0], x4 + i);
+                        atomicMax(&obox[best[i]][2], x4 + i);
+                        atomicMin(&obox[best[i]][1], y);
+                        atomicMax(&obox[best[i]][3], y);
+                    }
         }
     }
+    __syncthreads();
+    for (int k = threadIdx.x; k < K && k < kMaxTileItems; k += blockDim.x)
+        if (obox[k][2] >= 0)
+        {
+            int* ob = a.items[T.firstItem + k].bbox + kOwnedBox;
+            atomicMin(ob, obox[k][0]);
+            atomicMin(ob + 1, obox[k][1]);
+            atomicMax(ob + 2, obox[k][2]);
+            atomicMax(ob + 3, obox[k][3]);
+        }
 }
 
 // ---------------------------------------------------------------------------
@@ -1229,6 +1297,7 @@ __global__ void __launch_bounds__(kSeamThreads, 1) k_seam(BlendArgs a, const int
     __shared__ float dpBuf[2][64];
     __shared__ int sLast, sBestK;
     __shared__ int sDpStart, sDpLast, sDpLastW, sDpCur;  // where the warp form of the DP stopped
+    __shared__ int sBand[4];  // first and last contested line, lowest lo and highest hi of a pair
     const int tileIndex = tileList[blockIdx.x];
     const TileDev& T = a.tiles[tileIndex];
     const long long tileStart = clock64();
@@ -1463,6 +1532,11 @@ __global__ void __launch_bounds__(kSeamThreads, 1) k_seam(BlendArgs a, const int
                     if (lane >= d) incl += v;
                 }
                 if (lane == 31) sWarpCnt[warp] = incl;
+                if (tid == 0)
+                {
+                    sBand[0] = sBand[2] = 0x7fffffff;
+                    sBand[1] = sBand[3] = -1;
+                }
                 __syncthreads();
                 if (tid == 0)
                 {
@@ -1477,12 +1551,50 @@ __global__ void __launch_bounds__(kSeamThreads, 1) k_seam(BlendArgs a, const int
                 }
                 __syncthreads();
                 int pos = sWarpCnt[warp] + incl - c;
+                // and the box of the contested bands (lines x positions): the
+                // reassignment gives I or J pixels only inside it
+                int bl0 = 0x7fffffff, bl1 = -1, bt0 = 0x7fffffff, bt1 = -1;
                 for (int l = l0; l < l1; ++l)
                 {
                     sPrev[l] = -1;
-                    if (sHi[l] >= sLo[l]) sList[pos++] = l;
+                    if (sHi[l] >= sLo[l])
+                    {
+                        sList[pos++] = l;
+                        bl0 = min(bl0, l);
+                        bl1 = max(bl1, l);
+                        bt0 = min(bt0, sLo[l]);
+                        bt1 = max(bt1, sHi[l]);
+                    }
+                }
+                bl0 = __reduce_min_sync(kFull, bl0);
+                bl1 = __reduce_max_sync(kFull, bl1);
+                bt0 = __reduce_min_sync(kFull, bt0);
+                bt1 = __reduce_max_sync(kFull, bt1);
+                if (lane == 0 && bl1 >= 0)
+                {
+                    atomicMin(&sBand[0], bl0);
+                    atomicMax(&sBand[1], bl1);
+                    atomicMin(&sBand[2], bt0);
+                    atomicMax(&sBand[3], bt1);
                 }
                 __syncthreads();
+                if (tid == 0 && sBand[1] >= 0)
+                {
+                    // tile coordinates: a row line is a y and its positions x;
+                    // a column line the reverse
+                    const int bx0 = rowScan ? ox0 + sBand[2] : ox0 + sBand[0];
+                    const int bx1 = rowScan ? ox0 + sBand[3] : ox0 + sBand[1];
+                    const int by0 = rowScan ? oy0 + sBand[0] : oy0 + sBand[2];
+                    const int by1 = rowScan ? oy0 + sBand[1] : oy0 + sBand[3];
+                    for (int q = 0; q < 2; ++q)
+                    {
+                        int* ob = a.items[T.firstItem + (q == 0 ? ci : cj)].bbox + kOwnedBox;
+                        atomicMin(ob, bx0);
+                        atomicMin(ob + 1, by0);
+                        atomicMax(ob + 2, bx1);
+                        atomicMax(ob + 3, by1);
+                    }
+                }
             }
             // Phase 3b: dynamic program over contested lines
             // (SeamBlend.cpp:362-407).  First on one warp while its values
@@ -1811,8 +1923,12 @@ __global__ void __launch_bounds__(256) k_down(BlendArgs a, const Unit* __restric
     const int tid = threadIdx.x;
     // A footprint (rows 2Y0-2 .. 2Y0+33, columns 2X0-2 .. 2X0+65) outside
     // the contributor's support at this level reads only zeros.
+    // Likewise a block outside the box where level l+1's num/den are read
+    // (needed_box): its weights are zero.
     const int4 B = support_box(covered_box(it.bbox), level);
-    if (2 * X0 + 2 * kDnTW + 1 < B.x || 2 * X0 - 2 > B.z || 2 * Y0 + 2 * kDnTH + 1 < B.y || 2 * Y0 - 2 > B.w)
+    const int4 nb = needed_box(it.bbox, level + 1, T.bands - 1);
+    if (2 * X0 + 2 * kDnTW + 1 < B.x || 2 * X0 - 2 > B.z || 2 * Y0 + 2 * kDnTH + 1 < B.y || 2 * Y0 - 2 > B.w ||
+        X0 + kDnTW - 1 < nb.x || X0 > nb.z || Y0 + kDnTH - 1 < nb.y || Y0 > nb.w)
     {
         for (int idx = tid; idx < kDnTW * kDnTH; idx += 256)
         {
@@ -1957,7 +2073,11 @@ __global__ void __launch_bounds__(256, 4) k_down0s(BlendArgs a, const Unit* __re
     // (SeamBlend.cpp:439-442, 580) - so its outputs are exactly zero.
     {
         const int bx0 = __ldg(it.bbox), by0 = __ldg(it.bbox + 1), bx1 = __ldg(it.bbox + 2), by1 = __ldg(it.bbox + 3);
-        if (2 * X0 + 2 * kDn0W + 1 < bx0 || 2 * X0 - 2 > bx1 || 2 * Y0 + 2 * kDnTH + 1 < by0 || 2 * Y0 - 2 > by1)
+        // and a block outside the box where level 1's num/den are read (see
+        // needed_box) needs only its weights, which are zero there too
+        const int4 nb = needed_box(it.bbox, 1, T.bands - 1);
+        if (2 * X0 + 2 * kDn0W + 1 < bx0 || 2 * X0 - 2 > bx1 || 2 * Y0 + 2 * kDnTH + 1 < by0 || 2 * Y0 - 2 > by1 ||
+            X0 + kDn0W - 1 < nb.x || X0 > nb.z || Y0 + kDnTH - 1 < nb.y || Y0 > nb.w)
         {
             for (int j = 0; j < kDnTH && Y0 + j < dh; ++j)
 #pragma unroll
@@ -2210,7 +2330,7 @@ __global__ void __launch_bounds__(256, 3) k_blend_level(BlendArgs a, const Unit*
     const Unit u = units[blockIdx.x];
     const TileDev& T = a.tiles[u.id];
     load_item_cache(C, a, T);
-    level_boxes(C, T, level);
+    level_boxes(C, a, T, level);
     const int K = T.numItems;
     const int lw = T.lw[level], lh = T.lh[level];
     const bool top = level == T.bands - 1;

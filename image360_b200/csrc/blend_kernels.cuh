@@ -20,7 +20,8 @@ struct ItemDev
     uint32_t* cov;              // coverage bits, covWords per row
     float* d1;                  // chamfer forward pass
     float* d;                   // chamfer distance (final)
-    int* bbox;                  // x0, y0, x1, y1 of covered pixels (x0 > x1 = empty), then the covered count
+    int* bbox;                  // x0, y0, x1, y1 of covered pixels (x0 > x1 = empty), then the covered count;
+                                // at 8..11 the box of the pixels it owns after the seam step (see kOwnedBox)
     float4* nd;                 // pyramid levels 1.. : (num.rgb, den)
     float* wg;                  // pyramid levels 1.. : weight
     float H[9];                 // destination(tile) -> source(frame) matrix
@@ -69,6 +70,11 @@ struct Unit
 // Default limit of every bounded device wait, in SM cycles (~1 s at B200
 // clocks).
 constexpr long long kSpinCyclesDefault = 2000000000ll;
+
+// Offset in an item's bbox record of its owned box: x0, y0, x1, y1 of the
+// pixels it owns once the seam step has run (a superset: the argmax owner's
+// box grown by the seam's contested bands), x0 > x1 when it owns none.
+constexpr int kOwnedBox = 8;
 
 struct BlendArgs
 {

@@ -29,6 +29,10 @@ __global__ void k_init_bbox(ItemDev* items, int n)
     b[2] = -1;
     b[3] = -1;
     b[4] = 0;
+    b[kOwnedBox] = 0x7fffffff;
+    b[kOwnedBox + 1] = 0x7fffffff;
+    b[kOwnedBox + 2] = -1;
+    b[kOwnedBox + 3] = -1;
 }
 
 // Frame homography -> per-item destination->source matrix.
