@@ -585,6 +585,9 @@ __global__ void __launch_bounds__(32 * kDtWarps, 2) k_dt(BlendArgs a, const int*
         int seen = -1;                            // lane 0: progress of the group above already observed
         int wIdx = -4;                            // forward: coverage words wIdx .. wIdx+2 held
         uint32_t wLo = 0, wHi = 0, wNx = 0;
+        // Interior chunk: every lane's row and columns lie in the tile, so no
+        // cell is virtual (but lane 0's row above, in group 0).
+        auto is_interior = [&](int c0) { return fullGroup && c0 - 64 >= 0 && c0 + kDtChunk - 2 <= W; };
         for (int t0 = 0; t0 < nSteps; t0 += kDtChunk)
         {
             int bad = 0;
@@ -613,15 +616,11 @@ __global__ void __launch_bounds__(32 * kDtWarps, 2) k_dt(BlendArgs a, const int*
             }
             if (__shfl_sync(kFull, bad, 0)) return;  // gave up waiting (error flag set)
             const int xs = t0 - 2 * lane - 2;  // this lane's column at the chunk's first step
-            // Interior chunk: every lane's row and columns lie in the tile, so
-            // no cell is virtual (but lane 0's row above, in group 0).
-            // Interior chunk: every lane's row and columns lie in the tile, so
-            // no cell is virtual (but lane 0's row above, in group 0).
-            // Elsewhere cells outside the tile are +inf and never stored; with
-            // an even row length a column pair is in or out as a whole.  The
-            // backward pass takes its edge chunks cell by cell (fewer registers
-            // in its staged path).
-            const bool interior = fullGroup && t0 - 64 >= 0 && t0 + kDtChunk - 2 <= W;
+            // Outside interior chunks cells outside the tile are +inf and never
+            // stored; with an even row length a column pair is in or out as a
+            // whole.  The backward pass takes its edge chunks cell by cell
+            // (fewer registers in its staged path).
+            const bool interior = is_interior(t0);
             if (pairs && (!BACK || interior))
             {
                 // The chunk's initial values enter, and its results leave, this
@@ -671,11 +670,8 @@ __global__ void __launch_bounds__(32 * kDtWarps, 2) k_dt(BlendArgs a, const int*
                 // Lane 0's row above: columns t0-1 .. t0+14 (slot entries
                 // t0+3 .. t0+18) as five 16-byte reads, the same for every lane.
                 const float4* slot4 = reinterpret_cast<const float4*>(ringIn - 4) + (t0 >> 2);
-                float prevW = interior ? slot4[0].w : 0.0f;
-#pragma unroll
-                for (int m4 = 0; m4 < kDtChunk / 4; ++m4)
-                {
-                    float in[4], o[4];
+                // The chunk's initial values, four columns at a time.
+                auto chunk_in = [&](int m4, float in[4]) {
                     if (BACK)
                     {
                         const float4 v = myRow[3 - m4];  // memory columns 12-4m4 .. 15-4m4
@@ -689,28 +685,62 @@ __global__ void __launch_bounds__(32 * kDtWarps, 2) k_dt(BlendArgs a, const int*
 #pragma unroll
                         for (int i = 0; i < 4; ++i) in[i] = ((bits >> (4 * m4 + i)) & 1u) ? kInf : 0.0f;
                     }
-                    if (interior)
+                };
+                auto chunk_out = [&](int m4, const float o[4]) {
+                    if (BACK) myRow[3 - m4] = make_float4(o[3], o[2], o[1], o[0]);
+                    else myRow[m4] = make_float4(o[0], o[1], o[2], o[3]);
+                };
+                if (interior)
+                {
+                    // Every cell of the chunk is in the tile.  The sums with the
+                    // row above are carried between steps: fadd(up0, 1) is formed
+                    // one step ahead, and fadd(upm1, kDiag) is the fadd(upp1,
+                    // kDiag) of two steps back (the same operands, so the same
+                    // value).  min is exact in any order, so the candidates known
+                    // early are combined first and a step's dependency chain is
+                    // the shuffle, one add and two mins.  Lane 0 of group 0 has no
+                    // row above (+inf).
+                    const float4 inf4 = make_float4(INF, INF, INF, INF);
+                    float prevW = hasAbove ? slot4[0].w : INF;
+                    float up1 = fadd(up0, 1.0f), dg1 = fadd(up0, kDiag), dg2 = fadd(upm1, kDiag);
+                    float u1 = up0, u2 = upm1;  // the row above at x and x - 1 after the chunk
+#pragma unroll
+                    for (int m4 = 0; m4 < kDtChunk / 4; ++m4)
                     {
-                        const float4 blk = slot4[m4 + 1];
+                        float in[4], o[4];
+                        chunk_in(m4, in);
+                        const float4 blk = hasAbove ? slot4[m4 + 1] : inf4;
                         const float above[4] = {prevW, blk.x, blk.y, blk.z};
                         prevW = blk.w;
 #pragma unroll
                         for (int i = 0; i < 4; ++i)
                         {
                             const float recv = __shfl_up_sync(kFull, left, 1);
-                            const float upp1 = lane == 0 ? (hasAbove ? above[i] : INF) : recv;
-                            float av = fminf(in[i], fadd(up0, 1.0f));
-                            av = fminf(av, fadd(upm1, kDiag));
-                            av = fminf(av, fadd(upp1, kDiag));
+                            const float upp1 = lane == 0 ? above[i] : recv;
+                            const float dg = fadd(upp1, kDiag);
+                            float av = fminf(fminf(in[i], up1), dg2);
+                            av = fminf(av, dg);
                             av = fminf(av, fadd(left, 1.0f));
-                            upm1 = up0;
-                            up0 = upp1;
+                            up1 = fadd(upp1, 1.0f);
+                            dg2 = dg1;
+                            dg1 = dg;
+                            u2 = u1;
+                            u1 = upp1;
                             left = av;
                             o[i] = av;
                         }
+                        chunk_out(m4, o);
                     }
-                    else
+                    up0 = u1;
+                    upm1 = u2;
+                }
+                else
+                {
+#pragma unroll
+                    for (int m4 = 0; m4 < kDtChunk / 4; ++m4)
                     {
+                        float in[4], o[4];
+                        chunk_in(m4, in);
 #pragma unroll
                         for (int i = 0; i < 4; ++i)
                         {
@@ -731,9 +761,8 @@ __global__ void __launch_bounds__(32 * kDtWarps, 2) k_dt(BlendArgs a, const int*
                             left = d;
                             o[i] = d;
                         }
+                        chunk_out(m4, o);
                     }
-                    if (BACK) myRow[3 - m4] = make_float4(o[3], o[2], o[1], o[0]);
-                    else myRow[m4] = make_float4(o[0], o[1], o[2], o[3]);
                 }
                 // 64-byte row segments to the output.
                 __syncwarp();
