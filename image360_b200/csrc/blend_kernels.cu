@@ -176,9 +176,8 @@ __device__ __forceinline__ void warp_mix(const WarpItem& it, float fx, float fy,
     {
         const float v = fadd(fadd(fadd(fmul(w00, u2f(t00[c])), fmul(w10, u2f(t10[c]))), fmul(w01, u2f(t01[c]))),
                              fmul(w11, u2f(t11[c])));
-        unsigned short q = clamp_trunc_u16(v);
-        if (it.applyGain) q = clamp_trunc_u16(fmul(u2f(q), it.gain));
-        o[c] = q;
+        // the warp's truncation to uint16, then the gain's (one float round trip)
+        o[c] = it.applyGain ? clamp_trunc_u16(fmul(clamp_floor_u16f(v), it.gain)) : clamp_trunc_u16(v);
     }
 }
 

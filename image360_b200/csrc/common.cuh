@@ -43,6 +43,17 @@ __device__ __forceinline__ unsigned short clamp_trunc_u16(float v)
     return static_cast<unsigned short>(f2u_floor(v));  // truncation = floor on [0, 65535]
 }
 
+// (float)clamp_trunc_u16(v) without the round trip through an integer: on
+// [0, 65535], v + 2^23 rounded toward zero is 2^23 + floor(v) (the floats of
+// [2^23, 2^24) are the integers) and subtracting 2^23 is exact, so this is
+// u2f(clamp_trunc_u16(v)) bit for bit.
+__device__ __forceinline__ float clamp_floor_u16f(float v)
+{
+    v = v > 0.0f ? v : 0.0f;  // NaN -> 0
+    v = v < 65535.0f ? v : 65535.0f;
+    return __fsub_rn(__fadd_rz(v, 8388608.0f), 8388608.0f);
+}
+
 // ApplyGain's skip rule (GainColorOps.cpp:22 and RenderExecutor.cpp:111).
 __host__ __device__ __forceinline__ bool gain_is_identity(float gain)
 {

@@ -78,9 +78,14 @@ __global__ void __launch_bounds__(256) k_demosaic(const unsigned short* __restri
     const int tid = threadIdx.y * 32 + threadIdx.x;
     // Black level and white balance of one CFA value (BayerDemosaicKernels.h
     // BLS/WB steps), as the float the interpolation reads.
+    // The uint16 truncation and the float the interpolation reads in one step
+    // (clamp_floor_u16f); `mul` is the multiplier of the value's colour.
+    auto level_m = [&](unsigned raw, float mul) {
+        raw = raw > P.black ? raw - P.black : 0u;
+        return clamp_floor_u16f(fmul(u2f(raw), mul));
+    };
     auto level = [&](unsigned short raw, int gy, int gx) {
-        raw = raw > P.black ? (unsigned short)(raw - P.black) : (unsigned short)0;
-        return u2f(clamp_trunc_u16(fmul(u2f(raw), P.camMul[bayer_color(gy, gx, P.filters)])));
+        return level_m(raw, P.camMul[bayer_color(gy, gx, P.filters)]);
     };
     if ((w & 3) == 0 && (reinterpret_cast<uintptr_t>(cfa) & 7) == 0 && tx0 >= 4 && tx0 + kDmTW + 4 <= w)
     {
@@ -95,11 +100,15 @@ __global__ void __launch_bounds__(256) k_demosaic(const unsigned short* __restri
             float v[4] = {0.0f, 0.0f, 0.0f, 0.0f};
             if (gy >= 0 && gy < h)
             {
+                // gx0 is even: the four values alternate between two colours
+                // (a site's colour depends on its column only through x & 1)
+                const float me = P.camMul[bayer_color(gy, gx0, P.filters)];
+                const float mo = P.camMul[bayer_color(gy, gx0 + 1, P.filters)];
                 const uint2 q = __ldg(reinterpret_cast<const uint2*>(cfa + (size_t)gy * w + gx0));
-                v[0] = level((unsigned short)(q.x & 0xffffu), gy, gx0);
-                v[1] = level((unsigned short)(q.x >> 16), gy, gx0 + 1);
-                v[2] = level((unsigned short)(q.y & 0xffffu), gy, gx0 + 2);
-                v[3] = level((unsigned short)(q.y >> 16), gy, gx0 + 3);
+                v[0] = level_m(q.x & 0xffffu, me);
+                v[1] = level_m(q.x >> 16, mo);
+                v[2] = level_m(q.y & 0xffffu, me);
+                v[3] = level_m(q.y >> 16, mo);
             }
 #pragma unroll
             for (int k = 0; k < 4; ++k)
@@ -122,6 +131,8 @@ __global__ void __launch_bounds__(256) k_demosaic(const unsigned short* __restri
     }
     __syncthreads();
     const bool evenW = (w & 1) == 0;
+    // Every pixel of the block is an interior pixel (1 <= x <= w-2, 1 <= y <= h-2).
+    const bool blockInterior = tx0 >= 1 && ty0 >= 1 && tx0 + kDmTW <= w - 1 && ty0 + kDmTH <= h - 1;
     // The quad's 4x4 neighbourhood, read once.
     float nb[4][4];
 #pragma unroll
@@ -138,7 +149,7 @@ __global__ void __launch_bounds__(256) k_demosaic(const unsigned short* __restri
         {
             const int lx = threadIdx.x * 2 + ox, x = tx0 + lx;
             float R = 0.0f, G = 0.0f, B = 0.0f;
-            if (P.std2x2 && x >= 1 && y >= 1 && x < w - 1 && y < h - 1)
+            if (P.std2x2 && (blockInterior || (x >= 1 && y >= 1 && x < w - 1 && y < h - 1)))
             {
                 // Interior of a standard Bayer layout: the same-colour
                 // neighbours are the cross (4), the diagonals (4), or a
@@ -148,7 +159,8 @@ __global__ void __launch_bounds__(256) k_demosaic(const unsigned short* __restri
                 const float c = nb[oy + 1][ox + 1];
                 const float n = nb[oy][ox + 1], so = nb[oy + 2][ox + 1];
                 const float we = nb[oy + 1][ox], ea = nb[oy + 1][ox + 2];
-                const int cls = P.color2x2[((y & 1) << 1) | (x & 1)];
+                // tx0, ty0 and the quad's corner are even: y & 1 = oy, x & 1 = ox
+                const int cls = P.color2x2[(oy << 1) | ox];
                 if (cls != 1)
                 {
                     const float cross = ((n + we) + ea) + so;
@@ -160,7 +172,7 @@ __global__ void __launch_bounds__(256) k_demosaic(const unsigned short* __restri
                 }
                 else
                 {
-                    const int hc = P.color2x2[((y & 1) << 1) | ((x + 1) & 1)];  // colour of the left/right pair
+                    const int hc = P.color2x2[(oy << 1) | (ox ^ 1)];  // colour of the left/right pair
                     const float hp = fmul(we + ea, 0.5f), vp = fmul(n + so, 0.5f);
                     G = c;
                     R = hc == 0 ? hp : vp;
@@ -177,7 +189,7 @@ __global__ void __launch_bounds__(256) k_demosaic(const unsigned short* __restri
             }
             // Truncate to uint16 (DemosaicPixel), then the 3x4 colour matrix
             // (ApplyColorMatrixPixel, BayerDemosaicKernels.h:64-75).
-            const float r = u2f(clamp_trunc_u16(R)), g = u2f(clamp_trunc_u16(G)), b = u2f(clamp_trunc_u16(B));
+            const float r = clamp_floor_u16f(R), g = clamp_floor_u16f(G), b = clamp_floor_u16f(B);
 #pragma unroll
             for (int row = 0; row < 3; ++row)
             {
@@ -250,9 +262,7 @@ __device__ __forceinline__ void warp_pixel(const unsigned short* __restrict__ sr
         float v = fadd(fadd(fadd(fmul(w00, u2f(__ldg(r0 + c))), fmul(w10, u2f(__ldg(r0 + 3 + c)))),
                             fmul(w01, u2f(__ldg(r1 + c)))),
                        fmul(w11, u2f(__ldg(r1 + 3 + c))));
-        unsigned short q = clamp_trunc_u16(v);
-        if (P.applyGain) q = clamp_trunc_u16(fmul(u2f(q), P.gain));
-        o[c] = q;
+        o[c] = P.applyGain ? clamp_trunc_u16(fmul(clamp_floor_u16f(v), P.gain)) : clamp_trunc_u16(v);
     }
 }
 
